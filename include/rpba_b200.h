@@ -1,0 +1,181 @@
+/*
+ * rpba_b200.h -- C ABI of the B200 robust bundle adjuster.
+ *
+ * The library replaces the global robust bundle adjustment of RPBA
+ * (class LSA, rbacore.cpp) behind the reference's own entry points:
+ *
+ *   InputBlock   rpba.cpp:180-284      -> rpba_input_block
+ *   OutputBlock  rpba.cpp:288-338      -> rpba_output_block
+ *   CalcPLSA     rpba.h:693-703,
+ *                rpbacore.cpp:28-531   -> rpba_calc_plsa
+ *   EvalLSA      rpbacore.cpp:882-941  -> rpba_calc_plsa with exteval=1
+ *
+ * plus a handle API (rpba_create / rpba_solve / rpba_get_state /
+ * rpba_destroy) that keeps a problem resident on the GPU between solves.
+ *
+ * Every signature uses plain C types: pointers, sizes and status codes.
+ * No exception crosses the boundary.  All host buffers belong to the
+ * caller; device memory belongs to the handle.
+ *
+ * Data layout of a block (mirrors the containers CalcPLSA takes):
+ *   pmat        [n_images][3][4]  float, row major, PMat = [R | t]
+ *   K           [n_images][3][3]  float, row major, Camera::K
+ *   distpara    [n_images][2]     float, Camera::distpara (k1', k2')
+ *   XX          [n_points][3]     float, point coordinates (XX rows 0..2)
+ *   img_obs_off [n_images+1]      offsets of image slots (xg columns)
+ *   xg          [n_slots][2]      float, xg(0..1, slot), already negated
+ *                                 as InputBlock stores them (rpba.cpp:268-272)
+ *   wx, wy, wxy [n_slots]         float weights per slot
+ *   pt_obs_off  [n_points+1]      offsets into the per-point track lists
+ *   pt_obs_image, pt_obs_slot     [pt_obs_off[n_points]] IMAPNR entries
+ *                                 (image, pointnr) of pointXXv (rpba.h:88-93)
+ * n_slots = img_obs_off[n_images].  The track lists are rewritten in place by
+ * a solve (robustly deleted observations are removed, dropped points get an
+ * empty list), exactly as CalcPLSA rewrites pointXXvio.
+ */
+#ifndef RPBA_B200_H_
+#define RPBA_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference reports errors as "BA-Error: ..." text in its
+ * log stream and returns; the codes name the same cases. */
+typedef enum rpba_status {
+  RPBA_OK = 0,
+  RPBA_ERR_ARG = 1,             /* invalid argument or inconsistent block   */
+  RPBA_ERR_CUDA = 2,            /* CUDA runtime error                       */
+  RPBA_ERR_NO_OBS_IMAGE = 3,    /* image without observations, rbacore.cpp:415-424 */
+  RPBA_ERR_LOW_REDUNDANCY = 4,  /* redundancy < 0, rbacore.cpp:470-476      */
+  RPBA_ERR_NAN_STEP = 5,        /* NaN/Inf in the step, rbacore.cpp:541-546 */
+  RPBA_ERR_DEVICE_TIMEOUT = 6,  /* a bounded device-side wait expired       */
+  RPBA_ERR_IO = 7,              /* file could not be read or written        */
+  RPBA_ERR_UNSUPPORTED = 8,     /* input the GPU path does not accept       */
+  RPBA_ERR_NO_DEVICE = 9,       /* no CUDA device / library not usable      */
+  RPBA_ERR_SOLVER = 10          /* direct factorisation failed (not SPD)    */
+} rpba_status;
+
+typedef struct rpba_block {
+  int32_t n_images;
+  int32_t n_points;
+  float *pmat;
+  float *K;
+  float *distpara;
+  float *XX;
+  int32_t *img_obs_off;
+  float *xg;
+  float *wx;
+  float *wy;
+  float *wxy;
+  int32_t *pt_obs_off;
+  int32_t *pt_obs_image;
+  int32_t *pt_obs_slot;
+} rpba_block;
+
+/* Linear solver for the reduced camera system. */
+enum {
+  RPBA_SOLVER_PCG = 0,      /* block-Jacobi PCG with the reference's stop rule
+                               (SparsePCG, rbacore.cpp:1807-1914): the drop-in */
+  RPBA_SOLVER_DIRECT = 1,   /* dense Cholesky of the reduced camera system     */
+  RPBA_SOLVER_LEARNED = 2   /* PCG with a learned block-preconditioner correction */
+};
+
+/* Arithmetic of the assembly kernels. */
+enum {
+  RPBA_PREC_FP64 = 0,
+  RPBA_PREC_MIXED = 1       /* FP32 Jacobians / Schur assembly, FP64 cost and refinement */
+};
+
+typedef struct rpba_options {
+  int32_t robust;        /* parameters: Robust                              */
+  int32_t exteval;       /* parameters: Exteval (evaluate only, EvalLSA)    */
+  int32_t threads;       /* parameters: Threads (accepted; the GPU runs the
+                            global LSA, the reference's Threads=1 branch)   */
+  int32_t k2, k4, f;     /* parameters: k2, k4, f  -> addflags[0..2]        */
+  int32_t solver;        /* RPBA_SOLVER_*                                   */
+  int32_t precision;     /* RPBA_PREC_*                                     */
+  int32_t max_lm_iterations; /* < 0: the reference's own stop rule only;
+                                >= 0: additionally stop after this many
+                                linear solves in total                      */
+  int32_t pcg_max_iterations; /* <= 0: the reference's cap max(n_unknowns, 1000) */
+  double pcg_tolerance;  /* learned/direct-checked PCG relative tolerance
+                            (0: the reference's 1e5 decrease rule)          */
+  int32_t device;        /* CUDA device ordinal                             */
+  int32_t verbose;
+} rpba_options;
+
+/* Per-pass summary; index 0 = robust pass, 1 = refinement pass. */
+typedef struct rpba_report {
+  float sigma0_in[2];    /* sqrtf(sig0in * ihw2)                            */
+  float sigma0_out[2];   /* sqrtf(sig0old * ihw2)                           */
+  int32_t redundancy[2];
+  int32_t nrobs[2];
+  int32_t nrunknowns[2];
+  int32_t itt[2];        /* the reference's ITT counter at the end of a pass */
+  int32_t passes_done;
+  int32_t linear_solves; /* CalcBundleSep calls                             */
+  int64_t pcg_iterations;/* total PCG iterations                            */
+  int32_t pcg_fallbacks; /* learned PCG runs that fell back to the direct solve */
+  int32_t obs_deleted;   /* observations removed by RobustDelete            */
+  int32_t points_deleted;
+  int32_t points_used;   /* points kept by PointXXvIn                       */
+  double cost;           /* FP64 sum of w-weighted squared residuals, final state */
+  double rms;            /* sqrt(sum |r|^2 / n_alive) in pixels, final state */
+  float exteval_sigma0;  /* ITTTT value, rpbacore.cpp:938                   */
+  int64_t exteval_nrobs;
+  int64_t exteval_redundancy;
+  double solve_seconds;  /* device time of the solve (CUDA events)          */
+  double setup_seconds;  /* host+device time before the first LM iteration  */
+  int32_t status;
+} rpba_report;
+
+typedef struct rpba_handle rpba_handle;
+
+/* Human-readable name of a status code. */
+const char *rpba_status_string(int32_t status);
+
+/* Version string of the library build. */
+const char *rpba_version(void);
+
+/* InputBlock (rpba.cpp:180-284): parse a BAL text file into a block whose
+ * arrays are allocated by the library (free with rpba_block_free).  Same
+ * float quantisation, sign flip of the observations and k24out scaling. */
+int32_t rpba_input_block(const char *path, int32_t nraddpar, int32_t k24out,
+                         rpba_block *out);
+void rpba_block_free(rpba_block *blk);
+
+/* OutputBlock (rpba.cpp:288-338): write a block as BAL text. The per-point
+ * track lists are sorted by image in place, as the reference does. */
+int32_t rpba_output_block(const char *path, rpba_block *blk, int32_t k24out);
+
+/* CalcPLSA (rpbacore.cpp:28-531): adjust (or, with opt->exteval, evaluate)
+ * the block in place on the GPU.  The log receives the lines the reference
+ * writes to its ostream ("Sigma0: ...", "BA-Error: ...", "ITTTT: ...");
+ * pass log=NULL to skip it.  rep may be NULL. */
+int32_t rpba_calc_plsa(rpba_block *blk, const rpba_options *opt, char *log,
+                       size_t log_cap, rpba_report *rep);
+
+/* Handle API: upload once, solve many times from the uploaded state. */
+int32_t rpba_create(rpba_handle **h, const rpba_block *blk,
+                    const rpba_options *opt);
+int32_t rpba_solve(rpba_handle *h, rpba_report *rep);
+/* Copy the adjusted state into blk (pmat, K, distpara, XX, track lists). */
+int32_t rpba_get_state(rpba_handle *h, rpba_block *blk);
+/* Copy the log of the last solve (NUL terminated, truncated to cap). */
+int32_t rpba_get_log(rpba_handle *h, char *log, size_t cap);
+/* Per-observation back-projection errors of the uploaded block, in track
+ * order (dx, dy as double), as EvalLSA/CalcCorrPointMulti compute them
+ * (rpbacore.cpp:778-837, 882-941).  resid has 2*pt_obs_off[n_points]
+ * entries; entries of points with fewer than two observations are 0. */
+int32_t rpba_exteval(rpba_handle *h, double *resid, rpba_report *rep);
+void rpba_destroy(rpba_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RPBA_B200_H_ */

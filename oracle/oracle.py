@@ -1,0 +1,196 @@
+"""ctypes wrapper of the C++ oracle (test infrastructure only)."""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from rpba_b200.block import Block, RpbaBlockC, RpbaOptionsC, RpbaReportC, make_options
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+def build() -> str:
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = C.CDLL(_LIB_PATH)
+        dp = C.POINTER(C.c_double)
+        L.oracle_calc_plsa.argtypes = [C.POINTER(RpbaBlockC), C.POINTER(RpbaOptionsC), C.c_char_p,
+                                       C.c_size_t, C.POINTER(RpbaReportC)]
+        L.oracle_calc_plsa.restype = C.c_int32
+        L.oracle_exteval.argtypes = [C.POINTER(RpbaBlockC), C.POINTER(RpbaOptionsC), dp,
+                                     C.POINTER(RpbaReportC)]
+        L.oracle_exteval.restype = C.c_int32
+        L.oracle_cayley.argtypes = [C.c_double] * 3 + [dp]
+        L.oracle_rectify3.argtypes = [dp]
+        L.oracle_angleaxis_to_R.argtypes = [C.c_double] * 3 + [C.POINTER(C.c_float)]
+        L.oracle_R_to_angleaxis.argtypes = [C.POINTER(C.c_float), dp]
+        L.oracle_inv3.argtypes = [dp, dp]
+        L.oracle_inv3.restype = C.c_double
+        L.oracle_lu_inverse.argtypes = [C.c_int, dp, dp]
+        L.oracle_lsa_create.argtypes = [C.POINTER(RpbaBlockC), C.POINTER(RpbaOptionsC)]
+        L.oracle_lsa_create.restype = C.c_void_p
+        L.oracle_lsa_destroy.argtypes = [C.c_void_p]
+        for n in ("oracle_lsa_xm_size", "oracle_lsa_n_track_obs", "oracle_lsa_nrioff",
+                  "oracle_lsa_normcamera"):
+            getattr(L, n).argtypes = [C.c_void_p]
+            getattr(L, n).restype = C.c_int32
+        L.oracle_lsa_get_xm.argtypes = [C.c_void_p, dp]
+        L.oracle_lsa_residuals.argtypes = [C.c_void_p, dp, dp]
+        L.oracle_lsa_jacobian.argtypes = [C.c_void_p, C.c_int, dp, C.POINTER(C.c_int),
+                                          C.POINTER(C.c_int), dp]
+        L.oracle_input_block.argtypes = [C.c_char_p, C.c_int32, C.c_int32, C.POINTER(RpbaBlockC)]
+        L.oracle_input_block.restype = C.c_int32
+        L.oracle_block_free.argtypes = [C.POINTER(RpbaBlockC)]
+        L.oracle_output_block.argtypes = [C.c_char_p, C.POINTER(RpbaBlockC), C.c_int32]
+        L.oracle_output_block.restype = C.c_int32
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def calc_plsa(block: Block, opts: RpbaOptionsC | None = None, log_cap: int = 1 << 16):
+    """Run the oracle's CalcPLSA on a copy of ``block``.
+
+    Returns (status, adjusted block, report dict, log text)."""
+    b = block.copy()
+    cb = b.as_c()
+    o = opts if opts is not None else make_options()
+    rep = RpbaReportC()
+    buf = C.create_string_buffer(log_cap)
+    st = lib().oracle_calc_plsa(C.byref(cb), C.byref(o), buf, log_cap, C.byref(rep))
+    return st, b, rep.as_dict(), buf.value.decode()
+
+
+def exteval(block: Block, opts: RpbaOptionsC | None = None):
+    o = opts if opts is not None else make_options()
+    cb = block.as_c()
+    res = np.zeros(2 * max(block.n_obs, 1))
+    rep = RpbaReportC()
+    lib().oracle_exteval(C.byref(cb), C.byref(o), _dp(res), C.byref(rep))
+    return res[: 2 * block.n_obs].reshape(-1, 2), rep.as_dict()
+
+
+def input_block(path: str, k24out: bool = True) -> Block:
+    cb = RpbaBlockC()
+    st = lib().oracle_input_block(path.encode(), 3, int(k24out), C.byref(cb))
+    if st != 0:
+        raise IOError(f"oracle_input_block failed: {st}")
+    b = Block.from_c(cb)
+    lib().oracle_block_free(C.byref(cb))
+    return b
+
+
+def output_block(path: str, block: Block, k24out: bool = True) -> int:
+    cb = block.as_c()
+    return lib().oracle_output_block(path.encode(), C.byref(cb), int(k24out))
+
+
+def cayley(a, b, c):
+    R = np.zeros(9)
+    lib().oracle_cayley(a, b, c, _dp(R))
+    return R.reshape(3, 3)
+
+
+def rectify3(R):
+    R = np.ascontiguousarray(R, dtype=np.float64).copy()
+    lib().oracle_rectify3(_dp(R))
+    return R
+
+
+def angleaxis_to_R(a, b, c):
+    R = np.zeros(9, np.float32)
+    lib().oracle_angleaxis_to_R(a, b, c, R.ctypes.data_as(C.POINTER(C.c_float)))
+    return R.reshape(3, 3)
+
+
+def R_to_angleaxis(R):
+    R = np.ascontiguousarray(R, dtype=np.float32)
+    out = np.zeros(3)
+    lib().oracle_R_to_angleaxis(R.ctypes.data_as(C.POINTER(C.c_float)), _dp(out))
+    return out
+
+
+def inv3(m):
+    m = np.ascontiguousarray(m, dtype=np.float64)
+    out = np.zeros(9)
+    det = lib().oracle_inv3(_dp(m), _dp(out))
+    return out.reshape(3, 3), det
+
+
+def lu_inverse(A):
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    n = A.shape[0]
+    out = np.zeros(n * n)
+    lib().oracle_lu_inverse(n, _dp(A), _dp(out))
+    return out.reshape(n, n)
+
+
+class OracleLSA:
+    """An LSA after the pass-0 set-up (weights, EncodeCameras, DecodeCameras):
+    exposes the state vector, residuals and analytic Jacobians for
+    finite-difference known-answer tests."""
+
+    def __init__(self, block: Block, opts: RpbaOptionsC | None = None):
+        self._block = block
+        self._cb = block.as_c()
+        self._o = opts if opts is not None else make_options()
+        self.h = lib().oracle_lsa_create(C.byref(self._cb), C.byref(self._o))
+        if not self.h:
+            raise ValueError("degenerate block")
+
+    def close(self):
+        if self.h:
+            lib().oracle_lsa_destroy(self.h)
+            self.h = None
+
+    __del__ = close
+
+    @property
+    def n_xm(self):
+        return lib().oracle_lsa_xm_size(self.h)
+
+    @property
+    def n_obs(self):
+        return lib().oracle_lsa_n_track_obs(self.h)
+
+    @property
+    def nrioff(self):
+        return lib().oracle_lsa_nrioff(self.h)
+
+    @property
+    def normcamera(self):
+        return lib().oracle_lsa_normcamera(self.h)
+
+    def xm(self):
+        out = np.zeros(self.n_xm)
+        lib().oracle_lsa_get_xm(self.h, _dp(out))
+        return out
+
+    def residuals(self, xm):
+        xm = np.ascontiguousarray(xm, dtype=np.float64)
+        out = np.zeros(2 * self.n_obs)
+        lib().oracle_lsa_residuals(self.h, _dp(xm), _dp(out))
+        return out.reshape(-1, 2)
+
+    def jacobian(self, tobs):
+        Bc = np.zeros(18)
+        Bp = np.zeros(6)
+        nc = C.c_int()
+        co = C.c_int()
+        lib().oracle_lsa_jacobian(self.h, tobs, _dp(Bc), C.byref(nc), C.byref(co), _dp(Bp))
+        return Bc.reshape(2, 9)[:, : nc.value], co.value, Bp.reshape(2, 3)

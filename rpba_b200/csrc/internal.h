@@ -1,0 +1,139 @@
+// internal.h -- device-side state of one global LSA and the launchers of
+// its kernels.  Host code (solver.cu) owns the buffers; kernels receive the
+// plain-pointer view DevLSA by value.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+
+namespace rpba {
+
+// Per-observation linearisation record (doubles):
+//   [0..17]  Bc (2 x 9 camera Jacobian, row major)
+//   [18..23] G  = W Jp (2 x 3)
+//   [24..25] e  = W d
+//   [26..28] M  = W - G V^-1 G^T  (M00, M01, M11)
+//   [29..30] m  = e - G V^-1 g
+constexpr int REC = 32;
+// Per-point record: V^-1 (9, row major) and g (3).
+constexpr int PREC = 12;
+
+struct DevLSA {
+  int nimg, npts, nobs;
+  int nrioff, begini, normcamera, addmask, nadd, robust;
+  int minimagenrdel;
+  double defdiff;
+  const int *camparv;  // [nimg+1]
+  int *gauge;          // [4] esvm0, esvm1, esvmaxm
+  double *Pacc;        // [nimg*12] accepted PMatrices
+  double *Kc;          // [nimg*9]  accepted intrinsics (cameras)
+  double *dc;          // [nimg*2]
+  CamState *camn;      // [nimg]    trial cameras (camerasnew, eRMnew, ePCnew)
+  double *Rb, *PCb;    // [nimg*9], [nimg*3] pass-start eRM / ePC
+  // observations in track order (point major)
+  int *o_cam, *o_slot, *o_pt;
+  float2 *o_xg;
+  float4 *o_wold, *o_w;
+  float *o_s0rmv, *o_cost, *o_wterm;
+  uint8_t *o_flag, *o_flagnew;
+  int *pt_off, *pt_id;
+  // state
+  double *XPM, *XPMn, *x;
+  // linearisation
+  double *rec, *ptV;
+  // camera-grouped observation order (the reference's nro order)
+  int *camlist, *coff;
+  // reduced camera system
+  double *blocks;  // [(nimg + nboff) * 81], diagonal blocks first
+  double *rhs;     // [nimg * 9]
+  int nboff;
+  const int *boff;     // [nboff + 1] contribution ranges of the off-diagonal blocks
+  const int2 *contrib; // (obs in the row camera, obs in the column camera)
+  const int *rowoff;   // [nimg + 1]
+  const int2 *ent;     // (column camera, block index | 0x80000000 if transposed)
+  int *err;            // device error word
+};
+
+// ---- launchers (kernels.cu)
+void launch_cost(const DevLSA &L, const double *XM, bool srmv, cudaStream_t s);
+void launch_seq_sum(const float *v, int n, float *out, cudaStream_t s);
+void launch_point_pass(const DevLSA &L, double multfact1, cudaStream_t s);
+void launch_camera_pass(const DevLSA &L, double multfact1, cudaStream_t s);
+void launch_pair_pass(const DevLSA &L, cudaStream_t s);
+void launch_backsub(const DevLSA &L, const double *xsol, cudaStream_t s);
+void launch_xcam(const DevLSA &L, const double *xsol, cudaStream_t s);
+void launch_update(const DevLSA &L, int nunk, cudaStream_t s);
+void launch_decode(const DevLSA &L, const double *XM, cudaStream_t s);
+void launch_encode(const DevLSA &L, cudaStream_t s);
+void launch_store(const DevLSA &L, int xpmsize, cudaStream_t s);
+void launch_prepare_weights(const DevLSA &L, cudaStream_t s);
+void launch_reweight(const DevLSA &L, int iflag, float *vals_scratch, float *sig00v, int *nflag,
+                     cudaStream_t s);
+void launch_final_cost(const DevLSA &L, double *partials, int nparts, cudaStream_t s);
+void launch_exteval(int n_points, const int *pt_off, const int *pt_img, const int *pt_slot,
+                    const int *img_off, const float *pmat, const float *K, const float *dist,
+                    const float *XX, const float *xg, const float *wx, const float *wy,
+                    const float *wxy, double *resid, float *ptterm, int *ptred,
+                    cudaStream_t s);
+// robust deletion: marks, then compacts into the *_n buffers
+void launch_delete_mark(const DevLSA &L, int *okeep, int *pkeep, cudaStream_t s);
+void launch_delete_compact(const DevLSA &L, const int *oidx, const int *pidx, const int *okeep,
+                           const int *pkeep, int nobs_new, int npts_new, int *o_cam_n,
+                           int *o_slot_n, int *o_pt_n, float2 *o_xg_n, float4 *o_wold_n,
+                           int *pt_off_n, int *pt_id_n, double *X_n, cudaStream_t s);
+
+// ---- PCG (pcg.cu)
+struct PcgWork {
+  double *r, *r1, *d, *q, *h, *h1, *x, *xbest, *Cinv, *partials;
+  unsigned *bar;
+  int *iters;
+};
+int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s);
+int pcg_max_grid(int device);
+
+// ---- structure (structure.cu)
+struct StructWork {
+  void *cub_tmp;
+  size_t cub_bytes;
+  unsigned *pkey, *pkey2;
+  unsigned long long *pval, *pval2;
+  int *pcnt, *poff;
+  int *ccnt;
+  unsigned *bkey;
+  int *bcnt, *boff;
+  int *nrun;
+  int *cntN, *cntT, *firstN, *firstT, *rowtmp;
+  unsigned *tkey, *tkey2;
+  int *tidx, *tidx2;
+  int2 *contrib;
+  int *rowoff;
+  int2 *ent;
+  int *iota, *iota2;
+  unsigned *ckey, *ckey2;
+};
+size_t structure_cub_bytes(int nobs, long long npairs, int nimg);
+// camera grouping: returns 0, fills camlist/coff; counts in ccnt
+void build_camera_order(DevLSA &L, StructWork &S, cudaStream_t s);
+// pair structure: returns number of off-diagonal blocks (syncs the stream)
+int build_pairs(DevLSA &L, StructWork &S, long long max_pairs, long long *npairs_out,
+                cudaStream_t s);
+void build_bsr(DevLSA &L, StructWork &S, cudaStream_t s);
+cudaError_t cub_exclusive_sum_int(void *tmp, size_t &bytes, const int *in, int *out, int n, cudaStream_t s);
+
+}  // namespace rpba
+
+#define RPBA_CUDA_CHECK(x)                                  \
+  do {                                                      \
+    cudaError_t e__ = (x);                                  \
+    if (e__ != cudaSuccess) throw rpba::CudaError(e__, #x); \
+  } while (0)
+
+namespace rpba {
+struct CudaError {
+  cudaError_t code;
+  const char *what;
+  CudaError(cudaError_t c, const char *w) : code(c), what(w) {}
+};
+}  // namespace rpba

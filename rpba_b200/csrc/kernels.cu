@@ -1,0 +1,819 @@
+// kernels.cu -- per-observation, per-point and per-camera kernels of the
+// global LSA (rbacore.cpp).  FP64 throughout (the drop-in form).
+#include <cub/cub.cuh>
+
+#include "internal.h"
+
+namespace rpba {
+
+namespace {
+
+constexpr int GRP = 8;  // lanes per point in the point-major kernels
+
+__device__ __forceinline__ double grp_sum(double v) {
+#pragma unroll
+  for (int o = GRP / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, GRP);
+  return v;
+}
+
+__device__ __forceinline__ int role_of(const DevLSA &L, int k) {
+  return k == 0 ? ROLE_ZERO : (k == L.normcamera ? ROLE_NORM : ROLE_FREE);
+}
+
+// ----------------------------------------------------------- cost pass
+// CalcCorrections with derivflag = false (rbacore.cpp:1215-1331): per
+// observation float cost term and the reweighting statistic sig0rmv.
+__global__ void k_cost(DevLSA L, const double *__restrict__ XM, int srmv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= L.nobs) return;
+  const int k = L.o_cam[i], p = L.o_pt[i];
+  const double *X = XM + L.nrioff + 3 * p;
+  const float2 xg = L.o_xg[i];
+  ObsEval e;
+  eval_obs(L.camn[k], X[0], X[1], X[2], xg.x, xg.y, L.defdiff, e);
+  if (e.nan) {
+    L.o_cost[i] = 0.f;
+    L.o_s0rmv[i] = 1.e20f;
+    return;
+  }
+  const float4 w = L.o_w[i];
+  const float val = cost_term(e.d1, e.d2, w.x, w.y, w.z);
+  L.o_cost[i] = val;
+  if (srmv) {
+    if (L.robust) {
+      const float4 wo = L.o_wold[i];
+      L.o_s0rmv[i] = cost_term(e.d1, e.d2, wo.x, wo.y, wo.z);
+    } else {
+      L.o_s0rmv[i] = val;
+    }
+  }
+}
+
+// Sequential float sum in array order: the reference accumulates its cost
+// and weight sums in float, one observation after the other
+// (rbacore.cpp:1327, 727, 881).  One warp; every lane carries the same
+// running sum, so the result is bitwise that of the sequential loop.
+__global__ void k_seq_sum(const float *__restrict__ v, int n, float *out) {
+  const int lane = threadIdx.x;
+  constexpr int U = 8;
+  float s = 0.f;
+  float cur[U], nxt[U];
+#pragma unroll
+  for (int j = 0; j < U; ++j) {
+    const int idx = j * 32 + lane;
+    cur[j] = idx < n ? v[idx] : 0.f;
+  }
+  for (int base = 0; base < n; base += 32 * U) {
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
+      const int idx = base + 32 * U + j * 32 + lane;
+      nxt[j] = idx < n ? v[idx] : 0.f;
+    }
+    const int lim = n - base;
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
+#pragma unroll 8
+      for (int l = 0; l < 32; ++l) {
+        const float t = __shfl_sync(0xffffffffu, cur[j], l);
+        if (j * 32 + l < lim) s = __fadd_rn(s, t);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < U; ++j) cur[j] = nxt[j];
+  }
+  if (lane == 0) *out = s;
+}
+
+// ---------------------------------------------------------- point pass
+// CalcCorrections/CalcDerivatives with derivflag = true, solveflag = false
+// (rbacore.cpp:1215-1348, 1420-1616): Jacobians of every observation, the
+// point block V = sum Jp^T W Jp and g = sum Jp^T W d, V damped and inverted;
+// the per-observation record for the camera, pair and back-substitution
+// kernels.
+__global__ void k_point(DevLSA L, double multfact1) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = gt / GRP, ln = gt % GRP;
+  // no early exit: the group reductions below shuffle over the full warp
+  const bool valid = p < L.npts;
+  const int t0 = valid ? L.pt_off[p] : 0, t1 = valid ? L.pt_off[p + 1] : 0;
+  double X0 = 0., X1 = 0., X2 = 0.;
+  if (valid) {
+    const double *X = L.XPM + L.nrioff + 3 * p;
+    X0 = X[0];
+    X1 = X[1];
+    X2 = X[2];
+  }
+  const int esvm[2] = {L.gauge[0], L.gauge[1]};
+  double V[9], g[3];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) V[j] = 0.;
+  g[0] = g[1] = g[2] = 0.;
+  for (int o = t0 + ln; o < t1; o += GRP) {
+    const int k = L.o_cam[o];
+    const CamState c = L.camn[k];
+    const float2 xg = L.o_xg[o];
+    ObsEval e;
+    eval_obs(c, X0, X1, X2, xg.x, xg.y, L.defdiff, e);
+    if (e.nan) L.o_s0rmv[o] = 1.e20f;
+    double Bc[2][RPBA_P], Bp[2][3];
+    jacobians<double>(c, e, role_of(L, k), esvm, L.addmask, Bc, Bp);
+    const float4 w = L.o_w[o];
+    const double W0 = w.x, W1 = w.y, W2 = w.z;
+    double G[2][3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      G[0][j] = Bp[0][j] * W0 + Bp[1][j] * W2;
+      G[1][j] = Bp[0][j] * W2 + Bp[1][j] * W1;
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+#pragma unroll
+      for (int b = 0; b < 3; ++b) V[a * 3 + b] += G[0][a] * Bp[0][b] + G[1][a] * Bp[1][b];
+      g[a] += G[0][a] * e.d1 + G[1][a] * e.d2;
+    }
+    double *r = L.rec + (size_t)o * REC;
+    const bool cam_active = k >= L.begini;
+#pragma unroll
+    for (int j = 0; j < RPBA_P; ++j) {
+      r[j] = cam_active ? Bc[0][j] : 0.;
+      r[9 + j] = cam_active ? Bc[1][j] : 0.;
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      r[18 + j] = G[0][j];
+      r[21 + j] = G[1][j];
+    }
+    r[24] = e.d1 * W0 + e.d2 * W2;
+    r[25] = e.d1 * W2 + e.d2 * W1;
+  }
+#pragma unroll
+  for (int j = 0; j < 9; ++j) V[j] = grp_sum(V[j]);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) g[j] = grp_sum(g[j]);
+  V[0] *= multfact1;
+  V[4] *= multfact1;
+  V[8] *= multfact1;
+  double Vi[9];
+  inv3<double>(V, Vi);
+  if (ln == 0 && valid) {
+    double *pv = L.ptV + (size_t)p * PREC;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) pv[j] = Vi[j];
+    pv[9] = g[0];
+    pv[10] = g[1];
+    pv[11] = g[2];
+  }
+  double vg[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) vg[a] = Vi[a * 3] * g[0] + Vi[a * 3 + 1] * g[1] + Vi[a * 3 + 2] * g[2];
+  for (int o = t0 + ln; o < t1; o += GRP) {
+    double *r = L.rec + (size_t)o * REC;
+    double G[2][3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      G[0][j] = r[18 + j];
+      G[1][j] = r[21 + j];
+    }
+    const float4 w = L.o_w[o];
+    double GV[2][3];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b) GV[a][b] = G[a][0] * Vi[b] + G[a][1] * Vi[3 + b] + G[a][2] * Vi[6 + b];
+    r[26] = (double)w.x - (GV[0][0] * G[0][0] + GV[0][1] * G[0][1] + GV[0][2] * G[0][2]);
+    r[27] = (double)w.z - (GV[0][0] * G[1][0] + GV[0][1] * G[1][1] + GV[0][2] * G[1][2]);
+    r[28] = (double)w.y - (GV[1][0] * G[1][0] + GV[1][1] * G[1][1] + GV[1][2] * G[1][2]);
+    r[29] = r[24] - (G[0][0] * vg[0] + G[0][1] * vg[1] + G[0][2] * vg[2]);
+    r[30] = r[25] - (G[1][0] * vg[0] + G[1][1] * vg[1] + G[1][2] * vg[2]);
+  }
+}
+
+// --------------------------------------------------------- camera pass
+// Diagonal blocks of the reduced camera system and its right-hand side:
+// S_kk = sum_o Bc^T (W - G V^-1 G^T) Bc, b_k = sum_o Bc^T (W d - G V^-1 g)
+// (the camera terms of rbacore.cpp:1552-1561 minus the Schur terms of
+// :1358-1360), then the damping of rbacore.cpp:1164-1170.  One CTA per
+// camera sums its observations in the reference's nro order.
+constexpr int CAM_T = 64, CAM_B = 32, CAM_W = 24;
+
+__global__ void __launch_bounds__(CAM_T) k_camera(DevLSA L, double multfact1) {
+  const int k = blockIdx.x + L.begini;
+  if (k >= L.nimg) return;
+  __shared__ double s[CAM_B][CAM_W];
+  const int tid = threadIdx.x;
+  const int beg = L.coff[k], end = L.coff[k + 1];
+  double acc = 0.;
+  int ei = 0, ej = 0;
+  if (tid < 45) {
+    int t = tid;
+    while (t >= 9 - ei) {
+      t -= 9 - ei;
+      ++ei;
+    }
+    ej = ei + t;
+  } else if (tid < 54) {
+    ei = tid - 45;
+  }
+  for (int base = beg; base < end; base += CAM_B) {
+    const int nb = min(CAM_B, end - base);
+    for (int idx = tid; idx < nb * 23; idx += CAM_T) {
+      const int ob = idx / 23, c = idx % 23;
+      const int o = L.camlist[base + ob];
+      const double *r = L.rec + (size_t)o * REC;
+      s[ob][c] = c < 18 ? r[c] : r[26 + (c - 18)];
+    }
+    __syncthreads();
+    if (tid < 45) {
+      for (int ob = 0; ob < nb; ++ob) {
+        const double b0i = s[ob][ei], b1i = s[ob][9 + ei], b0j = s[ob][ej], b1j = s[ob][9 + ej];
+        const double M00 = s[ob][18], M01 = s[ob][19], M11 = s[ob][20];
+        acc += b0i * (M00 * b0j + M01 * b1j) + b1i * (M01 * b0j + M11 * b1j);
+      }
+    } else if (tid < 54) {
+      for (int ob = 0; ob < nb; ++ob) acc += s[ob][ei] * s[ob][21] + s[ob][9 + ei] * s[ob][22];
+    }
+    __syncthreads();
+  }
+  const int np = L.camparv[k + 1] - L.camparv[k];
+  double *D = L.blocks + (size_t)k * 81;
+  if (tid < 45) {
+    double v;
+    if (ei < np && ej < np) {
+      v = acc;
+      if (ei == ej) v = __dadd_rn(__dmul_rn(v, multfact1), 1.e-2);
+    } else {
+      v = ei == ej ? 1. : 0.;
+    }
+    D[ei * 9 + ej] = v;
+    D[ej * 9 + ei] = v;
+  } else if (tid < 54) {
+    L.rhs[k * 9 + ei] = ei < np ? acc : 0.;
+  }
+}
+
+// ----------------------------------------------------------- pair pass
+// Off-diagonal blocks: S_kl = - sum_p W_pk V_p^-1 W_pl^T over the points
+// seen by both cameras (rbacore.cpp:1362-1390), with W_po = Bc^T G.  One
+// warp per block sums its contributions in a fixed order.
+__global__ void k_pair(DevLSA L) {
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int wl = threadIdx.x >> 5;
+  __shared__ double sm[8][64];
+  if (wid >= L.nboff) return;
+  double *s = sm[wl];
+  double acc[3] = {0., 0., 0.};
+  const int cb = L.boff[wid], ce = L.boff[wid + 1];
+  for (int c = cb; c < ce; ++c) {
+    const int2 pr = L.contrib[c];
+    const int p = L.o_pt[pr.x];
+    const double *rs = L.rec + (size_t)pr.x * REC;
+    const double *rt = L.rec + (size_t)pr.y * REC;
+    const double *pv = L.ptV + (size_t)p * PREC;
+    for (int idx = lane; idx < 57; idx += 32)
+      s[idx] = idx < 24 ? rs[idx] : (idx < 48 ? rt[idx - 24] : pv[idx - 48]);
+    __syncwarp();
+    // N = G_s V^-1 G_t^T (2 x 2)
+    const double *Gs = s + 18, *Gt = s + 42, *Vi = s + 48;
+    double GV[2][3];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 3; ++b)
+        GV[a][b] = Gs[a * 3] * Vi[b] + Gs[a * 3 + 1] * Vi[3 + b] + Gs[a * 3 + 2] * Vi[6 + b];
+    double N[2][2];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b)
+        N[a][b] = GV[a][0] * Gt[b * 3] + GV[a][1] * Gt[b * 3 + 1] + GV[a][2] * Gt[b * 3 + 2];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const int e = lane + 32 * q;
+      if (e < 81) {
+        const int i = e / 9, j = e % 9;
+        const double bt0 = s[24 + j], bt1 = s[24 + 9 + j];
+        const double t0 = N[0][0] * bt0 + N[0][1] * bt1;
+        const double t1 = N[1][0] * bt0 + N[1][1] * bt1;
+        acc[q] -= s[i] * t0 + s[9 + i] * t1;
+      }
+    }
+    __syncwarp();
+  }
+  double *B = L.blocks + (size_t)(L.nimg + wid) * 81;
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const int e = lane + 32 * q;
+    if (e < 81) B[e] = acc[q];
+  }
+}
+
+// ------------------------------------------------- back-substitution
+// rbacore.cpp:1395-1410: dX_p = V^-1 (g - sum_o W_o^T dc_k), with
+// W_o^T dc = G^T (Bc dc).
+__global__ void k_backsub(DevLSA L, const double *__restrict__ xsol) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = gt / GRP, ln = gt % GRP;
+  const bool valid = p < L.npts;  // no early exit (full-warp shuffles below)
+  const int t0 = valid ? L.pt_off[p] : 0, t1 = valid ? L.pt_off[p + 1] : 0;
+  double a0 = 0., a1 = 0., a2 = 0.;
+  for (int o = t0 + ln; o < t1; o += GRP) {
+    const int k = L.o_cam[o];
+    if (k < L.begini) continue;
+    const double *r = L.rec + (size_t)o * REC;
+    const double *dc = xsol + (size_t)k * 9;
+    double s0 = 0., s1 = 0.;
+#pragma unroll
+    for (int a = 0; a < 9; ++a) {
+      s0 += r[a] * dc[a];
+      s1 += r[9 + a] * dc[a];
+    }
+    a0 += r[18] * s0 + r[21] * s1;
+    a1 += r[19] * s0 + r[22] * s1;
+    a2 += r[20] * s0 + r[23] * s1;
+  }
+  a0 = grp_sum(a0);
+  a1 = grp_sum(a1);
+  a2 = grp_sum(a2);
+  if (ln == 0 && valid) {
+    const double *pv = L.ptV + (size_t)p * PREC;
+    const double r0 = pv[9] - a0, r1 = pv[10] - a1, r2 = pv[11] - a2;
+    double *xo = L.x + L.nrioff + 3 * p;
+    xo[0] = pv[0] * r0 + pv[1] * r1 + pv[2] * r2;
+    xo[1] = pv[3] * r0 + pv[4] * r1 + pv[5] * r2;
+    xo[2] = pv[6] * r0 + pv[7] * r1 + pv[8] * r2;
+  }
+}
+
+// Camera entries of the step: x[k] = (float) exiv (rbacore.cpp:1181-1186).
+__global__ void k_xcam(DevLSA L, const double *__restrict__ xsol) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = i / 9 + L.begini, a = i % 9;
+  if (k >= L.nimg) return;
+  const int cp = L.camparv[k], np = L.camparv[k + 1] - cp;
+  if (a < np) L.x[cp + a] = (double)(float)xsol[(size_t)k * 9 + a];
+}
+
+// XPMatricesnew = XPMatrices - x with the NaN/Inf check (rbacore.cpp:541-548).
+__global__ void k_update(DevLSA L, int nunk) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nunk) return;
+  const double v = L.x[i];
+  if (!isfinite(v)) atomicOr(L.err, 1);
+  L.XPMn[i] = L.XPM[i] - v;
+}
+
+// ------------------------------------------------- camera (de)coding
+// DecodeCameras, rbacore.cpp:1733-1800.
+__global__ void k_decode(DevLSA L, const double *__restrict__ XM) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= L.nimg) return;
+  // a NaN step returns before DecodeCameras (rbacore.cpp:541-550): keep the
+  // previous trial cameras, which OutputLSAc reports
+  if (*(volatile int *)L.err & 1) return;
+  CamState &c = L.camn[k];
+  if (k == 0) {
+    int a = -1;
+    if (L.addmask & 1) c.d0 = XM[++a];
+    if (L.addmask & 2) c.d1 = XM[++a];
+    if (L.addmask & 4) c.K00 = c.K11 = XM[++a];
+    return;
+  }
+  const int cp = L.camparv[k];
+  double Ra[9];
+  cayley(XM[cp], XM[cp + 1], XM[cp + 2], Ra);
+  const double *B = L.Rb + (size_t)k * 9;
+  double R[9];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+#pragma unroll
+    for (int j = 0; j < 3; ++j) R[i * 3 + j] = Ra[i * 3] * B[j] + Ra[i * 3 + 1] * B[3 + j] + Ra[i * 3 + 2] * B[6 + j];
+  rectify(R, 3);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) c.R[i] = R[i];
+  double e[3];
+  if (k == L.normcamera) {
+    e[L.gauge[0]] = XM[cp + 3];
+    e[L.gauge[1]] = XM[cp + 4];
+    e[L.gauge[2]] = 0.;
+  } else {
+    e[0] = XM[cp + 3];
+    e[1] = XM[cp + 4];
+    e[2] = XM[cp + 5];
+  }
+  const double *pb = L.PCb + (size_t)k * 3;
+  c.PC[0] = e[0] + pb[0];
+  c.PC[1] = e[1] + pb[1];
+  c.PC[2] = e[2] + pb[2];
+  int a = k == L.normcamera ? 4 : 5;
+  if (L.addmask & 1) c.d0 = XM[++a + cp];
+  if (L.addmask & 2) c.d1 = XM[++a + cp];
+  if (L.addmask & 4) c.K00 = c.K11 = XM[++a + cp];
+}
+
+// EncodeCameras, rbacore.cpp:999-1087.
+__global__ void k_encode(DevLSA L) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= L.nimg) return;
+  if (k == 0) {
+    int a = -1;
+    if (L.addmask & 1) L.XPM[++a] = L.dc[0];
+    if (L.addmask & 2) L.XPM[++a] = L.dc[1];
+    if (L.addmask & 4) L.XPM[++a] = L.Kc[0];
+    return;
+  }
+  double *P = L.Pacc + (size_t)k * 12;
+  rectify(P, 4);
+  double *R = L.Rb + (size_t)k * 9;
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) R[r * 3 + c] = P[r * 4 + c];
+  double *pc = L.PCb + (size_t)k * 3;
+  for (int i = 0; i < 3; ++i) pc[i] = R[i] * P[3] + R[3 + i] * P[7] + R[6 + i] * P[11];
+  const int cp = L.camparv[k];
+  L.XPM[cp] = L.XPM[cp + 1] = L.XPM[cp + 2] = 0.;
+  int a;
+  if (k == L.normcamera) {
+    float maxv = 0.f;
+    int maxi = 0;
+    for (int i = 0; i < 3; ++i)
+      if (fabs(pc[i]) > (double)maxv) {
+        maxv = (float)fabs(pc[i]);
+        maxi = i;
+      }
+    int ii = 0;
+    for (int i = 0; i < 3; ++i)
+      if (i != maxi) L.gauge[ii++] = i;
+    L.gauge[2] = maxi;
+    L.XPM[cp + 3] = L.XPM[cp + 4] = 0.;
+    a = 4 + cp;
+  } else {
+    L.XPM[cp + 3] = L.XPM[cp + 4] = L.XPM[cp + 5] = 0.;
+    a = 5 + cp;
+  }
+  if (L.addmask & 1) L.XPM[++a] = L.dc[2 * k];
+  if (L.addmask & 2) L.XPM[++a] = L.dc[2 * k + 1];
+  if (L.addmask & 4) L.XPM[++a] = L.Kc[9 * k];
+}
+
+// StoreResultsIteration, rbacore.cpp:891-918.
+__global__ void k_store(DevLSA L, int xpmsize) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < xpmsize) L.XPM[i] = L.XPMn[i];
+  if (i < L.nobs) L.o_flagnew[i] = L.o_flag[i];
+  if (i < L.nimg) {
+    const CamState &c = L.camn[i];
+    double *P = L.Pacc + (size_t)i * 12;
+    for (int r = 0; r < 3; ++r) {
+      for (int cc = 0; cc < 3; ++cc) P[r * 4 + cc] = c.R[r * 3 + cc];
+      P[r * 4 + 3] = c.R[r * 3] * c.PC[0] + c.R[r * 3 + 1] * c.PC[1] + c.R[r * 3 + 2] * c.PC[2];
+    }
+    double *K = L.Kc + (size_t)i * 9;
+    K[0] = c.K00;
+    K[1] = c.K01;
+    K[2] = c.K02;
+    K[4] = c.K11;
+    K[5] = c.K12;
+    K[8] = 1.;
+    L.dc[2 * i] = c.d0;
+    L.dc[2 * i + 1] = c.d1;
+  }
+}
+
+// PrepareWeights2D (rbacore.cpp:704-783): Wij = Wijold and the terms of
+// the float weight sum.
+__global__ void k_prepare_weights(DevLSA L) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= L.nobs) return;
+  const float4 w = L.o_wold[i];
+  L.o_w[i] = w;
+  L.o_wterm[i] = __fadd_rn(w.x, w.y);
+  L.o_flag[i] = 0;
+  L.o_flagnew[i] = 0;
+}
+
+// ----------------------------------------------------------- reweight
+// Reweight2D, rbacore.cpp:823-887.
+__global__ void k_rw_vals(DevLSA L, float *vals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= L.nobs) return;
+  const int o = L.camlist[i];
+  const int p = L.o_pt[o];
+  int pxs = (L.pt_off[p + 1] - L.pt_off[p]) * 2;
+  if (pxs < 4) pxs = 4;
+  const float rf = __fdiv_rn((float)pxs, (float)(pxs - 3));
+  const float redfac = __fmul_rn(rf, rf);
+  vals[i] = __fmul_rn(L.o_s0rmv[o], redfac);
+}
+
+// Per-image median by an exact radix select on the float bit patterns
+// (values are >= 0, so the unsigned order is the numeric order).
+__global__ void __launch_bounds__(256) k_median(DevLSA L, const float *vals, float *sig00v, int iflag) {
+  const int k = blockIdx.x;
+  if (k >= L.nimg) return;
+  const int beg = L.coff[k], end = L.coff[k + 1], n = end - beg;
+  __shared__ unsigned hist[256];
+  __shared__ unsigned s_prefix, s_mask;
+  __shared__ int s_rank;
+  if (threadIdx.x == 0) {
+    s_prefix = 0u;
+    s_mask = 0u;
+    s_rank = n / 2;
+  }
+  __syncthreads();
+  for (int pass = 0; pass < 4; ++pass) {
+    const int shift = 24 - 8 * pass;
+    hist[threadIdx.x] = 0u;
+    __syncthreads();
+    const unsigned prefix = s_prefix, mask = s_mask;
+    for (int i = beg + threadIdx.x; i < end; i += blockDim.x) {
+      unsigned key = __float_as_uint(vals[i]);
+      if (key == 0x80000000u) key = 0u;
+      if ((key & mask) == prefix) atomicAdd(&hist[(key >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int r = s_rank;
+      unsigned b = 0;
+      for (; b < 256; ++b) {
+        if ((int)hist[b] > r) break;
+        r -= (int)hist[b];
+      }
+      if (b > 255) b = 255;
+      s_rank = r;
+      s_prefix = prefix | (b << shift);
+      s_mask = mask | (255u << shift);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    const float med = n > 0 ? __uint_as_float(s_prefix) : 0.f;
+    float s = __fdiv_rn(1.f, __fmul_rn(med, 2.1981f));
+    if (iflag > 1) s = __fmul_rn(s, 0.001f);
+    sig00v[k] = s;
+  }
+}
+
+__global__ void k_rw_apply(DevLSA L, const float *sig00v, int *nflag) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int f = 0;
+  if (i < L.nobs) {
+    float ww = __fmul_rn(L.o_s0rmv[i], sig00v[L.o_cam[i]]);
+    const bool fl = ww > 9.f;
+    L.o_flag[i] = fl ? 1 : 0;
+    if (fl) {
+      ww = 1.e-4f;
+      f = 1;
+    } else {
+      ww = 1.f;
+    }
+    const float4 wo = L.o_wold[i];
+    float4 w;
+    w.x = __fmul_rn(ww, wo.x);
+    w.y = __fmul_rn(ww, wo.y);
+    w.z = __fmul_rn(ww, wo.z);
+    w.w = 0.f;
+    if (__fadd_rn(w.x, w.y) < 2.e-8f) {
+      w.x = w.y = 1.e-8f;
+      w.z = 0.f;
+    }
+    L.o_w[i] = w;
+    L.o_wterm[i] = __fadd_rn(w.x, w.y);
+  }
+  f = __syncthreads_count(f);
+  if (threadIdx.x == 0 && f) atomicAdd(nflag, f);
+}
+
+// ------------------------------------------------------ final cost
+// FP64 cost and squared residual sum of the accepted state with the
+// Exteval projection (P X, distortion, f): the shared evaluator the oracle
+// uses too.
+__global__ void k_final_cost(DevLSA L, double *partials) {
+  __shared__ double sc[256], sq[256];
+  double c = 0., q = 0.;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < L.nobs; i += gridDim.x * blockDim.x) {
+    const int k = L.o_cam[i], p = L.o_pt[i];
+    const double *M = L.Pacc + (size_t)k * 12;
+    const double *X = L.XPM + L.nrioff + 3 * p;
+    double p1 = M[0] * X[0] + M[1] * X[1] + M[2] * X[2] + M[3];
+    double p2 = M[4] * X[0] + M[5] * X[1] + M[6] * X[2] + M[7];
+    double p3 = M[8] * X[0] + M[9] * X[1] + M[10] * X[2] + M[11];
+    if (fabs(p3) < 1.e-3)
+      p3 = p3 > 0. ? 1.e3 : -1.e3;
+    else
+      p3 = 1. / p3;
+    p1 *= p3;
+    p2 *= p3;
+    const double dist = p1 * p1 + p2 * p2;
+    const double z = 1. + (L.dc[2 * k] * dist + L.dc[2 * k + 1] * dist * dist);
+    p1 *= z * L.Kc[9 * k];
+    p2 *= z * L.Kc[9 * k];
+    const float2 xg = L.o_xg[i];
+    const double dx = (double)xg.x - p1, dy = (double)xg.y - p2;
+    const float4 w = L.o_wold[i];
+    c += dx * dx * w.x + dy * dy * w.y + 2. * dx * dy * w.z;
+    q += dx * dx + dy * dy;
+  }
+  sc[threadIdx.x] = c;
+  sq[threadIdx.x] = q;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      sc[threadIdx.x] += sc[threadIdx.x + s];
+      sq[threadIdx.x] += sq[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partials[2 * blockIdx.x] = sc[0];
+    partials[2 * blockIdx.x + 1] = sq[0];
+  }
+}
+
+// ------------------------------------------------------------ Exteval
+// EvalLSA + CalcCorrPointMulti (rpbacore.cpp:778-837, 882-941): one thread
+// per point, float sums in the reference's order within the point.
+__global__ void k_exteval(int n_points, const int *__restrict__ pt_off, const int *__restrict__ pt_img,
+                          const int *__restrict__ pt_slot, const int *__restrict__ img_off,
+                          const float *__restrict__ pmat, const float *__restrict__ Kf,
+                          const float *__restrict__ dist, const float *__restrict__ XX,
+                          const float *__restrict__ xg, const float *__restrict__ wx,
+                          const float *__restrict__ wy, const float *__restrict__ wxy, double *resid,
+                          float *ptterm, int *ptred) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n_points) return;
+  const int s = pt_off[p], e = pt_off[p + 1];
+  const int n = e - s;
+  for (int j = s; j < e; ++j) resid[2 * j] = resid[2 * j + 1] = 0.;
+  if (n <= 1) {
+    ptterm[p] = 0.f;
+    ptred[p] = 0;
+    return;
+  }
+  float wsum = 0.f;
+  for (int j = s; j < e; ++j) {
+    const int sl = img_off[pt_img[j]] + pt_slot[j];
+    wsum = __fadd_rn(wsum, __fadd_rn(wx[sl], wy[sl]));
+  }
+  wsum = __fdiv_rn(wsum, (float)(2 * n));
+  const double X0 = XX[3 * p], X1 = XX[3 * p + 1], X2 = XX[3 * p + 2];
+  float sig0 = 0.f;
+  for (int j = s; j < e; ++j) {
+    const int im = pt_img[j];
+    const int sl = img_off[im] + pt_slot[j];
+    const float *P = pmat + 12 * im;
+    double p1 = add(add(add(mul((double)P[0], X0), mul((double)P[1], X1)), mul((double)P[2], X2)), (double)P[3]);
+    double p2 = add(add(add(mul((double)P[4], X0), mul((double)P[5], X1)), mul((double)P[6], X2)), (double)P[7]);
+    double p3 = add(add(add(mul((double)P[8], X0), mul((double)P[9], X1)), mul((double)P[10], X2)), (double)P[11]);
+    if (fabs(p3) < 1.e-3)
+      p3 = p3 > 0. ? 1.e3 : -1.e3;
+    else
+      p3 = __ddiv_rn(1., p3);
+    p1 = mul(p1, p3);
+    p2 = mul(p2, p3);
+    const double dd = add(mul(p1, p1), mul(p2, p2));
+    const double z = add(1., add(mul((double)dist[2 * im], dd), mul(mul((double)dist[2 * im + 1], dd), dd)));
+    p1 = mul(p1, z);
+    p2 = mul(p2, z);
+    p1 = mul(p1, (double)Kf[9 * im]);
+    p2 = mul(p2, (double)Kf[9 * im]);
+    const double dx = sub((double)xg[2 * sl], p1), dy = sub((double)xg[2 * sl + 1], p2);
+    resid[2 * j] = dx;
+    resid[2 * j + 1] = dy;
+    const double t = add(add(mul(mul(dx, dx), (double)wx[sl]), mul(mul(dy, dy), (double)wy[sl])),
+                         mul(mul(mul(2., dx), dy), (double)wxy[sl]));
+    sig0 = __fadd_rn(sig0, (float)t);
+  }
+  ptterm[p] = __fdiv_rn(sig0, wsum);
+  ptred[p] = 2 * n - 3;
+}
+
+// ------------------------------------------------------ RobustDelete
+// rbacore.cpp:922-995: observations flagged at the last accepted step are
+// erased; a point left with fewer than minimagenrdel observations goes.
+__global__ void k_delete_mark(DevLSA L, int *okeep, int *pkeep) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= L.npts) return;
+  const int t0 = L.pt_off[p], t1 = L.pt_off[p + 1];
+  int nf = 0;
+  for (int o = t0; o < t1; ++o) nf += L.o_flagnew[o] ? 1 : 0;
+  const bool erase = nf > 0 && (t1 - t0 - nf) < L.minimagenrdel;
+  pkeep[p] = erase ? 0 : 1;
+  for (int o = t0; o < t1; ++o) okeep[o] = (!erase && !L.o_flagnew[o]) ? 1 : 0;
+}
+
+__global__ void k_delete_obs(DevLSA L, const int *oidx, const int *pidx, const int *okeep, int *o_cam_n,
+                             int *o_slot_n, int *o_pt_n, float2 *o_xg_n, float4 *o_wold_n) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= L.nobs || !okeep[o]) return;
+  const int q = oidx[o];
+  o_cam_n[q] = L.o_cam[o];
+  o_slot_n[q] = L.o_slot[o];
+  o_pt_n[q] = pidx[L.o_pt[o]];
+  o_xg_n[q] = L.o_xg[o];
+  o_wold_n[q] = L.o_wold[o];
+}
+
+__global__ void k_delete_pts(DevLSA L, const int *oidx, const int *pidx, const int *pkeep, int nobs_new,
+                             int npts_new, int *pt_off_n, int *pt_id_n, double *X_n) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p == 0) pt_off_n[npts_new] = nobs_new;
+  if (p >= L.npts || !pkeep[p]) return;
+  const int q = pidx[p];
+  pt_id_n[q] = L.pt_id[p];
+  pt_off_n[q] = oidx[L.pt_off[p]];
+  const double *X = L.XPM + L.nrioff + 3 * p;
+  X_n[3 * q] = X[0];
+  X_n[3 * q + 1] = X[1];
+  X_n[3 * q + 2] = X[2];
+}
+
+inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
+
+}  // namespace
+
+void launch_cost(const DevLSA &L, const double *XM, bool srmv, cudaStream_t s) {
+  if (L.nobs > 0) k_cost<<<nblk(L.nobs, 256), 256, 0, s>>>(L, XM, srmv ? 1 : 0);
+}
+
+void launch_seq_sum(const float *v, int n, float *out, cudaStream_t s) {
+  k_seq_sum<<<1, 32, 0, s>>>(v, n, out);
+}
+
+void launch_point_pass(const DevLSA &L, double multfact1, cudaStream_t s) {
+  if (L.npts > 0) k_point<<<nblk((long long)L.npts * GRP, 128), 128, 0, s>>>(L, multfact1);
+}
+
+void launch_camera_pass(const DevLSA &L, double multfact1, cudaStream_t s) {
+  const int nc = L.nimg - L.begini;
+  if (nc > 0) k_camera<<<nc, CAM_T, 0, s>>>(L, multfact1);
+}
+
+void launch_pair_pass(const DevLSA &L, cudaStream_t s) {
+  if (L.nboff > 0) k_pair<<<nblk((long long)L.nboff * 32, 256), 256, 0, s>>>(L);
+}
+
+void launch_backsub(const DevLSA &L, const double *xsol, cudaStream_t s) {
+  if (L.npts > 0) k_backsub<<<nblk((long long)L.npts * GRP, 128), 128, 0, s>>>(L, xsol);
+}
+
+void launch_xcam(const DevLSA &L, const double *xsol, cudaStream_t s) {
+  const int n = (L.nimg - L.begini) * 9;
+  if (n > 0) k_xcam<<<nblk(n, 256), 256, 0, s>>>(L, xsol);
+}
+
+void launch_update(const DevLSA &L, int nunk, cudaStream_t s) {
+  if (nunk > 0) k_update<<<nblk(nunk, 256), 256, 0, s>>>(L, nunk);
+}
+
+void launch_decode(const DevLSA &L, const double *XM, cudaStream_t s) {
+  k_decode<<<nblk(L.nimg, 128), 128, 0, s>>>(L, XM);
+}
+
+void launch_encode(const DevLSA &L, cudaStream_t s) { k_encode<<<nblk(L.nimg, 128), 128, 0, s>>>(L); }
+
+void launch_store(const DevLSA &L, int xpmsize, cudaStream_t s) {
+  long long n = xpmsize;
+  if (L.nobs > n) n = L.nobs;
+  if (L.nimg > n) n = L.nimg;
+  k_store<<<nblk(n, 256), 256, 0, s>>>(L, xpmsize);
+}
+
+void launch_prepare_weights(const DevLSA &L, cudaStream_t s) {
+  if (L.nobs > 0) k_prepare_weights<<<nblk(L.nobs, 256), 256, 0, s>>>(L);
+}
+
+void launch_reweight(const DevLSA &L, int iflag, float *vals, float *sig00v, int *nflag, cudaStream_t s) {
+  cudaMemsetAsync(nflag, 0, sizeof(int), s);
+  if (L.nobs > 0) k_rw_vals<<<nblk(L.nobs, 256), 256, 0, s>>>(L, vals);
+  k_median<<<L.nimg, 256, 0, s>>>(L, vals, sig00v, iflag);
+  if (L.nobs > 0) k_rw_apply<<<nblk(L.nobs, 256), 256, 0, s>>>(L, sig00v, nflag);
+}
+
+void launch_final_cost(const DevLSA &L, double *partials, int nparts, cudaStream_t s) {
+  k_final_cost<<<nparts, 256, 0, s>>>(L, partials);
+}
+
+void launch_exteval(int n_points, const int *pt_off, const int *pt_img, const int *pt_slot, const int *img_off,
+                    const float *pmat, const float *K, const float *dist, const float *XX, const float *xg,
+                    const float *wx, const float *wy, const float *wxy, double *resid, float *ptterm,
+                    int *ptred, cudaStream_t s) {
+  if (n_points > 0)
+    k_exteval<<<nblk(n_points, 128), 128, 0, s>>>(n_points, pt_off, pt_img, pt_slot, img_off, pmat, K, dist, XX,
+                                                  xg, wx, wy, wxy, resid, ptterm, ptred);
+}
+
+void launch_delete_mark(const DevLSA &L, int *okeep, int *pkeep, cudaStream_t s) {
+  if (L.npts > 0) k_delete_mark<<<nblk(L.npts, 256), 256, 0, s>>>(L, okeep, pkeep);
+}
+
+void launch_delete_compact(const DevLSA &L, const int *oidx, const int *pidx, const int *okeep, const int *pkeep,
+                           int nobs_new, int npts_new, int *o_cam_n, int *o_slot_n, int *o_pt_n, float2 *o_xg_n,
+                           float4 *o_wold_n, int *pt_off_n, int *pt_id_n, double *X_n, cudaStream_t s) {
+  if (L.nobs > 0)
+    k_delete_obs<<<nblk(L.nobs, 256), 256, 0, s>>>(L, oidx, pidx, okeep, o_cam_n, o_slot_n, o_pt_n, o_xg_n,
+                                                   o_wold_n);
+  k_delete_pts<<<nblk(L.npts > 0 ? L.npts : 1, 256), 256, 0, s>>>(L, oidx, pidx, pkeep, nobs_new, npts_new,
+                                                                  pt_off_n, pt_id_n, X_n);
+}
+
+}  // namespace rpba

@@ -1,0 +1,907 @@
+// solver.cu -- host driver of the GPU global LSA and the C ABI.
+//
+// The control flow is LSA::Adjust (rbacore.cpp:333-616) and
+// LSA::CalcBundleSep (rbacore.cpp:1094-1195): two passes (damping 1e-3 with
+// robust reweighting, then 1e-6), acceptance on the float sigma0, the
+// reference's stop counter.  Every O(observations) step runs on the GPU;
+// the host only takes the scalar decisions (one small device->host copy per
+// LM iteration).  Set-up that the reference does in its constructor
+// (PointXXvIn, PrepareCameras, PrepareIteration, rbacore.cpp:37-229,
+// 670-700, 1918-1974) runs once in rpba_create.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rpba_b200.h"
+#include "internal.h"
+
+using namespace rpba;
+
+namespace {
+
+template <typename T>
+T *dalloc(size_t n, std::vector<void *> &owned) {
+  void *p = nullptr;
+  RPBA_CUDA_CHECK(cudaMalloc(&p, sizeof(T) * (n ? n : 1)));
+  owned.push_back(p);
+  return (T *)p;
+}
+
+std::string fmt_g(double v) {
+  char b[64];
+  std::snprintf(b, sizeof b, "%g", v);
+  return b;
+}
+
+// RectifyRotationMatrix4 on the host (rpba.h:923-960), for PrepareIteration.
+void rectify_host(double *R, int rs) {
+  double a[3] = {R[2 * rs + 1] - R[rs + 2], R[2] - R[2 * rs], R[rs] - R[1]};
+  for (double &v : a)
+    if (std::fabs(v) < 1.e-20) v = 1.e-20;
+  const double al = std::sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+  for (double &v : a) v /= al;
+  const double phi = std::atan2(al, R[0] + R[rs + 1] + R[2 * rs + 2] - 1.);
+  const double q0 = std::cos(phi * 0.5), s = std::sin(phi * 0.5);
+  const double q1 = a[0] * s, q2 = a[1] * s, q3 = a[2] * s;
+  R[0] = q0 * q0 + q1 * q1 - q2 * q2 - q3 * q3;
+  R[1] = 2 * (q1 * q2 - q0 * q3);
+  R[2] = 2 * (q1 * q3 + q0 * q2);
+  R[rs] = 2 * (q2 * q1 + q0 * q3);
+  R[rs + 1] = q0 * q0 - q1 * q1 + q2 * q2 - q3 * q3;
+  R[rs + 2] = 2 * (q2 * q3 - q0 * q1);
+  R[2 * rs] = 2 * (q3 * q1 - q0 * q2);
+  R[2 * rs + 1] = 2 * (q3 * q2 + q0 * q1);
+  R[2 * rs + 2] = q0 * q0 - q1 * q1 - q2 * q2 + q3 * q3;
+}
+
+}  // namespace
+
+struct rpba_handle {
+  rpba_options opt{};
+  int dev = 0;
+  cudaStream_t s = nullptr;
+  std::vector<void *> owned;
+
+  // problem
+  int nimg = 0, XXnr = 0, n_slots = 0, n_track_in = 0;
+  std::vector<float> K_in, XX_in;
+  std::vector<int32_t> img_off_in;
+  rpba_block raw{};  // device copy of the caller's block (Exteval)
+  bool raw_uploaded = false;
+  std::vector<float> h_pmat, h_K, h_dist, h_XX, h_xg, h_wx, h_wy, h_wxy;
+  std::vector<int32_t> h_img_off, h_pt_off, h_pt_img, h_pt_slot;
+
+  // static parameterisation
+  int nadd = 0, addmask = 0, nrpari = 0, nrparir = 0, nrioff = 0, normcamera = -1, begini = 1;
+  int minimagenrdel = 2, xpmsize = 0, npts0 = 0, nobs0 = 0;
+  bool lflflag = false, robust = true;
+  float ihw2 = 1.f;
+  double defdiff = 5000.;
+  std::vector<int> camparv;
+  long long max_pairs = 0;
+  int pcg_grid = 1;
+
+  // original state (restored by every solve)
+  int *d0_o_cam, *d0_o_slot, *d0_o_pt, *d0_pt_off, *d0_pt_id;
+  float2 *d0_o_xg;
+  float4 *d0_o_wold;
+  double *d0_P, *d0_Kc, *d0_dc, *d0_X;
+  CamState *d0_camn;
+
+  // working state
+  DevLSA L{};
+  int *o_cam_n, *o_slot_n, *o_pt_n, *pt_off_n, *pt_id_n;
+  float2 *o_xg_n;
+  float4 *o_wold_n;
+  double *X_n;
+  int *okeep, *oidx, *pkeep, *pidx;
+  float *vals, *sig00v, *sums;
+  int *nflag;
+  double *fc_part;
+  int fc_nparts = 0;
+  StructWork S{};
+  PcgWork W{};
+  int blocks_cap = 0;
+  cudaEvent_t ev0, ev1;
+
+  std::string log;
+  rpba_report rep{};
+
+  ~rpba_handle() {
+    if (s) cudaStreamSynchronize(s);
+    for (void *p : owned) cudaFree(p);
+    if (s) {
+      cudaEventDestroy(ev0);
+      cudaEventDestroy(ev1);
+      cudaStreamDestroy(s);
+    }
+  }
+
+  void ensure_blocks(int nb) {
+    if (nb <= blocks_cap && L.blocks) return;
+    const int cap = std::max(nb, 1);
+    if (L.blocks) {
+      cudaFree(L.blocks);
+      cudaFree(S.ent);
+      owned.erase(std::remove(owned.begin(), owned.end(), (void *)L.blocks), owned.end());
+      owned.erase(std::remove(owned.begin(), owned.end(), (void *)S.ent), owned.end());
+    }
+    L.blocks = dalloc<double>((size_t)(nimg + cap) * 81, owned);
+    S.ent = dalloc<int2>((size_t)nimg + 2 * (size_t)cap, owned);
+    blocks_cap = cap;
+  }
+
+  float seq_sum(const float *v, int n) {
+    launch_seq_sum(v, n, sums, s);
+    float out = 0.f;
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(&out, sums, sizeof(float), cudaMemcpyDeviceToHost, s));
+    RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+    return out;
+  }
+
+  void reset();
+  int adjust();
+  bool calc_bundle_sep(double multfact, int nrunknowns);
+  void robust_delete();
+  void structure();
+};
+
+// ------------------------------------------------------------- create
+
+static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *o) {
+  H->opt = *o;
+  H->dev = o->device;
+  RPBA_CUDA_CHECK(cudaSetDevice(H->dev));
+  RPBA_CUDA_CHECK(cudaStreamCreateWithFlags(&H->s, cudaStreamNonBlocking));
+  RPBA_CUDA_CHECK(cudaEventCreate(&H->ev0));
+  RPBA_CUDA_CHECK(cudaEventCreate(&H->ev1));
+  auto &own = H->owned;
+  const int n = b->n_images, np = b->n_points;
+  H->nimg = n;
+  H->XXnr = np;
+  H->n_slots = b->img_obs_off[n];
+  H->n_track_in = b->pt_obs_off[np];
+  H->robust = o->robust != 0;
+  H->addmask = (o->k2 ? 1 : 0) | (o->k4 ? 2 : 0) | (o->f ? 4 : 0);
+  H->nadd = (o->k2 ? 1 : 0) + (o->k4 ? 1 : 0) + (o->f ? 1 : 0);
+  if (n > 65535) return RPBA_ERR_UNSUPPORTED;
+  // host copies of the caller's block (output of untouched points, Exteval)
+  H->h_pmat.assign(b->pmat, b->pmat + 12 * n);
+  H->h_K.assign(b->K, b->K + 9 * n);
+  H->h_dist.assign(b->distpara, b->distpara + 2 * n);
+  H->h_XX.assign(b->XX, b->XX + 3 * np);
+  H->h_img_off.assign(b->img_obs_off, b->img_obs_off + n + 1);
+  H->h_xg.assign(b->xg, b->xg + 2 * H->n_slots);
+  H->h_wx.assign(b->wx, b->wx + H->n_slots);
+  H->h_wy.assign(b->wy, b->wy + H->n_slots);
+  H->h_wxy.assign(b->wxy, b->wxy + H->n_slots);
+  H->h_pt_off.assign(b->pt_obs_off, b->pt_obs_off + np + 1);
+  H->h_pt_img.assign(b->pt_obs_image, b->pt_obs_image + H->n_track_in);
+  H->h_pt_slot.assign(b->pt_obs_slot, b->pt_obs_slot + H->n_track_in);
+  for (int i = 0; i < H->n_track_in; ++i) {
+    const int im = H->h_pt_img[i];
+    if (im < 0 || im >= n || H->h_pt_slot[i] < 0 || H->h_pt_slot[i] >= H->h_img_off[im + 1] - H->h_img_off[im])
+      return RPBA_ERR_ARG;
+  }
+  if (o->exteval) return RPBA_OK;
+
+  // ihw2 / defdiff for iwidth = iheight = 1 (rpba.cpp:264-265, rpbacore.cpp:87-90, rbacore.cpp:48)
+  float ihw2 = 0.f;
+  for (int i = 0; i < n; ++i) ihw2 += (float)((1 + 1) * (1 + 1)) * 0.25f;
+  ihw2 /= (float)n;
+  H->ihw2 = ihw2;
+  H->defdiff = 5000. / (double)std::sqrt(ihw2);
+  H->minimagenrdel = n > 2 ? 3 : 2;
+
+  // PointXXvIn (rbacore.cpp:1918-1974): points with >= 2 observations and |Z| > 1e-8
+  std::vector<int> pt_id, pt_off{0}, o_cam, o_slot, o_pt;
+  std::vector<float2> o_xg;
+  std::vector<float4> o_w;
+  for (int i = 0; i < np; ++i) {
+    const int s0 = H->h_pt_off[i], s1 = H->h_pt_off[i + 1];
+    int cnt = 0;
+    for (int j = s0; j < s1; ++j)
+      if (H->h_pt_img[j] > -1) ++cnt;
+    if (!(std::fabs((double)b->XX[3 * i + 2]) > 1.e-8 && cnt >= 2)) continue;
+    const int q = (int)pt_id.size();
+    for (int j = s0; j < s1; ++j) {
+      const int im = H->h_pt_img[j];
+      if (im < 0) continue;
+      for (int jj = s0; jj < j; ++jj)
+        if (H->h_pt_img[jj] == im) return RPBA_ERR_UNSUPPORTED;  // image twice in one track
+      const int sl = H->h_img_off[im] + H->h_pt_slot[j];
+      o_cam.push_back(im);
+      o_slot.push_back(H->h_pt_slot[j]);
+      o_pt.push_back(q);
+      o_xg.push_back(make_float2(b->xg[2 * sl], b->xg[2 * sl + 1]));
+      o_w.push_back(make_float4(b->wx[sl], b->wy[sl], b->wxy[sl], 0.f));
+    }
+    pt_id.push_back(i);
+    pt_off.push_back((int)o_cam.size());
+  }
+  const int npts = (int)pt_id.size(), nobs = (int)o_cam.size();
+  H->npts0 = npts;
+  H->nobs0 = nobs;
+  H->max_pairs = 0;
+  for (int q = 0; q < npts; ++q) {
+    const long long t = pt_off[q + 1] - pt_off[q];
+    H->max_pairs += t * (t - 1) / 2;
+  }
+  if (H->max_pairs > 0x7fffffffll) return RPBA_ERR_UNSUPPORTED;
+
+  // PrepareCameras (rbacore.cpp:670-700)
+  std::vector<double> P(12 * (size_t)n);
+  for (size_t i = 0; i < P.size(); ++i) P[i] = (double)b->pmat[i];
+  {
+    std::vector<double> Tv(3 * (size_t)n);
+    for (int i = 0; i < n; ++i)
+      for (int r = 0; r < 3; ++r)
+        Tv[3 * i + r] = P[12 * i + r * 4] * P[12 * i + 3] + P[12 * i + r * 4 + 1] * P[12 * i + 7] +
+                        P[12 * i + r * 4 + 2] * P[12 * i + 11];
+    double nd = 0.;
+    H->normcamera = -1;
+    for (int i = 1; i < n; ++i) {
+      double d = 0.;
+      for (int j = 0; j < 3; ++j) d += (Tv[3 * i + j] - Tv[j]) * (Tv[3 * i + j] - Tv[j]);
+      if (d > nd) {
+        nd = d;
+        H->normcamera = i;
+      }
+    }
+  }
+  if (n < 2 || H->normcamera < 1) return RPBA_ERR_ARG;
+  // PrepareIteration (rbacore.cpp:127-229)
+  rectify_host(&P[0], 4);
+  CamState c0{};
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) c0.R[r * 3 + c] = P[r * 4 + c];
+  for (int i = 0; i < 3; ++i) c0.PC[i] = c0.R[i] * P[3] + c0.R[3 + i] * P[7] + c0.R[6 + i] * P[11];
+  H->nrparir = 5 + H->nadd;
+  H->nrpari = 6 + H->nadd;
+  H->lflflag = false;
+  for (int i = 0; i < n; ++i)
+    if (b->K[9 * i] > 2.f || b->K[9 * i + 4] > 2.f) {
+      H->lflflag = true;
+      break;
+    }
+  H->nrioff = H->nadd + H->nrparir + H->nrpari * (n - 2);
+  H->begini = H->nadd > 0 ? 0 : 1;
+  H->xpmsize = n * 6 + 3 * np + 7 * n;
+  // camparv as EncodeCameras lays it out (rbacore.cpp:999-1087)
+  H->camparv.assign(n + 1, 0);
+  H->camparv[1] = H->nadd;
+  for (int k = 1; k < n; ++k) H->camparv[k + 1] = H->camparv[k] + (k == H->normcamera ? H->nrparir : H->nrpari);
+
+  std::vector<CamState> cams(n);
+  std::vector<double> Kc(9 * (size_t)n), dc(2 * (size_t)n);
+  for (int i = 0; i < n; ++i) {
+    CamState &c = cams[i];
+    c = i == 0 ? c0 : CamState{};
+    c.K00 = b->K[9 * i];
+    c.K01 = b->K[9 * i + 1];
+    c.K02 = b->K[9 * i + 2];
+    c.K11 = b->K[9 * i + 4];
+    c.K12 = b->K[9 * i + 5];
+    c.d0 = b->distpara[2 * i];
+    c.d1 = b->distpara[2 * i + 1];
+    for (int j = 0; j < 9; ++j) Kc[9 * i + j] = b->K[9 * i + j];
+    dc[2 * i] = b->distpara[2 * i];
+    dc[2 * i + 1] = b->distpara[2 * i + 1];
+  }
+  std::vector<double> X0(3 * (size_t)std::max(npts, 1));
+  for (int q = 0; q < npts; ++q)
+    for (int j = 0; j < 3; ++j) X0[3 * q + j] = (double)b->XX[3 * pt_id[q] + j];
+
+  // ---- device buffers
+  const int no = std::max(nobs, 1), npp = std::max(npts, 1);
+  H->d0_o_cam = dalloc<int>(no, own);
+  H->d0_o_slot = dalloc<int>(no, own);
+  H->d0_o_pt = dalloc<int>(no, own);
+  H->d0_o_xg = dalloc<float2>(no, own);
+  H->d0_o_wold = dalloc<float4>(no, own);
+  H->d0_pt_off = dalloc<int>(npp + 1, own);
+  H->d0_pt_id = dalloc<int>(npp, own);
+  H->d0_P = dalloc<double>(12 * (size_t)n, own);
+  H->d0_Kc = dalloc<double>(9 * (size_t)n, own);
+  H->d0_dc = dalloc<double>(2 * (size_t)n, own);
+  H->d0_X = dalloc<double>(3 * (size_t)npp, own);
+  H->d0_camn = dalloc<CamState>(n, own);
+  auto up = [&](void *d, const void *h, size_t bytes) {
+    if (bytes) RPBA_CUDA_CHECK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, H->s));
+  };
+  up(H->d0_o_cam, o_cam.data(), sizeof(int) * nobs);
+  up(H->d0_o_slot, o_slot.data(), sizeof(int) * nobs);
+  up(H->d0_o_pt, o_pt.data(), sizeof(int) * nobs);
+  up(H->d0_o_xg, o_xg.data(), sizeof(float2) * nobs);
+  up(H->d0_o_wold, o_w.data(), sizeof(float4) * nobs);
+  up(H->d0_pt_off, pt_off.data(), sizeof(int) * (npts + 1));
+  up(H->d0_pt_id, pt_id.data(), sizeof(int) * npts);
+  up(H->d0_P, P.data(), sizeof(double) * P.size());
+  up(H->d0_Kc, Kc.data(), sizeof(double) * Kc.size());
+  up(H->d0_dc, dc.data(), sizeof(double) * dc.size());
+  up(H->d0_X, X0.data(), sizeof(double) * 3 * npts);
+  up(H->d0_camn, cams.data(), sizeof(CamState) * n);
+
+  DevLSA &L = H->L;
+  L.nimg = n;
+  L.nrioff = H->nrioff;
+  L.begini = H->begini;
+  L.normcamera = H->normcamera;
+  L.addmask = H->addmask;
+  L.nadd = H->nadd;
+  L.robust = H->robust ? 1 : 0;
+  L.minimagenrdel = H->minimagenrdel;
+  L.defdiff = H->defdiff;
+  int *cp = dalloc<int>(n + 1, own);
+  up(cp, H->camparv.data(), sizeof(int) * (n + 1));
+  L.camparv = cp;
+  L.gauge = dalloc<int>(4, own);
+  L.Pacc = dalloc<double>(12 * (size_t)n, own);
+  L.Kc = dalloc<double>(9 * (size_t)n, own);
+  L.dc = dalloc<double>(2 * (size_t)n, own);
+  L.camn = dalloc<CamState>(n, own);
+  L.Rb = dalloc<double>(9 * (size_t)n, own);
+  L.PCb = dalloc<double>(3 * (size_t)n, own);
+  L.o_cam = dalloc<int>(no, own);
+  L.o_slot = dalloc<int>(no, own);
+  L.o_pt = dalloc<int>(no, own);
+  L.o_xg = dalloc<float2>(no, own);
+  L.o_wold = dalloc<float4>(no, own);
+  L.o_w = dalloc<float4>(no, own);
+  L.o_s0rmv = dalloc<float>(no, own);
+  L.o_cost = dalloc<float>(no, own);
+  L.o_wterm = dalloc<float>(no, own);
+  L.o_flag = dalloc<uint8_t>(no, own);
+  L.o_flagnew = dalloc<uint8_t>(no, own);
+  L.pt_off = dalloc<int>(npp + 1, own);
+  L.pt_id = dalloc<int>(npp, own);
+  L.XPM = dalloc<double>(H->xpmsize, own);
+  L.XPMn = dalloc<double>(H->xpmsize, own);
+  L.x = dalloc<double>(H->xpmsize, own);
+  L.rec = dalloc<double>((size_t)no * REC, own);
+  L.ptV = dalloc<double>((size_t)npp * PREC, own);
+  L.camlist = dalloc<int>(no, own);
+  L.coff = dalloc<int>(n + 1, own);
+  L.rhs = dalloc<double>(9 * (size_t)n, own);
+  L.err = dalloc<int>(4, own);
+  H->o_cam_n = dalloc<int>(no, own);
+  H->o_slot_n = dalloc<int>(no, own);
+  H->o_pt_n = dalloc<int>(no, own);
+  H->o_xg_n = dalloc<float2>(no, own);
+  H->o_wold_n = dalloc<float4>(no, own);
+  H->pt_off_n = dalloc<int>(npp + 1, own);
+  H->pt_id_n = dalloc<int>(npp, own);
+  H->X_n = dalloc<double>(3 * (size_t)npp, own);
+  H->okeep = dalloc<int>(no + 1, own);
+  H->oidx = dalloc<int>(no + 1, own);
+  H->pkeep = dalloc<int>(npp + 1, own);
+  H->pidx = dalloc<int>(npp + 1, own);
+  H->vals = dalloc<float>(no, own);
+  H->sig00v = dalloc<float>(n, own);
+  H->sums = dalloc<float>(4, own);
+  H->nflag = dalloc<int>(4, own);
+  H->fc_nparts = 296;
+  H->fc_part = dalloc<double>(2 * H->fc_nparts, own);
+  // structure work
+  StructWork &S = H->S;
+  const long long mp = std::max(H->max_pairs, 1ll);
+  const long long mb = std::min(mp, (long long)n * (n - 1) / 2 + 1);
+  S.cub_bytes = structure_cub_bytes(nobs, mp, n);
+  S.cub_tmp = dalloc<char>(S.cub_bytes, own);
+  S.pkey = dalloc<unsigned>(mp, own);
+  S.pkey2 = dalloc<unsigned>(mp, own);
+  S.pval = dalloc<unsigned long long>(mp, own);
+  S.pval2 = dalloc<unsigned long long>(mp, own);
+  S.contrib = dalloc<int2>(mp, own);
+  S.pcnt = dalloc<int>(npp + 1, own);
+  S.poff = dalloc<int>(npp + 1, own);
+  S.ccnt = dalloc<int>(n + 1, own);
+  S.bkey = dalloc<unsigned>(mb, own);
+  S.bcnt = dalloc<int>(mb + 1, own);
+  S.boff = dalloc<int>(mb + 1, own);
+  S.nrun = dalloc<int>(1, own);
+  S.cntN = dalloc<int>(n + 1, own);
+  S.cntT = dalloc<int>(n + 1, own);
+  S.firstN = dalloc<int>(n + 1, own);
+  S.firstT = dalloc<int>(n + 1, own);
+  S.rowtmp = dalloc<int>(n + 1, own);
+  S.rowoff = dalloc<int>(n + 1, own);
+  S.tkey = dalloc<unsigned>(mb, own);
+  S.tkey2 = dalloc<unsigned>(mb, own);
+  S.tidx = dalloc<int>(mb, own);
+  S.tidx2 = dalloc<int>(mb, own);
+  S.iota = dalloc<int>(no, own);
+  S.ckey = dalloc<unsigned>(no, own);
+  S.ckey2 = dalloc<unsigned>(no, own);
+  // PCG work
+  H->pcg_grid = pcg_max_grid(H->dev);
+  PcgWork &W = H->W;
+  const size_t nv = 9 * (size_t)n;
+  W.r = dalloc<double>(nv, own);
+  W.r1 = dalloc<double>(nv, own);
+  W.d = dalloc<double>(nv, own);
+  W.q = dalloc<double>(nv, own);
+  W.h = dalloc<double>(nv, own);
+  W.h1 = dalloc<double>(nv, own);
+  W.x = dalloc<double>(nv, own);
+  W.xbest = dalloc<double>(nv, own);
+  W.Cinv = dalloc<double>(81 * (size_t)n, own);
+  W.partials = dalloc<double>(4 * (size_t)H->pcg_grid, own);
+  W.bar = dalloc<unsigned>(2, own);
+  W.iters = dalloc<int>(1, own);
+  RPBA_CUDA_CHECK(cudaMemsetAsync(W.r1, 0, sizeof(double) * nv, H->s));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(W.h1, 0, sizeof(double) * nv, H->s));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(W.q, 0, sizeof(double) * nv, H->s));
+  RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
+  return RPBA_OK;
+}
+
+// Restore the uploaded input state (the LSA after its constructor).
+void rpba_handle::reset() {
+  L.nobs = nobs0;
+  L.npts = npts0;
+  auto cp = [&](void *d, const void *src, size_t bytes) {
+    if (bytes) RPBA_CUDA_CHECK(cudaMemcpyAsync(d, src, bytes, cudaMemcpyDeviceToDevice, s));
+  };
+  cp(L.o_cam, d0_o_cam, sizeof(int) * nobs0);
+  cp(L.o_slot, d0_o_slot, sizeof(int) * nobs0);
+  cp(L.o_pt, d0_o_pt, sizeof(int) * nobs0);
+  cp(L.o_xg, d0_o_xg, sizeof(float2) * nobs0);
+  cp(L.o_wold, d0_o_wold, sizeof(float4) * nobs0);
+  cp(L.pt_off, d0_pt_off, sizeof(int) * (npts0 + 1));
+  cp(L.pt_id, d0_pt_id, sizeof(int) * npts0);
+  cp(L.Pacc, d0_P, sizeof(double) * 12 * nimg);
+  cp(L.Kc, d0_Kc, sizeof(double) * 9 * nimg);
+  cp(L.dc, d0_dc, sizeof(double) * 2 * nimg);
+  cp(L.camn, d0_camn, sizeof(CamState) * nimg);
+  RPBA_CUDA_CHECK(cudaMemsetAsync(L.XPM, 0, sizeof(double) * xpmsize, s));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(L.XPMn, 0, sizeof(double) * xpmsize, s));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(L.x, 0, sizeof(double) * xpmsize, s));
+  cp(L.XPM + nrioff, d0_X, sizeof(double) * 3 * npts0);
+  RPBA_CUDA_CHECK(cudaMemsetAsync(L.err, 0, sizeof(int) * 4, s));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(L.gauge, 0, sizeof(int) * 4, s));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(L.o_flag, 0, nobs0 ? nobs0 : 1, s));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(L.o_flagnew, 0, nobs0 ? nobs0 : 1, s));
+}
+
+void rpba_handle::structure() {
+  long long npairs = 0;
+  const int nb = build_pairs(L, S, max_pairs, &npairs, s);
+  ensure_blocks(nb);
+  build_bsr(L, S, s);
+}
+
+// CalcBundleSep (rbacore.cpp:1094-1195): assemble, solve, back-substitute.
+bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
+  const double multfact1 = 1. + multfact;
+  launch_point_pass(L, multfact1, s);
+  launch_camera_pass(L, multfact1, s);
+  launch_pair_pass(L, s);
+  int msize = 0;
+  for (int k = begini; k < nimg; ++k) msize += camparv[k + 1] - camparv[k];
+  if (msize < 1000) msize = 1000;
+  if (opt.pcg_max_iterations > 0) msize = opt.pcg_max_iterations;
+  pcg_solve(L, W, msize, pcg_grid, s);
+  launch_backsub(L, W.xbest, s);
+  launch_xcam(L, W.xbest, s);
+  launch_update(L, nrunknowns, s);
+  RPBA_CUDA_CHECK(cudaGetLastError());
+  return false;
+}
+
+// RobustDelete (rbacore.cpp:922-995) as a device compaction.
+void rpba_handle::robust_delete() {
+  const int no = L.nobs, np = L.npts;
+  RPBA_CUDA_CHECK(cudaMemsetAsync(okeep + no, 0, sizeof(int), s));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(pkeep + np, 0, sizeof(int), s));
+  launch_delete_mark(L, okeep, pkeep, s);
+  size_t bytes = S.cub_bytes;
+  RPBA_CUDA_CHECK(cub_exclusive_sum_int(S.cub_tmp, bytes, okeep, oidx, no + 1, s));
+  bytes = S.cub_bytes;
+  RPBA_CUDA_CHECK(cub_exclusive_sum_int(S.cub_tmp, bytes, pkeep, pidx, np + 1, s));
+  int tot[2];
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(&tot[0], oidx + no, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(&tot[1], pidx + np, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+  const int nobs_new = tot[0], npts_new = tot[1];
+  launch_delete_compact(L, oidx, pidx, okeep, pkeep, nobs_new, npts_new, o_cam_n, o_slot_n, o_pt_n, o_xg_n,
+                        o_wold_n, pt_off_n, pt_id_n, X_n, s);
+  std::swap(L.o_cam, o_cam_n);
+  std::swap(L.o_slot, o_slot_n);
+  std::swap(L.o_pt, o_pt_n);
+  std::swap(L.o_xg, o_xg_n);
+  std::swap(L.o_wold, o_wold_n);
+  std::swap(L.pt_off, pt_off_n);
+  std::swap(L.pt_id, pt_id_n);
+  if (npts_new > 0)
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(L.XPM + nrioff, X_n, sizeof(double) * 3 * npts_new, cudaMemcpyDeviceToDevice, s));
+  rep.obs_deleted += no - nobs_new;
+  rep.points_deleted += np - npts_new;
+  L.nobs = nobs_new;
+  L.npts = npts_new;
+}
+
+// Adjust (rbacore.cpp:333-616, itbreakflag false, no GCPs).
+int rpba_handle::adjust() {
+  int itt = 0;
+  const float sig0frac = lflflag ? 1.01f : 1.05f;
+  double multfact = 1.e-3;
+  int solves = 0;
+  bool cap_hit = false;
+  float sig0old = 0.f, sig0in = 0.f, wsum = 0.f, wsumg = 0.f;
+  int nrobsnew = 0, nrunknownsnew = 0, redundancynew = 0;
+  std::vector<int> cnt(nimg + 1);
+  for (int it = 0; it < 2; ++it) {
+    if (cap_hit) break;
+    sig0old = 1.e20f;
+    if (it > 0) multfact = 1.e-6;
+    const int imagepointnr = L.nobs;
+    int nrobs = 2 * imagepointnr;
+    build_camera_order(L, S, s);
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(cnt.data(), S.ccnt, sizeof(int) * nimg, cudaMemcpyDeviceToHost, s));
+    RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+    for (int i = 0; i < nimg; ++i)
+      if (cnt[i] == 0) {
+        if (nimg > 3) log += "BA-Error: No observations in image " + std::to_string(i) + " (image index)\n";
+        return RPBA_ERR_NO_OBS_IMAGE;
+      }
+    launch_prepare_weights(L, s);
+    wsum = seq_sum(L.o_wterm, L.nobs);
+    wsum = (float)(2 * imagepointnr) / wsum;
+    wsumg = wsum;
+    launch_encode(L, s);
+    const int nrioff3 = nrioff + 3 * L.npts;
+    int nrunknowns = nrioff3 + nadd * nimg;
+    int redundancy = nrobs - nrunknowns;
+    if (redundancy < 0) {
+      if (nimg > 3) log += "BA-Error: Low redundancy\n";
+      return RPBA_ERR_LOW_REDUNDANCY;
+    }
+    RPBA_CUDA_CHECK(cudaMemsetAsync(L.x, 0, sizeof(double) * xpmsize, s));
+    structure();
+    if (it == 0) {
+      launch_decode(L, L.XPM, s);
+      launch_cost(L, L.XPM, true, s);
+      float sig0 = seq_sum(L.o_cost, L.nobs);
+      sig0 = sig0 * wsumg / (float)redundancy;
+      sig0in = sig0old = sig0;
+    } else {
+      sig0in = sig0old;
+    }
+    int iflag = robust ? 2 : 1;
+    int iter = 1;
+    const int nunk_given = nrunknowns, nobs_given = nrobs;
+    while (iflag > 0) {
+      if (it == 0 && robust) {
+        nrunknowns = nunk_given;
+        nrobs = nobs_given;
+        launch_reweight(L, iflag, vals, sig00v, nflag, s);
+        int nf = 0;
+        RPBA_CUDA_CHECK(cudaMemcpyAsync(&nf, nflag, sizeof(int), cudaMemcpyDeviceToHost, s));
+        wsum = seq_sum(L.o_wterm, L.nobs);
+        nrobs -= 2 * nf;
+        redundancy = nrobs - nrunknowns;
+        wsum = (float)(2 * imagepointnr) / wsum;
+        wsumg = wsum;
+      }
+      calc_bundle_sep(multfact, nrunknowns);
+      ++solves;
+      launch_decode(L, L.XPMn, s);
+      launch_cost(L, L.XPMn, true, s);
+      launch_seq_sum(L.o_cost, L.nobs, sums, s);
+      struct {
+        float sig0;
+        int err;
+        int iters;
+      } hv;
+      RPBA_CUDA_CHECK(cudaMemcpyAsync(&hv.sig0, sums, sizeof(float), cudaMemcpyDeviceToHost, s));
+      RPBA_CUDA_CHECK(cudaMemcpyAsync(&hv.err, L.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+      RPBA_CUDA_CHECK(cudaMemcpyAsync(&hv.iters, W.iters, sizeof(int), cudaMemcpyDeviceToHost, s));
+      RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+      rep.pcg_iterations += hv.iters;
+      if (hv.err & 2) return RPBA_ERR_DEVICE_TIMEOUT;
+      if (hv.err & 1) return RPBA_ERR_NAN_STEP;
+      float sig0 = hv.sig0 * wsumg / (float)redundancy;
+      if (sig0old < sig0 * sig0frac) --iflag;
+      if (sig0 <= sig0old || iter == 1) {
+        launch_store(L, xpmsize, s);
+        sig0old = sig0;
+        nrobsnew = nrobs;
+        nrunknownsnew = nrunknowns;
+        redundancynew = redundancy;
+      }
+      if (itt > 200) break;
+      ++itt;
+      ++iter;
+      if (opt.max_lm_iterations >= 0 && solves >= opt.max_lm_iterations) {
+        cap_hit = true;
+        break;
+      }
+    }
+    const float s_in = std::sqrt(sig0in * ihw2), s_out = std::sqrt(sig0old * ihw2);
+    int red = redundancy, nob = nrobs, nun = nrunknowns;
+    if (it == 0 && robust) {
+      red = redundancynew;
+      nob = nrobsnew;
+      nun = nrunknownsnew;
+    }
+    log += "Sigma0: " + fmt_g(s_in) + ' ' + fmt_g(s_out) + "  " + std::to_string(red) + ' ' + std::to_string(nob) +
+           ' ' + std::to_string(nun) + "  IT: " + std::to_string(it) + "  ITT: " + std::to_string(itt) + '\n';
+    rep.sigma0_in[it] = s_in;
+    rep.sigma0_out[it] = s_out;
+    rep.redundancy[it] = red;
+    rep.nrobs[it] = nob;
+    rep.nrunknowns[it] = nun;
+    rep.itt[it] = itt;
+    rep.passes_done = it + 1;
+    if (robust && it == 0) robust_delete();
+  }
+  rep.linear_solves = solves;
+  return RPBA_OK;
+}
+
+// ------------------------------------------------------------ C ABI
+
+namespace {
+
+int guard(int (*fn)(void *), void *arg) {
+  try {
+    return fn(arg);
+  } catch (const CudaError &e) {
+    std::fprintf(stderr, "rpba_b200: CUDA error %s at %s\n", cudaGetErrorString(e.code), e.what);
+    return RPBA_ERR_CUDA;
+  } catch (const std::bad_alloc &) {
+    return RPBA_ERR_CUDA;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *rpba_status_string(int32_t st) {
+  switch (st) {
+    case RPBA_OK: return "ok";
+    case RPBA_ERR_ARG: return "invalid argument";
+    case RPBA_ERR_CUDA: return "CUDA error";
+    case RPBA_ERR_NO_OBS_IMAGE: return "BA-Error: No observations in image";
+    case RPBA_ERR_LOW_REDUNDANCY: return "BA-Error: Low redundancy";
+    case RPBA_ERR_NAN_STEP: return "BA-Error: NANs in result vector";
+    case RPBA_ERR_DEVICE_TIMEOUT: return "device wait timed out";
+    case RPBA_ERR_IO: return "I/O error";
+    case RPBA_ERR_UNSUPPORTED: return "unsupported input";
+    case RPBA_ERR_NO_DEVICE: return "no CUDA device";
+    case RPBA_ERR_SOLVER: return "direct solve failed";
+    default: return "unknown status";
+  }
+}
+
+const char *rpba_version(void) { return "rpba_b200 0.1 (sm_100a)"; }
+
+int32_t rpba_create(rpba_handle **h, const rpba_block *blk, const rpba_options *opt) {
+  if (!h || !blk || !opt) return RPBA_ERR_ARG;
+  *h = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= opt->device) return RPBA_ERR_NO_DEVICE;
+  if (blk->n_images < 1 || blk->n_points < 0) return RPBA_ERR_ARG;
+  rpba_handle *H = new rpba_handle();
+  struct A {
+    rpba_handle *H;
+    const rpba_block *b;
+    const rpba_options *o;
+  } a{H, blk, opt};
+  const int st = guard([](void *p) {
+    A *a = (A *)p;
+    return create_impl(a->H, a->b, a->o);
+  }, &a);
+  if (st != RPBA_OK) {
+    delete H;
+    return st;
+  }
+  *h = H;
+  return RPBA_OK;
+}
+
+int32_t rpba_solve(rpba_handle *H, rpba_report *rep) {
+  if (!H || H->opt.exteval) return RPBA_ERR_ARG;
+  const int st = guard([](void *p) {
+    rpba_handle *H = (rpba_handle *)p;
+    RPBA_CUDA_CHECK(cudaSetDevice(H->dev));
+    H->log.clear();
+    std::memset(&H->rep, 0, sizeof H->rep);
+    H->rep.points_used = H->npts0;
+    RPBA_CUDA_CHECK(cudaEventRecord(H->ev0, H->s));
+    H->reset();
+    const int r = H->adjust();
+    RPBA_CUDA_CHECK(cudaEventRecord(H->ev1, H->s));
+    RPBA_CUDA_CHECK(cudaEventSynchronize(H->ev1));
+    float ms = 0.f;
+    RPBA_CUDA_CHECK(cudaEventElapsedTime(&ms, H->ev0, H->ev1));
+    H->rep.solve_seconds = ms * 1e-3;
+    launch_final_cost(H->L, H->fc_part, H->fc_nparts, H->s);
+    std::vector<double> part(2 * H->fc_nparts);
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(part.data(), H->fc_part, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, H->s));
+    RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
+    double c = 0., q = 0.;
+    for (int i = 0; i < H->fc_nparts; ++i) {
+      c += part[2 * i];
+      q += part[2 * i + 1];
+    }
+    H->rep.cost = c;
+    H->rep.rms = H->L.nobs > 0 ? std::sqrt(q / H->L.nobs) : 0.;
+    H->rep.status = r;
+    return r;
+  }, H);
+  if (rep) *rep = H->rep;
+  if (rep) rep->status = st;
+  return st;
+}
+
+int32_t rpba_get_log(rpba_handle *H, char *log, size_t cap) {
+  if (!H || !log || cap == 0) return RPBA_ERR_ARG;
+  const size_t n = std::min(cap - 1, H->log.size());
+  std::memcpy(log, H->log.data(), n);
+  log[n] = 0;
+  return RPBA_OK;
+}
+
+// OutputLSAc + PointXXvOut (rbacore.cpp:644-666, 1978-2010).
+int32_t rpba_get_state(rpba_handle *H, rpba_block *blk) {
+  if (!H || !blk || H->opt.exteval) return RPBA_ERR_ARG;
+  if (blk->n_images != H->nimg || blk->n_points != H->XXnr) return RPBA_ERR_ARG;
+  struct A {
+    rpba_handle *H;
+    rpba_block *b;
+  } a{H, blk};
+  return guard([](void *p) {
+    A *a = (A *)p;
+    rpba_handle *H = a->H;
+    rpba_block *b = a->b;
+    RPBA_CUDA_CHECK(cudaSetDevice(H->dev));
+    const int n = H->nimg, no = H->L.nobs, np = H->L.npts;
+    std::vector<double> P(12 * (size_t)n);
+    std::vector<CamState> cams(n);
+    std::vector<int> o_cam(no), o_slot(no), pt_off(np + 1), pt_id(np);
+    std::vector<double> X(3 * (size_t)np);
+    auto dn = [&](void *h, const void *d, size_t bytes) {
+      if (bytes) RPBA_CUDA_CHECK(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, H->s));
+    };
+    dn(P.data(), H->L.Pacc, sizeof(double) * P.size());
+    dn(cams.data(), H->L.camn, sizeof(CamState) * n);
+    dn(o_cam.data(), H->L.o_cam, sizeof(int) * no);
+    dn(o_slot.data(), H->L.o_slot, sizeof(int) * no);
+    dn(pt_off.data(), H->L.pt_off, sizeof(int) * (np + 1));
+    dn(pt_id.data(), H->L.pt_id, sizeof(int) * np);
+    dn(X.data(), H->L.XPM + H->nrioff, sizeof(double) * 3 * np);
+    RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
+    for (size_t i = 0; i < P.size(); ++i) b->pmat[i] = (float)P[i];
+    for (int i = 0; i < n; ++i) {
+      const CamState &c = cams[i];
+      float *K = b->K + 9 * i;
+      const float *Ki = H->h_K.data() + 9 * i;
+      K[0] = (float)c.K00;
+      K[1] = (float)c.K01;
+      K[2] = (float)c.K02;
+      K[3] = Ki[3];
+      K[4] = (float)c.K11;
+      K[5] = (float)c.K12;
+      K[6] = Ki[6];
+      K[7] = Ki[7];
+      K[8] = 1.f;
+      b->distpara[2 * i] = (float)c.d0;
+      b->distpara[2 * i + 1] = (float)c.d1;
+    }
+    std::memcpy(b->XX, H->h_XX.data(), sizeof(float) * H->h_XX.size());
+    int w = 0, q = 0;
+    b->pt_obs_off[0] = 0;
+    for (int i = 0; i < H->XXnr; ++i) {
+      if (q < np && pt_id[q] == i) {
+        for (int o = pt_off[q]; o < pt_off[q + 1]; ++o, ++w) {
+          b->pt_obs_image[w] = o_cam[o];
+          b->pt_obs_slot[w] = o_slot[o];
+        }
+        for (int j = 0; j < 3; ++j) b->XX[3 * i + j] = (float)X[3 * q + j];
+        ++q;
+      }
+      b->pt_obs_off[i + 1] = w;
+    }
+    return (int)RPBA_OK;
+  }, &a);
+}
+
+// EvalLSA on the uploaded block (rpbacore.cpp:882-941).
+int32_t rpba_exteval(rpba_handle *H, double *resid, rpba_report *rep) {
+  if (!H) return RPBA_ERR_ARG;
+  struct A {
+    rpba_handle *H;
+    double *resid;
+    rpba_report *rep;
+  } a{H, resid, rep};
+  return guard([](void *p) {
+    A *a = (A *)p;
+    rpba_handle *H = a->H;
+    RPBA_CUDA_CHECK(cudaSetDevice(H->dev));
+    auto &own = H->owned;
+    const int n = H->nimg, np = H->XXnr, ns = H->n_slots, nt = H->n_track_in;
+    float *pm = dalloc<float>(12 * (size_t)n, own), *K = dalloc<float>(9 * (size_t)n, own);
+    float *ds = dalloc<float>(2 * (size_t)n, own), *XX = dalloc<float>(3 * (size_t)std::max(np, 1), own);
+    float *xg = dalloc<float>(2 * (size_t)std::max(ns, 1), own), *wx = dalloc<float>(std::max(ns, 1), own);
+    float *wy = dalloc<float>(std::max(ns, 1), own), *wxy = dalloc<float>(std::max(ns, 1), own);
+    int *io = dalloc<int>(n + 1, own), *po = dalloc<int>(np + 1, own);
+    int *pi = dalloc<int>(std::max(nt, 1), own), *ps = dalloc<int>(std::max(nt, 1), own);
+    double *res = dalloc<double>(2 * (size_t)std::max(nt, 1), own);
+    float *term = dalloc<float>(std::max(np, 1), own), *sum = dalloc<float>(1, own);
+    int *red = dalloc<int>(std::max(np, 1), own);
+    auto up = [&](void *d, const void *h, size_t bytes) {
+      if (bytes) RPBA_CUDA_CHECK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, H->s));
+    };
+    up(pm, H->h_pmat.data(), sizeof(float) * 12 * n);
+    up(K, H->h_K.data(), sizeof(float) * 9 * n);
+    up(ds, H->h_dist.data(), sizeof(float) * 2 * n);
+    up(XX, H->h_XX.data(), sizeof(float) * 3 * np);
+    up(xg, H->h_xg.data(), sizeof(float) * 2 * ns);
+    up(wx, H->h_wx.data(), sizeof(float) * ns);
+    up(wy, H->h_wy.data(), sizeof(float) * ns);
+    up(wxy, H->h_wxy.data(), sizeof(float) * ns);
+    up(io, H->h_img_off.data(), sizeof(int) * (n + 1));
+    up(po, H->h_pt_off.data(), sizeof(int) * (np + 1));
+    up(pi, H->h_pt_img.data(), sizeof(int) * nt);
+    up(ps, H->h_pt_slot.data(), sizeof(int) * nt);
+    launch_exteval(np, po, pi, ps, io, pm, K, ds, XX, xg, wx, wy, wxy, res, term, red, H->s);
+    launch_seq_sum(term, np, sum, H->s);
+    std::vector<int> hred(np);
+    float s = 0.f;
+    if (np) RPBA_CUDA_CHECK(cudaMemcpyAsync(hred.data(), red, sizeof(int) * np, cudaMemcpyDeviceToHost, H->s));
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(&s, sum, sizeof(float), cudaMemcpyDeviceToHost, H->s));
+    if (a->resid && nt)
+      RPBA_CUDA_CHECK(cudaMemcpyAsync(a->resid, res, sizeof(double) * 2 * nt, cudaMemcpyDeviceToHost, H->s));
+    RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
+    long redundancy = 0, nrobs = 0;
+    for (int i = 0; i < np; ++i) {
+      redundancy += hred[i];
+      if (hred[i] > 0) nrobs += hred[i] + 3;
+    }
+    const long r = redundancy - (long)(n - 2) * 6 - 5 - (long)n * H->nadd;
+    float sig0g = s;
+    sig0g *= 1.f / (float)r;
+    float ihw2 = 0.f;
+    for (int i = 0; i < n; ++i) ihw2 += (float)((1 + 1) * (1 + 1)) * 0.25f;
+    ihw2 /= (float)n;
+    const float v = std::sqrt(sig0g * ihw2);
+    H->log += "ITTTT: " + fmt_g(v) + ' ' + std::to_string(nrobs) + " " + std::to_string(r) + '\n';
+    if (a->rep) {
+      a->rep->exteval_sigma0 = v;
+      a->rep->exteval_nrobs = nrobs;
+      a->rep->exteval_redundancy = r;
+    }
+    return (int)RPBA_OK;
+  }, &a);
+}
+
+void rpba_destroy(rpba_handle *H) { delete H; }
+
+int32_t rpba_calc_plsa(rpba_block *blk, const rpba_options *opt, char *log, size_t cap, rpba_report *rep) {
+  if (!blk || !opt) return RPBA_ERR_ARG;
+  if (rep) std::memset(rep, 0, sizeof *rep);
+  rpba_handle *H = nullptr;
+  int st = rpba_create(&H, blk, opt);
+  if (st != RPBA_OK) return st;
+  if (opt->exteval) {
+    st = rpba_exteval(H, nullptr, rep);
+  } else {
+    st = rpba_solve(H, rep);
+    if (st == RPBA_OK || st == RPBA_ERR_NO_OBS_IMAGE || st == RPBA_ERR_LOW_REDUNDANCY || st == RPBA_ERR_NAN_STEP) {
+      const int st2 = rpba_get_state(H, blk);
+      if (st == RPBA_OK) st = st2;
+    }
+  }
+  if (log && cap) rpba_get_log(H, log, cap);
+  rpba_destroy(H);
+  return st;
+}
+
+}  // extern "C"

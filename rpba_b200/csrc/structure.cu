@@ -1,0 +1,223 @@
+// structure.cu -- symbolic structure of one pass (rebuilt after
+// RobustDelete): the camera-grouped observation order (the reference's nro
+// indexing, rbacore.cpp:401-430), the covisible camera pairs that make up
+// the off-diagonal blocks of the reduced camera system (rbacore.cpp:
+// 1362-1390 grow the same set into a skyline), their per-point
+// contributions sorted by block, and the block rows used by the SpMV.
+// Setup only: sorts and scans come from CUB.
+#include <cub/cub.cuh>
+
+#include "internal.h"
+
+namespace rpba {
+
+namespace {
+
+inline int nblk(long long n, int t) { return (int)((n + t - 1) / t); }
+
+int key_bits(long long maxkey) {
+  int b = 1;
+  while (b < 32 && (1ll << b) <= maxkey) ++b;
+  return b;
+}
+
+__global__ void k_iota_key(const int *o_cam, int n, unsigned *key, int *iota) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  key[i] = (unsigned)o_cam[i];
+  iota[i] = i;
+}
+
+__global__ void k_hist(const int *v, int n, int *cnt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) atomicAdd(cnt + v[i], 1);
+}
+
+__global__ void k_pair_count(DevLSA L, int *pcnt) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p > L.npts) return;
+  if (p == L.npts) {
+    pcnt[p] = 0;
+    return;
+  }
+  const int t0 = L.pt_off[p], t1 = L.pt_off[p + 1];
+  int c = 0;
+  for (int s = t0; s < t1; ++s) {
+    const int ks = L.o_cam[s];
+    if (ks < L.begini) continue;
+    for (int t = s + 1; t < t1; ++t) {
+      const int kt = L.o_cam[t];
+      if (kt >= L.begini && kt != ks) ++c;
+    }
+  }
+  pcnt[p] = c;
+}
+
+__global__ void k_pair_emit(DevLSA L, const int *poff, unsigned *key, unsigned long long *val) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= L.npts) return;
+  const int t0 = L.pt_off[p], t1 = L.pt_off[p + 1];
+  int w = poff[p];
+  const unsigned n = (unsigned)L.nimg;
+  for (int s = t0; s < t1; ++s) {
+    const int ks = L.o_cam[s];
+    if (ks < L.begini) continue;
+    for (int t = s + 1; t < t1; ++t) {
+      const int kt = L.o_cam[t];
+      if (kt < L.begini || kt == ks) continue;
+      const bool sf = ks < kt;
+      const unsigned kmin = sf ? ks : kt, kmax = sf ? kt : ks;
+      const unsigned omin = sf ? s : t, omax = sf ? t : s;
+      key[w] = kmin * n + kmax;
+      val[w] = ((unsigned long long)omin << 32) | omax;
+      ++w;
+    }
+  }
+}
+
+__global__ void k_unpack_contrib(const unsigned long long *val, long long n, int2 *contrib) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned long long v = val[i];
+  contrib[i] = make_int2((int)(v >> 32), (int)(v & 0xffffffffu));
+}
+
+__global__ void k_block_count(const unsigned *bkey, int nb, int nimg, int *cntN, int *cntT, unsigned *tkey,
+                              int *tidx) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const unsigned row = bkey[b] / (unsigned)nimg, col = bkey[b] % (unsigned)nimg;
+  atomicAdd(cntN + row, 1);
+  atomicAdd(cntT + col, 1);
+  tkey[b] = col * (unsigned)nimg + row;
+  tidx[b] = b;
+}
+
+__global__ void k_row_sizes(const int *cntN, const int *cntT, int nimg, int *rs) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > nimg) return;
+  rs[k] = k < nimg ? cntN[k] + cntT[k] + 1 : 0;
+}
+
+__global__ void k_fill_normal(const unsigned *bkey, int nb, int nimg, const int *rowoff, const int *cntT,
+                              const int *firstN, int2 *ent) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  const int row = (int)(bkey[b] / (unsigned)nimg), col = (int)(bkey[b] % (unsigned)nimg);
+  const int pos = rowoff[row] + cntT[row] + 1 + (b - firstN[row]);
+  ent[pos] = make_int2(col, nimg + b);
+}
+
+__global__ void k_fill_transposed(const unsigned *bkey, const int *tidx_sorted, int nb, int nimg,
+                                  const int *rowoff, const int *firstT, int2 *ent) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nb) return;
+  const int b = tidx_sorted[q];
+  const int row = (int)(bkey[b] / (unsigned)nimg), col = (int)(bkey[b] % (unsigned)nimg);
+  const int pos = rowoff[col] + (q - firstT[col]);
+  ent[pos] = make_int2(row, (int)((unsigned)(nimg + b) | 0x80000000u));
+}
+
+__global__ void k_fill_diag(int nimg, const int *rowoff, const int *cntT, int2 *ent) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nimg) return;
+  ent[rowoff[k] + cntT[k]] = make_int2(k, k);
+}
+
+}  // namespace
+
+size_t structure_cub_bytes(int nobs, long long npairs, int nimg) {
+  size_t m = 0, b = 0;
+  const int np = (int)(npairs > 0 ? npairs : 1);
+  cub::DeviceRadixSort::SortPairs(nullptr, b, (unsigned *)nullptr, (unsigned *)nullptr, (int *)nullptr,
+                                  (int *)nullptr, nobs > 0 ? nobs : 1);
+  m = std::max(m, b);
+  cub::DeviceRadixSort::SortPairs(nullptr, b, (unsigned *)nullptr, (unsigned *)nullptr,
+                                  (unsigned long long *)nullptr, (unsigned long long *)nullptr, np);
+  m = std::max(m, b);
+  cub::DeviceRadixSort::SortPairs(nullptr, b, (unsigned *)nullptr, (unsigned *)nullptr, (int *)nullptr,
+                                  (int *)nullptr, np);
+  m = std::max(m, b);
+  cub::DeviceRunLengthEncode::Encode(nullptr, b, (unsigned *)nullptr, (unsigned *)nullptr, (int *)nullptr,
+                                     (int *)nullptr, np);
+  m = std::max(m, b);
+  const int ns = std::max(std::max(nimg + 1, np + 1), nobs + 1);
+  cub::DeviceScan::ExclusiveSum(nullptr, b, (int *)nullptr, (int *)nullptr, ns);
+  m = std::max(m, b);
+  return m + 256;
+}
+
+void build_camera_order(DevLSA &L, StructWork &S, cudaStream_t s) {
+  if (L.nobs > 0) {
+    k_iota_key<<<nblk(L.nobs, 256), 256, 0, s>>>(L.o_cam, L.nobs, S.ckey, S.iota);
+    size_t bytes = S.cub_bytes;
+    RPBA_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(S.cub_tmp, bytes, S.ckey, S.ckey2, S.iota, L.camlist, L.nobs,
+                                                    0, key_bits(L.nimg), s));
+  }
+  RPBA_CUDA_CHECK(cudaMemsetAsync(S.ccnt, 0, sizeof(int) * (L.nimg + 1), s));
+  if (L.nobs > 0) k_hist<<<nblk(L.nobs, 256), 256, 0, s>>>(L.o_cam, L.nobs, S.ccnt);
+  size_t bytes = S.cub_bytes;
+  RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(S.cub_tmp, bytes, S.ccnt, L.coff, L.nimg + 1, s));
+}
+
+int build_pairs(DevLSA &L, StructWork &S, long long max_pairs, long long *npairs_out, cudaStream_t s) {
+  k_pair_count<<<nblk(L.npts + 1, 256), 256, 0, s>>>(L, S.pcnt);
+  size_t bytes = S.cub_bytes;
+  RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(S.cub_tmp, bytes, S.pcnt, S.poff, L.npts + 1, s));
+  int total = 0;
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(&total, S.poff + L.npts, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+  if (total < 0 || total > max_pairs) throw CudaError(cudaErrorInvalidValue, "pair count exceeds capacity");
+  *npairs_out = total;
+  if (total == 0) {
+    L.nboff = 0;
+    return 0;
+  }
+  k_pair_emit<<<nblk(L.npts, 256), 256, 0, s>>>(L, S.poff, S.pkey, S.pval);
+  bytes = S.cub_bytes;
+  RPBA_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(S.cub_tmp, bytes, S.pkey, S.pkey2, S.pval, S.pval2, total, 0,
+                                                  key_bits((long long)L.nimg * L.nimg), s));
+  bytes = S.cub_bytes;
+  RPBA_CUDA_CHECK(cub::DeviceRunLengthEncode::Encode(S.cub_tmp, bytes, S.pkey2, S.bkey, S.bcnt, S.nrun, total, s));
+  int nb = 0;
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(&nb, S.nrun, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(S.bcnt + nb, 0, sizeof(int), s));
+  bytes = S.cub_bytes;
+  RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(S.cub_tmp, bytes, S.bcnt, S.boff, nb + 1, s));
+  k_unpack_contrib<<<nblk(total, 256), 256, 0, s>>>(S.pval2, total, S.contrib);
+  L.nboff = nb;
+  L.boff = S.boff;
+  L.contrib = S.contrib;
+  return nb;
+}
+
+void build_bsr(DevLSA &L, StructWork &S, cudaStream_t s) {
+  const int n = L.nimg, nb = L.nboff;
+  RPBA_CUDA_CHECK(cudaMemsetAsync(S.cntN, 0, sizeof(int) * (n + 1), s));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(S.cntT, 0, sizeof(int) * (n + 1), s));
+  if (nb > 0) k_block_count<<<nblk(nb, 256), 256, 0, s>>>(S.bkey, nb, n, S.cntN, S.cntT, S.tkey, S.tidx);
+  size_t bytes = S.cub_bytes;
+  RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(S.cub_tmp, bytes, S.cntN, S.firstN, n + 1, s));
+  bytes = S.cub_bytes;
+  RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(S.cub_tmp, bytes, S.cntT, S.firstT, n + 1, s));
+  k_row_sizes<<<nblk(n + 1, 256), 256, 0, s>>>(S.cntN, S.cntT, n, S.rowtmp);
+  bytes = S.cub_bytes;
+  RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(S.cub_tmp, bytes, S.rowtmp, S.rowoff, n + 1, s));
+  if (nb > 0) {
+    bytes = S.cub_bytes;
+    RPBA_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(S.cub_tmp, bytes, S.tkey, S.tkey2, S.tidx, S.tidx2, nb, 0,
+                                                    key_bits((long long)n * n), s));
+    k_fill_normal<<<nblk(nb, 256), 256, 0, s>>>(S.bkey, nb, n, S.rowoff, S.cntT, S.firstN, S.ent);
+    k_fill_transposed<<<nblk(nb, 256), 256, 0, s>>>(S.bkey, S.tidx2, nb, n, S.rowoff, S.firstT, S.ent);
+  }
+  k_fill_diag<<<nblk(n, 256), 256, 0, s>>>(n, S.rowoff, S.cntT, S.ent);
+  L.rowoff = S.rowoff;
+  L.ent = S.ent;
+}
+
+cudaError_t cub_exclusive_sum_int(void *tmp, size_t &bytes, const int *in, int *out, int n, cudaStream_t s) {
+  return cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, n, s);
+}
+
+}  // namespace rpba

@@ -1,0 +1,176 @@
+"""ctypes binding of ``librpba_b200.so`` with the reference's entry points.
+
+The names mirror RPBA's own functions (rpba.cpp / rpbacore.cpp):
+
+* ``InputBlock(path, nraddpar, k24out)`` -- rpba.cpp:180-284
+* ``OutputBlock(path, block, k24out)``   -- rpba.cpp:288-338
+* ``CalcPLSA(block, ...)``               -- rpbacore.cpp:28-531; adjusts the
+  block in place (cameras, points, track lists), returns (status, log, report)
+
+plus ``Solver`` for the handle API (upload once, solve many times).
+
+There is no CPU fallback: the library must be built (``__graft_entry__.build``
+or ``make -C rpba_b200/csrc``) and a CUDA device must be present, otherwise
+the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .block import (Block, RpbaBlockC, RpbaOptionsC, RpbaReportC, make_options,
+                    SOLVER_PCG, SOLVER_DIRECT, SOLVER_LEARNED, PREC_FP64, PREC_MIXED)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librpba_b200.so")
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no observations in image",
+          4: "low redundancy", 5: "NaN step", 6: "device timeout", 7: "I/O error",
+          8: "unsupported input", 9: "no CUDA device", 10: "direct solve failed"}
+
+# Every entry point include/rpba_b200.h declares.
+EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block_free",
+           "rpba_output_block", "rpba_calc_plsa", "rpba_create", "rpba_solve",
+           "rpba_get_state", "rpba_get_log", "rpba_exteval", "rpba_destroy")
+
+_lib = None
+
+
+class RpbaError(RuntimeError):
+    def __init__(self, status: int, what: str = ""):
+        super().__init__(f"{what}: {STATUS.get(status, status)} ({status})")
+        self.status = status
+
+
+def load():
+    """Load the library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with __graft_entry__.build()")
+    L = C.CDLL(LIB_PATH)
+    bp, op, rp = C.POINTER(RpbaBlockC), C.POINTER(RpbaOptionsC), C.POINTER(RpbaReportC)
+    L.rpba_status_string.argtypes = [C.c_int32]
+    L.rpba_status_string.restype = C.c_char_p
+    L.rpba_version.restype = C.c_char_p
+    L.rpba_input_block.argtypes = [C.c_char_p, C.c_int32, C.c_int32, bp]
+    L.rpba_input_block.restype = C.c_int32
+    L.rpba_block_free.argtypes = [bp]
+    L.rpba_output_block.argtypes = [C.c_char_p, bp, C.c_int32]
+    L.rpba_output_block.restype = C.c_int32
+    L.rpba_calc_plsa.argtypes = [bp, op, C.c_char_p, C.c_size_t, rp]
+    L.rpba_calc_plsa.restype = C.c_int32
+    L.rpba_create.argtypes = [C.POINTER(C.c_void_p), bp, op]
+    L.rpba_create.restype = C.c_int32
+    L.rpba_solve.argtypes = [C.c_void_p, rp]
+    L.rpba_solve.restype = C.c_int32
+    L.rpba_get_state.argtypes = [C.c_void_p, bp]
+    L.rpba_get_state.restype = C.c_int32
+    L.rpba_get_log.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
+    L.rpba_get_log.restype = C.c_int32
+    L.rpba_exteval.argtypes = [C.c_void_p, C.POINTER(C.c_double), rp]
+    L.rpba_exteval.restype = C.c_int32
+    L.rpba_destroy.argtypes = [C.c_void_p]
+    _lib = L
+    return L
+
+
+def InputBlock(path: str, nraddpar: int = 3, k24out: bool = True) -> Block:
+    L = load()
+    cb = RpbaBlockC()
+    st = L.rpba_input_block(path.encode(), int(nraddpar), int(k24out), C.byref(cb))
+    if st != 0:
+        raise RpbaError(st, f"InputBlock({path})")
+    b = Block.from_c(cb)
+    L.rpba_block_free(C.byref(cb))
+    return b
+
+
+def OutputBlock(path: str, block: Block, k24out: bool = True) -> None:
+    cb = block.as_c()
+    st = load().rpba_output_block(path.encode(), C.byref(cb), int(k24out))
+    if st != 0:
+        raise RpbaError(st, f"OutputBlock({path})")
+
+
+def CalcPLSA(block: Block, robust: bool = True, addflags=(True, True, True), threads: int = 1,
+             exteval: bool = False, solver: int = SOLVER_PCG, precision: int = PREC_FP64,
+             max_lm_iterations: int = -1, device: int = 0, log_cap: int = 1 << 20):
+    """Adjust ``block`` in place on the GPU (or evaluate it, ``exteval``).
+
+    Returns (status, log text, report dict).  Like the reference, the
+    adjusted state is written back on the error returns that keep a stored
+    state (no observations in an image, low redundancy, NaN step)."""
+    o = make_options(robust=robust, exteval=exteval, threads=threads, k2=addflags[0],
+                     k4=addflags[1], f=addflags[2], solver=solver, precision=precision,
+                     max_lm_iterations=max_lm_iterations, device=device)
+    cb = block.as_c()
+    rep = RpbaReportC()
+    buf = C.create_string_buffer(log_cap)
+    st = load().rpba_calc_plsa(C.byref(cb), C.byref(o), buf, log_cap, C.byref(rep))
+    if st in (2, 9):
+        raise RpbaError(st, "CalcPLSA")
+    return st, buf.value.decode(), rep.as_dict()
+
+
+class Solver:
+    """Handle API: the block is uploaded once; ``solve`` restarts from it."""
+
+    def __init__(self, block: Block, **kw):
+        self.block = block
+        self.opts = make_options(**kw)
+        self._cb = block.as_c()
+        self.h = C.c_void_p()
+        st = load().rpba_create(C.byref(self.h), C.byref(self._cb), C.byref(self.opts))
+        if st != 0:
+            self.h = None
+            raise RpbaError(st, "rpba_create")
+
+    def solve(self) -> tuple[int, dict]:
+        rep = RpbaReportC()
+        st = load().rpba_solve(self.h, C.byref(rep))
+        if st in (2, 6, 9):
+            raise RpbaError(st, "rpba_solve")
+        return st, rep.as_dict()
+
+    def log(self, cap: int = 1 << 20) -> str:
+        buf = C.create_string_buffer(cap)
+        load().rpba_get_log(self.h, buf, cap)
+        return buf.value.decode()
+
+    def state(self) -> Block:
+        out = self.block.copy()
+        cb = out.as_c()
+        st = load().rpba_get_state(self.h, C.byref(cb))
+        if st != 0:
+            raise RpbaError(st, "rpba_get_state")
+        return out
+
+    def exteval(self):
+        n = self.block.n_obs
+        res = np.zeros(2 * max(n, 1))
+        rep = RpbaReportC()
+        st = load().rpba_exteval(self.h, res.ctypes.data_as(C.POINTER(C.c_double)), C.byref(rep))
+        if st != 0:
+            raise RpbaError(st, "rpba_exteval")
+        return res[: 2 * n].reshape(-1, 2), rep.as_dict()
+
+    def close(self):
+        if self.h:
+            load().rpba_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

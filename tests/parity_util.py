@@ -1,0 +1,42 @@
+"""Comparison helpers for GPU-vs-oracle parity tests.
+
+Tolerances (stated by the drop-in contract):
+  final cost         relative 1e-8
+  parameters         relative 1e-6 (scaled by the array's magnitude)
+  Exteval residuals  absolute 1e-10 px
+"""
+import numpy as np
+
+COST_RTOL = 1e-8
+PARAM_RTOL = 1e-6
+EXTEVAL_ATOL = 1e-10
+
+
+def scaled_err(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    if a.size == 0:
+        return 0.0
+    scale = max(np.abs(b).max(), 1e-12)
+    return float(np.abs(a - b).max() / scale)
+
+
+def param_errors(gpu_blk, ora_blk):
+    """Scaled relative errors of the adjusted parameters."""
+    n = gpu_blk.n_images
+    P_g = gpu_blk.pmat.reshape(n, 3, 4)
+    P_o = ora_blk.pmat.reshape(n, 3, 4)
+    return {
+        "R": scaled_err(P_g[:, :, :3], P_o[:, :, :3]),
+        "t": scaled_err(P_g[:, :, 3], P_o[:, :, 3]),
+        "f": scaled_err(gpu_blk.K[:, 0], ora_blk.K[:, 0]),
+        "k1": scaled_err(gpu_blk.distpara[:, 0], ora_blk.distpara[:, 0]),
+        "k2": scaled_err(gpu_blk.distpara[:, 1], ora_blk.distpara[:, 1]),
+        "XX": scaled_err(gpu_blk.XX, ora_blk.XX),
+    }
+
+
+def same_tracks(a, b):
+    return (np.array_equal(a.pt_obs_off, b.pt_obs_off)
+            and np.array_equal(a.pt_obs_image[: a.n_obs], b.pt_obs_image[: b.n_obs])
+            and np.array_equal(a.pt_obs_slot[: a.n_obs], b.pt_obs_slot[: b.n_obs]))

@@ -1,0 +1,136 @@
+"""GPU parity: the sm_100a library against the CPU oracle on the same seeded
+inputs, through the C ABI (CalcPLSA / the handle API)."""
+import numpy as np
+import pytest
+
+from rpba_b200 import scenes
+from tests.parity_util import (COST_RTOL, PARAM_RTOL, EXTEVAL_ATOL, param_errors, same_tracks)
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_pair(oracle_mod, blk, **kw):
+    import rpba_b200 as rb
+    o = rb.make_options(**kw)
+    st_o, blk_o, rep_o, log_o = oracle_mod.calc_plsa(blk, o)
+    blk_g = blk.copy()
+    addflags = (kw.get("k2", True), kw.get("k4", True), kw.get("f", True))
+    st_g, log_g, rep_g = rb.CalcPLSA(blk_g, robust=kw.get("robust", True), addflags=addflags,
+                                     max_lm_iterations=kw.get("max_lm_iterations", -1))
+    return (st_o, blk_o, rep_o, log_o), (st_g, blk_g, rep_g, log_g)
+
+
+def _check(o, g):
+    st_o, blk_o, rep_o, log_o = o
+    st_g, blk_g, rep_g, log_g = g
+    assert st_g == st_o, (st_g, st_o, log_g, log_o)
+    # identical decisions: same passes, same ITT counters, same printed sigma0
+    assert log_g == log_o, f"\nGPU:\n{log_g}\nORACLE:\n{log_o}"
+    for k in ("linear_solves", "obs_deleted", "points_deleted", "points_used", "passes_done"):
+        assert rep_g[k] == rep_o[k], (k, rep_g[k], rep_o[k])
+    assert abs(rep_g["cost"] - rep_o["cost"]) <= COST_RTOL * abs(rep_o["cost"]), (rep_g["cost"], rep_o["cost"])
+    errs = param_errors(blk_g, blk_o)
+    assert max(errs.values()) <= PARAM_RTOL, errs
+    assert same_tracks(blk_g, blk_o)
+
+
+@pytest.fixture(scope="module")
+def arc_block():
+    return scenes.to_block(scenes.make_scene(0))
+
+
+@pytest.fixture(scope="module")
+def street_small():
+    return scenes.to_block(scenes.make_scene(1, scale=0.06))
+
+
+def test_parity_arc_robust(oracle_mod, arc_block):
+    o, g = _run_pair(oracle_mod, arc_block)
+    _check(o, g)
+
+
+def test_parity_street_robust(oracle_mod, street_small):
+    o, g = _run_pair(oracle_mod, street_small)
+    _check(o, g)
+
+
+@pytest.mark.parametrize("kw", [
+    dict(robust=False),
+    dict(k2=False, k4=False, f=False),
+    dict(k2=True, k4=False, f=True),
+    dict(k2=False, k4=True, f=False, robust=False),
+])
+def test_parity_variants(oracle_mod, kw):
+    blk = scenes.to_block(scenes.arc_scene(seed=11, n_cams=12, n_pts=1500))
+    o, g = _run_pair(oracle_mod, blk, **kw)
+    _check(o, g)
+
+
+def test_parity_fixed_iterations(oracle_mod, arc_block):
+    o, g = _run_pair(oracle_mod, arc_block, max_lm_iterations=3)
+    _check(o, g)
+
+
+def test_exteval_parity(oracle_mod, arc_block):
+    import rpba_b200 as rb
+    res_o, rep_o = oracle_mod.exteval(arc_block, rb.make_options())
+    with rb.Solver(arc_block, exteval=True) as s:
+        res_g, rep_g = s.exteval()
+    assert np.abs(res_g - res_o).max() <= EXTEVAL_ATOL
+    assert rep_g["exteval_sigma0"] == rep_o["exteval_sigma0"]
+    assert rep_g["exteval_nrobs"] == rep_o["exteval_nrobs"]
+    assert rep_g["exteval_redundancy"] == rep_o["exteval_redundancy"]
+    st, log, rep = rb.CalcPLSA(arc_block.copy(), exteval=True)
+    assert st == 0 and log.startswith("ITTTT: ")
+
+
+def test_exteval_after_adjustment(oracle_mod, arc_block):
+    """Back-projection errors of the adjusted block (a realistic Exteval input)."""
+    import rpba_b200 as rb
+    _, adj, _, _ = oracle_mod.calc_plsa(arc_block, rb.make_options())
+    res_o, rep_o = oracle_mod.exteval(adj, rb.make_options())
+    with rb.Solver(adj, exteval=True) as s:
+        res_g, rep_g = s.exteval()
+    assert np.abs(res_g - res_o).max() <= EXTEVAL_ATOL
+    assert rep_g["exteval_sigma0"] == rep_o["exteval_sigma0"]
+
+
+def test_repeat_solve_deterministic(arc_block):
+    import rpba_b200 as rb
+    with rb.Solver(arc_block) as s:
+        st1, rep1 = s.solve()
+        b1 = s.state()
+        log1 = s.log()
+        st2, rep2 = s.solve()
+        b2 = s.state()
+        log2 = s.log()
+    assert st1 == st2 == 0
+    assert log1 == log2
+    assert rep1["cost"] == rep2["cost"]
+    assert np.array_equal(b1.pmat, b2.pmat) and np.array_equal(b1.XX, b2.XX)
+
+
+def test_error_no_observations_in_image(oracle_mod):
+    """An image whose observations all belong to single-observation points
+    ends the adjustment with the reference's BA-Error (rbacore.cpp:415-424)."""
+    import rpba_b200 as rb
+    blk = scenes.to_block(scenes.arc_scene(seed=3, n_cams=8, n_pts=400))
+    # detach image 5: every observation of image 5 becomes the only one of a new point
+    img = blk.pt_obs_image
+    keep = img != 5
+    off = blk.pt_obs_off
+    counts = np.add.reduceat(keep.astype(np.int64), off[:-1]) if blk.n_points else np.zeros(0)
+    new_img = img[keep]
+    new_slot = blk.pt_obs_slot[keep]
+    new_off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+    extra = np.nonzero(~keep)[0]
+    XX = np.concatenate([blk.XX, blk.XX[np.searchsorted(off, extra, side="right") - 1]])
+    b2 = rb.Block(blk.pmat, blk.K, blk.distpara, XX.astype(np.float32), blk.img_obs_off, blk.xg, blk.wx,
+                  blk.wy, blk.wxy,
+                  np.concatenate([new_off, new_off[-1] + np.arange(1, extra.size + 1)]).astype(np.int32),
+                  np.concatenate([new_img, img[extra]]).astype(np.int32),
+                  np.concatenate([new_slot, blk.pt_obs_slot[extra]]).astype(np.int32))
+    o, g = _run_pair(oracle_mod, b2)
+    assert o[0] == 3 and g[0] == 3
+    assert "BA-Error: No observations in image 5" in g[3]
+    assert g[3] == o[3]
