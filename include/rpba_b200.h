@@ -131,6 +131,7 @@ typedef struct rpba_report {
   double solve_seconds;  /* device time of the solve (CUDA events)          */
   double setup_seconds;  /* host+device time before the first LM iteration  */
   int32_t status;
+  int64_t kernel_launches; /* launches of this library's kernels in the solve */
 } rpba_report;
 
 typedef struct rpba_handle rpba_handle;
@@ -172,6 +173,11 @@ int32_t rpba_get_log(rpba_handle *h, char *log, size_t cap);
  * (rpbacore.cpp:778-837, 882-941).  resid has 2*pt_obs_off[n_points]
  * entries; entries of points with fewer than two observations are 0. */
 int32_t rpba_exteval(rpba_handle *h, double *resid, rpba_report *rep);
+/* Per-kernel device time of the last solve as a JSON object
+ * {"name": {"launches": n, "ms": t}, ...}; filled only when the handle was
+ * created with rpba_options.verbose bit 1 (value 2) set.  No counterpart in
+ * the reference (its only instrument is a wall-clock print, rpba.cpp:140). */
+int32_t rpba_kernel_stats(rpba_handle *h, char *json, size_t cap);
 void rpba_destroy(rpba_handle *h);
 
 #ifdef __cplusplus

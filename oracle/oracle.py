@@ -29,6 +29,10 @@ def lib():
         L.oracle_calc_plsa.argtypes = [C.POINTER(RpbaBlockC), C.POINTER(RpbaOptionsC), C.c_char_p,
                                        C.c_size_t, C.POINTER(RpbaReportC)]
         L.oracle_calc_plsa.restype = C.c_int32
+        L.oracle_calc_plsa_variant.argtypes = [C.POINTER(RpbaBlockC), C.POINTER(RpbaOptionsC),
+                                               C.c_char_p, C.c_size_t, C.POINTER(RpbaReportC),
+                                               C.c_int32]
+        L.oracle_calc_plsa_variant.restype = C.c_int32
         L.oracle_exteval.argtypes = [C.POINTER(RpbaBlockC), C.POINTER(RpbaOptionsC), dp,
                                      C.POINTER(RpbaReportC)]
         L.oracle_exteval.restype = C.c_int32
@@ -73,6 +77,19 @@ def calc_plsa(block: Block, opts: RpbaOptionsC | None = None, log_cap: int = 1 <
     rep = RpbaReportC()
     buf = C.create_string_buffer(log_cap)
     st = lib().oracle_calc_plsa(C.byref(cb), C.byref(o), buf, log_cap, C.byref(rep))
+    return st, b, rep.as_dict(), buf.value.decode()
+
+
+def calc_plsa_variant(block: Block, opts: RpbaOptionsC | None = None, variant: int = 1,
+                      log_cap: int = 1 << 16):
+    """calc_plsa with the SpMV blocks of each column visited in reverse order:
+    the same arithmetic up to summation order (a self-sensitivity probe)."""
+    b = block.copy()
+    cb = b.as_c()
+    o = opts if opts is not None else make_options()
+    rep = RpbaReportC()
+    buf = C.create_string_buffer(log_cap)
+    st = lib().oracle_calc_plsa_variant(C.byref(cb), C.byref(o), buf, log_cap, C.byref(rep), variant)
     return st, b, rep.as_dict(), buf.value.decode()
 
 

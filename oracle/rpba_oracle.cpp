@@ -258,6 +258,11 @@ std::string fmt_g(double v) {
 
 /* ---------------------------------------------------------------- LSA */
 
+/* Test hook: 1 reverses the order in which the off-diagonal blocks of a
+ * column are visited in the SpMV.  Used only to measure how sensitive the
+ * reference's inexact PCG is to summation order. */
+int g_order_variant = 0;
+
 struct Opts {
   bool robust = true;
   bool addf[3] = {true, true, true};
@@ -994,7 +999,11 @@ void LSA::sparse_pcg() {
         for (int c = 0; c < ni; ++c) s += Dg[i][a * ni + c] * bv[off[i] + c];
         cv[off[i] + a] += s;
       }
-      for (auto &kv : Off[i]) {
+      std::vector<const std::pair<const int, std::vector<double>> *> order;
+      for (auto &kv : Off[i]) order.push_back(&kv);
+      if (g_order_variant == 1) std::reverse(order.begin(), order.end());
+      for (auto *kvp : order) {
+        const auto &kv = *kvp;
         const int row = kv.first, nr = cam_np(row);
         const std::vector<double> &B = kv.second; /* nr x ni */
         for (int a = 0; a < nr; ++a) {
@@ -1506,6 +1515,15 @@ int32_t oracle_calc_plsa(rpba_block *blk, const rpba_options *o, char *log, size
     rep->solve_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   }
   copy_log(os, log, cap);
+  return st;
+}
+
+/* CalcPLSA with a summation-order variant of the SpMV (see g_order_variant). */
+int32_t oracle_calc_plsa_variant(rpba_block *blk, const rpba_options *o, char *log, size_t cap,
+                                 rpba_report *rep, int32_t variant) {
+  g_order_variant = variant;
+  const int32_t st = oracle_calc_plsa(blk, o, log, cap, rep);
+  g_order_variant = 0;
   return st;
 }
 

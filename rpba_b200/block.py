@@ -75,6 +75,7 @@ class RpbaReportC(C.Structure):
         ("solve_seconds", C.c_double),
         ("setup_seconds", C.c_double),
         ("status", C.c_int32),
+        ("kernel_launches", C.c_int64),
     ]
 
     def as_dict(self) -> dict:

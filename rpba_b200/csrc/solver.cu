@@ -60,8 +60,93 @@ void rectify_host(double *R, int rs) {
 
 }  // namespace
 
+// Per-kernel device timing (CUDA events around each launch on the solve's
+// stream), enabled by rpba_options.verbose bit 1; launch counts always.
+struct KernelProf {
+  struct Rec {
+    const char *name;
+    cudaEvent_t a, b;
+    double bytes;
+  };
+  bool on = false;
+  cudaStream_t s = nullptr;
+  std::vector<Rec> pending;
+  std::vector<cudaEvent_t> pool;
+  struct Stat {
+    std::string name;
+    long long launches;
+    double ms, bytes;
+  };
+  std::vector<Stat> stats;
+  double next_bytes = 0.;
+  long long launches = 0, lib_launches = 0;
+  const char *cur = nullptr;
+  cudaEvent_t ev() {
+    if (pool.empty()) {
+      cudaEvent_t e;
+      RPBA_CUDA_CHECK(cudaEventCreate(&e));
+      return e;
+    }
+    cudaEvent_t e = pool.back();
+    pool.pop_back();
+    return e;
+  }
+  void begin(const char *name, int n = 1) {
+    launches += n;
+    if (!on) return;
+    Rec r{name, ev(), ev(), next_bytes};
+    next_bytes = 0.;
+    RPBA_CUDA_CHECK(cudaEventRecord(r.a, s));
+    pending.push_back(r);
+  }
+  void end() {
+    if (!on) return;
+    RPBA_CUDA_CHECK(cudaEventRecord(pending.back().b, s));
+  }
+  void add(const char *name, long long n, double ms, double bytes) {
+    for (auto &st : stats)
+      if (st.name == name) {
+        st.launches += n;
+        st.ms += ms;
+        st.bytes += bytes;
+        return;
+      }
+    stats.push_back({name, n, ms, bytes});
+  }
+  void resolve() {
+    for (auto &r : pending) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, r.a, r.b);
+      add(r.name, 1, ms, r.bytes);
+      pool.push_back(r.a);
+      pool.push_back(r.b);
+    }
+    pending.clear();
+  }
+  void reset() {
+    resolve();
+    stats.clear();
+    launches = lib_launches = 0;
+  }
+  ~KernelProf() {
+    for (auto e : pool) cudaEventDestroy(e);
+    for (auto &r : pending) {
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+  }
+};
+
+#define PROF(name, n, call) \
+  do {                          \
+    prof.begin(name, n);        \
+    call;                       \
+    prof.end();                 \
+  } while (0)
+
 struct rpba_handle {
   rpba_options opt{};
+  KernelProf prof;
   int dev = 0;
   cudaStream_t s = nullptr;
   std::vector<void *> owned;
@@ -82,8 +167,9 @@ struct rpba_handle {
   float ihw2 = 1.f;
   double defdiff = 5000.;
   std::vector<int> camparv;
-  long long max_pairs = 0;
+  long long max_pairs = 0, npairs_cur = 0;
   int pcg_grid = 1;
+  bool pcg_pending = false;
 
   // original state (restored by every solve)
   int *d0_o_cam, *d0_o_slot, *d0_o_pt, *d0_pt_off, *d0_pt_id;
@@ -136,7 +222,7 @@ struct rpba_handle {
   }
 
   float seq_sum(const float *v, int n) {
-    launch_seq_sum(v, n, sums, s);
+    PROF("seq_sum", 1, launch_seq_sum(v, n, sums, s));
     float out = 0.f;
     RPBA_CUDA_CHECK(cudaMemcpyAsync(&out, sums, sizeof(float), cudaMemcpyDeviceToHost, s));
     RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -470,25 +556,38 @@ void rpba_handle::reset() {
 
 void rpba_handle::structure() {
   long long npairs = 0;
-  const int nb = build_pairs(L, S, max_pairs, &npairs, s);
+  int nb = 0;
+  PROF("structure_pairs", 3, nb = build_pairs(L, S, max_pairs, &npairs, s));
+  npairs_cur = npairs;
   ensure_blocks(nb);
-  build_bsr(L, S, s);
+  PROF("structure_bsr", 6, build_bsr(L, S, s));
 }
 
 // CalcBundleSep (rbacore.cpp:1094-1195): assemble, solve, back-substitute.
 bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
   const double multfact1 = 1. + multfact;
-  launch_point_pass(L, multfact1, s);
-  launch_camera_pass(L, multfact1, s);
-  launch_pair_pass(L, s);
+  // Algorithmic bytes of each launch (inputs read once, outputs written once):
+  //  point : obs (cam 4, xg 8, w 16, record 248 out) + point (X 24, off 8,
+  //          V^-1 g 96 out) + trial cameras 160
+  //  camera: obs (list 4, record part 184) + camera (block 648 + rhs 72 out)
+  //  pair  : obs records (Bc G, 192) + points (V^-1, 72) + contributions (8)
+  //          + off-diagonal blocks out (648)
+  const double No = L.nobs, Np = L.npts, Nc = nimg, Nb = L.nboff;
+  prof.next_bytes = No * (4 + 8 + 16 + 248) + Np * (24 + 8 + 96) + Nc * 160;
+  PROF("point", 1, launch_point_pass(L, multfact1, s));
+  prof.next_bytes = No * (4 + 184) + (Nc - begini) * (648 + 72);
+  PROF("camera", 1, launch_camera_pass(L, multfact1, s));
+  prof.next_bytes = No * 192 + Np * 72 + npairs_cur * 8. + Nb * 648;
+  PROF("pair", 1, launch_pair_pass(L, s));
   int msize = 0;
   for (int k = begini; k < nimg; ++k) msize += camparv[k + 1] - camparv[k];
   if (msize < 1000) msize = 1000;
   if (opt.pcg_max_iterations > 0) msize = opt.pcg_max_iterations;
-  pcg_solve(L, W, msize, pcg_grid, s);
-  launch_backsub(L, W.xbest, s);
-  launch_xcam(L, W.xbest, s);
-  launch_update(L, nrunknowns, s);
+  PROF("pcg", 2, pcg_solve(L, W, msize, pcg_grid, s));
+  pcg_pending = true;
+  PROF("backsub", 1, launch_backsub(L, W.xbest, s));
+  PROF("xcam", 1, launch_xcam(L, W.xbest, s));
+  PROF("update", 1, launch_update(L, nrunknowns, s));
   RPBA_CUDA_CHECK(cudaGetLastError());
   return false;
 }
@@ -498,7 +597,7 @@ void rpba_handle::robust_delete() {
   const int no = L.nobs, np = L.npts;
   RPBA_CUDA_CHECK(cudaMemsetAsync(okeep + no, 0, sizeof(int), s));
   RPBA_CUDA_CHECK(cudaMemsetAsync(pkeep + np, 0, sizeof(int), s));
-  launch_delete_mark(L, okeep, pkeep, s);
+  PROF("delete", 1, launch_delete_mark(L, okeep, pkeep, s));
   size_t bytes = S.cub_bytes;
   RPBA_CUDA_CHECK(cub_exclusive_sum_int(S.cub_tmp, bytes, okeep, oidx, no + 1, s));
   bytes = S.cub_bytes;
@@ -508,8 +607,8 @@ void rpba_handle::robust_delete() {
   RPBA_CUDA_CHECK(cudaMemcpyAsync(&tot[1], pidx + np, sizeof(int), cudaMemcpyDeviceToHost, s));
   RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
   const int nobs_new = tot[0], npts_new = tot[1];
-  launch_delete_compact(L, oidx, pidx, okeep, pkeep, nobs_new, npts_new, o_cam_n, o_slot_n, o_pt_n, o_xg_n,
-                        o_wold_n, pt_off_n, pt_id_n, X_n, s);
+  PROF("delete", 2, launch_delete_compact(L, oidx, pidx, okeep, pkeep, nobs_new, npts_new, o_cam_n, o_slot_n, o_pt_n,
+                                          o_xg_n, o_wold_n, pt_off_n, pt_id_n, X_n, s));
   std::swap(L.o_cam, o_cam_n);
   std::swap(L.o_slot, o_slot_n);
   std::swap(L.o_pt, o_pt_n);
@@ -541,7 +640,7 @@ int rpba_handle::adjust() {
     if (it > 0) multfact = 1.e-6;
     const int imagepointnr = L.nobs;
     int nrobs = 2 * imagepointnr;
-    build_camera_order(L, S, s);
+    PROF("structure_cam", 2, build_camera_order(L, S, s));
     RPBA_CUDA_CHECK(cudaMemcpyAsync(cnt.data(), S.ccnt, sizeof(int) * nimg, cudaMemcpyDeviceToHost, s));
     RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
     for (int i = 0; i < nimg; ++i)
@@ -549,11 +648,11 @@ int rpba_handle::adjust() {
         if (nimg > 3) log += "BA-Error: No observations in image " + std::to_string(i) + " (image index)\n";
         return RPBA_ERR_NO_OBS_IMAGE;
       }
-    launch_prepare_weights(L, s);
+    PROF("weights", 1, launch_prepare_weights(L, s));
     wsum = seq_sum(L.o_wterm, L.nobs);
     wsum = (float)(2 * imagepointnr) / wsum;
     wsumg = wsum;
-    launch_encode(L, s);
+    PROF("encode", 1, launch_encode(L, s));
     const int nrioff3 = nrioff + 3 * L.npts;
     int nrunknowns = nrioff3 + nadd * nimg;
     int redundancy = nrobs - nrunknowns;
@@ -564,8 +663,8 @@ int rpba_handle::adjust() {
     RPBA_CUDA_CHECK(cudaMemsetAsync(L.x, 0, sizeof(double) * xpmsize, s));
     structure();
     if (it == 0) {
-      launch_decode(L, L.XPM, s);
-      launch_cost(L, L.XPM, true, s);
+      PROF("decode", 1, launch_decode(L, L.XPM, s));
+      PROF("cost", 1, launch_cost(L, L.XPM, true, s));
       float sig0 = seq_sum(L.o_cost, L.nobs);
       sig0 = sig0 * wsumg / (float)redundancy;
       sig0in = sig0old = sig0;
@@ -579,7 +678,7 @@ int rpba_handle::adjust() {
       if (it == 0 && robust) {
         nrunknowns = nunk_given;
         nrobs = nobs_given;
-        launch_reweight(L, iflag, vals, sig00v, nflag, s);
+        PROF("reweight", 3, launch_reweight(L, iflag, vals, sig00v, nflag, s));
         int nf = 0;
         RPBA_CUDA_CHECK(cudaMemcpyAsync(&nf, nflag, sizeof(int), cudaMemcpyDeviceToHost, s));
         wsum = seq_sum(L.o_wterm, L.nobs);
@@ -590,9 +689,9 @@ int rpba_handle::adjust() {
       }
       calc_bundle_sep(multfact, nrunknowns);
       ++solves;
-      launch_decode(L, L.XPMn, s);
-      launch_cost(L, L.XPMn, true, s);
-      launch_seq_sum(L.o_cost, L.nobs, sums, s);
+      PROF("decode", 1, launch_decode(L, L.XPMn, s));
+      PROF("cost", 1, launch_cost(L, L.XPMn, true, s));
+      PROF("seq_sum", 1, launch_seq_sum(L.o_cost, L.nobs, sums, s));
       struct {
         float sig0;
         int err;
@@ -603,12 +702,24 @@ int rpba_handle::adjust() {
       RPBA_CUDA_CHECK(cudaMemcpyAsync(&hv.iters, W.iters, sizeof(int), cudaMemcpyDeviceToHost, s));
       RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
       rep.pcg_iterations += hv.iters;
+      if (prof.on && pcg_pending) {
+        // per PCG iteration: blocks read from both sides (648 * (Nc + 2 Nb)),
+        // block entries (8 each), per camera row the preconditioner (648) and
+        // 22 reads/writes of 9-vectors (72 B each)
+        const double Nc = nimg - begini, Nb = L.nboff;
+        for (auto it = prof.pending.rbegin(); it != prof.pending.rend(); ++it)
+          if (std::string(it->name) == "pcg") {
+            it->bytes = (double)hv.iters * (656. * (Nc + 2. * Nb) + Nc * (648. + 22. * 72.));
+            break;
+          }
+      }
+      pcg_pending = false;
       if (hv.err & 2) return RPBA_ERR_DEVICE_TIMEOUT;
       if (hv.err & 1) return RPBA_ERR_NAN_STEP;
       float sig0 = hv.sig0 * wsumg / (float)redundancy;
       if (sig0old < sig0 * sig0frac) --iflag;
       if (sig0 <= sig0old || iter == 1) {
-        launch_store(L, xpmsize, s);
+        PROF("store", 1, launch_store(L, xpmsize, s));
         sig0old = sig0;
         nrobsnew = nrobs;
         nrunknownsnew = nrunknowns;
@@ -713,6 +824,9 @@ int32_t rpba_solve(rpba_handle *H, rpba_report *rep) {
     RPBA_CUDA_CHECK(cudaSetDevice(H->dev));
     H->log.clear();
     std::memset(&H->rep, 0, sizeof H->rep);
+    H->prof.s = H->s;
+    H->prof.on = (H->opt.verbose & 2) != 0;
+    H->prof.reset();
     H->rep.points_used = H->npts0;
     RPBA_CUDA_CHECK(cudaEventRecord(H->ev0, H->s));
     H->reset();
@@ -722,6 +836,8 @@ int32_t rpba_solve(rpba_handle *H, rpba_report *rep) {
     float ms = 0.f;
     RPBA_CUDA_CHECK(cudaEventElapsedTime(&ms, H->ev0, H->ev1));
     H->rep.solve_seconds = ms * 1e-3;
+    H->prof.resolve();
+    H->rep.kernel_launches = H->prof.launches;
     launch_final_cost(H->L, H->fc_part, H->fc_nparts, H->s);
     std::vector<double> part(2 * H->fc_nparts);
     RPBA_CUDA_CHECK(cudaMemcpyAsync(part.data(), H->fc_part, sizeof(double) * part.size(), cudaMemcpyDeviceToHost, H->s));
@@ -880,6 +996,24 @@ int32_t rpba_exteval(rpba_handle *H, double *resid, rpba_report *rep) {
     }
     return (int)RPBA_OK;
   }, &a);
+}
+
+int32_t rpba_kernel_stats(rpba_handle *H, char *json, size_t cap) {
+  if (!H || !json || cap == 0) return RPBA_ERR_ARG;
+  std::string o = "{";
+  bool first = true;
+  for (auto &st : H->prof.stats) {
+    char b[200];
+    std::snprintf(b, sizeof b, "%s\"%s\": {\"launches\": %lld, \"ms\": %.6f, \"bytes\": %.0f}", first ? "" : ", ",
+                  st.name.c_str(), st.launches, st.ms, st.bytes);
+    o += b;
+    first = false;
+  }
+  o += "}";
+  const size_t n = std::min(cap - 1, o.size());
+  std::memcpy(json, o.data(), n);
+  json[n] = 0;
+  return RPBA_OK;
 }
 
 void rpba_destroy(rpba_handle *H) { delete H; }

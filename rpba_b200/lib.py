@@ -33,7 +33,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no observations i
 # Every entry point include/rpba_b200.h declares.
 EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block_free",
            "rpba_output_block", "rpba_calc_plsa", "rpba_create", "rpba_solve",
-           "rpba_get_state", "rpba_get_log", "rpba_exteval", "rpba_destroy")
+           "rpba_get_state", "rpba_get_log", "rpba_exteval", "rpba_kernel_stats", "rpba_destroy")
 
 _lib = None
 
@@ -73,6 +73,8 @@ def load():
     L.rpba_get_log.restype = C.c_int32
     L.rpba_exteval.argtypes = [C.c_void_p, C.POINTER(C.c_double), rp]
     L.rpba_exteval.restype = C.c_int32
+    L.rpba_kernel_stats.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
+    L.rpba_kernel_stats.restype = C.c_int32
     L.rpba_destroy.argtypes = [C.c_void_p]
     _lib = L
     return L
@@ -157,6 +159,13 @@ class Solver:
         if st != 0:
             raise RpbaError(st, "rpba_exteval")
         return res[: 2 * n].reshape(-1, 2), rep.as_dict()
+
+    def kernel_stats(self) -> dict:
+        """Per-kernel device time of the last solve (needs verbose=2)."""
+        import json
+        buf = C.create_string_buffer(1 << 16)
+        load().rpba_kernel_stats(self.h, buf, 1 << 16)
+        return json.loads(buf.value.decode())
 
     def close(self):
         if self.h:

@@ -40,3 +40,28 @@ def same_tracks(a, b):
     return (np.array_equal(a.pt_obs_off, b.pt_obs_off)
             and np.array_equal(a.pt_obs_image[: a.n_obs], b.pt_obs_image[: b.n_obs])
             and np.array_equal(a.pt_obs_slot[: a.n_obs], b.pt_obs_slot[: b.n_obs]))
+
+
+SIGMA_RTOL = 1e-5  # printed float sigma0: a few float ulps of the cost sum
+
+
+def same_log(a: str, b: str) -> bool:
+    """Log lines agree: words equal, numbers with a '.' or 'e' within
+    SIGMA_RTOL, integers exactly."""
+    la, lb = a.strip().splitlines(), b.strip().splitlines()
+    if len(la) != len(lb):
+        return False
+    for x, y in zip(la, lb):
+        wx, wy = x.split(), y.split()
+        if len(wx) != len(wy):
+            return False
+        for u, v in zip(wx, wy):
+            if u == v:
+                continue
+            try:
+                fu, fv = float(u), float(v)
+            except ValueError:
+                return False
+            if not any(c in u + v for c in ".e") or abs(fu - fv) > SIGMA_RTOL * max(abs(fv), 1e-30):
+                return False
+    return True
