@@ -173,6 +173,13 @@ int32_t rpba_get_log(rpba_handle *h, char *log, size_t cap);
  * (rpbacore.cpp:778-837, 882-941).  resid has 2*pt_obs_off[n_points]
  * entries; entries of points with fewer than two observations are 0. */
 int32_t rpba_exteval(rpba_handle *h, double *resid, rpba_report *rep);
+/* The float sum of v[0..n) accumulated left to right, one rounding per
+ * addition -- the way the reference accumulates its cost and weight sums
+ * (rbacore.cpp:727, 881, 1327) -- computed on the GPU with a bitwise equal
+ * result (values must be finite and >= 0).  No counterpart in the reference;
+ * exposed for verification. */
+int32_t rpba_float_sequential_sum(const float *v, int64_t n, int32_t device, float *out);
+
 /* Per-kernel device time of the last solve as a JSON object
  * {"name": {"launches": n, "ms": t}, ...}; filled only when the handle was
  * created with rpba_options.verbose bit 1 (value 2) set.  No counterpart in

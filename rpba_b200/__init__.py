@@ -8,9 +8,9 @@ package is the Python side of that ABI (``lib``), the block container
 from .block import (Block, RpbaBlockC, RpbaOptionsC, RpbaReportC, make_options,
                     SOLVER_PCG, SOLVER_DIRECT, SOLVER_LEARNED, PREC_FP64, PREC_MIXED)
 from .lib import (InputBlock, OutputBlock, CalcPLSA, Solver, RpbaError, load, LIB_PATH,
-                  EXPORTS, STATUS)
+                  EXPORTS, STATUS, float_sequential_sum)
 
 __all__ = ["Block", "RpbaBlockC", "RpbaOptionsC", "RpbaReportC", "make_options", "SOLVER_PCG",
            "SOLVER_DIRECT", "SOLVER_LEARNED", "PREC_FP64", "PREC_MIXED", "InputBlock",
            "OutputBlock", "CalcPLSA", "Solver", "RpbaError", "load", "LIB_PATH", "EXPORTS",
-           "STATUS"]
+           "STATUS", "float_sequential_sum"]

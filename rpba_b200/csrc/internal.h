@@ -84,6 +84,18 @@ void launch_delete_compact(const DevLSA &L, const int *oidx, const int *pidx, co
                            int *o_slot_n, int *o_pt_n, float2 *o_xg_n, float4 *o_wold_n,
                            int *pt_off_n, int *pt_id_n, double *X_n, cudaStream_t s);
 
+// ---- exact sequential float sums (exactsum.cu)
+struct ExactSumWork {
+  long long *Rc, *Mc;
+  int *Tc;
+  void *ctl;
+  unsigned *bar;
+  int *err;
+  int max_grid;
+};
+int exact_sum_max_grid(int device);
+void launch_exact_sum(const float *v, int n, float *out, const ExactSumWork &W, cudaStream_t s);
+
 // ---- PCG (pcg.cu)
 struct PcgWork {
   double *r, *r1, *d, *q, *h, *h1, *x, *xbest, *Cinv, *partials;

@@ -11,6 +11,7 @@
 // barrier's wait is bounded: after 2 s it sets an error bit and returns.
 #include <cooperative_groups.h>
 
+#include "gridsync.cuh"
 #include "internal.h"
 
 namespace rpba {
@@ -19,44 +20,6 @@ namespace {
 
 constexpr int PCG_T = 256;
 constexpr int PCG_W = PCG_T / 32;
-constexpr unsigned long long BAR_TIMEOUT_NS = 2000000000ull;
-
-__device__ __forceinline__ unsigned long long gtimer() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-// Grid barrier for a cooperative launch (all CTAs co-resident).  Bounded:
-// returns false (and sets err bit 2) if the other CTAs do not arrive.
-__device__ bool grid_barrier(unsigned *bar, unsigned nblocks, int *err) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    volatile unsigned *vgen = bar + 1;
-    const unsigned gen = *vgen;
-    __threadfence();
-    const unsigned arrived = atomicAdd(bar, 1u);
-    if (arrived == nblocks - 1) {
-      atomicExch(bar, 0u);
-      __threadfence();
-      atomicAdd(bar + 1, 1u);
-    } else {
-      const unsigned long long t0 = gtimer();
-      while (*vgen == gen) {
-        if (*(volatile int *)err) break;
-        if (gtimer() - t0 > BAR_TIMEOUT_NS) {
-          atomicOr(err, 2);
-          break;
-        }
-        __nanosleep(40);
-      }
-    }
-    __threadfence();
-  }
-  __syncthreads();
-  return *(volatile int *)err == 0;
-}
-
 struct PcgArgs {
   const double *blocks;
   const int *rowoff;

@@ -191,6 +191,7 @@ struct rpba_handle {
   int fc_nparts = 0;
   StructWork S{};
   PcgWork W{};
+  ExactSumWork ES{};
   int blocks_cap = 0;
   cudaEvent_t ev0, ev1;
 
@@ -222,7 +223,7 @@ struct rpba_handle {
   }
 
   float seq_sum(const float *v, int n) {
-    PROF("seq_sum", 1, launch_seq_sum(v, n, sums, s));
+    PROF("seq_sum", 1, launch_exact_sum(v, n, sums, ES, s));
     float out = 0.f;
     RPBA_CUDA_CHECK(cudaMemcpyAsync(&out, sums, sizeof(float), cudaMemcpyDeviceToHost, s));
     RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -272,6 +273,16 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
     const int im = H->h_pt_img[i];
     if (im < 0 || im >= n || H->h_pt_slot[i] < 0 || H->h_pt_slot[i] >= H->h_img_off[im + 1] - H->h_img_off[im])
       return RPBA_ERR_ARG;
+  }
+  {
+    H->ES.max_grid = exact_sum_max_grid(H->dev);
+    H->ES.Rc = dalloc<long long>(H->ES.max_grid, own);
+    H->ES.Mc = dalloc<long long>(H->ES.max_grid, own);
+    H->ES.Tc = dalloc<int>(H->ES.max_grid, own);
+    H->ES.ctl = dalloc<char>(16, own);
+    H->ES.bar = dalloc<unsigned>(2, own);
+    H->ES.err = dalloc<int>(4, own);
+    RPBA_CUDA_CHECK(cudaMemsetAsync(H->ES.err, 0, 4 * sizeof(int), H->s));
   }
   if (o->exteval) return RPBA_OK;
 
@@ -503,6 +514,7 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   S.iota = dalloc<int>(no, own);
   S.ckey = dalloc<unsigned>(no, own);
   S.ckey2 = dalloc<unsigned>(no, own);
+  H->ES.err = L.err;  // a barrier timeout in a sum surfaces in the LSA's error word
   // PCG work
   H->pcg_grid = pcg_max_grid(H->dev);
   PcgWork &W = H->W;
@@ -691,7 +703,7 @@ int rpba_handle::adjust() {
       ++solves;
       PROF("decode", 1, launch_decode(L, L.XPMn, s));
       PROF("cost", 1, launch_cost(L, L.XPMn, true, s));
-      PROF("seq_sum", 1, launch_seq_sum(L.o_cost, L.nobs, sums, s));
+      PROF("seq_sum", 1, launch_exact_sum(L.o_cost, L.nobs, sums, ES, s));
       struct {
         float sig0;
         int err;
@@ -968,7 +980,7 @@ int32_t rpba_exteval(rpba_handle *H, double *resid, rpba_report *rep) {
     up(pi, H->h_pt_img.data(), sizeof(int) * nt);
     up(ps, H->h_pt_slot.data(), sizeof(int) * nt);
     launch_exteval(np, po, pi, ps, io, pm, K, ds, XX, xg, wx, wy, wxy, res, term, red, H->s);
-    launch_seq_sum(term, np, sum, H->s);
+    launch_exact_sum(term, np, sum, H->ES, H->s);
     std::vector<int> hred(np);
     float s = 0.f;
     if (np) RPBA_CUDA_CHECK(cudaMemcpyAsync(hred.data(), red, sizeof(int) * np, cudaMemcpyDeviceToHost, H->s));
@@ -995,6 +1007,45 @@ int32_t rpba_exteval(rpba_handle *H, double *resid, rpba_report *rep) {
       a->rep->exteval_redundancy = r;
     }
     return (int)RPBA_OK;
+  }, &a);
+}
+
+int32_t rpba_float_sequential_sum(const float *v, int64_t n, int32_t device, float *out) {
+  if (!out || n < 0 || n > 0x7fffffff || (n > 0 && !v)) return RPBA_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device) return RPBA_ERR_NO_DEVICE;
+  struct A {
+    const float *v;
+    int n, dev;
+    float *out;
+  } a{v, (int)n, device, out};
+  return guard([](void *p) {
+    A *a = (A *)p;
+    RPBA_CUDA_CHECK(cudaSetDevice(a->dev));
+    std::vector<void *> own;
+    struct Free {
+      std::vector<void *> &o;
+      ~Free() {
+        for (void *q : o) cudaFree(q);
+      }
+    } fr{own};
+    cudaStream_t s = 0;
+    ExactSumWork W{};
+    W.max_grid = exact_sum_max_grid(a->dev);
+    W.Rc = dalloc<long long>(W.max_grid, own);
+    W.Mc = dalloc<long long>(W.max_grid, own);
+    W.Tc = dalloc<int>(W.max_grid, own);
+    W.ctl = dalloc<char>(16, own);
+    W.bar = dalloc<unsigned>(2, own);
+    W.err = dalloc<int>(1, own);
+    float *dv = dalloc<float>(std::max(a->n, 1), own), *dout = dalloc<float>(1, own);
+    RPBA_CUDA_CHECK(cudaMemset(W.err, 0, sizeof(int)));
+    if (a->n) RPBA_CUDA_CHECK(cudaMemcpy(dv, a->v, sizeof(float) * a->n, cudaMemcpyHostToDevice));
+    launch_exact_sum(dv, a->n, dout, W, s);
+    int err = 0;
+    RPBA_CUDA_CHECK(cudaMemcpy(a->out, dout, sizeof(float), cudaMemcpyDeviceToHost));
+    RPBA_CUDA_CHECK(cudaMemcpy(&err, W.err, sizeof(int), cudaMemcpyDeviceToHost));
+    return err ? (int)RPBA_ERR_DEVICE_TIMEOUT : (int)RPBA_OK;
   }, &a);
 }
 

@@ -33,7 +33,8 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no observations i
 # Every entry point include/rpba_b200.h declares.
 EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block_free",
            "rpba_output_block", "rpba_calc_plsa", "rpba_create", "rpba_solve",
-           "rpba_get_state", "rpba_get_log", "rpba_exteval", "rpba_kernel_stats", "rpba_destroy")
+           "rpba_get_state", "rpba_get_log", "rpba_exteval", "rpba_kernel_stats", "rpba_float_sequential_sum",
+           "rpba_destroy")
 
 _lib = None
 
@@ -73,6 +74,9 @@ def load():
     L.rpba_get_log.restype = C.c_int32
     L.rpba_exteval.argtypes = [C.c_void_p, C.POINTER(C.c_double), rp]
     L.rpba_exteval.restype = C.c_int32
+    L.rpba_float_sequential_sum.argtypes = [C.POINTER(C.c_float), C.c_int64, C.c_int32,
+                                            C.POINTER(C.c_float)]
+    L.rpba_float_sequential_sum.restype = C.c_int32
     L.rpba_kernel_stats.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     L.rpba_kernel_stats.restype = C.c_int32
     L.rpba_destroy.argtypes = [C.c_void_p]
@@ -116,6 +120,18 @@ def CalcPLSA(block: Block, robust: bool = True, addflags=(True, True, True), thr
     if st in (2, 9):
         raise RpbaError(st, "CalcPLSA")
     return st, buf.value.decode(), rep.as_dict()
+
+
+def float_sequential_sum(v, device: int = 0) -> np.float32:
+    """Left-to-right float32 sum of ``v`` (values finite, >= 0) on the GPU,
+    bitwise equal to the sequential loop."""
+    a = np.ascontiguousarray(v, dtype=np.float32)
+    out = C.c_float()
+    st = load().rpba_float_sequential_sum(a.ctypes.data_as(C.POINTER(C.c_float)), a.size, device,
+                                          C.byref(out))
+    if st != 0:
+        raise RpbaError(st, "rpba_float_sequential_sum")
+    return np.float32(out.value)
 
 
 class Solver:
