@@ -53,6 +53,10 @@ struct DevLSA {
   const int2 *contrib; // (obs in the row camera, obs in the column camera)
   const int *rowoff;   // [nimg + 1]
   const int2 *ent;     // (column camera, block index | 0x80000000 if transposed)
+  // SpMV work items: runs of <= 3 entries of one row
+  int nitems;
+  const int *row_item_off;  // [nimg + 1]
+  const int4 *item_meta;    // (row, first entry, end entry, 0)
   int *err;            // device error word
 };
 
@@ -98,7 +102,7 @@ void launch_exact_sum(const float *v, int n, float *out, const ExactSumWork &W, 
 
 // ---- PCG (pcg.cu)
 struct PcgWork {
-  double *r, *r1, *d, *q, *h, *h1, *x, *xbest, *Cinv, *partials;
+  double *r, *r1, *d, *q, *h, *h1, *x, *xbest, *Cinv, *partials, *part;
   unsigned *bar;
   int *iters;
 };
@@ -124,6 +128,8 @@ struct StructWork {
   int2 *ent;
   int *iota, *iota2;
   unsigned *ckey, *ckey2;
+  int *row_items, *row_item_off;
+  int4 *item_meta;
 };
 size_t structure_cub_bytes(int nobs, long long npairs, int nimg);
 // camera grouping: returns 0, fills camlist/coff; counts in ccnt

@@ -18,189 +18,254 @@ namespace rpba {
 
 namespace {
 
-constexpr int PCG_T = 256;
+constexpr int PCG_T = 1024;
 constexpr int PCG_W = PCG_T / 32;
+
 struct PcgArgs {
   const double *blocks;
-  const int *rowoff;
   const int2 *ent;
+  const int *rowoff;
+  const int *row_item_off;
+  const int4 *item_meta;  // (row, first entry, end entry, 0)
   const double *Cinv;
-  double *r, *r1, *d, *q, *h, *h1, *x, *xbest;
-  double *part1, *part2;
+  double *r, *h, *x, *xbest, *D0, *D1;
+  double *part;        // [nitems * 9] SpMV partial rows
+  double *red1, *red2; // [gridDim * 4] per-CTA partial sums of phase 1 / phase 2
+                       // (separate, so a fast CTA never overwrites a slot that
+                       // a slow CTA is still reading)
   unsigned *bar;
   int *err;
   int *iters;
-  int row0, row1, msize;
+  int row0, row1, nitems, msize;
 };
 
-// Deterministic CTA sum of two values; the result is valid in thread 0.
-__device__ __forceinline__ void cta_sum2(double &a, double &b, double (*sh)[2]) {
+// Deterministic CTA sum of up to three values; valid in every thread.
+template <int N>
+__device__ __forceinline__ void cta_sum(double (&v)[N], double (*sh)[4]) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_xor_sync(0xffffffffu, a, o);
-    b += __shfl_xor_sync(0xffffffffu, b, o);
-  }
+  for (int j = 0; j < N; ++j)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[j] += __shfl_xor_sync(0xffffffffu, v[j], o);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) {
-    sh[warp][0] = a;
-    sh[warp][1] = b;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s0 = 0., s1 = 0.;
-    for (int w = 0; w < PCG_W; ++w) {
-      s0 += sh[w][0];
-      s1 += sh[w][1];
-    }
-    a = s0;
-    b = s1;
-  }
-  __syncthreads();
-}
-
-// Sum of the per-CTA partials in a fixed order; identical in every CTA.
-__device__ __forceinline__ void grid_sum2(const double *part, int n, double &a, double &b,
-                                          double *bc) {
-  if (threadIdx.x < 32) {
-    double s0 = 0., s1 = 0.;
-    for (int i = threadIdx.x; i < n; i += 32) {
-      s0 += __ldcg(part + 2 * i);
-      s1 += __ldcg(part + 2 * i + 1);
-    }
+  if (lane == 0)
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-      s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-    }
-    if (threadIdx.x == 0) {
-      bc[0] = s0;
-      bc[1] = s1;
+    for (int j = 0; j < N; ++j) sh[warp][j] = v[j];
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      double t = lane < PCG_W ? sh[lane][j] : 0.;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (lane == 0) sh[PCG_W][j] = t;
     }
   }
   __syncthreads();
-  a = bc[0];
-  b = bc[1];
+#pragma unroll
+  for (int j = 0; j < N; ++j) v[j] = sh[PCG_W][j];
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(PCG_T) k_pcg(PcgArgs A) {
+// Sum of the per-CTA partials (stride 4) in a fixed order; every CTA gets
+// the same values.
+template <int N>
+__device__ __forceinline__ void grid_sum(const double *red, int G, double (&v)[N], double (*sh)[4]) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (warp == 0) {
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+      double t = 0.;
+      for (int i = lane; i < G; i += 32) t += __ldcg(red + 4 * i + j);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (lane == 0) sh[PCG_W][j] = t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < N; ++j) v[j] = sh[PCG_W][j];
+  __syncthreads();
+}
+
+// Iteration k (two grid barriers):
+//  phase 1  q-partials of A d^k per work item (<= 3 blocks of one row), with
+//           d^k = h^k + beta^(k-1) d^(k-1) formed on the fly; partial d^T q
+//  phase 2  per row: q = sum of its items' partials, x += alpha d,
+//           r1 = r - alpha q, h1 = C r1; partials of (alpha q)^2,
+//           r1^T (h1 - h) and r1^T h1 (the next r^T h); d^k is stored
+__global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gwarp = blockIdx.x * PCG_W + warp, nwarps = gridDim.x * PCG_W;
-  const int grp = lane / 9, rr = lane % 9;
-  __shared__ double sh[PCG_W][2];
-  __shared__ double bc[2];
-  double meandrold = 1.e50, meandr0 = 1.e50;
+  const int grp = lane / 9, rr = lane % 9, gbase = grp * 9;
+  const int G = gridDim.x;
+  __shared__ double sh[PCG_W + 1][4];
+  // r^T h of the start vectors
+  {
+    double v[1] = {0.};
+    for (int row = A.row0 + gwarp; row < A.row1; row += nwarps)
+      if (lane < 9) {
+        const size_t i = (size_t)row * 9 + lane;
+        v[0] += A.r[i] * A.h[i];
+      }
+    cta_sum<1>(v, sh);
+    if (threadIdx.x == 0) A.red2[4 * blockIdx.x] = v[0];
+  }
+  if (!grid_barrier(A.bar, G, A.err)) return;
+  double erthk;
+  {
+    double v[1];
+    grid_sum<1>(A.red2, G, v, sh);
+    erthk = v[0];
+  }
+  double meandrold = 1.e50, meandr0 = 1.e50, beta_prev = 0.;
   int k;
   for (k = 0; k < A.msize; ++k) {
-    // q = A d ; r^T h ; d^T q
-    double prh = 0., pdq = 0.;
-    for (int row = A.row0 + gwarp; row < A.row1; row += nwarps) {
+    const double *dprev = (k & 1) ? A.D0 : A.D1;
+    double *dcur = (k & 1) ? A.D1 : A.D0;
+    // ---- phase 1
+    double pdq[1] = {0.};
+    // item metadata and the block entry of the next item are prefetched
+    int it = gwarp;
+    int4 meta = it < A.nitems ? A.item_meta[it] : make_int4(0, 0, 0, 0);
+    int2 en_next = make_int2(0, 0);
+    if (it < A.nitems && lane < 27 && meta.y + grp < meta.z) en_next = A.ent[meta.y + grp];
+    for (; it < A.nitems; it += nwarps) {
+      const int row = meta.x;
+      const int e = meta.y + grp;
+      const bool act = lane < 27 && e < meta.z;
+      const int2 en = en_next;
+      const int itn = it + nwarps;
+      if (itn < A.nitems) {
+        meta = A.item_meta[itn];
+        if (lane < 27 && meta.y + grp < meta.z) en_next = A.ent[meta.y + grp];
+      }
       double acc = 0.;
-      if (lane < 27) {
-        const int e1 = A.rowoff[row + 1];
-        for (int e = A.rowoff[row] + grp; e < e1; e += 3) {
-          const int2 en = A.ent[e];
-          const double *B = A.blocks + (size_t)(en.y & 0x7fffffff) * 81;
-          const double *xv = A.d + (size_t)en.x * 9;
-          if (en.y >= 0) {
+      int col = 0, blk = 0;
+      bool tr = false;
+      if (act) {
+        col = en.x;
+        blk = en.y & 0x7fffffff;
+        tr = en.y < 0;
+      }
+      // lane (gbase + c) forms d^k[col][c]; the group gathers it by shuffles
+      double dc = 0.;
+      if (act) {
+        const size_t j = (size_t)col * 9 + rr;
+        dc = __ldcg(A.h + j) + beta_prev * __ldcg(dprev + j);
+      }
+      const double *B = A.blocks + (size_t)blk * 81;
 #pragma unroll
-            for (int c = 0; c < 9; ++c) acc += B[rr * 9 + c] * __ldcg(xv + c);
-          } else {
-#pragma unroll
-            for (int c = 0; c < 9; ++c) acc += B[c * 9 + rr] * __ldcg(xv + c);
-          }
-        }
+      for (int c = 0; c < 9; ++c) {
+        const double xc = __shfl_sync(0xffffffffu, dc, (lane < 27 ? gbase : 0) + c);
+        if (act) acc += __ldg(B + (tr ? c * 9 + rr : rr * 9 + c)) * xc;
       }
       const double a1 = __shfl_down_sync(0xffffffffu, acc, 9);
       const double a2 = __shfl_down_sync(0xffffffffu, acc, 18);
       if (lane < 9) {
+        const double p = acc + a1 + a2;
+        A.part[(size_t)it * 9 + lane] = p;
         const size_t i = (size_t)row * 9 + lane;
-        const double qv = acc + a1 + a2;
-        A.q[i] = qv;
-        prh += __ldcg(A.r + i) * __ldcg(A.h + i);
-        pdq += __ldcg(A.d + i) * qv;
+        const double dk = __ldcg(A.h + i) + beta_prev * __ldcg(dprev + i);
+        pdq[0] += dk * p;
       }
     }
-    cta_sum2(prh, pdq, sh);
-    if (threadIdx.x == 0) {
-      A.part1[2 * blockIdx.x] = prh;
-      A.part1[2 * blockIdx.x + 1] = pdq;
+    cta_sum<1>(pdq, sh);
+    if (threadIdx.x == 0) A.red1[4 * blockIdx.x] = pdq[0];
+    if (!grid_barrier(A.bar, G, A.err)) return;
+    double edtAdk;
+    {
+      double v[1];
+      grid_sum<1>(A.red1, G, v, sh);
+      edtAdk = v[0];
     }
-    if (!grid_barrier(A.bar, gridDim.x, A.err)) return;
-    double erthk, edtAdk;
-    grid_sum2(A.part1, gridDim.x, erthk, edtAdk, bc);
     double alpha;
     if (fabs(erthk) < 1.e-20 || fabs(erthk) > 1.e20)
       alpha = 0.;
     else
       alpha = erthk / edtAdk;
-    // x += alpha d ; r1 = r - alpha q ; h1 = C r1
-    double pmd = 0., pe1 = 0.;
+    // ---- phase 2
+    double p2[3] = {0., 0., 0.};
     for (int row = A.row0 + gwarp; row < A.row1; row += nwarps) {
       const size_t i = (size_t)row * 9 + (lane < 9 ? lane : 0);
       double r1v = 0., hv = 0.;
+      // q = sum of the row's item partials: the three 9-lane groups take
+      // every third item, four independent loads in flight, fixed order
+      double qg = 0.;
+      if (lane < 27) {
+        const int t0 = A.row_item_off[row], t1 = A.row_item_off[row + 1];
+        double q0 = 0., q1 = 0., q2 = 0., q3 = 0.;
+        int t = t0 + grp;
+        for (; t + 9 < t1; t += 12) {
+          q0 += __ldcg(A.part + (size_t)t * 9 + rr);
+          q1 += __ldcg(A.part + (size_t)(t + 3) * 9 + rr);
+          q2 += __ldcg(A.part + (size_t)(t + 6) * 9 + rr);
+          q3 += __ldcg(A.part + (size_t)(t + 9) * 9 + rr);
+        }
+        for (; t < t1; t += 3) q0 += __ldcg(A.part + (size_t)t * 9 + rr);
+        qg = (q0 + q1) + (q2 + q3);
+      }
+      const double qa = __shfl_down_sync(0xffffffffu, qg, 9);
+      const double qb = __shfl_down_sync(0xffffffffu, qg, 18);
       if (lane < 9) {
-        const double dv = __ldcg(A.d + i);
-        A.x[i] = __ldcg(A.x + i) + alpha * dv;
-        const double dr = alpha * A.q[i];
-        r1v = __ldcg(A.r + i) - dr;
-        pmd += dr * dr;
+        const double q = qg + qa + qb;
         hv = __ldcg(A.h + i);
+        const double dk = hv + beta_prev * __ldcg(dprev + i);
+        dcur[i] = dk;
+        A.x[i] = A.x[i] + alpha * dk;
+        const double dr = alpha * q;
+        r1v = A.r[i] - dr;
+        p2[0] += dr * dr;
       }
       const double *C = A.Cinv + (size_t)row * 81;
       double h1v = 0.;
 #pragma unroll
       for (int c = 0; c < 9; ++c) {
         const double rc = __shfl_sync(0xffffffffu, r1v, c);
-        if (lane < 9) h1v += C[lane * 9 + c] * rc;
+        if (lane < 9) h1v += __ldg(C + lane * 9 + c) * rc;
       }
       if (lane < 9) {
-        A.r1[i] = r1v;
-        A.h1[i] = h1v;
-        pe1 += r1v * (h1v - hv);
+        A.r[i] = r1v;
+        A.h[i] = h1v;
+        p2[1] += r1v * (h1v - hv);
+        p2[2] += r1v * h1v;
       }
     }
-    cta_sum2(pmd, pe1, sh);
+    cta_sum<3>(p2, sh);
     if (threadIdx.x == 0) {
-      A.part2[2 * blockIdx.x] = pmd;
-      A.part2[2 * blockIdx.x + 1] = pe1;
+      A.red2[4 * blockIdx.x] = p2[0];
+      A.red2[4 * blockIdx.x + 1] = p2[1];
+      A.red2[4 * blockIdx.x + 2] = p2[2];
     }
-    if (!grid_barrier(A.bar, gridDim.x, A.err)) return;
-    double meandr, er1th1;
-    grid_sum2(A.part2, gridDim.x, meandr, er1th1, bc);
+    if (!grid_barrier(A.bar, G, A.err)) return;
+    double g3[3];
+    grid_sum<3>(A.red2, G, g3, sh);
+    const double meandr = g3[0], er1th1 = g3[1];
     if (k == 0) meandr0 = meandr;
     const bool improved = meandr < meandrold;
-    if (improved) meandrold = meandr;
-    const bool stop = meandr * 1.e5 < meandr0;
+    if (improved) {
+      meandrold = meandr;
+      for (int row = A.row0 + gwarp; row < A.row1; row += nwarps)
+        if (lane < 9) A.xbest[(size_t)row * 9 + lane] = A.x[(size_t)row * 9 + lane];
+    }
+    if (meandr * 1.e5 < meandr0) break;
     double beta = fabs(er1th1) < 1.e-10 ? 0. : er1th1 / erthk;
     if (beta < 0.) beta = 0.;
-    for (int row = A.row0 + gwarp; row < A.row1; row += nwarps) {
-      if (lane < 9) {
-        const size_t i = (size_t)row * 9 + lane;
-        if (improved) A.xbest[i] = A.x[i];
-        if (!stop) {
-          const double h1v = A.h1[i];
-          A.d[i] = h1v + beta * __ldcg(A.d + i);
-          A.r[i] = A.r1[i];
-          A.h[i] = h1v;
-        }
-      }
-    }
-    if (stop) break;
-    if (!grid_barrier(A.bar, gridDim.x, A.err)) return;
+    beta_prev = beta;
+    erthk = g3[2];
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) *A.iters = k < A.msize ? k + 1 : A.msize;
 }
 
 // Preconditioner C_k = S_kk^-1 (rbacore.cpp:1839-1846) and the start
-// vectors: r = b, h = C r, d = h, x = 0, best = b.
+// vectors: r = b, h = C r, d^(-1) = 0, x = 0, best = b.
 __global__ void k_pcg_setup(DevLSA L, PcgWork W) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= L.nimg) return;
   double *C = W.Cinv + (size_t)k * 81;
   const size_t o = (size_t)k * 9;
+  for (int a = 0; a < 9; ++a) W.d[o + a] = W.r1[o + a] = 0.;
   if (k < L.begini) {
-    for (int a = 0; a < 9; ++a) W.r[o + a] = W.h[o + a] = W.d[o + a] = W.x[o + a] = W.xbest[o + a] = 0.;
+    for (int a = 0; a < 9; ++a) W.r[o + a] = W.h[o + a] = W.x[o + a] = W.xbest[o + a] = 0.;
     return;
   }
   const int np = L.camparv[k + 1] - L.camparv[k];
@@ -212,7 +277,6 @@ __global__ void k_pcg_setup(DevLSA L, PcgWork W) {
     for (int c = 0; c < 9; ++c) s += C[a * 9 + c] * rv[c];
     W.r[o + a] = rv[a];
     W.h[o + a] = s;
-    W.d[o + a] = s;
     W.x[o + a] = 0.;
     W.xbest[o + a] = rv[a];
   }
@@ -228,35 +292,38 @@ int pcg_max_grid(int device) {
   return nsm * per;
 }
 
-// Returns the number of PCG iterations; throws CudaError on launch errors.
+// Returns 0; throws CudaError on launch errors.  The iteration count is
+// left in W.iters.
 int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s) {
   k_pcg_setup<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W);
   RPBA_CUDA_CHECK(cudaGetLastError());
   const int nrows = L.nimg - L.begini;
   if (nrows <= 0) return 0;
-  int g = (nrows + PCG_W - 1) / PCG_W;
+  int g = (L.nitems + PCG_W - 1) / PCG_W;
   if (g > grid) g = grid;
   if (g < 1) g = 1;
   PcgArgs A;
   A.blocks = L.blocks;
-  A.rowoff = L.rowoff;
   A.ent = L.ent;
+  A.rowoff = L.rowoff;
+  A.row_item_off = L.row_item_off;
+  A.item_meta = L.item_meta;
   A.Cinv = W.Cinv;
   A.r = W.r;
-  A.r1 = W.r1;
-  A.d = W.d;
-  A.q = W.q;
   A.h = W.h;
-  A.h1 = W.h1;
   A.x = W.x;
   A.xbest = W.xbest;
-  A.part1 = W.partials;
-  A.part2 = W.partials + 2 * (size_t)grid;
+  A.D0 = W.q;
+  A.D1 = W.d;
+  A.part = W.part;
+  A.red1 = W.partials;
+  A.red2 = W.partials + 4 * (size_t)grid;
   A.bar = W.bar;
   A.err = L.err;
   A.iters = W.iters;
   A.row0 = L.begini;
   A.row1 = L.nimg;
+  A.nitems = L.nitems;
   A.msize = msize;
   RPBA_CUDA_CHECK(cudaMemsetAsync(W.bar, 0, 2 * sizeof(unsigned), s));
   void *args[] = {&A};

@@ -212,13 +212,17 @@ struct rpba_handle {
     if (nb <= blocks_cap && L.blocks) return;
     const int cap = std::max(nb, 1);
     if (L.blocks) {
-      cudaFree(L.blocks);
-      cudaFree(S.ent);
-      owned.erase(std::remove(owned.begin(), owned.end(), (void *)L.blocks), owned.end());
-      owned.erase(std::remove(owned.begin(), owned.end(), (void *)S.ent), owned.end());
+      for (void *p : {(void *)L.blocks, (void *)S.ent, (void *)S.item_meta, (void *)W.part}) {
+        cudaFree(p);
+        owned.erase(std::remove(owned.begin(), owned.end(), p), owned.end());
+      }
     }
     L.blocks = dalloc<double>((size_t)(nimg + cap) * 81, owned);
     S.ent = dalloc<int2>((size_t)nimg + 2 * (size_t)cap, owned);
+    // SpMV work items: at most ceil(entries / 3) per row
+    const size_t items = (size_t)nimg + ((size_t)nimg + 2 * (size_t)cap) / 3 + 1;
+    S.item_meta = dalloc<int4>(items, owned);
+    W.part = dalloc<double>(items * 9, owned);
     blocks_cap = cap;
   }
 
@@ -512,6 +516,8 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   S.tidx = dalloc<int>(mb, own);
   S.tidx2 = dalloc<int>(mb, own);
   S.iota = dalloc<int>(no, own);
+  S.row_items = dalloc<int>(n + 1, own);
+  S.row_item_off = dalloc<int>(n + 1, own);
   S.ckey = dalloc<unsigned>(no, own);
   S.ckey2 = dalloc<unsigned>(no, own);
   H->ES.err = L.err;  // a barrier timeout in a sum surfaces in the LSA's error word
@@ -528,7 +534,7 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   W.x = dalloc<double>(nv, own);
   W.xbest = dalloc<double>(nv, own);
   W.Cinv = dalloc<double>(81 * (size_t)n, own);
-  W.partials = dalloc<double>(4 * (size_t)H->pcg_grid, own);
+  W.partials = dalloc<double>(8 * (size_t)H->pcg_grid, own);
   W.bar = dalloc<unsigned>(2, own);
   W.iters = dalloc<int>(1, own);
   RPBA_CUDA_CHECK(cudaMemsetAsync(W.r1, 0, sizeof(double) * nv, H->s));

@@ -118,6 +118,23 @@ __global__ void k_fill_transposed(const unsigned *bkey, const int *tidx_sorted, 
   ent[pos] = make_int2(row, (int)((unsigned)(nimg + b) | 0x80000000u));
 }
 
+// Work items of the SpMV: each row's entry list cut into runs of <= 3.
+__global__ void k_row_items(const int *rowoff, int nimg, int begini, int *cnt) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > nimg) return;
+  cnt[k] = (k < nimg && k >= begini) ? (rowoff[k + 1] - rowoff[k] + 2) / 3 : 0;
+}
+
+__global__ void k_fill_items(const int *rowoff, const int *row_item_off, int nimg, int begini, int4 *meta) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nimg || k < begini) return;
+  const int end = rowoff[k + 1];
+  for (int t = row_item_off[k], j = 0; t < row_item_off[k + 1]; ++t, ++j) {
+    const int e0 = rowoff[k] + 3 * j;
+    meta[t] = make_int4(k, e0, min(e0 + 3, end), 0);
+  }
+}
+
 __global__ void k_fill_diag(int nimg, const int *rowoff, const int *cntT, int2 *ent) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nimg) return;
@@ -212,8 +229,18 @@ void build_bsr(DevLSA &L, StructWork &S, cudaStream_t s) {
     k_fill_transposed<<<nblk(nb, 256), 256, 0, s>>>(S.bkey, S.tidx2, nb, n, S.rowoff, S.firstT, S.ent);
   }
   k_fill_diag<<<nblk(n, 256), 256, 0, s>>>(n, S.rowoff, S.cntT, S.ent);
+  k_row_items<<<nblk(n + 1, 256), 256, 0, s>>>(S.rowoff, n, L.begini, S.row_items);
+  bytes = S.cub_bytes;
+  RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(S.cub_tmp, bytes, S.row_items, S.row_item_off, n + 1, s));
+  int nitems = 0;
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(&nitems, S.row_item_off + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+  k_fill_items<<<nblk(n, 256), 256, 0, s>>>(S.rowoff, S.row_item_off, n, L.begini, S.item_meta);
   L.rowoff = S.rowoff;
   L.ent = S.ent;
+  L.nitems = nitems;
+  L.row_item_off = S.row_item_off;
+  L.item_meta = S.item_meta;
 }
 
 cudaError_t cub_exclusive_sum_int(void *tmp, size_t &bytes, const int *in, int *out, int n, cudaStream_t s) {
