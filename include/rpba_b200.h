@@ -56,7 +56,8 @@ typedef enum rpba_status {
   RPBA_ERR_IO = 7,              /* file could not be read or written        */
   RPBA_ERR_UNSUPPORTED = 8,     /* input the GPU path does not accept       */
   RPBA_ERR_NO_DEVICE = 9,       /* no CUDA device / library not usable      */
-  RPBA_ERR_SOLVER = 10          /* direct factorisation failed (not SPD)    */
+  RPBA_ERR_SOLVER = 10,         /* direct factorisation failed (not SPD)    */
+  RPBA_ERR_TOO_LARGE = 11       /* input exceeds a fixed-size scratch area  */
 } rpba_status;
 
 typedef struct rpba_block {
@@ -179,6 +180,23 @@ int32_t rpba_exteval(rpba_handle *h, double *resid, rpba_report *rep);
  * result (values must be finite and >= 0).  No counterpart in the reference;
  * exposed for verification. */
 int32_t rpba_float_sequential_sum(const float *v, int64_t n, int32_t device, float *out);
+
+/* Allocation-free form of rpba_float_sequential_sum, for callers that must
+ * not have a library call cudaMalloc or cudaFree -- an application that hands
+ * out all device memory from its own fixed-budget pool, or a latency-critical
+ * loop that cannot take the device-wide synchronisation cudaFree implies.
+ * d_v and d_out are device pointers on the calling thread's current device;
+ * the work is enqueued on `stream` (a cudaStream_t; NULL = legacy default
+ * stream) and the call returns without waiting for it.  Scratch lives in one
+ * static device array of the library (about 20 KB, held by every GPU that
+ * loads the library until the process exits), which caps n at 4,194,304
+ * (1024 CTAs x 4096 elements): larger n returns RPBA_ERR_TOO_LARGE.  The first
+ * call on a device looks up that array's device address (a blocking runtime
+ * query), so make the first call on each device before any stream capture.
+ * All calls share the one array: calls that overlap on the GPU (different
+ * streams, or different host threads, on the same device) race and must be
+ * serialised by the caller.  No counterpart in the reference. */
+int32_t rpba_float_sequential_sum_noalloc(const float *d_v, int64_t n, float *d_out, void *stream);
 
 /* Per-kernel device time of the last solve as a JSON object
  * {"name": {"launches": n, "ms": t}, ...}; filled only when the handle was

@@ -17,6 +17,9 @@
 //
 // The first HEAD elements and any stretch where s is zero or subnormal are
 // added by one warp in plain sequence.  Inputs must be finite and >= 0.
+#include <mutex>
+
+#include "../../include/rpba_b200.h"
 #include "gridsync.cuh"
 #include "internal.h"
 
@@ -299,3 +302,90 @@ void launch_exact_sum(const float *v, int n, float *out, const ExactSumWork &W, 
 }
 
 }  // namespace rpba
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the exact float sum.
+//
+// Some callers cannot let a library call cudaMalloc or cudaFree: a host
+// application that hands all device memory out of its own fixed-budget pool
+// (a stray cudaMalloc breaks its accounting or fails when the pool owns the
+// whole device), or a latency-critical loop that cannot absorb the
+// device-wide synchronisation cudaFree implies.  For them this entry point
+// keeps its scratch -- the per-CTA run sums, the run control word and the
+// grid-barrier counters of k_exact_sum -- in one statically sized device
+// array that every GPU loading the library holds until the process exits
+// (about 20 KB).  Its size caps the input at NA_MAX_CTAS CTAs of NA_CHUNK
+// elements each.
+using namespace rpba;
+
+namespace {
+
+constexpr int NA_MAX_CTAS = 1024;
+constexpr int NA_CHUNK = 4096;
+constexpr long long NA_MAX_N = (long long)NA_MAX_CTAS * NA_CHUNK;  // 4,194,304
+constexpr size_t NA_OFF_RC = 0;
+constexpr size_t NA_OFF_MC = NA_OFF_RC + sizeof(long long) * NA_MAX_CTAS;
+constexpr size_t NA_OFF_TC = NA_OFF_MC + sizeof(long long) * NA_MAX_CTAS;
+constexpr size_t NA_OFF_CTL = NA_OFF_TC + sizeof(int) * NA_MAX_CTAS;
+constexpr size_t NA_OFF_BAR = NA_OFF_CTL + 16;
+constexpr size_t NA_OFF_ERR = NA_OFF_BAR + 16;
+constexpr size_t NA_BYTES = NA_OFF_ERR + 16;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
+
+constexpr int NA_MAX_DEVICES = 64;
+std::mutex g_na_mutex;
+unsigned char *g_na_addr[NA_MAX_DEVICES];  // device address of the scratch, per device
+
+}  // namespace
+
+extern "C" int32_t rpba_float_sequential_sum_noalloc(const float *d_v, int64_t n, float *d_out, void *stream) {
+  if (!d_out || n < 0 || (n > 0 && !d_v)) return RPBA_ERR_ARG;
+  if (n > NA_MAX_N) return RPBA_ERR_TOO_LARGE;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return RPBA_ERR_NO_DEVICE;
+  if (dev < 0 || dev >= NA_MAX_DEVICES) return RPBA_ERR_UNSUPPORTED;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned char *base;
+  {
+    // set-up, once per device, with that device current: the array's name
+    // is only a host-side stand-in, so its device address is looked up
+    std::lock_guard<std::mutex> lock(g_na_mutex);
+    if (!g_na_addr[dev]) {
+      void *p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return RPBA_ERR_CUDA;
+      g_na_addr[dev] = (unsigned char *)p;
+    }
+    base = g_na_addr[dev];
+  }
+  const int ni = (int)n;
+  if (ni <= 4 * HEAD) {
+    k_warp_sum<<<1, 32, 0, s>>>(d_v, ni, d_out);
+    return cudaGetLastError() == cudaSuccess ? RPBA_OK : RPBA_ERR_CUDA;
+  }
+  const int G = (ni + NA_CHUNK - 1) / NA_CHUNK;
+  int nsm = 0, per = 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_exact_sum, ES_T, 0) != cudaSuccess)
+    return RPBA_ERR_CUDA;
+  if (G > nsm * per) return RPBA_ERR_TOO_LARGE;  // the CTAs would not all be resident
+  EsArgs A;
+  A.v = d_v;
+  A.n = ni;
+  A.out = d_out;
+  A.Rc = (long long *)(base + NA_OFF_RC);
+  A.Mc = (long long *)(base + NA_OFF_MC);
+  A.Tc = (int *)(base + NA_OFF_TC);
+  A.ctl = (EsCtl *)(base + NA_OFF_CTL);
+  A.bar = (unsigned *)(base + NA_OFF_BAR);
+  A.err = (int *)(base + NA_OFF_ERR);
+  // the array keeps the previous call's contents: the barrier counters and
+  // the error word must start at zero; the rest is written before it is read
+  if (cudaMemsetAsync(A.bar, 0, 2 * sizeof(unsigned), s) != cudaSuccess ||
+      cudaMemsetAsync(A.err, 0, sizeof(int), s) != cudaSuccess)
+    return RPBA_ERR_CUDA;
+  void *args[] = {&A};
+  if (cudaLaunchCooperativeKernel((const void *)k_exact_sum, dim3(G), dim3(ES_T), args, 0, s) != cudaSuccess)
+    return RPBA_ERR_CUDA;
+  return RPBA_OK;
+}

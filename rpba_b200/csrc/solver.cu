@@ -805,6 +805,7 @@ const char *rpba_status_string(int32_t st) {
     case RPBA_ERR_UNSUPPORTED: return "unsupported input";
     case RPBA_ERR_NO_DEVICE: return "no CUDA device";
     case RPBA_ERR_SOLVER: return "direct solve failed";
+    case RPBA_ERR_TOO_LARGE: return "input exceeds the fixed scratch of an allocation-free call";
     default: return "unknown status";
   }
 }

@@ -28,13 +28,14 @@ LIB_PATH = os.path.join(_HERE, "librpba_b200.so")
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no observations in image",
           4: "low redundancy", 5: "NaN step", 6: "device timeout", 7: "I/O error",
-          8: "unsupported input", 9: "no CUDA device", 10: "direct solve failed"}
+          8: "unsupported input", 9: "no CUDA device", 10: "direct solve failed",
+          11: "input too large for an allocation-free call"}
 
 # Every entry point include/rpba_b200.h declares.
 EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block_free",
            "rpba_output_block", "rpba_calc_plsa", "rpba_create", "rpba_solve",
            "rpba_get_state", "rpba_get_log", "rpba_exteval", "rpba_kernel_stats", "rpba_float_sequential_sum",
-           "rpba_destroy")
+           "rpba_float_sequential_sum_noalloc", "rpba_destroy")
 
 _lib = None
 
@@ -77,6 +78,8 @@ def load():
     L.rpba_float_sequential_sum.argtypes = [C.POINTER(C.c_float), C.c_int64, C.c_int32,
                                             C.POINTER(C.c_float)]
     L.rpba_float_sequential_sum.restype = C.c_int32
+    L.rpba_float_sequential_sum_noalloc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+    L.rpba_float_sequential_sum_noalloc.restype = C.c_int32
     L.rpba_kernel_stats.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     L.rpba_kernel_stats.restype = C.c_int32
     L.rpba_destroy.argtypes = [C.c_void_p]
