@@ -100,6 +100,17 @@ struct ExactSumWork {
 int exact_sum_max_grid(int device);
 void launch_exact_sum(const float *v, int n, float *out, const ExactSumWork &W, cudaStream_t s);
 
+// ---- dense direct solve (direct.cu)
+struct DirectWork {
+  int n;          // unknowns of the reduced camera system
+  double *A;      // n x n
+  double *Linv;   // ceil(n / 64) tiles of 64 x 64
+  double *y;      // n
+  int *coff;      // [nimg + 1] compact parameter offsets
+};
+size_t direct_bytes(int n);
+void direct_solve(const DevLSA &L, const DirectWork &W, double *xsol, cudaStream_t s);
+
 // ---- PCG (pcg.cu)
 struct PcgWork {
   double *r, *r1, *d, *q, *h, *h1, *x, *xbest, *Cinv, *partials, *part;

@@ -192,6 +192,7 @@ struct rpba_handle {
   StructWork S{};
   PcgWork W{};
   ExactSumWork ES{};
+  DirectWork DW{};
   int blocks_cap = 0;
   cudaEvent_t ev0, ev1;
 
@@ -224,6 +225,21 @@ struct rpba_handle {
     S.item_meta = dalloc<int4>(items, owned);
     W.part = dalloc<double>(items * 9, owned);
     blocks_cap = cap;
+  }
+
+  // dense direct-solve buffers, allocated on first use
+  void ensure_direct() {
+    if (DW.A) return;
+    std::vector<int> coff(nimg + 1, 0);
+    for (int k = 0; k < nimg; ++k) coff[k + 1] = coff[k] + (k >= begini ? camparv[k + 1] - camparv[k] : 0);
+    for (int k = 0; k < begini; ++k) coff[k] = 0;
+    const int n = coff[nimg];
+    DW.n = n;
+    DW.A = dalloc<double>((size_t)n * n, owned);
+    DW.Linv = dalloc<double>((size_t)((n + 63) / 64) * 64 * 64, owned);
+    DW.y = dalloc<double>(n, owned);
+    DW.coff = dalloc<int>(nimg + 1, owned);
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(DW.coff, coff.data(), sizeof(int) * (nimg + 1), cudaMemcpyHostToDevice, s));
   }
 
   float seq_sum(const float *v, int n) {
@@ -601,8 +617,13 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
   for (int k = begini; k < nimg; ++k) msize += camparv[k + 1] - camparv[k];
   if (msize < 1000) msize = 1000;
   if (opt.pcg_max_iterations > 0) msize = opt.pcg_max_iterations;
-  PROF("pcg", 2, pcg_solve(L, W, msize, pcg_grid, s));
-  pcg_pending = true;
+  if (opt.solver == RPBA_SOLVER_DIRECT) {
+    ensure_direct();
+    PROF("direct", 1, direct_solve(L, DW, W.xbest, s));
+  } else {
+    PROF("pcg", 2, pcg_solve(L, W, msize, pcg_grid, s));
+    pcg_pending = true;
+  }
   PROF("backsub", 1, launch_backsub(L, W.xbest, s));
   PROF("xcam", 1, launch_xcam(L, W.xbest, s));
   PROF("update", 1, launch_update(L, nrunknowns, s));
@@ -733,6 +754,7 @@ int rpba_handle::adjust() {
       }
       pcg_pending = false;
       if (hv.err & 2) return RPBA_ERR_DEVICE_TIMEOUT;
+      if (hv.err & 4) return RPBA_ERR_SOLVER;
       if (hv.err & 1) return RPBA_ERR_NAN_STEP;
       float sig0 = hv.sig0 * wsumg / (float)redundancy;
       if (sig0old < sig0 * sig0frac) --iflag;

@@ -154,32 +154,49 @@ def _track_lengths(rng, n, mean, lo, hi):
     return np.minimum(t, hi)
 
 
+def _chunk_tracks(job):
+    """Tracks of the points [s, e): proposals, visibility, selection.  Each
+    chunk draws from its own seed, so the result does not depend on how the
+    chunks are spread over processes."""
+    s, e, seed, props, vis_fn, t_want, n_c = job
+    rng = np.random.default_rng(seed)
+    prop = props(rng, s, e)
+    n, K = prop.shape
+    pt = np.repeat(np.arange(s, e), K)
+    vis = vis_fn(prop.ravel(), pt).reshape(n, K)
+    take = _select_tracks(rng, prop, vis, t_want[s:e])
+    cnt = take.sum(1)
+    take &= (cnt >= 2)[:, None]
+    rows, cols = np.nonzero(take)
+    c = prop[rows, cols]
+    # cameras ascending within a track
+    key = (rows + s).astype(np.int64) * (n_c + 1) + c
+    o = np.argsort(key, kind="stable")
+    return c[o].astype(np.int32), (rows[o] + s).astype(np.int32)
+
+
 def _assemble(rng, R_true, C_true, f_true, k_true, X_true, props, vis_fn, t_want,
               noise=0.5, outlier_frac=0.03, outlier_px=50.0, rot_pert=0.01,
-              t_pert=0.05, pt_pert=0.05, f_pert=0.02, chunk=200_000):
+              t_pert=0.05, pt_pert=0.05, f_pert=0.02, chunk=200_000, workers=None):
     """Build a BAL problem from proposals; drops points seen < 2 times."""
     n_c = R_true.shape[0]
     t_true = -np.einsum("nij,nj->ni", R_true, C_true)
-    cams, pts = [], []
-    for s in range(0, X_true.shape[0], chunk):
-        e = min(s + chunk, X_true.shape[0])
-        prop = props(s, e)
-        n, K = prop.shape
-        pt = np.repeat(np.arange(s, e), K)
-        vis = vis_fn(prop.ravel(), pt).reshape(n, K)
-        take = _select_tracks(rng, prop, vis, t_want[s:e])
-        cnt = take.sum(1)
-        ok = cnt >= 2
-        take &= ok[:, None]
-        rows, cols = np.nonzero(take)
-        c = prop[rows, cols]
-        # cameras ascending within a track
-        key = (rows + s).astype(np.int64) * (n_c + 1) + c
-        o = np.argsort(key, kind="stable")
-        cams.append(c[o].astype(np.int32))
-        pts.append((rows[o] + s).astype(np.int32))
-    obs_cam = np.concatenate(cams)
-    obs_pt = np.concatenate(pts)
+    n_p = X_true.shape[0]
+    base = int(rng.integers(0, 2**62))
+    jobs = [(s, min(s + chunk, n_p), base + s, props, vis_fn, t_want, n_c) for s in range(0, n_p, chunk)]
+    if workers is None:
+        import os
+        workers = min(len(jobs), os.cpu_count() or 1, 32) if n_p > 1_000_000 else 1
+    if workers > 1:
+        # spawn (not fork): callers may already hold a CUDA context
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+            res = list(ex.map(_chunk_tracks, jobs))
+    else:
+        res = [_chunk_tracks(j) for j in jobs]
+    obs_cam = np.concatenate([r[0] for r in res])
+    obs_pt = np.concatenate([r[1] for r in res])
     # re-index points seen >= 2 times
     used = np.unique(obs_pt)
     remap = -np.ones(X_true.shape[0], np.int64)
@@ -204,17 +221,67 @@ def _assemble(rng, R_true, C_true, f_true, k_true, X_true, props, vis_fn, t_want
                xy.astype(np.float32))
 
 
-def _vis(R, t, f, k, X, max_p, min_depth):
-    tt = t
+class _Vis:
+    """Visibility: in front of the camera and inside the image."""
 
-    def fn(cam, pt):
+    def __init__(self, R, t, f, k, X, max_p, min_depth):
+        self.a = (R, t, f, k, X)
+        self.max_p, self.min_depth = max_p, min_depth
+
+    def __call__(self, cam, pt):
         out = np.zeros(cam.size, bool)
         for s in range(0, cam.size, 2_000_000):
             e = min(s + 2_000_000, cam.size)
-            _, pz, pinf = project(R, tt, f, k, X, cam[s:e], pt[s:e])
-            out[s:e] = (pz < -min_depth) & (pinf < max_p)
+            _, pz, pinf = project(*self.a, cam[s:e], pt[s:e])
+            out[s:e] = (pz < -self.min_depth) & (pinf < self.max_p)
         return out
-    return fn
+
+
+class _ArcProps:
+    def __init__(self, n_cams, K):
+        self.n_cams, self.K = n_cams, K
+
+    def __call__(self, rng, s, e):
+        return np.argsort(rng.random((e - s, self.n_cams)), axis=1)[:, :self.K].astype(np.int64)
+
+
+class _StreetProps:
+    def __init__(self, xp, lo, hi, spacing, n_cams, K):
+        self.xp, self.lo, self.hi, self.spacing, self.n_cams, self.K = xp, lo, hi, spacing, n_cams, K
+
+    def __call__(self, rng, s, e):
+        i_hi = np.floor((self.xp[s:e] - self.lo) / self.spacing).astype(np.int64)
+        span = int(np.ceil((self.hi - self.lo) / self.spacing))
+        off = rng.integers(0, span, size=(e - s, self.K))
+        return np.clip(i_hi[:, None] - off, 0, self.n_cams - 1)
+
+
+class _AerialProps:
+    def __init__(self, xz, x0, y0, spacing, nx, ny, K):
+        self.xz, self.x0, self.y0, self.spacing, self.nx, self.ny, self.K = xz, x0, y0, spacing, nx, ny, K
+
+    def __call__(self, rng, s, e):
+        ix = np.round((self.xz[s:e, 0] - self.x0) / self.spacing).astype(np.int64)
+        iy = np.round((self.xz[s:e, 1] - self.y0) / self.spacing).astype(np.int64)
+        dx = rng.integers(-2, 3, size=(e - s, self.K))
+        dy = rng.integers(-2, 3, size=(e - s, self.K))
+        cx = np.clip(ix[:, None] + dx, 0, self.nx - 1)
+        cy = np.clip(iy[:, None] + dy, 0, self.ny - 1)
+        return cy * self.nx + cx
+
+
+class _CityProps:
+    def __init__(self, pc, nbr_pad, is_inter, cpc, K):
+        self.pc, self.nbr_pad, self.is_inter, self.cpc, self.K = pc, nbr_pad, is_inter, cpc, K
+
+    def __call__(self, rng, s, e):
+        n, K = e - s, self.K
+        home = self.pc[s:e]
+        own = home[:, None] * self.cpc + rng.integers(0, self.cpc, (n, K))
+        other_c = self.nbr_pad[home, rng.integers(0, 8, n)]
+        oth = other_c[:, None] * self.cpc + rng.integers(0, self.cpc, (n, K))
+        use_oth = self.is_inter[s:e, None] & (rng.random((n, K)) < 0.3)
+        return np.where(use_oth, oth, own)
 
 
 def _intrinsics(rng, n, flo, fhi):
@@ -236,11 +303,8 @@ def arc_scene(seed=20260, n_cams=50, n_pts=8000, track_mean=4.0, track_max=12,
     X = rng.uniform(-box / 2, box / 2, (n_pts, 3))
     t_want = _track_lengths(rng, n_pts, track_mean, 2, min(track_max, n_cams))
     K = min(n_cams, 3 * track_max)
-
-    def props(s, e):
-        return np.argsort(rng.random((e - s, n_cams)), axis=1)[:, :K].astype(np.int64)
     t = -np.einsum("nij,nj->ni", R, C)
-    return _assemble(rng, R, C, f, k, X, props, _vis(R, t, f, k, X, 1.5, 0.5), t_want,
+    return _assemble(rng, R, C, f, k, X, _ArcProps(n_cams, K), _Vis(R, t, f, k, X, 1.5, 0.5), t_want,
                      outlier_frac=outlier_frac, noise=noise, **kw)
 
 
@@ -259,16 +323,9 @@ def street_scene(seed=20261, n_cams=1000, n_pts=190_000, spacing=3.0, track_mean
                   rng.uniform(-10, 10, n_pts)], 1)
     t_want = _track_lengths(rng, n_pts, track_mean, 2, track_max)
     K = 2 * track_max
-
-    def props(s, e):
-        xp = X[s:e, 0]
-        i_hi = np.floor((xp - lo) / spacing).astype(np.int64)
-        span = int(np.ceil((hi - lo) / spacing))
-        off = rng.integers(0, span, size=(e - s, K))
-        return np.clip(i_hi[:, None] - off, 0, n_cams - 1)
     t = -np.einsum("nij,nj->ni", R, C)
-    return _assemble(rng, R, C, f, k, X, props, _vis(R, t, f, k, X, 1.2, 3.0), t_want,
-                     outlier_frac=outlier_frac, **kw)
+    return _assemble(rng, R, C, f, k, X, _StreetProps(X[:, 0].copy(), lo, hi, spacing, n_cams, K),
+                     _Vis(R, t, f, k, X, 1.2, 3.0), t_want, outlier_frac=outlier_frac, **kw)
 
 
 def _height(x, y):
@@ -294,19 +351,9 @@ def aerial_scene(seed=20262, nx=60, ny=50, n_pts=310_000, track_mean=5.3, track_
     X = np.stack([px, _height(px, pz), pz], 1)
     t_want = _track_lengths(rng, n_pts, track_mean, 2, track_max)
     K = 2 * track_max
-    x0, y0 = gx.min(), gy.min()
-
-    def props(s, e):
-        ix = np.round((X[s:e, 0] - x0) / spacing).astype(np.int64)
-        iy = np.round((X[s:e, 2] - y0) / spacing).astype(np.int64)
-        dx = rng.integers(-2, 3, size=(e - s, K))
-        dy = rng.integers(-2, 3, size=(e - s, K))
-        cx = np.clip(ix[:, None] + dx, 0, nx - 1)
-        cy = np.clip(iy[:, None] + dy, 0, ny - 1)
-        return cy * nx + cx
     t = -np.einsum("nij,nj->ni", R, C)
-    return _assemble(rng, R, C, f, k, X, props, _vis(R, t, f, k, X, 0.45, 10.0), t_want,
-                     outlier_frac=outlier_frac, **kw)
+    return _assemble(rng, R, C, f, k, X, _AerialProps(X[:, [0, 2]].copy(), gx.min(), gy.min(), spacing, nx, ny, K),
+                     _Vis(R, t, f, k, X, 0.45, 10.0), t_want, outlier_frac=outlier_frac, **kw)
 
 
 def city_scene(seed=20263, n_clusters=50, cams_per_cluster=274, n_pts=4_500_000,
@@ -336,18 +383,9 @@ def city_scene(seed=20263, n_clusters=50, cams_per_cluster=274, n_pts=4_500_000,
         nbr.append(cand)
     nbr_pad = np.array([(n + n * 8)[:8] for n in nbr])
     is_inter = rng.random(n_pts) < inter
-
-    def props(s, e):
-        n = e - s
-        home = pc[s:e]
-        own = home[:, None] * cams_per_cluster + rng.integers(0, cams_per_cluster, (n, K))
-        other_c = nbr_pad[home, rng.integers(0, 8, n)]
-        oth = other_c[:, None] * cams_per_cluster + rng.integers(0, cams_per_cluster, (n, K))
-        use_oth = is_inter[s:e, None] & (rng.random((n, K)) < 0.3)
-        return np.where(use_oth, oth, own)
     t = -np.einsum("nij,nj->ni", R, C)
-    return _assemble(rng, R, C, f, k, X, props, _vis(R, t, f, k, X, 1.0, 2.0), t_want,
-                     outlier_frac=outlier_frac, chunk=100_000, **kw)
+    return _assemble(rng, R, C, f, k, X, _CityProps(pc, nbr_pad, is_inter, cams_per_cluster, K),
+                     _Vis(R, t, f, k, X, 1.0, 2.0), t_want, outlier_frac=outlier_frac, chunk=100_000, **kw)
 
 
 def batch_scenes(seed=20264, n_scenes=256, cmin=20, cmax=400, pts_per_cam=150):

@@ -16,7 +16,8 @@ def _run_pair(oracle_mod, blk, **kw):
     blk_g = blk.copy()
     addflags = (kw.get("k2", True), kw.get("k4", True), kw.get("f", True))
     st_g, log_g, rep_g = rb.CalcPLSA(blk_g, robust=kw.get("robust", True), addflags=addflags,
-                                     max_lm_iterations=kw.get("max_lm_iterations", -1))
+                                     max_lm_iterations=kw.get("max_lm_iterations", -1),
+                                     solver=kw.get("solver", rb.SOLVER_PCG))
     return (st_o, blk_o, rep_o, log_o), (st_g, blk_g, rep_g, log_g)
 
 
@@ -92,6 +93,16 @@ def test_parity_variants(oracle_mod, kw):
 
 def test_parity_fixed_iterations(oracle_mod, arc_block):
     o, g = _run_pair(oracle_mod, arc_block, max_lm_iterations=3)
+    _check(o, g)
+
+
+@pytest.mark.parametrize("scene", ["arc", "street"])
+def test_parity_direct_strict(oracle_mod, arc_block, street_small, scene):
+    """Dense Cholesky on both sides: no inexact-PCG amplification, so the
+    contract's bars hold without any allowance (cost 1e-8, parameters 1e-6)."""
+    import rpba_b200 as rb
+    blk = arc_block if scene == "arc" else street_small
+    o, g = _run_pair(oracle_mod, blk, solver=rb.SOLVER_DIRECT)
     _check(o, g)
 
 
