@@ -181,6 +181,69 @@ int32_t rpba_exteval(rpba_handle *h, double *resid, rpba_report *rep);
  * exposed for verification. */
 int32_t rpba_float_sequential_sum(const float *v, int64_t n, int32_t device, float *out);
 
+/* ---- learned block-Jacobi correction (RPBA_SOLVER_LEARNED) ----
+ * The reference preconditions its PCG with the inverse diagonal blocks of
+ * the reduced camera system (rbacore.cpp:1841).  The learned form scales
+ * each block's inverse per parameter, C_k = diag(s) S_kk^-1 diag(s), with s
+ * from a 2-layer network (19 -> 64 tanh -> 9) over scale-free features of
+ * the assembled system; weights are BF16-rounded for inference. */
+#define RPBA_PRECOND_WEIGHTS 1865 /* W1[64][19], b1[64], W2[9][64], b2[9] */
+
+typedef struct rpba_train_options {
+  int32_t steps;        /* Adam steps (0: 300)                           */
+  int32_t batch;        /* unused: every step uses the whole set         */
+  float lr;             /* learning rate (0: 3e-3)                       */
+  int32_t probes;       /* random right-hand sides per system besides the
+                           LM step's own                                 */
+  int32_t max_samples;  /* block-row capacity of the training set (0: 2^18) */
+  uint64_t seed;
+} rpba_train_options;
+
+typedef struct rpba_train_report {
+  int32_t samples;      /* block rows in the training set                */
+  int32_t steps;
+  float loss_initial;   /* mean of ln(u^T S u) - 2 ln(b^T u), untrained (s = 1) */
+  float loss_final;
+  int32_t systems;      /* recorded reduced camera systems              */
+  float err_initial;    /* mean relative A-norm error after one
+                           preconditioned step on the LM right-hand sides */
+  float err_final;
+} rpba_train_report;
+
+/* Train the preconditioner network on the reduced camera systems that the
+ * direct solver's own LM iterations assemble on the given scenes (solved with
+ * *opt, solver forced to DIRECT).  Objective: the relative A-norm error left
+ * after one preconditioned step, over the LM right-hand sides and random
+ * ones.  weights receives RPBA_PRECOND_WEIGHTS floats.  No counterpart in the
+ * reference. */
+int32_t rpba_train_preconditioner(const rpba_block *scenes, int32_t nscenes, const rpba_options *opt,
+                                  const rpba_train_options *topt, float *weights,
+                                  rpba_train_report *rep);
+/* Use these weights in the handle's RPBA_SOLVER_LEARNED solves (NULL: plain
+ * block-Jacobi under the same stopping rule).  n = RPBA_PRECOND_WEIGHTS.
+ * No counterpart in the reference. */
+int32_t rpba_set_preconditioner(rpba_handle *h, const float *weights, int32_t n);
+
+/* A training set in host memory (diagonally scaled, block-diagonal union of
+ * systems) for rpba_precond_loss_grad. */
+typedef struct rpba_precond_set {
+  int32_t rows, systems, probes, nent, nblocks;
+  const float *features;   /* [rows][19]                                  */
+  const float *sinv;       /* [rows][81] D^1/2 S_kk^-1 D^1/2             */
+  const float *b;          /* [probes][rows][9]                           */
+  const float *xs;         /* [rows][9] solution of right-hand side 0     */
+  const int32_t *np, *sys; /* [rows] parameter count, system index        */
+  const int32_t *rowoff;   /* [rows + 1]                                  */
+  const int32_t *ent_col;  /* [nent] column row                           */
+  const int32_t *ent_blk;  /* [nent] block index, bit 31: transposed      */
+  const float *blocks;     /* [nblocks][81] D^-1/2 S D^-1/2               */
+  const int32_t *sys_row;  /* [systems + 1]                               */
+} rpba_precond_set;
+/* Training loss and its gradient for `weights`, computed by the GPU's
+ * training kernels (for checking against an independent implementation).
+ * No counterpart in the reference. */
+int32_t rpba_precond_loss_grad(const rpba_precond_set *set, const float *weights, float *loss, float *grad);
+
 /* Allocation-free form of rpba_float_sequential_sum, for callers that must
  * not have a library call cudaMalloc or cudaFree -- an application that hands
  * out all device memory from its own fixed-budget pool, or a latency-critical

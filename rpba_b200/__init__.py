@@ -5,12 +5,13 @@ hand-written sm_100a CUDA behind a C ABI (include/rpba_b200.h).  This
 package is the Python side of that ABI (``lib``), the block container
 (``block``) and seeded synthetic scenes (``scenes``).
 """
-from .block import (Block, RpbaBlockC, RpbaOptionsC, RpbaReportC, make_options,
+from .block import (Block, RpbaBlockC, RpbaOptionsC, RpbaReportC, make_options, PRECOND_WEIGHTS,
                     SOLVER_PCG, SOLVER_DIRECT, SOLVER_LEARNED, PREC_FP64, PREC_MIXED)
 from .lib import (InputBlock, OutputBlock, CalcPLSA, Solver, RpbaError, load, LIB_PATH,
-                  EXPORTS, STATUS, float_sequential_sum)
+                  EXPORTS, STATUS, float_sequential_sum, train_preconditioner,
+                  precond_loss_grad)
 
-__all__ = ["Block", "RpbaBlockC", "RpbaOptionsC", "RpbaReportC", "make_options", "SOLVER_PCG",
+__all__ = ["Block", "RpbaBlockC", "RpbaOptionsC", "RpbaReportC", "make_options", "PRECOND_WEIGHTS", "SOLVER_PCG",
            "SOLVER_DIRECT", "SOLVER_LEARNED", "PREC_FP64", "PREC_MIXED", "InputBlock",
            "OutputBlock", "CalcPLSA", "Solver", "RpbaError", "load", "LIB_PATH", "EXPORTS",
-           "STATUS", "float_sequential_sum"]
+           "STATUS", "float_sequential_sum", "train_preconditioner", "precond_loss_grad"]

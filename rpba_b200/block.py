@@ -86,6 +86,25 @@ class RpbaReportC(C.Structure):
         return out
 
 
+class RpbaTrainOptionsC(C.Structure):
+    _fields_ = [("steps", C.c_int32), ("batch", C.c_int32), ("lr", C.c_float), ("probes", C.c_int32),
+                ("max_samples", C.c_int32), ("seed", C.c_uint64)]
+
+
+class RpbaTrainReportC(C.Structure):
+    _fields_ = [("samples", C.c_int32), ("steps", C.c_int32), ("loss_initial", C.c_float),
+                ("loss_final", C.c_float), ("systems", C.c_int32), ("err_initial", C.c_float),
+                ("err_final", C.c_float)]
+
+
+class RpbaPrecondSetC(C.Structure):
+    _fields_ = [("rows", C.c_int32), ("systems", C.c_int32), ("probes", C.c_int32), ("nent", C.c_int32),
+                ("nblocks", C.c_int32), ("features", _f32p), ("sinv", _f32p), ("b", _f32p), ("xs", _f32p),
+                ("np", _i32p), ("sys", _i32p), ("rowoff", _i32p), ("ent_col", _i32p), ("ent_blk", _i32p),
+                ("blocks", _f32p), ("sys_row", _i32p)]
+
+
+PRECOND_WEIGHTS = 1865
 SOLVER_PCG, SOLVER_DIRECT, SOLVER_LEARNED = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 

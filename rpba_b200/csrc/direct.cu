@@ -59,6 +59,13 @@ __global__ void k_gather_rhs(DevLSA L, const int *coff, double *y) {
   for (int a = 0; a < np; ++a) y[coff[k] + a] = L.rhs[(size_t)k * 9 + a];
 }
 
+__global__ void k_gather_vec(DevLSA L, const int *coff, const double *b, double *y) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x + L.begini;
+  if (k >= L.nimg) return;
+  const int np = L.camparv[k + 1] - L.camparv[k];
+  for (int a = 0; a < np; ++a) y[coff[k] + a] = b[(size_t)k * 9 + a];
+}
+
 __global__ void k_scatter_solution(DevLSA L, const int *coff, const double *y, double *xsol) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= L.nimg) return;
@@ -231,9 +238,10 @@ __global__ void k_panel_update(const double *A, int n, int j0, int tb, double *y
 
 size_t direct_bytes(int n) { return (size_t)n * n * sizeof(double); }
 
-// Solve S x = b for the reduced camera system; x in xsol (padded 9 per
-// camera).  Returns 0 or RPBA_ERR_SOLVER-like error bits in L.err (bit 3).
-void direct_solve(const DevLSA &L, const DirectWork &W, double *xsol, cudaStream_t s) {
+// Factor S = L L^T (kept in W.A / W.Linv) and solve S x = b for the
+// reduced camera system; x in xsol (padded 9 per camera).  A non-positive
+// pivot sets L.err bit 4.
+void direct_factor(const DevLSA &L, const DirectWork &W, cudaStream_t s) {
   const int n = W.n;
   if (n <= 0) return;
   RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
@@ -245,7 +253,6 @@ void direct_solve(const DevLSA &L, const DirectWork &W, double *xsol, cudaStream
     k_dense_fill<<<(int)((nd + 255) / 256), 256, 0, s>>>(L, W.coff, n, W.A);
     k_dense_fill_off<<<(int)((nd + 255) / 256), 256, 0, s>>>(L, W.coff, n, W.A);
   }
-  k_gather_rhs<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W.coff, W.y);
   const int ntiles = (n + T - 1) / T;
   for (int jt = 0; jt < ntiles; ++jt) {
     const int j0 = jt * T, tb = min(T, n - j0);
@@ -257,20 +264,35 @@ void direct_solve(const DevLSA &L, const DirectWork &W, double *xsol, cudaStream
       k_syrk<<<m * (m + 1) / 2, DT, SMEM2, s>>>(W.A, n, j0, tb, m);
     }
   }
-  // forward: L y = b
+}
+
+// x = S^-1 b with the factor from direct_factor; b and x padded 9 per camera
+// (b == nullptr: the assembled right-hand side L.rhs).
+void direct_resolve(const DevLSA &L, const DirectWork &W, const double *b, double *xsol, cudaStream_t s) {
+  const int n = W.n;
+  if (n <= 0) return;
+  if (b)
+    k_gather_vec<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W.coff, b, W.y);
+  else
+    k_gather_rhs<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W.coff, W.y);
+  const int ntiles = (n + T - 1) / T;
   for (int jt = 0; jt < ntiles; ++jt) {
     const int j0 = jt * T, tb = min(T, n - j0);
     k_tile_solve<<<1, T, 0, s>>>(W.Linv + (size_t)jt * T * T, tb, W.y, j0, 0);
     const int rows = n - j0 - tb;
     if (rows > 0) k_panel_update<<<(rows * 32 + 255) / 256, 256, 0, s>>>(W.A, n, j0, tb, W.y, 0);
   }
-  // backward: L^T x = y
   for (int jt = ntiles - 1; jt >= 0; --jt) {
     const int j0 = jt * T, tb = min(T, n - j0);
     k_tile_solve<<<1, T, 0, s>>>(W.Linv + (size_t)jt * T * T, tb, W.y, j0, 1);
     if (j0 > 0) k_panel_update<<<(j0 * 32 + 255) / 256, 256, 0, s>>>(W.A, n, j0, tb, W.y, 1);
   }
   k_scatter_solution<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W.coff, W.y, xsol);
+}
+
+void direct_solve(const DevLSA &L, const DirectWork &W, double *xsol, cudaStream_t s) {
+  direct_factor(L, W, s);
+  direct_resolve(L, W, nullptr, xsol, s);
 }
 
 }  // namespace rpba

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace rpba {
@@ -110,6 +112,41 @@ struct DirectWork {
 };
 size_t direct_bytes(int n);
 void direct_solve(const DevLSA &L, const DirectWork &W, double *xsol, cudaStream_t s);
+void direct_factor(const DevLSA &L, const DirectWork &W, cudaStream_t s);
+void direct_resolve(const DevLSA &L, const DirectWork &W, const double *b, double *xsol, cudaStream_t s);
+
+// ---- learned preconditioner (learned.cu)
+constexpr int NN_F = 19, NN_H = 64, NN_O = 9;
+constexpr int NN_WEIGHTS = NN_H * NN_F + NN_H + NN_O * NN_H + NN_O;  // 1865
+// Training set: recorded reduced camera systems, diagonally scaled and
+// concatenated into one block-diagonal system (device arrays).
+struct TrainSet {
+  int rows, rows_cap, systems, probes;
+  float *f;          // [rows_cap][NN_F]
+  float *sinv;       // [rows_cap][81]  D^1/2 S_kk^-1 D^1/2
+  float *b;          // [probes][rows_cap][9] right-hand sides (D^-1/2 b)
+  float *xs;         // [rows_cap][9]   D^1/2 x* of right-hand side 0
+  int *np, *sys;     // [rows_cap]
+  int *rowoff;       // [rows_cap + 1]
+  int2 *ent;         // (row, block | 0x80000000 if transposed)
+  float *blocks;     // [.][81]        D^-1/2 S D^-1/2
+  int *sys_row;      // [systems + 1]
+};
+struct TrainHost {  // host-side capacities and fill levels
+  int ents, ents_cap, blocks, blocks_cap, sys_cap;
+  int2 *rc;  // device scratch: (row, col) of a system's off-diagonal blocks
+  std::vector<int> sys_row;
+};
+struct TrainBufs {
+  float *sv, *ov, *hv, *u, *v, *d2, *d1, *grad;
+  double *pq;
+};
+struct PcgWork;
+void learned_pcg_setup(const DevLSA &L, const PcgWork &W, const float *weights, cudaStream_t s);
+void learned_record(const DevLSA &L, const DirectWork &DW, const double *xstar, unsigned long long seed,
+                    TrainSet &T, TrainHost &H, cudaStream_t s);
+void learned_loss_grad(const TrainSet &T, const float *W, TrainBufs &B, float *loss, float *err, cudaStream_t s);
+void learned_adam(float *W, float *m, float *v, const float *grad, float lr, int t, cudaStream_t s);
 
 // ---- PCG (pcg.cu)
 struct PcgWork {
@@ -117,7 +154,11 @@ struct PcgWork {
   unsigned *bar;
   int *iters;
 };
-int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s);
+// mode 0: the reference's stop rule; mode 1: stop when r^T M^-1 r falls
+// below tol^2 times its start value (W.iters[1] = 1 when it did), with the
+// learned preconditioner `weights` (nullptr: plain block-Jacobi).
+int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s, int mode = 0,
+              double tol = 0., const float *weights = nullptr);
 int pcg_max_grid(int device);
 
 // ---- structure (structure.cu)

@@ -37,6 +37,8 @@ struct PcgArgs {
   int *err;
   int *iters;
   int row0, row1, nitems, msize;
+  int mode;     // 0: reference stop rule; 1: relative preconditioned residual
+  double tol2;  // mode 1: stop when r^T M^-1 r <= tol2 * (r0^T M^-1 r0)
 };
 
 // Deterministic CTA sum of up to three values; valid in every thread.
@@ -118,6 +120,8 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
     erthk = v[0];
   }
   double meandrold = 1.e50, meandr0 = 1.e50, beta_prev = 0.;
+  const double erthk0 = erthk;
+  bool converged = false;
   int k;
   for (k = 0; k < A.msize; ++k) {
     const double *dprev = (k & 1) ? A.D0 : A.D1;
@@ -241,19 +245,28 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
     grid_sum<3>(A.red2, G, g3, sh);
     const double meandr = g3[0], er1th1 = g3[1];
     if (k == 0) meandr0 = meandr;
-    const bool improved = meandr < meandrold;
+    // mode 0 keeps the iterate with the smallest increment (the reference's
+    // exivold); mode 1 keeps the latest
+    const bool improved = A.mode == 1 || meandr < meandrold;
     if (improved) {
       meandrold = meandr;
       for (int row = A.row0 + gwarp; row < A.row1; row += nwarps)
         if (lane < 9) A.xbest[(size_t)row * 9 + lane] = A.x[(size_t)row * 9 + lane];
     }
-    if (meandr * 1.e5 < meandr0) break;
+    if (A.mode == 0 && meandr * 1.e5 < meandr0) break;
+    if (A.mode == 1 && !(g3[2] > A.tol2 * erthk0)) {
+      converged = true;
+      break;
+    }
     double beta = fabs(er1th1) < 1.e-10 ? 0. : er1th1 / erthk;
     if (beta < 0.) beta = 0.;
     beta_prev = beta;
     erthk = g3[2];
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) *A.iters = k < A.msize ? k + 1 : A.msize;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    A.iters[0] = k < A.msize ? k + 1 : A.msize;
+    A.iters[1] = converged ? 1 : 0;
+  }
 }
 
 // Preconditioner C_k = S_kk^-1 (rbacore.cpp:1839-1846) and the start
@@ -294,8 +307,12 @@ int pcg_max_grid(int device) {
 
 // Returns 0; throws CudaError on launch errors.  The iteration count is
 // left in W.iters.
-int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s) {
-  k_pcg_setup<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W);
+int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s, int mode, double tol,
+              const float *weights) {
+  if (mode == 1 || weights)
+    learned_pcg_setup(L, W, weights, s);
+  else
+    k_pcg_setup<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W);
   RPBA_CUDA_CHECK(cudaGetLastError());
   const int nrows = L.nimg - L.begini;
   if (nrows <= 0) return 0;
@@ -325,6 +342,8 @@ int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream
   A.row1 = L.nimg;
   A.nitems = L.nitems;
   A.msize = msize;
+  A.mode = mode;
+  A.tol2 = tol * tol;
   RPBA_CUDA_CHECK(cudaMemsetAsync(W.bar, 0, 2 * sizeof(unsigned), s));
   void *args[] = {&A};
   RPBA_CUDA_CHECK(cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(g), dim3(PCG_T), args, 0, s));

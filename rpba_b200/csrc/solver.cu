@@ -167,7 +167,7 @@ struct rpba_handle {
   float ihw2 = 1.f;
   double defdiff = 5000.;
   std::vector<int> camparv;
-  long long max_pairs = 0, npairs_cur = 0;
+  long long max_pairs = 0, npairs_cur = 0, learned_iters = 0;
   int pcg_grid = 1;
   bool pcg_pending = false;
 
@@ -193,6 +193,12 @@ struct rpba_handle {
   PcgWork W{};
   ExactSumWork ES{};
   DirectWork DW{};
+  // learned preconditioner (device copy of the weights; nullptr: none)
+  float *d_weights = nullptr;
+  // training-data recording (set by rpba_train_preconditioner)
+  TrainSet *rec_T = nullptr;
+  TrainHost *rec_H = nullptr;
+  unsigned long long rec_seed = 1;
   int blocks_cap = 0;
   cudaEvent_t ev0, ev1;
 
@@ -552,7 +558,7 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   W.Cinv = dalloc<double>(81 * (size_t)n, own);
   W.partials = dalloc<double>(8 * (size_t)H->pcg_grid, own);
   W.bar = dalloc<unsigned>(2, own);
-  W.iters = dalloc<int>(1, own);
+  W.iters = dalloc<int>(2, own);
   RPBA_CUDA_CHECK(cudaMemsetAsync(W.r1, 0, sizeof(double) * nv, H->s));
   RPBA_CUDA_CHECK(cudaMemsetAsync(W.h1, 0, sizeof(double) * nv, H->s));
   RPBA_CUDA_CHECK(cudaMemsetAsync(W.q, 0, sizeof(double) * nv, H->s));
@@ -620,10 +626,29 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
   if (opt.solver == RPBA_SOLVER_DIRECT) {
     ensure_direct();
     PROF("direct", 1, direct_solve(L, DW, W.xbest, s));
+  } else if (opt.solver == RPBA_SOLVER_LEARNED) {
+    // PCG with the learned preconditioner.  Stop rule: the reference's
+    // (pcg_tolerance == 0) or a relative preconditioned residual; past the
+    // iteration cap the direct solve takes over
+    const int mode = opt.pcg_tolerance > 0. ? 1 : 0;
+    const int cap = opt.pcg_max_iterations > 0 ? opt.pcg_max_iterations : msize;
+    PROF("pcg", 2, pcg_solve(L, W, cap, pcg_grid, s, mode, opt.pcg_tolerance, d_weights));
+    int it[2] = {0, 0};
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(it, W.iters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+    RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+    learned_iters += it[0];
+    const bool ok = mode == 1 ? it[1] != 0 : it[0] < cap;
+    if (!ok) {
+      ++rep.pcg_fallbacks;
+      ensure_direct();
+      PROF("direct", 1, direct_solve(L, DW, W.xbest, s));
+    }
   } else {
     PROF("pcg", 2, pcg_solve(L, W, msize, pcg_grid, s));
     pcg_pending = true;
   }
+  if (rec_T)
+    learned_record(L, DW, W.xbest, rec_seed + 104729ull * (unsigned long long)rep.linear_solves, *rec_T, *rec_H, s);
   PROF("backsub", 1, launch_backsub(L, W.xbest, s));
   PROF("xcam", 1, launch_xcam(L, W.xbest, s));
   PROF("update", 1, launch_update(L, nrunknowns, s));
@@ -728,6 +753,7 @@ int rpba_handle::adjust() {
       }
       calc_bundle_sep(multfact, nrunknowns);
       ++solves;
+      rep.linear_solves = solves;
       PROF("decode", 1, launch_decode(L, L.XPMn, s));
       PROF("cost", 1, launch_cost(L, L.XPMn, true, s));
       PROF("seq_sum", 1, launch_exact_sum(L.o_cost, L.nobs, sums, ES, s));
@@ -740,7 +766,7 @@ int rpba_handle::adjust() {
       RPBA_CUDA_CHECK(cudaMemcpyAsync(&hv.err, L.err, sizeof(int), cudaMemcpyDeviceToHost, s));
       RPBA_CUDA_CHECK(cudaMemcpyAsync(&hv.iters, W.iters, sizeof(int), cudaMemcpyDeviceToHost, s));
       RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
-      rep.pcg_iterations += hv.iters;
+      rep.pcg_iterations += opt.solver == RPBA_SOLVER_PCG ? hv.iters : 0;
       if (prof.on && pcg_pending) {
         // per PCG iteration: blocks read from both sides (648 * (Nc + 2 Nb)),
         // block entries (8 each), per camera row the preconditioner (648) and
@@ -792,6 +818,7 @@ int rpba_handle::adjust() {
     if (robust && it == 0) robust_delete();
   }
   rep.linear_solves = solves;
+  if (opt.solver == RPBA_SOLVER_LEARNED) rep.pcg_iterations = learned_iters;
   return RPBA_OK;
 }
 
@@ -865,6 +892,7 @@ int32_t rpba_solve(rpba_handle *H, rpba_report *rep) {
     RPBA_CUDA_CHECK(cudaSetDevice(H->dev));
     H->log.clear();
     std::memset(&H->rep, 0, sizeof H->rep);
+    H->learned_iters = 0;
     H->prof.s = H->s;
     H->prof.on = (H->opt.verbose & 2) != 0;
     H->prof.reset();
@@ -1075,6 +1103,203 @@ int32_t rpba_float_sequential_sum(const float *v, int64_t n, int32_t device, flo
     RPBA_CUDA_CHECK(cudaMemcpy(a->out, dout, sizeof(float), cudaMemcpyDeviceToHost));
     RPBA_CUDA_CHECK(cudaMemcpy(&err, W.err, sizeof(int), cudaMemcpyDeviceToHost));
     return err ? (int)RPBA_ERR_DEVICE_TIMEOUT : (int)RPBA_OK;
+  }, &a);
+}
+
+int32_t rpba_set_preconditioner(rpba_handle *H, const float *weights, int32_t n) {
+  if (!H || H->opt.exteval) return RPBA_ERR_ARG;
+  if (weights && n != RPBA_PRECOND_WEIGHTS) return RPBA_ERR_ARG;
+  struct A {
+    rpba_handle *H;
+    const float *w;
+  } a{H, weights};
+  return guard([](void *p) {
+    A *a = (A *)p;
+    rpba_handle *H = a->H;
+    RPBA_CUDA_CHECK(cudaSetDevice(H->dev));
+    if (!a->w) {
+      H->d_weights = nullptr;
+      return (int)RPBA_OK;
+    }
+    static_assert(NN_WEIGHTS == RPBA_PRECOND_WEIGHTS, "weight count");
+    if (!H->d_weights) {
+      float *d = dalloc<float>(NN_WEIGHTS, H->owned);
+      H->d_weights = d;
+    }
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(H->d_weights, a->w, sizeof(float) * NN_WEIGHTS, cudaMemcpyHostToDevice, H->s));
+    RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
+    return (int)RPBA_OK;
+  }, &a);
+}
+
+namespace {
+
+// device training set with the given capacities
+struct TrainAlloc {
+  TrainSet T{};
+  TrainHost H{};
+  TrainBufs B{};
+  std::vector<void *> own;
+  ~TrainAlloc() {
+    for (void *q : own) cudaFree(q);
+  }
+  void alloc(int rows_cap, int ents_cap, int blocks_cap, int sys_cap, int probes) {
+    T.rows_cap = rows_cap;
+    T.probes = probes;
+    T.f = dalloc<float>((size_t)rows_cap * NN_F, own);
+    T.sinv = dalloc<float>((size_t)rows_cap * 81, own);
+    T.b = dalloc<float>((size_t)probes * rows_cap * 9, own);
+    T.xs = dalloc<float>((size_t)rows_cap * 9, own);
+    T.np = dalloc<int>(rows_cap, own);
+    T.sys = dalloc<int>(rows_cap, own);
+    T.rowoff = dalloc<int>((size_t)rows_cap + 1, own);
+    T.ent = dalloc<int2>(ents_cap, own);
+    T.blocks = dalloc<float>((size_t)blocks_cap * 81, own);
+    T.sys_row = dalloc<int>((size_t)sys_cap + 1, own);
+    H.ents_cap = ents_cap;
+    H.blocks_cap = blocks_cap;
+    H.sys_cap = sys_cap;
+    H.sys_row.assign(1, 0);
+  }
+  void bufs() {
+    const size_t R = T.rows, P = T.probes;
+    B.sv = dalloc<float>(R * NN_O, own);
+    B.ov = dalloc<float>(R * NN_O, own);
+    B.hv = dalloc<float>(R * NN_H, own);
+    B.u = dalloc<float>(P * R * 9, own);
+    B.v = dalloc<float>(P * R * 9, own);
+    B.d2 = dalloc<float>(R * NN_O, own);
+    B.d1 = dalloc<float>(R * NN_H, own);
+    B.grad = dalloc<float>(NN_WEIGHTS, own);
+    B.pq = dalloc<double>(3 * (size_t)T.systems * P, own);
+  }
+};
+
+}  // namespace
+
+int32_t rpba_precond_loss_grad(const rpba_precond_set *set, const float *weights, float *loss, float *grad) {
+  if (!set || !weights || !grad || set->rows <= 0 || set->systems <= 0 || set->probes <= 0) return RPBA_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return RPBA_ERR_NO_DEVICE;
+  struct A {
+    const rpba_precond_set *st;
+    const float *w;
+    float *loss, *grad;
+  } a{set, weights, loss, grad};
+  return guard([](void *p) {
+    A *a = (A *)p;
+    const rpba_precond_set &S = *a->st;
+    TrainAlloc TA;
+    TA.alloc(S.rows, std::max(S.nent, 1), std::max(S.nblocks, 1), S.systems, S.probes);
+    TrainSet &T = TA.T;
+    T.rows = S.rows;
+    T.systems = S.systems;
+    // a given set is laid out with rows_cap == rows
+    auto up = [](void *d, const void *h, size_t n) { RPBA_CUDA_CHECK(cudaMemcpy(d, h, n, cudaMemcpyHostToDevice)); };
+    up(T.f, S.features, sizeof(float) * S.rows * NN_F);
+    up(T.sinv, S.sinv, sizeof(float) * S.rows * 81);
+    up(T.b, S.b, sizeof(float) * (size_t)S.probes * S.rows * 9);
+    up(T.xs, S.xs, sizeof(float) * S.rows * 9);
+    up(T.np, S.np, sizeof(int) * S.rows);
+    up(T.sys, S.sys, sizeof(int) * S.rows);
+    up(T.rowoff, S.rowoff, sizeof(int) * (S.rows + 1));
+    std::vector<int2> ent(std::max(S.nent, 1));
+    for (int i = 0; i < S.nent; ++i) ent[i] = make_int2(S.ent_col[i], S.ent_blk[i]);
+    up(T.ent, ent.data(), sizeof(int2) * S.nent);
+    up(T.blocks, S.blocks, sizeof(float) * (size_t)S.nblocks * 81);
+    up(T.sys_row, S.sys_row, sizeof(int) * (S.systems + 1));
+    TA.bufs();
+    float *dw = dalloc<float>(NN_WEIGHTS, TA.own);
+    up(dw, a->w, sizeof(float) * NN_WEIGHTS);
+    float l = 0.f;
+    learned_loss_grad(T, dw, TA.B, &l, nullptr, 0);
+    RPBA_CUDA_CHECK(cudaMemcpy(a->grad, TA.B.grad, sizeof(float) * NN_WEIGHTS, cudaMemcpyDeviceToHost));
+    if (a->loss) *a->loss = l;
+    return (int)RPBA_OK;
+  }, &a);
+}
+
+int32_t rpba_train_preconditioner(const rpba_block *scenes, int32_t nscenes, const rpba_options *opt,
+                                  const rpba_train_options *topt, float *weights, rpba_train_report *rep) {
+  if (!scenes || nscenes <= 0 || !opt || !topt || !weights) return RPBA_ERR_ARG;
+  if (rep) std::memset(rep, 0, sizeof *rep);
+  struct A {
+    const rpba_block *sc;
+    int ns;
+    const rpba_options *o;
+    const rpba_train_options *t;
+    float *w;
+    rpba_train_report *rep;
+  } a{scenes, nscenes, opt, topt, weights, rep};
+  return guard([](void *p) {
+    A *a = (A *)p;
+    const rpba_train_options &t = *a->t;
+    RPBA_CUDA_CHECK(cudaSetDevice(a->o->device));
+    const int probes = 1 + std::max(0, t.probes);
+    const int rows_cap = t.max_samples > 0 ? t.max_samples : 1 << 18;
+    TrainAlloc TA;
+    TA.alloc(rows_cap, rows_cap * 96, rows_cap * 48, 4096, probes);
+    // 1. systems of the direct solver's own LM iterations
+    for (int i = 0; i < a->ns; ++i) {
+      rpba_options o = *a->o;
+      o.solver = RPBA_SOLVER_DIRECT;
+      o.exteval = 0;
+      rpba_handle *H = nullptr;
+      int st = rpba_create(&H, &a->sc[i], &o);
+      if (st != RPBA_OK) return st;
+      if (!TA.H.rc) TA.H.rc = dalloc<int2>((size_t)rows_cap * 48, TA.own);
+      H->rec_T = &TA.T;
+      H->rec_H = &TA.H;
+      H->rec_seed = t.seed * 1000003ull + (unsigned long long)i;
+      rpba_report r{};
+      st = rpba_solve(H, &r);
+      rpba_destroy(H);
+      if (st != RPBA_OK) return st;
+    }
+    TrainSet &T = TA.T;
+    if (T.systems <= 0) return (int)RPBA_ERR_ARG;
+    RPBA_CUDA_CHECK(cudaMemcpy(T.sys_row, TA.H.sys_row.data(), sizeof(int) * (T.systems + 1), cudaMemcpyHostToDevice));
+    TA.bufs();
+    // 2. Adam on the one-step objective
+    float *W = dalloc<float>(NN_WEIGHTS, TA.own), *m = dalloc<float>(NN_WEIGHTS, TA.own);
+    float *v = dalloc<float>(NN_WEIGHTS, TA.own);
+    std::vector<float> w0(NN_WEIGHTS, 0.f);
+    {
+      // W1 ~ U(-1/sqrt(F), 1/sqrt(F)), everything else 0: the untrained
+      // network gives s = 1, i.e. plain block-Jacobi
+      unsigned long long z = t.seed ^ 0x2545f4914f6cdd1dull;
+      for (int i = 0; i < NN_H * NN_F; ++i) {
+        z ^= z << 13;
+        z ^= z >> 7;
+        z ^= z << 17;
+        w0[i] = (float)(((double)(z >> 11) / 9007199254740992.0 * 2. - 1.) / std::sqrt((double)NN_F));
+      }
+    }
+    RPBA_CUDA_CHECK(cudaMemcpy(W, w0.data(), sizeof(float) * NN_WEIGHTS, cudaMemcpyHostToDevice));
+    RPBA_CUDA_CHECK(cudaMemset(m, 0, sizeof(float) * NN_WEIGHTS));
+    RPBA_CUDA_CHECK(cudaMemset(v, 0, sizeof(float) * NN_WEIGHTS));
+    float loss0 = 0.f, err0 = 0.f, loss1 = 0.f, err1 = 0.f;
+    learned_loss_grad(T, W, TA.B, &loss0, &err0, 0);
+    const int steps = t.steps > 0 ? t.steps : 300;
+    const float lr = t.lr > 0.f ? t.lr : 3e-3f;
+    for (int st = 0; st < steps; ++st) {
+      learned_loss_grad(T, W, TA.B, nullptr, nullptr, 0);
+      learned_adam(W, m, v, TA.B.grad, lr, st + 1, 0);
+    }
+    learned_loss_grad(T, W, TA.B, &loss1, &err1, 0);
+    std::vector<float> wout(NN_WEIGHTS);
+    RPBA_CUDA_CHECK(cudaMemcpy(wout.data(), W, sizeof(float) * NN_WEIGHTS, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < NN_WEIGHTS; ++i) a->w[i] = wout[i];
+    if (a->rep) {
+      a->rep->samples = T.rows;
+      a->rep->systems = T.systems;
+      a->rep->steps = steps;
+      a->rep->loss_initial = loss0;
+      a->rep->loss_final = loss1;
+      a->rep->err_initial = err0;
+      a->rep->err_final = err1;
+    }
+    return (int)RPBA_OK;
   }, &a);
 }
 

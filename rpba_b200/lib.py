@@ -20,8 +20,10 @@ import os
 
 import numpy as np
 
-from .block import (Block, RpbaBlockC, RpbaOptionsC, RpbaReportC, make_options,
-                    SOLVER_PCG, SOLVER_DIRECT, SOLVER_LEARNED, PREC_FP64, PREC_MIXED)
+from .block import (Block, RpbaBlockC, RpbaOptionsC, RpbaReportC, RpbaTrainOptionsC, RpbaTrainReportC,
+                    RpbaPrecondSetC,
+                    make_options, PRECOND_WEIGHTS, SOLVER_PCG, SOLVER_DIRECT, SOLVER_LEARNED, PREC_FP64,
+                    PREC_MIXED)
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "librpba_b200.so")
@@ -35,7 +37,8 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no observations i
 EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block_free",
            "rpba_output_block", "rpba_calc_plsa", "rpba_create", "rpba_solve",
            "rpba_get_state", "rpba_get_log", "rpba_exteval", "rpba_kernel_stats", "rpba_float_sequential_sum",
-           "rpba_float_sequential_sum_noalloc", "rpba_destroy")
+           "rpba_float_sequential_sum_noalloc", "rpba_train_preconditioner",
+           "rpba_set_preconditioner", "rpba_precond_loss_grad", "rpba_destroy")
 
 _lib = None
 
@@ -80,6 +83,14 @@ def load():
     L.rpba_float_sequential_sum.restype = C.c_int32
     L.rpba_float_sequential_sum_noalloc.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
     L.rpba_float_sequential_sum_noalloc.restype = C.c_int32
+    fp = C.POINTER(C.c_float)
+    L.rpba_train_preconditioner.argtypes = [bp, C.c_int32, op, C.POINTER(RpbaTrainOptionsC), fp,
+                                            C.POINTER(RpbaTrainReportC)]
+    L.rpba_train_preconditioner.restype = C.c_int32
+    L.rpba_set_preconditioner.argtypes = [C.c_void_p, fp, C.c_int32]
+    L.rpba_set_preconditioner.restype = C.c_int32
+    L.rpba_precond_loss_grad.argtypes = [C.POINTER(RpbaPrecondSetC), fp, fp, fp]
+    L.rpba_precond_loss_grad.restype = C.c_int32
     L.rpba_kernel_stats.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     L.rpba_kernel_stats.restype = C.c_int32
     L.rpba_destroy.argtypes = [C.c_void_p]
@@ -137,6 +148,44 @@ def float_sequential_sum(v, device: int = 0) -> np.float32:
     return np.float32(out.value)
 
 
+def train_preconditioner(blocks, steps=300, batch=0, lr=3e-3, probes=2, seed=1, max_samples=0,
+                         **opt_kw):
+    """Train the learned block-Jacobi correction on the direct solver's own
+    systems for ``blocks``; returns (weights float32[1865], report dict)."""
+    arr = (RpbaBlockC * len(blocks))(*[b.as_c() for b in blocks])
+    o = make_options(**opt_kw)
+    t = RpbaTrainOptionsC(int(steps), int(batch), float(lr), int(probes), int(max_samples), int(seed))
+    w = np.zeros(PRECOND_WEIGHTS, np.float32)
+    rep = RpbaTrainReportC()
+    st = load().rpba_train_preconditioner(arr, len(blocks), C.byref(o), C.byref(t),
+                                          w.ctypes.data_as(C.POINTER(C.c_float)), C.byref(rep))
+    if st != 0:
+        raise RpbaError(st, "rpba_train_preconditioner")
+    return w, {k: getattr(rep, k) for k, _ in rep._fields_}
+
+
+def precond_loss_grad(ts: dict, weights):
+    """Training loss and gradient for a host training set (dict of numpy
+    arrays laid out as rpba_precond_set), computed by the GPU kernels."""
+    f32 = lambda k: np.ascontiguousarray(ts[k], np.float32)
+    i32 = lambda k: np.ascontiguousarray(ts[k], np.int32)
+    keep = {k: f32(k) for k in ("features", "sinv", "b", "xs", "blocks")}
+    keep.update({k: i32(k) for k in ("np", "sys", "rowoff", "ent_col", "ent_blk", "sys_row")})
+    fp, ip = C.POINTER(C.c_float), C.POINTER(C.c_int32)
+    st = RpbaPrecondSetC(int(ts["rows"]), int(ts["systems"]), int(ts["probes"]), int(keep["ent_col"].size),
+                         int(keep["blocks"].shape[0]),
+                         *(keep[k].ctypes.data_as(fp) for k in ("features", "sinv", "b", "xs")),
+                         *(keep[k].ctypes.data_as(ip) for k in ("np", "sys", "rowoff", "ent_col", "ent_blk")),
+                         keep["blocks"].ctypes.data_as(fp), keep["sys_row"].ctypes.data_as(ip))
+    w = np.ascontiguousarray(weights, np.float32)
+    loss = C.c_float()
+    g = np.zeros(PRECOND_WEIGHTS, np.float32)
+    r = load().rpba_precond_loss_grad(C.byref(st), w.ctypes.data_as(fp), C.byref(loss), g.ctypes.data_as(fp))
+    if r != 0:
+        raise RpbaError(r, "rpba_precond_loss_grad")
+    return loss.value, g
+
+
 class Solver:
     """Handle API: the block is uploaded once; ``solve`` restarts from it."""
 
@@ -178,6 +227,17 @@ class Solver:
         if st != 0:
             raise RpbaError(st, "rpba_exteval")
         return res[: 2 * n].reshape(-1, 2), rep.as_dict()
+
+    def set_preconditioner(self, weights):
+        """Weights for RPBA_SOLVER_LEARNED solves (None: plain block-Jacobi)."""
+        if weights is None:
+            st = load().rpba_set_preconditioner(self.h, None, 0)
+        else:
+            self._w = np.ascontiguousarray(weights, np.float32)
+            st = load().rpba_set_preconditioner(self.h, self._w.ctypes.data_as(C.POINTER(C.c_float)),
+                                                self._w.size)
+        if st != 0:
+            raise RpbaError(st, "rpba_set_preconditioner")
 
     def kernel_stats(self) -> dict:
         """Per-kernel device time of the last solve (needs verbose=2)."""
