@@ -107,6 +107,10 @@ typedef struct rpba_options {
                             (0: the reference's 1e5 decrease rule)          */
   int32_t device;        /* CUDA device ordinal                             */
   int32_t verbose;
+  int32_t coarse_aggregates; /* learned solver's coarse space: 0 = default
+                                (up to 148 camera aggregates), > 0 = at most
+                                this many (<= 200), < 0 = none (block-Jacobi
+                                part only)                                  */
 } rpba_options;
 
 /* Per-pass summary; index 0 = robust pass, 1 = refinement pass. */
@@ -121,6 +125,7 @@ typedef struct rpba_report {
   int32_t linear_solves; /* CalcBundleSep calls                             */
   int64_t pcg_iterations;/* total PCG iterations                            */
   int32_t pcg_fallbacks; /* learned PCG runs that fell back to the direct solve */
+  int32_t coarse_rebuilds; /* learned PCG solves repeated with a rebuilt coarse operator */
   int32_t obs_deleted;   /* observations removed by RobustDelete            */
   int32_t points_deleted;
   int32_t points_used;   /* points kept by PointXXvIn                       */
@@ -238,6 +243,8 @@ typedef struct rpba_precond_set {
   const int32_t *ent_blk;  /* [nent] block index, bit 31: transposed      */
   const float *blocks;     /* [nblocks][81] D^-1/2 S D^-1/2               */
   const int32_t *sys_row;  /* [systems + 1]                               */
+  const float *uc;         /* [probes][rows][9] coarse part of the
+                              preconditioned right-hand sides, or NULL     */
 } rpba_precond_set;
 /* Training loss and its gradient for `weights`, computed by the GPU's
  * training kernels (for checking against an independent implementation).

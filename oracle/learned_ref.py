@@ -4,7 +4,8 @@ INFRASTRUCTURE ONLY.  Written independently of the GPU kernels in torch
 against which the GPU's hand-written backward pass is checked.
 
 Objective (see rpba_b200/csrc/learned.cu): per system and right-hand side b,
-with C = blockdiag(diag(s_k) Sinv_k diag(s_k)), u = C b, v = S u,
+with C = blockdiag(diag(s_k) Sinv_k diag(s_k)), u = C b + uc (uc: the fixed
+coarse-space part of the preconditioned right-hand side), v = S u,
 loss = ln(u^T v) - 2 ln(b^T u), averaged over systems and right-hand sides;
 s_k = exp(tanh(W2 tanh(W1 f_k + b1) + b2)) on the block's parameters.
 """
@@ -32,6 +33,8 @@ def loss(ts: dict, weights: np.ndarray):
     Si = torch.tensor(np.asarray(ts["sinv"], np.float64).reshape(R, 9, 9))
     b = torch.tensor(np.asarray(ts["b"], np.float64).reshape(P, R, 9))
     u = s[None] * torch.einsum("rac,prc->pra", Si, s[None] * b)
+    if ts.get("uc") is not None:
+        u = u + torch.tensor(np.asarray(ts["uc"], np.float64).reshape(P, R, 9))
     # v = S u over the block rows
     blocks = torch.tensor(np.asarray(ts["blocks"], np.float64).reshape(-1, 9, 9))
     rowoff = np.asarray(ts["rowoff"])

@@ -1002,6 +1002,7 @@ void LSA::sparse_pcg() {
       std::vector<const std::pair<const int, std::vector<double>> *> order;
       for (auto &kv : Off[i]) order.push_back(&kv);
       if (g_order_variant == 1) std::reverse(order.begin(), order.end());
+      if (g_order_variant == 2) std::rotate(order.begin(), order.begin() + order.size() / 2, order.end());
       for (auto *kvp : order) {
         const auto &kv = *kvp;
         const int row = kv.first, nr = cam_np(row);

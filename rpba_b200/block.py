@@ -49,6 +49,7 @@ class RpbaOptionsC(C.Structure):
         ("pcg_tolerance", C.c_double),
         ("device", C.c_int32),
         ("verbose", C.c_int32),
+        ("coarse_aggregates", C.c_int32),
     ]
 
 
@@ -64,6 +65,7 @@ class RpbaReportC(C.Structure):
         ("linear_solves", C.c_int32),
         ("pcg_iterations", C.c_int64),
         ("pcg_fallbacks", C.c_int32),
+        ("coarse_rebuilds", C.c_int32),
         ("obs_deleted", C.c_int32),
         ("points_deleted", C.c_int32),
         ("points_used", C.c_int32),
@@ -101,7 +103,7 @@ class RpbaPrecondSetC(C.Structure):
     _fields_ = [("rows", C.c_int32), ("systems", C.c_int32), ("probes", C.c_int32), ("nent", C.c_int32),
                 ("nblocks", C.c_int32), ("features", _f32p), ("sinv", _f32p), ("b", _f32p), ("xs", _f32p),
                 ("np", _i32p), ("sys", _i32p), ("rowoff", _i32p), ("ent_col", _i32p), ("ent_blk", _i32p),
-                ("blocks", _f32p), ("sys_row", _i32p)]
+                ("blocks", _f32p), ("sys_row", _i32p), ("uc", _f32p)]
 
 
 PRECOND_WEIGHTS = 1865
@@ -111,10 +113,12 @@ PREC_FP64, PREC_MIXED = 0, 1
 
 def make_options(robust=True, exteval=False, threads=1, k2=True, k4=True, f=True,
                  solver=SOLVER_PCG, precision=PREC_FP64, max_lm_iterations=-1,
-                 pcg_max_iterations=0, pcg_tolerance=0.0, device=0, verbose=0) -> RpbaOptionsC:
+                 pcg_max_iterations=0, pcg_tolerance=0.0, device=0, verbose=0,
+                 coarse_aggregates=0) -> RpbaOptionsC:
     return RpbaOptionsC(int(robust), int(exteval), int(threads), int(k2), int(k4), int(f),
                         int(solver), int(precision), int(max_lm_iterations),
-                        int(pcg_max_iterations), float(pcg_tolerance), int(device), int(verbose))
+                        int(pcg_max_iterations), float(pcg_tolerance), int(device), int(verbose),
+                        int(coarse_aggregates))
 
 
 def _p(a: np.ndarray, t):

@@ -1,0 +1,341 @@
+// coarse.cu -- coarse space of the two-level preconditioner of the reduced
+// camera system (RCS).
+//
+// Block-Jacobi (rbacore.cpp:1841) removes the error of each camera block
+// against its own diagonal, but not the smooth error in which neighbouring
+// cameras move together: on a long street or a city those modes take CG
+// hundreds of iterations.  The near-null space of the RCS is known: a small
+// similarity transform of the world (all cameras and, through the Schur
+// complement, all points) changes no residual, so it is opposed only by the
+// gauge and by damping.  Grouping cameras into spatially compact aggregates
+// and giving each aggregate its own small similarity transform spans the
+// smooth modes; with P the prolongation and A_c = P^T S P the Galerkin
+// matrix, the preconditioner is
+//     M^-1 = C + P A_c^-1 P^T          (C: the (learned) block-Jacobi part)
+//
+// Per camera k (x = R (X + PC), R_new = Cayley(w) R), a world motion
+// X' = (I + [d]x) X + t seen by unchanged images needs
+//     w = -R d,   dPC = d x (PC - c_a) - t',   and a scale s: dPC = s (PC - c_a)
+// (c_a the aggregate's mean PC).  The coarse unknowns of aggregate a are
+// (d 3, t 3, s, and common shifts of k1, k2, f): CO_M = 10.
+//
+// Everything here is deterministic: every sum has a fixed order.
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "internal.h"
+
+namespace rpba {
+
+namespace {
+
+constexpr int CP = CO_M * 9;  // P_k entries
+
+// P_k for the rows of aggregate blockIdx.x (row major, 9 x CO_M).
+__global__ void k_coarse_P(DevLSA L, CoarseWork C) {
+  const int a = blockIdx.x;
+  const int t0 = C.agg_off[a], t1 = C.agg_off[a + 1];
+  __shared__ double cen[3], rho_inv;
+  if (threadIdx.x == 0) {
+    double c[3] = {0., 0., 0.};
+    int n = 0;
+    for (int t = t0; t < t1; ++t) {
+      const int k = C.agg_rows[t];
+      if (k < 1) continue;
+      for (int j = 0; j < 3; ++j) c[j] += L.camn[k].PC[j];
+      ++n;
+    }
+    for (int j = 0; j < 3; ++j) c[j] /= (n > 0 ? n : 1);
+    double r2 = 0.;
+    for (int t = t0; t < t1; ++t) {
+      const int k = C.agg_rows[t];
+      if (k < 1) continue;
+      for (int j = 0; j < 3; ++j) {
+        const double d = L.camn[k].PC[j] - c[j];
+        r2 += d * d;
+      }
+    }
+    const double rho = sqrt(r2 / (n > 0 ? n : 1));
+    for (int j = 0; j < 3; ++j) cen[j] = c[j];
+    rho_inv = rho > 0. ? 1. / rho : 0.;
+  }
+  __syncthreads();
+  for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x) {
+    const int k = C.agg_rows[t];
+    double *P = C.P + (size_t)k * CP;
+    for (int i = 0; i < CP; ++i) P[i] = 0.;
+    if (k < 1) continue;  // camera 0's intrinsics row: block-Jacobi only
+    const CamState &cs = L.camn[k];
+    for (int r = 0; r < 3; ++r)
+      for (int j = 0; j < 3; ++j) P[r * CO_M + j] = -cs.R[r * 3 + j];
+    const double lev[3] = {cs.PC[0] - cen[0], cs.PC[1] - cen[1], cs.PC[2] - cen[2]};
+    // cr[j][c] = (e_j x lev)_c
+    const double cr[3][3] = {{0., -lev[2], lev[1]}, {lev[2], 0., -lev[0]}, {-lev[1], lev[0], 0.}};
+    int comp[3] = {0, 1, 2}, npc = 3;
+    if (k == L.normcamera) {
+      comp[0] = L.gauge[0];
+      comp[1] = L.gauge[1];
+      npc = 2;
+    }
+    for (int q = 0; q < npc; ++q) {
+      const int c = comp[q], r = 3 + q;
+      for (int j = 0; j < 3; ++j) P[r * CO_M + j] = cr[j][c];
+      P[r * CO_M + 3 + c] = 1.;
+      P[r * CO_M + 6] = lev[c] * rho_inv;
+    }
+    int r = 3 + npc;
+    if (L.addmask & 1) P[(r++) * CO_M + 7] = 1.;
+    if (L.addmask & 2) P[(r++) * CO_M + 8] = 1.;
+    if (L.addmask & 4) P[(r++) * CO_M + 9] = 1.;
+  }
+}
+
+// Galerkin matrix, one CTA per aggregate a: the strip A_c[a rows][:] is
+// accumulated in shared memory.  Coarse column c of the strip belongs to warp
+// c % 32, which walks the aggregate's rows and their entries in order and
+// adds, for each entry (k, l) with l in aggregate b, column j of
+// P_k^T S_kl P_l to column c = 10 b + j.  Every strip element therefore has
+// one owner and one summation order: the result does not depend on
+// scheduling, and no synchronisation is needed inside the walk.
+constexpr int AS_T = 1024;
+__global__ void __launch_bounds__(AS_T) k_coarse_assemble(DevLSA L, CoarseWork C) {
+  extern __shared__ double strip[];  // [CO_M][nc]
+  const int nc = C.nc;
+  const int a = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < CO_M * nc; i += AS_T) strip[i] = 0.;
+  __syncthreads();
+  for (int t = C.agg_off[a]; t < C.agg_off[a + 1]; ++t) {
+    const int k = C.agg_rows[t];
+    const int e0 = L.rowoff[k], e1 = L.rowoff[k + 1];
+    const int npk = L.camparv[k + 1] - L.camparv[k];
+    const double *Pk = C.P + (size_t)k * CP;
+    for (int c0 = e0; c0 < e1; c0 += 32) {
+      // which of the next 32 entries have a column of this warp
+      int b = -1, j = 32;
+      int2 en = make_int2(0, 0);
+      if (c0 + lane < e1) {
+        en = L.ent[c0 + lane];
+        b = C.row_agg[en.x];
+        if (b >= 0) j = ((warp - b * CO_M) % 32 + 32) % 32;
+      }
+      unsigned m = __ballot_sync(0xffffffffu, b >= 0 && j < CO_M);
+      while (m) {
+        const int src = __ffs(m) - 1;
+        m &= m - 1;
+        const int bb = __shfl_sync(0xffffffffu, b, src), jj = __shfl_sync(0xffffffffu, j, src);
+        const int l = __shfl_sync(0xffffffffu, en.x, src), ey = __shfl_sync(0xffffffffu, en.y, src);
+        const bool tr = ey < 0;
+        const double *B = L.blocks + (size_t)(ey & 0x7fffffff) * 81;
+        const double *Pl = C.P + (size_t)l * CP;
+        const int npl = L.camparv[l + 1] - L.camparv[l];
+        // u_p = sum_q S_kl[p][q] P_l[q][jj]   (lane p < npk)
+        double u = 0.;
+        if (lane < npk)
+          for (int q = 0; q < npl; ++q) u += (tr ? B[q * 9 + lane] : B[lane * 9 + q]) * Pl[q * CO_M + jj];
+        // v_i = sum_p P_k[p][i] u_p            (lane i < CO_M)
+        double v = 0.;
+        for (int p = 0; p < 9; ++p) {
+          const double up = __shfl_sync(0xffffffffu, u, p);
+          if (lane < CO_M && p < npk) v += Pk[p * CO_M + lane] * up;
+        }
+        if (lane < CO_M) strip[lane * nc + bb * CO_M + jj] += v;
+      }
+    }
+  }
+  __syncthreads();
+  // a coarse unknown that no parameter carries (an intrinsic that is not
+  // estimated) has an empty row and column: give it a unit diagonal
+  if (tid < CO_M) {
+    double &d = strip[tid * nc + a * CO_M + tid];
+    if (d == 0.) d = 1.;
+  }
+  __syncthreads();
+  for (int i = tid; i < CO_M * nc; i += AS_T) C.Ac[(size_t)(a * CO_M + i / nc) * nc + i % nc] = strip[i];
+}
+
+// Symmetric Jacobi scaling of A_c before the factorisation (the coarse
+// unknowns mix radians, metres, pixels and distortion coefficients, whose
+// diagonal entries span many decades): dsc = diag^-1/2, A <- D A D with a
+// unit diagonal (+1e-12 against roundoff); the same kernel without the
+// diagonal term maps the inverse back (A^-1 = D (D A D)^-1 D).
+__global__ void k_coarse_diag(CoarseWork C) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= C.nc) return;
+  const double d = C.Ac[(size_t)i * C.nc + i];
+  C.dsc[i] = d > 0. ? 1. / sqrt(d) : 1.;
+}
+__global__ void k_coarse_scale(double *A, const double *dsc, int n, int add_diag) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= (long long)n * n) return;
+  const int i = (int)(g / n), j = (int)(g % n);
+  double v = A[g] * dsc[i] * dsc[j];
+  if (add_diag && i == j) v += 1e-12;
+  A[g] = v;
+}
+
+// rc_a = sum_{k in a} P_k^T r_k (rows in order)
+__global__ void k_coarse_restrict(CoarseWork C, const double *r) {
+  const int a = blockIdx.x, j = threadIdx.x;
+  if (j >= CO_M) return;
+  double s = 0.;
+  for (int t = C.agg_off[a]; t < C.agg_off[a + 1]; ++t) {
+    const int k = C.agg_rows[t];
+    const double *P = C.P + (size_t)k * CP;
+    for (int c = 0; c < 9; ++c) s += P[c * CO_M + j] * r[(size_t)k * 9 + c];
+  }
+  C.rc[a * CO_M + j] = s;
+}
+
+// z_a = A_c^-1[a rows] rc; h_k += P_k z_a for the rows of a
+constexpr int PR_T = 256;
+__global__ void __launch_bounds__(PR_T) k_coarse_prolong(CoarseWork C, double *h) {
+  const int a = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __shared__ double part[PR_T / 32][CO_M];
+  __shared__ double z[CO_M];
+  double zz[CO_M];
+#pragma unroll
+  for (int j = 0; j < CO_M; ++j) zz[j] = 0.;
+  for (int i = threadIdx.x; i < C.nc; i += PR_T) {
+    const double rv = C.rc[i];
+#pragma unroll
+    for (int j = 0; j < CO_M; ++j) zz[j] += C.Ainv[(size_t)(a * CO_M + j) * C.nc + i] * rv;
+  }
+#pragma unroll
+  for (int j = 0; j < CO_M; ++j) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) zz[j] += __shfl_xor_sync(0xffffffffu, zz[j], o);
+    if (lane == 0) part[warp][j] = zz[j];
+  }
+  __syncthreads();
+  if (threadIdx.x < CO_M) {
+    double s = 0.;
+    for (int w = 0; w < PR_T / 32; ++w) s += part[w][threadIdx.x];
+    z[threadIdx.x] = s;
+  }
+  __syncthreads();
+  for (int t = C.agg_off[a] + threadIdx.x; t < C.agg_off[a + 1]; t += PR_T) {
+    const int k = C.agg_rows[t];
+    const double *P = C.P + (size_t)k * CP;
+    for (int c = 0; c < 9; ++c) {
+      double s = 0.;
+#pragma unroll
+      for (int j = 0; j < CO_M; ++j) s += P[c * CO_M + j] * z[j];
+      h[(size_t)k * 9 + c] += s;
+    }
+  }
+}
+
+// Recursive coordinate bisection of idx[lo, hi) into K groups: split along
+// the widest axis at the share of the first half's groups.
+void rcb(const std::vector<double> &pc, std::vector<int> &idx, int lo, int hi, int K, std::vector<int> &cuts) {
+  if (K <= 1 || hi - lo <= 1) {
+    cuts.push_back(hi);
+    return;
+  }
+  double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
+  for (int i = lo; i < hi; ++i)
+    for (int j = 0; j < 3; ++j) {
+      mn[j] = std::min(mn[j], pc[3 * idx[i] + j]);
+      mx[j] = std::max(mx[j], pc[3 * idx[i] + j]);
+    }
+  int ax = 0;
+  for (int j = 1; j < 3; ++j)
+    if (mx[j] - mn[j] > mx[ax] - mn[ax]) ax = j;
+  const int K1 = K / 2;
+  const int mid = lo + (int)((long long)(hi - lo) * K1 / K);
+  std::nth_element(idx.begin() + lo, idx.begin() + mid, idx.begin() + hi, [&](int u, int v) {
+    const double a = pc[3 * u + ax], b = pc[3 * v + ax];
+    return a < b || (a == b && u < v);
+  });
+  rcb(pc, idx, lo, mid, K1, cuts);
+  rcb(pc, idx, mid, hi, K - K1, cuts);
+}
+
+template <class T>
+T *calloc_dev(size_t n, std::vector<void *> &owned) {
+  void *p = nullptr;
+  RPBA_CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+  owned.push_back(p);
+  return (T *)p;
+}
+
+}  // namespace
+
+void coarse_build(const DevLSA &L, int max_aggs, CoarseWork &C, std::vector<void *> &owned, cudaStream_t s) {
+  C.nagg = C.nc = 0;
+  const int nimg = L.nimg;
+  const int ncam = nimg - 1;  // camera rows k >= 1
+  if (ncam < 8) return;
+  std::vector<CamState> cams(nimg);
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(cams.data(), L.camn, sizeof(CamState) * nimg, cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+  std::vector<double> pc(3 * (size_t)nimg);
+  for (int k = 0; k < nimg; ++k)
+    for (int j = 0; j < 3; ++j) pc[3 * k + j] = cams[k].PC[j];
+  const int K = std::max(1, std::min(std::min(max_aggs, 200), ncam / 16));
+  std::vector<int> idx(ncam);
+  std::iota(idx.begin(), idx.end(), 1);
+  std::vector<int> cuts;
+  rcb(pc, idx, 0, ncam, K, cuts);
+  const int nagg = (int)cuts.size();
+  std::vector<int> off(nagg + 1, 0), rows, row_agg(nimg, -1);
+  for (int a = 0, lo = 0; a < nagg; ++a) {
+    const int hi = cuts[a];
+    std::vector<int> g(idx.begin() + lo, idx.begin() + hi);
+    if (a == 0 && L.begini == 0) g.push_back(0);  // camera 0's intrinsics row rides along
+    std::sort(g.begin(), g.end());
+    for (int k : g) {
+      rows.push_back(k);
+      row_agg[k] = a;
+    }
+    off[a + 1] = (int)rows.size();
+    lo = hi;
+  }
+  C.nagg = nagg;
+  C.nc = nagg * CO_M;
+  const size_t nc = C.nc;
+  C.agg_off = calloc_dev<int>(nagg + 1, owned);
+  C.agg_rows = calloc_dev<int>(rows.size(), owned);
+  C.row_agg = calloc_dev<int>(nimg, owned);
+  C.P = calloc_dev<double>((size_t)nimg * CP, owned);
+  C.Ac = calloc_dev<double>(nc * nc, owned);
+  C.X = calloc_dev<double>(nc * nc, owned);
+  C.Ainv = calloc_dev<double>(nc * nc, owned);
+  C.Linv = calloc_dev<double>((nc + 63) / 64 * 64 * 64, owned);
+  C.rc = calloc_dev<double>(nc, owned);
+  C.dsc = calloc_dev<double>(nc, owned);
+  C.hj = calloc_dev<double>((size_t)nimg * 9, owned);
+  C.err = calloc_dev<int>(1, owned);
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(C.agg_off, off.data(), sizeof(int) * (nagg + 1), cudaMemcpyHostToDevice, s));
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(C.agg_rows, rows.data(), sizeof(int) * rows.size(), cudaMemcpyHostToDevice, s));
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(C.row_agg, row_agg.data(), sizeof(int) * nimg, cudaMemcpyHostToDevice, s));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(C.P, 0, sizeof(double) * (size_t)nimg * CP, s));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(C.X, 0, sizeof(double) * nc * nc, s));
+  RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+}
+
+void coarse_setup(const DevLSA &L, const CoarseWork &C, cudaStream_t s) {
+  if (C.nagg <= 0) return;
+  RPBA_CUDA_CHECK(cudaMemsetAsync(C.err, 0, sizeof(int), s));
+  k_coarse_P<<<C.nagg, 128, 0, s>>>(L, C);
+  const size_t smem = sizeof(double) * (size_t)CO_M * C.nc;
+  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_coarse_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_coarse_assemble<<<C.nagg, AS_T, smem, s>>>(L, C);
+  const long long nn = (long long)C.nc * C.nc;
+  k_coarse_diag<<<(C.nc + 255) / 256, 256, 0, s>>>(C);
+  k_coarse_scale<<<(int)((nn + 255) / 256), 256, 0, s>>>(C.Ac, C.dsc, C.nc, 1);
+  dense_cholesky(C.Ac, C.nc, C.Linv, C.err, s);
+  dense_spd_inverse(C.Ac, C.nc, C.Linv, C.X, C.Ainv, s);
+  k_coarse_scale<<<(int)((nn + 255) / 256), 256, 0, s>>>(C.Ainv, C.dsc, C.nc, 0);
+  RPBA_CUDA_CHECK(cudaGetLastError());
+}
+
+void coarse_apply(const DevLSA &L, const CoarseWork &C, const double *r, double *h, cudaStream_t s) {
+  (void)L;
+  if (C.nagg <= 0) return;
+  k_coarse_restrict<<<C.nagg, 32, 0, s>>>(C, r);
+  k_coarse_prolong<<<C.nagg, PR_T, 0, s>>>(C, h);
+}
+
+}  // namespace rpba

@@ -234,9 +234,158 @@ __global__ void k_panel_update(const double *A, int n, int j0, int tb, double *y
   if (lane == 0) y[i] -= s;
 }
 
+
+// Tile row it of X = L^-1: CTA j < it forms X_ij = -Linv_i sum_{j<=m<i}
+// L_im X_mj (tile rows < it are complete); CTA j == it copies Linv_i.
+__global__ void __launch_bounds__(DT) k_inv_row(const double *A, int n, const double *Linv, double *X, int it) {
+  extern __shared__ double dyn[];
+  double(*a)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn);
+  double(*b)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn + T * (T + 1));
+  const int jt = blockIdx.x, tid = threadIdx.x;
+  const int i0 = it * T, ib = min(T, n - i0), j0 = jt * T, jb = min(T, n - j0);
+  const double *Li = Linv + (size_t)it * T * T;
+  if (jt == it) {
+    for (int idx = tid; idx < T * T; idx += DT) {
+      const int i = idx / T, j = idx % T;
+      if (i < ib && j < jb) X[(size_t)(i0 + i) * n + j0 + j] = Li[idx];
+    }
+    return;
+  }
+  const int ti = (tid / 16) * 4, tj = (tid % 16) * 4;
+  double o[4][4] = {};
+  for (int mt = jt; mt < it; ++mt) {
+    const int m0 = mt * T, mb = min(T, n - m0);
+    __syncthreads();
+    for (int idx = tid; idx < T * T; idx += DT) {
+      const int i = idx / T, j = idx % T;
+      a[i][j] = (i < ib && j < mb) ? A[(size_t)(i0 + i) * n + m0 + j] : 0.;    // L_im
+      b[i][j] = (i < mb && j < jb) ? X[(size_t)(m0 + i) * n + j0 + j] : 0.;    // X_mj
+    }
+    __syncthreads();
+    for (int m = 0; m < mb; ++m) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        av[u] = a[ti + u][m];
+        bv[u] = b[m][tj + u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) o[u][v] += av[u] * bv[v];
+    }
+  }
+  __syncthreads();
+  // Y -> shared b, then X_ij = -Linv_i Y
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) b[ti + u][tj + v] = o[u][v];
+  for (int idx = tid; idx < T * T; idx += DT) a[idx / T][idx % T] = Li[idx];
+  __syncthreads();
+  double y[4][4] = {};
+  for (int m = 0; m < ib; ++m) {
+    double av[4], bv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      av[u] = a[ti + u][m];
+      bv[u] = b[m][tj + u];
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) y[u][v] += av[u] * bv[v];
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      if (ti + u < ib && tj + v < jb) X[(size_t)(i0 + ti + u) * n + j0 + tj + v] = -y[u][v];
+}
+
+// A^-1 = X^T X for tile (bi, bk), bk <= bi: sum over tile rows m >= bi of
+// X_m,bi^T X_m,bk; written to both triangles.
+__global__ void __launch_bounds__(DT) k_xtx(const double *X, int n, double *Ainv) {
+  const int t = blockIdx.x;
+  int bi = (int)((sqrt(8. * t + 1.) - 1.) / 2.);
+  while ((bi + 1) * (bi + 2) / 2 <= t) ++bi;
+  while (bi * (bi + 1) / 2 > t) --bi;
+  const int bk = t - bi * (bi + 1) / 2;
+  const int ri = bi * T, rk = bk * T, nbi = min(T, n - ri), nbk = min(T, n - rk);
+  extern __shared__ double dyn[];
+  double(*pi)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn);
+  double(*pk)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn + T * (T + 1));
+  const int tid = threadIdx.x, ti = (tid / 16) * 4, tj = (tid % 16) * 4;
+  const int ntiles = (n + T - 1) / T;
+  double o[4][4] = {};
+  for (int mt = bi; mt < ntiles; ++mt) {
+    const int m0 = mt * T, mb = min(T, n - m0);
+    __syncthreads();
+    for (int idx = tid; idx < T * T; idx += DT) {
+      const int m = idx / T, j = idx % T;
+      pi[m][j] = (m < mb && j < nbi) ? X[(size_t)(m0 + m) * n + ri + j] : 0.;
+      pk[m][j] = (m < mb && j < nbk) ? X[(size_t)(m0 + m) * n + rk + j] : 0.;
+    }
+    __syncthreads();
+    for (int m = 0; m < mb; ++m) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        av[u] = pi[m][ti + u];
+        bv[u] = pk[m][tj + u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) o[u][v] += av[u] * bv[v];
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v)
+      if (ti + u < nbi && tj + v < nbk) {
+        Ainv[(size_t)(ri + ti + u) * n + rk + tj + v] = o[u][v];
+        Ainv[(size_t)(rk + tj + v) * n + ri + ti + u] = o[u][v];
+      }
+}
+
 }  // namespace
 
 size_t direct_bytes(int n) { return (size_t)n * n * sizeof(double); }
+
+// Factor a dense SPD matrix in place: the lower triangle of A (row major,
+// n x n) becomes L with A = L L^T; Linv receives the inverses of L's
+// diagonal T x T tiles.  A non-positive pivot sets bit 4 of *err.
+void dense_cholesky(double *A, int n, double *Linv, int *err, cudaStream_t s) {
+  if (n <= 0) return;
+  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
+  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
+  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
+  const int ntiles = (n + T - 1) / T;
+  for (int jt = 0; jt < ntiles; ++jt) {
+    const int j0 = jt * T, tb = min(T, n - j0);
+    k_potrf<<<1, DT, SMEM2, s>>>(A, n, j0, tb, Linv + (size_t)jt * T * T, err);
+    const int rows_below = n - j0 - tb;
+    if (rows_below > 0) {
+      const int m = (rows_below + T - 1) / T;
+      k_trsm<<<m, DT, SMEM2, s>>>(A, n, j0, tb, Linv + (size_t)jt * T * T);
+      k_syrk<<<m * (m + 1) / 2, DT, SMEM2, s>>>(A, n, j0, tb, m);
+    }
+  }
+}
+
+// Explicit inverse from the factor: X = L^-1 tile row by tile row
+// (X_ij = -L_ii^-1 sum_{j <= m < i} L_im X_mj), then A^-1 = X^T X, both
+// triangles written.  X and Ainv are n x n row major.
+void dense_spd_inverse(const double *A, int n, const double *Linv, double *X, double *Ainv, cudaStream_t s) {
+  if (n <= 0) return;
+  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_inv_row, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
+  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_xtx, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
+  const int ntiles = (n + T - 1) / T;
+  for (int it = 0; it < ntiles; ++it) k_inv_row<<<it + 1, DT, SMEM2, s>>>(A, n, Linv, X, it);
+  k_xtx<<<ntiles * (ntiles + 1) / 2, DT, SMEM2, s>>>(X, n, Ainv);
+}
 
 // Factor S = L L^T (kept in W.A / W.Linv) and solve S x = b for the
 // reduced camera system; x in xsol (padded 9 per camera).  A non-positive
@@ -244,26 +393,13 @@ size_t direct_bytes(int n) { return (size_t)n * n * sizeof(double); }
 void direct_factor(const DevLSA &L, const DirectWork &W, cudaStream_t s) {
   const int n = W.n;
   if (n <= 0) return;
-  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
-  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
-  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
   RPBA_CUDA_CHECK(cudaMemsetAsync(W.A, 0, (size_t)n * n * sizeof(double), s));
   const long long nd = (long long)(L.nimg - L.begini) * 81;
   if (nd > 0) {
     k_dense_fill<<<(int)((nd + 255) / 256), 256, 0, s>>>(L, W.coff, n, W.A);
     k_dense_fill_off<<<(int)((nd + 255) / 256), 256, 0, s>>>(L, W.coff, n, W.A);
   }
-  const int ntiles = (n + T - 1) / T;
-  for (int jt = 0; jt < ntiles; ++jt) {
-    const int j0 = jt * T, tb = min(T, n - j0);
-    k_potrf<<<1, DT, SMEM2, s>>>(W.A, n, j0, tb, W.Linv + (size_t)jt * T * T, L.err);
-    const int rows_below = n - j0 - tb;
-    if (rows_below > 0) {
-      const int m = (rows_below + T - 1) / T;
-      k_trsm<<<m, DT, SMEM2, s>>>(W.A, n, j0, tb, W.Linv + (size_t)jt * T * T);
-      k_syrk<<<m * (m + 1) / 2, DT, SMEM2, s>>>(W.A, n, j0, tb, m);
-    }
-  }
+  dense_cholesky(W.A, n, W.Linv, L.err, s);
 }
 
 // x = S^-1 b with the factor from direct_factor; b and x padded 9 per camera

@@ -114,6 +114,35 @@ size_t direct_bytes(int n);
 void direct_solve(const DevLSA &L, const DirectWork &W, double *xsol, cudaStream_t s);
 void direct_factor(const DevLSA &L, const DirectWork &W, cudaStream_t s);
 void direct_resolve(const DevLSA &L, const DirectWork &W, const double *b, double *xsol, cudaStream_t s);
+// dense SPD helpers (row major n x n, 64 x 64 tiles)
+void dense_cholesky(double *A, int n, double *Linv, int *err, cudaStream_t s);
+void dense_spd_inverse(const double *A, int n, const double *Linv, double *X, double *Ainv, cudaStream_t s);
+
+// ---- coarse space of the two-level preconditioner (coarse.cu)
+// Cameras are grouped into spatially compact aggregates; each aggregate
+// contributes CO_M coarse unknowns: a small rigid motion of its cameras
+// (rotation 3, translation 3), a scale about its centre, and common shifts
+// of the three intrinsics.  P_k (9 x CO_M) maps them onto camera k's block.
+constexpr int CO_M = 10;
+struct CoarseWork {
+  int nagg = 0, nc = 0;          // aggregates, coarse unknowns (CO_M each)
+  int *agg_off = nullptr;        // [nagg + 1]
+  int *agg_rows = nullptr;       // rows of the system grouped by aggregate
+  int *row_agg = nullptr;        // [nimg] aggregate of a row, -1 outside
+  double *P = nullptr;           // [nimg * 9 * CO_M]
+  double *Ac = nullptr, *X = nullptr, *Ainv = nullptr, *Linv = nullptr;
+  double *rc = nullptr;          // [nc] restricted residual
+  double *dsc = nullptr;         // [nc] Jacobi scaling of A_c
+  double *hj = nullptr;          // [nimg * 9] fine part of the preconditioned residual
+  int *err = nullptr;            // bit 4: coarse matrix not positive definite
+};
+// Aggregates from the cameras' projection centres (recursive coordinate
+// bisection into at most max_aggs groups of about 16 cameras or more).
+void coarse_build(const DevLSA &L, int max_aggs, CoarseWork &C, std::vector<void *> &owned, cudaStream_t s);
+// Per linear system: P, the Galerkin matrix P^T S P and its inverse.
+void coarse_setup(const DevLSA &L, const CoarseWork &C, cudaStream_t s);
+// h += P A_c^-1 P^T r over the rows of the system.
+void coarse_apply(const DevLSA &L, const CoarseWork &C, const double *r, double *h, cudaStream_t s);
 
 // ---- learned preconditioner (learned.cu)
 constexpr int NN_F = 19, NN_H = 64, NN_O = 9;
@@ -131,10 +160,13 @@ struct TrainSet {
   int2 *ent;         // (row, block | 0x80000000 if transposed)
   float *blocks;     // [.][81]        D^-1/2 S D^-1/2
   int *sys_row;      // [systems + 1]
+  float *uc;         // [probes][rows_cap][9] coarse part D^1/2 P A_c^-1 P^T b
+                     // of the preconditioned right-hand sides (nullptr: none)
 };
 struct TrainHost {  // host-side capacities and fill levels
   int ents, ents_cap, blocks, blocks_cap, sys_cap;
   int2 *rc;  // device scratch: (row, col) of a system's off-diagonal blocks
+  double *vb, *vz;  // device scratch: [nimg * 9] right-hand side, coarse part
   std::vector<int> sys_row;
 };
 struct TrainBufs {
@@ -143,7 +175,8 @@ struct TrainBufs {
 };
 struct PcgWork;
 void learned_pcg_setup(const DevLSA &L, const PcgWork &W, const float *weights, cudaStream_t s);
-void learned_record(const DevLSA &L, const DirectWork &DW, const double *xstar, unsigned long long seed,
+struct CoarseWork;
+void learned_record(const DevLSA &L, const CoarseWork *coarse, const double *xstar, unsigned long long seed,
                     TrainSet &T, TrainHost &H, cudaStream_t s);
 void learned_loss_grad(const TrainSet &T, const float *W, TrainBufs &B, float *loss, float *err, cudaStream_t s);
 void learned_adam(float *W, float *m, float *v, const float *grad, float lr, int t, cudaStream_t s);
@@ -157,8 +190,10 @@ struct PcgWork {
 // mode 0: the reference's stop rule; mode 1: stop when r^T M^-1 r falls
 // below tol^2 times its start value (W.iters[1] = 1 when it did), with the
 // learned preconditioner `weights` (nullptr: plain block-Jacobi).
+// With `coarse` the preconditioner is two-level: the (learned) block
+// Jacobi part plus the coarse correction P A_c^-1 P^T.
 int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s, int mode = 0,
-              double tol = 0., const float *weights = nullptr);
+              double tol = 0., const float *weights = nullptr, const CoarseWork *coarse = nullptr);
 int pcg_max_grid(int device);
 
 // ---- structure (structure.cu)

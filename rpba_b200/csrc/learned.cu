@@ -38,8 +38,10 @@ constexpr float ALPHA = 1.0f;
 
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
-// Features of camera row k (>= begini) of the assembled system.
-__device__ void block_features(const DevLSA &L, int k, float f[NN_F]) {
+// Features of camera row k (>= begini) of the assembled system, computed by
+// one warp (the row's entries are split over the lanes and the coupling sums
+// reduced in a fixed butterfly order); every lane returns the same f.
+__device__ void block_features(const DevLSA &L, int k, int lane, float f[NN_F]) {
   const int np = L.camparv[k + 1] - L.camparv[k];
   const double *D = L.blocks + (size_t)k * 81;
   double ld[9], mean = 0.;
@@ -50,7 +52,7 @@ __device__ void block_features(const DevLSA &L, int k, float f[NN_F]) {
   mean /= (np > 0 ? np : 1);
   double cpl[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   int deg = 0;
-  for (int t = L.rowoff[k]; t < L.rowoff[k + 1]; ++t) {
+  for (int t = L.rowoff[k] + lane; t < L.rowoff[k + 1]; t += 32) {
     const int2 en = L.ent[t];
     const int col = en.x;
     if (col == k) continue;
@@ -65,6 +67,12 @@ __device__ void block_features(const DevLSA &L, int k, float f[NN_F]) {
         cpl[a] += fabs(v) / sqrt(fmax(D[a * 9 + a] * Dl[c * 9 + c], 1e-300));
       }
   }
+#pragma unroll
+  for (int a = 0; a < 9; ++a)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cpl[a] += __shfl_xor_sync(0xffffffffu, cpl[a], o);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) deg += __shfl_xor_sync(0xffffffffu, deg, o);
   for (int a = 0; a < 9; ++a) {
     f[a] = a < np ? (float)(ld[a] - mean) : 0.f;
     f[9 + a] = a < np ? (float)log1p(cpl[a]) : 0.f;
@@ -90,62 +98,71 @@ __device__ __forceinline__ void mlp_forward(const float *W, const float f[NN_F],
   }
 }
 
-// PCG start with the learned preconditioner (replaces k_pcg_setup):
-// C_k = diag(s) S_kk^-1 diag(s); W == nullptr gives plain block-Jacobi.
+// The same forward pass by one warp (hidden units lane and lane + 32; the
+// output sums run over the hidden units in order, as in mlp_forward); every
+// lane returns the same s.
+__device__ __forceinline__ void mlp_forward_warp(const float *W, const float f[NN_F], int lane, float s[NN_O]) {
+  const float *W1 = W, *b1 = W + NN_H * NN_F, *W2 = b1 + NN_H, *b2 = W2 + NN_O * NN_H;
+  float h2[2];
+  for (int u = 0; u < 2; ++u) {
+    const int i = lane + 32 * u;
+    float a = b1[i];
+#pragma unroll
+    for (int j = 0; j < NN_F; ++j) a += W1[i * NN_F + j] * f[j];
+    h2[u] = tanhf(a);
+  }
+  float o[NN_O];
+  for (int i = 0; i < NN_O; ++i) o[i] = b2[i];
+  for (int j = 0; j < NN_H; ++j) {
+    const float hj = __shfl_sync(0xffffffffu, h2[j >> 5], j & 31);
+#pragma unroll
+    for (int i = 0; i < NN_O; ++i) o[i] += W2[i * NN_H + j] * hj;
+  }
+  for (int i = 0; i < NN_O; ++i) s[i] = expf(ALPHA * tanhf(o[i]));
+}
+
+// PCG start with the learned preconditioner (replaces k_pcg_setup), one
+// warp per camera row: C_k = diag(s) S_kk^-1 diag(s); W == nullptr gives
+// plain block-Jacobi.
 __global__ void k_learned_setup(DevLSA L, PcgWork Wk, const float *weights) {
   __shared__ float Ws[NN_WEIGHTS];
   for (int i = threadIdx.x; i < NN_WEIGHTS; i += blockDim.x) Ws[i] = weights ? bf16r(weights[i]) : 0.f;
   __syncthreads();
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (k >= L.nimg) return;
   double *C = Wk.Cinv + (size_t)k * 81;
   const size_t o = (size_t)k * 9;
-  for (int a = 0; a < 9; ++a) Wk.d[o + a] = Wk.r1[o + a] = 0.;
+  if (lane < 9) Wk.d[o + lane] = Wk.r1[o + lane] = 0.;
   if (k < L.begini) {
-    for (int a = 0; a < 9; ++a) Wk.r[o + a] = Wk.h[o + a] = Wk.x[o + a] = Wk.xbest[o + a] = 0.;
+    if (lane < 9) Wk.r[o + lane] = Wk.h[o + lane] = Wk.x[o + lane] = Wk.xbest[o + lane] = 0.;
     return;
   }
   const int np = L.camparv[k + 1] - L.camparv[k];
-  lu_inverse9(np, L.blocks + (size_t)k * 81, C);
+  if (lane == 0) lu_inverse9(np, L.blocks + (size_t)k * 81, C);
+  float sc[NN_O];
+  for (int a = 0; a < NN_O; ++a) sc[a] = 1.f;
   if (weights) {
-    float f[NN_F], h[NN_H], ov[NN_O], s[NN_O];
-    block_features(L, k, f);
-    mlp_forward(Ws, f, h, ov, s);
-    for (int a = 0; a < 9; ++a)
-      for (int c = 0; c < 9; ++c)
-        if (a < np && c < np) C[a * 9 + c] *= (double)s[a] * (double)s[c];
+    float f[NN_F];
+    block_features(L, k, lane, f);
+    mlp_forward_warp(Ws, f, lane, sc);
   }
-  double rv[9];
-  for (int a = 0; a < 9; ++a) rv[a] = L.rhs[o + a];
-  for (int a = 0; a < 9; ++a) {
+  __syncwarp();
+  if (lane < 9) {
+    const int a = lane;
     double sum = 0.;
-    for (int c = 0; c < 9; ++c) sum += C[a * 9 + c] * rv[c];
-    Wk.r[o + a] = rv[a];
+    for (int c = 0; c < 9; ++c) {
+      double cv = C[a * 9 + c];
+      if (weights && a < np && c < np) {
+        cv *= (double)sc[a] * (double)sc[c];
+        C[a * 9 + c] = cv;
+      }
+      sum += cv * L.rhs[o + c];
+    }
+    Wk.r[o + a] = L.rhs[o + a];
     Wk.h[o + a] = sum;
     Wk.x[o + a] = 0.;
-    Wk.xbest[o + a] = rv[a];
+    Wk.xbest[o + a] = L.rhs[o + a];
   }
-}
-
-// y = S x over the block rows (one warp per row, 27 lanes, fixed order).
-__global__ void k_spmv(DevLSA L, const double *x, double *y) {
-  const int row = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) + L.begini;
-  const int lane = threadIdx.x & 31, grp = lane / 9, rr = lane % 9;
-  if (row >= L.nimg) return;
-  double acc = 0.;
-  if (lane < 27)
-    for (int e = L.rowoff[row] + grp; e < L.rowoff[row + 1]; e += 3) {
-      const int2 en = L.ent[e];
-      const double *B = L.blocks + (size_t)(en.y & 0x7fffffff) * 81;
-      const double *xv = x + (size_t)en.x * 9;
-      if (en.y >= 0)
-        for (int c = 0; c < 9; ++c) acc += B[rr * 9 + c] * xv[c];
-      else
-        for (int c = 0; c < 9; ++c) acc += B[c * 9 + rr] * xv[c];
-    }
-  const double a1 = __shfl_down_sync(0xffffffffu, acc, 9);
-  const double a2 = __shfl_down_sync(0xffffffffu, acc, 18);
-  if (lane < 9) y[(size_t)row * 9 + lane] = acc + a1 + a2;
 }
 
 __device__ __forceinline__ double hash_normal(unsigned long long seed, unsigned long long i) {
@@ -160,23 +177,6 @@ __device__ __forceinline__ double hash_normal(unsigned long long seed, unsigned 
   const double u1 = ((a >> 11) + 0.5) * (1.0 / 9007199254740992.0);
   const double u2 = (b >> 11) * (1.0 / 9007199254740992.0);
   return sqrt(-2. * log(u1)) * cos(6.283185307179586 * u2);
-}
-
-// random right-hand side w = D^1/2 xi on the active parameters
-__global__ void k_probe(DevLSA L, unsigned long long seed, double *w) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = i / 9, a = i % 9;
-  if (k >= L.nimg) return;
-  const int np = L.camparv[k + 1] - L.camparv[k];
-  double v = 0.;
-  if (k >= L.begini && a < np) v = hash_normal(seed, (unsigned long long)i) * sqrt(L.blocks[(size_t)k * 81 + a * 10]);
-  w[i] = v;
-}
-
-__global__ void k_sinv(DevLSA L, double *Cinv) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x + L.begini;
-  if (k >= L.nimg) return;
-  lu_inverse9(L.camparv[k + 1] - L.camparv[k], L.blocks + (size_t)k * 81, Cinv + (size_t)k * 81);
 }
 
 // ---------------------------------------------------------------- training
@@ -209,7 +209,7 @@ __global__ void k_t_forward(TrainSet T, const float *W, float *sv, float *ov, fl
   for (int j = 0; j < NN_H; ++j) hv[(size_t)r * NN_H + j] = h[j];
 }
 
-// u_p = s o (Sinv (s o b_p)) for every row and right-hand side
+// u_p = s o (Sinv (s o b_p)) + uc_p for every row and right-hand side
 __global__ void k_t_apply(TrainSet T, const float *sv, float *u) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int r = i % T.rows, pr = i / T.rows;
@@ -221,7 +221,8 @@ __global__ void k_t_apply(TrainSet T, const float *sv, float *u) {
   for (int a = 0; a < 9; ++a) {
     float t = 0.f;
     for (int c = 0; c < 9; ++c) t += Si[a * 9 + c] * w[c];
-    u[((size_t)pr * T.rows + r) * 9 + a] = sc[a] * t;
+    const float cu = T.uc ? T.uc[((size_t)pr * T.rows_cap + r) * 9 + a] : 0.f;
+    u[((size_t)pr * T.rows + r) * 9 + a] = sc[a] * t + cu;
   }
 }
 
@@ -299,7 +300,8 @@ __global__ void k_t_backward(TrainSet T, const float *W, const float *sv, const 
     float g[9], y[9], sg[9];
     for (int a = 0; a < 9; ++a) {
       g[a] = (2.f * v[o + a] * iq - 2.f * T.b[ob + a] * ip) * scale;
-      y[a] = sc[a] != 0.f ? u[o + a] / sc[a] : 0.f;
+      const float cu = T.uc ? T.uc[ob + a] : 0.f;
+      y[a] = sc[a] != 0.f ? (u[o + a] - cu) / sc[a] : 0.f;
       sg[a] = sc[a] * g[a];
     }
     for (int j = 0; j < np; ++j) {
@@ -358,11 +360,12 @@ __global__ void k_adam(float *W, float *m, float *v, const float *grad, float lr
 
 // ---- recording a system into the training set
 __global__ void k_rec_rows(DevLSA L, TrainSet T, int row0, int sys, const double *xstar, unsigned long long seed) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x + L.begini;
+  const int k = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) + L.begini, lane = threadIdx.x & 31;
   if (k >= L.nimg) return;
   const int r = row0 + (k - L.begini);
   float f[NN_F];
-  block_features(L, k, f);
+  block_features(L, k, lane, f);
+  if (lane != 0) return;
   for (int j = 0; j < NN_F; ++j) T.f[(size_t)r * NN_F + j] = f[j];
   const int np = L.camparv[k + 1] - L.camparv[k];
   T.np[r] = np;
@@ -409,15 +412,36 @@ __global__ void k_rec_blocks(DevLSA L, TrainSet T, int blk0, const int2 *rc, int
   T.blocks[(size_t)(blk0 + b) * 81 + e] = v;
 }
 
+// unscaled right-hand side pr of the system being recorded: b = D^1/2 b~
+__global__ void k_rec_bvec(DevLSA L, TrainSet T, int row0, int pr, double *vb) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = i / 9, a = i % 9;
+  if (k >= L.nimg) return;
+  double v = 0.;
+  if (k >= L.begini && a < L.camparv[k + 1] - L.camparv[k])
+    v = (double)T.b[((size_t)pr * T.rows_cap + row0 + (k - L.begini)) * 9 + a] *
+        sqrt(L.blocks[(size_t)k * 81 + a * 10]);
+  vb[i] = v;
+}
+
+// uc~ = D^1/2 z for the rows of the system being recorded
+__global__ void k_rec_uc(DevLSA L, TrainSet T, int row0, int pr, const double *vz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x + L.begini * 9;
+  const int k = i / 9, a = i % 9;
+  if (k >= L.nimg) return;
+  const int np = L.camparv[k + 1] - L.camparv[k];
+  T.uc[((size_t)pr * T.rows_cap + row0 + (k - L.begini)) * 9 + a] =
+      a < np ? (float)(vz[i] * sqrt(L.blocks[(size_t)k * 81 + a * 10])) : 0.f;
+}
+
 }  // namespace
 
 void learned_pcg_setup(const DevLSA &L, const PcgWork &W, const float *weights, cudaStream_t s) {
-  k_learned_setup<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W, weights);
+  k_learned_setup<<<(L.nimg + 7) / 8, 256, 0, s>>>(L, W, weights);
 }
 
-void learned_record(const DevLSA &L, const DirectWork &DW, const double *xstar, unsigned long long seed,
+void learned_record(const DevLSA &L, const CoarseWork *coarse, const double *xstar, unsigned long long seed,
                     TrainSet &T, TrainHost &H, cudaStream_t s) {
-  (void)DW;
   const int nimg = L.nimg, nd = nimg - L.begini, nb = L.nboff;
   if (nd <= 0) return;
   const int nent = [&] {
@@ -460,9 +484,20 @@ void learned_record(const DevLSA &L, const DirectWork &DW, const double *xstar, 
   RPBA_CUDA_CHECK(cudaMemcpyAsync(T.rowoff + row0, new_off.data(), sizeof(int) * (nd + 1), cudaMemcpyHostToDevice, s));
   RPBA_CUDA_CHECK(cudaMemcpyAsync(T.ent + H.ents, new_ent.data(), sizeof(int2) * new_ent.size(), cudaMemcpyHostToDevice, s));
   RPBA_CUDA_CHECK(cudaMemcpyAsync(H.rc, rc.data(), sizeof(int2) * std::max(nb, 1), cudaMemcpyHostToDevice, s));
-  k_rec_rows<<<(nd + 127) / 128, 128, 0, s>>>(L, T, row0, T.systems, xstar, seed);
+  k_rec_rows<<<(nd + 7) / 8, 256, 0, s>>>(L, T, row0, T.systems, xstar, seed);
   const long long nthreads = (long long)(nd + nb) * 81;
   k_rec_blocks<<<(int)((nthreads + 255) / 256), 256, 0, s>>>(L, T, blk0, H.rc, nb);
+  if (T.uc) {
+    // coarse part of each preconditioned right-hand side (zero without a
+    // coarse space)
+    const int nv = nimg * 9;
+    for (int pr = 0; pr < T.probes; ++pr) {
+      k_rec_bvec<<<(nv + 255) / 256, 256, 0, s>>>(L, T, row0, pr, H.vb);
+      RPBA_CUDA_CHECK(cudaMemsetAsync(H.vz, 0, sizeof(double) * nv, s));
+      if (coarse) coarse_apply(L, *coarse, H.vb, H.vz, s);
+      k_rec_uc<<<(nd * 9 + 255) / 256, 256, 0, s>>>(L, T, row0, pr, H.vz);
+    }
+  }
   RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
   T.rows += nd;
   H.ents += (int)new_ent.size();

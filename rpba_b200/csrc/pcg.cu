@@ -11,6 +11,8 @@
 // barrier's wait is bounded: after 2 s it sets an error bit and returns.
 #include <cooperative_groups.h>
 
+#include <algorithm>
+
 #include "gridsync.cuh"
 #include "internal.h"
 
@@ -39,6 +41,11 @@ struct PcgArgs {
   int row0, row1, nitems, msize;
   int mode;     // 0: reference stop rule; 1: relative preconditioned residual
   double tol2;  // mode 1: stop when r^T M^-1 r <= tol2 * (r0^T M^-1 r0)
+  // two-level preconditioner (coarse.cu): rows are owned per aggregate
+  int nagg, nc;
+  const int *agg_off, *agg_rows;
+  const double *P, *Ainv;
+  double *rc, *hj;
 };
 
 // Deterministic CTA sum of up to three values; valid in every thread.
@@ -95,6 +102,12 @@ __device__ __forceinline__ void grid_sum(const double *red, int G, double (&v)[N
 //  phase 2  per row: q = sum of its items' partials, x += alpha d,
 //           r1 = r - alpha q, h1 = C r1; partials of (alpha q)^2,
 //           r1^T (h1 - h) and r1^T h1 (the next r^T h); d^k is stored
+// With the coarse correction (CO) phase 2 is split by one more barrier:
+//  phase 2a per aggregate (one CTA): as above but h1 is only the block part
+//           (kept in hj), and the aggregate's restriction P^T r1 is formed
+//  phase 2b per aggregate: z = A_c^-1[aggregate rows] (P^T r1), then
+//           h1 = hj + P z and the two dot products
+template <bool CO>
 __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gwarp = blockIdx.x * PCG_W + warp, nwarps = gridDim.x * PCG_W;
@@ -189,49 +202,150 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
       alpha = erthk / edtAdk;
     // ---- phase 2
     double p2[3] = {0., 0., 0.};
-    for (int row = A.row0 + gwarp; row < A.row1; row += nwarps) {
-      const size_t i = (size_t)row * 9 + (lane < 9 ? lane : 0);
-      double r1v = 0., hv = 0.;
-      // q = sum of the row's item partials: the three 9-lane groups take
-      // every third item, four independent loads in flight, fixed order
-      double qg = 0.;
-      if (lane < 27) {
-        const int t0 = A.row_item_off[row], t1 = A.row_item_off[row + 1];
-        double q0 = 0., q1 = 0., q2 = 0., q3 = 0.;
-        int t = t0 + grp;
-        for (; t + 9 < t1; t += 12) {
-          q0 += __ldcg(A.part + (size_t)t * 9 + rr);
-          q1 += __ldcg(A.part + (size_t)(t + 3) * 9 + rr);
-          q2 += __ldcg(A.part + (size_t)(t + 6) * 9 + rr);
-          q3 += __ldcg(A.part + (size_t)(t + 9) * 9 + rr);
+    if constexpr (!CO) {
+      for (int row = A.row0 + gwarp; row < A.row1; row += nwarps) {
+        const size_t i = (size_t)row * 9 + (lane < 9 ? lane : 0);
+        double r1v = 0., hv = 0.;
+        // q = sum of the row's item partials: the three 9-lane groups take
+        // every third item, four independent loads in flight, fixed order
+        double qg = 0.;
+        if (lane < 27) {
+          const int t0 = A.row_item_off[row], t1 = A.row_item_off[row + 1];
+          double q0 = 0., q1 = 0., q2 = 0., q3 = 0.;
+          int t = t0 + grp;
+          for (; t + 9 < t1; t += 12) {
+            q0 += __ldcg(A.part + (size_t)t * 9 + rr);
+            q1 += __ldcg(A.part + (size_t)(t + 3) * 9 + rr);
+            q2 += __ldcg(A.part + (size_t)(t + 6) * 9 + rr);
+            q3 += __ldcg(A.part + (size_t)(t + 9) * 9 + rr);
+          }
+          for (; t < t1; t += 3) q0 += __ldcg(A.part + (size_t)t * 9 + rr);
+          qg = (q0 + q1) + (q2 + q3);
         }
-        for (; t < t1; t += 3) q0 += __ldcg(A.part + (size_t)t * 9 + rr);
-        qg = (q0 + q1) + (q2 + q3);
-      }
-      const double qa = __shfl_down_sync(0xffffffffu, qg, 9);
-      const double qb = __shfl_down_sync(0xffffffffu, qg, 18);
-      if (lane < 9) {
-        const double q = qg + qa + qb;
-        hv = __ldcg(A.h + i);
-        const double dk = hv + beta_prev * __ldcg(dprev + i);
-        dcur[i] = dk;
-        A.x[i] = A.x[i] + alpha * dk;
-        const double dr = alpha * q;
-        r1v = A.r[i] - dr;
-        p2[0] += dr * dr;
-      }
-      const double *C = A.Cinv + (size_t)row * 81;
-      double h1v = 0.;
+        const double qa = __shfl_down_sync(0xffffffffu, qg, 9);
+        const double qb = __shfl_down_sync(0xffffffffu, qg, 18);
+        if (lane < 9) {
+          const double q = qg + qa + qb;
+          hv = __ldcg(A.h + i);
+          const double dk = hv + beta_prev * __ldcg(dprev + i);
+          dcur[i] = dk;
+          A.x[i] = A.x[i] + alpha * dk;
+          const double dr = alpha * q;
+          r1v = A.r[i] - dr;
+          p2[0] += dr * dr;
+        }
+        const double *C = A.Cinv + (size_t)row * 81;
+        double h1v = 0.;
 #pragma unroll
-      for (int c = 0; c < 9; ++c) {
-        const double rc = __shfl_sync(0xffffffffu, r1v, c);
-        if (lane < 9) h1v += __ldg(C + lane * 9 + c) * rc;
+        for (int c = 0; c < 9; ++c) {
+          const double rc = __shfl_sync(0xffffffffu, r1v, c);
+          if (lane < 9) h1v += __ldg(C + lane * 9 + c) * rc;
+        }
+        if (lane < 9) {
+          A.r[i] = r1v;
+          A.h[i] = h1v;
+          p2[1] += r1v * (h1v - hv);
+          p2[2] += r1v * h1v;
+        }
       }
-      if (lane < 9) {
-        A.r[i] = r1v;
-        A.h[i] = h1v;
-        p2[1] += r1v * (h1v - hv);
-        p2[2] += r1v * h1v;
+    } else {
+      __shared__ double shr[PCG_W][CO_M];
+      __shared__ double shz[CO_M];
+      for (int a = blockIdx.x; a < A.nagg; a += G) {
+        const int t0 = A.agg_off[a], t1 = A.agg_off[a + 1];
+        double rcw = 0.;
+        for (int t = t0 + warp; t < t1; t += PCG_W) {
+          const int row = A.agg_rows[t];
+          const size_t i = (size_t)row * 9 + (lane < 9 ? lane : 0);
+          double r1v = 0.;
+          double qg = 0.;
+          if (lane < 27) {
+            const int u0 = A.row_item_off[row], u1 = A.row_item_off[row + 1];
+            double q0 = 0., q1 = 0., q2 = 0., q3 = 0.;
+            int u = u0 + grp;
+            for (; u + 9 < u1; u += 12) {
+              q0 += __ldcg(A.part + (size_t)u * 9 + rr);
+              q1 += __ldcg(A.part + (size_t)(u + 3) * 9 + rr);
+              q2 += __ldcg(A.part + (size_t)(u + 6) * 9 + rr);
+              q3 += __ldcg(A.part + (size_t)(u + 9) * 9 + rr);
+            }
+            for (; u < u1; u += 3) q0 += __ldcg(A.part + (size_t)u * 9 + rr);
+            qg = (q0 + q1) + (q2 + q3);
+          }
+          const double qa = __shfl_down_sync(0xffffffffu, qg, 9);
+          const double qb = __shfl_down_sync(0xffffffffu, qg, 18);
+          if (lane < 9) {
+            const double q = qg + qa + qb;
+            const double hv = __ldcg(A.h + i);
+            const double dk = hv + beta_prev * __ldcg(dprev + i);
+            dcur[i] = dk;
+            A.x[i] = __ldcg(A.x + i) + alpha * dk;
+            const double dr = alpha * q;
+            r1v = __ldcg(A.r + i) - dr;
+            p2[0] += dr * dr;
+          }
+          const double *C = A.Cinv + (size_t)row * 81;
+          const double *Pk = A.P + (size_t)row * (9 * CO_M);
+          double h1v = 0.;
+#pragma unroll
+          for (int c = 0; c < 9; ++c) {
+            const double rc = __shfl_sync(0xffffffffu, r1v, c);
+            if (lane < 9) h1v += __ldg(C + lane * 9 + c) * rc;
+            if (lane < CO_M) rcw += __ldg(Pk + c * CO_M + lane) * rc;
+          }
+          if (lane < 9) {
+            A.r[i] = r1v;
+            A.hj[i] = h1v;
+          }
+        }
+        if (lane < CO_M) shr[warp][lane] = rcw;
+        __syncthreads();
+        if (threadIdx.x < CO_M) {
+          double sum = 0.;
+          for (int w = 0; w < PCG_W; ++w) sum += shr[w][threadIdx.x];
+          A.rc[a * CO_M + threadIdx.x] = sum;
+        }
+        __syncthreads();
+      }
+      if (!grid_barrier(A.bar, G, A.err)) return;
+      for (int a = blockIdx.x; a < A.nagg; a += G) {
+        double z[CO_M];
+#pragma unroll
+        for (int j = 0; j < CO_M; ++j) z[j] = 0.;
+        for (int i = threadIdx.x; i < A.nc; i += PCG_T) {
+          const double rv = __ldcg(A.rc + i);
+#pragma unroll
+          for (int j = 0; j < CO_M; ++j) z[j] += __ldg(A.Ainv + (size_t)(a * CO_M + j) * A.nc + i) * rv;
+        }
+#pragma unroll
+        for (int j = 0; j < CO_M; ++j) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) z[j] += __shfl_xor_sync(0xffffffffu, z[j], o);
+          if (lane == 0) shr[warp][j] = z[j];
+        }
+        __syncthreads();
+        if (threadIdx.x < CO_M) {
+          double sum = 0.;
+          for (int w = 0; w < PCG_W; ++w) sum += shr[w][threadIdx.x];
+          shz[threadIdx.x] = sum;
+        }
+        __syncthreads();
+        const int t0 = A.agg_off[a], t1 = A.agg_off[a + 1];
+        for (int t = t0 + warp; t < t1; t += PCG_W) {
+          const int row = A.agg_rows[t];
+          if (lane < 9) {
+            const size_t i = (size_t)row * 9 + lane;
+            const double *Pk = A.P + (size_t)row * (9 * CO_M) + lane * CO_M;
+            double h1v = __ldcg(A.hj + i);
+#pragma unroll
+            for (int j = 0; j < CO_M; ++j) h1v += __ldg(Pk + j) * shz[j];
+            const double hv = __ldcg(A.h + i), r1v = __ldcg(A.r + i);
+            p2[1] += r1v * (h1v - hv);
+            p2[2] += r1v * h1v;
+            A.h[i] = h1v;
+          }
+        }
+        __syncthreads();
       }
     }
     cta_sum<3>(p2, sh);
@@ -251,7 +365,7 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
     if (improved) {
       meandrold = meandr;
       for (int row = A.row0 + gwarp; row < A.row1; row += nwarps)
-        if (lane < 9) A.xbest[(size_t)row * 9 + lane] = A.x[(size_t)row * 9 + lane];
+        if (lane < 9) A.xbest[(size_t)row * 9 + lane] = __ldcg(A.x + (size_t)row * 9 + lane);
     }
     if (A.mode == 0 && meandr * 1.e5 < meandr0) break;
     if (A.mode == 1 && !(g3[2] > A.tol2 * erthk0)) {
@@ -298,9 +412,11 @@ __global__ void k_pcg_setup(DevLSA L, PcgWork W) {
 }  // namespace
 
 int pcg_max_grid(int device) {
-  int nsm = 0, per = 0;
+  int nsm = 0, per = 0, per2 = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg, PCG_T, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<false>, PCG_T, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true>, PCG_T, 0);
+  per = std::min(per, per2);
   if (per < 1) per = 1;
   return nsm * per;
 }
@@ -308,11 +424,13 @@ int pcg_max_grid(int device) {
 // Returns 0; throws CudaError on launch errors.  The iteration count is
 // left in W.iters.
 int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s, int mode, double tol,
-              const float *weights) {
-  if (mode == 1 || weights)
+              const float *weights, const CoarseWork *coarse) {
+  const bool co = coarse && coarse->nagg > 0;
+  if (mode == 1 || weights || co)
     learned_pcg_setup(L, W, weights, s);
   else
     k_pcg_setup<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W);
+  if (co) coarse_apply(L, *coarse, W.r, W.h, s);
   RPBA_CUDA_CHECK(cudaGetLastError());
   const int nrows = L.nimg - L.begini;
   if (nrows <= 0) return 0;
@@ -344,9 +462,18 @@ int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream
   A.msize = msize;
   A.mode = mode;
   A.tol2 = tol * tol;
+  A.nagg = co ? coarse->nagg : 0;
+  A.nc = co ? coarse->nc : 0;
+  A.agg_off = co ? coarse->agg_off : nullptr;
+  A.agg_rows = co ? coarse->agg_rows : nullptr;
+  A.P = co ? coarse->P : nullptr;
+  A.Ainv = co ? coarse->Ainv : nullptr;
+  A.rc = co ? coarse->rc : nullptr;
+  A.hj = co ? coarse->hj : nullptr;
   RPBA_CUDA_CHECK(cudaMemsetAsync(W.bar, 0, 2 * sizeof(unsigned), s));
   void *args[] = {&A};
-  RPBA_CUDA_CHECK(cudaLaunchCooperativeKernel((const void *)k_pcg, dim3(g), dim3(PCG_T), args, 0, s));
+  const void *fn = co ? (const void *)k_pcg<true> : (const void *)k_pcg<false>;
+  RPBA_CUDA_CHECK(cudaLaunchCooperativeKernel(fn, dim3(g), dim3(PCG_T), args, 0, s));
   return 0;
 }
 

@@ -234,6 +234,21 @@ struct rpba_handle {
   }
 
   // dense direct-solve buffers, allocated on first use
+  // coarse space of the learned solver, built once per handle from the
+  // cameras of the first linear system (nullptr: none)
+  CoarseWork CW{};
+  bool coarse_built = false, coarse_stale = true;
+  int coarse_ref_iters = 0;
+  const CoarseWork *ensure_coarse() {
+    if (opt.coarse_aggregates < 0) return nullptr;
+    if (!coarse_built) {
+      coarse_built = true;
+      const int want = opt.coarse_aggregates > 0 ? opt.coarse_aggregates : 148;
+      coarse_build(L, want, CW, owned, s);
+    }
+    return CW.nagg > 0 ? &CW : nullptr;
+  }
+
   void ensure_direct() {
     if (DW.A) return;
     std::vector<int> coff(nimg + 1, 0);
@@ -595,6 +610,7 @@ void rpba_handle::reset() {
 }
 
 void rpba_handle::structure() {
+  coarse_stale = true;
   long long npairs = 0;
   int nb = 0;
   PROF("structure_pairs", 3, nb = build_pairs(L, S, max_pairs, &npairs, s));
@@ -627,17 +643,48 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
     ensure_direct();
     PROF("direct", 1, direct_solve(L, DW, W.xbest, s));
   } else if (opt.solver == RPBA_SOLVER_LEARNED) {
-    // PCG with the learned preconditioner.  Stop rule: the reference's
+    // PCG with the two-level preconditioner: the learned block-Jacobi part
+    // plus the aggregate coarse space.  Stop rule: the reference's
     // (pcg_tolerance == 0) or a relative preconditioned residual; past the
     // iteration cap the direct solve takes over
     const int mode = opt.pcg_tolerance > 0. ? 1 : 0;
     const int cap = opt.pcg_max_iterations > 0 ? opt.pcg_max_iterations : msize;
-    PROF("pcg", 2, pcg_solve(L, W, cap, pcg_grid, s, mode, opt.pcg_tolerance, d_weights));
-    int it[2] = {0, 0};
-    RPBA_CUDA_CHECK(cudaMemcpyAsync(it, W.iters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
-    RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
-    learned_iters += it[0];
-    const bool ok = mode == 1 ? it[1] != 0 : it[0] < cap;
+    // The coarse operator is rebuilt whenever the observation weights or
+    // the structure changed (every step of the robust pass: reweighting
+    // rescales S); in the refinement pass the operator of an earlier
+    // linearisation is reused -- any SPD coarse operator keeps M SPD -- with
+    // the iteration cap cut to three times the iterations of its first use.
+    // If a reused operator misses that cap, it is rebuilt and the solve
+    // repeated.
+    const CoarseWork *cw = ensure_coarse();
+    int it[3] = {0, 0, 0};
+    bool fresh = false;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+      if (cw && (coarse_stale || attempt > 0)) {
+        const double nc = CW.nc;
+        prof.next_bytes = (Nc + 2. * Nb) * 648 + 3. * nc * nc * 8;
+        PROF("coarse_setup", 1, coarse_setup(L, CW, s));
+        coarse_stale = false;
+        fresh = true;
+      }
+      const int cap_try = (cw && !fresh) ? std::min(cap, 3 * coarse_ref_iters + 20) : cap;
+      PROF("pcg", 2, pcg_solve(L, W, cap_try, pcg_grid, s, mode, opt.pcg_tolerance, d_weights, cw));
+      RPBA_CUDA_CHECK(cudaMemcpyAsync(it, W.iters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+      if (cw) RPBA_CUDA_CHECK(cudaMemcpyAsync(it + 2, CW.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+      RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+      learned_iters += it[0];
+      if (fresh) coarse_ref_iters = it[0];
+      const bool conv = (mode == 1 ? it[1] != 0 : it[0] < cap_try) && it[2] == 0;
+      if (conv || fresh || !cw) break;
+      ++rep.coarse_rebuilds;
+    }
+    const bool ok = (mode == 1 ? it[1] != 0 : it[0] < cap) && it[2] == 0;
+    if (opt.verbose & 4) {
+      char line[128];
+      std::snprintf(line, sizeof line, "PCG: iterations %d converged %d coarse %d status %d\n", it[0], it[1],
+                    cw ? CW.nagg : 0, it[2]);
+      log += line;
+    }
     if (!ok) {
       ++rep.pcg_fallbacks;
       ensure_direct();
@@ -647,8 +694,11 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
     PROF("pcg", 2, pcg_solve(L, W, msize, pcg_grid, s));
     pcg_pending = true;
   }
-  if (rec_T)
-    learned_record(L, DW, W.xbest, rec_seed + 104729ull * (unsigned long long)rep.linear_solves, *rec_T, *rec_H, s);
+  if (rec_T) {
+    const CoarseWork *cw = ensure_coarse();
+    if (cw) coarse_setup(L, CW, s);
+    learned_record(L, cw, W.xbest, rec_seed + 104729ull * (unsigned long long)rep.linear_solves, *rec_T, *rec_H, s);
+  }
   PROF("backsub", 1, launch_backsub(L, W.xbest, s));
   PROF("xcam", 1, launch_xcam(L, W.xbest, s));
   PROF("update", 1, launch_update(L, nrunknowns, s));
@@ -743,6 +793,7 @@ int rpba_handle::adjust() {
         nrunknowns = nunk_given;
         nrobs = nobs_given;
         PROF("reweight", 3, launch_reweight(L, iflag, vals, sig00v, nflag, s));
+        coarse_stale = true;
         int nf = 0;
         RPBA_CUDA_CHECK(cudaMemcpyAsync(&nf, nflag, sizeof(int), cudaMemcpyDeviceToHost, s));
         wsum = seq_sum(L.o_wterm, L.nobs);
@@ -1156,6 +1207,7 @@ struct TrainAlloc {
     T.ent = dalloc<int2>(ents_cap, own);
     T.blocks = dalloc<float>((size_t)blocks_cap * 81, own);
     T.sys_row = dalloc<int>((size_t)sys_cap + 1, own);
+    T.uc = nullptr;
     H.ents_cap = ents_cap;
     H.blocks_cap = blocks_cap;
     H.sys_cap = sys_cap;
@@ -1208,6 +1260,10 @@ int32_t rpba_precond_loss_grad(const rpba_precond_set *set, const float *weights
     up(T.ent, ent.data(), sizeof(int2) * S.nent);
     up(T.blocks, S.blocks, sizeof(float) * (size_t)S.nblocks * 81);
     up(T.sys_row, S.sys_row, sizeof(int) * (S.systems + 1));
+    if (S.uc) {
+      T.uc = dalloc<float>((size_t)S.probes * S.rows * 9, TA.own);
+      up(T.uc, S.uc, sizeof(float) * (size_t)S.probes * S.rows * 9);
+    }
     TA.bufs();
     float *dw = dalloc<float>(NN_WEIGHTS, TA.own);
     up(dw, a->w, sizeof(float) * NN_WEIGHTS);
@@ -1239,6 +1295,9 @@ int32_t rpba_train_preconditioner(const rpba_block *scenes, int32_t nscenes, con
     const int rows_cap = t.max_samples > 0 ? t.max_samples : 1 << 18;
     TrainAlloc TA;
     TA.alloc(rows_cap, rows_cap * 96, rows_cap * 48, 4096, probes);
+    TA.T.uc = dalloc<float>((size_t)probes * rows_cap * 9, TA.own);
+    TA.H.vb = dalloc<double>(((size_t)rows_cap + 1) * 9, TA.own);
+    TA.H.vz = dalloc<double>(((size_t)rows_cap + 1) * 9, TA.own);
     // 1. systems of the direct solver's own LM iterations
     for (int i = 0; i < a->ns; ++i) {
       rpba_options o = *a->o;
@@ -1278,14 +1337,32 @@ int32_t rpba_train_preconditioner(const rpba_block *scenes, int32_t nscenes, con
     RPBA_CUDA_CHECK(cudaMemcpy(W, w0.data(), sizeof(float) * NN_WEIGHTS, cudaMemcpyHostToDevice));
     RPBA_CUDA_CHECK(cudaMemset(m, 0, sizeof(float) * NN_WEIGHTS));
     RPBA_CUDA_CHECK(cudaMemset(v, 0, sizeof(float) * NN_WEIGHTS));
+    // Adam with a cosine learning-rate decay; the weights with the lowest
+    // training loss seen are returned (the untrained network, plain
+    // block-Jacobi, is the first candidate)
+    float *Wbest = dalloc<float>(NN_WEIGHTS, TA.own);
     float loss0 = 0.f, err0 = 0.f, loss1 = 0.f, err1 = 0.f;
     learned_loss_grad(T, W, TA.B, &loss0, &err0, 0);
+    RPBA_CUDA_CHECK(cudaMemcpy(Wbest, W, sizeof(float) * NN_WEIGHTS, cudaMemcpyDeviceToDevice));
+    float best = loss0;
     const int steps = t.steps > 0 ? t.steps : 300;
     const float lr = t.lr > 0.f ? t.lr : 3e-3f;
     for (int st = 0; st < steps; ++st) {
-      learned_loss_grad(T, W, TA.B, nullptr, nullptr, 0);
-      learned_adam(W, m, v, TA.B.grad, lr, st + 1, 0);
+      float l = 0.f;
+      learned_loss_grad(T, W, TA.B, &l, nullptr, 0);
+      if (st > 0 && l < best) {
+        best = l;
+        RPBA_CUDA_CHECK(cudaMemcpy(Wbest, W, sizeof(float) * NN_WEIGHTS, cudaMemcpyDeviceToDevice));
+      }
+      const float lr_t = lr * 0.5f * (1.f + std::cos(3.14159265f * (float)st / (float)steps));
+      learned_adam(W, m, v, TA.B.grad, lr_t, st + 1, 0);
     }
+    {
+      float l = 0.f;
+      learned_loss_grad(T, W, TA.B, &l, nullptr, 0);
+      if (l < best) RPBA_CUDA_CHECK(cudaMemcpy(Wbest, W, sizeof(float) * NN_WEIGHTS, cudaMemcpyDeviceToDevice));
+    }
+    W = Wbest;
     learned_loss_grad(T, W, TA.B, &loss1, &err1, 0);
     std::vector<float> wout(NN_WEIGHTS);
     RPBA_CUDA_CHECK(cudaMemcpy(wout.data(), W, sizeof(float) * NN_WEIGHTS, cudaMemcpyDeviceToHost));

@@ -171,12 +171,15 @@ def precond_loss_grad(ts: dict, weights):
     i32 = lambda k: np.ascontiguousarray(ts[k], np.int32)
     keep = {k: f32(k) for k in ("features", "sinv", "b", "xs", "blocks")}
     keep.update({k: i32(k) for k in ("np", "sys", "rowoff", "ent_col", "ent_blk", "sys_row")})
+    if ts.get("uc") is not None:
+        keep["uc"] = f32("uc")
     fp, ip = C.POINTER(C.c_float), C.POINTER(C.c_int32)
     st = RpbaPrecondSetC(int(ts["rows"]), int(ts["systems"]), int(ts["probes"]), int(keep["ent_col"].size),
                          int(keep["blocks"].shape[0]),
                          *(keep[k].ctypes.data_as(fp) for k in ("features", "sinv", "b", "xs")),
                          *(keep[k].ctypes.data_as(ip) for k in ("np", "sys", "rowoff", "ent_col", "ent_blk")),
-                         keep["blocks"].ctypes.data_as(fp), keep["sys_row"].ctypes.data_as(ip))
+                         keep["blocks"].ctypes.data_as(fp), keep["sys_row"].ctypes.data_as(ip),
+                         keep["uc"].ctypes.data_as(fp) if "uc" in keep else None)
     w = np.ascontiguousarray(weights, np.float32)
     loss = C.c_float()
     g = np.zeros(PRECOND_WEIGHTS, np.float32)

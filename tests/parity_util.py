@@ -45,9 +45,23 @@ def same_tracks(a, b):
 SIGMA_RTOL = 1e-5  # printed float sigma0: a few float ulps of the cost sum
 
 
-def same_log(a: str, b: str) -> bool:
+def log_float_dev(a: str, b: str) -> float:
+    """Largest relative difference between the float words of two logs with
+    the same layout (0 when the layouts differ)."""
+    dev = 0.0
+    for x, y in zip(a.strip().splitlines(), b.strip().splitlines()):
+        for u, v in zip(x.split(), y.split()):
+            if u != v and any(c in u + v for c in ".e"):
+                try:
+                    dev = max(dev, abs(float(u) - float(v)) / max(abs(float(v)), 1e-30))
+                except ValueError:
+                    pass
+    return dev
+
+
+def same_log(a: str, b: str, rtol: float = SIGMA_RTOL) -> bool:
     """Log lines agree: words equal, numbers with a '.' or 'e' within
-    SIGMA_RTOL, integers exactly."""
+    rtol (default SIGMA_RTOL), integers exactly."""
     la, lb = a.strip().splitlines(), b.strip().splitlines()
     if len(la) != len(lb):
         return False
@@ -62,6 +76,6 @@ def same_log(a: str, b: str) -> bool:
                 fu, fv = float(u), float(v)
             except ValueError:
                 return False
-            if not any(c in u + v for c in ".e") or abs(fu - fv) > SIGMA_RTOL * max(abs(fv), 1e-30):
+            if not any(c in u + v for c in ".e") or abs(fu - fv) > rtol * max(abs(fv), 1e-30):
                 return False
     return True

@@ -4,7 +4,8 @@ import numpy as np
 import pytest
 
 from rpba_b200 import scenes
-from tests.parity_util import (COST_RTOL, PARAM_RTOL, EXTEVAL_ATOL, param_errors, same_tracks, same_log)
+from tests.parity_util import (COST_RTOL, PARAM_RTOL, SIGMA_RTOL, EXTEVAL_ATOL, param_errors, same_tracks,
+                               same_log, log_float_dev)
 
 pytestmark = pytest.mark.gpu
 
@@ -22,14 +23,21 @@ def _run_pair(oracle_mod, blk, **kw):
 
 
 def _self_sensitivity(oracle_mod, blk, o, **kw):
-    """How far the oracle moves when only the SpMV summation order changes:
-    the reference's inexact PCG (loose 1e5 stop rule) amplifies roundoff, so
-    no reordered implementation can agree with it more closely than this."""
+    """How far the oracle moves when only the SpMV summation order changes
+    (two reorderings, the larger deviation): the reference's inexact PCG
+    (loose 1e5 stop rule) amplifies roundoff, so no reordered implementation
+    can agree with it more closely than this.  Returns (cost, parameters,
+    printed sigma0) relative deviations."""
     import rpba_b200 as rb
-    st_v, blk_v, rep_v, _ = oracle_mod.calc_plsa_variant(blk, rb.make_options(**kw))
-    _, blk_o, rep_o, _ = o
-    cost = abs(rep_v["cost"] - rep_o["cost"]) / abs(rep_o["cost"])
-    return cost, param_errors(blk_v, blk_o)
+    _, blk_o, rep_o, log_o = o
+    cost, params, sigma = 0.0, None, 0.0
+    for variant in (1, 2):
+        st_v, blk_v, rep_v, log_v = oracle_mod.calc_plsa_variant(blk, rb.make_options(**kw), variant=variant)
+        cost = max(cost, abs(rep_v["cost"] - rep_o["cost"]) / abs(rep_o["cost"]))
+        pe = param_errors(blk_v, blk_o)
+        params = pe if params is None else {k: max(params[k], pe[k]) for k in pe}
+        sigma = max(sigma, log_float_dev(log_v, log_o))
+    return cost, params, sigma
 
 
 def _check(o, g, sens=None):
@@ -42,7 +50,8 @@ def _check(o, g, sens=None):
     # identical decisions: the integer fields of every log line (redundancy,
     # observations, unknowns, IT, ITT) match exactly; the printed sigma0
     # values are float sums and may differ in the last printed digit.
-    assert same_log(log_g, log_o), f"\nGPU:\n{log_g}\nORACLE:\n{log_o}"
+    sigma_tol = SIGMA_RTOL if sens is None else max(SIGMA_RTOL, 4 * sens[2])
+    assert same_log(log_g, log_o, sigma_tol), f"\nGPU:\n{log_g}\nORACLE:\n{log_o}"
     for k in ("linear_solves", "obs_deleted", "points_deleted", "points_used", "passes_done"):
         assert rep_g[k] == rep_o[k], (k, rep_g[k], rep_o[k])
     cost_rel = abs(rep_g["cost"] - rep_o["cost"]) / abs(rep_o["cost"])
