@@ -246,6 +246,23 @@ typedef struct rpba_precond_set {
   const float *uc;         /* [probes][rows][9] coarse part of the
                               preconditioned right-hand sides, or NULL     */
 } rpba_precond_set;
+/* Caller-allocated host buffers for rpba_record_systems: capacities in,
+ * counts out; the arrays have the layout of rpba_precond_set; NULL arrays
+ * are skipped. */
+typedef struct rpba_precond_buffers {
+  int32_t rows_cap, ents_cap, blocks_cap, systems_cap;
+  int32_t rows, systems, probes, nent, nblocks;
+  float *features, *sinv, *b, *xs, *blocks, *uc;
+  int32_t *np, *sys, *rowoff, *ent_col, *ent_blk, *sys_row;
+} rpba_precond_buffers;
+/* The training set rpba_train_preconditioner would train on (the direct
+ * solver's systems for the scenes, diagonally scaled), copied to the host:
+ * for checking the recording and the training objective independently.
+ * RPBA_ERR_TOO_LARGE when a capacity is short (the counts say how much is
+ * needed).  No counterpart in the reference. */
+int32_t rpba_record_systems(const rpba_block *scenes, int32_t nscenes, const rpba_options *opt,
+                            const rpba_train_options *topt, rpba_precond_buffers *out);
+
 /* Training loss and its gradient for `weights`, computed by the GPU's
  * training kernels (for checking against an independent implementation).
  * No counterpart in the reference. */
@@ -260,7 +277,7 @@ int32_t rpba_precond_loss_grad(const rpba_precond_set *set, const float *weights
  * stream) and the call returns without waiting for it.  Scratch lives in one
  * static device array of the library (about 20 KB, held by every GPU that
  * loads the library until the process exits), which caps n at 4,194,304
- * (1024 CTAs x 4096 elements): larger n returns RPBA_ERR_TOO_LARGE.  The first
+ * (512 CTAs x 8192 elements): larger n returns RPBA_ERR_TOO_LARGE.  The first
  * call on a device looks up that array's device address (a blocking runtime
  * query), so make the first call on each device before any stream capture.
  * All calls share the one array: calls that overlap on the GPU (different

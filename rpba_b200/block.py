@@ -106,6 +106,14 @@ class RpbaPrecondSetC(C.Structure):
                 ("blocks", _f32p), ("sys_row", _i32p), ("uc", _f32p)]
 
 
+class RpbaPrecondBuffersC(C.Structure):
+    _fields_ = [("rows_cap", C.c_int32), ("ents_cap", C.c_int32), ("blocks_cap", C.c_int32),
+                ("systems_cap", C.c_int32), ("rows", C.c_int32), ("systems", C.c_int32), ("probes", C.c_int32),
+                ("nent", C.c_int32), ("nblocks", C.c_int32), ("features", _f32p), ("sinv", _f32p), ("b", _f32p),
+                ("xs", _f32p), ("blocks", _f32p), ("uc", _f32p), ("np", _i32p), ("sys", _i32p),
+                ("rowoff", _i32p), ("ent_col", _i32p), ("ent_blk", _i32p), ("sys_row", _i32p)]
+
+
 PRECOND_WEIGHTS = 1865
 SOLVER_PCG, SOLVER_DIRECT, SOLVER_LEARNED = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1

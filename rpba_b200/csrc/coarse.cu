@@ -20,6 +20,8 @@
 // (d 3, t 3, s, and common shifts of k1, k2, f): CO_M = 10.
 //
 // Everything here is deterministic: every sum has a fixed order.
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <numeric>
 #include <vector>
@@ -91,67 +93,100 @@ __global__ void k_coarse_P(DevLSA L, CoarseWork C) {
   }
 }
 
-// Galerkin matrix, one CTA per aggregate a: the strip A_c[a rows][:] is
-// accumulated in shared memory.  Coarse column c of the strip belongs to warp
-// c % 32, which walks the aggregate's rows and their entries in order and
-// adds, for each entry (k, l) with l in aggregate b, column j of
-// P_k^T S_kl P_l to column c = 10 b + j.  Every strip element therefore has
-// one owner and one summation order: the result does not depend on
-// scheduling, and no synchronisation is needed inside the walk.
-constexpr int AS_T = 1024;
-__global__ void __launch_bounds__(AS_T) k_coarse_assemble(DevLSA L, CoarseWork C) {
-  extern __shared__ double strip[];  // [CO_M][nc]
-  const int nc = C.nc;
-  const int a = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int i = tid; i < CO_M * nc; i += AS_T) strip[i] = 0.;
-  __syncthreads();
-  for (int t = C.agg_off[a]; t < C.agg_off[a + 1]; ++t) {
-    const int k = C.agg_rows[t];
-    const int e0 = L.rowoff[k], e1 = L.rowoff[k + 1];
-    const int npk = L.camparv[k + 1] - L.camparv[k];
-    const double *Pk = C.P + (size_t)k * CP;
-    for (int c0 = e0; c0 < e1; c0 += 32) {
-      // which of the next 32 entries have a column of this warp
-      int b = -1, j = 32;
-      int2 en = make_int2(0, 0);
-      if (c0 + lane < e1) {
-        en = L.ent[c0 + lane];
-        b = C.row_agg[en.x];
-        if (b >= 0) j = ((warp - b * CO_M) % 32 + 32) % 32;
-      }
-      unsigned m = __ballot_sync(0xffffffffu, b >= 0 && j < CO_M);
-      while (m) {
-        const int src = __ffs(m) - 1;
-        m &= m - 1;
-        const int bb = __shfl_sync(0xffffffffu, b, src), jj = __shfl_sync(0xffffffffu, j, src);
-        const int l = __shfl_sync(0xffffffffu, en.x, src), ey = __shfl_sync(0xffffffffu, en.y, src);
-        const bool tr = ey < 0;
-        const double *B = L.blocks + (size_t)(ey & 0x7fffffff) * 81;
-        const double *Pl = C.P + (size_t)l * CP;
-        const int npl = L.camparv[l + 1] - L.camparv[l];
-        // u_p = sum_q S_kl[p][q] P_l[q][jj]   (lane p < npk)
-        double u = 0.;
-        if (lane < npk)
-          for (int q = 0; q < npl; ++q) u += (tr ? B[q * 9 + lane] : B[lane * 9 + q]) * Pl[q * CO_M + jj];
-        // v_i = sum_p P_k[p][i] u_p            (lane i < CO_M)
-        double v = 0.;
-        for (int p = 0; p < 9; ++p) {
-          const double up = __shfl_sync(0xffffffffu, u, p);
-          if (lane < CO_M && p < npk) v += Pk[p * CO_M + lane] * up;
-        }
-        if (lane < CO_M) strip[lane * nc + bb * CO_M + jj] += v;
-      }
+// Galerkin matrix A_c = P^T S P in three deterministic steps.
+//  1. The entries (k, l) of every row are sorted by (k, aggregate of l)
+//     (a stable sort: entry order inside a run), once per structure.
+//  2. One warp per run (row k, aggregate b): Y = sum_l S_kl P_l (9 x 10),
+//     Z = P_k^T Y (10 x 10).
+//  3. The runs sorted by (aggregate of k, b) (stable: row order); one warp
+//     per coarse block (a, b) sums its runs' Z in that order.
+__global__ void k_entry_keys(DevLSA L, CoarseWork C, unsigned *key, int *val) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= L.nimg) return;
+  for (int e = L.rowoff[k]; e < L.rowoff[k + 1]; ++e) {
+    const int b = C.row_agg[L.ent[e].x];
+    key[e] = b < 0 ? 0xffffffffu : (unsigned)k * (unsigned)C.nagg + (unsigned)b;
+    val[e] = e;
+  }
+}
+
+constexpr int RS_T = 256;
+__global__ void __launch_bounds__(RS_T) k_coarse_runs(DevLSA L, CoarseWork C, int nruns) {
+  __shared__ double Ysh[RS_T / 32][9 * CO_M];
+  const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  if (r >= nruns) return;
+  const int k = (int)(C.run_key[r] / (unsigned)C.nagg);
+  const int npk = L.camparv[k + 1] - L.camparv[k];
+  double y[3] = {0., 0., 0.};
+  for (int t = C.run_off[r]; t < C.run_off[r + 1]; ++t) {
+    const int2 en = L.ent[C.ent_sorted[t]];
+    const int l = en.x;
+    const bool tr = en.y < 0;
+    const size_t B = (size_t)(en.y & 0x7fffffff) * 81;
+    const double *Pl = C.P + (size_t)l * CP;
+    const int npl = L.camparv[l + 1] - L.camparv[l];
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const int o = lane + 32 * m, p = o / CO_M, j = o % CO_M;
+      if (o < 9 * CO_M && p < npk)
+        for (int q = 0; q < npl; ++q) y[m] += blk_at(L, B + (tr ? q * 9 + p : p * 9 + q)) * Pl[q * CO_M + j];
     }
   }
-  __syncthreads();
-  // a coarse unknown that no parameter carries (an intrinsic that is not
-  // estimated) has an empty row and column: give it a unit diagonal
-  if (tid < CO_M) {
-    double &d = strip[tid * nc + a * CO_M + tid];
-    if (d == 0.) d = 1.;
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const int o = lane + 32 * m;
+    if (o < 9 * CO_M) Ysh[wl][o] = y[m];
   }
-  __syncthreads();
-  for (int i = tid; i < CO_M * nc; i += AS_T) C.Ac[(size_t)(a * CO_M + i / nc) * nc + i % nc] = strip[i];
+  __syncwarp();
+  const double *Pk = C.P + (size_t)k * CP;
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const int o = lane + 32 * m, i = o / CO_M, j = o % CO_M;
+    if (o < CO_M * CO_M) {
+      double z = 0.;
+      for (int p = 0; p < npk; ++p) z += Pk[p * CO_M + i] * Ysh[wl][p * CO_M + j];
+      C.Z[(size_t)r * CO_M * CO_M + o] = z;
+    }
+  }
+}
+
+__global__ void k_run_keys2(CoarseWork C, int nruns, unsigned *key2, int *idx) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nruns) return;
+  const unsigned key = C.run_key[r];
+  const int k = (int)(key / (unsigned)C.nagg), b = (int)(key % (unsigned)C.nagg);
+  key2[r] = (unsigned)C.row_agg[k] * (unsigned)C.nagg + (unsigned)b;
+  idx[r] = r;
+}
+
+__global__ void k_coarse_blocks(CoarseWork C, int nsegs) {
+  const int sg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (sg >= nsegs) return;
+  const unsigned key = C.seg_key[sg];
+  const int a = (int)(key / (unsigned)C.nagg), b = (int)(key % (unsigned)C.nagg);
+  double acc[4] = {0., 0., 0., 0.};
+  for (int t = C.seg_off[sg]; t < C.seg_off[sg + 1]; ++t) {
+    const double *Z = C.Z + (size_t)C.run_sorted[t] * CO_M * CO_M;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+      const int o = lane + 32 * m;
+      if (o < CO_M * CO_M) acc[m] += Z[o];
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < 4; ++m) {
+    const int o = lane + 32 * m, i = o / CO_M, j = o % CO_M;
+    if (o < CO_M * CO_M) C.Ac[(size_t)(a * CO_M + i) * C.nc + b * CO_M + j] = acc[m];
+  }
+}
+
+// a coarse unknown that no parameter carries (an intrinsic that is not
+// estimated) has an empty row and column: give it a unit diagonal
+__global__ void k_coarse_fixdiag(CoarseWork C) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= C.nc) return;
+  double &d = C.Ac[(size_t)i * C.nc + i];
+  if (d == 0.) d = 1.;
 }
 
 // Symmetric Jacobi scaling of A_c before the factorisation (the coarse
@@ -315,20 +350,114 @@ void coarse_build(const DevLSA &L, int max_aggs, CoarseWork &C, std::vector<void
   RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
 }
 
-void coarse_setup(const DevLSA &L, const CoarseWork &C, cudaStream_t s) {
+template <class T>
+T *grow(T *&p, size_t &cap, size_t n) {
+  if (n > cap) {
+    if (p) cudaFree(p);
+    p = nullptr;
+    RPBA_CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+    cap = n;
+  }
+  return p;
+}
+
+void coarse_setup(const DevLSA &L, CoarseWork &C, int structure_version, cudaStream_t s) {
   if (C.nagg <= 0) return;
   RPBA_CUDA_CHECK(cudaMemsetAsync(C.err, 0, sizeof(int), s));
   k_coarse_P<<<C.nagg, 128, 0, s>>>(L, C);
-  const size_t smem = sizeof(double) * (size_t)CO_M * C.nc;
-  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_coarse_assemble, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_coarse_assemble<<<C.nagg, AS_T, smem, s>>>(L, C);
-  const long long nn = (long long)C.nc * C.nc;
+  if (C.built_version != structure_version) {
+    // runs (row, aggregate of the column) and coarse blocks (a, b): once per
+    // structure
+    int nent = 0;
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(&nent, L.rowoff + L.nimg, sizeof(int), cudaMemcpyDeviceToHost, s));
+    RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+    unsigned *k1 = grow(C.ekey, C.ekey_cap, (size_t)nent), *k2 = grow(C.ekey2, C.ekey2_cap, (size_t)nent);
+    int *v1 = grow(C.eval, C.eval_cap, (size_t)nent);
+    grow(C.ent_sorted, C.ent_sorted_cap, (size_t)nent);
+    grow(C.run_key, C.run_key_cap, (size_t)nent);
+    grow(C.run_cnt, C.run_cnt_cap, (size_t)nent + 1);
+    grow(C.run_off, C.run_off_cap, (size_t)nent + 1);
+    grow(C.counts, C.counts_cap, 2);
+    k_entry_keys<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, C, k1, v1);
+    size_t need = 0, b1 = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, b1, k1, k2, v1, C.ent_sorted, nent, 0, 32, s);
+    need = std::max(need, b1);
+    cub::DeviceRunLengthEncode::Encode(nullptr, b1, k2, C.run_key, C.run_cnt, C.counts, nent, s);
+    need = std::max(need, b1);
+    cub::DeviceScan::ExclusiveSum(nullptr, b1, C.run_cnt, C.run_off, nent + 1, s);
+    need = std::max(need, b1);
+    void *tmp = grow(C.cub_tmp, C.cub_tmp_cap, need);
+    RPBA_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(tmp, need, k1, k2, v1, C.ent_sorted, nent, 0, 32, s));
+    size_t bb = C.cub_tmp_cap;
+    RPBA_CUDA_CHECK(cub::DeviceRunLengthEncode::Encode(tmp, bb, k2, C.run_key, C.run_cnt, C.counts, nent, s));
+    int nr = 0;
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(&nr, C.counts, sizeof(int), cudaMemcpyDeviceToHost, s));
+    RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+    // the entries whose column lies outside the coarse space sort last
+    unsigned lastkey = 0;
+    if (nr > 0)
+      RPBA_CUDA_CHECK(cudaMemcpy(&lastkey, C.run_key + nr - 1, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (nr > 0 && lastkey == 0xffffffffu) --nr;
+    RPBA_CUDA_CHECK(cudaMemsetAsync(C.run_cnt + nr, 0, sizeof(int), s));
+    bb = C.cub_tmp_cap;
+    RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(tmp, bb, C.run_cnt, C.run_off, nr + 1, s));
+    C.nruns = nr;
+    // coarse blocks
+    unsigned *q1 = grow(C.rkey, C.rkey_cap, (size_t)nr), *q2 = grow(C.rkey2, C.rkey2_cap, (size_t)nr);
+    int *w1 = grow(C.ridx, C.ridx_cap, (size_t)nr);
+    grow(C.run_sorted, C.run_sorted_cap, (size_t)nr);
+    grow(C.seg_key, C.seg_key_cap, (size_t)nr);
+    grow(C.seg_cnt, C.seg_cnt_cap, (size_t)nr + 1);
+    grow(C.seg_off, C.seg_off_cap, (size_t)nr + 1);
+    grow(C.Z, C.Z_cap, (size_t)std::max(nr, 1) * CO_M * CO_M);
+    if (nr > 0) {
+      k_run_keys2<<<(nr + 255) / 256, 256, 0, s>>>(C, nr, q1, w1);
+      need = 0;
+      cub::DeviceRadixSort::SortPairs(nullptr, b1, q1, q2, w1, C.run_sorted, nr, 0, 32, s);
+      need = std::max(need, b1);
+      cub::DeviceRunLengthEncode::Encode(nullptr, b1, q2, C.seg_key, C.seg_cnt, C.counts + 1, nr, s);
+      need = std::max(need, b1);
+      cub::DeviceScan::ExclusiveSum(nullptr, b1, C.seg_cnt, C.seg_off, nr + 1, s);
+      need = std::max(need, b1);
+      tmp = grow(C.cub_tmp, C.cub_tmp_cap, need);
+      bb = C.cub_tmp_cap;
+      RPBA_CUDA_CHECK(cub::DeviceRadixSort::SortPairs(tmp, bb, q1, q2, w1, C.run_sorted, nr, 0, 32, s));
+      bb = C.cub_tmp_cap;
+      RPBA_CUDA_CHECK(cub::DeviceRunLengthEncode::Encode(tmp, bb, q2, C.seg_key, C.seg_cnt, C.counts + 1, nr, s));
+      int ns = 0;
+      RPBA_CUDA_CHECK(cudaMemcpyAsync(&ns, C.counts + 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+      RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+      RPBA_CUDA_CHECK(cudaMemsetAsync(C.seg_cnt + ns, 0, sizeof(int), s));
+      bb = C.cub_tmp_cap;
+      RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(tmp, bb, C.seg_cnt, C.seg_off, ns + 1, s));
+      C.nsegs = ns;
+    } else {
+      C.nsegs = 0;
+    }
+    C.built_version = structure_version;
+  }
+  const size_t nn = (size_t)C.nc * C.nc;
+  RPBA_CUDA_CHECK(cudaMemsetAsync(C.Ac, 0, sizeof(double) * nn, s));
+  if (C.nruns > 0) {
+    k_coarse_runs<<<(C.nruns + RS_T / 32 - 1) / (RS_T / 32), RS_T, 0, s>>>(L, C, C.nruns);
+    k_coarse_blocks<<<(C.nsegs + 7) / 8, 256, 0, s>>>(C, C.nsegs);
+  }
+  k_coarse_fixdiag<<<(C.nc + 255) / 256, 256, 0, s>>>(C);
   k_coarse_diag<<<(C.nc + 255) / 256, 256, 0, s>>>(C);
   k_coarse_scale<<<(int)((nn + 255) / 256), 256, 0, s>>>(C.Ac, C.dsc, C.nc, 1);
   dense_cholesky(C.Ac, C.nc, C.Linv, C.err, s);
   dense_spd_inverse(C.Ac, C.nc, C.Linv, C.X, C.Ainv, s);
   k_coarse_scale<<<(int)((nn + 255) / 256), 256, 0, s>>>(C.Ainv, C.dsc, C.nc, 0);
   RPBA_CUDA_CHECK(cudaGetLastError());
+}
+
+void coarse_release(CoarseWork &C) {
+  for (void *p : {(void *)C.ekey, (void *)C.ekey2, (void *)C.eval, (void *)C.ent_sorted, (void *)C.run_key,
+                  (void *)C.run_cnt, (void *)C.run_off, (void *)C.counts, (void *)C.rkey, (void *)C.rkey2,
+                  (void *)C.ridx, (void *)C.run_sorted, (void *)C.seg_key, (void *)C.seg_cnt, (void *)C.seg_off,
+                  (void *)C.Z, (void *)C.cub_tmp})
+    if (p) cudaFree(p);
+  C = CoarseWork{};
 }
 
 void coarse_apply(const DevLSA &L, const CoarseWork &C, const double *r, double *h, cudaStream_t s) {

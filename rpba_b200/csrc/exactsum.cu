@@ -4,16 +4,19 @@
 //
 // Method.  Let s be the running float sum, s in [2^E, 2^(E+1)), u = ulp(s) =
 // 2^(E-23), S = s/u (an integer in [2^23, 2^24)).  For v >= 0 with
-// S + floor(v/u) < 2^24 the float addition is fl(s + v) = s + u*rne(v/u),
-// and rne(v/u) does not depend on s unless v/u is exactly halfway between
-// integers (a tie, where round-half-even looks at the parity of S).  So
-// inside one binade a whole run of additions is an exact integer prefix sum
-// of r_k = rne(v_k/u).  The run ends at the first element k with a tie or
-// with S + R_(k-1) + floor(v_k/u) >= 2^24 (the sum leaves the binade); that
-// single element is added with a real float addition, and a new run starts
-// with the new binade.  Runs are few (the sum leaves a binade only when it
-// doubles; ties have probability ~ v/s), so the loop takes a handful of grid
-// passes instead of n dependent additions.
+// S + floor(v/u) < 2^24 the float addition is fl(s + v) = s + u*rne(v/u)
+// with rne(v/u) = floor(v/u) + [frac > 1/2], except when v/u is exactly
+// halfway between integers (a tie): then round-half-even gives
+// floor(v/u) + [S + floor(v/u) odd], and the new S is even.  So inside one
+// binade each element acts on the parity p of the running integer sum as a
+// two-state transform  p -> (increment r(p), new parity q(p)), and a run of
+// elements is the composition of their transforms, an associative operation:
+// a grid-wide scan of per-thread and per-CTA composites gives every prefix
+// without a sequential pass, ties included.  A run ends only at the first
+// element k with S + R_(k-1) + floor(v_k/u) >= 2^24 (the sum leaves the
+// binade); that element is added with a real float addition and a new run
+// starts in the new binade.  Runs are few: the sum leaves a binade only when
+// it doubles.
 //
 // The first HEAD elements and any stretch where s is zero or subnormal are
 // added by one warp in plain sequence.  Inputs must be finite and >= 0.
@@ -37,12 +40,40 @@ struct EsCtl {
   int i;      // next element
 };
 
+// Composite transform of a run of elements for incoming parity 0 and 1:
+// total increment R, outgoing parity q, and M = max over the run of
+// (increment before the element + floor(v/u)), the crossing test.
+struct Xf {
+  long long R[2], M[2];
+  int q[2];
+};
+__device__ __forceinline__ Xf xf_identity() {
+  Xf x;
+  for (int p = 0; p < 2; ++p) {
+    x.R[p] = 0;
+    x.M[p] = LLONG_MIN;
+    x.q[p] = p;
+  }
+  return x;
+}
+// a then b
+__device__ __forceinline__ Xf xf_then(const Xf &a, const Xf &b) {
+  Xf x;
+  for (int p = 0; p < 2; ++p) {
+    const int m = a.q[p];
+    x.R[p] = a.R[p] + b.R[m];
+    x.q[p] = b.q[m];
+    x.M[p] = b.M[m] == LLONG_MIN ? a.M[p] : max(a.M[p], a.R[p] + b.M[m]);
+  }
+  return x;
+}
+
 struct EsArgs {
   const float *v;
   int n;
   float *out;
-  long long *Rc, *Mc;  // per CTA: sum of r, max of (exclusive prefix + floor)
-  int *Tc;             // per CTA: first tie index (INT_MAX if none)
+  long long *Rc, *Mc;  // per CTA composite: R[2], M[2]
+  int *Tc;             // per CTA composite: q[2]
   EsCtl *ctl;
   unsigned *bar;
   int *err;
@@ -60,6 +91,17 @@ __device__ __forceinline__ void classify(float v, double scale, long long &fl, l
   fl = (long long)ff;
   tie = fr == 0.5;
   r = fl + (fr > 0.5 ? 1 : 0);
+}
+
+// Apply one element to a composite (in place, both incoming parities).
+__device__ __forceinline__ void xf_push(Xf &x, long long fl, long long r, bool tie) {
+  for (int p = 0; p < 2; ++p) {
+    const long long m = x.R[p] + fl;
+    if (m > x.M[p]) x.M[p] = m;
+    const long long rr = tie ? fl + ((x.q[p] + fl) & 1) : r;
+    x.R[p] += rr;
+    x.q[p] = (int)((x.q[p] + rr) & 1);
+  }
 }
 
 // Sequential float additions of v[i..i_end) onto s by one warp.
@@ -83,14 +125,9 @@ __global__ void __launch_bounds__(ES_T) k_exact_sum(EsArgs A) {
   const int chunk = (n + G - 1) / G;
   const int lo = min(n, c * chunk), hi = min(n, lo + chunk);
   const int per = (chunk + ES_T - 1) / ES_T;
-  __shared__ long long s_off[ES_T];  // per-thread exclusive offsets within the chunk
-  __shared__ long long s_tsum[ES_T];
-  __shared__ long long s_tmax[ES_T];
-  __shared__ int s_ttie[ES_T];
-  __shared__ long long s_roff;       // exclusive prefix of r over earlier chunks
-  __shared__ int s_cx, s_ct, s_tmin;
-  __shared__ long long s_rtot;
-  __shared__ int s_kx;
+  __shared__ Xf s_x[ES_T];  // per-thread composites of the current run
+  __shared__ long long s_rtot, s_R;
+  __shared__ int s_cx, s_qx, s_tcross, s_q;
 
   if (c == 0 && tid < 32) {
     float s = warp_seq(A.v, 0, min(n, HEAD), 0.f);
@@ -112,8 +149,8 @@ __global__ void __launch_bounds__(ES_T) k_exact_sum(EsArgs A) {
     const int i0 = __ldcg(&A.ctl->i);
     if (i0 >= n) break;
     if (seg >= MAX_SEGMENTS) {
-      // pathological input (a tie at nearly every element): finish in plain
-      // sequence, still exact
+      // more binade changes than any finite float sum can make: finish in
+      // plain sequence, still exact
       if (c == 0 && tid < 32) {
         const float sr = warp_seq(A.v, i0, n, s);
         if (tid == 0) A.ctl->s = sr;
@@ -126,118 +163,103 @@ __global__ void __launch_bounds__(ES_T) k_exact_sum(EsArgs A) {
     const double u = ldexp(1.0, E - 23);
     const double scale = ldexp(1.0, 23 - E);
     const long long S = (long long)((double)s * scale);
+    const int p0 = (int)(S & 1);
     const long long TOP = 1ll << 24;
 
-    // phase A: per thread contiguous sub-range of this chunk, from max(lo, i0)
+    // phase A: composite of each thread's contiguous sub-range of this
+    // chunk (from max(lo, i0)), then of the chunk
     const int a0 = max(lo, i0);
     const int t_lo = lo + tid * per, t_hi = min(hi, t_lo + per);
-    long long tsum = 0, tmax = LLONG_MIN;
-    int ttie = INT_MAX;
+    Xf tx = xf_identity();
     for (int k = max(t_lo, a0); k < t_hi; ++k) {
       long long fl, r;
       bool tie;
       classify(A.v[k], scale, fl, r, tie);
-      const long long m = tsum + fl;
-      if (m > tmax) tmax = m;
-      if (tie && k < ttie) ttie = k;
-      tsum += r;
+      xf_push(tx, fl, r, tie);
     }
-    s_tsum[tid] = tsum;
-    s_tmax[tid] = tmax;
-    s_ttie[tid] = ttie;
+    s_x[tid] = tx;
     __syncthreads();
     if (tid == 0) {
-      long long acc = 0, mx = LLONG_MIN;
-      int tt = INT_MAX;
-      for (int t = 0; t < ES_T; ++t) {
-        s_off[t] = acc;
-        if (s_tmax[t] != LLONG_MIN && acc + s_tmax[t] > mx) mx = acc + s_tmax[t];
-        if (s_ttie[t] < tt) tt = s_ttie[t];
-        acc += s_tsum[t];
+      Xf cx = xf_identity();
+      for (int t = 0; t < ES_T; ++t) cx = xf_then(cx, s_x[t]);
+      for (int p = 0; p < 2; ++p) {
+        A.Rc[2 * c + p] = cx.R[p];
+        A.Mc[2 * c + p] = cx.M[p];
+        A.Tc[2 * c + p] = cx.q[p];
       }
-      A.Rc[c] = acc;
-      A.Mc[c] = mx;
-      A.Tc[c] = tt;
     }
     if (!grid_barrier(A.bar, G, A.err)) return;
 
-    // phase B (every CTA, warp 0): chunk prefix, first crossing chunk, first tie
-    if (tid < 32) {
-      const int cper = (G + 31) / 32;
-      const int c0 = tid * cper, c1 = min(G, c0 + cper);
-      long long lsum = 0;
-      for (int q = c0; q < c1; ++q) lsum += __ldcg(A.Rc + q);
-      long long incl = lsum;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const long long y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (tid >= o) incl += y;
+    // phase B (every CTA, one thread): walk the chunk composites in order
+    // from the run's start state; find the first chunk that crosses, the
+    // state at its start, and the state at the end
+    if (tid == 0) {
+      long long R = 0;
+      int q = p0, cxq = INT_MAX;
+      long long Rx = 0;
+      int qx = 0;
+      for (int cc = 0; cc < G; ++cc) {
+        const long long Mq = __ldcg(A.Mc + 2 * cc + q);
+        if (Mq != LLONG_MIN && S + R + Mq >= TOP) {
+          cxq = cc;
+          Rx = R;
+          qx = q;
+          break;
+        }
+        const long long Rq = __ldcg(A.Rc + 2 * cc + q);
+        const int qn = __ldcg(A.Tc + 2 * cc + q);
+        R += Rq;
+        q = qn;
       }
-      long long off = incl - lsum;
-      int cx = INT_MAX, tmin = INT_MAX;
-      for (int q = c0; q < c1; ++q) {
-        const long long mq = __ldcg(A.Mc + q);
-        if (cx == INT_MAX && mq != LLONG_MIN && S + off + mq >= TOP) cx = q;
-        const int tq = __ldcg(A.Tc + q);
-        if (tq < tmin) tmin = tq;
-        if (q == c) s_roff = off;
-        off += __ldcg(A.Rc + q);
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        cx = min(cx, __shfl_xor_sync(0xffffffffu, cx, o));
-        tmin = min(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
-      }
-      const long long tot = __shfl_sync(0xffffffffu, incl, 31);
-      if (tid == 0) {
-        s_cx = cx;
-        s_tmin = tmin;
-        s_ct = tmin == INT_MAX ? INT_MAX : tmin / chunk;
-        s_rtot = tot;
-      }
+      s_cx = cxq;
+      s_rtot = cxq == INT_MAX ? R : Rx;
+      s_qx = qx;
     }
     __syncthreads();
-    const int cx = s_cx, ct = s_ct, tmin = s_tmin;
-    const int ev_cta = (cx == INT_MAX && ct == INT_MAX) ? 0 : (ct < cx ? ct : cx);
-    if (c == ev_cta) {
-      const long long roff = s_roff;
-      if (cx == INT_MAX && ct == INT_MAX) {
-        if (tid == 0) {
-          A.ctl->s = (float)((double)(S + s_rtot) * u);
-          A.ctl->i = n;
-        }
-      } else {
-        // first crossing inside this chunk (when it is the crossing chunk)
-        if (tid == 0) s_kx = INT_MAX;
-        __syncthreads();
-        if (c == cx) {
-          long long run = roff + s_off[tid];
-          for (int k = max(t_lo, a0); k < t_hi; ++k) {
-            long long fl, r;
-            bool tie;
-            classify(A.v[k], scale, fl, r, tie);
-            if (S + run + fl >= TOP) {
-              atomicMin(&s_kx, k);
-              break;
-            }
-            run += r;
+    const int cxi = s_cx;
+    if (cxi == INT_MAX) {
+      if (c == 0 && tid == 0) {
+        A.ctl->s = (float)((double)(S + s_rtot) * u);
+        A.ctl->i = n;
+      }
+    } else if (c == cxi) {
+      // the crossing chunk: thread 0 finds the first crossing thread range,
+      // whose thread then finds the element and adds it with a float addition
+      if (tid == 0) {
+        long long R = s_rtot;
+        int q = s_qx;
+        int tx_first = ES_T;
+        for (int t = 0; t < ES_T; ++t) {
+          const Xf &x = s_x[t];
+          if (x.M[q] != LLONG_MIN && S + R + x.M[q] >= TOP) {
+            tx_first = t;
+            break;
           }
+          R += x.R[q];
+          q = x.q[q];
         }
-        __syncthreads();
-        const int kstar = min(s_kx, tmin);
-        // the thread owning kstar adds it with a float addition
-        if (kstar >= max(t_lo, a0) && kstar < t_hi) {
-          long long run = roff + s_off[tid];
-          for (int k = max(t_lo, a0); k < kstar; ++k) {
-            long long fl, r;
-            bool tie;
-            classify(A.v[k], scale, fl, r, tie);
-            run += r;
+        s_tcross = tx_first;
+        s_R = R;
+        s_q = q;
+      }
+      __syncthreads();
+      if (tid == s_tcross) {
+        long long R = s_R;
+        int q = s_q;
+        for (int k = max(t_lo, a0); k < t_hi; ++k) {
+          long long fl, r;
+          bool tie;
+          classify(A.v[k], scale, fl, r, tie);
+          if (S + R + fl >= TOP) {
+            const float sb = (float)((double)(S + R) * u);
+            const float sn = __fadd_rn(sb, A.v[k]);
+            A.ctl->s = sn;
+            A.ctl->i = isfinite(sn) ? k + 1 : n;
+            break;
           }
-          const float sb = (float)((double)(S + run) * u);
-          const float sn = __fadd_rn(sb, A.v[kstar]);
-          A.ctl->s = sn;
-          A.ctl->i = isfinite(sn) ? kstar + 1 : n;
+          const long long rr = tie ? fl + ((q + fl) & 1) : r;
+          R += rr;
+          q = (int)((q + rr) & 1);
         }
       }
     }
@@ -320,13 +342,14 @@ using namespace rpba;
 
 namespace {
 
-constexpr int NA_MAX_CTAS = 1024;
-constexpr int NA_CHUNK = 4096;
+constexpr int NA_MAX_CTAS = 512;  // resident on 148 SMs at 4 CTAs per SM
+constexpr int NA_CHUNK = 8192;
 constexpr long long NA_MAX_N = (long long)NA_MAX_CTAS * NA_CHUNK;  // 4,194,304
 constexpr size_t NA_OFF_RC = 0;
-constexpr size_t NA_OFF_MC = NA_OFF_RC + sizeof(long long) * NA_MAX_CTAS;
-constexpr size_t NA_OFF_TC = NA_OFF_MC + sizeof(long long) * NA_MAX_CTAS;
-constexpr size_t NA_OFF_CTL = NA_OFF_TC + sizeof(int) * NA_MAX_CTAS;
+// two entries per CTA (one per incoming parity)
+constexpr size_t NA_OFF_MC = NA_OFF_RC + sizeof(long long) * 2 * NA_MAX_CTAS;
+constexpr size_t NA_OFF_TC = NA_OFF_MC + sizeof(long long) * 2 * NA_MAX_CTAS;
+constexpr size_t NA_OFF_CTL = NA_OFF_TC + sizeof(int) * 2 * NA_MAX_CTAS;
 constexpr size_t NA_OFF_BAR = NA_OFF_CTL + 16;
 constexpr size_t NA_OFF_ERR = NA_OFF_BAR + 16;
 constexpr size_t NA_BYTES = NA_OFF_ERR + 16;

@@ -47,6 +47,9 @@ struct DevLSA {
   double *rec, *ptV;
   // camera-grouped observation order (the reference's nro order)
   int *camlist, *coff;
+  // mixed-precision form: FP32 records, point blocks and reduced camera
+  // system (the FP64 arrays above and below are then unused)
+  float *rec32, *ptV32, *blocks32;
   // reduced camera system
   double *blocks;  // [(nimg + nboff) * 81], diagonal blocks first
   double *rhs;     // [nimg * 9]
@@ -61,6 +64,18 @@ struct DevLSA {
   const int4 *item_meta;    // (row, first entry, end entry, 0)
   int *err;            // device error word
 };
+
+// Element i of the reduced camera system's block array in either form
+// (for set-up kernels; the PCG's SpMV is compiled for each form).
+__device__ __forceinline__ double blk_at(const DevLSA &L, size_t i) {
+  return L.blocks32 ? (double)L.blocks32[i] : L.blocks[i];
+}
+__device__ __forceinline__ void load_block(const DevLSA &L, size_t b, double out[81]) {
+  if (L.blocks32)
+    for (int e = 0; e < 81; ++e) out[e] = (double)L.blocks32[b * 81 + e];
+  else
+    for (int e = 0; e < 81; ++e) out[e] = L.blocks[b * 81 + e];
+}
 
 // ---- launchers (kernels.cu)
 void launch_cost(const DevLSA &L, const double *XM, bool srmv, cudaStream_t s);
@@ -135,12 +150,25 @@ struct CoarseWork {
   double *dsc = nullptr;         // [nc] Jacobi scaling of A_c
   double *hj = nullptr;          // [nimg * 9] fine part of the preconditioned residual
   int *err = nullptr;            // bit 4: coarse matrix not positive definite
+  // Galerkin assembly (grown on demand, released by coarse_release)
+  int built_version = -1, nruns = 0, nsegs = 0;
+  unsigned *ekey = nullptr, *ekey2 = nullptr, *run_key = nullptr, *rkey = nullptr, *rkey2 = nullptr,
+           *seg_key = nullptr;
+  int *eval = nullptr, *ent_sorted = nullptr, *run_cnt = nullptr, *run_off = nullptr, *counts = nullptr,
+      *ridx = nullptr, *run_sorted = nullptr, *seg_cnt = nullptr, *seg_off = nullptr;
+  double *Z = nullptr;           // [nruns][CO_M * CO_M]
+  unsigned char *cub_tmp = nullptr;
+  size_t ekey_cap = 0, ekey2_cap = 0, eval_cap = 0, ent_sorted_cap = 0, run_key_cap = 0, run_cnt_cap = 0,
+         run_off_cap = 0, counts_cap = 0, rkey_cap = 0, rkey2_cap = 0, ridx_cap = 0, run_sorted_cap = 0,
+         seg_key_cap = 0, seg_cnt_cap = 0, seg_off_cap = 0, Z_cap = 0, cub_tmp_cap = 0;
 };
 // Aggregates from the cameras' projection centres (recursive coordinate
 // bisection into at most max_aggs groups of about 16 cameras or more).
 void coarse_build(const DevLSA &L, int max_aggs, CoarseWork &C, std::vector<void *> &owned, cudaStream_t s);
-// Per linear system: P, the Galerkin matrix P^T S P and its inverse.
-void coarse_setup(const DevLSA &L, const CoarseWork &C, cudaStream_t s);
+// Per linear system: P, the Galerkin matrix P^T S P and its inverse (the
+// run structure of the assembly is rebuilt when structure_version changes).
+void coarse_setup(const DevLSA &L, CoarseWork &C, int structure_version, cudaStream_t s);
+void coarse_release(CoarseWork &C);
 // h += P A_c^-1 P^T r over the rows of the system.
 void coarse_apply(const DevLSA &L, const CoarseWork &C, const double *r, double *h, cudaStream_t s);
 
@@ -176,8 +204,9 @@ struct TrainBufs {
 struct PcgWork;
 void learned_pcg_setup(const DevLSA &L, const PcgWork &W, const float *weights, cudaStream_t s);
 struct CoarseWork;
-void learned_record(const DevLSA &L, const CoarseWork *coarse, const double *xstar, unsigned long long seed,
-                    TrainSet &T, TrainHost &H, cudaStream_t s);
+// scratch: [nimg * 81] doubles
+void learned_record(const DevLSA &L, const CoarseWork *coarse, const double *xstar, double *scratch,
+                    unsigned long long seed, TrainSet &T, TrainHost &H, cudaStream_t s);
 void learned_loss_grad(const TrainSet &T, const float *W, TrainBufs &B, float *loss, float *err, cudaStream_t s);
 void learned_adam(float *W, float *m, float *v, const float *grad, float lr, int t, cudaStream_t s);
 

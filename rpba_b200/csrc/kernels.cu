@@ -1,5 +1,9 @@
 // kernels.cu -- per-observation, per-point and per-camera kernels of the
-// global LSA (rbacore.cpp).  FP64 throughout (the drop-in form).
+// global LSA (rbacore.cpp).  The linearisation kernels (point, camera,
+// pair, back-substitution) are compiled for two forms: FP64 throughout (the
+// drop-in form) and FP32 records/blocks with FP32 arithmetic, compensated
+// (Kahan) per-camera and per-pair sums and FP64 inversion of ill-conditioned
+// point blocks (the mixed-precision form).  Residuals and the cost stay FP64.
 #include <cub/cub.cuh>
 
 #include "internal.h"
@@ -10,11 +14,45 @@ namespace {
 
 constexpr int GRP = 8;  // lanes per point in the point-major kernels
 
-__device__ __forceinline__ double grp_sum(double v) {
+template <class T>
+__device__ __forceinline__ T grp_sum(T v) {
 #pragma unroll
   for (int o = GRP / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o, GRP);
   return v;
 }
+
+// Storage of the linearisation in either form.
+template <class T>
+struct Store;
+template <>
+struct Store<double> {
+  static __device__ __forceinline__ double *rec(const DevLSA &L) { return L.rec; }
+  static __device__ __forceinline__ double *ptV(const DevLSA &L) { return L.ptV; }
+  static __device__ __forceinline__ double *blocks(const DevLSA &L) { return L.blocks; }
+};
+template <>
+struct Store<float> {
+  static __device__ __forceinline__ float *rec(const DevLSA &L) { return L.rec32; }
+  static __device__ __forceinline__ float *ptV(const DevLSA &L) { return L.ptV32; }
+  static __device__ __forceinline__ float *blocks(const DevLSA &L) { return L.blocks32; }
+};
+
+// Compensated (Kahan) accumulation for the FP32 form; plain in FP64.
+template <class T>
+struct Acc {
+  T s = T(0), c = T(0);
+  __device__ __forceinline__ void add(T x) {
+    if constexpr (sizeof(T) == 4) {
+      const T y = x - c;
+      const T t = s + y;
+      c = (t - s) - y;
+      s = t;
+    } else {
+      s += x;
+    }
+  }
+  __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
 
 __device__ __forceinline__ int role_of(const DevLSA &L, int k) {
   return k == 0 ? ROLE_ZERO : (k == L.normcamera ? ROLE_NORM : ROLE_FREE);
@@ -90,6 +128,7 @@ __global__ void k_seq_sum(const float *__restrict__ v, int n, float *out) {
 // point block V = sum Jp^T W Jp and g = sum Jp^T W d, V damped and inverted;
 // the per-observation record for the camera, pair and back-substitution
 // kernels.
+template <class T>
 __global__ void k_point(DevLSA L, double multfact1) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int p = gt / GRP, ln = gt % GRP;
@@ -104,7 +143,7 @@ __global__ void k_point(DevLSA L, double multfact1) {
     X2 = X[2];
   }
   const int esvm[2] = {L.gauge[0], L.gauge[1]};
-  double V[9], g[3];
+  T V[9], g[3];
 #pragma unroll
   for (int j = 0; j < 9; ++j) V[j] = 0.;
   g[0] = g[1] = g[2] = 0.;
@@ -115,11 +154,12 @@ __global__ void k_point(DevLSA L, double multfact1) {
     ObsEval e;
     eval_obs(c, X0, X1, X2, xg.x, xg.y, L.defdiff, e);
     if (e.nan) L.o_s0rmv[o] = 1.e20f;
-    double Bc[2][RPBA_P], Bp[2][3];
-    jacobians<double>(c, e, role_of(L, k), esvm, L.addmask, Bc, Bp);
+    T Bc[2][RPBA_P], Bp[2][3];
+    jacobians<T>(c, e, role_of(L, k), esvm, L.addmask, Bc, Bp);
     const float4 w = L.o_w[o];
-    const double W0 = w.x, W1 = w.y, W2 = w.z;
-    double G[2][3];
+    const T W0 = w.x, W1 = w.y, W2 = w.z;
+    const T d1 = (T)e.d1, d2 = (T)e.d2;
+    T G[2][3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       G[0][j] = Bp[0][j] * W0 + Bp[1][j] * W2;
@@ -129,60 +169,75 @@ __global__ void k_point(DevLSA L, double multfact1) {
     for (int a = 0; a < 3; ++a) {
 #pragma unroll
       for (int b = 0; b < 3; ++b) V[a * 3 + b] += G[0][a] * Bp[0][b] + G[1][a] * Bp[1][b];
-      g[a] += G[0][a] * e.d1 + G[1][a] * e.d2;
+      g[a] += G[0][a] * d1 + G[1][a] * d2;
     }
-    double *r = L.rec + (size_t)o * REC;
+    T *r = Store<T>::rec(L) + (size_t)o * REC;
     const bool cam_active = k >= L.begini;
 #pragma unroll
     for (int j = 0; j < RPBA_P; ++j) {
-      r[j] = cam_active ? Bc[0][j] : 0.;
-      r[9 + j] = cam_active ? Bc[1][j] : 0.;
+      r[j] = cam_active ? Bc[0][j] : T(0);
+      r[9 + j] = cam_active ? Bc[1][j] : T(0);
     }
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       r[18 + j] = G[0][j];
       r[21 + j] = G[1][j];
     }
-    r[24] = e.d1 * W0 + e.d2 * W2;
-    r[25] = e.d1 * W2 + e.d2 * W1;
+    r[24] = d1 * W0 + d2 * W2;
+    r[25] = d1 * W2 + d2 * W1;
   }
 #pragma unroll
   for (int j = 0; j < 9; ++j) V[j] = grp_sum(V[j]);
 #pragma unroll
   for (int j = 0; j < 3; ++j) g[j] = grp_sum(g[j]);
-  V[0] *= multfact1;
-  V[4] *= multfact1;
-  V[8] *= multfact1;
-  double Vi[9];
-  inv3<double>(V, Vi);
+  V[0] = (T)(V[0] * multfact1);
+  V[4] = (T)(V[4] * multfact1);
+  V[8] = (T)(V[8] * multfact1);
+  T Vi[9];
+  if constexpr (sizeof(T) == 8) {
+    inv3<double>(V, Vi);
+  } else {
+    // FP32 unless the point block is ill-conditioned (determinant small
+    // against the diagonal product): then FP64
+    const T det = V[0] * (V[4] * V[8] - V[5] * V[7]) - V[1] * (V[3] * V[8] - V[5] * V[6]) +
+                  V[2] * (V[3] * V[7] - V[4] * V[6]);
+    if (fabsf(det) > 1e-3f * fabsf(V[0] * V[4] * V[8])) {
+      inv3<float>(V, Vi);
+    } else {
+      double Vd[9], Vid[9];
+      for (int j = 0; j < 9; ++j) Vd[j] = V[j];
+      inv3<double>(Vd, Vid);
+      for (int j = 0; j < 9; ++j) Vi[j] = (T)Vid[j];
+    }
+  }
   if (ln == 0 && valid) {
-    double *pv = L.ptV + (size_t)p * PREC;
+    T *pv = Store<T>::ptV(L) + (size_t)p * PREC;
 #pragma unroll
     for (int j = 0; j < 9; ++j) pv[j] = Vi[j];
     pv[9] = g[0];
     pv[10] = g[1];
     pv[11] = g[2];
   }
-  double vg[3];
+  T vg[3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) vg[a] = Vi[a * 3] * g[0] + Vi[a * 3 + 1] * g[1] + Vi[a * 3 + 2] * g[2];
   for (int o = t0 + ln; o < t1; o += GRP) {
-    double *r = L.rec + (size_t)o * REC;
-    double G[2][3];
+    T *r = Store<T>::rec(L) + (size_t)o * REC;
+    T G[2][3];
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
       G[0][j] = r[18 + j];
       G[1][j] = r[21 + j];
     }
     const float4 w = L.o_w[o];
-    double GV[2][3];
+    T GV[2][3];
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
       for (int b = 0; b < 3; ++b) GV[a][b] = G[a][0] * Vi[b] + G[a][1] * Vi[3 + b] + G[a][2] * Vi[6 + b];
-    r[26] = (double)w.x - (GV[0][0] * G[0][0] + GV[0][1] * G[0][1] + GV[0][2] * G[0][2]);
-    r[27] = (double)w.z - (GV[0][0] * G[1][0] + GV[0][1] * G[1][1] + GV[0][2] * G[1][2]);
-    r[28] = (double)w.y - (GV[1][0] * G[1][0] + GV[1][1] * G[1][1] + GV[1][2] * G[1][2]);
+    r[26] = (T)w.x - (GV[0][0] * G[0][0] + GV[0][1] * G[0][1] + GV[0][2] * G[0][2]);
+    r[27] = (T)w.z - (GV[0][0] * G[1][0] + GV[0][1] * G[1][1] + GV[0][2] * G[1][2]);
+    r[28] = (T)w.y - (GV[1][0] * G[1][0] + GV[1][1] * G[1][1] + GV[1][2] * G[1][2]);
     r[29] = r[24] - (G[0][0] * vg[0] + G[0][1] * vg[1] + G[0][2] * vg[2]);
     r[30] = r[25] - (G[1][0] * vg[0] + G[1][1] * vg[1] + G[1][2] * vg[2]);
   }
@@ -196,13 +251,14 @@ __global__ void k_point(DevLSA L, double multfact1) {
 // camera sums its observations in the reference's nro order.
 constexpr int CAM_T = 64, CAM_B = 32, CAM_W = 24;
 
+template <class T>
 __global__ void __launch_bounds__(CAM_T) k_camera(DevLSA L, double multfact1) {
   const int k = blockIdx.x + L.begini;
   if (k >= L.nimg) return;
-  __shared__ double s[CAM_B][CAM_W];
+  __shared__ T s[CAM_B][CAM_W];
   const int tid = threadIdx.x;
   const int beg = L.coff[k], end = L.coff[k + 1];
-  double acc = 0.;
+  Acc<T> acc;
   int ei = 0, ej = 0;
   if (tid < 45) {
     int t = tid;
@@ -219,35 +275,35 @@ __global__ void __launch_bounds__(CAM_T) k_camera(DevLSA L, double multfact1) {
     for (int idx = tid; idx < nb * 23; idx += CAM_T) {
       const int ob = idx / 23, c = idx % 23;
       const int o = L.camlist[base + ob];
-      const double *r = L.rec + (size_t)o * REC;
+      const T *r = Store<T>::rec(L) + (size_t)o * REC;
       s[ob][c] = c < 18 ? r[c] : r[26 + (c - 18)];
     }
     __syncthreads();
     if (tid < 45) {
       for (int ob = 0; ob < nb; ++ob) {
-        const double b0i = s[ob][ei], b1i = s[ob][9 + ei], b0j = s[ob][ej], b1j = s[ob][9 + ej];
-        const double M00 = s[ob][18], M01 = s[ob][19], M11 = s[ob][20];
-        acc += b0i * (M00 * b0j + M01 * b1j) + b1i * (M01 * b0j + M11 * b1j);
+        const T b0i = s[ob][ei], b1i = s[ob][9 + ei], b0j = s[ob][ej], b1j = s[ob][9 + ej];
+        const T M00 = s[ob][18], M01 = s[ob][19], M11 = s[ob][20];
+        acc.add(b0i * (M00 * b0j + M01 * b1j) + b1i * (M01 * b0j + M11 * b1j));
       }
     } else if (tid < 54) {
-      for (int ob = 0; ob < nb; ++ob) acc += s[ob][ei] * s[ob][21] + s[ob][9 + ei] * s[ob][22];
+      for (int ob = 0; ob < nb; ++ob) acc.add(s[ob][ei] * s[ob][21] + s[ob][9 + ei] * s[ob][22]);
     }
     __syncthreads();
   }
   const int np = L.camparv[k + 1] - L.camparv[k];
-  double *D = L.blocks + (size_t)k * 81;
+  T *D = Store<T>::blocks(L) + (size_t)k * 81;
   if (tid < 45) {
     double v;
     if (ei < np && ej < np) {
-      v = acc;
+      v = acc.value();
       if (ei == ej) v = __dadd_rn(__dmul_rn(v, multfact1), 1.e-2);
     } else {
       v = ei == ej ? 1. : 0.;
     }
-    D[ei * 9 + ej] = v;
-    D[ej * 9 + ei] = v;
+    D[ei * 9 + ej] = (T)v;
+    D[ej * 9 + ei] = (T)v;
   } else if (tid < 54) {
-    L.rhs[k * 9 + ei] = ei < np ? acc : 0.;
+    L.rhs[k * 9 + ei] = ei < np ? (double)(T)acc.value() : 0.;
   }
 }
 
@@ -255,33 +311,34 @@ __global__ void __launch_bounds__(CAM_T) k_camera(DevLSA L, double multfact1) {
 // Off-diagonal blocks: S_kl = - sum_p W_pk V_p^-1 W_pl^T over the points
 // seen by both cameras (rbacore.cpp:1362-1390), with W_po = Bc^T G.  One
 // warp per block sums its contributions in a fixed order.
+template <class T>
 __global__ void k_pair(DevLSA L) {
   const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int wl = threadIdx.x >> 5;
-  __shared__ double sm[8][64];
+  __shared__ T sm[8][64];
   if (wid >= L.nboff) return;
-  double *s = sm[wl];
-  double acc[3] = {0., 0., 0.};
+  T *s = sm[wl];
+  Acc<T> acc[3];
   const int cb = L.boff[wid], ce = L.boff[wid + 1];
   for (int c = cb; c < ce; ++c) {
     const int2 pr = L.contrib[c];
     const int p = L.o_pt[pr.x];
-    const double *rs = L.rec + (size_t)pr.x * REC;
-    const double *rt = L.rec + (size_t)pr.y * REC;
-    const double *pv = L.ptV + (size_t)p * PREC;
+    const T *rs = Store<T>::rec(L) + (size_t)pr.x * REC;
+    const T *rt = Store<T>::rec(L) + (size_t)pr.y * REC;
+    const T *pv = Store<T>::ptV(L) + (size_t)p * PREC;
     for (int idx = lane; idx < 57; idx += 32)
       s[idx] = idx < 24 ? rs[idx] : (idx < 48 ? rt[idx - 24] : pv[idx - 48]);
     __syncwarp();
     // N = G_s V^-1 G_t^T (2 x 2)
-    const double *Gs = s + 18, *Gt = s + 42, *Vi = s + 48;
-    double GV[2][3];
+    const T *Gs = s + 18, *Gt = s + 42, *Vi = s + 48;
+    T GV[2][3];
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
       for (int b = 0; b < 3; ++b)
         GV[a][b] = Gs[a * 3] * Vi[b] + Gs[a * 3 + 1] * Vi[3 + b] + Gs[a * 3 + 2] * Vi[6 + b];
-    double N[2][2];
+    T N[2][2];
 #pragma unroll
     for (int a = 0; a < 2; ++a)
 #pragma unroll
@@ -292,41 +349,42 @@ __global__ void k_pair(DevLSA L) {
       const int e = lane + 32 * q;
       if (e < 81) {
         const int i = e / 9, j = e % 9;
-        const double bt0 = s[24 + j], bt1 = s[24 + 9 + j];
-        const double t0 = N[0][0] * bt0 + N[0][1] * bt1;
-        const double t1 = N[1][0] * bt0 + N[1][1] * bt1;
-        acc[q] -= s[i] * t0 + s[9 + i] * t1;
+        const T bt0 = s[24 + j], bt1 = s[24 + 9 + j];
+        const T t0 = N[0][0] * bt0 + N[0][1] * bt1;
+        const T t1 = N[1][0] * bt0 + N[1][1] * bt1;
+        acc[q].add(-(s[i] * t0 + s[9 + i] * t1));
       }
     }
     __syncwarp();
   }
-  double *B = L.blocks + (size_t)(L.nimg + wid) * 81;
+  T *B = Store<T>::blocks(L) + (size_t)(L.nimg + wid) * 81;
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
     const int e = lane + 32 * q;
-    if (e < 81) B[e] = acc[q];
+    if (e < 81) B[e] = (T)acc[q].value();
   }
 }
 
 // ------------------------------------------------- back-substitution
 // rbacore.cpp:1395-1410: dX_p = V^-1 (g - sum_o W_o^T dc_k), with
 // W_o^T dc = G^T (Bc dc).
+template <class T>
 __global__ void k_backsub(DevLSA L, const double *__restrict__ xsol) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int p = gt / GRP, ln = gt % GRP;
   const bool valid = p < L.npts;  // no early exit (full-warp shuffles below)
   const int t0 = valid ? L.pt_off[p] : 0, t1 = valid ? L.pt_off[p + 1] : 0;
-  double a0 = 0., a1 = 0., a2 = 0.;
+  T a0 = 0., a1 = 0., a2 = 0.;
   for (int o = t0 + ln; o < t1; o += GRP) {
     const int k = L.o_cam[o];
     if (k < L.begini) continue;
-    const double *r = L.rec + (size_t)o * REC;
+    const T *r = Store<T>::rec(L) + (size_t)o * REC;
     const double *dc = xsol + (size_t)k * 9;
-    double s0 = 0., s1 = 0.;
+    T s0 = 0., s1 = 0.;
 #pragma unroll
     for (int a = 0; a < 9; ++a) {
-      s0 += r[a] * dc[a];
-      s1 += r[9 + a] * dc[a];
+      s0 += r[a] * (T)dc[a];
+      s1 += r[9 + a] * (T)dc[a];
     }
     a0 += r[18] * s0 + r[21] * s1;
     a1 += r[19] * s0 + r[22] * s1;
@@ -336,8 +394,8 @@ __global__ void k_backsub(DevLSA L, const double *__restrict__ xsol) {
   a1 = grp_sum(a1);
   a2 = grp_sum(a2);
   if (ln == 0 && valid) {
-    const double *pv = L.ptV + (size_t)p * PREC;
-    const double r0 = pv[9] - a0, r1 = pv[10] - a1, r2 = pv[11] - a2;
+    const T *pv = Store<T>::ptV(L) + (size_t)p * PREC;
+    const T r0 = pv[9] - a0, r1 = pv[10] - a1, r2 = pv[11] - a2;
     double *xo = L.x + L.nrioff + 3 * p;
     xo[0] = pv[0] * r0 + pv[1] * r1 + pv[2] * r2;
     xo[1] = pv[3] * r0 + pv[4] * r1 + pv[5] * r2;
@@ -740,20 +798,36 @@ void launch_seq_sum(const float *v, int n, float *out, cudaStream_t s) {
 }
 
 void launch_point_pass(const DevLSA &L, double multfact1, cudaStream_t s) {
-  if (L.npts > 0) k_point<<<nblk((long long)L.npts * GRP, 128), 128, 0, s>>>(L, multfact1);
+  if (L.npts <= 0) return;
+  if (L.rec32)
+    k_point<float><<<nblk((long long)L.npts * GRP, 128), 128, 0, s>>>(L, multfact1);
+  else
+    k_point<double><<<nblk((long long)L.npts * GRP, 128), 128, 0, s>>>(L, multfact1);
 }
 
 void launch_camera_pass(const DevLSA &L, double multfact1, cudaStream_t s) {
   const int nc = L.nimg - L.begini;
-  if (nc > 0) k_camera<<<nc, CAM_T, 0, s>>>(L, multfact1);
+  if (nc <= 0) return;
+  if (L.rec32)
+    k_camera<float><<<nc, CAM_T, 0, s>>>(L, multfact1);
+  else
+    k_camera<double><<<nc, CAM_T, 0, s>>>(L, multfact1);
 }
 
 void launch_pair_pass(const DevLSA &L, cudaStream_t s) {
-  if (L.nboff > 0) k_pair<<<nblk((long long)L.nboff * 32, 256), 256, 0, s>>>(L);
+  if (L.nboff <= 0) return;
+  if (L.rec32)
+    k_pair<float><<<nblk((long long)L.nboff * 32, 256), 256, 0, s>>>(L);
+  else
+    k_pair<double><<<nblk((long long)L.nboff * 32, 256), 256, 0, s>>>(L);
 }
 
 void launch_backsub(const DevLSA &L, const double *xsol, cudaStream_t s) {
-  if (L.npts > 0) k_backsub<<<nblk((long long)L.npts * GRP, 128), 128, 0, s>>>(L, xsol);
+  if (L.npts <= 0) return;
+  if (L.rec32)
+    k_backsub<float><<<nblk((long long)L.npts * GRP, 128), 128, 0, s>>>(L, xsol);
+  else
+    k_backsub<double><<<nblk((long long)L.npts * GRP, 128), 128, 0, s>>>(L, xsol);
 }
 
 void launch_xcam(const DevLSA &L, const double *xsol, cudaStream_t s) {

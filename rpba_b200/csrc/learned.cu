@@ -43,10 +43,11 @@ __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__floa
 // reduced in a fixed butterfly order); every lane returns the same f.
 __device__ void block_features(const DevLSA &L, int k, int lane, float f[NN_F]) {
   const int np = L.camparv[k + 1] - L.camparv[k];
-  const double *D = L.blocks + (size_t)k * 81;
+  double Dd[9];
+  for (int a = 0; a < 9; ++a) Dd[a] = blk_at(L, (size_t)k * 81 + a * 10);
   double ld[9], mean = 0.;
   for (int a = 0; a < 9; ++a) {
-    ld[a] = a < np ? log(fmax(D[a * 9 + a], 1e-300)) : 0.;
+    ld[a] = a < np ? log(fmax(Dd[a], 1e-300)) : 0.;
     if (a < np) mean += ld[a];
   }
   mean /= (np > 0 ? np : 1);
@@ -58,13 +59,12 @@ __device__ void block_features(const DevLSA &L, int k, int lane, float f[NN_F]) 
     if (col == k) continue;
     ++deg;
     const bool tr = en.y < 0;
-    const double *B = L.blocks + (size_t)(en.y & 0x7fffffff) * 81;
-    const double *Dl = L.blocks + (size_t)col * 81;
+    const size_t B = (size_t)(en.y & 0x7fffffff) * 81, Dl = (size_t)col * 81;
     const int nc = L.camparv[col + 1] - L.camparv[col];
     for (int a = 0; a < np; ++a)
       for (int c = 0; c < nc; ++c) {
-        const double v = tr ? B[c * 9 + a] : B[a * 9 + c];
-        cpl[a] += fabs(v) / sqrt(fmax(D[a * 9 + a] * Dl[c * 9 + c], 1e-300));
+        const double v = blk_at(L, B + (tr ? c * 9 + a : a * 9 + c));
+        cpl[a] += fabs(v) / sqrt(fmax(Dd[a] * blk_at(L, Dl + c * 10), 1e-300));
       }
   }
 #pragma unroll
@@ -138,7 +138,11 @@ __global__ void k_learned_setup(DevLSA L, PcgWork Wk, const float *weights) {
     return;
   }
   const int np = L.camparv[k + 1] - L.camparv[k];
-  if (lane == 0) lu_inverse9(np, L.blocks + (size_t)k * 81, C);
+  if (lane == 0) {
+    double Dk[81];
+    load_block(L, (size_t)k, Dk);
+    lu_inverse9(np, Dk, C);
+  }
   float sc[NN_O];
   for (int a = 0; a < NN_O; ++a) sc[a] = 1.f;
   if (weights) {
@@ -359,32 +363,39 @@ __global__ void k_adam(float *W, float *m, float *v, const float *grad, float lr
 }
 
 // ---- recording a system into the training set
-__global__ void k_rec_rows(DevLSA L, TrainSet T, int row0, int sys, const double *xstar, unsigned long long seed) {
+// One warp per row of the system being recorded (FP64 form): features, the
+// scaled block inverse (LU by lane 0 into the FP64 scratch Si, then scaled
+// by lanes 0..8), right-hand sides and the scaled solution.
+__global__ void k_rec_rows(DevLSA L, TrainSet T, int row0, int sys, const double *xstar, unsigned long long seed,
+                           double *Si) {
   const int k = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) + L.begini, lane = threadIdx.x & 31;
   if (k >= L.nimg) return;
   const int r = row0 + (k - L.begini);
   float f[NN_F];
   block_features(L, k, lane, f);
-  if (lane != 0) return;
-  for (int j = 0; j < NN_F; ++j) T.f[(size_t)r * NN_F + j] = f[j];
   const int np = L.camparv[k + 1] - L.camparv[k];
-  T.np[r] = np;
-  T.sys[r] = sys;
   const double *D = L.blocks + (size_t)k * 81;
-  double sq[9], Si[81];
-  for (int a = 0; a < 9; ++a) sq[a] = a < np ? sqrt(D[a * 10]) : 1.;
-  lu_inverse9(np, D, Si);
-  for (int a = 0; a < 9; ++a)
-    for (int c = 0; c < 9; ++c)
-      T.sinv[(size_t)r * 81 + a * 9 + c] = (a < np && c < np) ? (float)(sq[a] * Si[a * 9 + c] * sq[c]) : 0.f;
-  for (int a = 0; a < 9; ++a) {
-    // right-hand side 0: the LM step's (b~ = D^-1/2 b, x~* = D^1/2 x*)
-    T.b[(size_t)r * 9 + a] = a < np ? (float)(L.rhs[(size_t)k * 9 + a] / sq[a]) : 0.f;
-    T.xs[(size_t)r * 9 + a] = a < np ? (float)(xstar[(size_t)k * 9 + a] * sq[a]) : 0.f;
-    for (int pr = 1; pr < T.probes; ++pr)
-      T.b[((size_t)pr * T.rows_cap + r) * 9 + a] =
-          a < np ? (float)hash_normal(seed + 7919ull * pr, (unsigned long long)r * 9 + a) : 0.f;
+  double *Sk = Si + (size_t)k * 81;
+  if (lane == 0) {
+    for (int j = 0; j < NN_F; ++j) T.f[(size_t)r * NN_F + j] = f[j];
+    T.np[r] = np;
+    T.sys[r] = sys;
+    lu_inverse9(np, D, Sk);
   }
+  __syncwarp();
+  if (lane >= 9) return;
+  const int a = lane;
+  const double sqa = a < np ? sqrt(D[a * 10]) : 1.;
+  for (int c = 0; c < 9; ++c) {
+    const double sqc = c < np ? sqrt(D[c * 10]) : 1.;
+    T.sinv[(size_t)r * 81 + a * 9 + c] = (a < np && c < np) ? (float)(sqa * Sk[a * 9 + c] * sqc) : 0.f;
+  }
+  // right-hand side 0: the LM step's (b~ = D^-1/2 b, x~* = D^1/2 x*)
+  T.b[(size_t)r * 9 + a] = a < np ? (float)(L.rhs[(size_t)k * 9 + a] / sqa) : 0.f;
+  T.xs[(size_t)r * 9 + a] = a < np ? (float)(xstar[(size_t)k * 9 + a] * sqa) : 0.f;
+  for (int pr = 1; pr < T.probes; ++pr)
+    T.b[((size_t)pr * T.rows_cap + r) * 9 + a] =
+        a < np ? (float)hash_normal(seed + 7919ull * pr, (unsigned long long)r * 9 + a) : 0.f;
 }
 
 // scaled blocks: diagonal blocks of rows >= begini, then the off-diagonal
@@ -408,7 +419,7 @@ __global__ void k_rec_blocks(DevLSA L, TrainSet T, int blk0, const int2 *rc, int
   const int nr = L.camparv[r + 1] - L.camparv[r], nc = L.camparv[c + 1] - L.camparv[c];
   float v = 0.f;
   if (i < nr && j < nc)
-    v = (float)(L.blocks[src + e] / sqrt(L.blocks[(size_t)r * 81 + i * 10] * L.blocks[(size_t)c * 81 + j * 10]));
+    v = (float)(blk_at(L, src + e) / sqrt(blk_at(L, (size_t)r * 81 + i * 10) * blk_at(L, (size_t)c * 81 + j * 10)));
   T.blocks[(size_t)(blk0 + b) * 81 + e] = v;
 }
 
@@ -420,7 +431,7 @@ __global__ void k_rec_bvec(DevLSA L, TrainSet T, int row0, int pr, double *vb) {
   double v = 0.;
   if (k >= L.begini && a < L.camparv[k + 1] - L.camparv[k])
     v = (double)T.b[((size_t)pr * T.rows_cap + row0 + (k - L.begini)) * 9 + a] *
-        sqrt(L.blocks[(size_t)k * 81 + a * 10]);
+        sqrt(blk_at(L, (size_t)k * 81 + a * 10));
   vb[i] = v;
 }
 
@@ -431,7 +442,7 @@ __global__ void k_rec_uc(DevLSA L, TrainSet T, int row0, int pr, const double *v
   if (k >= L.nimg) return;
   const int np = L.camparv[k + 1] - L.camparv[k];
   T.uc[((size_t)pr * T.rows_cap + row0 + (k - L.begini)) * 9 + a] =
-      a < np ? (float)(vz[i] * sqrt(L.blocks[(size_t)k * 81 + a * 10])) : 0.f;
+      a < np ? (float)(vz[i] * sqrt(blk_at(L, (size_t)k * 81 + a * 10))) : 0.f;
 }
 
 }  // namespace
@@ -440,8 +451,9 @@ void learned_pcg_setup(const DevLSA &L, const PcgWork &W, const float *weights, 
   k_learned_setup<<<(L.nimg + 7) / 8, 256, 0, s>>>(L, W, weights);
 }
 
-void learned_record(const DevLSA &L, const CoarseWork *coarse, const double *xstar, unsigned long long seed,
-                    TrainSet &T, TrainHost &H, cudaStream_t s) {
+void learned_record(const DevLSA &L, const CoarseWork *coarse, const double *xstar, double *scratch,
+                    unsigned long long seed, TrainSet &T, TrainHost &H, cudaStream_t s) {
+  if (!L.blocks) return;  // systems are recorded in the FP64 form only
   const int nimg = L.nimg, nd = nimg - L.begini, nb = L.nboff;
   if (nd <= 0) return;
   const int nent = [&] {
@@ -484,7 +496,7 @@ void learned_record(const DevLSA &L, const CoarseWork *coarse, const double *xst
   RPBA_CUDA_CHECK(cudaMemcpyAsync(T.rowoff + row0, new_off.data(), sizeof(int) * (nd + 1), cudaMemcpyHostToDevice, s));
   RPBA_CUDA_CHECK(cudaMemcpyAsync(T.ent + H.ents, new_ent.data(), sizeof(int2) * new_ent.size(), cudaMemcpyHostToDevice, s));
   RPBA_CUDA_CHECK(cudaMemcpyAsync(H.rc, rc.data(), sizeof(int2) * std::max(nb, 1), cudaMemcpyHostToDevice, s));
-  k_rec_rows<<<(nd + 7) / 8, 256, 0, s>>>(L, T, row0, T.systems, xstar, seed);
+  k_rec_rows<<<(nd + 7) / 8, 256, 0, s>>>(L, T, row0, T.systems, xstar, seed, scratch);
   const long long nthreads = (long long)(nd + nb) * 81;
   k_rec_blocks<<<(int)((nthreads + 255) / 256), 256, 0, s>>>(L, T, blk0, H.rc, nb);
   if (T.uc) {

@@ -24,7 +24,7 @@ constexpr int PCG_T = 1024;
 constexpr int PCG_W = PCG_T / 32;
 
 struct PcgArgs {
-  const double *blocks;
+  const void *blocks;  // BT[(nimg + nboff) * 81]
   const int2 *ent;
   const int *rowoff;
   const int *row_item_off;
@@ -107,7 +107,9 @@ __device__ __forceinline__ void grid_sum(const double *red, int G, double (&v)[N
 //           (kept in hj), and the aggregate's restriction P^T r1 is formed
 //  phase 2b per aggregate: z = A_c^-1[aggregate rows] (P^T r1), then
 //           h1 = hj + P z and the two dot products
-template <bool CO>
+// BT: the storage type of the reduced camera system's blocks (double, or
+// float in the mixed-precision form); vectors and sums are FP64 either way.
+template <bool CO, class BT>
 __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gwarp = blockIdx.x * PCG_W + warp, nwarps = gridDim.x * PCG_W;
@@ -170,7 +172,7 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
         const size_t j = (size_t)col * 9 + rr;
         dc = __ldcg(A.h + j) + beta_prev * __ldcg(dprev + j);
       }
-      const double *B = A.blocks + (size_t)blk * 81;
+      const BT *B = (const BT *)A.blocks + (size_t)blk * 81;
 #pragma unroll
       for (int c = 0; c < 9; ++c) {
         const double xc = __shfl_sync(0xffffffffu, dc, (lane < 27 ? gbase : 0) + c);
@@ -396,7 +398,9 @@ __global__ void k_pcg_setup(DevLSA L, PcgWork W) {
     return;
   }
   const int np = L.camparv[k + 1] - L.camparv[k];
-  lu_inverse9(np, L.blocks + (size_t)k * 81, C);
+  double Dk[81];
+  load_block(L, (size_t)k, Dk);
+  lu_inverse9(np, Dk, C);
   double rv[9];
   for (int a = 0; a < 9; ++a) rv[a] = L.rhs[o + a];
   for (int a = 0; a < 9; ++a) {
@@ -414,8 +418,12 @@ __global__ void k_pcg_setup(DevLSA L, PcgWork W) {
 int pcg_max_grid(int device) {
   int nsm = 0, per = 0, per2 = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<false>, PCG_T, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true>, PCG_T, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<false, double>, PCG_T, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true, double>, PCG_T, 0);
+  per = std::min(per, per2);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<false, float>, PCG_T, 0);
+  per = std::min(per, per2);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true, float>, PCG_T, 0);
   per = std::min(per, per2);
   if (per < 1) per = 1;
   return nsm * per;
@@ -438,7 +446,7 @@ int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream
   if (g > grid) g = grid;
   if (g < 1) g = 1;
   PcgArgs A;
-  A.blocks = L.blocks;
+  A.blocks = L.blocks32 ? (const void *)L.blocks32 : (const void *)L.blocks;
   A.ent = L.ent;
   A.rowoff = L.rowoff;
   A.row_item_off = L.row_item_off;
@@ -472,7 +480,11 @@ int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream
   A.hj = co ? coarse->hj : nullptr;
   RPBA_CUDA_CHECK(cudaMemsetAsync(W.bar, 0, 2 * sizeof(unsigned), s));
   void *args[] = {&A};
-  const void *fn = co ? (const void *)k_pcg<true> : (const void *)k_pcg<false>;
+  const void *fn;
+  if (L.blocks32)
+    fn = co ? (const void *)k_pcg<true, float> : (const void *)k_pcg<false, float>;
+  else
+    fn = co ? (const void *)k_pcg<true, double> : (const void *)k_pcg<false, double>;
   RPBA_CUDA_CHECK(cudaLaunchCooperativeKernel(fn, dim3(g), dim3(PCG_T), args, 0, s));
   return 0;
 }

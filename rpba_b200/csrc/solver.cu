@@ -206,6 +206,7 @@ struct rpba_handle {
   rpba_report rep{};
 
   ~rpba_handle() {
+    coarse_release(CW);
     if (s) cudaStreamSynchronize(s);
     for (void *p : owned) cudaFree(p);
     if (s) {
@@ -215,16 +216,22 @@ struct rpba_handle {
     }
   }
 
+  // reduced camera system storage: FP64, or FP32 in the mixed form
   void ensure_blocks(int nb) {
-    if (nb <= blocks_cap && L.blocks) return;
+    const bool mixed = opt.precision == RPBA_PREC_MIXED;
+    void *cur = mixed ? (void *)L.blocks32 : (void *)L.blocks;
+    if (nb <= blocks_cap && cur) return;
     const int cap = std::max(nb, 1);
-    if (L.blocks) {
-      for (void *p : {(void *)L.blocks, (void *)S.ent, (void *)S.item_meta, (void *)W.part}) {
+    if (cur) {
+      for (void *p : {cur, (void *)S.ent, (void *)S.item_meta, (void *)W.part}) {
         cudaFree(p);
         owned.erase(std::remove(owned.begin(), owned.end(), p), owned.end());
       }
     }
-    L.blocks = dalloc<double>((size_t)(nimg + cap) * 81, owned);
+    if (mixed)
+      L.blocks32 = dalloc<float>((size_t)(nimg + cap) * 81, owned);
+    else
+      L.blocks = dalloc<double>((size_t)(nimg + cap) * 81, owned);
     S.ent = dalloc<int2>((size_t)nimg + 2 * (size_t)cap, owned);
     // SpMV work items: at most ceil(entries / 3) per row
     const size_t items = (size_t)nimg + ((size_t)nimg + 2 * (size_t)cap) / 3 + 1;
@@ -238,6 +245,7 @@ struct rpba_handle {
   // cameras of the first linear system (nullptr: none)
   CoarseWork CW{};
   bool coarse_built = false, coarse_stale = true;
+  int structure_version = 0;
   int coarse_ref_iters = 0;
   const CoarseWork *ensure_coarse() {
     if (opt.coarse_aggregates < 0) return nullptr;
@@ -317,9 +325,9 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   }
   {
     H->ES.max_grid = exact_sum_max_grid(H->dev);
-    H->ES.Rc = dalloc<long long>(H->ES.max_grid, own);
-    H->ES.Mc = dalloc<long long>(H->ES.max_grid, own);
-    H->ES.Tc = dalloc<int>(H->ES.max_grid, own);
+    H->ES.Rc = dalloc<long long>(2 * (size_t)H->ES.max_grid, own);
+    H->ES.Mc = dalloc<long long>(2 * (size_t)H->ES.max_grid, own);
+    H->ES.Tc = dalloc<int>(2 * (size_t)H->ES.max_grid, own);
     H->ES.ctl = dalloc<char>(16, own);
     H->ES.bar = dalloc<unsigned>(2, own);
     H->ES.err = dalloc<int>(4, own);
@@ -500,8 +508,13 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   L.XPM = dalloc<double>(H->xpmsize, own);
   L.XPMn = dalloc<double>(H->xpmsize, own);
   L.x = dalloc<double>(H->xpmsize, own);
-  L.rec = dalloc<double>((size_t)no * REC, own);
-  L.ptV = dalloc<double>((size_t)npp * PREC, own);
+  if (H->opt.precision == RPBA_PREC_MIXED) {
+    L.rec32 = dalloc<float>((size_t)no * REC, own);
+    L.ptV32 = dalloc<float>((size_t)npp * PREC, own);
+  } else {
+    L.rec = dalloc<double>((size_t)no * REC, own);
+    L.ptV = dalloc<double>((size_t)npp * PREC, own);
+  }
   L.camlist = dalloc<int>(no, own);
   L.coff = dalloc<int>(n + 1, own);
   L.rhs = dalloc<double>(9 * (size_t)n, own);
@@ -611,12 +624,19 @@ void rpba_handle::reset() {
 
 void rpba_handle::structure() {
   coarse_stale = true;
+  ++structure_version;
   long long npairs = 0;
   int nb = 0;
   PROF("structure_pairs", 3, nb = build_pairs(L, S, max_pairs, &npairs, s));
   npairs_cur = npairs;
   ensure_blocks(nb);
   PROF("structure_bsr", 6, build_bsr(L, S, s));
+  if (opt.verbose & 4) {
+    char line[160];
+    std::snprintf(line, sizeof line, "Structure: cameras %d points %d observations %d pair contributions %lld "
+                  "off-diagonal blocks %d work items %d\n", L.nimg, L.npts, L.nobs, npairs, L.nboff, L.nitems);
+    log += line;
+  }
 }
 
 // CalcBundleSep (rbacore.cpp:1094-1195): assemble, solve, back-substitute.
@@ -663,7 +683,7 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
       if (cw && (coarse_stale || attempt > 0)) {
         const double nc = CW.nc;
         prof.next_bytes = (Nc + 2. * Nb) * 648 + 3. * nc * nc * 8;
-        PROF("coarse_setup", 1, coarse_setup(L, CW, s));
+        PROF("coarse_setup", 1, coarse_setup(L, CW, structure_version, s));
         coarse_stale = false;
         fresh = true;
       }
@@ -696,8 +716,9 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
   }
   if (rec_T) {
     const CoarseWork *cw = ensure_coarse();
-    if (cw) coarse_setup(L, CW, s);
-    learned_record(L, cw, W.xbest, rec_seed + 104729ull * (unsigned long long)rep.linear_solves, *rec_T, *rec_H, s);
+    if (cw) coarse_setup(L, CW, structure_version, s);
+    learned_record(L, cw, W.xbest, W.Cinv, rec_seed + 104729ull * (unsigned long long)rep.linear_solves, *rec_T,
+                   *rec_H, s);
   }
   PROF("backsub", 1, launch_backsub(L, W.xbest, s));
   PROF("xcam", 1, launch_xcam(L, W.xbest, s));
@@ -1140,9 +1161,9 @@ int32_t rpba_float_sequential_sum(const float *v, int64_t n, int32_t device, flo
     cudaStream_t s = 0;
     ExactSumWork W{};
     W.max_grid = exact_sum_max_grid(a->dev);
-    W.Rc = dalloc<long long>(W.max_grid, own);
-    W.Mc = dalloc<long long>(W.max_grid, own);
-    W.Tc = dalloc<int>(W.max_grid, own);
+    W.Rc = dalloc<long long>(2 * (size_t)W.max_grid, own);
+    W.Mc = dalloc<long long>(2 * (size_t)W.max_grid, own);
+    W.Tc = dalloc<int>(2 * (size_t)W.max_grid, own);
     W.ctl = dalloc<char>(16, own);
     W.bar = dalloc<unsigned>(2, own);
     W.err = dalloc<int>(1, own);
@@ -1275,6 +1296,96 @@ int32_t rpba_precond_loss_grad(const rpba_precond_set *set, const float *weights
   }, &a);
 }
 
+namespace {
+
+// Record the systems of the direct solver's own LM iterations on the scenes
+// into TA (allocated here).
+int record_systems(const rpba_block *sc, int ns, const rpba_options *opt, const rpba_train_options &t,
+                   TrainAlloc &TA) {
+  RPBA_CUDA_CHECK(cudaSetDevice(opt->device));
+  const int probes = 1 + std::max(0, t.probes);
+  const int rows_cap = t.max_samples > 0 ? t.max_samples : 1 << 18;
+  TA.alloc(rows_cap, rows_cap * 96, rows_cap * 48, 4096, probes);
+  TA.T.uc = dalloc<float>((size_t)probes * rows_cap * 9, TA.own);
+  TA.H.vb = dalloc<double>(((size_t)rows_cap + 1) * 9, TA.own);
+  TA.H.vz = dalloc<double>(((size_t)rows_cap + 1) * 9, TA.own);
+  TA.H.rc = dalloc<int2>((size_t)rows_cap * 48, TA.own);
+  for (int i = 0; i < ns; ++i) {
+    rpba_options o = *opt;
+    o.solver = RPBA_SOLVER_DIRECT;
+    o.precision = RPBA_PREC_FP64;
+    o.exteval = 0;
+    rpba_handle *H = nullptr;
+    int st = rpba_create(&H, &sc[i], &o);
+    if (st != RPBA_OK) return st;
+    H->rec_T = &TA.T;
+    H->rec_H = &TA.H;
+    H->rec_seed = t.seed * 1000003ull + (unsigned long long)i;
+    rpba_report r{};
+    st = rpba_solve(H, &r);
+    rpba_destroy(H);
+    if (st != RPBA_OK) return st;
+  }
+  if (TA.T.systems <= 0) return (int)RPBA_ERR_ARG;
+  RPBA_CUDA_CHECK(cudaMemcpy(TA.T.sys_row, TA.H.sys_row.data(), sizeof(int) * (TA.T.systems + 1),
+                             cudaMemcpyHostToDevice));
+  return RPBA_OK;
+}
+
+}  // namespace
+
+int32_t rpba_record_systems(const rpba_block *scenes, int32_t nscenes, const rpba_options *opt,
+                            const rpba_train_options *topt, rpba_precond_buffers *out) {
+  if (!scenes || nscenes <= 0 || !opt || !topt || !out) return RPBA_ERR_ARG;
+  struct A {
+    const rpba_block *sc;
+    int ns;
+    const rpba_options *o;
+    const rpba_train_options *t;
+    rpba_precond_buffers *out;
+  } a{scenes, nscenes, opt, topt, out};
+  return guard([](void *p) {
+    A *a = (A *)p;
+    TrainAlloc TA;
+    const int st = record_systems(a->sc, a->ns, a->o, *a->t, TA);
+    if (st != RPBA_OK) return st;
+    const TrainSet &T = TA.T;
+    rpba_precond_buffers &o = *a->out;
+    const int rows = T.rows, nent = TA.H.ents, nb = TA.H.blocks, P = T.probes;
+    o.rows = rows;
+    o.systems = T.systems;
+    o.probes = P;
+    o.nent = nent;
+    o.nblocks = nb;
+    if (rows > o.rows_cap || nent > o.ents_cap || nb > o.blocks_cap || T.systems > o.systems_cap)
+      return (int)RPBA_ERR_TOO_LARGE;
+    auto down = [](void *h, const void *d, size_t n) {
+      if (h && n) RPBA_CUDA_CHECK(cudaMemcpy(h, d, n, cudaMemcpyDeviceToHost));
+    };
+    down(o.features, T.f, sizeof(float) * rows * NN_F);
+    down(o.sinv, T.sinv, sizeof(float) * rows * 81);
+    for (int pr = 0; pr < P; ++pr) {
+      down(o.b ? o.b + (size_t)pr * rows * 9 : nullptr, T.b + (size_t)pr * T.rows_cap * 9, sizeof(float) * rows * 9);
+      down(o.uc ? o.uc + (size_t)pr * rows * 9 : nullptr, T.uc + (size_t)pr * T.rows_cap * 9,
+           sizeof(float) * rows * 9);
+    }
+    down(o.xs, T.xs, sizeof(float) * rows * 9);
+    down(o.np, T.np, sizeof(int) * rows);
+    down(o.sys, T.sys, sizeof(int) * rows);
+    down(o.rowoff, T.rowoff, sizeof(int) * (rows + 1));
+    std::vector<int2> ent(std::max(nent, 1));
+    down(ent.data(), T.ent, sizeof(int2) * nent);
+    for (int i = 0; i < nent; ++i) {
+      if (o.ent_col) o.ent_col[i] = ent[i].x;
+      if (o.ent_blk) o.ent_blk[i] = ent[i].y;
+    }
+    down(o.blocks, T.blocks, sizeof(float) * (size_t)nb * 81);
+    if (o.sys_row)
+      for (int i = 0; i <= T.systems; ++i) o.sys_row[i] = TA.H.sys_row[i];
+    return (int)RPBA_OK;
+  }, &a);
+}
+
 int32_t rpba_train_preconditioner(const rpba_block *scenes, int32_t nscenes, const rpba_options *opt,
                                   const rpba_train_options *topt, float *weights, rpba_train_report *rep) {
   if (!scenes || nscenes <= 0 || !opt || !topt || !weights) return RPBA_ERR_ARG;
@@ -1290,34 +1401,11 @@ int32_t rpba_train_preconditioner(const rpba_block *scenes, int32_t nscenes, con
   return guard([](void *p) {
     A *a = (A *)p;
     const rpba_train_options &t = *a->t;
-    RPBA_CUDA_CHECK(cudaSetDevice(a->o->device));
-    const int probes = 1 + std::max(0, t.probes);
-    const int rows_cap = t.max_samples > 0 ? t.max_samples : 1 << 18;
     TrainAlloc TA;
-    TA.alloc(rows_cap, rows_cap * 96, rows_cap * 48, 4096, probes);
-    TA.T.uc = dalloc<float>((size_t)probes * rows_cap * 9, TA.own);
-    TA.H.vb = dalloc<double>(((size_t)rows_cap + 1) * 9, TA.own);
-    TA.H.vz = dalloc<double>(((size_t)rows_cap + 1) * 9, TA.own);
     // 1. systems of the direct solver's own LM iterations
-    for (int i = 0; i < a->ns; ++i) {
-      rpba_options o = *a->o;
-      o.solver = RPBA_SOLVER_DIRECT;
-      o.exteval = 0;
-      rpba_handle *H = nullptr;
-      int st = rpba_create(&H, &a->sc[i], &o);
-      if (st != RPBA_OK) return st;
-      if (!TA.H.rc) TA.H.rc = dalloc<int2>((size_t)rows_cap * 48, TA.own);
-      H->rec_T = &TA.T;
-      H->rec_H = &TA.H;
-      H->rec_seed = t.seed * 1000003ull + (unsigned long long)i;
-      rpba_report r{};
-      st = rpba_solve(H, &r);
-      rpba_destroy(H);
-      if (st != RPBA_OK) return st;
-    }
+    const int st = record_systems(a->sc, a->ns, a->o, t, TA);
+    if (st != RPBA_OK) return st;
     TrainSet &T = TA.T;
-    if (T.systems <= 0) return (int)RPBA_ERR_ARG;
-    RPBA_CUDA_CHECK(cudaMemcpy(T.sys_row, TA.H.sys_row.data(), sizeof(int) * (T.systems + 1), cudaMemcpyHostToDevice));
     TA.bufs();
     // 2. Adam on the one-step objective
     float *W = dalloc<float>(NN_WEIGHTS, TA.own), *m = dalloc<float>(NN_WEIGHTS, TA.own);

@@ -21,7 +21,7 @@ import os
 import numpy as np
 
 from .block import (Block, RpbaBlockC, RpbaOptionsC, RpbaReportC, RpbaTrainOptionsC, RpbaTrainReportC,
-                    RpbaPrecondSetC,
+                    RpbaPrecondSetC, RpbaPrecondBuffersC,
                     make_options, PRECOND_WEIGHTS, SOLVER_PCG, SOLVER_DIRECT, SOLVER_LEARNED, PREC_FP64,
                     PREC_MIXED)
 
@@ -38,7 +38,7 @@ EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block
            "rpba_output_block", "rpba_calc_plsa", "rpba_create", "rpba_solve",
            "rpba_get_state", "rpba_get_log", "rpba_exteval", "rpba_kernel_stats", "rpba_float_sequential_sum",
            "rpba_float_sequential_sum_noalloc", "rpba_train_preconditioner",
-           "rpba_set_preconditioner", "rpba_precond_loss_grad", "rpba_destroy")
+           "rpba_set_preconditioner", "rpba_precond_loss_grad", "rpba_record_systems", "rpba_destroy")
 
 _lib = None
 
@@ -91,6 +91,9 @@ def load():
     L.rpba_set_preconditioner.restype = C.c_int32
     L.rpba_precond_loss_grad.argtypes = [C.POINTER(RpbaPrecondSetC), fp, fp, fp]
     L.rpba_precond_loss_grad.restype = C.c_int32
+    L.rpba_record_systems.argtypes = [bp, C.c_int32, op, C.POINTER(RpbaTrainOptionsC),
+                                      C.POINTER(RpbaPrecondBuffersC)]
+    L.rpba_record_systems.restype = C.c_int32
     L.rpba_kernel_stats.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     L.rpba_kernel_stats.restype = C.c_int32
     L.rpba_destroy.argtypes = [C.c_void_p]
@@ -162,6 +165,44 @@ def train_preconditioner(blocks, steps=300, batch=0, lr=3e-3, probes=2, seed=1, 
     if st != 0:
         raise RpbaError(st, "rpba_train_preconditioner")
     return w, {k: getattr(rep, k) for k, _ in rep._fields_}
+
+
+def record_systems(blocks, probes=2, seed=1, max_samples=0, caps=None, **opt_kw) -> dict:
+    """The training set the GPU records for ``blocks`` (the direct solver's
+    own systems, diagonally scaled), as a dict of numpy arrays laid out as
+    ``precond_loss_grad`` takes them."""
+    arr = (RpbaBlockC * len(blocks))(*[b.as_c() for b in blocks])
+    o = make_options(**opt_kw)
+    t = RpbaTrainOptionsC(0, 0, 0.0, int(probes), int(max_samples), int(seed))
+    rows_cap, ents_cap, blocks_cap, sys_cap = caps or (0, 0, 0, 0)
+    for attempt in range(2):
+        P = 1 + max(0, int(probes))
+        arrs = {"features": np.zeros((rows_cap, 19), np.float32), "sinv": np.zeros((rows_cap, 81), np.float32),
+                "b": np.zeros((P, rows_cap, 9), np.float32), "xs": np.zeros((rows_cap, 9), np.float32),
+                "blocks": np.zeros((blocks_cap, 81), np.float32), "uc": np.zeros((P, rows_cap, 9), np.float32),
+                "np": np.zeros(rows_cap, np.int32), "sys": np.zeros(rows_cap, np.int32),
+                "rowoff": np.zeros(rows_cap + 1, np.int32), "ent_col": np.zeros(ents_cap, np.int32),
+                "ent_blk": np.zeros(ents_cap, np.int32), "sys_row": np.zeros(sys_cap + 1, np.int32)}
+        fp = lambda k: arrs[k].ctypes.data_as(C.POINTER(C.c_float))
+        ip = lambda k: arrs[k].ctypes.data_as(C.POINTER(C.c_int32))
+        buf = RpbaPrecondBuffersC(rows_cap, ents_cap, blocks_cap, sys_cap, 0, 0, 0, 0, 0,
+                                  fp("features"), fp("sinv"), fp("b"), fp("xs"), fp("blocks"), fp("uc"),
+                                  ip("np"), ip("sys"), ip("rowoff"), ip("ent_col"), ip("ent_blk"), ip("sys_row"))
+        st = load().rpba_record_systems(arr, len(blocks), C.byref(o), C.byref(t), C.byref(buf))
+        if st == 11 and attempt == 0:  # too large: retry with the reported sizes
+            rows_cap, ents_cap, blocks_cap, sys_cap = buf.rows, buf.nent, buf.nblocks, buf.systems
+            continue
+        if st != 0:
+            raise RpbaError(st, "rpba_record_systems")
+        break
+    R, S = buf.rows, buf.systems
+    out = {"rows": R, "systems": S, "probes": buf.probes,
+           "features": arrs["features"][:R], "sinv": arrs["sinv"][:R], "b": arrs["b"][:, :R],
+           "xs": arrs["xs"][:R], "blocks": arrs["blocks"][:buf.nblocks], "uc": arrs["uc"][:, :R],
+           "np": arrs["np"][:R], "sys": arrs["sys"][:R], "rowoff": arrs["rowoff"][:R + 1],
+           "ent_col": arrs["ent_col"][:buf.nent], "ent_blk": arrs["ent_blk"][:buf.nent],
+           "sys_row": arrs["sys_row"][:S + 1]}
+    return out
 
 
 def precond_loss_grad(ts: dict, weights):

@@ -75,3 +75,58 @@ def test_learned_correction_gain(city_blocks):
     assert learned["pcg_fallbacks"] == 0
     assert abs(learned["rms"] - ref["rms"]) <= 1e-6 * ref["rms"]
     assert learned["pcg_iterations"] <= 1.1 * plain["pcg_iterations"]
+
+
+def _spmv(ts, x):
+    """y = S~ x over the recorded block rows (numpy, float64)."""
+    R = ts["rows"]
+    blocks = ts["blocks"].astype(np.float64).reshape(-1, 9, 9)
+    blk = ts["ent_blk"].astype(np.int64) & 0xFFFFFFFF
+    tr = (blk & 0x80000000) != 0
+    B = blocks[blk & 0x7FFFFFFF]
+    B = np.where(tr[:, None, None], B.transpose(0, 2, 1), B)
+    rows = np.repeat(np.arange(R), np.diff(ts["rowoff"]))
+    y = np.zeros((R, 9))
+    np.add.at(y, rows, np.einsum("eac,ec->ea", B, x[ts["ent_col"]]))
+    return y
+
+
+def test_recorded_systems_are_consistent(city_blocks):
+    """The training set recorded from the direct solver's own LM steps:
+    each row's scaled block inverse inverts its scaled diagonal block, and
+    the recorded (scaled) step solves the recorded (scaled) system."""
+    import rpba_b200 as rb
+    train, _ = city_blocks
+    ts = rb.record_systems(train[:1], probes=2)
+    R = ts["rows"]
+    assert ts["systems"] >= 5 and R == ts["sys_row"][-1]
+    blocks = ts["blocks"].astype(np.float64).reshape(-1, 9, 9)
+    for r in range(0, R, max(1, R // 40)):
+        n = ts["np"][r]
+        e = [t for t in range(ts["rowoff"][r], ts["rowoff"][r + 1]) if ts["ent_col"][t] == r][0]
+        D = blocks[ts["ent_blk"][e] & 0x7FFFFFFF][:n, :n]
+        assert np.allclose(np.diag(D), 1.0, atol=1e-5)
+        Si = ts["sinv"][r].reshape(9, 9)[:n, :n].astype(np.float64)
+        assert np.abs(Si @ D - np.eye(n)).max() < 2e-3 * max(1.0, np.abs(Si).max())
+    # S~ x~* = b~ per system (float32 recording of an FP64 solve)
+    res = _spmv(ts, ts["xs"].astype(np.float64)) - ts["b"][0].astype(np.float64)
+    for s in range(ts["systems"]):
+        a, b = ts["sys_row"][s], ts["sys_row"][s + 1]
+        rel = np.linalg.norm(res[a:b]) / np.linalg.norm(ts["b"][0][a:b])
+        assert rel < 1e-2, (s, rel)
+
+
+def test_learned_gradient_on_recorded_systems(city_blocks):
+    """GPU loss and gradient against autograd on real recorded systems,
+    coarse part included."""
+    import rpba_b200 as rb
+    from oracle import learned_ref as lr
+    train, _ = city_blocks
+    ts = rb.record_systems(train[:1], probes=2)
+    rng = np.random.default_rng(5)
+    w = (rng.normal(size=rb.PRECOND_WEIGHTS) * 0.1).astype(np.float32)
+    L_gpu, g_gpu = rb.precond_loss_grad(ts, w)
+    L_ref, g_ref = lr.loss(ts, w)
+    assert np.isfinite(L_ref)
+    assert abs(L_gpu - L_ref) <= 1e-4 * max(1.0, abs(L_ref)), (L_gpu, L_ref)
+    assert np.abs(g_gpu - g_ref).max() <= 5e-3 * np.abs(g_ref).max()

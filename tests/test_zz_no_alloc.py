@@ -35,7 +35,7 @@ def test_noalloc_sum_matches_allocating_entry_point_twice():
     L = rb.load()
     rng = np.random.default_rng(123)
     inputs = [
-        (rng.normal(0, 0.5, 3_000_001) ** 2 * 2).astype(np.float32),             # ~733 CTAs
+        (rng.normal(0, 0.5, 3_000_001) ** 2 * 2).astype(np.float32),             # ~367 CTAs
         np.where(rng.random(NA_MAX_N) < 0.05, rng.uniform(0, 2500, NA_MAX_N),
                  rng.normal(0, 0.5, NA_MAX_N) ** 2).astype(np.float32),          # the maximum size
     ]
