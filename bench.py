@@ -1,19 +1,29 @@
 #!/usr/bin/env python
-"""Time to converge of the robust bundle adjuster on B200.
+"""Seconds to converge at matched final RMS reprojection error on one B200:
+the learned-PCG solver against the plain one.
 
-One step = one complete robust bundle adjustment (the reference's own stop
-rule: two passes, reweighting, RobustDelete) of a seeded synthetic scene
-that is already resident in HBM.  The default workload is the street scene
-(1,000 cameras, 189k points, 943k observations; the drop-in configuration)
-solved by the plain FP64 form with the reference's block-Jacobi PCG.
+One step = one complete robust bundle adjustment (the reference's stop rule:
+two LM passes, robust reweighting, RobustDelete) of a seeded synthetic scene
+that is already resident in HBM, timed on the device (CUDA events around the
+whole LM run).  The default workload is the city scene (13,700 cameras in 50
+clustered blocks, 4.5M points, ~29M observations).
+
+  ours   the learned two-level PCG solver in the mixed-precision form: FP32
+         Jacobians / Schur blocks, the learned block-Jacobi correction plus
+         the aggregate coarse space, inexact Newton with relative residual
+         tolerance --tol, weights from rpba_b200/precond_weights.npy
+  plain  the plain FP64 GPU solver: the reference's block-Jacobi PCG and its
+         stop rule (the drop-in form), timed in the same run
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
 
-With N > 1 (torchrun, one rank per GPU) every rank solves its own scene
+value = ours' median seconds; "plain" carries the plain solver's time and the
+matched-RMS check (ours' final RMS <= plain's x (1 + 1e-6)).  With N > 1
+(torchrun, one rank per GPU) every rank solves its own copy of the scene
 (independent replicas, no collective on the data path); the value is the
 slowest rank's time.  ``--impl reference`` times the reference algorithm's
 CPU implementation (the C++ restatement under oracle/, single-threaded like
-the reference's global LSA) on the host cores, rank 0 only.
+the reference's global LSA) on a bounded sample of the workload, rank 0 only.
 """
 from __future__ import annotations
 
@@ -24,7 +34,6 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 import numpy as np
@@ -38,9 +47,9 @@ WORKLOADS = {
     0: "arc: 50 cameras, 8k points, ~32k observations",
     1: "street: 1000 cameras, 190k points, ~950k observations",
     2: "aerial: 3000 cameras, 310k points, ~1.65M observations",
-    3: "city: 13700 cameras, 4.5M points, ~29M observations",
+    3: "city: 13700 cameras in 50 clusters, 4.5M points, ~29M observations",
 }
-SOLVERS = {"pcg": 0, "direct": 1, "learned": 2}
+RMS_MATCH = 1e-6
 
 
 def parse():
@@ -49,12 +58,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=1)
+    ap.add_argument("--config", type=int, default=3)
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--solver", default="pcg", choices=list(SOLVERS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--tol", type=float, default=1e-5, help="relative PCG tolerance of the learned solver")
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
+    ap.add_argument("--no-plain", action="store_true", help="skip timing the plain solver")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--cpu-sample-scale", type=float, default=0.01,
+                    help="scale of the scene the CPU baseline solves (bounded sample)")
+    ap.add_argument("--e2e-steps", type=int, default=1)
     return ap.parse_args()
 
 
@@ -65,6 +77,19 @@ def peaks():
             d = json.load(fh)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def traffic_ratio():
+    """DRAM bytes / algorithmic bytes of the PCG kernel from the committed ncu
+    summary (measured on a smaller case of the same scene family)."""
+    path = os.path.join(ROOT, "profiles", "k_pcg_traffic.txt")
+    if not os.path.exists(path):
+        return None, None
+    with open(path) as fh:
+        for line in fh:
+            if line.startswith("traffic_over_algorithmic:"):
+                return float(line.split(":")[1]), "profiles/k_pcg_traffic.txt"
+    return None, None
 
 
 class Clocks:
@@ -126,46 +151,62 @@ def state_bytes(b) -> int:
                                                      "pt_obs_slot")))
 
 
-def make_block(config, scale, rank):
+def make_block(config, scale, seed_offset=0):
     from rpba_b200 import scenes
-    seed = 20260 + config + 1000 * rank
-    return scenes.to_block(scenes.make_scene(config, scale=scale, seed=seed))
+    return scenes.to_block(scenes.make_scene(config, scale=scale, seed=20260 + config + seed_offset))
 
 
-def cpu_baseline(blk, opts_kw, max_seconds=60.0):
-    """The oracle (C++ restatement of the reference's global LSA) on the host:
-    one complete solve of the same scene, one thread."""
+def learned_weights():
+    from rpba_b200 import train_precond
+    w = train_precond.load()
+    if w is None:
+        raise RuntimeError("rpba_b200/precond_weights.npy is missing: python -m rpba_b200.train_precond")
+    return w
+
+
+def cpu_sample(config, scale):
+    """The oracle (C++ restatement of the reference's global LSA, one thread)
+    on a bounded sample: one complete solve of a scene of the same family at
+    `scale` of the workload's size."""
     import oracle
     import rpba_b200 as rb
-    o = rb.make_options(**opts_kw)
+    blk = make_block(config, scale)
     t0 = time.perf_counter()
-    st, _, rep, _ = oracle.calc_plsa(blk, o)
-    dt = time.perf_counter() - t0
-    return dt, rep, st
+    st, _, rep, _ = oracle.calc_plsa(blk, rb.make_options(solver=rb.SOLVER_PCG))
+    return time.perf_counter() - t0, rep, st, blk
+
+
+def config_dict(args, blk=None):
+    d = {"workload": WORKLOADS[args.config], "scale": args.scale, "robust": True, "addflags": "k2 k4 f",
+         "ours": f"learned two-level PCG, {args.precision}, relative tolerance {args.tol:g}",
+         "plain": "FP64 block-Jacobi PCG, the reference's stop rule",
+         "l2": "inputs larger than L2 (scene > 1 GB); 256 MB buffer written before every step",
+         "parallelism": f"replicas x{args.gpus}"}
+    if blk is not None:
+        d.update({"n_images": blk.n_images, "n_points": blk.n_points, "n_obs": blk.n_obs})
+    return d
 
 
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    blk = make_block(args.config, args.scale, 0)
-    kw = dict(solver=SOLVERS["direct" if args.solver == "direct" else "pcg"])
-    for _ in range(args.warmup):
-        cpu_baseline(blk, kw)
-    times = []
-    for _ in range(args.steps):
-        dt, rep, st = cpu_baseline(blk, kw)
-        times.append(dt)
-    v = statistics.mean(times)
+    times, rep, st, blk = [], None, 0, None
+    for i in range(args.warmup + args.steps):
+        dt, rep, st, blk = cpu_sample(args.config, args.cpu_sample_scale)
+        if i >= args.warmup:
+            times.append(dt)
+    v = statistics.median(times)
+    sample = (f"one complete solve (reference stop rule) of the same scene family at "
+              f"{args.cpu_sample_scale:g} of the workload: {blk.n_images} cameras, {blk.n_points} points, "
+              f"{blk.n_obs} observations; one thread (the reference's global LSA is single-threaded)")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOADS[args.config], "scale": args.scale, "solver": args.solver,
-                   "robust": True, "addflags": "k2 k4 f"},
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port",
-                         "sample": "complete solves of the scene (reference stop rule)",
-                         "linear_solves": rep["linear_solves"], "status": st},
+        "config": dict(config_dict(args), sample=sample),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample,
+                         "linear_solves": rep["linear_solves"], "final_rms": rep["rms"], "status": st},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -186,106 +227,137 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
 
     def barrier():
         if world > 1:
             dist.barrier()
 
-    blk = make_block(args.config, args.scale, rank)
-    solver_kw = dict(solver=SOLVERS[args.solver], precision=1 if args.precision == "mixed" else 0, device=local)
-    S = rb.Solver(blk, **solver_kw)
-    for _ in range(args.warmup):
-        S.solve()
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    blk = make_block(args.config, args.scale)
+    w = learned_weights()
+    prec = rb.PREC_MIXED if args.precision == "mixed" else rb.PREC_FP64
+    ours_kw = dict(solver=rb.SOLVER_LEARNED, precision=prec, pcg_tolerance=args.tol, device=local)
+    plain_kw = dict(solver=rb.SOLVER_PCG, precision=rb.PREC_FP64, device=local)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
     try:
         uuid = "GPU-" + str(torch.cuda.get_device_properties(local).uuid)
     except Exception:
         uuid = None
-    clk = Clocks(uuid)
-    times, reps = [], []
-    for _ in range(args.steps):
-        flush.zero_()
-        barrier()
-        torch.cuda.synchronize()
-        st, rep = S.solve()
-        torch.cuda.synchronize()
-        times.append(rep["solve_seconds"])
-        reps.append(rep)
-    barrier()
-    clocks = clk.stop()
-    t_mean = statistics.mean(times)
-    t = torch.tensor([t_mean], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    value = float(t.item())
 
-    # end to end through the C ABI with host buffers: create (H2D), solve,
-    # get_state (D2H), destroy -- the reference-facing CalcPLSA call
+    def timed(kw, weights, steps, warmup):
+        S = rb.Solver(blk, **kw)
+        if weights is not None:
+            S.set_preconditioner(weights)
+        for _ in range(warmup):
+            S.solve()
+        ts, reps = [], []
+        for _ in range(steps):
+            flush.zero_()
+            barrier()
+            torch.cuda.synchronize()
+            st, rep = S.solve()
+            torch.cuda.synchronize()
+            ts.append(rep["solve_seconds"])
+            reps.append(rep)
+        S.close()
+        return ts, reps
+
+    clk = Clocks(uuid)
+    times, reps = timed(ours_kw, w, args.steps, args.warmup)
+    clocks = clk.stop()
+    value = max_over_ranks(statistics.median(times))
+    plain = None
+    if not args.no_plain:
+        p_times, p_reps = timed(plain_kw, None, args.steps, args.warmup)
+        pv = max_over_ranks(statistics.median(p_times))
+        rms_o, rms_p = reps[-1]["rms"], p_reps[-1]["rms"]
+        plain = {"value": pv, "unit": UNIT, "final_rms": rms_p, "pcg_iterations": p_reps[-1]["pcg_iterations"],
+                 "linear_solves": p_reps[-1]["linear_solves"], "step_times": p_times,
+                 "speedup": pv / value, "rms_rel_diff": (rms_o - rms_p) / rms_p,
+                 "matched": bool(rms_o <= rms_p * (1 + RMS_MATCH))}
+
+    # end to end through the C ABI with host buffers: rpba_create (scene
+    # H2D), the weights, rpba_solve, rpba_get_state (D2H), rpba_destroy
     e2e_times = []
     for _ in range(max(1, args.e2e_steps)):
-        b = blk.copy()
         flush.zero_()
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        st_e, _, rep_e = rb.CalcPLSA(b, solver=solver_kw["solver"], precision=solver_kw["precision"], device=local)
+        S = rb.Solver(blk, **ours_kw)
+        S.set_preconditioner(w)
+        S.solve()
+        S.state()
+        S.close()
         torch.cuda.synchronize()
         e2e_times.append(time.perf_counter() - t0)
-    te = torch.tensor([statistics.mean(e2e_times)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e = max_over_ranks(statistics.median(e2e_times))
 
     # per-kernel device times of one more solve (CUDA events around launches)
-    P = rb.Solver(blk, verbose=2, **solver_kw)
+    P = rb.Solver(blk, verbose=2, **ours_kw)
+    P.set_preconditioner(w)
     P.solve()
     kstats = P.kernel_stats()
     P.close()
     hbm, peak_kind = peaks()
-    timed = {k: v for k, v in kstats.items() if v.get("bytes", 0) > 0}
-    dom = max(timed, key=lambda k: timed[k]["ms"]) if timed else None
+    timed_k = {k: v for k, v in kstats.items() if v.get("bytes", 0) > 0}
+    dom = max(timed_k, key=lambda k: timed_k[k]["ms"]) if timed_k else None
     roofline = None
     if dom:
-        d = timed[dom]
+        d = timed_k[dom]
         avg_s = d["ms"] * 1e-3 / d["launches"]
-        ach = d["bytes"] / d["launches"] / avg_s / 1e9
+        alg = d["bytes"] / d["launches"]
+        ach = alg / avg_s / 1e9
+        ratio, src = traffic_ratio() if dom == "pcg" else (None, None)
         roofline = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                    "frac": ach / hbm, "peak_kind": peak_kind, "traffic": None,
-                    "algorithmic_bytes_per_launch": d["bytes"] / d["launches"],
-                    "avg_launch_ms": d["ms"] / d["launches"]}
+                    "frac": ach / hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                    "traffic": alg * ratio if ratio else None,
+                    "traffic_note": (f"ncu DRAM bytes / algorithmic bytes = {ratio:.3f} from {src}, scaled to "
+                                     "this launch's algorithmic bytes") if ratio else None,
+                    "algorithmic_bytes_per_launch": alg, "avg_launch_ms": d["ms"] / d["launches"]}
     total_ms = sum(v["ms"] for v in kstats.values())
     kernel_share = {k: round(v["ms"] / total_ms, 4) for k, v in sorted(kstats.items(), key=lambda kv: -kv[1]["ms"])}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        dt, rep_c, st_c = cpu_baseline(blk, dict(solver=solver_kw["solver"]))
+        dt, rep_c, st_c, sblk = cpu_sample(args.config, args.cpu_sample_scale)
+        S = rb.Solver(sblk, **ours_kw)
+        S.set_preconditioner(w)
+        S.solve()
+        _, rep_g = S.solve()
+        S.close()
         cpu = {"value": dt, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": "one complete solve of the same scene on one host core",
-               "linear_solves": rep_c["linear_solves"], "final_rms": rep_c["rms"]}
+               "sample": (f"one complete solve of the same scene family at {args.cpu_sample_scale:g} of the "
+                          f"workload ({sblk.n_images} cameras, {sblk.n_obs} observations) on one host core"),
+               "linear_solves": rep_c["linear_solves"], "final_rms": rep_c["rms"],
+               "gpu_same_sample_s": rep_g["solve_seconds"]}
 
     if rank == 0:
         r0 = reps[-1]
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOADS[args.config], "scale": args.scale, "solver": args.solver,
-                       "precision": args.precision, "robust": True, "addflags": "k2 k4 f",
-                       "l2": "flushed before every step (256 MB write)", "parallelism": f"replicas x{world}",
-                       "n_images": blk.n_images, "n_points": blk.n_points, "n_obs": blk.n_obs},
-            "e2e": {"value": float(te.item()), "unit": UNIT, "h2d_bytes_per_step": block_bytes(blk),
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64" if prec else "f64", "data": "synthetic",
+            "config": config_dict(args, blk),
+            "plain": plain,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": block_bytes(blk),
                     "d2h_bytes_per_step": state_bytes(blk)},
             "gpu_launches": int(r0["kernel_launches"]),
             "roofline": roofline,
             "cpu_baseline": cpu,
             "clocks": clocks,
             "solve": {"linear_solves": r0["linear_solves"], "pcg_iterations": r0["pcg_iterations"],
-                      "final_rms": r0["rms"], "final_cost": r0["cost"], "obs_deleted": r0["obs_deleted"],
-                      "step_times": times},
+                      "pcg_fallbacks": r0["pcg_fallbacks"], "final_rms": r0["rms"], "final_cost": r0["cost"],
+                      "obs_deleted": r0["obs_deleted"], "step_times": times},
             "kernel_share": kernel_share,
         }
         print(json.dumps(line), flush=True)
-    S.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

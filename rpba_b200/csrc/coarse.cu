@@ -361,7 +361,7 @@ T *grow(T *&p, size_t &cap, size_t n) {
   return p;
 }
 
-void coarse_setup(const DevLSA &L, CoarseWork &C, int structure_version, cudaStream_t s) {
+void coarse_assemble(const DevLSA &L, CoarseWork &C, int structure_version, cudaStream_t s) {
   if (C.nagg <= 0) return;
   RPBA_CUDA_CHECK(cudaMemsetAsync(C.err, 0, sizeof(int), s));
   k_coarse_P<<<C.nagg, 128, 0, s>>>(L, C);
@@ -443,12 +443,23 @@ void coarse_setup(const DevLSA &L, CoarseWork &C, int structure_version, cudaStr
     k_coarse_blocks<<<(C.nsegs + 7) / 8, 256, 0, s>>>(C, C.nsegs);
   }
   k_coarse_fixdiag<<<(C.nc + 255) / 256, 256, 0, s>>>(C);
+  RPBA_CUDA_CHECK(cudaGetLastError());
+}
+
+void coarse_factor(CoarseWork &C, cudaStream_t s) {
+  if (C.nagg <= 0) return;
+  const size_t nn = (size_t)C.nc * C.nc;
   k_coarse_diag<<<(C.nc + 255) / 256, 256, 0, s>>>(C);
   k_coarse_scale<<<(int)((nn + 255) / 256), 256, 0, s>>>(C.Ac, C.dsc, C.nc, 1);
   dense_cholesky(C.Ac, C.nc, C.Linv, C.err, s);
   dense_spd_inverse(C.Ac, C.nc, C.Linv, C.X, C.Ainv, s);
   k_coarse_scale<<<(int)((nn + 255) / 256), 256, 0, s>>>(C.Ainv, C.dsc, C.nc, 0);
   RPBA_CUDA_CHECK(cudaGetLastError());
+}
+
+void coarse_setup(const DevLSA &L, CoarseWork &C, int structure_version, cudaStream_t s) {
+  coarse_assemble(L, C, structure_version, s);
+  coarse_factor(C, s);
 }
 
 void coarse_release(CoarseWork &C) {

@@ -168,6 +168,9 @@ void coarse_build(const DevLSA &L, int max_aggs, CoarseWork &C, std::vector<void
 // Per linear system: P, the Galerkin matrix P^T S P and its inverse (the
 // run structure of the assembly is rebuilt when structure_version changes).
 void coarse_setup(const DevLSA &L, CoarseWork &C, int structure_version, cudaStream_t s);
+// the two halves of coarse_setup: P and P^T S P; the factorisation and inverse
+void coarse_assemble(const DevLSA &L, CoarseWork &C, int structure_version, cudaStream_t s);
+void coarse_factor(CoarseWork &C, cudaStream_t s);
 void coarse_release(CoarseWork &C);
 // h += P A_c^-1 P^T r over the rows of the system.
 void coarse_apply(const DevLSA &L, const CoarseWork &C, const double *r, double *h, cudaStream_t s);
@@ -248,6 +251,26 @@ struct StructWork {
   int4 *item_meta;
 };
 size_t structure_cub_bytes(int nobs, long long npairs, int nimg);
+// PointXXvIn on the device (structure.cu): the caller's block in device
+// memory, the scan scratch, and the track-ordered outputs.
+struct TrackIn {
+  const int *pt_off, *pt_img, *pt_slot, *img_off;
+  const float *xg, *wx, *wy, *wxy, *XX;
+  int np, n;
+};
+struct TrackScan {
+  int *cnt, *pval, *ooff, *pidx, *err;  // [np + 1]
+  long long *pairs, *psum;              // [np], [1]
+};
+struct TrackOut {
+  int *o_cam, *o_slot, *o_pt, *pt_off, *pt_id;
+  float2 *o_xg;
+  float4 *o_w;
+  double *X;
+};
+// returns the error bits (1: an index out of range, 2: an image twice in a track)
+int track_count(const TrackIn &T, TrackScan &W, int *nobs, int *npts, long long *max_pairs, cudaStream_t s);
+void track_scatter(const TrackIn &T, const TrackScan &W, const TrackOut &O, int nobs, int npts, cudaStream_t s);
 // camera grouping: returns 0, fills camlist/coff; counts in ccnt
 void build_camera_order(DevLSA &L, StructWork &S, cudaStream_t s);
 // pair structure: returns number of off-diagonal blocks (syncs the stream)

@@ -318,11 +318,6 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   H->h_pt_off.assign(b->pt_obs_off, b->pt_obs_off + np + 1);
   H->h_pt_img.assign(b->pt_obs_image, b->pt_obs_image + H->n_track_in);
   H->h_pt_slot.assign(b->pt_obs_slot, b->pt_obs_slot + H->n_track_in);
-  for (int i = 0; i < H->n_track_in; ++i) {
-    const int im = H->h_pt_img[i];
-    if (im < 0 || im >= n || H->h_pt_slot[i] < 0 || H->h_pt_slot[i] >= H->h_img_off[im + 1] - H->h_img_off[im])
-      return RPBA_ERR_ARG;
-  }
   {
     H->ES.max_grid = exact_sum_max_grid(H->dev);
     H->ES.Rc = dalloc<long long>(2 * (size_t)H->ES.max_grid, own);
@@ -333,7 +328,14 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
     H->ES.err = dalloc<int>(4, own);
     RPBA_CUDA_CHECK(cudaMemsetAsync(H->ES.err, 0, 4 * sizeof(int), H->s));
   }
-  if (o->exteval) return RPBA_OK;
+  if (o->exteval) {
+    for (int i = 0; i < H->n_track_in; ++i) {
+      const int im = H->h_pt_img[i];
+      if (im < 0 || im >= n || H->h_pt_slot[i] < 0 || H->h_pt_slot[i] >= H->h_img_off[im + 1] - H->h_img_off[im])
+        return RPBA_ERR_ARG;
+    }
+    return RPBA_OK;
+  }
 
   // ihw2 / defdiff for iwidth = iheight = 1 (rpba.cpp:264-265, rpbacore.cpp:87-90, rbacore.cpp:48)
   float ihw2 = 0.f;
@@ -343,40 +345,56 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   H->defdiff = 5000. / (double)std::sqrt(ihw2);
   H->minimagenrdel = n > 2 ? 3 : 2;
 
-  // PointXXvIn (rbacore.cpp:1918-1974): points with >= 2 observations and |Z| > 1e-8
-  std::vector<int> pt_id, pt_off{0}, o_cam, o_slot, o_pt;
-  std::vector<float2> o_xg;
-  std::vector<float4> o_w;
-  for (int i = 0; i < np; ++i) {
-    const int s0 = H->h_pt_off[i], s1 = H->h_pt_off[i + 1];
-    int cnt = 0;
-    for (int j = s0; j < s1; ++j)
-      if (H->h_pt_img[j] > -1) ++cnt;
-    if (!(std::fabs((double)b->XX[3 * i + 2]) > 1.e-8 && cnt >= 2)) continue;
-    const int q = (int)pt_id.size();
-    for (int j = s0; j < s1; ++j) {
-      const int im = H->h_pt_img[j];
-      if (im < 0) continue;
-      for (int jj = s0; jj < j; ++jj)
-        if (H->h_pt_img[jj] == im) return RPBA_ERR_UNSUPPORTED;  // image twice in one track
-      const int sl = H->h_img_off[im] + H->h_pt_slot[j];
-      o_cam.push_back(im);
-      o_slot.push_back(H->h_pt_slot[j]);
-      o_pt.push_back(q);
-      o_xg.push_back(make_float2(b->xg[2 * sl], b->xg[2 * sl + 1]));
-      o_w.push_back(make_float4(b->wx[sl], b->wy[sl], b->wxy[sl], 0.f));
+  // PointXXvIn (rbacore.cpp:1918-1974): points with >= 2 observations and
+  // |Z| > 1e-8, track order, compacted on the device from the caller's
+  // arrays (also validated there: image and slot indices in range, no image
+  // twice in one track)
+  std::vector<void *> tmp;
+  auto tmalloc = [&](size_t bytes) {
+    void *p = nullptr;
+    RPBA_CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+    tmp.push_back(p);
+    return p;
+  };
+  struct TmpFree {
+    std::vector<void *> &v;
+    ~TmpFree() {
+      for (void *p : v) cudaFree(p);
     }
-    pt_id.push_back(i);
-    pt_off.push_back((int)o_cam.size());
-  }
-  const int npts = (int)pt_id.size(), nobs = (int)o_cam.size();
+  } tmp_free{tmp};
+  auto upt = [&](const void *h, size_t bytes) {
+    void *d = tmalloc(bytes);
+    if (bytes) RPBA_CUDA_CHECK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, H->s));
+    return d;
+  };
+  TrackIn TI;
+  TI.np = np;
+  TI.n = n;
+  TI.pt_off = (const int *)upt(b->pt_obs_off, sizeof(int) * (np + 1));
+  TI.pt_img = (const int *)upt(b->pt_obs_image, sizeof(int) * H->n_track_in);
+  TI.pt_slot = (const int *)upt(b->pt_obs_slot, sizeof(int) * H->n_track_in);
+  TI.img_off = (const int *)upt(b->img_obs_off, sizeof(int) * (n + 1));
+  TI.xg = (const float *)upt(b->xg, sizeof(float) * 2 * H->n_slots);
+  TI.wx = (const float *)upt(b->wx, sizeof(float) * H->n_slots);
+  TI.wy = (const float *)upt(b->wy, sizeof(float) * H->n_slots);
+  TI.wxy = (const float *)upt(b->wxy, sizeof(float) * H->n_slots);
+  TI.XX = (const float *)upt(b->XX, sizeof(float) * 3 * np);
+  TrackScan TW;
+  TW.cnt = (int *)tmalloc(sizeof(int) * (np + 1));
+  TW.pval = (int *)tmalloc(sizeof(int) * (np + 1));
+  TW.ooff = (int *)tmalloc(sizeof(int) * (np + 1));
+  TW.pidx = (int *)tmalloc(sizeof(int) * (np + 1));
+  TW.err = (int *)tmalloc(sizeof(int));
+  TW.pairs = (long long *)tmalloc(sizeof(long long) * std::max(np, 1));
+  TW.psum = (long long *)tmalloc(sizeof(long long));
+  int nobs = 0, npts = 0;
+  long long max_pairs = 0;
+  const int terr = track_count(TI, TW, &nobs, &npts, &max_pairs, H->s);
+  if (terr & 1) return RPBA_ERR_ARG;
+  if (terr & 2) return RPBA_ERR_UNSUPPORTED;
   H->npts0 = npts;
   H->nobs0 = nobs;
-  H->max_pairs = 0;
-  for (int q = 0; q < npts; ++q) {
-    const long long t = pt_off[q + 1] - pt_off[q];
-    H->max_pairs += t * (t - 1) / 2;
-  }
+  H->max_pairs = max_pairs;
   if (H->max_pairs > 0x7fffffffll) return RPBA_ERR_UNSUPPORTED;
 
   // PrepareCameras (rbacore.cpp:670-700)
@@ -438,9 +456,6 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
     dc[2 * i] = b->distpara[2 * i];
     dc[2 * i + 1] = b->distpara[2 * i + 1];
   }
-  std::vector<double> X0(3 * (size_t)std::max(npts, 1));
-  for (int q = 0; q < npts; ++q)
-    for (int j = 0; j < 3; ++j) X0[3 * q + j] = (double)b->XX[3 * pt_id[q] + j];
 
   // ---- device buffers
   const int no = std::max(nobs, 1), npp = std::max(npts, 1);
@@ -459,17 +474,21 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   auto up = [&](void *d, const void *h, size_t bytes) {
     if (bytes) RPBA_CUDA_CHECK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, H->s));
   };
-  up(H->d0_o_cam, o_cam.data(), sizeof(int) * nobs);
-  up(H->d0_o_slot, o_slot.data(), sizeof(int) * nobs);
-  up(H->d0_o_pt, o_pt.data(), sizeof(int) * nobs);
-  up(H->d0_o_xg, o_xg.data(), sizeof(float2) * nobs);
-  up(H->d0_o_wold, o_w.data(), sizeof(float4) * nobs);
-  up(H->d0_pt_off, pt_off.data(), sizeof(int) * (npts + 1));
-  up(H->d0_pt_id, pt_id.data(), sizeof(int) * npts);
+  {
+    TrackOut TO;
+    TO.o_cam = H->d0_o_cam;
+    TO.o_slot = H->d0_o_slot;
+    TO.o_pt = H->d0_o_pt;
+    TO.o_xg = H->d0_o_xg;
+    TO.o_w = H->d0_o_wold;
+    TO.pt_off = H->d0_pt_off;
+    TO.pt_id = H->d0_pt_id;
+    TO.X = H->d0_X;
+    track_scatter(TI, TW, TO, nobs, npts, H->s);
+  }
   up(H->d0_P, P.data(), sizeof(double) * P.size());
   up(H->d0_Kc, Kc.data(), sizeof(double) * Kc.size());
   up(H->d0_dc, dc.data(), sizeof(double) * dc.size());
-  up(H->d0_X, X0.data(), sizeof(double) * 3 * npts);
   up(H->d0_camn, cams.data(), sizeof(CamState) * n);
 
   DevLSA &L = H->L;
@@ -682,8 +701,10 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
     for (int attempt = 0; attempt < 2; ++attempt) {
       if (cw && (coarse_stale || attempt > 0)) {
         const double nc = CW.nc;
-        prof.next_bytes = (Nc + 2. * Nb) * 648 + 3. * nc * nc * 8;
-        PROF("coarse_setup", 1, coarse_setup(L, CW, structure_version, s));
+        prof.next_bytes = (Nc + 2. * Nb) * (L.blocks32 ? 324. : 648.) + nc * nc * 8;
+        PROF("coarse_assemble", 4, coarse_assemble(L, CW, structure_version, s));
+        prof.next_bytes = 4. * nc * nc * 8;
+        PROF("coarse_factor", 4, coarse_factor(CW, s));
         coarse_stale = false;
         fresh = true;
       }
@@ -693,6 +714,19 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
       if (cw) RPBA_CUDA_CHECK(cudaMemcpyAsync(it + 2, CW.err, sizeof(int), cudaMemcpyDeviceToHost, s));
       RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
       learned_iters += it[0];
+      if (prof.on) {
+        // per iteration: blocks read from both sides plus their entries,
+        // per camera row the preconditioner (648), 22 reads/writes of
+        // 9-vectors, and with the coarse space P_k twice (720 each) and the
+        // block part of h twice; A_c^-1 stays in L2 and is not counted
+        const double Nc = nimg - begini, Nb = L.nboff, bs = L.blocks32 ? 324. : 648.;
+        const double row = 648. + 22. * 72. + (cw ? 2. * 720. + 2. * 72. : 0.);
+        for (auto itp = prof.pending.rbegin(); itp != prof.pending.rend(); ++itp)
+          if (std::string(itp->name) == "pcg") {
+            itp->bytes = (double)it[0] * ((bs + 8.) * (Nc + 2. * Nb) + Nc * row);
+            break;
+          }
+      }
       if (fresh) coarse_ref_iters = it[0];
       const bool conv = (mode == 1 ? it[1] != 0 : it[0] < cap_try) && it[2] == 0;
       if (conv || fresh || !cw) break;

@@ -243,6 +243,94 @@ void build_bsr(DevLSA &L, StructWork &S, cudaStream_t s) {
   L.item_meta = S.item_meta;
 }
 
+// ---- PointXXvIn (rbacore.cpp:1918-1974) on the device: the track-ordered
+// observation arrays (point major, observations in track order) of the
+// points with at least two observations and |Z| > 1e-8.
+namespace {
+
+__global__ void k_track_count(TrackIn T, int *cnt, int *pval, long long *pairs, int *err) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p > T.np) return;
+  if (p == T.np) {  // exclusive-scan sentinels
+    cnt[p] = 0;
+    pval[p] = 0;
+    return;
+  }
+  const int s0 = T.pt_off[p], s1 = T.pt_off[p + 1];
+  int c = 0;
+  for (int j = s0; j < s1; ++j) {
+    const int im = T.pt_img[j];
+    if (im < 0 || im >= T.n) {
+      atomicOr(err, 1);
+      continue;
+    }
+    const int sl = T.pt_slot[j];
+    if (sl < 0 || sl >= T.img_off[im + 1] - T.img_off[im]) atomicOr(err, 1);
+    for (int jj = s0; jj < j; ++jj)
+      if (T.pt_img[jj] == im) atomicOr(err, 2);  // an image twice in one track
+    ++c;
+  }
+  const bool valid = fabs((double)T.XX[3 * p + 2]) > 1.e-8 && c >= 2;
+  cnt[p] = valid ? c : 0;
+  pval[p] = valid ? 1 : 0;
+  pairs[p] = valid ? (long long)c * (c - 1) / 2 : 0;
+}
+
+__global__ void k_track_scatter(TrackIn T, const int *ooff, const int *pidx, const int *pval, TrackOut O) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= T.np || !pval[p]) return;
+  const int q = pidx[p];
+  int o = ooff[p];
+  O.pt_id[q] = p;
+  O.pt_off[q] = o;
+  for (int j = 0; j < 3; ++j) O.X[3 * (size_t)q + j] = (double)T.XX[3 * (size_t)p + j];
+  for (int j = T.pt_off[p]; j < T.pt_off[p + 1]; ++j, ++o) {
+    const int im = T.pt_img[j], slot = T.pt_slot[j];
+    const size_t sl = (size_t)T.img_off[im] + slot;
+    O.o_cam[o] = im;
+    O.o_slot[o] = slot;
+    O.o_pt[o] = q;
+    O.o_xg[o] = make_float2(T.xg[2 * sl], T.xg[2 * sl + 1]);
+    O.o_w[o] = make_float4(T.wx[sl], T.wy[sl], T.wxy[sl], 0.f);
+  }
+}
+
+}  // namespace
+
+int track_count(const TrackIn &T, TrackScan &W, int *nobs, int *npts, long long *max_pairs, cudaStream_t s) {
+  const int n1 = T.np + 1;
+  RPBA_CUDA_CHECK(cudaMemsetAsync(W.err, 0, sizeof(int), s));
+  k_track_count<<<(n1 + 255) / 256, 256, 0, s>>>(T, W.cnt, W.pval, W.pairs, W.err);
+  size_t b1 = 0, b2 = 0, b3 = 0;
+  RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, b1, W.cnt, W.ooff, n1, s));
+  RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(nullptr, b2, W.pval, W.pidx, n1, s));
+  RPBA_CUDA_CHECK(cub::DeviceReduce::Sum(nullptr, b3, W.pairs, W.psum, std::max(T.np, 1), s));
+  const size_t need = std::max(b1, std::max(b2, b3));
+  void *tmp = nullptr;
+  RPBA_CUDA_CHECK(cudaMallocAsync(&tmp, need, s));
+  RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(tmp, b1, W.cnt, W.ooff, n1, s));
+  RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(tmp, b2, W.pval, W.pidx, n1, s));
+  RPBA_CUDA_CHECK(cub::DeviceReduce::Sum(tmp, b3, W.pairs, W.psum, std::max(T.np, 1), s));
+  RPBA_CUDA_CHECK(cudaFreeAsync(tmp, s));
+  int hv[3] = {0, 0, 0};
+  long long hp = 0;
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(hv, W.ooff + T.np, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(hv + 1, W.pidx + T.np, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(hv + 2, W.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(&hp, W.psum, sizeof(long long), cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+  *nobs = hv[0];
+  *npts = hv[1];
+  *max_pairs = T.np > 0 ? hp : 0;
+  return hv[2];
+}
+
+void track_scatter(const TrackIn &T, const TrackScan &W, const TrackOut &O, int nobs, int npts, cudaStream_t s) {
+  if (T.np > 0) k_track_scatter<<<(T.np + 255) / 256, 256, 0, s>>>(T, W.ooff, W.pidx, W.pval, O);
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(O.pt_off + npts, &nobs, sizeof(int), cudaMemcpyHostToDevice, s));
+  RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+}
+
 cudaError_t cub_exclusive_sum_int(void *tmp, size_t &bytes, const int *in, int *out, int n, cudaStream_t s) {
   return cub::DeviceScan::ExclusiveSum(tmp, bytes, in, out, n, s);
 }
