@@ -218,26 +218,16 @@ def main():
     if args.impl == "reference":
         return run_reference(args)
     import torch
-    import torch.distributed as dist
     import rpba_b200 as rb
+
+    from rpba_b200.replicas import Group, time_steps
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    g = Group(rank, world, "nccl", 600.0, device=torch.device("cuda", local))
+    barrier, max_over_ranks = g.barrier, g.max
 
     blk = make_block(args.config, args.scale)
     w = learned_weights()
@@ -254,28 +244,27 @@ def main():
         S = rb.Solver(blk, **kw)
         if weights is not None:
             S.set_preconditioner(weights)
-        for _ in range(warmup):
-            S.solve()
-        ts, reps = [], []
-        for _ in range(steps):
-            flush.zero_()
-            barrier()
+        reps = []
+
+        def step():
             torch.cuda.synchronize()
             st, rep = S.solve()
             torch.cuda.synchronize()
-            ts.append(rep["solve_seconds"])
             reps.append(rep)
+            return rep["solve_seconds"]
+
+        res = time_steps(g, step, steps, warmup, before_step=flush.zero_)
         S.close()
-        return ts, reps
+        return res, reps[warmup:]
 
     clk = Clocks(uuid)
-    times, reps = timed(ours_kw, w, args.steps, args.warmup)
+    res, reps = timed(ours_kw, w, args.steps, args.warmup)
     clocks = clk.stop()
-    value = max_over_ranks(statistics.median(times))
+    times, value = res["times"], res["max_over_ranks"]
     plain = None
     if not args.no_plain:
-        p_times, p_reps = timed(plain_kw, None, args.steps, args.warmup)
-        pv = max_over_ranks(statistics.median(p_times))
+        p_res, p_reps = timed(plain_kw, None, args.steps, args.warmup)
+        p_times, pv = p_res["times"], p_res["max_over_ranks"]
         rms_o, rms_p = reps[-1]["rms"], p_reps[-1]["rms"]
         plain = {"value": pv, "unit": UNIT, "final_rms": rms_p, "pcg_iterations": p_reps[-1]["pcg_iterations"],
                  "linear_solves": p_reps[-1]["linear_solves"], "step_times": p_times,
@@ -358,9 +347,7 @@ def main():
             "kernel_share": kernel_share,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    g.close()
     return 0
 
 

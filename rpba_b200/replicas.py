@@ -1,0 +1,78 @@
+"""Independent replicas over ranks: one process per GPU, each solving its own
+scene, with no collective on the data path.
+
+The reference's global LSA does not shard (one linear system per LM step);
+its own parallel form partitions the scene into independent LSAs
+(rpbacore.cpp:100-510).  Across GPUs this library therefore runs replicas:
+every rank times its own solves, and the job's time is the slowest rank's
+(max over ranks), its throughput the units of all ranks over that time.
+Only these host-side reductions cross ranks, through torch.distributed
+(NCCL on GPUs, gloo on CPU).
+"""
+from __future__ import annotations
+
+import statistics
+from datetime import timedelta
+from typing import Callable
+
+
+class Group:
+    """torch.distributed plumbing of a replica job (world 1: no-op)."""
+
+    def __init__(self, rank: int, world: int, backend: str = "nccl", timeout_s: float = 600.0,
+                 device=None, init_method: str | None = None):
+        import torch.distributed as dist
+        self.rank, self.world, self.dist = rank, world, dist
+        self.device = device
+        if world > 1 and not dist.is_initialized():
+            kw = {"timeout": timedelta(seconds=timeout_s)}
+            if init_method:
+                kw.update(init_method=init_method, rank=rank, world_size=world)
+            if device is not None and backend == "nccl":
+                kw["device_id"] = device
+            dist.init_process_group(backend, **kw)
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        """Max over ranks (every rank gets it)."""
+        if self.world == 1:
+            return float(x)
+        import torch
+        t = torch.tensor([float(x)], dtype=torch.float64,
+                         device=self.device if self.device is not None else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def gather(self, obj) -> list:
+        """Every rank's object, in rank order (on every rank)."""
+        if self.world == 1:
+            return [obj]
+        out = [None] * self.world
+        self.dist.all_gather_object(out, obj)
+        return out
+
+    def close(self):
+        if self.world > 1 and self.dist.is_initialized():
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+
+
+def time_steps(g: Group, step: Callable[[], float], steps: int, warmup: int,
+               before_step: Callable[[], None] | None = None) -> dict:
+    """Warm-up, then `steps` timed calls of `step` (which returns its own
+    device-measured seconds), a barrier before every step.  Returns this
+    rank's step times, its median, and the max of the medians over ranks."""
+    for _ in range(warmup):
+        step()
+    times = []
+    for _ in range(steps):
+        if before_step is not None:
+            before_step()
+        g.barrier()
+        times.append(float(step()))
+    g.barrier()
+    med = statistics.median(times)
+    return {"times": times, "median": med, "max_over_ranks": g.max(med)}
