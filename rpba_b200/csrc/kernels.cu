@@ -320,42 +320,63 @@ __global__ void k_pair(DevLSA L) {
   if (wid >= L.nboff) return;
   T *s = sm[wl];
   Acc<T> acc[3];
+  const T *rec = Store<T>::rec(L), *ptv = Store<T>::ptV(L);
+  // lane's two record values of one contribution: 24 of the row camera's
+  // observation (Bc 18, G 6), 24 of the column camera's, V^-1 (9) of the point
+  auto fetch = [&](int ox, int oy, int p, T &v0, T &v1) {
+    v0 = lane < 24 ? rec[(size_t)ox * REC + lane] : rec[(size_t)oy * REC + lane - 24];
+    const int i1 = lane + 32;
+    v1 = i1 < 48 ? rec[(size_t)oy * REC + i1 - 24] : (i1 < 57 ? ptv[(size_t)p * PREC + i1 - 48] : T(0));
+  };
   const int cb = L.boff[wid], ce = L.boff[wid + 1];
-  for (int c = cb; c < ce; ++c) {
-    const int2 pr = L.contrib[c];
-    const int p = L.o_pt[pr.x];
-    const T *rs = Store<T>::rec(L) + (size_t)pr.x * REC;
-    const T *rt = Store<T>::rec(L) + (size_t)pr.y * REC;
-    const T *pv = Store<T>::ptV(L) + (size_t)p * PREC;
-    for (int idx = lane; idx < 57; idx += 32)
-      s[idx] = idx < 24 ? rs[idx] : (idx < 48 ? rt[idx - 24] : pv[idx - 48]);
-    __syncwarp();
-    // N = G_s V^-1 G_t^T (2 x 2)
-    const T *Gs = s + 18, *Gt = s + 42, *Vi = s + 48;
-    T GV[2][3];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int b = 0; b < 3; ++b)
-        GV[a][b] = Gs[a * 3] * Vi[b] + Gs[a * 3 + 1] * Vi[3 + b] + Gs[a * 3 + 2] * Vi[6 + b];
-    T N[2][2];
-#pragma unroll
-    for (int a = 0; a < 2; ++a)
-#pragma unroll
-      for (int b = 0; b < 2; ++b)
-        N[a][b] = GV[a][0] * Gt[b * 3] + GV[a][1] * Gt[b * 3 + 1] + GV[a][2] * Gt[b * 3 + 2];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      const int e = lane + 32 * q;
-      if (e < 81) {
-        const int i = e / 9, j = e % 9;
-        const T bt0 = s[24 + j], bt1 = s[24 + 9 + j];
-        const T t0 = N[0][0] * bt0 + N[0][1] * bt1;
-        const T t1 = N[1][0] * bt0 + N[1][1] * bt1;
-        acc[q].add(-(s[i] * t0 + s[9 + i] * t1));
-      }
+  for (int c0 = cb; c0 < ce; c0 += 32) {
+    // the next (up to) 32 contributions' observation pairs and points, one
+    // per lane; the record values of contribution j + 1 are fetched while j
+    // is accumulated
+    const int n = min(32, ce - c0);
+    int2 pr = make_int2(0, 0);
+    int pp = 0;
+    if (lane < n) {
+      pr = L.contrib[c0 + lane];
+      pp = L.o_pt[pr.x];
     }
-    __syncwarp();
+    T v0, v1;
+    fetch(__shfl_sync(0xffffffffu, pr.x, 0), __shfl_sync(0xffffffffu, pr.y, 0), __shfl_sync(0xffffffffu, pp, 0),
+          v0, v1);
+    for (int j = 0; j < n; ++j) {
+      s[lane] = v0;
+      if (lane + 32 < 57) s[lane + 32] = v1;
+      if (j + 1 < n)
+        fetch(__shfl_sync(0xffffffffu, pr.x, j + 1), __shfl_sync(0xffffffffu, pr.y, j + 1),
+              __shfl_sync(0xffffffffu, pp, j + 1), v0, v1);
+      __syncwarp();
+      // N = G_s V^-1 G_t^T (2 x 2)
+      const T *Gs = s + 18, *Gt = s + 42, *Vi = s + 48;
+      T GV[2][3];
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 3; ++b)
+          GV[a][b] = Gs[a * 3] * Vi[b] + Gs[a * 3 + 1] * Vi[3 + b] + Gs[a * 3 + 2] * Vi[6 + b];
+      T N[2][2];
+#pragma unroll
+      for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+          N[a][b] = GV[a][0] * Gt[b * 3] + GV[a][1] * Gt[b * 3 + 1] + GV[a][2] * Gt[b * 3 + 2];
+#pragma unroll
+      for (int q = 0; q < 3; ++q) {
+        const int e = lane + 32 * q;
+        if (e < 81) {
+          const int i = e / 9, jj = e % 9;
+          const T bt0 = s[24 + jj], bt1 = s[24 + 9 + jj];
+          const T t0 = N[0][0] * bt0 + N[0][1] * bt1;
+          const T t1 = N[1][0] * bt0 + N[1][1] * bt1;
+          acc[q].add(-(s[i] * t0 + s[9 + i] * t1));
+        }
+      }
+      __syncwarp();
+    }
   }
   T *B = Store<T>::blocks(L) + (size_t)(L.nimg + wid) * 81;
 #pragma unroll

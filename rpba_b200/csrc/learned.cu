@@ -39,8 +39,11 @@ constexpr float ALPHA = 1.0f;
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
 // Features of camera row k (>= begini) of the assembled system, computed by
-// one warp (the row's entries are split over the lanes and the coupling sums
-// reduced in a fixed butterfly order); every lane returns the same f.
+// one warp.  Lane l owns the block elements e = l, l + 32, l + 64 of every
+// off-diagonal block of the row (coalesced reads of the 81 values) and keeps
+// their normalised magnitudes in two accumulators, for the block stored as
+// (k, l) and as (l, k); the coupling sum of parameter a is then reduced over
+// the lanes in a fixed butterfly order.  Every lane returns the same f.
 __device__ void block_features(const DevLSA &L, int k, int lane, float f[NN_F]) {
   const int np = L.camparv[k + 1] - L.camparv[k];
   double Dd[9];
@@ -51,28 +54,51 @@ __device__ void block_features(const DevLSA &L, int k, int lane, float f[NN_F]) 
     if (a < np) mean += ld[a];
   }
   mean /= (np > 0 ? np : 1);
-  double cpl[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  int deg = 0;
-  for (int t = L.rowoff[k] + lane; t < L.rowoff[k + 1]; t += 32) {
+  // per owned slot: row i, column j of the stored block, and this row's
+  // diagonal entry for either orientation
+  int ei[3], ej[3];
+  double dn[3], dt[3], an[3] = {0., 0., 0.}, at[3] = {0., 0., 0.};
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const int e = lane + 32 * m;
+    ei[m] = e < 81 ? e / 9 : 9;
+    ej[m] = e < 81 ? e % 9 : 9;
+    dn[m] = ei[m] < 9 ? Dd[ei[m]] : 1.;
+    dt[m] = ej[m] < 9 ? Dd[ej[m]] : 1.;
+  }
+  for (int t = L.rowoff[k]; t < L.rowoff[k + 1]; ++t) {
     const int2 en = L.ent[t];
     const int col = en.x;
     if (col == k) continue;
-    ++deg;
     const bool tr = en.y < 0;
     const size_t B = (size_t)(en.y & 0x7fffffff) * 81, Dl = (size_t)col * 81;
     const int nc = L.camparv[col + 1] - L.camparv[col];
-    for (int a = 0; a < np; ++a)
-      for (int c = 0; c < nc; ++c) {
-        const double v = blk_at(L, B + (tr ? c * 9 + a : a * 9 + c));
-        cpl[a] += fabs(v) / sqrt(fmax(Dd[a] * blk_at(L, Dl + c * 10), 1e-300));
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      const int i = ei[m], j = ej[m];
+      if (i >= 9) continue;
+      // stored (k, col): element (i, j) couples parameter i of k to j of col;
+      // stored (col, k): it couples parameter j of k to i of col
+      if (!tr) {
+        if (i < np && j < nc)
+          an[m] += fabs(blk_at(L, B + i * 9 + j)) / sqrt(fmax(dn[m] * blk_at(L, Dl + j * 10), 1e-300));
+      } else {
+        if (j < np && i < nc)
+          at[m] += fabs(blk_at(L, B + i * 9 + j)) / sqrt(fmax(dt[m] * blk_at(L, Dl + i * 10), 1e-300));
       }
+    }
   }
+  double cpl[9];
 #pragma unroll
-  for (int a = 0; a < 9; ++a)
+  for (int a = 0; a < 9; ++a) {
+    double v = 0.;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) cpl[a] += __shfl_xor_sync(0xffffffffu, cpl[a], o);
+    for (int m = 0; m < 3; ++m) v += (ei[m] == a ? an[m] : 0.) + (ej[m] == a ? at[m] : 0.);
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) deg += __shfl_xor_sync(0xffffffffu, deg, o);
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    cpl[a] = v;
+  }
+  const int deg = L.rowoff[k + 1] - L.rowoff[k] - 1;  // entries besides the diagonal block
   for (int a = 0; a < 9; ++a) {
     f[a] = a < np ? (float)(ld[a] - mean) : 0.f;
     f[9 + a] = a < np ? (float)log1p(cpl[a]) : 0.f;
@@ -139,9 +165,10 @@ __global__ void k_learned_setup(DevLSA L, PcgWork Wk, const float *weights) {
   }
   const int np = L.camparv[k + 1] - L.camparv[k];
   if (lane == 0) {
-    double Dk[81];
-    load_block(L, (size_t)k, Dk);
-    lu_inverse9(np, Dk, C);
+    // the block goes to C first, then is inverted in place (lu_inverse9
+    // copies its input before writing the inverse)
+    load_block(L, (size_t)k, C);
+    lu_inverse9(np, C, C);
   }
   float sc[NN_O];
   for (int a = 0; a < NN_O; ++a) sc[a] = 1.f;

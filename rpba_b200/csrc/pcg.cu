@@ -96,6 +96,79 @@ __device__ __forceinline__ void grid_sum(const double *red, int G, double (&v)[N
   __syncthreads();
 }
 
+// Asynchronous global -> shared copies of one element (the blocks are
+// constant during the launch, so the L1-allocating form is safe).
+template <class BT>
+__device__ __forceinline__ void cp_async_elem(BT *dst, const BT *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(BT) == 8)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src));
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// Phase-1 software pipeline: each warp has two work items in flight.  The
+// next item's three blocks are copied to a shared-memory stage (cp.async),
+// and its d^k values (column and row) are loaded into registers, while the
+// current item is multiplied.
+constexpr int P1_ELEMS = 3 * 81;
+template <class BT>
+constexpr size_t pcg_smem_bytes() {
+  return sizeof(BT) == 8 ? sizeof(BT) * (size_t)PCG_W * 2 * P1_ELEMS : 0;
+}
+struct P1Item {
+  int it, row, ne;  // item, its row, entries (0 past the end)
+  int2 en;          // this lane's entry (group grp)
+  double dc;        // d^k[col][rr] of this lane's entry
+  double dk;        // d^k[row][lane] (lanes < 9)
+};
+
+template <class BT>
+__device__ __forceinline__ void p1_issue(const PcgArgs &A, int it, BT *stage, const double *dprev, double beta,
+                                         int lane, int grp, int rr, P1Item &I) {
+  I.it = it;
+  I.ne = 0;
+  I.row = 0;
+  I.en = make_int2(0, 0);
+  I.dc = 0.;
+  I.dk = 0.;
+  if (it < A.nitems) {
+    const int4 m = A.item_meta[it];
+    I.row = m.x;
+    I.ne = m.z - m.y;
+    if (lane < 27 && grp < I.ne) {
+      I.en = A.ent[m.y + grp];
+      const size_t j = (size_t)I.en.x * 9 + rr;
+      I.dc = __ldcg(A.h + j) + beta * __ldcg(dprev + j);
+    }
+    if (lane < 9) {
+      const size_t i = (size_t)I.row * 9 + lane;
+      I.dk = __ldcg(A.h + i) + beta * __ldcg(dprev + i);
+    }
+    const int b0 = __shfl_sync(0xffffffffu, I.en.y, 0) & 0x7fffffff;
+    const int b1 = __shfl_sync(0xffffffffu, I.en.y, 9) & 0x7fffffff;
+    const int b2 = __shfl_sync(0xffffffffu, I.en.y, 18) & 0x7fffffff;
+    const BT *blocks = (const BT *)A.blocks;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int e = lane + 32 * q;
+      if (e < P1_ELEMS) {
+        const int g = e / 81, off = e - g * 81;
+        if (g < I.ne) {
+          const int b = g == 0 ? b0 : (g == 1 ? b1 : b2);
+          cp_async_elem(stage + e, blocks + (size_t)b * 81 + off);
+        }
+      }
+    }
+  }
+  cp_async_commit();
+}
+
 // Iteration k (two grid barriers):
 //  phase 1  q-partials of A d^k per work item (<= 3 blocks of one row), with
 //           d^k = h^k + beta^(k-1) d^(k-1) formed on the fly; partial d^T q
@@ -116,6 +189,9 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
   const int grp = lane / 9, rr = lane % 9, gbase = grp * 9;
   const int G = gridDim.x;
   __shared__ double sh[PCG_W + 1][4];
+  extern __shared__ __align__(16) unsigned char pcg_dyn[];
+  BT *stage0 = (BT *)pcg_dyn + (size_t)warp * 2 * P1_ELEMS;
+  BT *stage1 = stage0 + P1_ELEMS;
   // r^T h of the start vectors
   {
     double v[1] = {0.};
@@ -143,49 +219,85 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
     double *dcur = (k & 1) ? A.D1 : A.D0;
     // ---- phase 1
     double pdq[1] = {0.};
-    // item metadata and the block entry of the next item are prefetched
-    int it = gwarp;
-    int4 meta = it < A.nitems ? A.item_meta[it] : make_int4(0, 0, 0, 0);
-    int2 en_next = make_int2(0, 0);
-    if (it < A.nitems && lane < 27 && meta.y + grp < meta.z) en_next = A.ent[meta.y + grp];
-    for (; it < A.nitems; it += nwarps) {
-      const int row = meta.x;
-      const int e = meta.y + grp;
-      const bool act = lane < 27 && e < meta.z;
-      const int2 en = en_next;
-      const int itn = it + nwarps;
-      if (itn < A.nitems) {
-        meta = A.item_meta[itn];
-        if (lane < 27 && meta.y + grp < meta.z) en_next = A.ent[meta.y + grp];
+    if constexpr (sizeof(BT) == 8) {
+      {
+        P1Item cur, nxt;
+        p1_issue<BT>(A, gwarp, stage0, dprev, beta_prev, lane, grp, rr, cur);
+        p1_issue<BT>(A, gwarp + nwarps, stage1, dprev, beta_prev, lane, grp, rr, nxt);
+        for (int t = 0; cur.it < A.nitems; ++t) {
+          BT *st = (t & 1) ? stage1 : stage0;
+          cp_async_wait<1>();
+          __syncwarp();
+          const bool act = lane < 27 && grp < cur.ne;
+          const bool tr = cur.en.y < 0;
+          const BT *B = st + grp * 81;
+          double acc = 0.;
+  #pragma unroll
+          for (int c = 0; c < 9; ++c) {
+            const double xc = __shfl_sync(0xffffffffu, cur.dc, (lane < 27 ? gbase : 0) + c);
+            if (act) acc += (double)B[tr ? c * 9 + rr : rr * 9 + c] * xc;
+          }
+          const double a1 = __shfl_down_sync(0xffffffffu, acc, 9);
+          const double a2 = __shfl_down_sync(0xffffffffu, acc, 18);
+          if (lane < 9) {
+            const double p = acc + a1 + a2;
+            A.part[(size_t)cur.it * 9 + lane] = p;
+            pdq[0] += cur.dk * p;
+          }
+          __syncwarp();
+          cur = nxt;
+          p1_issue<BT>(A, cur.it + nwarps, st, dprev, beta_prev, lane, grp, rr, nxt);
+        }
+        cp_async_wait<0>();
+        __syncwarp();
       }
-      double acc = 0.;
-      int col = 0, blk = 0;
-      bool tr = false;
-      if (act) {
-        col = en.x;
-        blk = en.y & 0x7fffffff;
-        tr = en.y < 0;
-      }
-      // lane (gbase + c) forms d^k[col][c]; the group gathers it by shuffles
-      double dc = 0.;
-      if (act) {
-        const size_t j = (size_t)col * 9 + rr;
-        dc = __ldcg(A.h + j) + beta_prev * __ldcg(dprev + j);
-      }
-      const BT *B = (const BT *)A.blocks + (size_t)blk * 81;
+    } else {
+      // FP32 blocks: direct loads (4-byte asynchronous copies cost more
+      // instructions than the latency they hide); item metadata and the
+      // next block entry are prefetched
+      int it = gwarp;
+      int4 meta = it < A.nitems ? A.item_meta[it] : make_int4(0, 0, 0, 0);
+      int2 en_next = make_int2(0, 0);
+      if (it < A.nitems && lane < 27 && meta.y + grp < meta.z) en_next = A.ent[meta.y + grp];
+      for (; it < A.nitems; it += nwarps) {
+        const int row = meta.x;
+        const int e = meta.y + grp;
+        const bool act = lane < 27 && e < meta.z;
+        const int2 en = en_next;
+        const int itn = it + nwarps;
+        if (itn < A.nitems) {
+          meta = A.item_meta[itn];
+          if (lane < 27 && meta.y + grp < meta.z) en_next = A.ent[meta.y + grp];
+        }
+        double acc = 0.;
+        int col = 0, blk = 0;
+        bool tr = false;
+        if (act) {
+          col = en.x;
+          blk = en.y & 0x7fffffff;
+          tr = en.y < 0;
+        }
+        // lane (gbase + c) forms d^k[col][c]; the group gathers it by shuffles
+        double dc = 0.;
+        if (act) {
+          const size_t j = (size_t)col * 9 + rr;
+          dc = __ldcg(A.h + j) + beta_prev * __ldcg(dprev + j);
+        }
+        const BT *B = (const BT *)A.blocks + (size_t)blk * 81;
 #pragma unroll
-      for (int c = 0; c < 9; ++c) {
-        const double xc = __shfl_sync(0xffffffffu, dc, (lane < 27 ? gbase : 0) + c);
-        if (act) acc += __ldg(B + (tr ? c * 9 + rr : rr * 9 + c)) * xc;
-      }
-      const double a1 = __shfl_down_sync(0xffffffffu, acc, 9);
-      const double a2 = __shfl_down_sync(0xffffffffu, acc, 18);
-      if (lane < 9) {
-        const double p = acc + a1 + a2;
-        A.part[(size_t)it * 9 + lane] = p;
-        const size_t i = (size_t)row * 9 + lane;
-        const double dk = __ldcg(A.h + i) + beta_prev * __ldcg(dprev + i);
-        pdq[0] += dk * p;
+        for (int c = 0; c < 9; ++c) {
+          const double xc = __shfl_sync(0xffffffffu, dc, (lane < 27 ? gbase : 0) + c);
+          if (act) acc += __ldg(B + (tr ? c * 9 + rr : rr * 9 + c)) * xc;
+        }
+        const double a1 = __shfl_down_sync(0xffffffffu, acc, 9);
+        const double a2 = __shfl_down_sync(0xffffffffu, acc, 18);
+        if (lane < 9) {
+          const double p = acc + a1 + a2;
+          A.part[(size_t)it * 9 + lane] = p;
+          const size_t i = (size_t)row * 9 + lane;
+          const double dk = __ldcg(A.h + i) + beta_prev * __ldcg(dprev + i);
+          pdq[0] += dk * p;
+        }
       }
     }
     cta_sum<1>(pdq, sh);
@@ -398,9 +510,8 @@ __global__ void k_pcg_setup(DevLSA L, PcgWork W) {
     return;
   }
   const int np = L.camparv[k + 1] - L.camparv[k];
-  double Dk[81];
-  load_block(L, (size_t)k, Dk);
-  lu_inverse9(np, Dk, C);
+  load_block(L, (size_t)k, C);  // inverted in place below
+  lu_inverse9(np, C, C);
   double rv[9];
   for (int a = 0; a < 9; ++a) rv[a] = L.rhs[o + a];
   for (int a = 0; a < 9; ++a) {
@@ -415,15 +526,28 @@ __global__ void k_pcg_setup(DevLSA L, PcgWork W) {
 
 }  // namespace
 
+// the phase-1 stages of the FP64 form live in dynamic shared memory (124 KB)
+void pcg_set_smem() {
+  cudaFuncSetAttribute(k_pcg<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)pcg_smem_bytes<double>());
+  cudaFuncSetAttribute(k_pcg<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)pcg_smem_bytes<double>());
+  cudaFuncSetAttribute(k_pcg<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)pcg_smem_bytes<float>());
+  cudaFuncSetAttribute(k_pcg<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)pcg_smem_bytes<float>());
+}
+
 int pcg_max_grid(int device) {
   int nsm = 0, per = 0, per2 = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<false, double>, PCG_T, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true, double>, PCG_T, 0);
+  pcg_set_smem();
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<false, double>, PCG_T, pcg_smem_bytes<double>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true, double>, PCG_T, pcg_smem_bytes<double>());
   per = std::min(per, per2);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<false, float>, PCG_T, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<false, float>, PCG_T, pcg_smem_bytes<float>());
   per = std::min(per, per2);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true, float>, PCG_T, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true, float>, PCG_T, pcg_smem_bytes<float>());
   per = std::min(per, per2);
   if (per < 1) per = 1;
   return nsm * per;
@@ -485,7 +609,9 @@ int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream
     fn = co ? (const void *)k_pcg<true, float> : (const void *)k_pcg<false, float>;
   else
     fn = co ? (const void *)k_pcg<true, double> : (const void *)k_pcg<false, double>;
-  RPBA_CUDA_CHECK(cudaLaunchCooperativeKernel(fn, dim3(g), dim3(PCG_T), args, 0, s));
+  const size_t smem = L.blocks32 ? pcg_smem_bytes<float>() : pcg_smem_bytes<double>();
+  pcg_set_smem();
+  RPBA_CUDA_CHECK(cudaLaunchCooperativeKernel(fn, dim3(g), dim3(PCG_T), args, smem, s));
   return 0;
 }
 
