@@ -285,6 +285,24 @@ int32_t rpba_precond_loss_grad(const rpba_precond_set *set, const float *weights
  * serialised by the caller.  No counterpart in the reference. */
 int32_t rpba_float_sequential_sum_noalloc(const float *d_v, int64_t n, float *d_out, void *stream);
 
+/* Batched form: many independent scenes of uneven size on one GPU.  Every
+ * scene is solved as rpba_calc_plsa would solve it (in place; reports[i] and
+ * status[i] per scene); `workers` scenes run at once, each on its own stream,
+ * so that the kernels of small scenes fill the GPU together (workers <= 0:
+ * chosen by timing a sample of the batch, reported in br->workers).  The
+ * cooperative kernels of different scenes run one at a time.  Returns
+ * RPBA_ERR_SOLVER when any scene failed (see status).  No counterpart in the
+ * reference (its parallel form partitions one scene, rpbacore.cpp:100-510). */
+typedef struct rpba_batch_report {
+  double seconds;            /* wall time of the batch, tuning excluded       */
+  double scenes_per_second;
+  double tune_seconds;       /* wall time spent choosing the worker count     */
+  int32_t workers;           /* scenes solved concurrently                    */
+  int32_t failed;            /* scenes whose status is not RPBA_OK            */
+} rpba_batch_report;
+int32_t rpba_solve_batch(rpba_block *blocks, int32_t n, const rpba_options *opt, int32_t workers,
+                         rpba_report *reports, int32_t *status, rpba_batch_report *br);
+
 /* Per-kernel device time of the last solve as a JSON object
  * {"name": {"launches": n, "ms": t}, ...}; filled only when the handle was
  * created with rpba_options.verbose bit 1 (value 2) set.  No counterpart in

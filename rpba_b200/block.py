@@ -114,6 +114,11 @@ class RpbaPrecondBuffersC(C.Structure):
                 ("rowoff", _i32p), ("ent_col", _i32p), ("ent_blk", _i32p), ("sys_row", _i32p)]
 
 
+class RpbaBatchReportC(C.Structure):
+    _fields_ = [("seconds", C.c_double), ("scenes_per_second", C.c_double), ("tune_seconds", C.c_double),
+                ("workers", C.c_int32), ("failed", C.c_int32)]
+
+
 PRECOND_WEIGHTS = 1865
 SOLVER_PCG, SOLVER_DIRECT, SOLVER_LEARNED = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1

@@ -13,7 +13,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/rpba_b200.h"
@@ -23,11 +26,48 @@ using namespace rpba;
 
 namespace {
 
+// A handle's device memory comes from the device's stream-ordered pool
+// (cudaMallocAsync on the handle's stream, retained by the pool after
+// cudaFreeAsync): creating and destroying handles then never waits for the
+// whole device, as cudaFree does, so handles on other streams -- the batched
+// form, or an application's own work -- keep running.  The scope below,
+// active while a handle allocates, routes dalloc(n, handle->owned) there;
+// other lists (training sets) keep plain cudaMalloc.
+struct AsyncAlloc {
+  cudaStream_t s = nullptr;
+  std::vector<void *> *sync_list = nullptr;   // the handle's `owned`
+  std::vector<void *> *async_list = nullptr;  // where pool allocations are recorded
+};
+thread_local AsyncAlloc g_aa;
+struct AsyncScope {
+  AsyncAlloc prev;
+  AsyncScope(cudaStream_t s, std::vector<void *> &sync_list, std::vector<void *> &async_list) : prev(g_aa) {
+    g_aa.s = s;
+    g_aa.sync_list = &sync_list;
+    g_aa.async_list = &async_list;
+  }
+  ~AsyncScope() { g_aa = prev; }
+};
+
+void retain_pool(int dev) {
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+    unsigned long long thr = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+}
+
 template <typename T>
 T *dalloc(size_t n, std::vector<void *> &owned) {
   void *p = nullptr;
-  RPBA_CUDA_CHECK(cudaMalloc(&p, sizeof(T) * (n ? n : 1)));
-  owned.push_back(p);
+  const size_t bytes = sizeof(T) * (n ? n : 1);
+  if (g_aa.s && &owned == g_aa.sync_list) {
+    RPBA_CUDA_CHECK(cudaMallocAsync(&p, bytes, g_aa.s));
+    g_aa.async_list->push_back(p);
+  } else {
+    RPBA_CUDA_CHECK(cudaMalloc(&p, bytes));
+    owned.push_back(p);
+  }
   return (T *)p;
 }
 
@@ -205,9 +245,14 @@ struct rpba_handle {
   std::string log;
   rpba_report rep{};
 
+  std::vector<void *> owned_async;  // pool allocations on stream s
+
   ~rpba_handle() {
     coarse_release(CW);
-    if (s) cudaStreamSynchronize(s);
+    if (s) {
+      for (void *p : owned_async) cudaFreeAsync(p, s);
+      cudaStreamSynchronize(s);
+    }
     for (void *p : owned) cudaFree(p);
     if (s) {
       cudaEventDestroy(ev0);
@@ -224,8 +269,14 @@ struct rpba_handle {
     const int cap = std::max(nb, 1);
     if (cur) {
       for (void *p : {cur, (void *)S.ent, (void *)S.item_meta, (void *)W.part}) {
-        cudaFree(p);
-        owned.erase(std::remove(owned.begin(), owned.end(), p), owned.end());
+        auto it = std::find(owned_async.begin(), owned_async.end(), p);
+        if (it != owned_async.end()) {
+          cudaFreeAsync(p, s);
+          owned_async.erase(it);
+        } else {
+          cudaFree(p);
+          owned.erase(std::remove(owned.begin(), owned.end(), p), owned.end());
+        }
       }
     }
     if (mixed)
@@ -271,8 +322,32 @@ struct rpba_handle {
     RPBA_CUDA_CHECK(cudaMemcpyAsync(DW.coff, coff.data(), sizeof(int) * (nimg + 1), cudaMemcpyHostToDevice, s));
   }
 
+  // Batched solves (rpba_solve_batch) run many handles on one GPU at once.
+  // Cooperative kernels (the persistent PCG, the exact sums) need all their
+  // CTAs resident together; two of them from different scenes could each
+  // hold part of the SMs and wait for the rest.  In a batch they are
+  // therefore run one at a time: the launch takes `coop` and releases it
+  // once the kernel has finished.  Ordinary kernels of other scenes keep
+  // running meanwhile.
+  std::mutex *coop = nullptr;
+  struct CoopLock {
+    rpba_handle *H;
+    explicit CoopLock(rpba_handle *h) : H(h) {
+      if (H->coop) H->coop->lock();
+    }
+    ~CoopLock() {
+      if (H->coop) {
+        cudaStreamSynchronize(H->s);
+        H->coop->unlock();
+      }
+    }
+  };
+
   float seq_sum(const float *v, int n) {
-    PROF("seq_sum", 1, launch_exact_sum(v, n, sums, ES, s));
+    {
+      CoopLock lk(this);
+      PROF("seq_sum", 1, launch_exact_sum(v, n, sums, ES, s));
+    }
     float out = 0.f;
     RPBA_CUDA_CHECK(cudaMemcpyAsync(&out, sums, sizeof(float), cudaMemcpyDeviceToHost, s));
     RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -295,6 +370,8 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   RPBA_CUDA_CHECK(cudaStreamCreateWithFlags(&H->s, cudaStreamNonBlocking));
   RPBA_CUDA_CHECK(cudaEventCreate(&H->ev0));
   RPBA_CUDA_CHECK(cudaEventCreate(&H->ev1));
+  retain_pool(H->dev);
+  AsyncScope scope(H->s, H->owned, H->owned_async);
   auto &own = H->owned;
   const int n = b->n_images, np = b->n_points;
   H->nimg = n;
@@ -329,6 +406,7 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
     RPBA_CUDA_CHECK(cudaMemsetAsync(H->ES.err, 0, 4 * sizeof(int), H->s));
   }
   if (o->exteval) {
+    RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
     for (int i = 0; i < H->n_track_in; ++i) {
       const int im = H->h_pt_img[i];
       if (im < 0 || im >= n || H->h_pt_slot[i] < 0 || H->h_pt_slot[i] >= H->h_img_off[im + 1] - H->h_img_off[im])
@@ -352,16 +430,17 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   std::vector<void *> tmp;
   auto tmalloc = [&](size_t bytes) {
     void *p = nullptr;
-    RPBA_CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(bytes, 16)));
+    RPBA_CUDA_CHECK(cudaMallocAsync(&p, std::max<size_t>(bytes, 16), H->s));
     tmp.push_back(p);
     return p;
   };
   struct TmpFree {
     std::vector<void *> &v;
+    cudaStream_t s;
     ~TmpFree() {
-      for (void *p : v) cudaFree(p);
+      for (void *p : v) cudaFreeAsync(p, s);
     }
-  } tmp_free{tmp};
+  } tmp_free{tmp, H->s};
   auto upt = [&](const void *h, size_t bytes) {
     void *d = tmalloc(bytes);
     if (bytes) RPBA_CUDA_CHECK(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, H->s));
@@ -709,7 +788,10 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
         fresh = true;
       }
       const int cap_try = (cw && !fresh) ? std::min(cap, 3 * coarse_ref_iters + 20) : cap;
-      PROF("pcg", 2, pcg_solve(L, W, cap_try, pcg_grid, s, mode, opt.pcg_tolerance, d_weights, cw));
+      {
+        CoopLock lk(this);
+        PROF("pcg", 2, pcg_solve(L, W, cap_try, pcg_grid, s, mode, opt.pcg_tolerance, d_weights, cw));
+      }
       RPBA_CUDA_CHECK(cudaMemcpyAsync(it, W.iters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
       if (cw) RPBA_CUDA_CHECK(cudaMemcpyAsync(it + 2, CW.err, sizeof(int), cudaMemcpyDeviceToHost, s));
       RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -745,7 +827,10 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
       PROF("direct", 1, direct_solve(L, DW, W.xbest, s));
     }
   } else {
-    PROF("pcg", 2, pcg_solve(L, W, msize, pcg_grid, s));
+    {
+      CoopLock lk(this);
+      PROF("pcg", 2, pcg_solve(L, W, msize, pcg_grid, s));
+    }
     pcg_pending = true;
   }
   if (rec_T) {
@@ -996,6 +1081,7 @@ int32_t rpba_solve(rpba_handle *H, rpba_report *rep) {
   const int st = guard([](void *p) {
     rpba_handle *H = (rpba_handle *)p;
     RPBA_CUDA_CHECK(cudaSetDevice(H->dev));
+    AsyncScope scope(H->s, H->owned, H->owned_async);
     H->log.clear();
     std::memset(&H->rep, 0, sizeof H->rep);
     H->learned_iters = 0;
@@ -1540,6 +1626,94 @@ int32_t rpba_calc_plsa(rpba_block *blk, const rpba_options *opt, char *log, size
   if (log && cap) rpba_get_log(H, log, cap);
   rpba_destroy(H);
   return st;
+}
+
+int32_t rpba_solve_batch(rpba_block *blocks, int32_t n, const rpba_options *opt, int32_t workers,
+                         rpba_report *reports, int32_t *status, rpba_batch_report *br) {
+  if (!blocks || n <= 0 || !opt || !status || opt->exteval) return RPBA_ERR_ARG;
+  if (br) std::memset(br, 0, sizeof *br);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= opt->device) return RPBA_ERR_NO_DEVICE;
+  // largest scenes first: the tail of the batch is made of small scenes
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  auto obs = [&](int i) { return blocks[i].pt_obs_off ? (long long)blocks[i].pt_obs_off[blocks[i].n_points] : 0ll; };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return obs(a) > obs(b); });
+  std::mutex coop;
+  std::vector<rpba_report> reps(n);
+  // solve the scenes of `ord` with `w` concurrent workers, each driving its
+  // own handle (and stream; handle memory comes from the stream-ordered
+  // pool, so creating and destroying handles does not stall the others);
+  // returns the wall time
+  auto run = [&](const std::vector<int> &ord, int w, bool keep) {
+    std::atomic<int> next{0};
+    auto body = [&]() {
+      cudaSetDevice(opt->device);
+      for (;;) {
+        const int q = next.fetch_add(1);
+        if (q >= (int)ord.size()) break;
+        const int i = ord[q];
+        rpba_report r{};
+        rpba_handle *H = nullptr;
+        int st = rpba_create(&H, &blocks[i], opt);
+        if (st == RPBA_OK) {
+          H->coop = &coop;
+          st = rpba_solve(H, &r);
+          if (keep && (st == RPBA_OK || st == RPBA_ERR_NO_OBS_IMAGE || st == RPBA_ERR_LOW_REDUNDANCY ||
+                       st == RPBA_ERR_NAN_STEP)) {
+            const int st2 = rpba_get_state(H, &blocks[i]);
+            if (st == RPBA_OK) st = st2;
+          }
+          rpba_destroy(H);
+        }
+        if (keep) {
+          status[i] = st;
+          reps[i] = r;
+        }
+      }
+    };
+    const auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> th;
+    for (int k = 1; k < w; ++k) th.emplace_back(body);
+    body();
+    for (auto &t : th) t.join();
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  };
+  int w = workers;
+  double tune = 0.;
+  if (w <= 0) {
+    // autotune the number of concurrent scenes on a sample spread over the
+    // size order (the solutions are discarded)
+    std::vector<int> sample;
+    const int ns = std::min(n, 24);
+    for (int j = 0; j < ns; ++j) sample.push_back(order[(long long)j * n / ns]);
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    double best = 1e300;
+    w = 1;
+    for (int cand : {1, 2, 4, 8, 16, 32}) {
+      if (cand > ns || cand > hw) break;
+      const double t = run(sample, cand, false);
+      tune += t;
+      if (t < best * 0.97) {
+        best = t;
+        w = cand;
+      }
+    }
+  }
+  const double secs = run(order, w, true);
+  int failed = 0;
+  for (int i = 0; i < n; ++i) {
+    if (reports) reports[i] = reps[i];
+    if (status[i] != RPBA_OK) ++failed;
+  }
+  if (br) {
+    br->seconds = secs;
+    br->scenes_per_second = n / secs;
+    br->tune_seconds = tune;
+    br->workers = w;
+    br->failed = failed;
+  }
+  return failed ? RPBA_ERR_SOLVER : RPBA_OK;
 }
 
 }  // extern "C"

@@ -21,7 +21,7 @@ import os
 import numpy as np
 
 from .block import (Block, RpbaBlockC, RpbaOptionsC, RpbaReportC, RpbaTrainOptionsC, RpbaTrainReportC,
-                    RpbaPrecondSetC, RpbaPrecondBuffersC,
+                    RpbaPrecondSetC, RpbaPrecondBuffersC, RpbaBatchReportC,
                     make_options, PRECOND_WEIGHTS, SOLVER_PCG, SOLVER_DIRECT, SOLVER_LEARNED, PREC_FP64,
                     PREC_MIXED)
 
@@ -38,7 +38,8 @@ EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block
            "rpba_output_block", "rpba_calc_plsa", "rpba_create", "rpba_solve",
            "rpba_get_state", "rpba_get_log", "rpba_exteval", "rpba_kernel_stats", "rpba_float_sequential_sum",
            "rpba_float_sequential_sum_noalloc", "rpba_train_preconditioner",
-           "rpba_set_preconditioner", "rpba_precond_loss_grad", "rpba_record_systems", "rpba_destroy")
+           "rpba_set_preconditioner", "rpba_precond_loss_grad", "rpba_record_systems", "rpba_solve_batch",
+           "rpba_destroy")
 
 _lib = None
 
@@ -94,6 +95,9 @@ def load():
     L.rpba_record_systems.argtypes = [bp, C.c_int32, op, C.POINTER(RpbaTrainOptionsC),
                                       C.POINTER(RpbaPrecondBuffersC)]
     L.rpba_record_systems.restype = C.c_int32
+    L.rpba_solve_batch.argtypes = [bp, C.c_int32, op, C.c_int32, rp, C.POINTER(C.c_int32),
+                                   C.POINTER(RpbaBatchReportC)]
+    L.rpba_solve_batch.restype = C.c_int32
     L.rpba_kernel_stats.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     L.rpba_kernel_stats.restype = C.c_int32
     L.rpba_destroy.argtypes = [C.c_void_p]
@@ -165,6 +169,26 @@ def train_preconditioner(blocks, steps=300, batch=0, lr=3e-3, probes=2, seed=1, 
     if st != 0:
         raise RpbaError(st, "rpba_train_preconditioner")
     return w, {k: getattr(rep, k) for k, _ in rep._fields_}
+
+
+def solve_batch(blocks, workers: int = 0, **opt_kw):
+    """Solve many independent scenes in place, several at once on one GPU
+    (rpba_solve_batch; workers <= 0: chosen by the library).  Returns
+    (status list, report dicts, batch report dict)."""
+    n = len(blocks)
+    cbs = [b.as_c() for b in blocks]
+    arr = (RpbaBlockC * n)(*cbs)
+    o = make_options(**opt_kw)
+    reps = (RpbaReportC * n)()
+    st = (C.c_int32 * n)()
+    br = RpbaBatchReportC()
+    r = load().rpba_solve_batch(arr, n, C.byref(o), int(workers), reps, st, C.byref(br))
+    if r not in (0, 10):
+        raise RpbaError(r, "rpba_solve_batch")
+    # the results went straight into the blocks' arrays (as with CalcPLSA);
+    # cbs keeps the C views alive until here
+    del cbs
+    return list(st), [rp.as_dict() for rp in reps], {k: getattr(br, k) for k, _ in br._fields_}
 
 
 def record_systems(blocks, probes=2, seed=1, max_samples=0, caps=None, **opt_kw) -> dict:

@@ -23,6 +23,8 @@ from __future__ import annotations
 
 from dataclasses import dataclass
 
+import os
+
 import numpy as np
 
 from .block import Block
@@ -388,14 +390,34 @@ def city_scene(seed=20263, n_clusters=50, cams_per_cluster=274, n_pts=4_500_000,
                      _Vis(R, t, f, k, X, 1.0, 2.0), t_want, outlier_frac=outlier_frac, chunk=100_000, **kw)
 
 
-def batch_scenes(seed=20264, n_scenes=256, cmin=20, cmax=400, pts_per_cam=150):
+def batch_scene_specs(seed=20264, n_scenes=256, cmin=20, cmax=400, pts_per_cam=150):
+    """Keyword arguments of arc_scene for every scene of the batched workload."""
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n_scenes):
         nc = int(rng.integers(cmin, cmax + 1))
-        out.append(arc_scene(seed=seed * 1000 + i, n_cams=nc, n_pts=pts_per_cam * nc,
-                             track_mean=4.0, track_max=12))
+        out.append(dict(seed=seed * 1000 + i, n_cams=nc, n_pts=pts_per_cam * nc, track_mean=4.0, track_max=12))
     return out
+
+
+def _arc_block(kw):
+    return to_block(arc_scene(**kw))
+
+
+def batch_scenes(seed=20264, n_scenes=256, cmin=20, cmax=400, pts_per_cam=150):
+    return [arc_scene(**kw) for kw in batch_scene_specs(seed, n_scenes, cmin, cmax, pts_per_cam)]
+
+
+def batch_blocks(seed=20264, n_scenes=256, cmin=20, cmax=400, pts_per_cam=150, workers=None):
+    """The batched workload as blocks, generated in parallel processes."""
+    specs = batch_scene_specs(seed, n_scenes, cmin, cmax, pts_per_cam)
+    workers = workers or min(len(specs), os.cpu_count() or 1, 32)
+    if workers <= 1:
+        return [_arc_block(kw) for kw in specs]
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    with ProcessPoolExecutor(workers, mp_context=mp.get_context("spawn")) as ex:
+        return list(ex.map(_arc_block, specs, chunksize=4))
 
 
 CONFIGS = {
