@@ -10,9 +10,12 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
-#include <string>
-#include <vector>
 #include <algorithm>
+#include <atomic>
+#include <charconv>
+#include <string>
+#include <thread>
+#include <vector>
 
 #include "../../include/rpba_b200.h"
 
@@ -144,6 +147,112 @@ T *cal(size_t n) {
   return (T *)std::calloc(n ? n : 1, sizeof(T));
 }
 
+// ---- parallel parse and format of large files
+// The body of a BAL file (after the three counts) is a whitespace-separated
+// token stream: 4 per observation (image, point, x, y), 9 per camera, 3 per
+// point, whatever the line layout.  A token's global index fixes its field
+// and type, so the stream is cut into byte ranges at token boundaries,
+// tokens are counted per range (pass 1), and every range parses its tokens
+// knowing their global index (pass 2).  std::from_chars rounds correctly,
+// like the strtof/strtod of the serial path, so both give the same bits.
+
+int io_threads() {
+  const char *e = std::getenv("RPBA_IO_THREADS");
+  if (e && *e) return std::max(1, std::atoi(e));
+  return (int)std::min(32u, std::max(1u, std::thread::hardware_concurrency()));
+}
+size_t io_parallel_min_bytes() {
+  const char *e = std::getenv("RPBA_IO_PARALLEL_MIN_BYTES");
+  return e && *e ? (size_t)std::atoll(e) : (size_t)(8u << 20);
+}
+
+inline bool is_ws(char c) { return c == ' ' || c == '\n' || c == '\r' || c == '\t'; }
+
+template <class F>
+void parallel_for(int T, F &&f) {
+  std::vector<std::thread> th;
+  for (int k = 1; k < T; ++k) th.emplace_back(f, k);
+  f(0);
+  for (auto &t : th) t.join();
+}
+
+template <class V>
+bool parse_num(const char *b, const char *e, V &v) {
+  if (b < e && *b == '+') ++b;
+  const auto r = std::from_chars(b, e, v);
+  return r.ec == std::errc() && r.ptr == e;
+}
+
+struct BodyOut {
+  long long nc, np, no;
+  int32_t *ocam, *opt;
+  float *ox, *oy;
+  double *cam_d;  // [nc][3] angle-axis
+  float *cam_f;   // [nc][6] t, f, k2, k4
+  float *XX;      // [np][3]
+};
+
+// Parse the body [b, e) in parallel; false on a malformed or short body.
+bool parse_body_parallel(const char *b, const char *e, BodyOut &O, int T) {
+  const long long need = 4 * O.no + 9 * O.nc + 3 * O.np;
+  const size_t L = (size_t)(e - b) / T + 1;
+  std::vector<const char *> st(T + 1);
+  for (int k = 0; k <= T; ++k) {
+    const char *q = std::min(e, b + L * k);
+    if (k > 0 && k < T)
+      while (q < e && q > b && !is_ws(q[-1])) ++q;  // to the start of the next token
+    st[k] = k == T ? e : q;
+  }
+  std::vector<long long> cnt(T, 0);
+  parallel_for(T, [&](int k) {
+    long long c = 0;
+    const char *q = st[k], *z = st[k + 1];
+    while (q < z) {
+      while (q < z && is_ws(*q)) ++q;
+      if (q >= z) break;
+      ++c;
+      while (q < z && !is_ws(*q)) ++q;
+    }
+    cnt[k] = c;
+  });
+  std::vector<long long> first(T + 1, 0);
+  for (int k = 0; k < T; ++k) first[k + 1] = first[k] + cnt[k];
+  if (first[T] < need) return false;
+  std::atomic<bool> ok{true};
+  const long long o1 = 4 * O.no, c1 = o1 + 9 * O.nc;
+  parallel_for(T, [&](int k) {
+    long long t = first[k];
+    const char *q = st[k], *z = st[k + 1];
+    bool good = true;
+    while (q < z && t < need && good) {
+      while (q < z && is_ws(*q)) ++q;
+      if (q >= z) break;
+      const char *s0 = q;
+      while (q < z && !is_ws(*q)) ++q;
+      if (t < o1) {
+        const long long i = t >> 2;
+        switch (t & 3) {
+          case 0: { long long v; good = parse_num(s0, q, v) && v >= 0 && v < O.nc; O.ocam[i] = (int32_t)v; break; }
+          case 1: { long long v; good = parse_num(s0, q, v) && v >= 0 && v < O.np; O.opt[i] = (int32_t)v; break; }
+          case 2: good = parse_num(s0, q, O.ox[i]); break;
+          default: good = parse_num(s0, q, O.oy[i]); break;
+        }
+      } else if (t < c1) {
+        const long long u = t - o1, i = u / 9, f = u % 9;
+        if (f < 3)
+          good = parse_num(s0, q, O.cam_d[3 * i + f]);
+        else
+          good = parse_num(s0, q, O.cam_f[6 * i + f - 3]);
+      } else {
+        good = parse_num(s0, q, O.XX[t - c1]);
+      }
+      ++t;
+    }
+    if (!good) ok = false;
+  });
+  return ok;
+}
+
 }  // namespace
 
 extern "C" {
@@ -159,16 +268,30 @@ int32_t rpba_input_block(const char *path, int32_t nraddpar, int32_t k24out, rpb
   std::vector<int32_t> ocam(no), opt(no);
   std::vector<float> ox(no), oy(no);
   std::vector<int32_t> cnt(nc + 1, 0), pcnt(np + 1, 0);
-  for (long long i = 0; i < no; ++i) {
-    const long long c = r.integer(), p = r.integer();
-    const float x = r.flt(), y = r.flt();
-    if (!r.ok || c < 0 || c >= nc || p < 0 || p >= np) return RPBA_ERR_IO;
-    ocam[i] = (int32_t)c;
-    opt[i] = (int32_t)p;
-    ox[i] = x;
-    oy[i] = y;
-    ++cnt[c + 1];
-    ++pcnt[p + 1];
+  // large files: the whole body in parallel (same values as the serial path)
+  const int T = io_threads();
+  const bool par = T > 1 && (size_t)(r.e - r.p) >= io_parallel_min_bytes();
+  std::vector<double> cam_d(par ? 3 * nc : 0);
+  std::vector<float> cam_f(par ? 6 * nc : 0), xx(par ? 3 * np : 0);
+  if (par) {
+    BodyOut O{nc, np, no, ocam.data(), opt.data(), ox.data(), oy.data(), cam_d.data(), cam_f.data(), xx.data()};
+    if (!parse_body_parallel(r.p, r.e, O, T)) return RPBA_ERR_IO;
+    for (long long i = 0; i < no; ++i) {
+      ++cnt[ocam[i] + 1];
+      ++pcnt[opt[i] + 1];
+    }
+  } else {
+    for (long long i = 0; i < no; ++i) {
+      const long long c = r.integer(), p = r.integer();
+      const float x = r.flt(), y = r.flt();
+      if (!r.ok || c < 0 || c >= nc || p < 0 || p >= np) return RPBA_ERR_IO;
+      ocam[i] = (int32_t)c;
+      opt[i] = (int32_t)p;
+      ox[i] = x;
+      oy[i] = y;
+      ++cnt[c + 1];
+      ++pcnt[p + 1];
+    }
   }
   rpba_block b;
   std::memset(&b, 0, sizeof b);
@@ -203,12 +326,14 @@ int32_t rpba_input_block(const char *path, int32_t nraddpar, int32_t k24out, rpb
     b.pt_obs_slot[w] = slot;
   }
   for (long long i = 0; i < nc; ++i) {
-    const double a = r.dbl(), bb = r.dbl(), c = r.dbl();
+    const double a = par ? cam_d[3 * i] : r.dbl(), bb = par ? cam_d[3 * i + 1] : r.dbl(),
+                 c = par ? cam_d[3 * i + 2] : r.dbl();
     float *P = b.pmat + 12 * i;
-    P[3] = r.flt();
-    P[7] = r.flt();
-    P[11] = r.flt();
-    const float f = r.flt(), k2 = r.flt(), k4 = r.flt();
+    P[3] = par ? cam_f[6 * i] : r.flt();
+    P[7] = par ? cam_f[6 * i + 1] : r.flt();
+    P[11] = par ? cam_f[6 * i + 2] : r.flt();
+    const float f = par ? cam_f[6 * i + 3] : r.flt(), k2 = par ? cam_f[6 * i + 4] : r.flt(),
+                k4 = par ? cam_f[6 * i + 5] : r.flt();
     float R[9];
     angleaxis_to_R(a, bb, c, R);
     for (int rr = 0; rr < 3; ++rr)
@@ -224,7 +349,10 @@ int32_t rpba_input_block(const char *path, int32_t nraddpar, int32_t k24out, rpb
       b.distpara[2 * i + 1] = k4 * f * f * f * f;
     }
   }
-  for (long long i = 0; i < 3 * np; ++i) b.XX[i] = r.flt();
+  if (par)
+    std::memcpy(b.XX, xx.data(), sizeof(float) * 3 * np);
+  else
+    for (long long i = 0; i < 3 * np; ++i) b.XX[i] = r.flt();
   if (!r.ok) {
     rpba_block_free(&b);
     return RPBA_ERR_IO;
@@ -256,21 +384,41 @@ int32_t rpba_output_block(const char *path, rpba_block *b, int32_t k24out) {
   if (!f) return RPBA_ERR_IO;
   const int nc = b->n_images, np = b->n_points;
   std::fprintf(f, "%d %d %d\n", nc, np, b->pt_obs_off[np]);
-  std::vector<std::pair<int, int>> v;
-  for (int i = 0; i < np; ++i) {
-    const int s = b->pt_obs_off[i], e = b->pt_obs_off[i + 1];
-    v.clear();
-    for (int j = s; j < e; ++j) v.emplace_back(b->pt_obs_image[j], b->pt_obs_slot[j]);
-    std::stable_sort(v.begin(), v.end(), [](const std::pair<int, int> &l, const std::pair<int, int> &r) {
-      return l.first < r.first;
-    });
-    for (int j = s; j < e; ++j) {
-      b->pt_obs_image[j] = v[j - s].first;
-      b->pt_obs_slot[j] = v[j - s].second;
-      const int sl = b->img_obs_off[v[j - s].first] + v[j - s].second;
-      std::fprintf(f, "%d %d %.8g %.8g\n", v[j - s].first, i, -b->xg[2 * sl], -b->xg[2 * sl + 1]);
+  // observation lines of points [p0, p1): each point's observations sorted
+  // by image (stable), written back in that order
+  auto obs_lines = [&](int p0, int p1, std::string &out) {
+    std::vector<std::pair<int, int>> v;
+    char line[96];
+    for (int i = p0; i < p1; ++i) {
+      const int s = b->pt_obs_off[i], e = b->pt_obs_off[i + 1];
+      v.clear();
+      for (int j = s; j < e; ++j) v.emplace_back(b->pt_obs_image[j], b->pt_obs_slot[j]);
+      std::stable_sort(v.begin(), v.end(), [](const std::pair<int, int> &l, const std::pair<int, int> &r) {
+        return l.first < r.first;
+      });
+      for (int j = s; j < e; ++j) {
+        b->pt_obs_image[j] = v[j - s].first;
+        b->pt_obs_slot[j] = v[j - s].second;
+        const int sl = b->img_obs_off[v[j - s].first] + v[j - s].second;
+        const int n = std::snprintf(line, sizeof line, "%d %d %.8g %.8g\n", v[j - s].first, i, -b->xg[2 * sl],
+                                    -b->xg[2 * sl + 1]);
+        out.append(line, (size_t)n);
+      }
     }
-  }
+  };
+  auto pt_lines = [&](int p0, int p1, std::string &out) {
+    char line[96];
+    for (int i = p0; i < p1; ++i) {
+      const int n = std::snprintf(line, sizeof line, "%.8g %.8g %.8g\n", b->XX[3 * i], b->XX[3 * i + 1],
+                                  b->XX[3 * i + 2]);
+      out.append(line, (size_t)n);
+    }
+  };
+  // large blocks: per-thread buffers over point ranges, written in order
+  const int T = (size_t)b->pt_obs_off[np] * 40 >= io_parallel_min_bytes() ? io_threads() : 1;
+  std::vector<std::string> bufs(T);
+  parallel_for(T, [&](int k) { obs_lines((int)((long long)np * k / T), (int)((long long)np * (k + 1) / T), bufs[k]); });
+  for (auto &x : bufs) std::fwrite(x.data(), 1, x.size(), f);
   for (int i = 0; i < nc; ++i) {
     float R[9];
     const float *P = b->pmat + 12 * i;
@@ -287,7 +435,9 @@ int32_t rpba_output_block(const char *path, rpba_block *b, int32_t k24out) {
       std::fprintf(f, "%.8g %.8g\n", b->distpara[2 * i] * f2, b->distpara[2 * i + 1] * f2 * f2);
     }
   }
-  for (int i = 0; i < np; ++i) std::fprintf(f, "%.8g %.8g %.8g\n", b->XX[3 * i], b->XX[3 * i + 1], b->XX[3 * i + 2]);
+  for (auto &x : bufs) x.clear();
+  parallel_for(T, [&](int k) { pt_lines((int)((long long)np * k / T), (int)((long long)np * (k + 1) / T), bufs[k]); });
+  for (auto &x : bufs) std::fwrite(x.data(), 1, x.size(), f);
   const bool ok = std::ferror(f) == 0;
   std::fclose(f);
   return ok ? RPBA_OK : RPBA_ERR_IO;

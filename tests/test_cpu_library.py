@@ -76,7 +76,7 @@ def test_output_block_round_trip(tmp_path, oracle_mod):
     p2, p3 = str(tmp_path / "b.txt"), str(tmp_path / "c.txt")
     rb.OutputBlock(p2, a)
     oracle_mod.output_block(p3, a.copy())
-    assert open(p2).read().split() == open(p3).read().split() or True
+    assert open(p2).read().split() == open(p3).read().split()
     b = rb.InputBlock(p2)
     assert np.array_equal(a.pt_obs_off, b.pt_obs_off)
     assert np.array_equal(a.pt_obs_image, b.pt_obs_image)
