@@ -285,6 +285,26 @@ int32_t rpba_precond_loss_grad(const rpba_precond_set *set, const float *weights
  * serialised by the caller.  No counterpart in the reference. */
 int32_t rpba_float_sequential_sum_noalloc(const float *d_v, int64_t n, float *d_out, void *stream);
 
+/* Per-point refinement against fixed cameras: CalcLSAXMulti
+ * (rpbacore.cpp:536-773), the per-point bundle adjustment of the
+ * reference's parallel RPBA, for every point of the block at once on the GPU
+ * (one thread per point).  robustmode 0: plain; 1: also return each
+ * observation's weighted squared residual in sig0v (the statistic of the
+ * per-image thresholds); 2: observations whose residual exceeds 16 x the
+ * image's threshold sig0w[image] are down-weighted and dropped (keep = 0).
+ * weight_only: evaluate and accumulate only (the reference's first pass).
+ * Outputs per point: the refined point (XX_out, 3 doubles; the input when the
+ * point did not converge) and conv; per track entry (pt_obs_off order): keep
+ * and sig0v; totals: sig0io and redundancy as the reference accumulates them.
+ * The per-partition weight blocks (wxyflag) are not computed. */
+typedef struct rpba_tri_options {
+  int32_t robustmode;   /* 0, 1 or 2                                        */
+  int32_t weight_only;  /* weightonlyflag                                   */
+  int32_t device;
+} rpba_tri_options;
+int32_t rpba_triangulate(const rpba_block *blk, const float *sig0w, const rpba_tri_options *opt, double *XX_out,
+                         uint8_t *keep, float *sig0v, uint8_t *conv, double *sig0io, int64_t *redundancy);
+
 /* Batched form: many independent scenes of uneven size on one GPU.  Every
  * scene is solved as rpba_calc_plsa would solve it (in place; reports[i] and
  * status[i] per scene); `workers` scenes run at once, each on its own stream,

@@ -102,6 +102,17 @@ def exteval(block: Block, opts: RpbaOptionsC | None = None):
     return res[: 2 * block.n_obs].reshape(-1, 2), rep.as_dict()
 
 
+def triangulate(block: Block, sig0w=None, robustmode: int = 0, weight_only: bool = False) -> dict:
+    """CalcLSAXMulti for every point (the oracle's restatement)."""
+    from rpba_b200 import lib as rlib
+    L = lib()
+    L.oracle_triangulate.restype = C.c_int32
+    L.oracle_triangulate.argtypes = [C.POINTER(RpbaBlockC), C.POINTER(C.c_float), C.c_int32, C.c_int32,
+                                     C.POINTER(C.c_double), C.POINTER(C.c_uint8), C.POINTER(C.c_float),
+                                     C.POINTER(C.c_uint8), C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    return rlib.triangulate(block, sig0w, robustmode, weight_only, fn=L.oracle_triangulate)
+
+
 def input_block(path: str, k24out: bool = True) -> Block:
     cb = RpbaBlockC()
     st = lib().oracle_input_block(path.encode(), 3, int(k24out), C.byref(cb))

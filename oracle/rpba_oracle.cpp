@@ -1485,6 +1485,209 @@ void copy_log(const std::string &s, char *log, size_t cap) {
 
 } // namespace
 
+/* ------------------------------------------- per-point triangulation
+ * CalcLSAXMulti (rpbacore.cpp:536-773) with CalcCorrPointMulti (:778-837)
+ * and CalcCalibratedDerivatives (:841-877): robust Gauss-Newton of one
+ * point against fixed cameras.  The per-partition weight blocks
+ * (wxyflag) are not restated: they only feed the partitioned merge. */
+namespace {
+
+struct TriObs {
+  int im, sl;
+};
+
+// residuals and projections of one point (CalcCorrPointMulti)
+void tri_corr(const rpba_block *b, const std::vector<TriObs> &ob, double X0, double X1, double X2,
+              const std::vector<float> &wx, const std::vector<float> &wy, const std::vector<float> &wxy,
+              const std::vector<float> &wxo, const std::vector<float> &wyo, const std::vector<float> &wxyo,
+              std::vector<double> &corr, float &sig0, std::vector<float> &sig0v, std::vector<float> &p1v,
+              std::vector<float> &p2v, std::vector<float> &p3v) {
+  sig0 = 0.f;
+  for (size_t js = 0; js < ob.size(); ++js) {
+    const int j = ob[js].im;
+    const float *P = &b->pmat[12 * j];
+    double p1 = (double)P[0] * X0 + (double)P[1] * X1 + (double)P[2] * X2 + (double)P[3];
+    double p2 = (double)P[4] * X0 + (double)P[5] * X1 + (double)P[6] * X2 + (double)P[7];
+    double p3 = (double)P[8] * X0 + (double)P[9] * X1 + (double)P[10] * X2 + (double)P[11];
+    if (std::fabs(p3) < 1.e-3)
+      p3 = p3 > 0. ? 1.e3 : -1.e3;
+    else
+      p3 = 1. / p3;
+    p1 *= p3;
+    p2 *= p3;
+    p1v[js] = (float)p1;
+    p2v[js] = (float)p2;
+    p3v[js] = (float)p3;
+    const double dist = p1 * p1 + p2 * p2;
+    const double z = 1. + (double)(b->distpara[2 * j] * dist + b->distpara[2 * j + 1] * dist * dist);
+    p1 *= z;
+    p2 *= z;
+    p1 *= b->K[9 * j];
+    p2 *= b->K[9 * j];
+    const double dx = b->xg[2 * ob[js].sl] - p1, dy = b->xg[2 * ob[js].sl + 1] - p2;
+    corr[2 * js] = dx;
+    corr[2 * js + 1] = dy;
+    sig0 += (float)(dx * dx * wx[js] + dy * dy * wy[js] + 2 * dx * dy * wxy[js]);
+    sig0v[js] = (float)(dx * dx * wxo[js] + dy * dy * wyo[js] + 2 * dx * dy * wxyo[js]);
+  }
+}
+
+// d(projection)/dX chained through the distortion and the calibration
+void tri_calibrated(double *xp, double *yp, double x, double y, double k2, double k4, double fx, double fy,
+                    double sk) {
+  const double r2 = x * x + y * y, r4 = r2 * r2;
+  const double axx = k4 * r4 + x * (2 * k2 * x + 4 * k4 * x * r2) + k2 * r2 + 1.;
+  const double axy = x * (4 * k4 * r2 * y + 2 * k2 * y);
+  const double ayx = y * (4 * k4 * x * r2 + 2 * k2 * x);
+  const double ayy = y * (2 * k2 * y + 4 * k4 * r2 * y) + k4 * r4 + k2 * r2 + 1.;
+  for (int c = 0; c < 3; ++c) {
+    const double u = xp[c], v = yp[c];
+    double nx = axx * u + axy * v;
+    double ny = ayy * v + ayx * u;
+    nx = nx * fx + ny * sk;
+    ny *= fy;
+    xp[c] = nx;
+    yp[c] = ny;
+  }
+}
+
+}  // namespace
+
+extern "C" int32_t oracle_triangulate(const rpba_block *b, const float *sig0w, int32_t robustmode,
+                                      int32_t weight_only, double *XXo, uint8_t *keep, float *sig0v_out,
+                                      uint8_t *conv, double *sig0io, int64_t *redundancy) {
+  double s0io = 0.;
+  long long red = 0;
+  for (int pi = 0; pi < b->n_points; ++pi) {
+    const int s = b->pt_obs_off[pi], e = b->pt_obs_off[pi + 1], pxs = e - s;
+    for (int j = s; j < e; ++j) keep[j] = 0;
+    conv[pi] = 0;
+    const double Xin[3] = {(double)b->XX[3 * pi], (double)b->XX[3 * pi + 1], (double)b->XX[3 * pi + 2]};
+    for (int q = 0; q < 3; ++q) XXo[3 * pi + q] = Xin[q];
+    if (pxs <= 0) continue;
+    std::vector<TriObs> ob(pxs);
+    std::vector<float> wx(pxs), wy(pxs), wxy(pxs), wxo(pxs), wyo(pxs), wxyo(pxs), sv(pxs), p1v(pxs), p2v(pxs),
+        p3v(pxs);
+    std::vector<double> corr(2 * pxs), Bw(6 * pxs);
+    std::vector<bool> del(pxs, false);
+    float wsum = 0.f;
+    for (int js = 0; js < pxs; ++js) {
+      ob[js].im = b->pt_obs_image[s + js];
+      ob[js].sl = b->img_obs_off[ob[js].im] + b->pt_obs_slot[s + js];
+      wx[js] = wxo[js] = b->wx[ob[js].sl];
+      wy[js] = wyo[js] = b->wy[ob[js].sl];
+      wxy[js] = wxyo[js] = b->wxy[ob[js].sl];
+      wsum += wx[js] + wy[js];
+    }
+    int pxs2 = 2 * pxs, pxsd = pxs;
+    float X0 = (float)Xin[0], X1 = (float)Xin[1], X2 = (float)Xin[2];
+    float Xo0 = X0, Xo1 = X1, Xo2 = X2, sig0 = 1.e20f, sig0opt = 1.e20f;
+    int iflag = robustmode > 0 ? 2 : 1, iter = 1;
+    bool cv = false;
+    tri_corr(b, ob, X0, X1, X2, wx, wy, wxy, wxo, wyo, wxyo, corr, sig0opt, sv, p1v, p2v, p3v);
+    if (weight_only) {
+      wsum /= (float)pxs2;
+      s0io += sig0opt / wsum;
+      red += pxs2 - 3;
+    }
+    while (iflag > -1 && iter < 101) {
+      double N[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      for (int js = 0; js < pxs; ++js) {
+        const int j = ob[js].im;
+        const float *P = &b->pmat[12 * j];
+        const double x = p1v[js], y = p2v[js], P3 = p3v[js], P1 = (double)p1v[js] * p3v[js],
+                     P2 = (double)p2v[js] * p3v[js];
+        double xp[3], yp[3];
+        for (int c = 0; c < 3; ++c) {
+          xp[c] = (double)P[c] * P3 - (double)P[8 + c] * P1;
+          yp[c] = (double)P[4 + c] * P3 - (double)P[8 + c] * P2;
+        }
+        tri_calibrated(xp, yp, x, y, b->distpara[2 * j], b->distpara[2 * j + 1], b->K[9 * j], b->K[9 * j + 4],
+                       b->K[9 * j + 1]);
+        double *W = &Bw[6 * js];  // row 0: x, row 1: y; weighted
+        for (int c = 0; c < 3; ++c) {
+          W[c] = xp[c] * wx[js] + yp[c] * wxy[js];
+          W[3 + c] = yp[c] * wy[js] + xp[c] * wxy[js];
+        }
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) N[r * 3 + c] += xp[r] * W[c] + yp[r] * W[3 + c];
+      }
+      N[0] *= 1.001;
+      N[4] *= 1.001;
+      N[8] *= 1.001;
+      double Ni[9];
+      inv3(N, Ni);
+      double dx[3] = {0., 0., 0.};
+      for (int js = 0; js < pxs; ++js) {
+        const double *W = &Bw[6 * js];
+        for (int r = 0; r < 3; ++r) {
+          double t = 0.;
+          for (int c = 0; c < 3; ++c) t += Ni[r * 3 + c] * (W[c] * corr[2 * js] + W[3 + c] * corr[2 * js + 1]);
+          dx[r] += t;
+        }
+      }
+      X0 = Xo0 + (float)dx[0];
+      X1 = Xo1 + (float)dx[1];
+      X2 = Xo2 + (float)dx[2];
+      tri_corr(b, ob, X0, X1, X2, wx, wy, wxy, wxo, wyo, wxyo, corr, sig0, sv, p1v, p2v, p3v);
+      if (iflag == 1 && robustmode == 2) {
+        for (int js = 0; js < pxs; ++js)
+          if (sv[js] * sig0w[ob[js].im] > 16.f) {
+            wx[js] *= 1.e-4f;
+            wy[js] *= 1.e-4f;
+            wxy[js] *= 1.e-4f;
+            if (wx[js] + wy[js] < 2.e-8f) {
+              wx[js] = wy[js] = 1.e-8f;
+              wxy[js] = 0.f;
+            }
+            --pxsd;
+            del[js] = true;
+          }
+        if (pxsd < 2) break;
+      }
+      if (sig0 < sig0opt * 1.001) {
+        if (sig0opt < sig0 * 1.05f) --iflag;
+        if (!weight_only) {
+          Xo0 = X0;
+          Xo1 = X1;
+          Xo2 = X2;
+        }
+        sig0opt = sig0;
+        cv = true;
+      } else {
+        --iflag;
+      }
+      if (weight_only) break;
+      ++iter;
+    }
+    int kept = 0;
+    for (int js = 0; js < pxs; ++js) {
+      sig0v_out[s + js] = sv[js];
+      const bool k = !(robustmode == 2 && del[js]);
+      keep[s + js] = k ? 1 : 0;
+      if (!k) pxs2 -= 2;
+      kept += k;
+    }
+    if (kept < 2 || !cv) {
+      for (int js = 0; js < pxs; ++js) keep[s + js] = 0;
+      for (int q = 0; q < 3; ++q) XXo[3 * pi + q] = Xin[q];
+      continue;
+    }
+    conv[pi] = 1;
+    if (!weight_only) {
+      XXo[3 * pi] = Xo0;
+      XXo[3 * pi + 1] = Xo1;
+      XXo[3 * pi + 2] = Xo2;
+      wsum /= (float)pxs2;
+      s0io += sig0opt / wsum;
+      red += pxs2 - 3;
+    }
+  }
+  *sig0io = s0io;
+  *redundancy = red;
+  return RPBA_OK;
+}
+
 extern "C" {
 
 /* CalcPLSA single-LSA / Exteval branches (rpbacore.cpp:28-98, 511-527). */

@@ -114,6 +114,10 @@ class RpbaPrecondBuffersC(C.Structure):
                 ("rowoff", _i32p), ("ent_col", _i32p), ("ent_blk", _i32p), ("sys_row", _i32p)]
 
 
+class RpbaTriOptionsC(C.Structure):
+    _fields_ = [("robustmode", C.c_int32), ("weight_only", C.c_int32), ("device", C.c_int32)]
+
+
 class RpbaBatchReportC(C.Structure):
     _fields_ = [("seconds", C.c_double), ("scenes_per_second", C.c_double), ("tune_seconds", C.c_double),
                 ("workers", C.c_int32), ("failed", C.c_int32)]

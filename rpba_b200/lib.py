@@ -21,7 +21,7 @@ import os
 import numpy as np
 
 from .block import (Block, RpbaBlockC, RpbaOptionsC, RpbaReportC, RpbaTrainOptionsC, RpbaTrainReportC,
-                    RpbaPrecondSetC, RpbaPrecondBuffersC, RpbaBatchReportC,
+                    RpbaPrecondSetC, RpbaPrecondBuffersC, RpbaBatchReportC, RpbaTriOptionsC,
                     make_options, PRECOND_WEIGHTS, SOLVER_PCG, SOLVER_DIRECT, SOLVER_LEARNED, PREC_FP64,
                     PREC_MIXED)
 
@@ -39,7 +39,7 @@ EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block
            "rpba_get_state", "rpba_get_log", "rpba_exteval", "rpba_kernel_stats", "rpba_float_sequential_sum",
            "rpba_float_sequential_sum_noalloc", "rpba_train_preconditioner",
            "rpba_set_preconditioner", "rpba_precond_loss_grad", "rpba_record_systems", "rpba_solve_batch",
-           "rpba_destroy")
+           "rpba_triangulate", "rpba_destroy")
 
 _lib = None
 
@@ -98,6 +98,10 @@ def load():
     L.rpba_solve_batch.argtypes = [bp, C.c_int32, op, C.c_int32, rp, C.POINTER(C.c_int32),
                                    C.POINTER(RpbaBatchReportC)]
     L.rpba_solve_batch.restype = C.c_int32
+    L.rpba_triangulate.argtypes = [bp, C.POINTER(C.c_float), C.POINTER(RpbaTriOptionsC), C.POINTER(C.c_double),
+                                   C.POINTER(C.c_uint8), C.POINTER(C.c_float), C.POINTER(C.c_uint8),
+                                   C.POINTER(C.c_double), C.POINTER(C.c_int64)]
+    L.rpba_triangulate.restype = C.c_int32
     L.rpba_kernel_stats.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     L.rpba_kernel_stats.restype = C.c_int32
     L.rpba_destroy.argtypes = [C.c_void_p]
@@ -169,6 +173,34 @@ def train_preconditioner(blocks, steps=300, batch=0, lr=3e-3, probes=2, seed=1, 
     if st != 0:
         raise RpbaError(st, "rpba_train_preconditioner")
     return w, {k: getattr(rep, k) for k, _ in rep._fields_}
+
+
+def triangulate(block: Block, sig0w=None, robustmode: int = 0, weight_only: bool = False, device: int = 0,
+                fn=None) -> dict:
+    """Per-point refinement of every point against the block's fixed cameras
+    (rpba_triangulate; ``fn`` substitutes another implementation with the
+    same C signature, e.g. the oracle's)."""
+    cb = block.as_c()
+    nt, np_ = block.n_obs, block.n_points
+    out = {"XX": np.zeros(3 * np_), "keep": np.zeros(nt, np.uint8), "sig0v": np.zeros(nt, np.float32),
+           "conv": np.zeros(np_, np.uint8)}
+    s0, red = C.c_double(), C.c_int64()
+    w = None if sig0w is None else np.ascontiguousarray(sig0w, np.float32)
+    wp = None if w is None else w.ctypes.data_as(C.POINTER(C.c_float))
+    args = (C.byref(cb), wp)
+    tail = (out["XX"].ctypes.data_as(C.POINTER(C.c_double)), out["keep"].ctypes.data_as(C.POINTER(C.c_uint8)),
+            out["sig0v"].ctypes.data_as(C.POINTER(C.c_float)), out["conv"].ctypes.data_as(C.POINTER(C.c_uint8)),
+            C.byref(s0), C.byref(red))
+    if fn is None:
+        o = RpbaTriOptionsC(int(robustmode), int(weight_only), int(device))
+        st = load().rpba_triangulate(*args, C.byref(o), *tail)
+    else:
+        st = fn(*args, int(robustmode), int(weight_only), *tail)
+    if st != 0:
+        raise RpbaError(st, "rpba_triangulate")
+    out["XX"] = out["XX"].reshape(np_, 3)
+    out["sig0io"], out["redundancy"] = s0.value, red.value
+    return out
 
 
 def solve_batch(blocks, workers: int = 0, **opt_kw):
