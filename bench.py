@@ -60,7 +60,7 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", type=int, default=3)
     ap.add_argument("--scale", type=float, default=1.0)
-    ap.add_argument("--tol", type=float, default=1e-5, help="relative PCG tolerance of the learned solver")
+    ap.add_argument("--tol", type=float, default=3e-5, help="relative PCG tolerance of the learned solver")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--no-plain", action="store_true", help="skip timing the plain solver")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -192,7 +192,9 @@ __global__ void k_coarse_fixdiag(CoarseWork C) {
 // Symmetric Jacobi scaling of A_c before the factorisation (the coarse
 // unknowns mix radians, metres, pixels and distortion coefficients, whose
 // diagonal entries span many decades): dsc = diag^-1/2, A <- D A D with a
-// unit diagonal (+1e-12 against roundoff); the same kernel without the
+// unit diagonal (+1e-6: an aggregate whose cameras barely fix one of its
+// coarse unknowns leaves A_c nearly singular, and a preconditioner needs
+// only to stay SPD); the same kernel without the
 // diagonal term maps the inverse back (A^-1 = D (D A D)^-1 D).
 __global__ void k_coarse_diag(CoarseWork C) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -205,7 +207,7 @@ __global__ void k_coarse_scale(double *A, const double *dsc, int n, int add_diag
   if (g >= (long long)n * n) return;
   const int i = (int)(g / n), j = (int)(g % n);
   double v = A[g] * dsc[i] * dsc[j];
-  if (add_diag && i == j) v += 1e-12;
+  if (add_diag && i == j) v += 1e-6;
   A[g] = v;
 }
 

@@ -474,15 +474,18 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
     const double meandr = g3[0], er1th1 = g3[1];
     if (k == 0) meandr0 = meandr;
     // mode 0 keeps the iterate with the smallest increment (the reference's
-    // exivold); mode 1 keeps the latest
-    const bool improved = A.mode == 1 || meandr < meandrold;
+    // exivold); mode 1 keeps the latest finite one and stops, unconverged,
+    // at a breakdown (a non-finite residual or increment)
+    const bool finite = isfinite(g3[0]) && isfinite(g3[2]);
+    const bool improved = (A.mode == 1 && finite) || meandr < meandrold;
     if (improved) {
       meandrold = meandr;
       for (int row = A.row0 + gwarp; row < A.row1; row += nwarps)
         if (lane < 9) A.xbest[(size_t)row * 9 + lane] = __ldcg(A.x + (size_t)row * 9 + lane);
     }
     if (A.mode == 0 && meandr * 1.e5 < meandr0) break;
-    if (A.mode == 1 && !(g3[2] > A.tol2 * erthk0)) {
+    if (A.mode == 1 && !finite) break;
+    if (A.mode == 1 && g3[2] <= A.tol2 * erthk0) {
       converged = true;
       break;
     }

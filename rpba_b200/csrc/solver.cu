@@ -755,6 +755,7 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
   PROF("pair", 1, launch_pair_pass(L, s));
   int msize = 0;
   for (int k = begini; k < nimg; ++k) msize += camparv[k + 1] - camparv[k];
+  const int nunk = msize;
   if (msize < 1000) msize = 1000;
   if (opt.pcg_max_iterations > 0) msize = opt.pcg_max_iterations;
   if (opt.solver == RPBA_SOLVER_DIRECT) {
@@ -822,9 +823,28 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
       log += line;
     }
     if (!ok) {
+      // fallbacks: block-Jacobi PCG alone (no coarse space, no network) to
+      // the same tolerance and the reference's cap; then the dense direct
+      // solve where it fits (the dense matrix of 40k unknowns is 12.8 GB);
+      // past that the block-Jacobi PCG's best iterate is used
       ++rep.pcg_fallbacks;
-      ensure_direct();
-      PROF("direct", 1, direct_solve(L, DW, W.xbest, s));
+      int it2[2] = {0, 0};
+      {
+        CoopLock lk(this);
+        PROF("pcg", 2, pcg_solve(L, W, msize, pcg_grid, s, 1, opt.pcg_tolerance > 0. ? opt.pcg_tolerance : 1e-6));
+      }
+      RPBA_CUDA_CHECK(cudaMemcpyAsync(it2, W.iters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+      RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+      learned_iters += it2[0];
+      if (opt.verbose & 4) {
+        char line[128];
+        std::snprintf(line, sizeof line, "PCG fallback (block-Jacobi): iterations %d converged %d\n", it2[0], it2[1]);
+        log += line;
+      }
+      if (it2[1] == 0 && nunk <= 40000) {
+        ensure_direct();
+        PROF("direct", 1, direct_solve(L, DW, W.xbest, s));
+      }
     }
   } else {
     {
