@@ -14,12 +14,13 @@ namespace rpba {
 
 // Per-observation linearisation record (doubles):
 //   [0..17]  Bc (2 x 9 camera Jacobian, row major)
-//   [18..23] G  = W Jp (2 x 3)
+//   [18..23] G  = W Jp (2 x 3); in the FP32 form H = G L^-T, V = L L^T
 //   [24..25] e  = W d
 //   [26..28] M  = W - G V^-1 G^T  (M00, M01, M11)
 //   [29..30] m  = e - G V^-1 g
 constexpr int REC = 32;
-// Per-point record: V^-1 (9, row major) and g (3).
+// Per-point record: V^-1 (9, row major) and g (3); in the FP32 form L^-1
+// (9, row major, lower) and q = L^-1 g.
 constexpr int PREC = 12;
 
 struct DevLSA {
@@ -219,13 +220,17 @@ struct PcgWork {
   unsigned *bar;
   int *iters;
 };
+// A PCG solve is pcg_prepare (the preconditioner and the start vectors;
+// returns its launch count) followed by pcg_iterate (the persistent kernel).
 // mode 0: the reference's stop rule; mode 1: stop when r^T M^-1 r falls
 // below tol^2 times its start value (W.iters[1] = 1 when it did), with the
 // learned preconditioner `weights` (nullptr: plain block-Jacobi).
 // With `coarse` the preconditioner is two-level: the (learned) block
 // Jacobi part plus the coarse correction P A_c^-1 P^T.
-int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s, int mode = 0,
-              double tol = 0., const float *weights = nullptr, const CoarseWork *coarse = nullptr);
+int pcg_prepare(const DevLSA &L, const PcgWork &W, int mode, const float *weights, const CoarseWork *coarse,
+                cudaStream_t s);
+int pcg_iterate(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s, int mode, double tol,
+                const CoarseWork *coarse);
 int pcg_max_grid(int device);
 
 // ---- structure (structure.cu)

@@ -1,9 +1,10 @@
 // kernels.cu -- per-observation, per-point and per-camera kernels of the
 // global LSA (rbacore.cpp).  The linearisation kernels (point, camera,
 // pair, back-substitution) are compiled for two forms: FP64 throughout (the
-// drop-in form) and FP32 records/blocks with FP32 arithmetic, compensated
-// (Kahan) per-camera and per-pair sums and FP64 inversion of ill-conditioned
-// point blocks (the mixed-precision form).  Residuals and the cost stay FP64.
+// drop-in form) and the mixed-precision form: FP32 records and blocks with
+// FP32 arithmetic and compensated (Kahan) per-camera and per-pair sums, the
+// point blocks factored in FP64 and the records whitened by the factor
+// (k_point32).  Residuals and the cost stay FP64.
 #include <cub/cub.cuh>
 
 #include "internal.h"
@@ -127,9 +128,10 @@ __global__ void k_seq_sum(const float *__restrict__ v, int n, float *out) {
 // (rbacore.cpp:1215-1348, 1420-1616): Jacobians of every observation, the
 // point block V = sum Jp^T W Jp and g = sum Jp^T W d, V damped and inverted;
 // the per-observation record for the camera, pair and back-substitution
-// kernels.
+// kernels.  FP64 form (T = double); the FP32 form is k_point32.
 template <class T>
 __global__ void k_point(DevLSA L, double multfact1) {
+  static_assert(sizeof(T) == 8, "the FP32 form is k_point32");
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
   const int p = gt / GRP, ln = gt % GRP;
   // no early exit: the group reductions below shuffle over the full warp
@@ -194,22 +196,7 @@ __global__ void k_point(DevLSA L, double multfact1) {
   V[4] = (T)(V[4] * multfact1);
   V[8] = (T)(V[8] * multfact1);
   T Vi[9];
-  if constexpr (sizeof(T) == 8) {
-    inv3<double>(V, Vi);
-  } else {
-    // FP32 unless the point block is ill-conditioned (determinant small
-    // against the diagonal product): then FP64
-    const T det = V[0] * (V[4] * V[8] - V[5] * V[7]) - V[1] * (V[3] * V[8] - V[5] * V[6]) +
-                  V[2] * (V[3] * V[7] - V[4] * V[6]);
-    if (fabsf(det) > 1e-3f * fabsf(V[0] * V[4] * V[8])) {
-      inv3<float>(V, Vi);
-    } else {
-      double Vd[9], Vid[9];
-      for (int j = 0; j < 9; ++j) Vd[j] = V[j];
-      inv3<double>(Vd, Vid);
-      for (int j = 0; j < 9; ++j) Vi[j] = (T)Vid[j];
-    }
-  }
+  inv3<T>(V, Vi);
   if (ln == 0 && valid) {
     T *pv = Store<T>::ptV(L) + (size_t)p * PREC;
 #pragma unroll
@@ -240,6 +227,145 @@ __global__ void k_point(DevLSA L, double multfact1) {
     r[28] = (T)w.y - (GV[1][0] * G[1][0] + GV[1][1] * G[1][1] + GV[1][2] * G[1][2]);
     r[29] = r[24] - (G[0][0] * vg[0] + G[0][1] * vg[1] + G[0][2] * vg[2]);
     r[30] = r[25] - (G[1][0] * vg[0] + G[1][1] * vg[1] + G[1][2] * vg[2]);
+  }
+}
+
+// FP32 form of the point pass, whitened.  V and g are summed in FP64 from
+// the FP32-rounded point Jacobians, V = L L^T is factored in FP64, and the
+// record carries H = G L^-T in place of G, so that every Schur product
+// G V^-1 G^T = H H^T is formed from bounded factors (H H^T <= W for each
+// observation) however ill-conditioned V is: the explicit V^-1 of a distant,
+// down-weighted point overflows FP32, and products with it lose all digits.
+// A pivot at or below 1e-13 of its diagonal entry (not resolvable in FP64
+// arithmetic) or below 1e-60 drops its coordinate: the step leaves that
+// coordinate of the point unchanged (the factor is that of V without its row
+// and column), and the Schur contribution stays positive semidefinite.
+// Point record: L^-1 (9, row major, zeros above the diagonal), q = L^-1 g.
+__global__ void k_point32(DevLSA L, double multfact1) {
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = gt / GRP, ln = gt % GRP;
+  const bool valid = p < L.npts;  // no early exit (full-warp shuffles below)
+  const int t0 = valid ? L.pt_off[p] : 0, t1 = valid ? L.pt_off[p + 1] : 0;
+  double X0 = 0., X1 = 0., X2 = 0.;
+  if (valid) {
+    const double *X = L.XPM + L.nrioff + 3 * p;
+    X0 = X[0];
+    X1 = X[1];
+    X2 = X[2];
+  }
+  const int esvm[2] = {L.gauge[0], L.gauge[1]};
+  double V[6] = {0., 0., 0., 0., 0., 0.};  // V00 V01 V02 V11 V12 V22
+  double g[3] = {0., 0., 0.};
+  for (int o = t0 + ln; o < t1; o += GRP) {
+    const int k = L.o_cam[o];
+    const CamState c = L.camn[k];
+    const float2 xg = L.o_xg[o];
+    ObsEval e;
+    eval_obs(c, X0, X1, X2, xg.x, xg.y, L.defdiff, e);
+    if (e.nan) L.o_s0rmv[o] = 1.e20f;
+    float Bc[2][RPBA_P], Bp[2][3];
+    jacobians<float>(c, e, role_of(L, k), esvm, L.addmask, Bc, Bp);
+    const float4 w = L.o_w[o];
+    const double W0 = w.x, W1 = w.y, W2 = w.z;
+    double G[2][3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      G[0][j] = Bp[0][j] * W0 + Bp[1][j] * W2;
+      G[1][j] = Bp[0][j] * W2 + Bp[1][j] * W1;
+    }
+    V[0] += G[0][0] * Bp[0][0] + G[1][0] * Bp[1][0];
+    V[1] += G[0][0] * Bp[0][1] + G[1][0] * Bp[1][1];
+    V[2] += G[0][0] * Bp[0][2] + G[1][0] * Bp[1][2];
+    V[3] += G[0][1] * Bp[0][1] + G[1][1] * Bp[1][1];
+    V[4] += G[0][1] * Bp[0][2] + G[1][1] * Bp[1][2];
+    V[5] += G[0][2] * Bp[0][2] + G[1][2] * Bp[1][2];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) g[a] += G[0][a] * e.d1 + G[1][a] * e.d2;
+    float *r = L.rec32 + (size_t)o * REC;
+    const bool cam_active = k >= L.begini;
+#pragma unroll
+    for (int j = 0; j < RPBA_P; ++j) {
+      r[j] = cam_active ? Bc[0][j] : 0.f;
+      r[9 + j] = cam_active ? Bc[1][j] : 0.f;
+    }
+    // Jp until the factor is known; replaced by H below
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      r[18 + j] = Bp[0][j];
+      r[21 + j] = Bp[1][j];
+    }
+    r[24] = (float)(e.d1 * W0 + e.d2 * W2);
+    r[25] = (float)(e.d1 * W2 + e.d2 * W1);
+  }
+#pragma unroll
+  for (int j = 0; j < 6; ++j) V[j] = grp_sum(V[j]);
+#pragma unroll
+  for (int j = 0; j < 3; ++j) g[j] = grp_sum(g[j]);
+  V[0] *= multfact1;
+  V[3] *= multfact1;
+  V[5] *= multfact1;
+  // V = L L^T with guarded pivots; m = L^-1 (lower)
+  auto root = [](double d, double diag) { return (d > 1.e-13 * diag && d > 1.e-60) ? sqrt(d) : 0.; };
+  const double l00 = root(V[0], V[0]);
+  const double i00 = l00 > 0. ? 1. / l00 : 0.;
+  const double l10 = V[1] * i00, l20 = V[2] * i00;
+  const double l11 = root(V[3] - l10 * l10, V[3]);
+  const double i11 = l11 > 0. ? 1. / l11 : 0.;
+  const double l21 = (V[4] - l20 * l10) * i11;
+  const double l22 = root(V[5] - l20 * l20 - l21 * l21, V[5]);
+  const double i22 = l22 > 0. ? 1. / l22 : 0.;
+  double m[6] = {i00, -l10 * i00 * i11, i11, -(l20 * i00 - l21 * l10 * i00 * i11) * i22, -l21 * i11 * i22, i22};
+  // m00 m10 m11 m20 m21 m22; a factor beyond the FP32 range drops the point
+  bool inrange = true;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) inrange = inrange && fabs(m[j]) < 1.e30;
+  if (!inrange)
+#pragma unroll
+    for (int j = 0; j < 6; ++j) m[j] = 0.;
+  const double q0 = m[0] * g[0], q1 = m[1] * g[0] + m[2] * g[1], q2 = m[3] * g[0] + m[4] * g[1] + m[5] * g[2];
+  if (ln == 0 && valid) {
+    float *pv = L.ptV32 + (size_t)p * PREC;
+    pv[0] = (float)m[0];
+    pv[1] = pv[2] = 0.f;
+    pv[3] = (float)m[1];
+    pv[4] = (float)m[2];
+    pv[5] = 0.f;
+    pv[6] = (float)m[3];
+    pv[7] = (float)m[4];
+    pv[8] = (float)m[5];
+    pv[9] = (float)q0;
+    pv[10] = (float)q1;
+    pv[11] = (float)q2;
+  }
+  for (int o = t0 + ln; o < t1; o += GRP) {
+    float *r = L.rec32 + (size_t)o * REC;
+    const float4 w = L.o_w[o];
+    const double W0 = w.x, W1 = w.y, W2 = w.z;
+    double H[2][3];
+    {
+      const double p00 = r[18], p01 = r[19], p02 = r[20], p10 = r[21], p11 = r[22], p12 = r[23];
+      const double G0[3] = {p00 * W0 + p10 * W2, p01 * W0 + p11 * W2, p02 * W0 + p12 * W2};
+      const double G1[3] = {p00 * W2 + p10 * W1, p01 * W2 + p11 * W1, p02 * W2 + p12 * W1};
+      H[0][0] = m[0] * G0[0];
+      H[0][1] = m[1] * G0[0] + m[2] * G0[1];
+      H[0][2] = m[3] * G0[0] + m[4] * G0[1] + m[5] * G0[2];
+      H[1][0] = m[0] * G1[0];
+      H[1][1] = m[1] * G1[0] + m[2] * G1[1];
+      H[1][2] = m[3] * G1[0] + m[4] * G1[1] + m[5] * G1[2];
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      r[18 + j] = (float)H[0][j];
+      r[21 + j] = (float)H[1][j];
+    }
+    const double h00 = H[0][0] * H[0][0] + H[0][1] * H[0][1] + H[0][2] * H[0][2];
+    const double h01 = H[0][0] * H[1][0] + H[0][1] * H[1][1] + H[0][2] * H[1][2];
+    const double h11 = H[1][0] * H[1][0] + H[1][1] * H[1][1] + H[1][2] * H[1][2];
+    r[26] = (float)(W0 - h00);
+    r[27] = (float)(W2 - h01);
+    r[28] = (float)(W1 - h11);
+    r[29] = (float)((double)r[24] - (H[0][0] * q0 + H[0][1] * q1 + H[0][2] * q2));
+    r[30] = (float)((double)r[25] - (H[1][0] * q0 + H[1][1] * q1 + H[1][2] * q2));
   }
 }
 
@@ -321,12 +447,15 @@ __global__ void k_pair(DevLSA L) {
   T *s = sm[wl];
   Acc<T> acc[3];
   const T *rec = Store<T>::rec(L), *ptv = Store<T>::ptV(L);
-  // lane's two record values of one contribution: 24 of the row camera's
-  // observation (Bc 18, G 6), 24 of the column camera's, V^-1 (9) of the point
+  // values of one contribution: 24 of the row camera's observation (Bc 18,
+  // G 6), 24 of the column camera's and, in the FP64 form, V^-1 (9) of the
+  // point; the FP32 form's records hold H = G L^-T, whose products need no
+  // point term
+  constexpr int NV = sizeof(T) == 8 ? 57 : 48;
   auto fetch = [&](int ox, int oy, int p, T &v0, T &v1) {
     v0 = lane < 24 ? rec[(size_t)ox * REC + lane] : rec[(size_t)oy * REC + lane - 24];
     const int i1 = lane + 32;
-    v1 = i1 < 48 ? rec[(size_t)oy * REC + i1 - 24] : (i1 < 57 ? ptv[(size_t)p * PREC + i1 - 48] : T(0));
+    v1 = i1 < 48 ? rec[(size_t)oy * REC + i1 - 24] : (i1 < NV ? ptv[(size_t)p * PREC + i1 - 48] : T(0));
   };
   const int cb = L.boff[wid], ce = L.boff[wid + 1];
   for (int c0 = cb; c0 < ce; c0 += 32) {
@@ -338,32 +467,41 @@ __global__ void k_pair(DevLSA L) {
     int pp = 0;
     if (lane < n) {
       pr = L.contrib[c0 + lane];
-      pp = L.o_pt[pr.x];
+      if constexpr (sizeof(T) == 8) pp = L.o_pt[pr.x];
     }
     T v0, v1;
     fetch(__shfl_sync(0xffffffffu, pr.x, 0), __shfl_sync(0xffffffffu, pr.y, 0), __shfl_sync(0xffffffffu, pp, 0),
           v0, v1);
     for (int j = 0; j < n; ++j) {
       s[lane] = v0;
-      if (lane + 32 < 57) s[lane + 32] = v1;
+      if (lane + 32 < NV) s[lane + 32] = v1;
       if (j + 1 < n)
         fetch(__shfl_sync(0xffffffffu, pr.x, j + 1), __shfl_sync(0xffffffffu, pr.y, j + 1),
               __shfl_sync(0xffffffffu, pp, j + 1), v0, v1);
       __syncwarp();
-      // N = G_s V^-1 G_t^T (2 x 2)
-      const T *Gs = s + 18, *Gt = s + 42, *Vi = s + 48;
-      T GV[2][3];
-#pragma unroll
-      for (int a = 0; a < 2; ++a)
-#pragma unroll
-        for (int b = 0; b < 3; ++b)
-          GV[a][b] = Gs[a * 3] * Vi[b] + Gs[a * 3 + 1] * Vi[3 + b] + Gs[a * 3 + 2] * Vi[6 + b];
+      // N = G_s V^-1 G_t^T (2 x 2); H_s H_t^T in the FP32 form
+      const T *Gs = s + 18, *Gt = s + 42;
       T N[2][2];
+      if constexpr (sizeof(T) == 8) {
+        const T *Vi = s + 48;
+        T GV[2][3];
 #pragma unroll
-      for (int a = 0; a < 2; ++a)
+        for (int a = 0; a < 2; ++a)
 #pragma unroll
-        for (int b = 0; b < 2; ++b)
-          N[a][b] = GV[a][0] * Gt[b * 3] + GV[a][1] * Gt[b * 3 + 1] + GV[a][2] * Gt[b * 3 + 2];
+          for (int b = 0; b < 3; ++b)
+            GV[a][b] = Gs[a * 3] * Vi[b] + Gs[a * 3 + 1] * Vi[3 + b] + Gs[a * 3 + 2] * Vi[6 + b];
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int b = 0; b < 2; ++b)
+            N[a][b] = GV[a][0] * Gt[b * 3] + GV[a][1] * Gt[b * 3 + 1] + GV[a][2] * Gt[b * 3 + 2];
+      } else {
+#pragma unroll
+        for (int a = 0; a < 2; ++a)
+#pragma unroll
+          for (int b = 0; b < 2; ++b)
+            N[a][b] = Gs[a * 3] * Gt[b * 3] + Gs[a * 3 + 1] * Gt[b * 3 + 1] + Gs[a * 3 + 2] * Gt[b * 3 + 2];
+      }
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
         const int e = lane + 32 * q;
@@ -388,7 +526,7 @@ __global__ void k_pair(DevLSA L) {
 
 // ------------------------------------------------- back-substitution
 // rbacore.cpp:1395-1410: dX_p = V^-1 (g - sum_o W_o^T dc_k), with
-// W_o^T dc = G^T (Bc dc).
+// W_o^T dc = G^T (Bc dc); in the FP32 form L^-T (q - sum_o H^T (Bc dc)).
 template <class T>
 __global__ void k_backsub(DevLSA L, const double *__restrict__ xsol) {
   const int gt = blockIdx.x * blockDim.x + threadIdx.x;
@@ -416,11 +554,19 @@ __global__ void k_backsub(DevLSA L, const double *__restrict__ xsol) {
   a2 = grp_sum(a2);
   if (ln == 0 && valid) {
     const T *pv = Store<T>::ptV(L) + (size_t)p * PREC;
-    const T r0 = pv[9] - a0, r1 = pv[10] - a1, r2 = pv[11] - a2;
     double *xo = L.x + L.nrioff + 3 * p;
-    xo[0] = pv[0] * r0 + pv[1] * r1 + pv[2] * r2;
-    xo[1] = pv[3] * r0 + pv[4] * r1 + pv[5] * r2;
-    xo[2] = pv[6] * r0 + pv[7] * r1 + pv[8] * r2;
+    if constexpr (sizeof(T) == 8) {
+      const T r0 = pv[9] - a0, r1 = pv[10] - a1, r2 = pv[11] - a2;
+      xo[0] = pv[0] * r0 + pv[1] * r1 + pv[2] * r2;
+      xo[1] = pv[3] * r0 + pv[4] * r1 + pv[5] * r2;
+      xo[2] = pv[6] * r0 + pv[7] * r1 + pv[8] * r2;
+    } else {
+      // whitened: a = L^-1 sum G^T Bc dc, dX = L^-T (q - a)
+      const double y0 = (double)pv[9] - a0, y1 = (double)pv[10] - a1, y2 = (double)pv[11] - a2;
+      xo[0] = (double)pv[0] * y0 + (double)pv[3] * y1 + (double)pv[6] * y2;
+      xo[1] = (double)pv[4] * y1 + (double)pv[7] * y2;
+      xo[2] = (double)pv[8] * y2;
+    }
   }
 }
 
@@ -821,7 +967,7 @@ void launch_seq_sum(const float *v, int n, float *out, cudaStream_t s) {
 void launch_point_pass(const DevLSA &L, double multfact1, cudaStream_t s) {
   if (L.npts <= 0) return;
   if (L.rec32)
-    k_point<float><<<nblk((long long)L.npts * GRP, 128), 128, 0, s>>>(L, multfact1);
+    k_point32<<<nblk((long long)L.npts * GRP, 128), 128, 0, s>>>(L, multfact1);
   else
     k_point<double><<<nblk((long long)L.npts * GRP, 128), 128, 0, s>>>(L, multfact1);
 }

@@ -558,8 +558,8 @@ int pcg_max_grid(int device) {
 
 // Returns 0; throws CudaError on launch errors.  The iteration count is
 // left in W.iters.
-int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s, int mode, double tol,
-              const float *weights, const CoarseWork *coarse) {
+int pcg_prepare(const DevLSA &L, const PcgWork &W, int mode, const float *weights, const CoarseWork *coarse,
+                cudaStream_t s) {
   const bool co = coarse && coarse->nagg > 0;
   if (mode == 1 || weights || co)
     learned_pcg_setup(L, W, weights, s);
@@ -567,6 +567,12 @@ int pcg_solve(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream
     k_pcg_setup<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W);
   if (co) coarse_apply(L, *coarse, W.r, W.h, s);
   RPBA_CUDA_CHECK(cudaGetLastError());
+  return co ? 3 : 1;
+}
+
+int pcg_iterate(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s, int mode, double tol,
+                const CoarseWork *coarse) {
+  const bool co = coarse && coarse->nagg > 0;
   const int nrows = L.nimg - L.begini;
   if (nrows <= 0) return 0;
   int g = (L.nitems + PCG_W - 1) / PCG_W;

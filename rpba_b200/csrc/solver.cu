@@ -740,18 +740,20 @@ void rpba_handle::structure() {
 // CalcBundleSep (rbacore.cpp:1094-1195): assemble, solve, back-substitute.
 bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
   const double multfact1 = 1. + multfact;
-  // Algorithmic bytes of each launch (inputs read once, outputs written once):
-  //  point : obs (cam 4, xg 8, w 16, record 248 out) + point (X 24, off 8,
-  //          V^-1 g 96 out) + trial cameras 160
-  //  camera: obs (list 4, record part 184) + camera (block 648 + rhs 72 out)
-  //  pair  : obs records (Bc G, 192) + points (V^-1, 72) + contributions (8)
-  //          + off-diagonal blocks out (648)
+  // Algorithmic bytes of each launch (inputs read once, outputs written once;
+  // E = 8 or 4 bytes per record entry in the FP64 or FP32 form):
+  //  point : obs (cam 4, xg 8, w 16, record 31 E out) + point (X 24, off 8,
+  //          point record 12 E out) + trial cameras 160
+  //  camera: obs (list 4, record part 23 E) + camera (block 81 E + rhs 72 out)
+  //  pair  : obs records (Bc G, 24 E) + points (V^-1, 9 E; not read in the
+  //          FP32 form) + contributions (8) + off-diagonal blocks out (81 E)
   const double No = L.nobs, Np = L.npts, Nc = nimg, Nb = L.nboff;
-  prof.next_bytes = No * (4 + 8 + 16 + 248) + Np * (24 + 8 + 96) + Nc * 160;
+  const double E = L.rec32 ? 4. : 8.;
+  prof.next_bytes = No * (4 + 8 + 16 + 31 * E) + Np * (24 + 8 + 12 * E) + Nc * 160;
   PROF("point", 1, launch_point_pass(L, multfact1, s));
-  prof.next_bytes = No * (4 + 184) + (Nc - begini) * (648 + 72);
+  prof.next_bytes = No * (4 + 23 * E) + (Nc - begini) * (81 * E + 72);
   PROF("camera", 1, launch_camera_pass(L, multfact1, s));
-  prof.next_bytes = No * 192 + Np * 72 + npairs_cur * 8. + Nb * 648;
+  prof.next_bytes = No * 24 * E + (L.rec32 ? 0. : Np * 72) + npairs_cur * 8. + Nb * 81 * E;
   PROF("pair", 1, launch_pair_pass(L, s));
   int msize = 0;
   for (int k = begini; k < nimg; ++k) msize += camparv[k + 1] - camparv[k];
@@ -791,7 +793,8 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
       const int cap_try = (cw && !fresh) ? std::min(cap, 3 * coarse_ref_iters + 20) : cap;
       {
         CoopLock lk(this);
-        PROF("pcg", 2, pcg_solve(L, W, cap_try, pcg_grid, s, mode, opt.pcg_tolerance, d_weights, cw));
+        PROF("pcg_setup", cw ? 3 : 1, pcg_prepare(L, W, mode, d_weights, cw, s));
+        PROF("pcg", 1, pcg_iterate(L, W, cap_try, pcg_grid, s, mode, opt.pcg_tolerance, cw));
       }
       RPBA_CUDA_CHECK(cudaMemcpyAsync(it, W.iters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
       if (cw) RPBA_CUDA_CHECK(cudaMemcpyAsync(it + 2, CW.err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -831,7 +834,9 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
       int it2[2] = {0, 0};
       {
         CoopLock lk(this);
-        PROF("pcg", 2, pcg_solve(L, W, msize, pcg_grid, s, 1, opt.pcg_tolerance > 0. ? opt.pcg_tolerance : 1e-6));
+        PROF("pcg_setup", 1, pcg_prepare(L, W, 1, nullptr, nullptr, s));
+        PROF("pcg", 1, pcg_iterate(L, W, msize, pcg_grid, s, 1, opt.pcg_tolerance > 0. ? opt.pcg_tolerance : 1e-6,
+                                    nullptr));
       }
       RPBA_CUDA_CHECK(cudaMemcpyAsync(it2, W.iters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
       RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
@@ -849,7 +854,8 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
   } else {
     {
       CoopLock lk(this);
-      PROF("pcg", 2, pcg_solve(L, W, msize, pcg_grid, s));
+      PROF("pcg_setup", 1, pcg_prepare(L, W, 0, nullptr, nullptr, s));
+      PROF("pcg", 1, pcg_iterate(L, W, msize, pcg_grid, s, 0, 0., nullptr));
     }
     pcg_pending = true;
   }
