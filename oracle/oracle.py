@@ -82,8 +82,10 @@ def calc_plsa(block: Block, opts: RpbaOptionsC | None = None, log_cap: int = 1 <
 
 def calc_plsa_variant(block: Block, opts: RpbaOptionsC | None = None, variant: int = 1,
                       log_cap: int = 1 << 16):
-    """calc_plsa with the SpMV blocks of each column visited in reverse order:
-    the same arithmetic up to summation order (a self-sensitivity probe)."""
+    """calc_plsa with the SpMV blocks of each column visited in another
+    order (1 reversed, 2 rotated by half, >= 3 a shuffle seeded by the
+    variant): the same arithmetic up to summation order (a self-sensitivity
+    probe)."""
     b = block.copy()
     cb = b.as_c()
     o = opts if opts is not None else make_options()

@@ -46,7 +46,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <map>
+#include <random>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -258,9 +260,12 @@ std::string fmt_g(double v) {
 
 /* ---------------------------------------------------------------- LSA */
 
-/* Test hook: 1 reverses the order in which the off-diagonal blocks of a
- * column are visited in the SpMV.  Used only to measure how sensitive the
- * reference's inexact PCG is to summation order. */
+/* Test hook: the order in which the off-diagonal blocks of a column are
+ * visited in the SpMV.  0 the reference's (map order), 1 reversed, 2 rotated
+ * by half, 3..19 a shuffle seeded by the variant; 20..39 the map order with
+ * the PCG's sums over cameras blocked (dot_group); >= 40 the same sums as
+ * pairwise trees (tree_leaf).  Used only to measure
+ * how sensitive the reference's inexact PCG is to summation order. */
 int g_order_variant = 0;
 
 struct Opts {
@@ -1003,6 +1008,10 @@ void LSA::sparse_pcg() {
       for (auto &kv : Off[i]) order.push_back(&kv);
       if (g_order_variant == 1) std::reverse(order.begin(), order.end());
       if (g_order_variant == 2) std::rotate(order.begin(), order.begin() + order.size() / 2, order.end());
+      if (g_order_variant >= 3 && g_order_variant < 20) {
+        std::mt19937 g((unsigned)g_order_variant * 7919u + (unsigned)i);
+        std::shuffle(order.begin(), order.end(), g);
+      }
       for (auto *kvp : order) {
         const auto &kv = *kvp;
         const int row = kv.first, nr = cam_np(row);
@@ -1020,12 +1029,46 @@ void LSA::sparse_pcg() {
       }
     }
   };
+  /* variants >= 20: the PCG's sums over cameras are blocked, per group of
+   * (variant - 18) cameras, then the groups summed (a parallel reduction's
+   * order) */
+  const int dot_group = (g_order_variant >= 20 && g_order_variant < 40) ? g_order_variant - 18 : 0;
+  /* variants >= 40: per-camera partials summed as a pairwise tree whose
+   * leaves are groups of (variant - 39) cameras (a tree reduction's order) */
+  const int tree_leaf = g_order_variant >= 40 ? g_order_variant - 39 : 0;
+  std::function<double(const std::vector<double> &, int, int)> tree_sum =
+      [&](const std::vector<double> &v, int lo, int hi) -> double {
+    if (hi - lo <= tree_leaf) {
+      double c = 0.;
+      for (int i = lo; i < hi; ++i) c += v[i];
+      return c;
+    }
+    const int mid = lo + (hi - lo) / 2;
+    return tree_sum(v, lo, mid) + tree_sum(v, mid, hi);
+  };
+  std::vector<double> part_cam(nb > 0 ? nb : 1);
   auto dot = [&](const std::vector<double> &a, const std::vector<double> &bb) {
-    double c = 0.;
+    double c = 0., g = 0.;
+    if (tree_leaf) {
+      for (int i = begini; i < nb; ++i) {
+        double cc = 0.;
+        for (int j = off[i]; j < off[i + 1]; ++j) cc += bb[j] * a[j];
+        part_cam[i] = cc;
+      }
+      return tree_sum(part_cam, begini, nb);
+    }
     for (int i = begini; i < nb; ++i) {
       double cc = 0.;
       for (int j = off[i]; j < off[i + 1]; ++j) cc += bb[j] * a[j];
-      c += cc;
+      if (dot_group) {
+        g += cc;
+        if ((i - begini + 1) % dot_group == 0 || i + 1 == nb) {
+          c += g;
+          g = 0.;
+        }
+      } else {
+        c += cc;
+      }
     }
     return c;
   };
@@ -1040,14 +1083,26 @@ void LSA::sparse_pcg() {
       alpha = 0.;
     else
       alpha = erthk / edtAdk;
-    double meandr = 0.;
+    double meandr = 0., mg = 0.;
     for (int i = begini; i < nb; ++i) {
       const int ni = cam_np(i);
+      double mi = 0.;
       for (int j = off[i]; j < off[i + 1]; ++j) {
         xk[j] += alpha * d[j];
         const double dr = alpha * Ad[j];
         r1[j] = r[j] - dr;
-        meandr += dr * dr;
+        if (dot_group || tree_leaf)
+          mi += dr * dr;
+        else
+          meandr += dr * dr;
+      }
+      if (tree_leaf) part_cam[i] = mi;
+      if (dot_group) {
+        mg += mi;
+        if ((i - begini + 1) % dot_group == 0 || i + 1 == nb) {
+          meandr += mg;
+          mg = 0.;
+        }
       }
       for (int a = 0; a < ni; ++a) {
         double s = 0.;
@@ -1055,6 +1110,7 @@ void LSA::sparse_pcg() {
         h1[off[i] + a] = s;
       }
     }
+    if (tree_leaf) meandr = tree_sum(part_cam, begini, nb);
     if (k == 0) meandr0 = meandr;
     if (meandr < meandrold) {
       xbest = xk;

@@ -122,14 +122,14 @@ __global__ void __launch_bounds__(RS_T) k_coarse_runs(DevLSA L, CoarseWork C, in
     const int2 en = L.ent[C.ent_sorted[t]];
     const int l = en.x;
     const bool tr = en.y < 0;
-    const size_t B = (size_t)(en.y & 0x7fffffff) * 81;
+    const size_t B = (size_t)(en.y & 0x7fffffff);
     const double *Pl = C.P + (size_t)l * CP;
     const int npl = L.camparv[l + 1] - L.camparv[l];
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
       const int o = lane + 32 * m, p = o / CO_M, j = o % CO_M;
       if (o < 9 * CO_M && p < npk)
-        for (int q = 0; q < npl; ++q) y[m] += blk_at(L, B + (tr ? q * 9 + p : p * 9 + q)) * Pl[q * CO_M + j];
+        for (int q = 0; q < npl; ++q) y[m] += blk_at(L, B, tr ? q * 9 + p : p * 9 + q) * Pl[q * CO_M + j];
     }
   }
 #pragma unroll

@@ -28,7 +28,7 @@ __global__ void k_dense_fill(DevLSA L, const int *coff, int n, double *A) {
   const int nr = L.camparv[r + 1] - L.camparv[r];
   const int i = e / 9, j = e % 9;
   if (i >= nr || j > i) return;
-  A[(size_t)(coff[r] + i) * n + coff[r] + j] = blk_at(L, (size_t)r * 81 + e);
+  A[(size_t)(coff[r] + i) * n + coff[r] + j] = blk_at(L, (size_t)r, e);
 }
 
 // off-diagonal blocks through the row entries: row r, column c > r,
@@ -48,7 +48,7 @@ __global__ void k_dense_fill_off(DevLSA L, const int *coff, int n, double *A) {
     const int col = en.x;
     const int nc = L.camparv[col + 1] - L.camparv[col];
     if (j >= nc) continue;
-    A[(size_t)(coff[col] + j) * n + coff[row] + i] = blk_at(L, (size_t)en.y * 81 + i * 9 + j);
+    A[(size_t)(coff[col] + j) * n + coff[row] + i] = blk_at(L, (size_t)en.y, i * 9 + j);
   }
 }
 

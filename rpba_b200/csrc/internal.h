@@ -66,16 +66,20 @@ struct DevLSA {
   int *err;            // device error word
 };
 
-// Element i of the reduced camera system's block array in either form
-// (for set-up kernels; the PCG's SpMV is compiled for each form).
-__device__ __forceinline__ double blk_at(const DevLSA &L, size_t i) {
-  return L.blocks32 ? (double)L.blocks32[i] : L.blocks[i];
+// Storage stride (elements) of one 9x9 block of the reduced camera system in
+// the FP64 and the FP32 form (row major, packed).
+constexpr int BS64 = 81, BS32 = 81;
+
+// Element e of block b of the reduced camera system in either form (for
+// set-up kernels; the PCG's SpMV is compiled for each form).
+__device__ __forceinline__ double blk_at(const DevLSA &L, size_t b, int e) {
+  return L.blocks32 ? (double)L.blocks32[b * BS32 + e] : L.blocks[b * BS64 + e];
 }
 __device__ __forceinline__ void load_block(const DevLSA &L, size_t b, double out[81]) {
   if (L.blocks32)
-    for (int e = 0; e < 81; ++e) out[e] = (double)L.blocks32[b * 81 + e];
+    for (int e = 0; e < 81; ++e) out[e] = (double)L.blocks32[b * BS32 + e];
   else
-    for (int e = 0; e < 81; ++e) out[e] = L.blocks[b * 81 + e];
+    for (int e = 0; e < 81; ++e) out[e] = L.blocks[b * BS64 + e];
 }
 
 // ---- launchers (kernels.cu)
@@ -209,14 +213,15 @@ struct PcgWork;
 void learned_pcg_setup(const DevLSA &L, const PcgWork &W, const float *weights, cudaStream_t s);
 struct CoarseWork;
 // scratch: [nimg * 81] doubles
-void learned_record(const DevLSA &L, const CoarseWork *coarse, const double *xstar, double *scratch,
+void learned_record(const DevLSA &L, const CoarseWork *coarse, const double *xstar, double *scratch, double *drs,
                     unsigned long long seed, TrainSet &T, TrainHost &H, cudaStream_t s);
 void learned_loss_grad(const TrainSet &T, const float *W, TrainBufs &B, float *loss, float *err, cudaStream_t s);
 void learned_adam(float *W, float *m, float *v, const float *grad, float lr, int t, cudaStream_t s);
 
 // ---- PCG (pcg.cu)
 struct PcgWork {
-  double *r, *r1, *d, *q, *h, *h1, *x, *xbest, *Cinv, *partials, *part;
+  double *r, *d, *q, *h, *x, *xbest, *Cinv, *partials, *part;
+  double *drs;  // [nimg * 9] 1 / sqrt of the camera blocks' diagonal entries (learned features)
   unsigned *bar;
   int *iters;
 };

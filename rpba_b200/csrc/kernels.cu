@@ -30,12 +30,14 @@ struct Store<double> {
   static __device__ __forceinline__ double *rec(const DevLSA &L) { return L.rec; }
   static __device__ __forceinline__ double *ptV(const DevLSA &L) { return L.ptV; }
   static __device__ __forceinline__ double *blocks(const DevLSA &L) { return L.blocks; }
+  static constexpr int BS = BS64;
 };
 template <>
 struct Store<float> {
   static __device__ __forceinline__ float *rec(const DevLSA &L) { return L.rec32; }
   static __device__ __forceinline__ float *ptV(const DevLSA &L) { return L.ptV32; }
   static __device__ __forceinline__ float *blocks(const DevLSA &L) { return L.blocks32; }
+  static constexpr int BS = BS32;
 };
 
 // Compensated (Kahan) accumulation for the FP32 form; plain in FP64.
@@ -417,7 +419,7 @@ __global__ void __launch_bounds__(CAM_T) k_camera(DevLSA L, double multfact1) {
     __syncthreads();
   }
   const int np = L.camparv[k + 1] - L.camparv[k];
-  T *D = Store<T>::blocks(L) + (size_t)k * 81;
+  T *D = Store<T>::blocks(L) + (size_t)k * Store<T>::BS;
   if (tid < 45) {
     double v;
     if (ei < np && ej < np) {
@@ -516,7 +518,7 @@ __global__ void k_pair(DevLSA L) {
       __syncwarp();
     }
   }
-  T *B = Store<T>::blocks(L) + (size_t)(L.nimg + wid) * 81;
+  T *B = Store<T>::blocks(L) + (size_t)(L.nimg + wid) * Store<T>::BS;
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
     const int e = lane + 32 * q;

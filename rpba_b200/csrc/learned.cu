@@ -38,16 +38,28 @@ constexpr float ALPHA = 1.0f;
 
 __device__ __forceinline__ float bf16r(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
 
+// 1 / sqrt of the diagonal entries of every camera block (0 past the
+// camera's parameter count), for the normalised couplings of the features.
+// The diagonal is damped (+1e-2), so the clamp never binds on a real entry.
+__global__ void k_diag_rsqrt(DevLSA L, double *drs) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = i / 9, a = i % 9;
+  if (k >= L.nimg) return;
+  drs[i] = (k >= L.begini && a < L.camparv[k + 1] - L.camparv[k]) ? 1. / sqrt(fmax(blk_at(L, (size_t)k, a * 10), 1e-300))
+                                                                   : 0.;
+}
+
 // Features of camera row k (>= begini) of the assembled system, computed by
 // one warp.  Lane l owns the block elements e = l, l + 32, l + 64 of every
 // off-diagonal block of the row (coalesced reads of the 81 values) and keeps
 // their normalised magnitudes in two accumulators, for the block stored as
 // (k, l) and as (l, k); the coupling sum of parameter a is then reduced over
 // the lanes in a fixed butterfly order.  Every lane returns the same f.
-__device__ void block_features(const DevLSA &L, int k, int lane, float f[NN_F]) {
+// drs: 1 / sqrt of every camera block's diagonal entries (k_diag_rsqrt).
+__device__ void block_features(const DevLSA &L, const double *__restrict__ drs, int k, int lane, float f[NN_F]) {
   const int np = L.camparv[k + 1] - L.camparv[k];
   double Dd[9];
-  for (int a = 0; a < 9; ++a) Dd[a] = blk_at(L, (size_t)k * 81 + a * 10);
+  for (int a = 0; a < 9; ++a) Dd[a] = blk_at(L, (size_t)k, a * 10);
   double ld[9], mean = 0.;
   for (int a = 0; a < 9; ++a) {
     ld[a] = a < np ? log(fmax(Dd[a], 1e-300)) : 0.;
@@ -57,34 +69,34 @@ __device__ void block_features(const DevLSA &L, int k, int lane, float f[NN_F]) 
   // per owned slot: row i, column j of the stored block, and this row's
   // diagonal entry for either orientation
   int ei[3], ej[3];
-  double dn[3], dt[3], an[3] = {0., 0., 0.}, at[3] = {0., 0., 0.};
+  double rn[3], rt[3], an[3] = {0., 0., 0.}, at[3] = {0., 0., 0.};
 #pragma unroll
   for (int m = 0; m < 3; ++m) {
     const int e = lane + 32 * m;
     ei[m] = e < 81 ? e / 9 : 9;
     ej[m] = e < 81 ? e % 9 : 9;
-    dn[m] = ei[m] < 9 ? Dd[ei[m]] : 1.;
-    dt[m] = ej[m] < 9 ? Dd[ej[m]] : 1.;
+    rn[m] = ei[m] < 9 ? drs[(size_t)k * 9 + ei[m]] : 0.;
+    rt[m] = ej[m] < 9 ? drs[(size_t)k * 9 + ej[m]] : 0.;
   }
   for (int t = L.rowoff[k]; t < L.rowoff[k + 1]; ++t) {
     const int2 en = L.ent[t];
     const int col = en.x;
     if (col == k) continue;
     const bool tr = en.y < 0;
-    const size_t B = (size_t)(en.y & 0x7fffffff) * 81, Dl = (size_t)col * 81;
+    const size_t B = (size_t)(en.y & 0x7fffffff);
+    const double *rc = drs + (size_t)col * 9;
     const int nc = L.camparv[col + 1] - L.camparv[col];
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
       const int i = ei[m], j = ej[m];
       if (i >= 9) continue;
       // stored (k, col): element (i, j) couples parameter i of k to j of col;
-      // stored (col, k): it couples parameter j of k to i of col
+      // stored (col, k): it couples parameter j of k to i of col; both
+      // normalised by the two diagonal entries, |S_ij| / sqrt(S_ii S_jj)
       if (!tr) {
-        if (i < np && j < nc)
-          an[m] += fabs(blk_at(L, B + i * 9 + j)) / sqrt(fmax(dn[m] * blk_at(L, Dl + j * 10), 1e-300));
+        if (i < np && j < nc) an[m] += fabs(blk_at(L, B, i * 9 + j)) * rn[m] * __ldg(rc + j);
       } else {
-        if (j < np && i < nc)
-          at[m] += fabs(blk_at(L, B + i * 9 + j)) / sqrt(fmax(dt[m] * blk_at(L, Dl + i * 10), 1e-300));
+        if (j < np && i < nc) at[m] += fabs(blk_at(L, B, i * 9 + j)) * rt[m] * __ldg(rc + i);
       }
     }
   }
@@ -158,7 +170,7 @@ __global__ void k_learned_setup(DevLSA L, PcgWork Wk, const float *weights) {
   if (k >= L.nimg) return;
   double *C = Wk.Cinv + (size_t)k * 81;
   const size_t o = (size_t)k * 9;
-  if (lane < 9) Wk.d[o + lane] = Wk.r1[o + lane] = 0.;
+  if (lane < 9) Wk.d[o + lane] = 0.;
   if (k < L.begini) {
     if (lane < 9) Wk.r[o + lane] = Wk.h[o + lane] = Wk.x[o + lane] = Wk.xbest[o + lane] = 0.;
     return;
@@ -174,7 +186,7 @@ __global__ void k_learned_setup(DevLSA L, PcgWork Wk, const float *weights) {
   for (int a = 0; a < NN_O; ++a) sc[a] = 1.f;
   if (weights) {
     float f[NN_F];
-    block_features(L, k, lane, f);
+    block_features(L, Wk.drs, k, lane, f);
     mlp_forward_warp(Ws, f, lane, sc);
   }
   __syncwarp();
@@ -394,12 +406,12 @@ __global__ void k_adam(float *W, float *m, float *v, const float *grad, float lr
 // scaled block inverse (LU by lane 0 into the FP64 scratch Si, then scaled
 // by lanes 0..8), right-hand sides and the scaled solution.
 __global__ void k_rec_rows(DevLSA L, TrainSet T, int row0, int sys, const double *xstar, unsigned long long seed,
-                           double *Si) {
+                           double *Si, const double *drs) {
   const int k = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) + L.begini, lane = threadIdx.x & 31;
   if (k >= L.nimg) return;
   const int r = row0 + (k - L.begini);
   float f[NN_F];
-  block_features(L, k, lane, f);
+  block_features(L, drs, k, lane, f);
   const int np = L.camparv[k + 1] - L.camparv[k];
   const double *D = L.blocks + (size_t)k * 81;
   double *Sk = Si + (size_t)k * 81;
@@ -437,16 +449,16 @@ __global__ void k_rec_blocks(DevLSA L, TrainSet T, int blk0, const int2 *rc, int
   size_t src;
   if (b < nd) {
     r = c = (int)b + L.begini;
-    src = (size_t)r * 81;
+    src = (size_t)r;
   } else {
     r = rc[b - nd].x;
     c = rc[b - nd].y;
-    src = (size_t)(L.nimg + (b - nd)) * 81;
+    src = (size_t)(L.nimg + (b - nd));
   }
   const int nr = L.camparv[r + 1] - L.camparv[r], nc = L.camparv[c + 1] - L.camparv[c];
   float v = 0.f;
   if (i < nr && j < nc)
-    v = (float)(blk_at(L, src + e) / sqrt(blk_at(L, (size_t)r * 81 + i * 10) * blk_at(L, (size_t)c * 81 + j * 10)));
+    v = (float)(blk_at(L, src, e) / sqrt(blk_at(L, (size_t)r, i * 10) * blk_at(L, (size_t)c, j * 10)));
   T.blocks[(size_t)(blk0 + b) * 81 + e] = v;
 }
 
@@ -458,7 +470,7 @@ __global__ void k_rec_bvec(DevLSA L, TrainSet T, int row0, int pr, double *vb) {
   double v = 0.;
   if (k >= L.begini && a < L.camparv[k + 1] - L.camparv[k])
     v = (double)T.b[((size_t)pr * T.rows_cap + row0 + (k - L.begini)) * 9 + a] *
-        sqrt(blk_at(L, (size_t)k * 81 + a * 10));
+        sqrt(blk_at(L, (size_t)k, a * 10));
   vb[i] = v;
 }
 
@@ -469,16 +481,17 @@ __global__ void k_rec_uc(DevLSA L, TrainSet T, int row0, int pr, const double *v
   if (k >= L.nimg) return;
   const int np = L.camparv[k + 1] - L.camparv[k];
   T.uc[((size_t)pr * T.rows_cap + row0 + (k - L.begini)) * 9 + a] =
-      a < np ? (float)(vz[i] * sqrt(blk_at(L, (size_t)k * 81 + a * 10))) : 0.f;
+      a < np ? (float)(vz[i] * sqrt(blk_at(L, (size_t)k, a * 10))) : 0.f;
 }
 
 }  // namespace
 
 void learned_pcg_setup(const DevLSA &L, const PcgWork &W, const float *weights, cudaStream_t s) {
+  if (weights) k_diag_rsqrt<<<(L.nimg * 9 + 255) / 256, 256, 0, s>>>(L, W.drs);
   k_learned_setup<<<(L.nimg + 7) / 8, 256, 0, s>>>(L, W, weights);
 }
 
-void learned_record(const DevLSA &L, const CoarseWork *coarse, const double *xstar, double *scratch,
+void learned_record(const DevLSA &L, const CoarseWork *coarse, const double *xstar, double *scratch, double *drs,
                     unsigned long long seed, TrainSet &T, TrainHost &H, cudaStream_t s) {
   if (!L.blocks) return;  // systems are recorded in the FP64 form only
   const int nimg = L.nimg, nd = nimg - L.begini, nb = L.nboff;
@@ -523,7 +536,8 @@ void learned_record(const DevLSA &L, const CoarseWork *coarse, const double *xst
   RPBA_CUDA_CHECK(cudaMemcpyAsync(T.rowoff + row0, new_off.data(), sizeof(int) * (nd + 1), cudaMemcpyHostToDevice, s));
   RPBA_CUDA_CHECK(cudaMemcpyAsync(T.ent + H.ents, new_ent.data(), sizeof(int2) * new_ent.size(), cudaMemcpyHostToDevice, s));
   RPBA_CUDA_CHECK(cudaMemcpyAsync(H.rc, rc.data(), sizeof(int2) * std::max(nb, 1), cudaMemcpyHostToDevice, s));
-  k_rec_rows<<<(nd + 7) / 8, 256, 0, s>>>(L, T, row0, T.systems, xstar, seed, scratch);
+  k_diag_rsqrt<<<(nimg * 9 + 255) / 256, 256, 0, s>>>(L, drs);
+  k_rec_rows<<<(nd + 7) / 8, 256, 0, s>>>(L, T, row0, T.systems, xstar, seed, scratch, drs);
   const long long nthreads = (long long)(nd + nb) * 81;
   k_rec_blocks<<<(int)((nthreads + 255) / 256), 256, 0, s>>>(L, T, blk0, H.rc, nb);
   if (T.uc) {

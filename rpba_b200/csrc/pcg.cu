@@ -20,8 +20,19 @@ namespace rpba {
 
 namespace {
 
-constexpr int PCG_T = 1024;
-constexpr int PCG_W = PCG_T / 32;
+// Threads per CTA of the persistent kernel, per block storage type: 1024 in
+// the FP64 form (32 warps, two work items in flight each through shared
+// memory), 768 in the FP32 form (24 warps whose three-slot register pipeline
+// needs 80 registers a thread).
+template <class BT>
+constexpr int pcg_threads() {
+  return sizeof(BT) == 8 ? 1024 : 768;
+}
+template <class BT>
+constexpr int pcg_warps() {
+  return pcg_threads<BT>() / 32;
+}
+
 
 struct PcgArgs {
   const void *blocks;  // BT[(nimg + nboff) * 81]
@@ -49,7 +60,7 @@ struct PcgArgs {
 };
 
 // Deterministic CTA sum of up to three values; valid in every thread.
-template <int N>
+template <int N, int W>
 __device__ __forceinline__ void cta_sum(double (&v)[N], double (*sh)[4]) {
 #pragma unroll
   for (int j = 0; j < N; ++j)
@@ -63,21 +74,21 @@ __device__ __forceinline__ void cta_sum(double (&v)[N], double (*sh)[4]) {
   if (warp == 0) {
 #pragma unroll
     for (int j = 0; j < N; ++j) {
-      double t = lane < PCG_W ? sh[lane][j] : 0.;
+      double t = lane < W ? sh[lane][j] : 0.;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-      if (lane == 0) sh[PCG_W][j] = t;
+      if (lane == 0) sh[W][j] = t;
     }
   }
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < N; ++j) v[j] = sh[PCG_W][j];
+  for (int j = 0; j < N; ++j) v[j] = sh[W][j];
   __syncthreads();
 }
 
 // Sum of the per-CTA partials (stride 4) in a fixed order; every CTA gets
 // the same values.
-template <int N>
+template <int N, int W>
 __device__ __forceinline__ void grid_sum(const double *red, int G, double (&v)[N], double (*sh)[4]) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (warp == 0) {
@@ -87,12 +98,12 @@ __device__ __forceinline__ void grid_sum(const double *red, int G, double (&v)[N
       for (int i = lane; i < G; i += 32) t += __ldcg(red + 4 * i + j);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-      if (lane == 0) sh[PCG_W][j] = t;
+      if (lane == 0) sh[W][j] = t;
     }
   }
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < N; ++j) v[j] = sh[PCG_W][j];
+  for (int j = 0; j < N; ++j) v[j] = sh[W][j];
   __syncthreads();
 }
 
@@ -117,9 +128,11 @@ __device__ __forceinline__ void cp_async_wait() {
 // and its d^k values (column and row) are loaded into registers, while the
 // current item is multiplied.
 constexpr int P1_ELEMS = 3 * 81;
+// Dynamic shared memory: the FP64 form's stages; the FP32 form keeps its
+// pipeline in registers
 template <class BT>
 constexpr size_t pcg_smem_bytes() {
-  return sizeof(BT) == 8 ? sizeof(BT) * (size_t)PCG_W * 2 * P1_ELEMS : 0;
+  return sizeof(BT) == 8 ? sizeof(BT) * (size_t)pcg_warps<BT>() * 2 * P1_ELEMS : 0;
 }
 struct P1Item {
   int it, row, ne;  // item, its row, entries (0 past the end)
@@ -169,6 +182,57 @@ __device__ __forceinline__ void p1_issue(const PcgArgs &A, int it, BT *stage, co
   cp_async_commit();
 }
 
+// First item of warp w's chunk in the FP32 form's phase 1 (the items are
+// split into nwarps contiguous chunks of near-equal size).
+__device__ __forceinline__ int chunk_start(long long w, int nitems, int nwarps) {
+  return (int)(w * nitems / nwarps);
+}
+
+// q of one row (valid in lanes < 9) from the phase-1 partials.  FP32 form:
+// one partial per (row, chunk) segment, stored at the segment's first item:
+// the row's first item and every chunk start inside the row, summed in item
+// order.  FP64 form: one partial per item, the three 9-lane groups taking
+// every third item (four loads in flight), in a fixed order.
+template <class BT>
+__device__ __forceinline__ double row_q(const PcgArgs &A, int row, int nwarps, int lane, int grp, int rr) {
+  const int t0 = A.row_item_off[row], t1 = A.row_item_off[row + 1];
+  if constexpr (sizeof(BT) == 4) {
+    double q = 0.;
+    if (lane < 9 && t0 < t1) {
+      q = __ldcg(A.part + (size_t)t0 * 9 + lane);
+      // smallest w whose chunk starts after t0
+      long long w = ((long long)(t0 + 1) * nwarps + A.nitems - 1) / A.nitems;
+      int prev = t0;
+      for (; w < nwarps; ++w) {
+        const int st = chunk_start(w, A.nitems, nwarps);
+        if (st >= t1) break;
+        if (st != prev) {
+          q += __ldcg(A.part + (size_t)st * 9 + lane);
+          prev = st;
+        }
+      }
+    }
+    return q;
+  } else {
+    double qg = 0.;
+    if (lane < 27) {
+      double q0 = 0., q1 = 0., q2 = 0., q3 = 0.;
+      int t = t0 + grp;
+      for (; t + 9 < t1; t += 12) {
+        q0 += __ldcg(A.part + (size_t)t * 9 + rr);
+        q1 += __ldcg(A.part + (size_t)(t + 3) * 9 + rr);
+        q2 += __ldcg(A.part + (size_t)(t + 6) * 9 + rr);
+        q3 += __ldcg(A.part + (size_t)(t + 9) * 9 + rr);
+      }
+      for (; t < t1; t += 3) q0 += __ldcg(A.part + (size_t)t * 9 + rr);
+      qg = (q0 + q1) + (q2 + q3);
+    }
+    const double qa = __shfl_down_sync(0xffffffffu, qg, 9);
+    const double qb = __shfl_down_sync(0xffffffffu, qg, 18);
+    return qg + qa + qb;
+  }
+}
+
 // Iteration k (two grid barriers):
 //  phase 1  q-partials of A d^k per work item (<= 3 blocks of one row), with
 //           d^k = h^k + beta^(k-1) d^(k-1) formed on the fly; partial d^T q
@@ -183,7 +247,8 @@ __device__ __forceinline__ void p1_issue(const PcgArgs &A, int it, BT *stage, co
 // BT: the storage type of the reduced camera system's blocks (double, or
 // float in the mixed-precision form); vectors and sums are FP64 either way.
 template <bool CO, class BT>
-__global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
+__global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
+  constexpr int PCG_T = pcg_threads<BT>(), PCG_W = pcg_warps<BT>();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gwarp = blockIdx.x * PCG_W + warp, nwarps = gridDim.x * PCG_W;
   const int grp = lane / 9, rr = lane % 9, gbase = grp * 9;
@@ -200,14 +265,14 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
         const size_t i = (size_t)row * 9 + lane;
         v[0] += A.r[i] * A.h[i];
       }
-    cta_sum<1>(v, sh);
+    cta_sum<1, PCG_W>(v, sh);
     if (threadIdx.x == 0) A.red2[4 * blockIdx.x] = v[0];
   }
   if (!grid_barrier(A.bar, G, A.err)) return;
   double erthk;
   {
     double v[1];
-    grid_sum<1>(A.red2, G, v, sh);
+    grid_sum<1, PCG_W>(A.red2, G, v, sh);
     erthk = v[0];
   }
   double meandrold = 1.e50, meandr0 = 1.e50, beta_prev = 0.;
@@ -252,61 +317,107 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
         __syncwarp();
       }
     } else {
-      // FP32 blocks: direct loads (4-byte asynchronous copies cost more
-      // instructions than the latency they hide); item metadata and the
-      // next block entry are prefetched
-      int it = gwarp;
-      int4 meta = it < A.nitems ? A.item_meta[it] : make_int4(0, 0, 0, 0);
-      int2 en_next = make_int2(0, 0);
-      if (it < A.nitems && lane < 27 && meta.y + grp < meta.z) en_next = A.ent[meta.y + grp];
-      for (; it < A.nitems; it += nwarps) {
-        const int row = meta.x;
-        const int e = meta.y + grp;
-        const bool act = lane < 27 && e < meta.z;
-        const int2 en = en_next;
-        const int itn = it + nwarps;
-        if (itn < A.nitems) {
-          meta = A.item_meta[itn];
-          if (lane < 27 && meta.y + grp < meta.z) en_next = A.ent[meta.y + grp];
-        }
-        double acc = 0.;
-        int col = 0, blk = 0;
-        bool tr = false;
-        if (act) {
-          col = en.x;
-          blk = en.y & 0x7fffffff;
-          tr = en.y < 0;
-        }
-        // lane (gbase + c) forms d^k[col][c]; the group gathers it by shuffles
-        double dc = 0.;
-        if (act) {
-          const size_t j = (size_t)col * 9 + rr;
-          dc = __ldcg(A.h + j) + beta_prev * __ldcg(dprev + j);
-        }
-        const BT *B = (const BT *)A.blocks + (size_t)blk * 81;
+      // FP32 blocks: each warp walks one contiguous chunk of the work items
+      // (row order) with a three-slot register pipeline: the blocks of item
+      // t + 2 (and the d^k entries they multiply) are loaded while item t is
+      // multiplied, the entries of item t + 3 one step earlier; entry
+      // positions follow from the walk (row offsets), so no load waits on
+      // another.  Each block row is formed in FP32 (FP32 blocks times d^k
+      // rounded to FP32) and the row sums are carried in FP64; products are
+      // summed per row in registers and written once per (row, chunk)
+      // segment, at the segment's first item.
+      const int c0 = chunk_start(gwarp, A.nitems, nwarps);
+      const int c1 = chunk_start(gwarp + 1, A.nitems, nwarps);
+      if (c0 < c1) {
+        const BT *blocks = (const BT *)A.blocks;
+        const int4 m0 = A.item_meta[c0];
+        int wrow = m0.x, we = m0.y, wend = __ldg(A.rowoff + m0.x + 1);
+        int rowN = 0;
+        int2 enN = make_int2(-1, 0);
+        // entries of the walk's next item (lanes < 27, col -1 past the row)
+        auto ent_next = [&]() {
+          rowN = wrow;
+          enN = make_int2(-1, 0);
+          if (lane < 27 && we + grp < wend) enN = __ldg(A.ent + we + grp);
+          we += 3;
+          if (we >= wend) {
+            we = wend;
+            if (++wrow < A.row1) wend = __ldg(A.rowoff + wrow + 1);
+          }
+        };
+        // loads of the item whose entries are in enN into a slot, then the
+        // next entries (items past the chunk load nothing)
+        auto slot_load = [&](int t, float (&b)[9], float &dc, int &row) {
+          row = rowN;
+          dc = 0.f;
+          const int2 en = enN;
+          if (t < c1 && en.x >= 0) {
+            // row rr of the block, or column rr of a transposed one
+            const bool tr = en.y < 0;
+            const BT *B = blocks + (size_t)(en.y & 0x7fffffff) * BS32 + (tr ? rr : rr * 9);
+            const int sc = tr ? 9 : 1;
 #pragma unroll
-        for (int c = 0; c < 9; ++c) {
-          const double xc = __shfl_sync(0xffffffffu, dc, (lane < 27 ? gbase : 0) + c);
-          if (act) acc += __ldg(B + (tr ? c * 9 + rr : rr * 9 + c)) * xc;
+            for (int c = 0; c < 9; ++c) b[c] = __ldg(B + c * sc);
+            const size_t j = (size_t)en.x * 9 + rr;
+            dc = (float)(__ldcg(A.h + j) + beta_prev * __ldcg(dprev + j));
+          } else {
+#pragma unroll
+            for (int c = 0; c < 9; ++c) b[c] = 0.f;
+          }
+          if (t + 1 < c1) ent_next();
+        };
+        auto dk_of = [&](int row) {
+          return lane < 9 ? __ldcg(A.h + (size_t)row * 9 + lane) + beta_prev * __ldcg(dprev + (size_t)row * 9 + lane)
+                          : 0.;
+        };
+        float bA[9], bB[9], bC[9];
+        float dA, dB, dC;
+        int rA, rB, rC;
+        ent_next();
+        slot_load(c0, bA, dA, rA);
+        slot_load(c0 + 1, bB, dB, rB);
+        int seg = c0, segrow = rA;
+        double racc = 0., dseg = dk_of(segrow);
+        // item t from slot (b, d, r); the slot `nb` receives item t + 2
+        auto step = [&](int t, const float (&b)[9], float d, int r, float (&nb)[9], float &nd, int &nr) {
+          slot_load(t + 2, nb, nd, nr);
+          float acc = 0.f;
+#pragma unroll
+          for (int c = 0; c < 9; ++c) acc = fmaf(b[c], __shfl_sync(0xffffffffu, d, (lane < 27 ? gbase : 0) + c), acc);
+          const float a1 = __shfl_down_sync(0xffffffffu, acc, 9);
+          const float a2 = __shfl_down_sync(0xffffffffu, acc, 18);
+          if (r != segrow) {
+            if (lane < 9) {
+              A.part[(size_t)seg * 9 + lane] = racc;
+              pdq[0] += dseg * racc;
+            }
+            seg = t;
+            segrow = r;
+            racc = 0.;
+            dseg = dk_of(r);
+          }
+          if (lane < 9) racc += (double)acc + (double)a1 + (double)a2;
+        };
+        for (int t = c0; t < c1; t += 3) {
+          step(t, bA, dA, rA, bC, dC, rC);
+          if (t + 1 >= c1) break;
+          step(t + 1, bB, dB, rB, bA, dA, rA);
+          if (t + 2 >= c1) break;
+          step(t + 2, bC, dC, rC, bB, dB, rB);
         }
-        const double a1 = __shfl_down_sync(0xffffffffu, acc, 9);
-        const double a2 = __shfl_down_sync(0xffffffffu, acc, 18);
         if (lane < 9) {
-          const double p = acc + a1 + a2;
-          A.part[(size_t)it * 9 + lane] = p;
-          const size_t i = (size_t)row * 9 + lane;
-          const double dk = __ldcg(A.h + i) + beta_prev * __ldcg(dprev + i);
-          pdq[0] += dk * p;
+          A.part[(size_t)seg * 9 + lane] = racc;
+          pdq[0] += dseg * racc;
         }
       }
     }
-    cta_sum<1>(pdq, sh);
+    cta_sum<1, PCG_W>(pdq, sh);
     if (threadIdx.x == 0) A.red1[4 * blockIdx.x] = pdq[0];
     if (!grid_barrier(A.bar, G, A.err)) return;
     double edtAdk;
     {
       double v[1];
-      grid_sum<1>(A.red1, G, v, sh);
+      grid_sum<1, PCG_W>(A.red1, G, v, sh);
       edtAdk = v[0];
     }
     double alpha;
@@ -320,26 +431,8 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
       for (int row = A.row0 + gwarp; row < A.row1; row += nwarps) {
         const size_t i = (size_t)row * 9 + (lane < 9 ? lane : 0);
         double r1v = 0., hv = 0.;
-        // q = sum of the row's item partials: the three 9-lane groups take
-        // every third item, four independent loads in flight, fixed order
-        double qg = 0.;
-        if (lane < 27) {
-          const int t0 = A.row_item_off[row], t1 = A.row_item_off[row + 1];
-          double q0 = 0., q1 = 0., q2 = 0., q3 = 0.;
-          int t = t0 + grp;
-          for (; t + 9 < t1; t += 12) {
-            q0 += __ldcg(A.part + (size_t)t * 9 + rr);
-            q1 += __ldcg(A.part + (size_t)(t + 3) * 9 + rr);
-            q2 += __ldcg(A.part + (size_t)(t + 6) * 9 + rr);
-            q3 += __ldcg(A.part + (size_t)(t + 9) * 9 + rr);
-          }
-          for (; t < t1; t += 3) q0 += __ldcg(A.part + (size_t)t * 9 + rr);
-          qg = (q0 + q1) + (q2 + q3);
-        }
-        const double qa = __shfl_down_sync(0xffffffffu, qg, 9);
-        const double qb = __shfl_down_sync(0xffffffffu, qg, 18);
+        const double q = row_q<BT>(A, row, nwarps, lane, grp, rr);
         if (lane < 9) {
-          const double q = qg + qa + qb;
           hv = __ldcg(A.h + i);
           const double dk = hv + beta_prev * __ldcg(dprev + i);
           dcur[i] = dk;
@@ -372,24 +465,8 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
           const int row = A.agg_rows[t];
           const size_t i = (size_t)row * 9 + (lane < 9 ? lane : 0);
           double r1v = 0.;
-          double qg = 0.;
-          if (lane < 27) {
-            const int u0 = A.row_item_off[row], u1 = A.row_item_off[row + 1];
-            double q0 = 0., q1 = 0., q2 = 0., q3 = 0.;
-            int u = u0 + grp;
-            for (; u + 9 < u1; u += 12) {
-              q0 += __ldcg(A.part + (size_t)u * 9 + rr);
-              q1 += __ldcg(A.part + (size_t)(u + 3) * 9 + rr);
-              q2 += __ldcg(A.part + (size_t)(u + 6) * 9 + rr);
-              q3 += __ldcg(A.part + (size_t)(u + 9) * 9 + rr);
-            }
-            for (; u < u1; u += 3) q0 += __ldcg(A.part + (size_t)u * 9 + rr);
-            qg = (q0 + q1) + (q2 + q3);
-          }
-          const double qa = __shfl_down_sync(0xffffffffu, qg, 9);
-          const double qb = __shfl_down_sync(0xffffffffu, qg, 18);
+          const double q = row_q<BT>(A, row, nwarps, lane, grp, rr);
           if (lane < 9) {
-            const double q = qg + qa + qb;
             const double hv = __ldcg(A.h + i);
             const double dk = hv + beta_prev * __ldcg(dprev + i);
             dcur[i] = dk;
@@ -462,7 +539,7 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
         __syncthreads();
       }
     }
-    cta_sum<3>(p2, sh);
+    cta_sum<3, PCG_W>(p2, sh);
     if (threadIdx.x == 0) {
       A.red2[4 * blockIdx.x] = p2[0];
       A.red2[4 * blockIdx.x + 1] = p2[1];
@@ -470,7 +547,7 @@ __global__ void __launch_bounds__(PCG_T, 1) k_pcg(PcgArgs A) {
     }
     if (!grid_barrier(A.bar, G, A.err)) return;
     double g3[3];
-    grid_sum<3>(A.red2, G, g3, sh);
+    grid_sum<3, PCG_W>(A.red2, G, g3, sh);
     const double meandr = g3[0], er1th1 = g3[1];
     if (k == 0) meandr0 = meandr;
     // mode 0 keeps the iterate with the smallest increment (the reference's
@@ -507,7 +584,7 @@ __global__ void k_pcg_setup(DevLSA L, PcgWork W) {
   if (k >= L.nimg) return;
   double *C = W.Cinv + (size_t)k * 81;
   const size_t o = (size_t)k * 9;
-  for (int a = 0; a < 9; ++a) W.d[o + a] = W.r1[o + a] = 0.;
+  for (int a = 0; a < 9; ++a) W.d[o + a] = 0.;
   if (k < L.begini) {
     for (int a = 0; a < 9; ++a) W.r[o + a] = W.h[o + a] = W.x[o + a] = W.xbest[o + a] = 0.;
     return;
@@ -545,12 +622,16 @@ int pcg_max_grid(int device) {
   int nsm = 0, per = 0, per2 = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
   pcg_set_smem();
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<false, double>, PCG_T, pcg_smem_bytes<double>());
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true, double>, PCG_T, pcg_smem_bytes<double>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_pcg<false, double>, pcg_threads<double>(),
+                                                pcg_smem_bytes<double>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true, double>, pcg_threads<double>(),
+                                                pcg_smem_bytes<double>());
   per = std::min(per, per2);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<false, float>, PCG_T, pcg_smem_bytes<float>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<false, float>, pcg_threads<float>(),
+                                                pcg_smem_bytes<float>());
   per = std::min(per, per2);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true, float>, PCG_T, pcg_smem_bytes<float>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true, float>, pcg_threads<float>(),
+                                                pcg_smem_bytes<float>());
   per = std::min(per, per2);
   if (per < 1) per = 1;
   return nsm * per;
@@ -575,7 +656,8 @@ int pcg_iterate(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStre
   const bool co = coarse && coarse->nagg > 0;
   const int nrows = L.nimg - L.begini;
   if (nrows <= 0) return 0;
-  int g = (L.nitems + PCG_W - 1) / PCG_W;
+  const int wpc = L.blocks32 ? pcg_warps<float>() : pcg_warps<double>();
+  int g = (L.nitems + wpc - 1) / wpc;
   if (g > grid) g = grid;
   if (g < 1) g = 1;
   PcgArgs A;
@@ -620,7 +702,8 @@ int pcg_iterate(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStre
     fn = co ? (const void *)k_pcg<true, double> : (const void *)k_pcg<false, double>;
   const size_t smem = L.blocks32 ? pcg_smem_bytes<float>() : pcg_smem_bytes<double>();
   pcg_set_smem();
-  RPBA_CUDA_CHECK(cudaLaunchCooperativeKernel(fn, dim3(g), dim3(PCG_T), args, smem, s));
+  const int nthreads = L.blocks32 ? pcg_threads<float>() : pcg_threads<double>();
+  RPBA_CUDA_CHECK(cudaLaunchCooperativeKernel(fn, dim3(g), dim3(nthreads), args, smem, s));
   return 0;
 }
 

@@ -280,9 +280,9 @@ struct rpba_handle {
       }
     }
     if (mixed)
-      L.blocks32 = dalloc<float>((size_t)(nimg + cap) * 81, owned);
+      L.blocks32 = dalloc<float>((size_t)(nimg + cap) * BS32, owned);
     else
-      L.blocks = dalloc<double>((size_t)(nimg + cap) * 81, owned);
+      L.blocks = dalloc<double>((size_t)(nimg + cap) * BS64, owned);
     S.ent = dalloc<int2>((size_t)nimg + 2 * (size_t)cap, owned);
     // SpMV work items: at most ceil(entries / 3) per row
     const size_t items = (size_t)nimg + ((size_t)nimg + 2 * (size_t)cap) / 3 + 1;
@@ -674,19 +674,16 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   PcgWork &W = H->W;
   const size_t nv = 9 * (size_t)n;
   W.r = dalloc<double>(nv, own);
-  W.r1 = dalloc<double>(nv, own);
   W.d = dalloc<double>(nv, own);
   W.q = dalloc<double>(nv, own);
   W.h = dalloc<double>(nv, own);
-  W.h1 = dalloc<double>(nv, own);
+  W.drs = dalloc<double>(nv, own);
   W.x = dalloc<double>(nv, own);
   W.xbest = dalloc<double>(nv, own);
   W.Cinv = dalloc<double>(81 * (size_t)n, own);
   W.partials = dalloc<double>(8 * (size_t)H->pcg_grid, own);
   W.bar = dalloc<unsigned>(2, own);
   W.iters = dalloc<int>(2, own);
-  RPBA_CUDA_CHECK(cudaMemsetAsync(W.r1, 0, sizeof(double) * nv, H->s));
-  RPBA_CUDA_CHECK(cudaMemsetAsync(W.h1, 0, sizeof(double) * nv, H->s));
   RPBA_CUDA_CHECK(cudaMemsetAsync(W.q, 0, sizeof(double) * nv, H->s));
   RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
   return RPBA_OK;
@@ -862,7 +859,7 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
   if (rec_T) {
     const CoarseWork *cw = ensure_coarse();
     if (cw) coarse_setup(L, CW, structure_version, s);
-    learned_record(L, cw, W.xbest, W.Cinv, rec_seed + 104729ull * (unsigned long long)rep.linear_solves, *rec_T,
+    learned_record(L, cw, W.xbest, W.Cinv, W.drs, rec_seed + 104729ull * (unsigned long long)rep.linear_solves, *rec_T,
                    *rec_H, s);
   }
   PROF("backsub", 1, launch_backsub(L, W.xbest, s));

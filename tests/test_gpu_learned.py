@@ -116,6 +116,32 @@ def test_recorded_systems_are_consistent(city_blocks):
         assert rel < 1e-2, (s, rel)
 
 
+def test_recorded_coupling_features(city_blocks):
+    """The network's coupling features, recorded with the training set, are
+    log1p of the row sums of |S~| over each row's off-diagonal blocks (S~
+    the diagonally scaled system), recomputed here in numpy from the
+    recorded blocks; the degree feature is log1p(off-diagonal blocks) / 4."""
+    import rpba_b200 as rb
+    train, _ = city_blocks
+    ts = rb.record_systems(train[:1], probes=1)
+    R = ts["rows"]
+    blocks = ts["blocks"].astype(np.float64).reshape(-1, 9, 9)
+    blk = ts["ent_blk"].astype(np.int64) & 0xFFFFFFFF
+    tr = (blk & 0x80000000) != 0
+    B = blocks[blk & 0x7FFFFFFF]
+    B = np.where(tr[:, None, None], B.transpose(0, 2, 1), B)
+    rows = np.repeat(np.arange(R), np.diff(ts["rowoff"]))
+    off = ts["ent_col"] != rows
+    cpl = np.zeros((R, 9))
+    np.add.at(cpl, rows[off], np.abs(B[off]).sum(axis=2))
+    mask = np.arange(9)[None, :] < ts["np"][:, None]
+    want = np.where(mask, np.log1p(cpl), 0.0)
+    got = ts["features"][:, 9:18].astype(np.float64)
+    assert np.abs(got - want).max() <= 1e-5 * max(1.0, np.abs(want).max()), np.abs(got - want).max()
+    deg = np.bincount(rows[off], minlength=R)
+    assert np.allclose(ts["features"][:, 18], np.log1p(deg) / 4.0, rtol=1e-6, atol=1e-7)
+
+
 def test_learned_gradient_on_recorded_systems(city_blocks):
     """GPU loss and gradient against autograd on real recorded systems,
     coarse part included."""

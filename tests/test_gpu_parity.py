@@ -22,17 +22,26 @@ def _run_pair(oracle_mod, blk, **kw):
     return (st_o, blk_o, rep_o, log_o), (st_g, blk_g, rep_g, log_g)
 
 
-def _self_sensitivity(oracle_mod, blk, o, **kw):
-    """How far the oracle moves when only the SpMV summation order changes
-    (two reorderings, the larger deviation): the reference's inexact PCG
-    (loose 1e5 stop rule) amplifies roundoff, so no reordered implementation
-    can agree with it more closely than this.  Returns (cost, parameters,
-    printed sigma0) relative deviations."""
+def _self_sensitivity(oracle_mod, blk, o, n_orders=8, n_perturb=24, **kw):
+    """How far the oracle's own outcome moves under roundoff-level changes
+    (the largest deviation from its base run): the SpMV summation order
+    (variants 1..n_orders) and a one-ulp change of five observations
+    (n_perturb seeds).  The reference's inexact PCG (loose 1e5 stop rule)
+    amplifies roundoff on ill-conditioned scenes, and its outcome is not
+    even unimodal: on the street scene the final sigma0 is about 0.5432 or
+    0.5462, and one-ulp input changes reach both.  No implementation with
+    another summation order can be held closer to the oracle than this.
+    Returns (cost, parameters, printed sigma0) relative deviations."""
     import rpba_b200 as rb
     _, blk_o, rep_o, log_o = o
     cost, params, sigma = 0.0, None, 0.0
-    for variant in (1, 2):
-        st_v, blk_v, rep_v, log_v = oracle_mod.calc_plsa_variant(blk, rb.make_options(**kw), variant=variant)
+    runs = [oracle_mod.calc_plsa_variant(blk, rb.make_options(**kw), variant=v) for v in range(1, n_orders + 1)]
+    for seed in range(n_perturb):
+        b = blk.copy()
+        slots = b.pt_obs_slot[np.random.default_rng(seed).choice(b.n_obs, 5, replace=False)]
+        b.xg[slots, 0] = np.nextafter(b.xg[slots, 0], np.float32(np.inf))
+        runs.append(oracle_mod.calc_plsa(b, rb.make_options(**kw)))
+    for st_v, blk_v, rep_v, log_v in runs:
         cost = max(cost, abs(rep_v["cost"] - rep_o["cost"]) / abs(rep_o["cost"]))
         pe = param_errors(blk_v, blk_o)
         params = pe if params is None else {k: max(params[k], pe[k]) for k in pe}
@@ -42,15 +51,15 @@ def _self_sensitivity(oracle_mod, blk, o, **kw):
 
 def _check(o, g, sens=None):
     """Parity within the contract's bars (cost 1e-8, parameters 1e-6), or
-    within 4x the oracle's own summation-order sensitivity where that is
-    larger (``sens``, PCG mode on ill-conditioned scenes)."""
+    within 1.5x the oracle's own roundoff sensitivity where that is larger
+    (``sens``, PCG mode on ill-conditioned scenes)."""
     st_o, blk_o, rep_o, log_o = o
     st_g, blk_g, rep_g, log_g = g
     assert st_g == st_o, (st_g, st_o, log_g, log_o)
     # identical decisions: the integer fields of every log line (redundancy,
     # observations, unknowns, IT, ITT) match exactly; the printed sigma0
     # values are float sums and may differ in the last printed digit.
-    sigma_tol = SIGMA_RTOL if sens is None else max(SIGMA_RTOL, 4 * sens[2])
+    sigma_tol = SIGMA_RTOL if sens is None else max(SIGMA_RTOL, 1.5 * sens[2])
     assert same_log(log_g, log_o, sigma_tol), f"\nGPU:\n{log_g}\nORACLE:\n{log_o}"
     for k in ("linear_solves", "obs_deleted", "points_deleted", "points_used", "passes_done"):
         assert rep_g[k] == rep_o[k], (k, rep_g[k], rep_o[k])
@@ -59,9 +68,9 @@ def _check(o, g, sens=None):
     print(f"cost rel {cost_rel:.3e} params {errs}")
     cost_tol, ptol = COST_RTOL, {k: PARAM_RTOL for k in errs}
     if sens is not None:
-        cost_tol = max(cost_tol, 4 * sens[0])
-        ptol = {k: max(PARAM_RTOL, 4 * sens[1][k]) for k in errs}
-        print(f"  oracle self-sensitivity: cost {sens[0]:.3e} params {sens[1]}")
+        cost_tol = max(cost_tol, 1.5 * sens[0])
+        ptol = {k: max(PARAM_RTOL, 1.5 * sens[1][k]) for k in errs}
+        print(f"  oracle roundoff sensitivity: cost {sens[0]:.3e} params {sens[1]} sigma {sens[2]:.3e}")
     assert cost_rel <= cost_tol, (rep_g["cost"], rep_o["cost"], cost_tol)
     for k in errs:
         assert errs[k] <= ptol[k], (k, errs[k], ptol[k])
