@@ -59,10 +59,14 @@ struct DevLSA {
   const int2 *contrib; // (obs in the row camera, obs in the column camera)
   const int *rowoff;   // [nimg + 1]
   const int2 *ent;     // (column camera, block index | 0x80000000 if transposed)
-  // SpMV work items: runs of <= 3 entries of one row
+  // SpMV work items: runs of <= 3 entries of one row.  In the FP32 form the
+  // items cover each row's diagonal and normal entries only: the SpMV reads
+  // every off-diagonal block once and forms both of its products.
   int nitems;
   const int *row_item_off;  // [nimg + 1]
   const int4 *item_meta;    // (row, first entry, end entry, 0)
+  const int2 *rowspan;      // [nimg] (diagonal entry, end entry) of each row
+  float *tpart;             // [nboff * 9] FP32 form: transposed block products
   int *err;            // device error word
 };
 
@@ -259,6 +263,7 @@ struct StructWork {
   unsigned *ckey, *ckey2;
   int *row_items, *row_item_off;
   int4 *item_meta;
+  int2 *rowspan;
 };
 size_t structure_cub_bytes(int nobs, long long npairs, int nimg);
 // PointXXvIn on the device (structure.cu): the caller's block in device

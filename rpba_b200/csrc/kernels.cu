@@ -438,9 +438,11 @@ __global__ void __launch_bounds__(CAM_T) k_camera(DevLSA L, double multfact1) {
 // ----------------------------------------------------------- pair pass
 // Off-diagonal blocks: S_kl = - sum_p W_pk V_p^-1 W_pl^T over the points
 // seen by both cameras (rbacore.cpp:1362-1390), with W_po = Bc^T G.  One
-// warp per block sums its contributions in a fixed order.
+// warp per block sums its contributions in a fixed order.  FP64 form; the
+// FP32 form is k_pair32.
 template <class T>
 __global__ void k_pair(DevLSA L) {
+  static_assert(sizeof(T) == 8, "the FP32 form is k_pair32");
   const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int wl = threadIdx.x >> 5;
@@ -450,10 +452,8 @@ __global__ void k_pair(DevLSA L) {
   Acc<T> acc[3];
   const T *rec = Store<T>::rec(L), *ptv = Store<T>::ptV(L);
   // values of one contribution: 24 of the row camera's observation (Bc 18,
-  // G 6), 24 of the column camera's and, in the FP64 form, V^-1 (9) of the
-  // point; the FP32 form's records hold H = G L^-T, whose products need no
-  // point term
-  constexpr int NV = sizeof(T) == 8 ? 57 : 48;
+  // G 6), 24 of the column camera's and V^-1 (9) of the point
+  constexpr int NV = 57;
   auto fetch = [&](int ox, int oy, int p, T &v0, T &v1) {
     v0 = lane < 24 ? rec[(size_t)ox * REC + lane] : rec[(size_t)oy * REC + lane - 24];
     const int i1 = lane + 32;
@@ -469,7 +469,7 @@ __global__ void k_pair(DevLSA L) {
     int pp = 0;
     if (lane < n) {
       pr = L.contrib[c0 + lane];
-      if constexpr (sizeof(T) == 8) pp = L.o_pt[pr.x];
+      pp = L.o_pt[pr.x];
     }
     T v0, v1;
     fetch(__shfl_sync(0xffffffffu, pr.x, 0), __shfl_sync(0xffffffffu, pr.y, 0), __shfl_sync(0xffffffffu, pp, 0),
@@ -481,29 +481,19 @@ __global__ void k_pair(DevLSA L) {
         fetch(__shfl_sync(0xffffffffu, pr.x, j + 1), __shfl_sync(0xffffffffu, pr.y, j + 1),
               __shfl_sync(0xffffffffu, pp, j + 1), v0, v1);
       __syncwarp();
-      // N = G_s V^-1 G_t^T (2 x 2); H_s H_t^T in the FP32 form
-      const T *Gs = s + 18, *Gt = s + 42;
-      T N[2][2];
-      if constexpr (sizeof(T) == 8) {
-        const T *Vi = s + 48;
-        T GV[2][3];
+      // N = G_s V^-1 G_t^T (2 x 2)
+      const T *Gs = s + 18, *Gt = s + 42, *Vi = s + 48;
+      T GV[2][3], N[2][2];
 #pragma unroll
-        for (int a = 0; a < 2; ++a)
+      for (int a = 0; a < 2; ++a)
 #pragma unroll
-          for (int b = 0; b < 3; ++b)
-            GV[a][b] = Gs[a * 3] * Vi[b] + Gs[a * 3 + 1] * Vi[3 + b] + Gs[a * 3 + 2] * Vi[6 + b];
+        for (int b = 0; b < 3; ++b)
+          GV[a][b] = Gs[a * 3] * Vi[b] + Gs[a * 3 + 1] * Vi[3 + b] + Gs[a * 3 + 2] * Vi[6 + b];
 #pragma unroll
-        for (int a = 0; a < 2; ++a)
+      for (int a = 0; a < 2; ++a)
 #pragma unroll
-          for (int b = 0; b < 2; ++b)
-            N[a][b] = GV[a][0] * Gt[b * 3] + GV[a][1] * Gt[b * 3 + 1] + GV[a][2] * Gt[b * 3 + 2];
-      } else {
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-          for (int b = 0; b < 2; ++b)
-            N[a][b] = Gs[a * 3] * Gt[b * 3] + Gs[a * 3 + 1] * Gt[b * 3 + 1] + Gs[a * 3 + 2] * Gt[b * 3 + 2];
-      }
+        for (int b = 0; b < 2; ++b)
+          N[a][b] = GV[a][0] * Gt[b * 3] + GV[a][1] * Gt[b * 3 + 1] + GV[a][2] * Gt[b * 3 + 2];
 #pragma unroll
       for (int q = 0; q < 3; ++q) {
         const int e = lane + 32 * q;
@@ -523,6 +513,72 @@ __global__ void k_pair(DevLSA L) {
   for (int q = 0; q < 3; ++q) {
     const int e = lane + 32 * q;
     if (e < 81) B[e] = (T)acc[q].value();
+  }
+}
+
+// FP32 form of the pair pass (whitened records): S_kl -= sum Bc_k^T (H_k
+// H_l^T) Bc_l over the block's contributions.  One warp per block: four
+// lanes form N = H_k H_l^T (2 x 2) and broadcast it; lanes 0..26 own the
+// three entries (i, 3 (lane % 3) .. + 2) of block row i = lane / 3.  Each
+// lane sums a chunk of up to 32 contributions in FP32, in order, and adds the
+// chunk into a compensated (Kahan) sum, so the entry is deterministic.
+__global__ void __launch_bounds__(256) k_pair32(DevLSA L) {
+  const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  const int wl = threadIdx.x >> 5;
+  __shared__ float sm[8][48];
+  if (wid >= L.nboff) return;
+  float *s = sm[wl];
+  const float *rec = L.rec32;
+  const int i = lane < 27 ? lane / 3 : 0, j0 = lane < 27 ? 3 * (lane - 3 * (lane / 3)) : 0;
+  float ks[3] = {0.f, 0.f, 0.f}, kc[3] = {0.f, 0.f, 0.f};
+  // record values of one contribution: Bc (18) and H (6) of the row
+  // camera's observation (s[0..23]), then of the column camera's (s[24..47])
+  auto fetch = [&](int ox, int oy, float &v0, float &v1) {
+    v0 = lane < 24 ? rec[(size_t)ox * REC + lane] : rec[(size_t)oy * REC + lane - 24];
+    v1 = lane < 16 ? rec[(size_t)oy * REC + lane + 8] : 0.f;
+  };
+  const int cb = L.boff[wid], ce = L.boff[wid + 1];
+  for (int c0 = cb; c0 < ce; c0 += 32) {
+    const int n = min(32, ce - c0);
+    int2 pr = make_int2(0, 0);
+    if (lane < n) pr = L.contrib[c0 + lane];
+    float v0, v1;
+    fetch(__shfl_sync(0xffffffffu, pr.x, 0), __shfl_sync(0xffffffffu, pr.y, 0), v0, v1);
+    float part[3] = {0.f, 0.f, 0.f};
+    for (int j = 0; j < n; ++j) {
+      s[lane] = v0;
+      if (lane < 16) s[32 + lane] = v1;
+      if (j + 1 < n)
+        fetch(__shfl_sync(0xffffffffu, pr.x, j + 1), __shfl_sync(0xffffffffu, pr.y, j + 1), v0, v1);
+      __syncwarp();
+      float nab = 0.f;
+      if (lane < 4) {
+        const float *hx = s + 18 + 3 * (lane >> 1), *hy = s + 42 + 3 * (lane & 1);
+        nab = hx[0] * hy[0] + hx[1] * hy[1] + hx[2] * hy[2];
+      }
+      const float n00 = __shfl_sync(0xffffffffu, nab, 0), n01 = __shfl_sync(0xffffffffu, nab, 1);
+      const float n10 = __shfl_sync(0xffffffffu, nab, 2), n11 = __shfl_sync(0xffffffffu, nab, 3);
+      if (lane < 27) {
+        const float bx0 = s[i], bx1 = s[9 + i];
+        const float u0 = bx0 * n00 + bx1 * n10, u1 = bx0 * n01 + bx1 * n11;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) part[q] -= u0 * s[24 + j0 + q] + u1 * s[33 + j0 + q];
+      }
+      __syncwarp();
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      const float y = part[q] - kc[q];
+      const float t = ks[q] + y;
+      kc[q] = (t - ks[q]) - y;
+      ks[q] = t;
+    }
+  }
+  if (lane < 27) {
+    float *B = L.blocks32 + (size_t)(L.nimg + wid) * BS32 + i * 9 + j0;
+#pragma unroll
+    for (int q = 0; q < 3; ++q) B[q] = (float)((double)ks[q] - (double)kc[q]);
   }
 }
 
@@ -986,7 +1042,7 @@ void launch_camera_pass(const DevLSA &L, double multfact1, cudaStream_t s) {
 void launch_pair_pass(const DevLSA &L, cudaStream_t s) {
   if (L.nboff <= 0) return;
   if (L.rec32)
-    k_pair<float><<<nblk((long long)L.nboff * 32, 256), 256, 0, s>>>(L);
+    k_pair32<<<nblk((long long)L.nboff * 32, 256), 256, 0, s>>>(L);
   else
     k_pair<double><<<nblk((long long)L.nboff * 32, 256), 256, 0, s>>>(L);
 }

@@ -22,11 +22,12 @@ namespace {
 
 // Threads per CTA of the persistent kernel, per block storage type: 1024 in
 // the FP64 form (32 warps, two work items in flight each through shared
-// memory), 768 in the FP32 form (24 warps whose three-slot register pipeline
-// needs 80 registers a thread).
+// memory), 640 in the FP32 form (20 warps whose three-slot register pipeline
+// and transposed products use 96 registers a thread; measured faster than
+// 768 and 1024).
 template <class BT>
 constexpr int pcg_threads() {
-  return sizeof(BT) == 8 ? 1024 : 768;
+  return sizeof(BT) == 8 ? 1024 : 640;
 }
 template <class BT>
 constexpr int pcg_warps() {
@@ -40,6 +41,8 @@ struct PcgArgs {
   const int *rowoff;
   const int *row_item_off;
   const int4 *item_meta;  // (row, first entry, end entry, 0)
+  const int2 *rowspan;    // (diagonal entry, end entry) of each row
+  float *tpart;           // FP32 form: transposed products of the off-diagonal blocks
   const double *Cinv;
   double *r, *h, *x, *xbest, *D0, *D1;
   double *part;        // [nitems * 9] SpMV partial rows
@@ -189,17 +192,31 @@ __device__ __forceinline__ int chunk_start(long long w, int nitems, int nwarps) 
 }
 
 // q of one row (valid in lanes < 9) from the phase-1 partials.  FP32 form:
-// one partial per (row, chunk) segment, stored at the segment's first item:
-// the row's first item and every chunk start inside the row, summed in item
-// order.  FP64 form: one partial per item, the three 9-lane groups taking
+// the transposed products of the row's transposed entries (in entry order,
+// three interleaved groups), then one partial per (row, chunk) segment,
+// stored at the segment's first item: the row's first item and every chunk
+// start inside the row, summed in item order.  FP64 form: one partial per item, the three 9-lane groups taking
 // every third item (four loads in flight), in a fixed order.
 template <class BT>
 __device__ __forceinline__ double row_q(const PcgArgs &A, int row, int nwarps, int lane, int grp, int rr) {
   const int t0 = A.row_item_off[row], t1 = A.row_item_off[row + 1];
   if constexpr (sizeof(BT) == 4) {
-    double q = 0.;
+    // transposed products of the row's transposed entries (blocks stored by
+    // the rows before it): the three 9-lane groups take every third entry
+    double qt = 0.;
+    if (lane < 27) {
+      const int e1 = __ldg(&A.rowspan[row].x);
+#pragma unroll 4
+      for (int e = A.rowoff[row] + grp; e < e1; e += 3) {
+        const int blk = (__ldg(&A.ent[e].y) & 0x7fffffff) - A.row1;
+        qt += (double)__ldcg(A.tpart + (size_t)blk * 9 + rr);
+      }
+    }
+    const double qa = __shfl_down_sync(0xffffffffu, qt, 9);
+    const double qb = __shfl_down_sync(0xffffffffu, qt, 18);
+    double q = qt + qa + qb;
     if (lane < 9 && t0 < t1) {
-      q = __ldcg(A.part + (size_t)t0 * 9 + lane);
+      q += __ldcg(A.part + (size_t)t0 * 9 + lane);
       // smallest w whose chunk starts after t0
       long long w = ((long long)(t0 + 1) * nwarps + A.nitems - 1) / A.nitems;
       int prev = t0;
@@ -317,41 +334,51 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
         __syncwarp();
       }
     } else {
-      // FP32 blocks: each warp walks one contiguous chunk of the work items
-      // (row order) with a three-slot register pipeline: the blocks of item
-      // t + 2 (and the d^k entries they multiply) are loaded while item t is
-      // multiplied, the entries of item t + 3 one step earlier; entry
-      // positions follow from the walk (row offsets), so no load waits on
-      // another.  Each block row is formed in FP32 (FP32 blocks times d^k
-      // rounded to FP32) and the row sums are carried in FP64; products are
-      // summed per row in registers and written once per (row, chunk)
-      // segment, at the segment's first item.
+      // FP32 blocks, symmetric SpMV: the items cover each row's diagonal and
+      // normal entries, so every off-diagonal block is read once and gives
+      // both products: its row's (block row rr times the column camera's
+      // d^k) and its column's (block column rr, re-read from L1, times the
+      // row camera's d^k, stored in the block's slot of tpart; phase 2 adds
+      // it to the column's row, and its share of d^T A d is summed here).
+      // Each warp walks one contiguous chunk of the items (row order) with a
+      // three-slot register pipeline: the blocks of item t + 2 (and the d^k
+      // entries they multiply) are loaded while item t is multiplied, the
+      // entries of item t + 3 one step earlier; entry positions follow from
+      // the walk (row spans), so no load waits on another.  Products are
+      // formed in FP32 (FP32 blocks times d^k rounded to FP32); the row sums
+      // are carried in FP64, per (row, chunk) segment in registers, written
+      // once at the segment's first item.
       const int c0 = chunk_start(gwarp, A.nitems, nwarps);
       const int c1 = chunk_start(gwarp + 1, A.nitems, nwarps);
       if (c0 < c1) {
         const BT *blocks = (const BT *)A.blocks;
         const int4 m0 = A.item_meta[c0];
-        int wrow = m0.x, we = m0.y, wend = __ldg(A.rowoff + m0.x + 1);
+        int wrow = m0.x, we = m0.y, wend = __ldg(&A.rowspan[m0.x].y);
         int rowN = 0;
         int2 enN = make_int2(-1, 0);
-        // entries of the walk's next item (lanes < 27, col -1 past the row)
+        // entries of the walk's next item (lanes < 27, col -1 past the row);
+        // a row's items run from its diagonal entry to its end
         auto ent_next = [&]() {
           rowN = wrow;
           enN = make_int2(-1, 0);
           if (lane < 27 && we + grp < wend) enN = __ldg(A.ent + we + grp);
           we += 3;
-          if (we >= wend) {
-            we = wend;
-            if (++wrow < A.row1) wend = __ldg(A.rowoff + wrow + 1);
+          if (we >= wend && ++wrow < A.row1) {
+            const int2 sp = __ldg(A.rowspan + wrow);
+            we = sp.x;
+            wend = sp.y;
           }
         };
         // loads of the item whose entries are in enN into a slot, then the
-        // next entries (items past the chunk load nothing)
-        auto slot_load = [&](int t, float (&b)[9], float &dc, int &row) {
+        // next entries (items past the chunk load nothing); ob: the lane's
+        // off-diagonal block (-1: none or the diagonal)
+        auto slot_load = [&](int t, float (&b)[9], float &dc, int &row, int &ob) {
           row = rowN;
           dc = 0.f;
+          ob = -1;
           const int2 en = enN;
           if (t < c1 && en.x >= 0) {
+            if (en.y >= A.row1) ob = en.y - A.row1;
             // row rr of the block, or column rr of a transposed one
             const bool tr = en.y < 0;
             const BT *B = blocks + (size_t)(en.y & 0x7fffffff) * BS32 + (tr ? rr : rr * 9);
@@ -372,15 +399,27 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
         };
         float bA[9], bB[9], bC[9];
         float dA, dB, dC;
-        int rA, rB, rC;
+        int rA, rB, rC, oA, oB, oC;
         ent_next();
-        slot_load(c0, bA, dA, rA);
-        slot_load(c0 + 1, bB, dB, rB);
+        slot_load(c0, bA, dA, rA, oA);
+        slot_load(c0 + 1, bB, dB, rB, oB);
         int seg = c0, segrow = rA;
         double racc = 0., dseg = dk_of(segrow);
-        // item t from slot (b, d, r); the slot `nb` receives item t + 2
-        auto step = [&](int t, const float (&b)[9], float d, int r, float (&nb)[9], float &nd, int &nr) {
-          slot_load(t + 2, nb, nd, nr);
+        // d^k of the segment's row in every lane (FP32), for the transposed
+        // products
+        float xr[9];
+        auto row_x = [&]() {
+          const float v = (float)dseg;
+#pragma unroll
+          for (int c = 0; c < 9; ++c) xr[c] = __shfl_sync(0xffffffffu, v, c);
+        };
+        row_x();
+        // item t from slot (b, d, r, o); the slot `nb` receives item t + 2.
+        // An off-diagonal block's transposed product (column rr of the block,
+        // re-read from L1, times the row's d^k) goes to its slot of tpart.
+        auto step = [&](int t, const float (&b)[9], float d, int r, int o, float (&nb)[9], float &nd, int &nr,
+                        int &no) {
+          slot_load(t + 2, nb, nd, nr, no);
           float acc = 0.f;
 #pragma unroll
           for (int c = 0; c < 9; ++c) acc = fmaf(b[c], __shfl_sync(0xffffffffu, d, (lane < 27 ? gbase : 0) + c), acc);
@@ -395,15 +434,25 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
             segrow = r;
             racc = 0.;
             dseg = dk_of(r);
+            row_x();
           }
           if (lane < 9) racc += (double)acc + (double)a1 + (double)a2;
+          if (o >= 0) {
+            const BT *Bc = blocks + (size_t)(o + A.row1) * BS32 + rr;
+            float yt = 0.f;
+#pragma unroll
+            for (int c = 0; c < 9; ++c) yt = fmaf(__ldg(Bc + c * 9), xr[c], yt);
+            A.tpart[(size_t)o * 9 + rr] = yt;
+            // the transposed product's share of d^T A d: d_c^T (B^T d_r)
+            pdq[0] += (double)d * (double)yt;
+          }
         };
         for (int t = c0; t < c1; t += 3) {
-          step(t, bA, dA, rA, bC, dC, rC);
+          step(t, bA, dA, rA, oA, bC, dC, rC, oC);
           if (t + 1 >= c1) break;
-          step(t + 1, bB, dB, rB, bA, dA, rA);
+          step(t + 1, bB, dB, rB, oB, bA, dA, rA, oA);
           if (t + 2 >= c1) break;
-          step(t + 2, bC, dC, rC, bB, dB, rB);
+          step(t + 2, bC, dC, rC, oC, bB, dB, rB, oB);
         }
         if (lane < 9) {
           A.part[(size_t)seg * 9 + lane] = racc;
@@ -666,6 +715,8 @@ int pcg_iterate(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStre
   A.rowoff = L.rowoff;
   A.row_item_off = L.row_item_off;
   A.item_meta = L.item_meta;
+  A.rowspan = L.rowspan;
+  A.tpart = L.tpart;
   A.Cinv = W.Cinv;
   A.r = W.r;
   A.h = W.h;

@@ -261,6 +261,21 @@ struct rpba_handle {
     }
   }
 
+  // Algorithmic bytes of one PCG iteration.  FP64 form: every block read from
+  // both sides with its entry (648 + 8 B per side).  FP32 form (symmetric):
+  // every block read once with its entry (324 + 8 B), and per off-diagonal
+  // block the transposed product written and read (36 B each) with the
+  // transposed entry (8 B).  Per camera row: the preconditioner (648 B) and
+  // 22 reads/writes of 9-vectors (72 B each); with the coarse space P_k twice
+  // (720 B each) and the block part of h twice; A_c^-1 stays in L2 and is
+  // not counted.
+  double pcg_bytes_per_iteration(bool coarse) const {
+    const double Nc = nimg - begini, Nb = L.nboff;
+    const double row = 648. + 22. * 72. + (coarse ? 2. * 720. + 2. * 72. : 0.);
+    const double blocks = L.blocks32 ? 332. * (Nc + Nb) + 80. * Nb : 656. * (Nc + 2. * Nb);
+    return blocks + Nc * row;
+  }
+
   // reduced camera system storage: FP64, or FP32 in the mixed form
   void ensure_blocks(int nb) {
     const bool mixed = opt.precision == RPBA_PREC_MIXED;
@@ -268,7 +283,8 @@ struct rpba_handle {
     if (nb <= blocks_cap && cur) return;
     const int cap = std::max(nb, 1);
     if (cur) {
-      for (void *p : {cur, (void *)S.ent, (void *)S.item_meta, (void *)W.part}) {
+      for (void *p : {cur, (void *)S.ent, (void *)S.item_meta, (void *)W.part, (void *)L.tpart}) {
+        if (!p) continue;
         auto it = std::find(owned_async.begin(), owned_async.end(), p);
         if (it != owned_async.end()) {
           cudaFreeAsync(p, s);
@@ -279,9 +295,10 @@ struct rpba_handle {
         }
       }
     }
-    if (mixed)
+    if (mixed) {
       L.blocks32 = dalloc<float>((size_t)(nimg + cap) * BS32, owned);
-    else
+      L.tpart = dalloc<float>((size_t)cap * 9, owned);
+    } else
       L.blocks = dalloc<double>((size_t)(nimg + cap) * BS64, owned);
     S.ent = dalloc<int2>((size_t)nimg + 2 * (size_t)cap, owned);
     // SpMV work items: at most ceil(entries / 3) per row
@@ -666,6 +683,7 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   S.iota = dalloc<int>(no, own);
   S.row_items = dalloc<int>(n + 1, own);
   S.row_item_off = dalloc<int>(n + 1, own);
+  S.rowspan = dalloc<int2>(n + 1, own);
   S.ckey = dalloc<unsigned>(no, own);
   S.ckey2 = dalloc<unsigned>(no, own);
   H->ES.err = L.err;  // a barrier timeout in a sum surfaces in the LSA's error word
@@ -797,19 +815,12 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
       if (cw) RPBA_CUDA_CHECK(cudaMemcpyAsync(it + 2, CW.err, sizeof(int), cudaMemcpyDeviceToHost, s));
       RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
       learned_iters += it[0];
-      if (prof.on) {
-        // per iteration: blocks read from both sides plus their entries,
-        // per camera row the preconditioner (648), 22 reads/writes of
-        // 9-vectors, and with the coarse space P_k twice (720 each) and the
-        // block part of h twice; A_c^-1 stays in L2 and is not counted
-        const double Nc = nimg - begini, Nb = L.nboff, bs = L.blocks32 ? 324. : 648.;
-        const double row = 648. + 22. * 72. + (cw ? 2. * 720. + 2. * 72. : 0.);
+      if (prof.on)
         for (auto itp = prof.pending.rbegin(); itp != prof.pending.rend(); ++itp)
           if (std::string(itp->name) == "pcg") {
-            itp->bytes = (double)it[0] * ((bs + 8.) * (Nc + 2. * Nb) + Nc * row);
+            itp->bytes = (double)it[0] * pcg_bytes_per_iteration(cw != nullptr);
             break;
           }
-      }
       if (fresh) coarse_ref_iters = it[0];
       const bool conv = (mode == 1 ? it[1] != 0 : it[0] < cap_try) && it[2] == 0;
       if (conv || fresh || !cw) break;
@@ -981,17 +992,12 @@ int rpba_handle::adjust() {
       RPBA_CUDA_CHECK(cudaMemcpyAsync(&hv.iters, W.iters, sizeof(int), cudaMemcpyDeviceToHost, s));
       RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
       rep.pcg_iterations += opt.solver == RPBA_SOLVER_PCG ? hv.iters : 0;
-      if (prof.on && pcg_pending) {
-        // per PCG iteration: blocks read from both sides (648 * (Nc + 2 Nb)),
-        // block entries (8 each), per camera row the preconditioner (648) and
-        // 22 reads/writes of 9-vectors (72 B each)
-        const double Nc = nimg - begini, Nb = L.nboff;
+      if (prof.on && pcg_pending)
         for (auto it = prof.pending.rbegin(); it != prof.pending.rend(); ++it)
           if (std::string(it->name) == "pcg") {
-            it->bytes = (double)hv.iters * (656. * (Nc + 2. * Nb) + Nc * (648. + 22. * 72.));
+            it->bytes = (double)hv.iters * pcg_bytes_per_iteration(false);
             break;
           }
-      }
       pcg_pending = false;
       if (hv.err & 2) return RPBA_ERR_DEVICE_TIMEOUT;
       if (hv.err & 4) return RPBA_ERR_SOLVER;

@@ -118,19 +118,26 @@ __global__ void k_fill_transposed(const unsigned *bkey, const int *tidx_sorted, 
   ent[pos] = make_int2(row, (int)((unsigned)(nimg + b) | 0x80000000u));
 }
 
-// Work items of the SpMV: each row's entry list cut into runs of <= 3.
-__global__ void k_row_items(const int *rowoff, int nimg, int begini, int *cnt) {
+// Work items of the SpMV: each row's entry list cut into runs of <= 3 (the
+// symmetric form: from the row's diagonal entry on, the transposed entries
+// before it are served by their blocks' rows).  rowspan: (diagonal entry,
+// end entry) of every row.
+__global__ void k_row_items(const int *rowoff, const int *cntT, int nimg, int begini, int sym, int *cnt,
+                            int2 *rowspan) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k > nimg) return;
-  cnt[k] = (k < nimg && k >= begini) ? (rowoff[k + 1] - rowoff[k] + 2) / 3 : 0;
+  const int first = k < nimg ? rowoff[k] + (sym ? cntT[k] : 0) : 0;
+  cnt[k] = (k < nimg && k >= begini) ? (rowoff[k + 1] - first + 2) / 3 : 0;
+  if (k < nimg) rowspan[k] = make_int2(rowoff[k] + cntT[k], rowoff[k + 1]);
 }
 
-__global__ void k_fill_items(const int *rowoff, const int *row_item_off, int nimg, int begini, int4 *meta) {
+__global__ void k_fill_items(const int *rowoff, const int *cntT, const int *row_item_off, int nimg, int begini,
+                             int sym, int4 *meta) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nimg || k < begini) return;
-  const int end = rowoff[k + 1];
+  const int end = rowoff[k + 1], first = rowoff[k] + (sym ? cntT[k] : 0);
   for (int t = row_item_off[k], j = 0; t < row_item_off[k + 1]; ++t, ++j) {
-    const int e0 = rowoff[k] + 3 * j;
+    const int e0 = first + 3 * j;
     meta[t] = make_int4(k, e0, min(e0 + 3, end), 0);
   }
 }
@@ -229,18 +236,20 @@ void build_bsr(DevLSA &L, StructWork &S, cudaStream_t s) {
     k_fill_transposed<<<nblk(nb, 256), 256, 0, s>>>(S.bkey, S.tidx2, nb, n, S.rowoff, S.firstT, S.ent);
   }
   k_fill_diag<<<nblk(n, 256), 256, 0, s>>>(n, S.rowoff, S.cntT, S.ent);
-  k_row_items<<<nblk(n + 1, 256), 256, 0, s>>>(S.rowoff, n, L.begini, S.row_items);
+  const int sym = L.blocks32 ? 1 : 0;
+  k_row_items<<<nblk(n + 1, 256), 256, 0, s>>>(S.rowoff, S.cntT, n, L.begini, sym, S.row_items, S.rowspan);
   bytes = S.cub_bytes;
   RPBA_CUDA_CHECK(cub::DeviceScan::ExclusiveSum(S.cub_tmp, bytes, S.row_items, S.row_item_off, n + 1, s));
   int nitems = 0;
   RPBA_CUDA_CHECK(cudaMemcpyAsync(&nitems, S.row_item_off + n, sizeof(int), cudaMemcpyDeviceToHost, s));
   RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
-  k_fill_items<<<nblk(n, 256), 256, 0, s>>>(S.rowoff, S.row_item_off, n, L.begini, S.item_meta);
+  k_fill_items<<<nblk(n, 256), 256, 0, s>>>(S.rowoff, S.cntT, S.row_item_off, n, L.begini, sym, S.item_meta);
   L.rowoff = S.rowoff;
   L.ent = S.ent;
   L.nitems = nitems;
   L.row_item_off = S.row_item_off;
   L.item_meta = S.item_meta;
+  L.rowspan = S.rowspan;
 }
 
 // ---- PointXXvIn (rbacore.cpp:1918-1974) on the device: the track-ordered
