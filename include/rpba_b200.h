@@ -305,6 +305,17 @@ typedef struct rpba_tri_options {
 int32_t rpba_triangulate(const rpba_block *blk, const float *sig0w, const rpba_tri_options *opt, double *XX_out,
                          uint8_t *keep, float *sig0v, uint8_t *conv, double *sig0io, int64_t *redundancy);
 
+/* Camera partition of the reference's parallel RPBA: replaces
+ * PartitionpointXXv (rpbacore.cpp:945-1037), which cuts the images'
+ * covisibility graph (an edge where two images share a point observed at
+ * least twice; vertex weight floor(BM^0.3333), BM the sum of the track
+ * lengths of the image's points) with METIS_PartGraphRecursive and
+ * METIS_OPTION_CONTIG.  METIS is not available here: the cut is this
+ * library's own deterministic recursive bisection, every part contiguous on
+ * a connected graph.  part[n_images] receives each image's part,
+ * 0 .. nparts - 1.  Host code; needs no GPU. */
+int32_t rpba_partition_images(const rpba_block *blk, int32_t nparts, int32_t *part);
+
 /* Batched form: many independent scenes of uneven size on one GPU.  Every
  * scene is solved as rpba_calc_plsa would solve it (in place; reports[i] and
  * status[i] per scene); `workers` scenes run at once, each on its own stream,

@@ -1,0 +1,207 @@
+// partition.cpp -- camera partition of the reference's parallel RPBA
+// (PartitionpointXXv, rpbacore.cpp:945-1037), host code.
+//
+// The reference builds the images' covisibility graph (an edge wherever two
+// images share a point observed at least twice; unweighted), weights every
+// image by floor(BM^0.3333) with BM the sum of the track lengths of its
+// points, and cuts it into nrthreads contiguous parts with
+// METIS_PartGraphRecursive and METIS_OPTION_CONTIG.  METIS is not available
+// here, so the cut is a deterministic recursive bisection of this library's
+// own: each half is grown breadth-first from a pseudo-peripheral vertex until
+// it holds its share of the weight, and the components that this leaves
+// detached from the rest join the grown half.  On a connected graph both
+// halves stay connected at every level, so every part is contiguous.
+// The graph is kept as sorted adjacency lists (the reference's dense
+// N_img x N_img matrix would take 750 MB at 13,700 images).
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <vector>
+
+#include "../../include/rpba_b200.h"
+
+namespace {
+
+struct Graph {
+  std::vector<int> off, adj;  // CSR adjacency, neighbours sorted by index
+  std::vector<long long> w;   // vertex weights
+};
+
+Graph build_graph(const rpba_block *b) {
+  const int n = b->n_images;
+  Graph g;
+  g.w.assign(n, 0);
+  // BM[i]: sum of the track lengths of the image's points (tracks of >= 2)
+  std::vector<long long> bm(n, 0);
+  std::vector<int> ipo(n + 1, 0);  // image -> points (CSR)
+  for (int p = 0; p < b->n_points; ++p) {
+    const int t0 = b->pt_obs_off[p], t1 = b->pt_obs_off[p + 1];
+    if (t1 - t0 < 2) continue;
+    for (int t = t0; t < t1; ++t) {
+      bm[b->pt_obs_image[t]] += t1 - t0;
+      ++ipo[b->pt_obs_image[t] + 1];
+    }
+  }
+  for (int i = 0; i < n; ++i) ipo[i + 1] += ipo[i];
+  std::vector<int> ipts(ipo[n]), fill(ipo.begin(), ipo.end() - 1);
+  for (int p = 0; p < b->n_points; ++p) {
+    const int t0 = b->pt_obs_off[p], t1 = b->pt_obs_off[p + 1];
+    if (t1 - t0 < 2) continue;
+    for (int t = t0; t < t1; ++t) ipts[fill[b->pt_obs_image[t]]++] = p;
+  }
+  for (int i = 0; i < n; ++i) g.w[i] = (long long)std::pow((double)bm[i], 0.3333);
+  // neighbours of every image through its points (a stamp array marks the
+  // ones already listed)
+  std::vector<int> stamp(n, -1);
+  g.off.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i) {
+    const size_t start = g.adj.size();
+    for (int q = ipo[i]; q < ipo[i + 1]; ++q) {
+      const int p = ipts[q];
+      for (int t = b->pt_obs_off[p]; t < b->pt_obs_off[p + 1]; ++t) {
+        const int j = b->pt_obs_image[t];
+        if (j != i && stamp[j] != i) {
+          stamp[j] = i;
+          g.adj.push_back(j);
+        }
+      }
+    }
+    std::sort(g.adj.begin() + (long)start, g.adj.end());
+    g.off[i + 1] = (int)g.adj.size();
+  }
+  return g;
+}
+
+class Bisector {
+ public:
+  Bisector(const Graph &g, int32_t *part) : g_(g), part_(part), in_(g.w.size(), 0), mark_(g.w.size(), 0) {}
+
+  // Cuts `verts` (sorted) into k parts numbered base .. base + k - 1.
+  void cut(std::vector<int> verts, int k, int base) {
+    if (k <= 1 || verts.size() <= 1) {
+      for (int v : verts) part_[v] = base;
+      return;
+    }
+    const int k1 = k / 2;
+    long long total = 0;
+    for (int v : verts) total += g_.w[v];
+    const long long target = (total * k1 + k / 2) / k;
+    const int tag = ++tag_;
+    for (int v : verts) in_[v] = tag;
+    // grow the first half breadth-first from a pseudo-peripheral vertex;
+    // a component exhausted before the target continues from the next
+    // unvisited vertex of the set
+    const int side1 = ++tag_;
+    long long w1 = 0;
+    size_t n1 = 0;
+    int last_added = -1;
+    std::vector<int> queue;
+    int seed = peripheral(verts.front(), tag);
+    size_t next_unvisited = 0;
+    while (w1 < target || n1 == 0) {
+      if (queue.empty()) {
+        if (mark_[seed] == side1) {
+          while (next_unvisited < verts.size() && mark_[verts[next_unvisited]] == side1) ++next_unvisited;
+          if (next_unvisited == verts.size()) break;
+          seed = verts[next_unvisited];
+        }
+        mark_[seed] = side1;
+        w1 += g_.w[seed];
+        ++n1;
+        last_added = seed;
+        queue.assign(1, seed);
+        continue;
+      }
+      std::vector<int> nextq;
+      for (size_t qi = 0; qi < queue.size() && (w1 < target); ++qi) {
+        const int v = queue[qi];
+        for (int e = g_.off[v]; e < g_.off[v + 1] && w1 < target; ++e) {
+          const int u = g_.adj[e];
+          if (in_[u] != tag || mark_[u] == side1) continue;
+          mark_[u] = side1;
+          w1 += g_.w[u];
+          ++n1;
+          last_added = u;
+          nextq.push_back(u);
+        }
+      }
+      queue.swap(nextq);
+    }
+    if (n1 == verts.size()) {  // nothing left for the second half
+      mark_[last_added] = 0;
+      --n1;
+    }
+    // the rest: keep its heaviest component, the others join the first half
+    std::vector<int> rest;
+    for (int v : verts)
+      if (mark_[v] != side1) rest.push_back(v);
+    const int comp_tag = ++tag_;
+    std::vector<int> best;
+    long long best_w = -1;
+    for (int r : rest) {
+      if (mark_[r] == comp_tag) continue;
+      std::vector<int> comp(1, r);
+      mark_[r] = comp_tag;
+      long long cw = g_.w[r];
+      for (size_t qi = 0; qi < comp.size(); ++qi) {
+        const int v = comp[qi];
+        for (int e = g_.off[v]; e < g_.off[v + 1]; ++e) {
+          const int u = g_.adj[e];
+          if (in_[u] != tag || mark_[u] == side1 || mark_[u] == comp_tag) continue;
+          mark_[u] = comp_tag;
+          cw += g_.w[u];
+          comp.push_back(u);
+        }
+      }
+      if (cw > best_w) {
+        best_w = cw;
+        best = comp;
+      }
+    }
+    std::vector<int> h1, h2;
+    const int keep = ++tag_;
+    for (int v : best) mark_[v] = keep;
+    for (int v : verts) (mark_[v] == keep ? h2 : h1).push_back(v);
+    cut(h1, k1, base);
+    cut(h2, k - k1, base + k1);
+  }
+
+ private:
+  // a pseudo-peripheral vertex of the set: the farthest vertex of a
+  // breadth-first search from the farthest vertex of one from `start`
+  int peripheral(int start, int tag) {
+    int v = start;
+    for (int round = 0; round < 2; ++round) {
+      const int seen = ++tag_;
+      std::vector<int> q(1, v);
+      mark_[v] = seen;
+      for (size_t qi = 0; qi < q.size(); ++qi) {
+        const int x = q[qi];
+        for (int e = g_.off[x]; e < g_.off[x + 1]; ++e) {
+          const int u = g_.adj[e];
+          if (in_[u] != tag || mark_[u] == seen) continue;
+          mark_[u] = seen;
+          q.push_back(u);
+        }
+      }
+      v = q.back();
+    }
+    return v;
+  }
+
+  const Graph &g_;
+  int32_t *part_;
+  std::vector<int> in_, mark_;
+  int tag_ = 0;
+};
+
+}  // namespace
+
+extern "C" int32_t rpba_partition_images(const rpba_block *blk, int32_t nparts, int32_t *part) {
+  if (!blk || !part || nparts < 1 || blk->n_images < 1) return RPBA_ERR_ARG;
+  const Graph g = build_graph(blk);
+  std::vector<int> all(blk->n_images);
+  for (int i = 0; i < blk->n_images; ++i) all[i] = i;
+  Bisector(g, part).cut(all, nparts, 0);
+  return RPBA_OK;
+}

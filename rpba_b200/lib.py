@@ -39,7 +39,7 @@ EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block
            "rpba_get_state", "rpba_get_log", "rpba_exteval", "rpba_kernel_stats", "rpba_float_sequential_sum",
            "rpba_float_sequential_sum_noalloc", "rpba_train_preconditioner",
            "rpba_set_preconditioner", "rpba_precond_loss_grad", "rpba_record_systems", "rpba_solve_batch",
-           "rpba_triangulate", "rpba_destroy")
+           "rpba_triangulate", "rpba_partition_images", "rpba_destroy")
 
 _lib = None
 
@@ -98,6 +98,8 @@ def load():
     L.rpba_solve_batch.argtypes = [bp, C.c_int32, op, C.c_int32, rp, C.POINTER(C.c_int32),
                                    C.POINTER(RpbaBatchReportC)]
     L.rpba_solve_batch.restype = C.c_int32
+    L.rpba_partition_images.argtypes = [bp, C.c_int32, C.POINTER(C.c_int32)]
+    L.rpba_partition_images.restype = C.c_int32
     L.rpba_triangulate.argtypes = [bp, C.POINTER(C.c_float), C.POINTER(RpbaTriOptionsC), C.POINTER(C.c_double),
                                    C.POINTER(C.c_uint8), C.POINTER(C.c_float), C.POINTER(C.c_uint8),
                                    C.POINTER(C.c_double), C.POINTER(C.c_int64)]
@@ -173,6 +175,18 @@ def train_preconditioner(blocks, steps=300, batch=0, lr=3e-3, probes=2, seed=1, 
     if st != 0:
         raise RpbaError(st, "rpba_train_preconditioner")
     return w, {k: getattr(rep, k) for k, _ in rep._fields_}
+
+
+def partition_images(block: Block, nparts: int) -> np.ndarray:
+    """Part (0 .. nparts - 1) of every image: the camera partition of the
+    reference's parallel RPBA (PartitionpointXXv, rpbacore.cpp:945-1037),
+    contiguous parts of the covisibility graph.  Host code, no GPU."""
+    part = np.zeros(block.n_images, np.int32)
+    cb = block.as_c()
+    st = load().rpba_partition_images(C.byref(cb), int(nparts), part.ctypes.data_as(C.POINTER(C.c_int32)))
+    if st != 0:
+        raise RpbaError(st, "rpba_partition_images")
+    return part
 
 
 def triangulate(block: Block, sig0w=None, robustmode: int = 0, weight_only: bool = False, device: int = 0,
