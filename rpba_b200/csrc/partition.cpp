@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <thread>
 #include <vector>
 
 #include "../../include/rpba_b200.h"
@@ -50,25 +51,37 @@ Graph build_graph(const rpba_block *b) {
     for (int t = t0; t < t1; ++t) ipts[fill[b->pt_obs_image[t]]++] = p;
   }
   for (int i = 0; i < n; ++i) g.w[i] = (long long)std::pow((double)bm[i], 0.3333);
-  // neighbours of every image through its points (a stamp array marks the
-  // ones already listed)
-  std::vector<int> stamp(n, -1);
-  g.off.assign(n + 1, 0);
-  for (int i = 0; i < n; ++i) {
-    const size_t start = g.adj.size();
-    for (int q = ipo[i]; q < ipo[i + 1]; ++q) {
-      const int p = ipts[q];
-      for (int t = b->pt_obs_off[p]; t < b->pt_obs_off[p + 1]; ++t) {
-        const int j = b->pt_obs_image[t];
-        if (j != i && stamp[j] != i) {
-          stamp[j] = i;
-          g.adj.push_back(j);
+  // neighbours of every image through its points (a stamp array per thread
+  // marks the ones already listed), images split over host threads in
+  // contiguous ranges; each list is sorted, so the result does not depend on
+  // the thread count
+  std::vector<std::vector<int>> nbr(n);
+  const int T = n >= 256 ? (int)std::min(32u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+  auto work = [&](int k) {
+    std::vector<int> stamp(n, -1);
+    for (int i = (int)((long long)n * k / T); i < (int)((long long)n * (k + 1) / T); ++i) {
+      std::vector<int> &out = nbr[i];
+      for (int q = ipo[i]; q < ipo[i + 1]; ++q) {
+        const int p = ipts[q];
+        for (int t = b->pt_obs_off[p]; t < b->pt_obs_off[p + 1]; ++t) {
+          const int j = b->pt_obs_image[t];
+          if (j != i && stamp[j] != i) {
+            stamp[j] = i;
+            out.push_back(j);
+          }
         }
       }
+      std::sort(out.begin(), out.end());
     }
-    std::sort(g.adj.begin() + (long)start, g.adj.end());
-    g.off[i + 1] = (int)g.adj.size();
-  }
+  };
+  std::vector<std::thread> th;
+  for (int k = 1; k < T; ++k) th.emplace_back(work, k);
+  work(0);
+  for (auto &t : th) t.join();
+  g.off.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i) g.off[i + 1] = g.off[i] + (int)nbr[i].size();
+  g.adj.resize(g.off[n]);
+  for (int i = 0; i < n; ++i) std::copy(nbr[i].begin(), nbr[i].end(), g.adj.begin() + g.off[i]);
   return g;
 }
 
