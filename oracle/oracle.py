@@ -115,6 +115,37 @@ def triangulate(block: Block, sig0w=None, robustmode: int = 0, weight_only: bool
     return rlib.triangulate(block, sig0w, robustmode, weight_only, fn=L.oracle_triangulate)
 
 
+def triangulate_parts(block: Block, part, nparts: int, sig0w=None, robustmode: int = 0,
+                      weight_only: bool = False) -> dict:
+    """CalcLSAXMulti with the camera partition ``part`` (image -> 0 ..
+    nparts - 1): also the per-partition weight blocks ``w3d`` (n_points x
+    nparts x 6: XX, YY, ZZ, XY, XZ, YZ) of the reference's wxyflag."""
+    cb = block.as_c()
+    nt, np_ = block.n_obs, block.n_points
+    part = np.ascontiguousarray(part, np.int32)
+    out = {"XX": np.zeros(3 * np_), "keep": np.zeros(nt, np.uint8), "sig0v": np.zeros(nt, np.float32),
+           "conv": np.zeros(np_, np.uint8), "w3d": np.zeros(np_ * nparts * 6, np.float32)}
+    s0, red = C.c_double(), C.c_int64()
+    w = None if sig0w is None else np.ascontiguousarray(sig0w, np.float32)
+    L = lib()
+    f = L.oracle_triangulate_parts
+    f.restype = C.c_int32
+    f.argtypes = [C.POINTER(RpbaBlockC), C.POINTER(C.c_float), C.c_int32, C.c_int32, C.POINTER(C.c_int32),
+                  C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_uint8), C.POINTER(C.c_float),
+                  C.POINTER(C.c_uint8), C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_float)]
+    st = f(C.byref(cb), None if w is None else w.ctypes.data_as(C.POINTER(C.c_float)), int(robustmode),
+           int(weight_only), part.ctypes.data_as(C.POINTER(C.c_int32)), int(nparts),
+           out["XX"].ctypes.data_as(C.POINTER(C.c_double)), out["keep"].ctypes.data_as(C.POINTER(C.c_uint8)),
+           out["sig0v"].ctypes.data_as(C.POINTER(C.c_float)), out["conv"].ctypes.data_as(C.POINTER(C.c_uint8)),
+           C.byref(s0), C.byref(red), out["w3d"].ctypes.data_as(C.POINTER(C.c_float)))
+    if st != 0:
+        raise RuntimeError(f"oracle_triangulate_parts: status {st}")
+    out["XX"] = out["XX"].reshape(np_, 3)
+    out["w3d"] = out["w3d"].reshape(np_, nparts, 6)
+    out["sig0io"], out["redundancy"] = s0.value, red.value
+    return out
+
+
 def input_block(path: str, k24out: bool = True) -> Block:
     cb = RpbaBlockC()
     st = lib().oracle_input_block(path.encode(), 3, int(k24out), C.byref(cb))

@@ -1544,8 +1544,13 @@ void copy_log(const std::string &s, char *log, size_t cap) {
 /* ------------------------------------------- per-point triangulation
  * CalcLSAXMulti (rpbacore.cpp:536-773) with CalcCorrPointMulti (:778-837)
  * and CalcCalibratedDerivatives (:841-877): robust Gauss-Newton of one
- * point against fixed cameras.  The per-partition weight blocks
- * (wxyflag) are not restated: they only feed the partitioned merge. */
+ * point against fixed cameras.  With a camera partition (part, nparts) the
+ * per-partition weight blocks (wxyflag, rpbacore.cpp:579-590, 612-622,
+ * 663-672) are formed too: for every partition i that sees the point, the
+ * normal matrix (B^T W B, undamped) of the point's observations in the
+ * other partitions (one partition: all of them), from the iteration last
+ * accepted, as floats; zero for partitions that do not see the point and
+ * for points without an accepted iteration. */
 namespace {
 
 struct TriObs {
@@ -1609,9 +1614,9 @@ void tri_calibrated(double *xp, double *yp, double x, double y, double k2, doubl
 
 }  // namespace
 
-extern "C" int32_t oracle_triangulate(const rpba_block *b, const float *sig0w, int32_t robustmode,
-                                      int32_t weight_only, double *XXo, uint8_t *keep, float *sig0v_out,
-                                      uint8_t *conv, double *sig0io, int64_t *redundancy) {
+static int32_t tri_impl(const rpba_block *b, const float *sig0w, int32_t robustmode, int32_t weight_only,
+                        const int32_t *part, int32_t nparts, double *XXo, uint8_t *keep, float *sig0v_out,
+                        uint8_t *conv, double *sig0io, int64_t *redundancy, float *w3d) {
   double s0io = 0.;
   long long red = 0;
   for (int pi = 0; pi < b->n_points; ++pi) {
@@ -1620,7 +1625,13 @@ extern "C" int32_t oracle_triangulate(const rpba_block *b, const float *sig0w, i
     conv[pi] = 0;
     const double Xin[3] = {(double)b->XX[3 * pi], (double)b->XX[3 * pi + 1], (double)b->XX[3 * pi + 2]};
     for (int q = 0; q < 3; ++q) XXo[3 * pi + q] = Xin[q];
+    if (w3d)
+      for (int q = 0; q < 6 * nparts; ++q) w3d[(size_t)pi * 6 * nparts + q] = 0.f;
     if (pxs <= 0) continue;
+    // partitions that see the point (pitflags)
+    std::vector<char> pit(w3d ? nparts : 0, 0);
+    if (w3d)
+      for (int j = s; j < e; ++j) pit[part[b->pt_obs_image[j]]] = 1;
     std::vector<TriObs> ob(pxs);
     std::vector<float> wx(pxs), wy(pxs), wxy(pxs), wxo(pxs), wyo(pxs), wxyo(pxs), sv(pxs), p1v(pxs), p2v(pxs),
         p3v(pxs);
@@ -1646,8 +1657,10 @@ extern "C" int32_t oracle_triangulate(const rpba_block *b, const float *sig0w, i
       s0io += sig0opt / wsum;
       red += pxs2 - 3;
     }
+    std::vector<double> Nv(w3d ? 9 * nparts : 0);
     while (iflag > -1 && iter < 101) {
       double N[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+      std::fill(Nv.begin(), Nv.end(), 0.);
       for (int js = 0; js < pxs; ++js) {
         const int j = ob[js].im;
         const float *P = &b->pmat[12 * j];
@@ -1667,7 +1680,15 @@ extern "C" int32_t oracle_triangulate(const rpba_block *b, const float *sig0w, i
         }
         for (int r = 0; r < 3; ++r)
           for (int c = 0; c < 3; ++c) N[r * 3 + c] += xp[r] * W[c] + yp[r] * W[3 + c];
+        if (w3d && nparts > 1) {
+          const int ij = part[j];
+          for (int i = 0; i < nparts; ++i)
+            if (pit[i] && i != ij)
+              for (int r = 0; r < 3; ++r)
+                for (int c = 0; c < 3; ++c) Nv[9 * i + r * 3 + c] += xp[r] * W[c] + yp[r] * W[3 + c];
+        }
       }
+      if (w3d && nparts == 1) std::copy(N, N + 9, Nv.begin());
       N[0] *= 1.001;
       N[4] *= 1.001;
       N[8] *= 1.001;
@@ -1710,6 +1731,17 @@ extern "C" int32_t oracle_triangulate(const rpba_block *b, const float *sig0w, i
         }
         sig0opt = sig0;
         cv = true;
+        if (w3d)
+          for (int i = 0; i < nparts; ++i) {
+            float *o = &w3d[((size_t)pi * nparts + i) * 6];
+            const double *M = &Nv[9 * i];
+            o[0] = (float)M[0];  // XX
+            o[1] = (float)M[4];  // YY
+            o[2] = (float)M[8];  // ZZ
+            o[3] = (float)M[1];  // XY
+            o[4] = (float)M[2];  // XZ
+            o[5] = (float)M[5];  // YZ
+          }
       } else {
         --iflag;
       }
@@ -1742,6 +1774,27 @@ extern "C" int32_t oracle_triangulate(const rpba_block *b, const float *sig0w, i
   *sig0io = s0io;
   *redundancy = red;
   return RPBA_OK;
+}
+
+extern "C" int32_t oracle_triangulate(const rpba_block *b, const float *sig0w, int32_t robustmode,
+                                      int32_t weight_only, double *XXo, uint8_t *keep, float *sig0v_out,
+                                      uint8_t *conv, double *sig0io, int64_t *redundancy) {
+  return tri_impl(b, sig0w, robustmode, weight_only, nullptr, 1, XXo, keep, sig0v_out, conv, sig0io, redundancy,
+                  nullptr);
+}
+
+/* The same with the camera partition part[image] in 0 .. nparts - 1 and
+ * the per-partition weight blocks w3d[n_points][nparts][6] (XX, YY, ZZ,
+ * XY, XZ, YZ). */
+extern "C" int32_t oracle_triangulate_parts(const rpba_block *b, const float *sig0w, int32_t robustmode,
+                                            int32_t weight_only, const int32_t *part, int32_t nparts,
+                                            double *XXo, uint8_t *keep, float *sig0v_out, uint8_t *conv,
+                                            double *sig0io, int64_t *redundancy, float *w3d) {
+  if (!part || nparts < 1 || !w3d) return RPBA_ERR_ARG;
+  for (int i = 0; i < b->n_images; ++i)
+    if (part[i] < 0 || part[i] >= nparts) return RPBA_ERR_ARG;
+  return tri_impl(b, sig0w, robustmode, weight_only, part, nparts, XXo, keep, sig0v_out, conv, sig0io, redundancy,
+                  w3d);
 }
 
 extern "C" {
