@@ -296,7 +296,7 @@ int32_t rpba_float_sequential_sum_noalloc(const float *d_v, int64_t n, float *d_
  * Outputs per point: the refined point (XX_out, 3 doubles; the input when the
  * point did not converge) and conv; per track entry (pt_obs_off order): keep
  * and sig0v; totals: sig0io and redundancy as the reference accumulates them.
- * The per-partition weight blocks (wxyflag) are not computed. */
+ * rpba_triangulate_parts below also forms the per-partition weight blocks. */
 typedef struct rpba_tri_options {
   int32_t robustmode;   /* 0, 1 or 2                                        */
   int32_t weight_only;  /* weightonlyflag                                   */
@@ -304,6 +304,18 @@ typedef struct rpba_tri_options {
 } rpba_tri_options;
 int32_t rpba_triangulate(const rpba_block *blk, const float *sig0w, const rpba_tri_options *opt, double *XX_out,
                          uint8_t *keep, float *sig0v, uint8_t *conv, double *sig0io, int64_t *redundancy);
+
+/* rpba_triangulate with the camera partition of the parallel RPBA
+ * (part[image] in 0 .. nparts - 1, e.g. from rpba_partition_images): also the
+ * per-partition weight blocks CalcLSAXMulti forms with wxyflag
+ * (rpbacore.cpp:579-590, 612-622, 663-672, the w3dvivv of rpbacore.cpp:
+ * 370-380): w3d[n_points][nparts][6] = (XX, YY, ZZ, XY, XZ, YZ) of the
+ * normal matrix of the point's observations outside partition i, for every
+ * partition i that sees the point (one partition: all observations),
+ * undamped, from the accepted iteration; zero elsewhere. */
+int32_t rpba_triangulate_parts(const rpba_block *blk, const float *sig0w, const rpba_tri_options *opt,
+                               const int32_t *part, int32_t nparts, double *XX_out, uint8_t *keep, float *sig0v,
+                               uint8_t *conv, double *sig0io, int64_t *redundancy, float *w3d);
 
 /* Camera partition of the reference's parallel RPBA: replaces
  * PartitionpointXXv (rpbacore.cpp:945-1037), which cuts the images'

@@ -9,10 +9,11 @@ from .block import (Block, RpbaBlockC, RpbaOptionsC, RpbaReportC, make_options, 
                     SOLVER_PCG, SOLVER_DIRECT, SOLVER_LEARNED, PREC_FP64, PREC_MIXED)
 from .lib import (InputBlock, OutputBlock, CalcPLSA, Solver, RpbaError, load, LIB_PATH,
                   EXPORTS, STATUS, float_sequential_sum, train_preconditioner,
-                  precond_loss_grad, record_systems, solve_batch, triangulate, partition_images)
+                  precond_loss_grad, record_systems, solve_batch, triangulate, triangulate_parts,
+                  partition_images)
 
 __all__ = ["Block", "RpbaBlockC", "RpbaOptionsC", "RpbaReportC", "make_options", "PRECOND_WEIGHTS", "SOLVER_PCG",
            "SOLVER_DIRECT", "SOLVER_LEARNED", "PREC_FP64", "PREC_MIXED", "InputBlock",
            "OutputBlock", "CalcPLSA", "Solver", "RpbaError", "load", "LIB_PATH", "EXPORTS",
            "STATUS", "float_sequential_sum", "train_preconditioner", "precond_loss_grad",
-           "record_systems", "solve_batch", "triangulate", "partition_images"]
+           "record_systems", "solve_batch", "triangulate", "triangulate_parts", "partition_images"]

@@ -11,8 +11,11 @@
 // temporaries of a point live in scratch arrays indexed by track entry.
 // This file is compiled without FMA contraction and keeps the reference's
 // operation order, so its results equal the CPU restatement's bit for bit.
-// The per-partition weight blocks of the reference (wxyflag) feed only its
-// partitioned merge and are not computed.
+// With a camera partition (rpba_triangulate_parts) the reference's
+// per-partition weight blocks (wxyflag) are formed as well: for every
+// partition that sees the point, the normal matrix of the point's
+// observations in the other partitions (track order, one partition: all of
+// them, undamped), taken at the start of the accepted iteration.
 #include <cstring>
 #include <vector>
 
@@ -26,12 +29,18 @@ namespace {
 struct TriIn {
   const float *pmat, *K, *dist, *XX, *xg, *wx, *wy, *wxy, *sig0w;
   const int *img_off, *pt_off, *pt_img, *pt_slot;
-  int np, robustmode, weight_only;
+  const int *part;  // image -> partition (weight blocks), or null
+  int np, robustmode, weight_only, nparts;
 };
 struct TriScratch {
   float *wx, *wy, *wxy, *p1, *p2, *p3;
   double *corr, *Bw;  // [2 x entry], [6 x entry]
   uint8_t *del;
+  // weight blocks: the derivative rows [6 x entry]; the distinct partitions
+  // of a point and their pending blocks, in the point's first entries
+  double *Bxy;
+  int *dpart;
+  float *wt;  // [6 x entry]
 };
 struct TriOut {
   double *XX;
@@ -39,6 +48,7 @@ struct TriOut {
   float *sig0v;
   double *s0;   // per point contribution to sig0io
   int *red;     // per point contribution to the redundancy
+  float *w3d;   // [np x nparts x 6] (XX, YY, ZZ, XY, XZ, YZ), or null
 };
 
 __device__ void tri_corr(const TriIn &I, const TriScratch &S, int s, int e, double X0, double X1, double X2,
@@ -102,7 +112,18 @@ __global__ void k_triangulate(TriIn I, TriScratch S, TriOut O) {
   O.s0[pi] = 0.;
   O.red[pi] = 0;
   for (int t = s; t < e; ++t) O.keep[t] = 0;
+  if (O.w3d)
+    for (int q = 0; q < 6 * I.nparts; ++q) O.w3d[(size_t)pi * 6 * I.nparts + q] = 0.f;
   if (pxs <= 0) return;
+  // the partitions that see the point, in order of first appearance
+  int nd = 0;
+  if (O.w3d && I.nparts > 1)
+    for (int t = s; t < e; ++t) {
+      const int q = I.part[I.pt_img[t]];
+      bool seen = false;
+      for (int u = 0; u < nd; ++u) seen = seen || S.dpart[s + u] == q;
+      if (!seen) S.dpart[s + nd++] = q;
+    }
   float wsum = 0.f;
   for (int t = s; t < e; ++t) {
     const int sl = I.img_off[I.pt_img[t]] + I.pt_slot[t];
@@ -145,6 +166,41 @@ __global__ void k_triangulate(TriIn I, TriScratch S, TriOut O) {
       }
       for (int r = 0; r < 3; ++r)
         for (int c = 0; c < 3; ++c) N[r * 3 + c] += xp[r] * W[c] + yp[r] * W[3 + c];
+      if (O.w3d)
+        for (int c = 0; c < 3; ++c) {
+          S.Bxy[6 * (size_t)t + c] = xp[c];
+          S.Bxy[6 * (size_t)t + 3 + c] = yp[c];
+        }
+    }
+    // pending weight blocks of this iteration (kept if it is accepted)
+    if (O.w3d) {
+      if (I.nparts == 1) {
+        float *o = S.wt + 6 * (size_t)s;
+        o[0] = (float)N[0];
+        o[1] = (float)N[4];
+        o[2] = (float)N[8];
+        o[3] = (float)N[1];
+        o[4] = (float)N[2];
+        o[5] = (float)N[5];
+      } else {
+        for (int u = 0; u < nd; ++u) {
+          const int q = S.dpart[s + u];
+          double M[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
+          for (int t = s; t < e; ++t) {
+            if (I.part[I.pt_img[t]] == q) continue;
+            const double *xp = S.Bxy + 6 * (size_t)t, *yp = xp + 3, *W = S.Bw + 6 * (size_t)t;
+            for (int r = 0; r < 3; ++r)
+              for (int c = 0; c < 3; ++c) M[r * 3 + c] += xp[r] * W[c] + yp[r] * W[3 + c];
+          }
+          float *o = S.wt + 6 * (size_t)(s + u);
+          o[0] = (float)M[0];
+          o[1] = (float)M[4];
+          o[2] = (float)M[8];
+          o[3] = (float)M[1];
+          o[4] = (float)M[2];
+          o[5] = (float)M[5];
+        }
+      }
     }
     N[0] *= 1.001;
     N[4] *= 1.001;
@@ -189,6 +245,14 @@ __global__ void k_triangulate(TriIn I, TriScratch S, TriOut O) {
       }
       sig0opt = sig0;
       cv = true;
+      if (O.w3d) {
+        const int n = I.nparts == 1 ? 1 : nd;
+        for (int u = 0; u < n; ++u) {
+          const int q = I.nparts == 1 ? 0 : S.dpart[s + u];
+          for (int k = 0; k < 6; ++k)
+            O.w3d[((size_t)pi * I.nparts + q) * 6 + k] = S.wt[6 * (size_t)(s + u) + k];
+        }
+      }
     } else {
       --iflag;
     }
@@ -227,9 +291,9 @@ __global__ void k_triangulate(TriIn I, TriScratch S, TriOut O) {
 
 using namespace rpba;
 
-extern "C" int32_t rpba_triangulate(const rpba_block *b, const float *sig0w, const rpba_tri_options *opt,
-                                    double *XX_out, uint8_t *keep, float *sig0v, uint8_t *conv, double *sig0io,
-                                    int64_t *redundancy) {
+static int32_t triangulate_impl(const rpba_block *b, const float *sig0w, const rpba_tri_options *opt,
+                                const int32_t *part, int32_t nparts, double *XX_out, uint8_t *keep, float *sig0v,
+                                uint8_t *conv, double *sig0io, int64_t *redundancy, float *w3d) {
   if (!b || !opt || !XX_out || !keep || !sig0v || !conv || !sig0io || !redundancy) return RPBA_ERR_ARG;
   if (opt->robustmode < 0 || opt->robustmode > 2 || (opt->robustmode == 2 && !sig0w)) return RPBA_ERR_ARG;
   int ndev = 0;
@@ -284,6 +348,8 @@ extern "C" int32_t rpba_triangulate(const rpba_block *b, const float *sig0w, con
     I.np = np;
     I.robustmode = opt->robustmode;
     I.weight_only = opt->weight_only != 0;
+    I.part = w3d ? (const int *)up(part, sizeof(int) * nc) : nullptr;
+    I.nparts = w3d ? nparts : 1;
     TriScratch S;
     S.wx = (float *)dev(sizeof(float) * ntr);
     S.wy = (float *)dev(sizeof(float) * ntr);
@@ -294,6 +360,9 @@ extern "C" int32_t rpba_triangulate(const rpba_block *b, const float *sig0w, con
     S.corr = (double *)dev(sizeof(double) * 2 * ntr);
     S.Bw = (double *)dev(sizeof(double) * 6 * ntr);
     S.del = (uint8_t *)dev(ntr);
+    S.Bxy = w3d ? (double *)dev(sizeof(double) * 6 * ntr) : nullptr;
+    S.dpart = w3d ? (int *)dev(sizeof(int) * ntr) : nullptr;
+    S.wt = w3d ? (float *)dev(sizeof(float) * 6 * ntr) : nullptr;
     TriOut O;
     O.XX = (double *)dev(sizeof(double) * 3 * np);
     O.keep = (uint8_t *)dev(ntr);
@@ -301,6 +370,7 @@ extern "C" int32_t rpba_triangulate(const rpba_block *b, const float *sig0w, con
     O.sig0v = (float *)dev(sizeof(float) * ntr);
     O.s0 = (double *)dev(sizeof(double) * np);
     O.red = (int *)dev(sizeof(int) * np);
+    O.w3d = w3d ? (float *)dev(sizeof(float) * 6 * (size_t)nparts * np) : nullptr;
     if (np > 0) k_triangulate<<<(np + 127) / 128, 128, 0, s>>>(I, S, O);
     RPBA_CUDA_CHECK(cudaGetLastError());
     std::vector<double> s0(np);
@@ -314,6 +384,7 @@ extern "C" int32_t rpba_triangulate(const rpba_block *b, const float *sig0w, con
     down(sig0v, O.sig0v, sizeof(float) * ntr);
     down(s0.data(), O.s0, sizeof(double) * np);
     down(red.data(), O.red, sizeof(int) * np);
+    if (w3d) down(w3d, O.w3d, sizeof(float) * 6 * (size_t)nparts * np);
     RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
     // the reference accumulates these over the points in order
     double a = 0.;
@@ -328,4 +399,20 @@ extern "C" int32_t rpba_triangulate(const rpba_block *b, const float *sig0w, con
     return RPBA_ERR_CUDA;
   }
   return RPBA_OK;
+}
+
+extern "C" int32_t rpba_triangulate(const rpba_block *b, const float *sig0w, const rpba_tri_options *opt,
+                                    double *XX_out, uint8_t *keep, float *sig0v, uint8_t *conv, double *sig0io,
+                                    int64_t *redundancy) {
+  return triangulate_impl(b, sig0w, opt, nullptr, 1, XX_out, keep, sig0v, conv, sig0io, redundancy, nullptr);
+}
+
+extern "C" int32_t rpba_triangulate_parts(const rpba_block *b, const float *sig0w, const rpba_tri_options *opt,
+                                          const int32_t *part, int32_t nparts, double *XX_out, uint8_t *keep,
+                                          float *sig0v, uint8_t *conv, double *sig0io, int64_t *redundancy,
+                                          float *w3d) {
+  if (!b || !part || nparts < 1 || !w3d) return RPBA_ERR_ARG;
+  for (int i = 0; i < b->n_images; ++i)
+    if (part[i] < 0 || part[i] >= nparts) return RPBA_ERR_ARG;
+  return triangulate_impl(b, sig0w, opt, part, nparts, XX_out, keep, sig0v, conv, sig0io, redundancy, w3d);
 }

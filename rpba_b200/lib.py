@@ -39,7 +39,7 @@ EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block
            "rpba_get_state", "rpba_get_log", "rpba_exteval", "rpba_kernel_stats", "rpba_float_sequential_sum",
            "rpba_float_sequential_sum_noalloc", "rpba_train_preconditioner",
            "rpba_set_preconditioner", "rpba_precond_loss_grad", "rpba_record_systems", "rpba_solve_batch",
-           "rpba_triangulate", "rpba_partition_images", "rpba_destroy")
+           "rpba_triangulate", "rpba_triangulate_parts", "rpba_partition_images", "rpba_destroy")
 
 _lib = None
 
@@ -98,6 +98,11 @@ def load():
     L.rpba_solve_batch.argtypes = [bp, C.c_int32, op, C.c_int32, rp, C.POINTER(C.c_int32),
                                    C.POINTER(RpbaBatchReportC)]
     L.rpba_solve_batch.restype = C.c_int32
+    L.rpba_triangulate_parts.argtypes = [bp, C.POINTER(C.c_float), C.POINTER(RpbaTriOptionsC),
+                                         C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_double),
+                                         C.POINTER(C.c_uint8), C.POINTER(C.c_float), C.POINTER(C.c_uint8),
+                                         C.POINTER(C.c_double), C.POINTER(C.c_int64), C.POINTER(C.c_float)]
+    L.rpba_triangulate_parts.restype = C.c_int32
     L.rpba_partition_images.argtypes = [bp, C.c_int32, C.POINTER(C.c_int32)]
     L.rpba_partition_images.restype = C.c_int32
     L.rpba_triangulate.argtypes = [bp, C.POINTER(C.c_float), C.POINTER(RpbaTriOptionsC), C.POINTER(C.c_double),
@@ -213,6 +218,33 @@ def triangulate(block: Block, sig0w=None, robustmode: int = 0, weight_only: bool
     if st != 0:
         raise RpbaError(st, "rpba_triangulate")
     out["XX"] = out["XX"].reshape(np_, 3)
+    out["sig0io"], out["redundancy"] = s0.value, red.value
+    return out
+
+
+def triangulate_parts(block: Block, part, nparts: int, sig0w=None, robustmode: int = 0,
+                      weight_only: bool = False, device: int = 0) -> dict:
+    """rpba_triangulate with the camera partition ``part`` (image -> 0 ..
+    nparts - 1): also the per-partition weight blocks ``w3d`` (n_points x
+    nparts x 6: XX, YY, ZZ, XY, XZ, YZ)."""
+    cb = block.as_c()
+    nt, np_ = block.n_obs, block.n_points
+    part = np.ascontiguousarray(part, np.int32)
+    out = {"XX": np.zeros(3 * np_), "keep": np.zeros(nt, np.uint8), "sig0v": np.zeros(nt, np.float32),
+           "conv": np.zeros(np_, np.uint8), "w3d": np.zeros(np_ * nparts * 6, np.float32)}
+    s0, red = C.c_double(), C.c_int64()
+    w = None if sig0w is None else np.ascontiguousarray(sig0w, np.float32)
+    o = RpbaTriOptionsC(int(robustmode), int(weight_only), int(device))
+    st = load().rpba_triangulate_parts(
+        C.byref(cb), None if w is None else w.ctypes.data_as(C.POINTER(C.c_float)), C.byref(o),
+        part.ctypes.data_as(C.POINTER(C.c_int32)), int(nparts), out["XX"].ctypes.data_as(C.POINTER(C.c_double)),
+        out["keep"].ctypes.data_as(C.POINTER(C.c_uint8)), out["sig0v"].ctypes.data_as(C.POINTER(C.c_float)),
+        out["conv"].ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(s0), C.byref(red),
+        out["w3d"].ctypes.data_as(C.POINTER(C.c_float)))
+    if st != 0:
+        raise RpbaError(st, "rpba_triangulate_parts")
+    out["XX"] = out["XX"].reshape(np_, 3)
+    out["w3d"] = out["w3d"].reshape(np_, nparts, 6)
     out["sig0io"], out["redundancy"] = s0.value, red.value
     return out
 

@@ -38,3 +38,23 @@ def test_triangulation_matches_oracle(oracle_mod, scene, mode, weight_only):
     assert g["sig0io"] == o["sig0io"]
     if mode == 2 and not weight_only:
         assert (g["keep"] == 0).any()
+
+
+@pytest.mark.parametrize("mode,weight_only,k", [(0, False, 3), (2, False, 4), (0, True, 3), (0, False, 1)])
+def test_weight_blocks_match_oracle(oracle_mod, scene, mode, weight_only, k):
+    """The per-partition weight blocks (rpba_triangulate_parts) against the
+    oracle's, bit for bit, with the partition of rpba_partition_images; the
+    other outputs equal rpba_triangulate's."""
+    import rpba_b200 as rb
+    part = rb.partition_images(scene, k)
+    sig0w = None
+    if mode == 2:
+        sig0w = _thresholds(scene, oracle_mod.triangulate(scene, robustmode=1)["sig0v"])
+    g = rb.triangulate_parts(scene, part, k, sig0w, mode, weight_only)
+    o = oracle_mod.triangulate_parts(scene, part, k, sig0w, mode, weight_only)
+    assert np.array_equal(g["w3d"], o["w3d"])
+    assert (g["w3d"] != 0).any()
+    plain = rb.triangulate(scene, sig0w, mode, weight_only)
+    for name in ("XX", "keep", "sig0v", "conv"):
+        assert np.array_equal(g[name], plain[name]), name
+    assert g["redundancy"] == plain["redundancy"] and g["sig0io"] == plain["sig0io"]
