@@ -146,6 +146,27 @@ def triangulate_parts(block: Block, part, nparts: int, sig0w=None, robustmode: i
     return out
 
 
+def lsa_gcp_step(block: Block, gcpinfo, W3, gcpdata, ncam_total: int, opts: RpbaOptionsC | None = None,
+                 log_cap: int = 1 << 16):
+    """One GCP-mode step of the LSA on ``block`` (modified in place): the
+    parallel RPBA's per-partition call.  gcpinfo: per point, GCP index or
+    -1; W3: (n_gcp_kept, 6) float weights; gcpdata: (n_gcp, 3) doubles."""
+    cb = block.as_c()
+    o = opts if opts is not None else make_options()
+    gi = np.ascontiguousarray(gcpinfo, np.int32)
+    w3 = np.ascontiguousarray(W3, np.float32).reshape(-1)
+    gd = np.ascontiguousarray(gcpdata, np.float64).reshape(-1)
+    buf = C.create_string_buffer(log_cap)
+    f = lib().oracle_lsa_gcp_step
+    f.restype = C.c_int32
+    f.argtypes = [C.POINTER(RpbaBlockC), C.POINTER(RpbaOptionsC), C.POINTER(C.c_int32), C.POINTER(C.c_float),
+                  C.POINTER(C.c_double), C.c_int32, C.c_char_p, C.c_size_t]
+    st = f(C.byref(cb), C.byref(o), gi.ctypes.data_as(C.POINTER(C.c_int32)),
+           w3.ctypes.data_as(C.POINTER(C.c_float)), gd.ctypes.data_as(C.POINTER(C.c_double)), int(ncam_total),
+           buf, log_cap)
+    return st, buf.value.decode()
+
+
 def input_block(path: str, k24out: bool = True) -> Block:
     cb = RpbaBlockC()
     st = lib().oracle_input_block(path.encode(), 3, int(k24out), C.byref(cb))

@@ -275,9 +275,29 @@ struct Opts {
   int max_lm = -1;
 };
 
+/* GCP mode of the LSA (gcpflag / aoflag, rbacore.cpp:36-125, 233-329): the
+ * per-partition LSA of the parallel RPBA.  Every camera of the block is
+ * free (no gauge camera, nrioff = nrpari * nrimages); points shared with
+ * other partitions carry a 3-D prior (CalcDerivatives3DGCP,
+ * rbacore.cpp:1677-1729).  gcpinfo: per block point, its GCP index (into
+ * gcpdata) or -1; W3: 6 weights (XX, YY, ZZ, XY, XZ, YZ) per GCP point of
+ * this LSA, in the order the LSA keeps its points (the W3ijit of the
+ * reference); ncam_total: the scene's camera count (the reference's
+ * nrcameras, which enters the unknown count). */
+struct GcpIn {
+  const int32_t *gcpinfo;
+  const float *W3;
+  const double *gcpdata;
+  int ncam_total;
+};
+
 class LSA {
  public:
   LSA(const rpba_block *blk, const Opts &o, std::string *os);
+  LSA(const rpba_block *blk, const Opts &o, std::string *os, const GcpIn &g);
+  /* Adjust(false, os, true, 0, W3, true, gcpdata), rbacore.cpp:333-616: one
+   * damped step in GCP mode, stored unconditionally. */
+  int adjust_gcp_step();
   /* rbacore.cpp:333-616; returns an rpba_status. */
   int adjust(rpba_report *rep);
   /* OutputLSAc, rbacore.cpp:644-666 + PointXXvOut rbacore.cpp:1978-2010. */
@@ -345,6 +365,14 @@ class LSA {
   std::vector<std::vector<double>> Dg, rhs;
   std::vector<std::map<int, std::vector<double>, std::greater<int>>> Off;
 
+  /* GCP mode */
+  bool ao = false;
+  int ncam_total = 0, nrgcp = 0, nrobsao = 0;
+  std::vector<int> gcpi;       /* per kept point: GCP index or -1       */
+  const float *W3 = nullptr;   /* 6 per GCP point in gcpnum order       */
+  const double *gdata = nullptr;
+  float sig0ao = 0.f, wsumao = 0.f, sig0aoi = 0.f, sig0aoiold = 0.f;
+
   /* per point scratch */
   double Vp[9], Vpi[9], gp[3];
   std::vector<std::vector<double>> Wl; /* eNlij per track obs (n x 3) */
@@ -373,7 +401,14 @@ class LSA {
               double *Bp) const;
 };
 
-LSA::LSA(const rpba_block *blk, const Opts &o, std::string *os_) : b(blk), opt(o), os(os_) {
+LSA::LSA(const rpba_block *blk, const Opts &o, std::string *os_)
+    : LSA(blk, o, os_, GcpIn{nullptr, nullptr, nullptr, 0}) {}
+
+LSA::LSA(const rpba_block *blk, const Opts &o, std::string *os_, const GcpIn &g) : b(blk), opt(o), os(os_) {
+  ao = g.gcpinfo != nullptr;
+  W3 = g.W3;
+  gdata = g.gcpdata;
+  ncam_total = g.ncam_total;
   nimg = blk->n_images;
   XXnr = blk->n_points;
   nadd = (int)o.addf[0] + (int)o.addf[1] + (int)o.addf[2];
@@ -388,7 +423,9 @@ LSA::LSA(const rpba_block *blk, const Opts &o, std::string *os_) : b(blk), opt(o
   P.resize(12 * nimg);
   for (int i = 0; i < 12 * nimg; ++i) P[i] = (double)blk->pmat[i];
 
-  /* PointXXvIn, rbacore.cpp:1918-1974 (all images selected, no GCPs) */
+  /* PointXXvIn, rbacore.cpp:1918-1974 (all images of the block selected);
+   * in GCP mode a GCP point is kept with a single observation, if its GCP
+   * index is above 0 (the reference's test is gcpinfoin[i] > 0) */
   toff.push_back(0);
   for (int i = 0; i < XXnr; ++i) {
     const int s = blk->pt_obs_off[i], e = blk->pt_obs_off[i + 1];
@@ -396,8 +433,12 @@ LSA::LSA(const rpba_block *blk, const Opts &o, std::string *os_) : b(blk), opt(o
     for (int j = s; j < e; ++j)
       if (blk->pt_obs_image[j] > -1) ++n;
     const double Z = (double)blk->XX[3 * i + 2];
-    if (std::fabs(Z) > 1.e-8 && n >= minimagenr) {
+    if (std::fabs(Z) > 1.e-8 && (n >= minimagenr || (ao && g.gcpinfo[i] > 0 && n > 0))) {
       nrpv.push_back(i);
+      if (ao) {
+        gcpi.push_back(g.gcpinfo[i]);
+        if (g.gcpinfo[i] > -1) ++nrgcp;
+      }
       for (int j = s; j < e; ++j)
         if (blk->pt_obs_image[j] > -1) {
           timg.push_back(blk->pt_obs_image[j]);
@@ -413,6 +454,7 @@ LSA::LSA(const rpba_block *blk, const Opts &o, std::string *os_) : b(blk), opt(o
   XXnew = XX;
 
   prepare_cameras();
+  if (ao) normcamera = -1; /* rbacore.cpp:697-698 */
 
   /* PrepareIteration, rbacore.cpp:127-229 */
   camparv.assign(nimg + 2, 0);
@@ -442,12 +484,12 @@ LSA::LSA(const rpba_block *blk, const Opts &o, std::string *os_) : b(blk), opt(o
       lflflag = true;
       break;
     }
-  nrioff = nadd + nrparir + nrpari * (nimg - 2);
+  nrioff = ao ? nrpari * nimg : nadd + nrparir + nrpari * (nimg - 2);
   sig00v.assign(nimg, 0.f);
   const int xpmsize = nimg * 6 + 3 * XXnr + 7 * nimg;
   XPM.assign(xpmsize, 0.);
   XPMn.assign(xpmsize, 0.);
-  if (nimg < 2 || normcamera < 1) bad_setup = 1;
+  if (nimg < 1 || (!ao && (nimg < 2 || normcamera < 1))) bad_setup = 1;
 }
 
 /* PrepareCameras, rbacore.cpp:670-700: normcamera = image whose R*t is
@@ -470,9 +512,31 @@ void LSA::prepare_cameras() {
   }
 }
 
-/* EncodeCameras, rbacore.cpp:999-1087 (aoflag false). */
+/* EncodeCameras, rbacore.cpp:999-1087. */
 void LSA::encode_cameras() {
   for (int k = 0; k < nimg + 1; ++k) camparv[k] = 0;
+  if (ao) {
+    /* every camera free, rotation, PC and the additional parameters */
+    camparv[1] = nrpari;
+    for (int k = 0; k < nimg; ++k) {
+      const int cp = camparv[k];
+      double *p = &P[12 * k];
+      rectify(p, 4);
+      double *R = &Rb[9 * k];
+      for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) R[r * 3 + c] = p[r * 4 + c];
+      for (int i = 0; i < 3; ++i)
+        PCb[3 * k + i] = R[0 * 3 + i] * p[3] + R[1 * 3 + i] * p[7] + R[2 * 3 + i] * p[11];
+      for (int i = 0; i < 6; ++i) XPM[cp + i] = 0.;
+      int a = 5 + cp;
+      if (opt.addf[0]) XPM[++a] = dc[2 * k];
+      if (opt.addf[1]) XPM[++a] = dc[2 * k + 1];
+      if (opt.addf[2]) XPM[++a] = Kc[9 * k];
+      camparv[k + 2] = camparv[k + 1] + nrpari;
+    }
+    nrioff3 = nrioff + 3 * nrpts;
+    return;
+  }
   camparv[1] = nadd;
   int addp = -1;
   if (opt.addf[0]) XPM[++addp] = dc[0];
@@ -519,9 +583,9 @@ void LSA::encode_cameras() {
   nrioff3 = nrioff + 3 * nrpts;
 }
 
-/* DecodeCameras, rbacore.cpp:1733-1800 (aoflag false). */
+/* DecodeCameras, rbacore.cpp:1733-1800. */
 void LSA::decode_cameras(const std::vector<double> &XM) {
-  for (int k = 1; k < nimg; ++k) {
+  for (int k = ao ? 0 : 1; k < nimg; ++k) {
     const int cp = camparv[k];
     double Ra[9];
     cayley(XM[cp], XM[cp + 1], XM[cp + 2], Ra);
@@ -546,6 +610,7 @@ void LSA::decode_cameras(const std::vector<double> &XM) {
     if (opt.addf[2]) Kn[9 * k] = Kn[9 * k + 4] = XM[++a + cp];
     Kn[9 * k + 8] = 1.;
   }
+  if (ao) return;
   int a = -1;
   if (opt.addf[0]) dn[0] = XM[++a];
   if (opt.addf[1]) dn[1] = XM[++a];
@@ -767,7 +832,7 @@ void LSA::derivs(const ObsEval &e, int k, const float *w, double *Bc, int *ncols
     ic1[ni] = -e.ex3u[1];
     ++ni;
   }
-  if (k == 0) {
+  if (k == 0 && !ao) {
     for (int j = 0; j < ni; ++j) {
       Bc[j] = ic0[j];
       Bc[9 + j] = ic1[j];
@@ -819,6 +884,7 @@ void LSA::calc_corrections(bool solveflag, double multfact1, const std::vector<d
                            bool srmvflag, bool derivflag) {
   sig0 = 0.f;
   int kkk = nrioff - 1;
+  int gcpnum = 0;
   for (int i = 0; i < nrpts; ++i) {
     if (derivflag) {
       for (int j = 0; j < 9; ++j) Vp[j] = 0.;
@@ -888,6 +954,22 @@ void LSA::calc_corrections(bool solveflag, double multfact1, const std::vector<d
         if (srmvflag) sig0rmv[o] = rval;
         sig0 += val;
       }
+    }
+    if (ao && gcpi[i] > -1) {
+      /* CalcDerivatives3DGCP, rbacore.cpp:1677-1729: the 3-D prior of a
+       * shared point, diff = gcp - X, B = -I */
+      const float *w = &W3[6 * gcpnum];
+      const double *gx = &gdata[3 * gcpi[i]];
+      const double d1 = gx[0] - XXnew[3 * i], d2 = gx[1] - XXnew[3 * i + 1], d3 = gx[2] - XXnew[3 * i + 2];
+      sig0ao += (float)(d1 * d1 * w[0] + d2 * d2 * w[1] + d3 * d3 * w[2] +
+                        2 * (d1 * d2 * w[3] + d1 * d3 * w[4] + d2 * d3 * w[5]));
+      if (derivflag) {
+        const double Wm[9] = {w[0], w[3], w[4], w[3], w[1], w[5], w[4], w[5], w[2]};
+        for (int r = 0; r < 3; ++r)
+          for (int c = 0; c < 3; ++c) Vp[r * 3 + c] += Wm[r * 3 + c];
+        for (int r = 0; r < 3; ++r) gp[r] += (-Wm[r * 3]) * d1 + (-Wm[r * 3 + 1]) * d2 + (-Wm[r * 3 + 2]) * d3;
+      }
+      ++gcpnum;
     }
     if (derivflag) {
       for (int j = 0; j < 3; ++j) Vp[j * 3 + j] *= multfact1;
@@ -1190,7 +1272,8 @@ void LSA::direct_solve() {
 
 /* CalcBundleSep, rbacore.cpp:1094-1195. */
 bool LSA::calc_bundle_sep(double multfact) {
-  begini = nadd > 0 ? 0 : 1;
+  begini = (ao || nadd > 0) ? 0 : 1;
+  sig0ao = 0.f;
   const double multfact1 = 1. + multfact;
   if (iniflag) {
     Dg.assign(nimg, {});
@@ -1350,6 +1433,79 @@ int LSA::adjust(rpba_report *rep) {
     rep->linear_solves = solves;
     rep->pcg_iterations = pcg_iters;
   }
+  return RPBA_OK;
+}
+
+/* Adjust(robust = false, itbreakflag = true, itmaxnum = 0, W3, gcp = true,
+ * gcpdata), rbacore.cpp:333-616, the per-partition call of the parallel
+ * RPBA (rpbacore.cpp:229): the GCP weights PrepareWeights3D sums
+ * (rbacore.cpp:787-818), the cost with the priors, one damped step
+ * (multfact 1e-4) stored unconditionally (iter == 1), the Sigma0 and
+ * Sigma0AO lines.  As in the reference, sig0ao is reset only where
+ * CalcBundleSep and the first cost evaluation reset it, so the printed
+ * post-step value accumulates the three evaluations since the reset. */
+int LSA::adjust_gcp_step() {
+  if (bad_setup) return RPBA_ERR_ARG;
+  iniflag = true;
+  const double multfact = 1.e-4;
+  sig0aoi = sig0aoiold = 1.e20f;
+  float sig0aoin = 1.e20f;
+  imagepointnr = toff[nrpts];
+  nrobs = 2 * imagepointnr;
+  nrobsao = 3 * nrgcp;
+  nrobs += nrobsao;
+  std::vector<int> cnt(nimg, 0);
+  for (int o = 0; o < imagepointnr; ++o) ++cnt[timg[o]];
+  for (int i = 0; i < nimg; ++i)
+    if (cnt[i] == 0) {
+      if (nimg > 3) *os += "BA-Error: No observations in image " + std::to_string(i) + " (image index)\n";
+      return RPBA_ERR_NO_OBS_IMAGE;
+    }
+  isflag.assign(imagepointnr, 0);
+  isflagnew.assign(imagepointnr, 0);
+  prepare_weights(0);
+  wsumao = 0.f;
+  for (int i = 0; i < nrgcp; ++i) wsumao += W3[6 * i] + W3[6 * i + 1] + W3[6 * i + 2];
+  wsumg = (float)(2 * imagepointnr + nrobsao) / (wsumao + wsum);
+  wsumao = (float)nrobsao / wsumao;
+  wsum = (float)(2 * imagepointnr) / wsum;
+  for (int i = 0; i < nrpts; ++i)
+    for (int j = 0; j < 3; ++j) XPM[nrioff + i * 3 + j] = XX[3 * i + j];
+  encode_cameras();
+  nrunknowns = nrioff3 + nadd * ncam_total;
+  XXnew = XX;
+  x.assign(nrunknowns, 0.);
+  redundancy = nrobs - nrunknowns;
+  if (redundancy < 0) {
+    if (nimg > 3) *os += "BA-Error: Low redundancy\n";
+    return RPBA_ERR_LOW_REDUNDANCY;
+  }
+  sig0rmv.assign(imagepointnr, 0.f);
+  decode_cameras(XPM);
+  sig0ao = 0.f;
+  calc_corrections(false, 1. + multfact, XPM, true, false);
+  sig0aoi = sig0 * wsumg / (float)redundancy;
+  sig0aoin = sig0aoi;
+  sig0 = (sig0 + sig0ao) * wsumg / (float)(redundancy + nrobsao - 7);
+  sig0in = sig0old = sig0;
+  if (calc_bundle_sep(multfact)) return status;
+  for (int i = 0; i < nrunknowns; ++i) {
+    if (!std::isfinite(x[i])) return RPBA_ERR_NAN_STEP;
+    XPMn[i] = XPM[i] - x[i];
+  }
+  decode_cameras(XPMn);
+  calc_corrections(false, 1. + multfact, XPMn, true, false);
+  sig0aoi = sig0 * wsumg / (float)redundancy;
+  sig0 = (sig0 + sig0ao) * wsumg / (float)(redundancy + nrobsao - 7);
+  store_results();
+  sig0old = sig0;
+  sig0aoiold = sig0aoi;
+  const float s_in = std::sqrt(sig0in * ihw2), s_out = std::sqrt(sig0old * ihw2);
+  *os += "Sigma0: " + fmt_g(std::sqrt(sig0aoin * ihw2)) + ' ' + fmt_g(std::sqrt(sig0aoiold * ihw2)) + "  " +
+         std::to_string(redundancy) + ' ' + std::to_string(nrobs) + ' ' + std::to_string(nrunknowns) +
+         "  IT: 0  ITT: 0\n";
+  *os += "Sigma0AO: " + fmt_g(std::sqrt(sig0ao * wsumao / (float)(nrobsao - 7))) + "  " + fmt_g(s_in) + ' ' +
+         fmt_g(s_out) + "  " + std::to_string(nrobsao) + " " + fmt_g(wsumao) + '\n';
   return RPBA_OK;
 }
 
@@ -1781,6 +1937,27 @@ extern "C" int32_t oracle_triangulate(const rpba_block *b, const float *sig0w, i
                                       uint8_t *conv, double *sig0io, int64_t *redundancy) {
   return tri_impl(b, sig0w, robustmode, weight_only, nullptr, 1, XXo, keep, sig0v_out, conv, sig0io, redundancy,
                   nullptr);
+}
+
+/* One GCP-mode step of the LSA on a block (the parallel RPBA's
+ * per-partition call; the block holds the partition's images and the
+ * observations in them): gcpinfo per point (GCP index or -1), W3 (6 per GCP
+ * point the LSA keeps, in point order), gcpdata (3 per GCP index), the
+ * scene's camera count.  The cameras (pmat, K, distpara), the points and the
+ * point lists of the block are replaced by the LSA's output.  Robust is off,
+ * as in the reference's call. */
+extern "C" int32_t oracle_lsa_gcp_step(rpba_block *blk, const rpba_options *o, const int32_t *gcpinfo,
+                                       const float *W3, const double *gcpdata, int32_t ncam_total, char *log,
+                                       size_t cap) {
+  if (!blk || !o || !gcpinfo || !gcpdata || ncam_total < blk->n_images) return RPBA_ERR_ARG;
+  std::string os;
+  Opts op = make_opts(o);
+  op.robust = false;
+  LSA lsa(blk, op, &os, GcpIn{gcpinfo, W3, gcpdata, ncam_total});
+  const int st = lsa.adjust_gcp_step();
+  if (st == RPBA_OK) lsa.output(blk);
+  copy_log(os, log, cap);
+  return st;
 }
 
 /* The same with the camera partition part[image] in 0 .. nparts - 1 and
