@@ -167,6 +167,42 @@ def lsa_gcp_step(block: Block, gcpinfo, W3, gcpdata, ncam_total: int, opts: Rpba
     return st, buf.value.decode()
 
 
+def parallel_threads(n_images: int, threads: int) -> int:
+    """Partition count of CalcPLSA (rpbacore.cpp:79-85): min(Threads,
+    iround(images / 70)), iround rounding halves away from zero; the
+    partitioned branch runs when it is above 1 and images > 5."""
+    q = n_images / 70.0
+    return int(min(threads, int(q + 0.5)))
+
+
+def calc_plsa_parallel(block: Block, part, nthreads: int, opts: RpbaOptionsC | None = None,
+                       log_cap: int = 1 << 20):
+    """The parallel RPBA (the partitioned branch of CalcPLSA,
+    rpbacore.cpp:100-510) on a copy of ``block`` with the camera partition
+    ``part`` (per image, 0 .. nthreads - 1).
+
+    Returns (status, adjusted block, {"sig0opt", "iterations"}, log text);
+    the block's tracks are the best iteration's (pointXXvold)."""
+    b = block.copy()
+    cb = b.as_c()
+    o = opts if opts is not None else make_options()
+    pt = np.ascontiguousarray(part, np.int32)
+    assert pt.shape == (b.n_images,)
+    stats = np.zeros(2)
+    buf = C.create_string_buffer(log_cap)
+    f = lib().oracle_calc_plsa_parallel
+    f.restype = C.c_int32
+    f.argtypes = [C.POINTER(RpbaBlockC), C.POINTER(RpbaOptionsC), C.c_int32, C.POINTER(C.c_int32), C.c_char_p,
+                  C.c_size_t, C.POINTER(C.c_double)]
+    st = f(C.byref(cb), C.byref(o), int(nthreads), pt.ctypes.data_as(C.POINTER(C.c_int32)), buf, log_cap,
+           _dp(stats))
+    # the track arrays were rewritten in place with fewer or equal entries
+    n = int(b.pt_obs_off[-1])
+    b.pt_obs_image = b.pt_obs_image[:n].copy()
+    b.pt_obs_slot = b.pt_obs_slot[:n].copy()
+    return st, b, {"sig0opt": float(stats[0]), "iterations": int(stats[1])}, buf.value.decode()
+
+
 def input_block(path: str, k24out: bool = True) -> Block:
     cb = RpbaBlockC()
     st = lib().oracle_input_block(path.encode(), 3, int(k24out), C.byref(cb))

@@ -47,6 +47,7 @@
 #include <cstring>
 #include <fstream>
 #include <functional>
+#include <thread>
 #include <map>
 #include <random>
 #include <sstream>
@@ -289,6 +290,7 @@ struct GcpIn {
   const float *W3;
   const double *gcpdata;
   int ncam_total;
+  const double *Pd = nullptr;  /* the cameras in double precision (12 per image), or null */
 };
 
 class LSA {
@@ -421,7 +423,7 @@ LSA::LSA(const rpba_block *blk, const Opts &o, std::string *os_, const GcpIn &g)
   minimagenrdel = nimg > 2 ? 3 : 2;
 
   P.resize(12 * nimg);
-  for (int i = 0; i < 12 * nimg; ++i) P[i] = (double)blk->pmat[i];
+  for (int i = 0; i < 12 * nimg; ++i) P[i] = g.Pd ? g.Pd[i] : (double)blk->pmat[i];
 
   /* PointXXvIn, rbacore.cpp:1918-1974 (all images of the block selected);
    * in GCP mode a GCP point is kept with a single observation, if its GCP
@@ -486,7 +488,8 @@ LSA::LSA(const rpba_block *blk, const Opts &o, std::string *os_, const GcpIn &g)
     }
   nrioff = ao ? nrpari * nimg : nadd + nrparir + nrpari * (nimg - 2);
   sig00v.assign(nimg, 0.f);
-  const int xpmsize = nimg * 6 + 3 * XXnr + 7 * nimg;
+  /* xpmsize with nrcameras = the scene's camera count (rbacore.cpp:324) */
+  const int xpmsize = nimg * 6 + 3 * XXnr + 7 * (ao ? std::max(ncam_total, nimg) : nimg);
   XPM.assign(xpmsize, 0.);
   XPMn.assign(xpmsize, 0.);
   if (nimg < 1 || (!ao && (nimg < 2 || normcamera < 1))) bad_setup = 1;
@@ -1714,7 +1717,7 @@ struct TriObs {
 };
 
 // residuals and projections of one point (CalcCorrPointMulti)
-void tri_corr(const rpba_block *b, const std::vector<TriObs> &ob, double X0, double X1, double X2,
+void tri_corr(const rpba_block *b, const double *Pd, const std::vector<TriObs> &ob, double X0, double X1, double X2,
               const std::vector<float> &wx, const std::vector<float> &wy, const std::vector<float> &wxy,
               const std::vector<float> &wxo, const std::vector<float> &wyo, const std::vector<float> &wxyo,
               std::vector<double> &corr, float &sig0, std::vector<float> &sig0v, std::vector<float> &p1v,
@@ -1722,10 +1725,10 @@ void tri_corr(const rpba_block *b, const std::vector<TriObs> &ob, double X0, dou
   sig0 = 0.f;
   for (size_t js = 0; js < ob.size(); ++js) {
     const int j = ob[js].im;
-    const float *P = &b->pmat[12 * j];
-    double p1 = (double)P[0] * X0 + (double)P[1] * X1 + (double)P[2] * X2 + (double)P[3];
-    double p2 = (double)P[4] * X0 + (double)P[5] * X1 + (double)P[6] * X2 + (double)P[7];
-    double p3 = (double)P[8] * X0 + (double)P[9] * X1 + (double)P[10] * X2 + (double)P[11];
+    const double *P = &Pd[12 * j];
+    double p1 = P[0] * X0 + P[1] * X1 + P[2] * X2 + P[3];
+    double p2 = P[4] * X0 + P[5] * X1 + P[6] * X2 + P[7];
+    double p3 = P[8] * X0 + P[9] * X1 + P[10] * X2 + P[11];
     if (std::fabs(p3) < 1.e-3)
       p3 = p3 > 0. ? 1.e3 : -1.e3;
     else
@@ -1770,12 +1773,21 @@ void tri_calibrated(double *xp, double *yp, double x, double y, double k2, doubl
 
 }  // namespace
 
-static int32_t tri_impl(const rpba_block *b, const float *sig0w, int32_t robustmode, int32_t weight_only,
-                        const int32_t *part, int32_t nparts, double *XXo, uint8_t *keep, float *sig0v_out,
-                        uint8_t *conv, double *sig0io, int64_t *redundancy, float *w3d) {
+/* Points p0 .. p1 - 1; Pd: the cameras in double precision (12 per image;
+ * null: the block's). */
+static int32_t tri_impl(const rpba_block *b, const double *Pd_in, int p0, int p1, const float *sig0w,
+                        int32_t robustmode, int32_t weight_only, const int32_t *part, int32_t nparts, double *XXo,
+                        uint8_t *keep, float *sig0v_out, uint8_t *conv, double *sig0io, int64_t *redundancy,
+                        float *w3d) {
+  std::vector<double> Pown;
+  if (!Pd_in) {
+    Pown.resize(12 * (size_t)b->n_images);
+    for (size_t i = 0; i < Pown.size(); ++i) Pown[i] = (double)b->pmat[i];
+  }
+  const double *Pd = Pd_in ? Pd_in : Pown.data();
   double s0io = 0.;
   long long red = 0;
-  for (int pi = 0; pi < b->n_points; ++pi) {
+  for (int pi = p0; pi < p1; ++pi) {
     const int s = b->pt_obs_off[pi], e = b->pt_obs_off[pi + 1], pxs = e - s;
     for (int j = s; j < e; ++j) keep[j] = 0;
     conv[pi] = 0;
@@ -1807,7 +1819,7 @@ static int32_t tri_impl(const rpba_block *b, const float *sig0w, int32_t robustm
     float Xo0 = X0, Xo1 = X1, Xo2 = X2, sig0 = 1.e20f, sig0opt = 1.e20f;
     int iflag = robustmode > 0 ? 2 : 1, iter = 1;
     bool cv = false;
-    tri_corr(b, ob, X0, X1, X2, wx, wy, wxy, wxo, wyo, wxyo, corr, sig0opt, sv, p1v, p2v, p3v);
+    tri_corr(b, Pd, ob, X0, X1, X2, wx, wy, wxy, wxo, wyo, wxyo, corr, sig0opt, sv, p1v, p2v, p3v);
     if (weight_only) {
       wsum /= (float)pxs2;
       s0io += sig0opt / wsum;
@@ -1819,13 +1831,13 @@ static int32_t tri_impl(const rpba_block *b, const float *sig0w, int32_t robustm
       std::fill(Nv.begin(), Nv.end(), 0.);
       for (int js = 0; js < pxs; ++js) {
         const int j = ob[js].im;
-        const float *P = &b->pmat[12 * j];
+        const double *P = &Pd[12 * j];
         const double x = p1v[js], y = p2v[js], P3 = p3v[js], P1 = (double)p1v[js] * p3v[js],
                      P2 = (double)p2v[js] * p3v[js];
         double xp[3], yp[3];
         for (int c = 0; c < 3; ++c) {
-          xp[c] = (double)P[c] * P3 - (double)P[8 + c] * P1;
-          yp[c] = (double)P[4 + c] * P3 - (double)P[8 + c] * P2;
+          xp[c] = P[c] * P3 - P[8 + c] * P1;
+          yp[c] = P[4 + c] * P3 - P[8 + c] * P2;
         }
         tri_calibrated(xp, yp, x, y, b->distpara[2 * j], b->distpara[2 * j + 1], b->K[9 * j], b->K[9 * j + 4],
                        b->K[9 * j + 1]);
@@ -1862,7 +1874,7 @@ static int32_t tri_impl(const rpba_block *b, const float *sig0w, int32_t robustm
       X0 = Xo0 + (float)dx[0];
       X1 = Xo1 + (float)dx[1];
       X2 = Xo2 + (float)dx[2];
-      tri_corr(b, ob, X0, X1, X2, wx, wy, wxy, wxo, wyo, wxyo, corr, sig0, sv, p1v, p2v, p3v);
+      tri_corr(b, Pd, ob, X0, X1, X2, wx, wy, wxy, wxo, wyo, wxyo, corr, sig0, sv, p1v, p2v, p3v);
       if (iflag == 1 && robustmode == 2) {
         for (int js = 0; js < pxs; ++js)
           if (sv[js] * sig0w[ob[js].im] > 16.f) {
@@ -1935,8 +1947,8 @@ static int32_t tri_impl(const rpba_block *b, const float *sig0w, int32_t robustm
 extern "C" int32_t oracle_triangulate(const rpba_block *b, const float *sig0w, int32_t robustmode,
                                       int32_t weight_only, double *XXo, uint8_t *keep, float *sig0v_out,
                                       uint8_t *conv, double *sig0io, int64_t *redundancy) {
-  return tri_impl(b, sig0w, robustmode, weight_only, nullptr, 1, XXo, keep, sig0v_out, conv, sig0io, redundancy,
-                  nullptr);
+  return tri_impl(b, nullptr, 0, b->n_points, sig0w, robustmode, weight_only, nullptr, 1, XXo, keep, sig0v_out,
+                  conv, sig0io, redundancy, nullptr);
 }
 
 /* One GCP-mode step of the LSA on a block (the parallel RPBA's
@@ -1960,6 +1972,387 @@ extern "C" int32_t oracle_lsa_gcp_step(rpba_block *blk, const rpba_options *o, c
   return st;
 }
 
+/* ---------------------------------------------------------------------
+ * Parallel RPBA: the partitioned branch of CalcPLSA, rpbacore.cpp:100-510.
+ * The images are cut into nthreads partitions (part[image]; the reference
+ * partitions with METIS, rpba_partition_images replaces it).  Outer
+ * iteration `iter`:
+ *   iter > 1: every partition's LSA takes one GCP-mode step (its images,
+ *     the observations in them, the points it shares with other partitions
+ *     held by 3-D priors with the weight blocks of the last merge; the
+ *     additional parameters stay fixed at iter 2) and its cameras replace
+ *     the scene's;
+ *   the merge: every point is refined against the new cameras by
+ *   CalcLSAXMulti (first a robust pass that gives the per-image thresholds
+ *   when the robust stage starts, then the main pass: robust deletion,
+ *   weight-only at iter 1, the per-partition weight blocks), in nthreads
+ *   chunks of points whose sums are added in chunk order;
+ *   sigma0 = sum / (redundancy - unknowns); the best state is kept, and the
+ *   points seen by more than one partition become the next GCPs at their
+ *   refined positions;
+ * until iflag runs out (sig0frac rule) or 50 iterations.  The partition
+ * LSAs and the point chunks run on host threads; results do not depend on
+ * the scheduling. */
+namespace {
+
+struct PObs {
+  int image, slot;
+};
+struct PCam {
+  float K[9], d[2];
+};
+
+template <class F>
+void par_for(int n, F &&f) {
+  std::vector<std::thread> th;
+  for (int k = 1; k < n; ++k) th.emplace_back(f, k);
+  if (n > 0) f(0);
+  for (auto &t : th) t.join();
+}
+
+// a block over the scene's cameras and slots with the given point lists
+struct TmpBlock {
+  rpba_block b{};
+  std::vector<int32_t> off, img, slot;
+  std::vector<float> XX, pmat, K, dist;
+};
+
+}  // namespace
+
+extern "C" int32_t oracle_calc_plsa_parallel(rpba_block *blk, const rpba_options *o, int32_t nthreads,
+                                             const int32_t *part, char *log, size_t cap, double *stats) {
+  const int nrimages = blk->n_images, pxs = blk->n_points, T = nthreads;
+  if (T < 2 || !part) return RPBA_ERR_ARG;
+  for (int i = 0; i < nrimages; ++i)
+    if (part[i] < 0 || part[i] >= T) return RPBA_ERR_ARG;
+  std::string os;
+  const Opts op = make_opts(o);
+  const bool robustflag = op.robust;
+  const int nraddp = (int)op.addf[0] + (int)op.addf[1] + (int)op.addf[2];
+  // partitions: images in index order
+  std::vector<std::vector<int>> imgindv(T);
+  std::vector<int> imgindbv(nrimages);
+  for (int i = 0; i < nrimages; ++i) {
+    imgindv[part[i]].push_back(i);
+    imgindbv[i] = part[i];
+  }
+  for (int it = 0; it < T; ++it)
+    if (imgindv[it].empty()) return RPBA_ERR_ARG;
+  // state
+  std::vector<double> XXd(3 * (size_t)pxs), XXdold, PMd(12 * (size_t)nrimages), PMdold;
+  for (size_t i = 0; i < XXd.size(); ++i) XXd[i] = (double)blk->XX[i];
+  for (size_t i = 0; i < PMd.size(); ++i) PMd[i] = (double)blk->pmat[i];
+  PMdold = PMd;
+  XXdold = XXd;
+  std::vector<PCam> cameras(nrimages), cameraps, camerasnew(nrimages), camerasold(nrimages);
+  for (int i = 0; i < nrimages; ++i) {
+    for (int c = 0; c < 9; ++c) cameras[i].K[c] = blk->K[9 * i + c];
+    cameras[i].d[0] = blk->distpara[2 * i];
+    cameras[i].d[1] = blk->distpara[2 * i + 1];
+  }
+  cameraps = cameras;
+  std::vector<std::vector<PObs>> pointXXv(pxs), pointXXvold;
+  for (int p = 0; p < pxs; ++p)
+    for (int t = blk->pt_obs_off[p]; t < blk->pt_obs_off[p + 1]; ++t)
+      pointXXv[p].push_back({blk->pt_obs_image[t], blk->pt_obs_slot[t]});
+  pointXXvold = pointXXv;
+  std::vector<std::vector<char>> pitflagsv(pxs);
+  std::vector<int> gcpinfo(pxs, -1);
+  std::vector<std::vector<PCam>> camerasoit(T, cameras);
+  std::vector<std::vector<double>> PMdd(T, PMd);
+  std::vector<std::vector<std::vector<PObs>>> pointXXvv(T);
+  std::vector<std::vector<int>> pindv(T), gcpinfov(T);
+  std::vector<std::vector<float>> W3ijiv(T);
+  std::vector<double> gcpdatav;
+  std::vector<float> sig0wv(nrimages, 0.f);
+  const int nrparimages = (nrimages - 2) * 6 + 5 + nrimages * nraddp;
+  const int nrppt = pxs / T;
+  std::vector<int> beginv(T), endv(T);
+  for (int c = 0; c < T; ++c) {
+    beginv[c] = nrppt * c;
+    endv[c] = c == T - 1 ? pxs : nrppt * (c + 1);
+  }
+  double sig0opt = 1.e20, sig0g = 0.;
+  int iflag = robustflag ? 2 : 1, iter = 1;
+  float sig0frac = 1.01f;
+  std::vector<float> w3d((size_t)pxs * T * 6, 0.f);
+
+  // a block of the whole scene with the current point lists and points
+  auto scene_block = [&](TmpBlock &tb) {
+    tb.b = *blk;
+    tb.off.assign(pxs + 1, 0);
+    tb.img.clear();
+    tb.slot.clear();
+    for (int p = 0; p < pxs; ++p) {
+      for (const PObs &q : pointXXv[p]) {
+        tb.img.push_back(q.image);
+        tb.slot.push_back(q.slot);
+      }
+      tb.off[p + 1] = (int32_t)tb.img.size();
+    }
+    tb.XX.resize(3 * (size_t)pxs);
+    for (size_t i = 0; i < tb.XX.size(); ++i) tb.XX[i] = (float)XXd[i];
+    tb.K.resize(9 * (size_t)nrimages);
+    tb.dist.resize(2 * (size_t)nrimages);
+    for (int i = 0; i < nrimages; ++i) {
+      for (int c = 0; c < 9; ++c) tb.K[9 * i + c] = cameraps[i].K[c];
+      tb.dist[2 * i] = cameraps[i].d[0];
+      tb.dist[2 * i + 1] = cameraps[i].d[1];
+    }
+    tb.b.pt_obs_off = tb.off.data();
+    tb.b.pt_obs_image = tb.img.data();
+    tb.b.pt_obs_slot = tb.slot.data();
+    tb.b.XX = tb.XX.data();
+    tb.b.K = tb.K.data();
+    tb.b.distpara = tb.dist.data();
+  };
+  // one CalcLSAXMulti sweep over all points in chunks; applies the point
+  // updates and the deletions; returns the chunk sums in chunk order
+  auto sweep = [&](int robustmode, bool weightonly, bool wxy, std::vector<std::vector<float>> *sig0vv) {
+    TmpBlock tb;
+    scene_block(tb);
+    const size_t nt = tb.img.size();
+    std::vector<double> XXo(3 * (size_t)pxs);
+    std::vector<uint8_t> keep(nt), conv(pxs);
+    std::vector<float> sv(nt);
+    std::vector<double> s0(T, 0.);
+    std::vector<int64_t> red(T, 0);
+    par_for(T, [&](int c) {
+      tri_impl(&tb.b, PMd.data(), beginv[c], endv[c], sig0wv.data(), robustmode, weightonly ? 1 : 0,
+               wxy ? imgindbv.data() : nullptr, wxy ? T : 1, XXo.data(), keep.data(), sv.data(), conv.data(), &s0[c],
+               &red[c], wxy ? w3d.data() : nullptr);
+    });
+    if (sig0vv)
+      for (int p = 0; p < pxs; ++p)
+        if (!pointXXv[p].empty())
+          for (int t = tb.off[p]; t < tb.off[p + 1]; ++t) (*sig0vv)[tb.img[t]].push_back(sv[t]);
+    for (int p = 0; p < pxs; ++p) {
+      if (pointXXv[p].empty()) continue;
+      for (int q = 0; q < 3; ++q) XXd[3 * (size_t)p + q] = XXo[3 * (size_t)p + q];
+      std::vector<PObs> kept;
+      for (int t = tb.off[p]; t < tb.off[p + 1]; ++t)
+        if (keep[t]) kept.push_back(pointXXv[p][t - tb.off[p]]);
+      pointXXv[p] = kept;
+    }
+    double a = 0.;
+    long long r = 0;
+    for (int c = 0; c < T; ++c) {
+      a += s0[c];
+      r += red[c];
+    }
+    return std::make_pair(a, r);
+  };
+
+  while (iflag > 0 && iter < 51) {
+    bool robustflagit = false;
+    if (iter > 1) {
+      Opts ol = op;
+      ol.robust = false;
+      if (iter < 3) ol.addf[0] = ol.addf[1] = ol.addf[2] = false;
+      std::vector<std::string> osv(T);
+      par_for(T, [&](int it) {
+        const std::vector<int> &imgs = imgindv[it];
+        const int m = (int)imgs.size();
+        TmpBlock tb;
+        std::vector<float> xg, wx, wy, wxy;
+        std::vector<int32_t> ioff(m + 1, 0);
+        std::vector<int> loc(nrimages, -1);
+        std::vector<double> Pd(12 * (size_t)m);
+        tb.pmat.resize(12 * (size_t)m);
+        tb.K.resize(9 * (size_t)m);
+        tb.dist.resize(2 * (size_t)m);
+        for (int li = 0; li < m; ++li) {
+          const int g = imgs[li];
+          loc[g] = li;
+          for (int c = 0; c < 12; ++c) {
+            Pd[12 * li + c] = PMdd[it][12 * (size_t)g + c];
+            tb.pmat[12 * li + c] = (float)Pd[12 * li + c];
+          }
+          for (int c = 0; c < 9; ++c) tb.K[9 * li + c] = camerasoit[it][g].K[c];
+          tb.dist[2 * li] = camerasoit[it][g].d[0];
+          tb.dist[2 * li + 1] = camerasoit[it][g].d[1];
+          for (int sl = blk->img_obs_off[g]; sl < blk->img_obs_off[g + 1]; ++sl) {
+            xg.push_back(blk->xg[2 * sl]);
+            xg.push_back(blk->xg[2 * sl + 1]);
+            wx.push_back(blk->wx[sl]);
+            wy.push_back(blk->wy[sl]);
+            wxy.push_back(blk->wxy[sl]);
+          }
+          ioff[li + 1] = (int32_t)wx.size();
+        }
+        const int np = (int)pindv[it].size();
+        tb.off.assign(np + 1, 0);
+        tb.XX.resize(3 * (size_t)np);
+        for (int j = 0; j < np; ++j) {
+          for (const PObs &q : pointXXvv[it][j]) {
+            tb.img.push_back(loc[q.image]);
+            tb.slot.push_back(q.slot);
+          }
+          tb.off[j + 1] = (int32_t)tb.img.size();
+          for (int c = 0; c < 3; ++c) tb.XX[3 * j + c] = (float)XXd[3 * (size_t)pindv[it][j] + c];
+        }
+        rpba_block &b = tb.b;
+        b.n_images = m;
+        b.n_points = np;
+        b.pmat = tb.pmat.data();
+        b.K = tb.K.data();
+        b.distpara = tb.dist.data();
+        b.XX = tb.XX.data();
+        b.img_obs_off = ioff.data();
+        b.xg = xg.data();
+        b.wx = wx.data();
+        b.wy = wy.data();
+        b.wxy = wxy.data();
+        b.pt_obs_off = tb.off.data();
+        b.pt_obs_image = tb.img.data();
+        b.pt_obs_slot = tb.slot.data();
+        GcpIn g{gcpinfov[it].data(), W3ijiv[it].data(), gcpdatav.data(), nrimages};
+        g.Pd = Pd.data();
+        LSA lsa(&b, ol, &osv[it], g);
+        lsa.adjust_gcp_step();
+        // OutputLSAP: PointXXvOut clears the lists of the points that
+        // PointXXvIn did not take; the stored cameras (rectified by the
+        // encoding even when the step did not run) and camerasnew
+        for (int j = 0, k = 0; j < np; ++j) {
+          if (k < lsa.nrpts && lsa.nrpv[k] == j)
+            ++k;
+          else
+            pointXXvv[it][j].clear();
+        }
+        for (int li = 0; li < m; ++li) {
+          const int gi = imgs[li];
+          for (int c = 0; c < 12; ++c) PMdd[it][12 * (size_t)gi + c] = lsa.P[12 * li + c];
+          for (int c = 0; c < 9; ++c) camerasoit[it][gi].K[c] = (float)lsa.Kn[9 * li + c];
+          camerasoit[it][gi].d[0] = (float)lsa.dn[2 * li];
+          camerasoit[it][gi].d[1] = (float)lsa.dn[2 * li + 1];
+        }
+      });
+      for (int it = 0; it < T; ++it) {
+        os += osv[it];
+        for (int gi : imgindv[it]) {
+          for (int c = 0; c < 12; ++c) PMd[12 * (size_t)gi + c] = PMdd[it][12 * (size_t)gi + c];
+          cameraps[gi] = camerasoit[it][gi];
+          camerasnew[gi] = camerasoit[it][gi];
+        }
+      }
+    }
+    if (iflag == 1) {
+      robustflagit = robustflag;
+      if (robustflag) sig0frac = 1.02f;
+    }
+    if (iter > 1) {
+      for (int p = 0; p < pxs; ++p) pointXXv[p].clear();
+      for (int it = 0; it < T; ++it)
+        for (size_t j = 0; j < pindv[it].size(); ++j)
+          for (const PObs &q : pointXXvv[it][j]) pointXXv[pindv[it][j]].push_back(q);
+      for (int p = 0; p < pxs; ++p)
+        if (pointXXv[p].size() < 2) pointXXv[p].clear();
+    } else {
+      for (int i = 0; i < nrimages; ++i) cameraps[i] = camerasnew[i] = cameras[i];
+    }
+    for (int p = 0; p < pxs; ++p)
+      if (!pointXXv[p].empty()) {
+        pitflagsv[p].assign(T, 0);
+        for (const PObs &q : pointXXv[p]) pitflagsv[p][imgindbv[q.image]] = 1;
+      }
+    if (robustflagit) {
+      std::vector<std::vector<float>> sig0vvs(nrimages);
+      sweep(1, false, false, &sig0vvs);
+      for (int i = 0; i < nrimages; ++i) {
+        if (sig0vvs[i].empty()) {
+          sig0wv[i] = 0.f;
+        } else {
+          std::sort(sig0vvs[i].begin(), sig0vvs[i].end());
+          sig0wv[i] = 1.f / (sig0vvs[i][(int)sig0vvs[i].size() / 2] * 2.1981f);
+        }
+      }
+    }
+    const auto sr = sweep(robustflagit ? 2 : 0, iter == 1, true, nullptr);
+    sig0g = sr.first / (double)(sr.second - nrparimages);
+    if (sig0g <= sig0opt) {
+      XXdold = XXd;
+      PMdold = PMd;
+      pointXXvold = pointXXv;
+      camerasold = camerasnew;
+    }
+    for (int it = 0; it < T; ++it) {
+      camerasoit[it] = camerasnew;
+      for (int gi : imgindv[it])
+        for (int c = 0; c < 12; ++c) PMdd[it][12 * (size_t)gi + c] = PMd[12 * (size_t)gi + c];
+      pointXXvv[it].clear();
+      pindv[it].clear();
+      W3ijiv[it].clear();
+    }
+    // the next GCPs: points (tracks of 2 or more) seen by more than one partition
+    int nrgcpnew = 0;
+    gcpdatav.clear();
+    for (int c = 0; c < T; ++c)
+      for (int p = beginv[c]; p < endv[c]; ++p) {
+        if (pointXXv[p].size() < 2) continue;
+        int gnum = 0;
+        for (int it = 0; it < T && gnum < 2; ++it) gnum += pitflagsv[p][it];
+        if (gnum > 1) {
+          gcpinfo[p] = nrgcpnew;
+          for (int q = 0; q < 3; ++q) gcpdatav.push_back(XXd[3 * (size_t)p + q]);
+          for (int it = 0; it < T; ++it)
+            if (pitflagsv[p][it])
+              for (int q = 0; q < 6; ++q) W3ijiv[it].push_back(w3d[((size_t)p * T + it) * 6 + q]);
+          ++nrgcpnew;
+        } else {
+          gcpinfo[p] = -1;
+        }
+      }
+    for (int p = 0; p < pxs; ++p) {
+      std::vector<std::vector<PObs>> per(T);
+      for (const PObs &q : pointXXv[p]) per[imgindbv[q.image]].push_back(q);
+      for (int it = 0; it < T; ++it)
+        if (!per[it].empty()) {
+          pointXXvv[it].push_back(per[it]);
+          pindv[it].push_back(p);
+        }
+    }
+    for (int it = 0; it < T; ++it) {
+      gcpinfov[it].resize(pindv[it].size());
+      for (size_t j = 0; j < pindv[it].size(); ++j) gcpinfov[it][j] = gcpinfo[pindv[it][j]];
+    }
+    if (iter > 1) {
+      if (sig0g <= sig0opt) {
+        if (sig0opt < sig0g * sig0frac && iter > 3)
+          --iflag;
+        else
+          sig0opt = sig0g;
+      } else if (iter > 3) {
+        --iflag;
+      }
+    }
+    ++iter;
+  }
+  // pointXXvio = pointXXvold, PMatrices, XX, cameras (rpbacore.cpp:498-507)
+  int32_t t = 0;
+  for (int p = 0; p < pxs; ++p) {
+    blk->pt_obs_off[p] = t;
+    for (const PObs &q : pointXXvold[p]) {
+      blk->pt_obs_image[t] = q.image;
+      blk->pt_obs_slot[t] = q.slot;
+      ++t;
+    }
+  }
+  blk->pt_obs_off[pxs] = t;
+  for (size_t i = 0; i < PMdold.size(); ++i) blk->pmat[i] = (float)PMdold[i];
+  for (size_t i = 0; i < XXdold.size(); ++i) blk->XX[i] = (float)XXdold[i];
+  for (int i = 0; i < nrimages; ++i) {
+    for (int c = 0; c < 9; ++c) blk->K[9 * i + c] = camerasold[i].K[c];
+    blk->distpara[2 * i] = camerasold[i].d[0];
+    blk->distpara[2 * i + 1] = camerasold[i].d[1];
+  }
+  if (stats) {
+    stats[0] = sig0opt;
+    stats[1] = iter - 1;
+  }
+  copy_log(os, log, cap);
+  return RPBA_OK;
+}
+
 /* The same with the camera partition part[image] in 0 .. nparts - 1 and
  * the per-partition weight blocks w3d[n_points][nparts][6] (XX, YY, ZZ,
  * XY, XZ, YZ). */
@@ -1970,8 +2363,8 @@ extern "C" int32_t oracle_triangulate_parts(const rpba_block *b, const float *si
   if (!part || nparts < 1 || !w3d) return RPBA_ERR_ARG;
   for (int i = 0; i < b->n_images; ++i)
     if (part[i] < 0 || part[i] >= nparts) return RPBA_ERR_ARG;
-  return tri_impl(b, sig0w, robustmode, weight_only, part, nparts, XXo, keep, sig0v_out, conv, sig0io, redundancy,
-                  w3d);
+  return tri_impl(b, nullptr, 0, b->n_points, sig0w, robustmode, weight_only, part, nparts, XXo, keep, sig0v_out,
+                  conv, sig0io, redundancy, w3d);
 }
 
 extern "C" {

@@ -1,9 +1,11 @@
-"""The oracle's restatement of the parallel RPBA's pieces (rpbacore.cpp:
-100-510): the LSA's GCP mode (every camera free, shared points held by
-3-D priors, one damped step per call).  No reference build exists here,
-so the checks are behavioural: with every point a stiff GCP at the global
-solution, GCP steps bring perturbed cameras back to that solution, and a
-step taken at the solution barely moves them (no GPU needed)."""
+"""The oracle's restatement of the parallel RPBA (rpbacore.cpp:100-510):
+the LSA's GCP mode (every camera free, shared points held by 3-D priors,
+one damped step per call) and the whole partitioned loop.  No reference
+build exists here, so the checks are behavioural: with every point a stiff
+GCP at the global solution, GCP steps bring perturbed cameras back to that
+solution, and a step taken at the solution barely moves them; the
+partitioned loop reaches the global LSA's Exteval sigma0, deterministically
+(no GPU needed)."""
 import numpy as np
 import pytest
 
@@ -59,3 +61,92 @@ def test_gcp_step_at_solution_is_small(oracle_mod, solved):
     assert st == 0, log
     scale = np.abs(ref).max()
     assert np.abs(_centres(blk) - ref).max() < 1e-4 * scale
+
+
+# ---------------------------------------------------------------------------
+# the whole partitioned loop (rpbacore.cpp:100-510)
+
+@pytest.fixture(scope="module")
+def par_scenes():
+    from rpba_b200 import scenes
+    return {
+        "arc": scenes.to_block(scenes.arc_scene(seed=5, n_cams=50, n_pts=8000)),
+        "street": scenes.to_block(scenes.street_scene(seed=6, n_cams=120, n_pts=20000)),
+        "city": scenes.to_block(scenes.city_scene(seed=8, n_clusters=4, cams_per_cluster=30, n_pts=20000)),
+    }
+
+
+def _ext_sigma(oracle_mod, blk):
+    return oracle_mod.exteval(blk)[1]["exteval_sigma0"]
+
+
+def _is_subtrack(inp, out, p):
+    """Every observation of the output track is one of the input track's
+    (the merge regroups a track partition by partition, rpbacore.cpp:272-276,
+    so the order may change)."""
+    track = lambda b: list(zip(b.pt_obs_image[b.pt_obs_off[p]:b.pt_obs_off[p + 1]].tolist(),
+                               b.pt_obs_slot[b.pt_obs_off[p]:b.pt_obs_off[p + 1]].tolist()))
+    o = track(out)
+    return len(set(o)) == len(o) and set(o) <= set(track(inp))
+
+
+@pytest.mark.parametrize("name", ["arc", "street", "city"])
+def test_parallel_rpba_matches_global_lsa(oracle_mod, par_scenes, name):
+    """From the perturbed scene (Exteval sigma0 ~8-9 px) the partitioned
+    RPBA at 2 and 4 partitions ends within 1% of the global LSA's Exteval
+    sigma0 (measured: -1.0% .. +0.2%), the observations of every track a
+    subset of its input track's, one GCP step per partition per outer
+    iteration after the first."""
+    import rpba_b200 as rb
+    blk = par_scenes[name]
+    s_in = _ext_sigma(oracle_mod, blk)
+    st, g, _, _ = oracle_mod.calc_plsa(blk)
+    assert st == 0
+    s_glob = _ext_sigma(oracle_mod, g)
+    for k in (2, 4):
+        part = rb.partition_images(blk, k)
+        st, b, stats, log = oracle_mod.calc_plsa_parallel(blk, part, k)
+        assert st == 0, log[-2000:]
+        s_par = _ext_sigma(oracle_mod, b)
+        print(f"{name} k={k}: Exteval sigma0 {s_in:.4f} -> {s_par:.5f} (global LSA {s_glob:.5f}), "
+              f"{stats['iterations']} iterations, {b.n_obs} of {blk.n_obs} observations")
+        assert s_par <= 1.01 * s_glob, (s_par, s_glob)
+        assert s_par < 0.1 * s_in
+        assert 4 <= stats["iterations"] <= 50
+        assert log.count("Sigma0AO:") == k * (stats["iterations"] - 1)
+        assert np.isfinite(b.pmat).all() and np.isfinite(b.XX).all()
+        assert b.n_obs <= blk.n_obs
+        assert all(_is_subtrack(blk, b, p) for p in range(0, blk.n_points, 7))
+
+
+def test_parallel_rpba_deterministic(oracle_mod, par_scenes):
+    """The partition LSAs and the point chunks run on host threads; sums
+    are added in chunk order, so two runs agree bit for bit."""
+    import rpba_b200 as rb
+    blk = par_scenes["city"]
+    part = rb.partition_images(blk, 3)
+    r1 = oracle_mod.calc_plsa_parallel(blk, part, 3)
+    r2 = oracle_mod.calc_plsa_parallel(blk, part, 3)
+    assert r1[0] == r2[0] == 0
+    for n in ("pmat", "K", "distpara", "XX", "pt_obs_off", "pt_obs_image", "pt_obs_slot"):
+        assert np.array_equal(getattr(r1[1], n), getattr(r2[1], n)), n
+    assert r1[2] == r2[2] and r1[3] == r2[3]
+
+
+def test_parallel_rpba_rejects_bad_partitions(oracle_mod, par_scenes):
+    blk = par_scenes["arc"]
+    n = blk.n_images
+    good = (np.arange(n) * 2) // n
+    assert oracle_mod.calc_plsa_parallel(blk, good, 1)[0] == 1          # fewer than 2 partitions
+    assert oracle_mod.calc_plsa_parallel(blk, np.where(good == 1, 2, 0), 2)[0] == 1  # out of range
+    assert oracle_mod.calc_plsa_parallel(blk, np.zeros(n, np.int32), 2)[0] == 1      # an empty partition
+
+
+def test_parallel_thread_rule(oracle_mod):
+    """nrthreads = min(Threads, iround(images / 70)); the partitioned branch
+    runs when nrthreads > 1 and images > 5 (rpbacore.cpp:79-92)."""
+    assert oracle_mod.parallel_threads(50, 8) == 1
+    assert oracle_mod.parallel_threads(105, 8) == 2      # 1.5 rounds away from zero
+    assert oracle_mod.parallel_threads(1000, 8) == 8
+    assert oracle_mod.parallel_threads(13700, 64) == 64
+    assert oracle_mod.parallel_threads(13700, 500) == 196
