@@ -23,7 +23,9 @@ matched-RMS check (ours' final RMS <= plain's x (1 + 1e-6)).  With N > 1
 (independent replicas, no collective on the data path); the value is the
 slowest rank's time.  ``--impl reference`` times the reference algorithm's
 CPU implementation (the C++ restatement under oracle/, single-threaded like
-the reference's global LSA) on a bounded sample of the workload, rank 0 only.
+the reference's global LSA) on a bounded sample of the workload, rank 0 only;
+beside it ("parallel") the reference's partitioned branch, which it takes
+with more than one thread, on the same sample with the host's cores.
 """
 from __future__ import annotations
 
@@ -156,6 +158,22 @@ def make_block(config, scale, seed_offset=0):
     return scenes.to_block(scenes.make_scene(config, scale=scale, seed=20260 + config + seed_offset))
 
 
+def pinned_copy(blk):
+    """The block with every array in page-locked host memory (the e2e
+    inputs are copied to the device from pinned memory)."""
+    import torch
+    from rpba_b200.block import Block, _ARRAYS
+    keep, arrs = [], []
+    for n in _ARRAYS:
+        a = np.ascontiguousarray(getattr(blk, n))
+        t = torch.empty(max(a.nbytes, 1), dtype=torch.uint8, pin_memory=True)
+        keep.append(t)
+        v = t.numpy()[:a.nbytes].view(a.dtype).reshape(a.shape)
+        v[...] = a
+        arrs.append(v)
+    return Block(*arrs, _keep=keep)
+
+
 def learned_weights():
     from rpba_b200 import train_precond
     w = train_precond.load()
@@ -172,8 +190,29 @@ def cpu_sample(config, scale):
     import rpba_b200 as rb
     blk = make_block(config, scale)
     t0 = time.perf_counter()
-    st, _, rep, _ = oracle.calc_plsa(blk, rb.make_options(solver=rb.SOLVER_PCG))
-    return time.perf_counter() - t0, rep, st, blk
+    st, out, rep, _ = oracle.calc_plsa(blk, rb.make_options(solver=rb.SOLVER_PCG))
+    return time.perf_counter() - t0, rep, st, blk, out
+
+
+def cpu_sample_parallel(blk, out_global):
+    """The reference's partitioned branch (Threads=0: min(host cores,
+    iround(images / 70)) partitions, rpbacore.cpp:79-92, 100-510) as restated
+    by the oracle, on the same sample, partition included in the time;
+    None when that sample takes the global branch."""
+    import oracle
+    import rpba_b200 as rb
+    threads = oracle.parallel_threads(blk.n_images, os.cpu_count() or 1)
+    if threads < 2 or blk.n_images <= 5:
+        return None
+    t0 = time.perf_counter()
+    part = rb.partition_images(blk, threads)
+    st, out, stats, _ = oracle.calc_plsa_parallel(blk, part, threads)
+    dt = time.perf_counter() - t0
+    ev = lambda b: oracle.exteval(b)[1]["exteval_sigma0"]
+    return {"value": dt, "unit": UNIT, "cores": threads, "partitions": threads, "status": st,
+            "outer_iterations": stats["iterations"], "exteval_sigma0": ev(out),
+            "global_exteval_sigma0": ev(out_global),
+            "note": "Threads=0 branch of the reference: partition, per-partition GCP steps, CalcLSAXMulti merge"}
 
 
 def config_dict(args, blk=None):
@@ -193,10 +232,11 @@ def run_reference(args):
         return 0
     times, rep, st, blk = [], None, 0, None
     for i in range(args.warmup + args.steps):
-        dt, rep, st, blk = cpu_sample(args.config, args.cpu_sample_scale)
+        dt, rep, st, blk, out = cpu_sample(args.config, args.cpu_sample_scale)
         if i >= args.warmup:
             times.append(dt)
     v = statistics.median(times)
+    par = cpu_sample_parallel(blk, out)
     sample = (f"one complete solve (reference stop rule) of the same scene family at "
               f"{args.cpu_sample_scale:g} of the workload: {blk.n_images} cameras, {blk.n_points} points, "
               f"{blk.n_obs} observations; one thread (the reference's global LSA is single-threaded)")
@@ -206,7 +246,8 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": dict(config_dict(args), sample=sample),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample,
-                         "linear_solves": rep["linear_solves"], "final_rms": rep["rms"], "status": st},
+                         "linear_solves": rep["linear_solves"], "final_rms": rep["rms"], "status": st,
+                         "parallel": par},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -273,13 +314,17 @@ def main():
 
     # end to end through the C ABI with host buffers: rpba_create (scene
     # H2D), the weights, rpba_solve, rpba_get_state (D2H), rpba_destroy
+    try:
+        eblk, e2e_mem = pinned_copy(blk), "pinned"
+    except Exception as e:  # page-locking refused: the caller's pageable arrays
+        eblk, e2e_mem = blk, f"pageable ({type(e).__name__})"
     e2e_times = []
     for _ in range(max(1, args.e2e_steps)):
         flush.zero_()
         barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        S = rb.Solver(blk, **ours_kw)
+        S = rb.Solver(eblk, **ours_kw)
         S.set_preconditioner(w)
         S.solve()
         S.state()
@@ -315,7 +360,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        dt, rep_c, st_c, sblk = cpu_sample(args.config, args.cpu_sample_scale)
+        dt, rep_c, st_c, sblk, sout = cpu_sample(args.config, args.cpu_sample_scale)
         S = rb.Solver(sblk, **ours_kw)
         S.set_preconditioner(w)
         S.solve()
@@ -325,7 +370,7 @@ def main():
                "sample": (f"one complete solve of the same scene family at {args.cpu_sample_scale:g} of the "
                           f"workload ({sblk.n_images} cameras, {sblk.n_obs} observations) on one host core"),
                "linear_solves": rep_c["linear_solves"], "final_rms": rep_c["rms"],
-               "gpu_same_sample_s": rep_g["solve_seconds"]}
+               "gpu_same_sample_s": rep_g["solve_seconds"], "parallel": cpu_sample_parallel(sblk, sout)}
 
     if rank == 0:
         r0 = reps[-1]
@@ -336,7 +381,7 @@ def main():
             "config": config_dict(args, blk),
             "plain": plain,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": block_bytes(blk),
-                    "d2h_bytes_per_step": state_bytes(blk)},
+                    "d2h_bytes_per_step": state_bytes(blk), "host_input_memory": e2e_mem},
             "gpu_launches": int(r0["kernel_launches"]),
             "roofline": roofline,
             "cpu_baseline": cpu,

@@ -177,7 +177,9 @@ int32_t rpba_get_log(rpba_handle *h, char *log, size_t cap);
 /* Per-observation back-projection errors of the uploaded block, in track
  * order (dx, dy as double), as EvalLSA/CalcCorrPointMulti compute them
  * (rpbacore.cpp:778-837, 882-941).  resid has 2*pt_obs_off[n_points]
- * entries; entries of points with fewer than two observations are 0. */
+ * entries; entries of points with fewer than two observations are 0.
+ * The handle must have been created with opt->exteval = 1 (RPBA_ERR_ARG
+ * otherwise), as Exteval is a mode of CalcPLSA (extevalflag). */
 int32_t rpba_exteval(rpba_handle *h, double *resid, rpba_report *rep);
 /* The float sum of v[0..n) accumulated left to right, one rounding per
  * addition -- the way the reference accumulates its cost and weight sums

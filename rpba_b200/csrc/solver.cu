@@ -399,19 +399,24 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   H->addmask = (o->k2 ? 1 : 0) | (o->k4 ? 2 : 0) | (o->f ? 4 : 0);
   H->nadd = (o->k2 ? 1 : 0) + (o->k4 ? 1 : 0) + (o->f ? 1 : 0);
   if (n > 65535) return RPBA_ERR_UNSUPPORTED;
-  // host copies of the caller's block (output of untouched points, Exteval)
+  // host copies of the caller's cameras and points (the output keeps the
+  // input values of points the solve does not use); the observations and
+  // tracks only for an Exteval handle, whose rpba_exteval reads them (a
+  // solve handle takes them straight from the caller's arrays to the device)
   H->h_pmat.assign(b->pmat, b->pmat + 12 * n);
   H->h_K.assign(b->K, b->K + 9 * n);
   H->h_dist.assign(b->distpara, b->distpara + 2 * n);
   H->h_XX.assign(b->XX, b->XX + 3 * np);
-  H->h_img_off.assign(b->img_obs_off, b->img_obs_off + n + 1);
-  H->h_xg.assign(b->xg, b->xg + 2 * H->n_slots);
-  H->h_wx.assign(b->wx, b->wx + H->n_slots);
-  H->h_wy.assign(b->wy, b->wy + H->n_slots);
-  H->h_wxy.assign(b->wxy, b->wxy + H->n_slots);
-  H->h_pt_off.assign(b->pt_obs_off, b->pt_obs_off + np + 1);
-  H->h_pt_img.assign(b->pt_obs_image, b->pt_obs_image + H->n_track_in);
-  H->h_pt_slot.assign(b->pt_obs_slot, b->pt_obs_slot + H->n_track_in);
+  if (o->exteval) {
+    H->h_img_off.assign(b->img_obs_off, b->img_obs_off + n + 1);
+    H->h_xg.assign(b->xg, b->xg + 2 * H->n_slots);
+    H->h_wx.assign(b->wx, b->wx + H->n_slots);
+    H->h_wy.assign(b->wy, b->wy + H->n_slots);
+    H->h_wxy.assign(b->wxy, b->wxy + H->n_slots);
+    H->h_pt_off.assign(b->pt_obs_off, b->pt_obs_off + np + 1);
+    H->h_pt_img.assign(b->pt_obs_image, b->pt_obs_image + H->n_track_in);
+    H->h_pt_slot.assign(b->pt_obs_slot, b->pt_obs_slot + H->n_track_in);
+  }
   {
     H->ES.max_grid = exact_sum_max_grid(H->dev);
     H->ES.Rc = dalloc<long long>(2 * (size_t)H->ES.max_grid, own);
@@ -1171,18 +1176,35 @@ int32_t rpba_get_state(rpba_handle *H, rpba_block *blk) {
     const int n = H->nimg, no = H->L.nobs, np = H->L.npts;
     std::vector<double> P(12 * (size_t)n);
     std::vector<CamState> cams(n);
-    std::vector<int> o_cam(no), o_slot(no), pt_off(np + 1), pt_id(np);
+    std::vector<int> pt_off(np + 1), pt_id(np);
     std::vector<double> X(3 * (size_t)np);
     auto dn = [&](void *h, const void *d, size_t bytes) {
       if (bytes) RPBA_CUDA_CHECK(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, H->s));
     };
     dn(P.data(), H->L.Pacc, sizeof(double) * P.size());
     dn(cams.data(), H->L.camn, sizeof(CamState) * n);
-    dn(o_cam.data(), H->L.o_cam, sizeof(int) * no);
-    dn(o_slot.data(), H->L.o_slot, sizeof(int) * no);
     dn(pt_off.data(), H->L.pt_off, sizeof(int) * (np + 1));
     dn(pt_id.data(), H->L.pt_id, sizeof(int) * np);
     dn(X.data(), H->L.XPM + H->nrioff, sizeof(double) * 3 * np);
+    RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
+    // The output tracks are the device's, point by point in increasing
+    // point order.  When the device lists are one CSR from 0 to nobs over
+    // strictly increasing point ids (the layout the solver keeps), that
+    // concatenation is the device arrays as they are: copy them straight
+    // into the caller's; otherwise gather them point by point.
+    bool direct = pt_off[0] == 0 && pt_off[np] == no && no <= H->n_track_in;
+    for (int q = 0; q < np && direct; ++q)
+      direct = pt_off[q] <= pt_off[q + 1] && pt_id[q] >= 0 && pt_id[q] < H->XXnr && (q == 0 || pt_id[q - 1] < pt_id[q]);
+    std::vector<int> o_cam, o_slot;
+    if (direct) {
+      dn(b->pt_obs_image, H->L.o_cam, sizeof(int) * no);
+      dn(b->pt_obs_slot, H->L.o_slot, sizeof(int) * no);
+    } else {
+      o_cam.resize(no);
+      o_slot.resize(no);
+      dn(o_cam.data(), H->L.o_cam, sizeof(int) * no);
+      dn(o_slot.data(), H->L.o_slot, sizeof(int) * no);
+    }
     RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
     for (size_t i = 0; i < P.size(); ++i) b->pmat[i] = (float)P[i];
     for (int i = 0; i < n; ++i) {
@@ -1206,9 +1228,13 @@ int32_t rpba_get_state(rpba_handle *H, rpba_block *blk) {
     b->pt_obs_off[0] = 0;
     for (int i = 0; i < H->XXnr; ++i) {
       if (q < np && pt_id[q] == i) {
-        for (int o = pt_off[q]; o < pt_off[q + 1]; ++o, ++w) {
-          b->pt_obs_image[w] = o_cam[o];
-          b->pt_obs_slot[w] = o_slot[o];
+        if (direct) {
+          w = pt_off[q + 1];
+        } else {
+          for (int o = pt_off[q]; o < pt_off[q + 1]; ++o, ++w) {
+            b->pt_obs_image[w] = o_cam[o];
+            b->pt_obs_slot[w] = o_slot[o];
+          }
         }
         for (int j = 0; j < 3; ++j) b->XX[3 * i + j] = (float)X[3 * q + j];
         ++q;
@@ -1221,7 +1247,7 @@ int32_t rpba_get_state(rpba_handle *H, rpba_block *blk) {
 
 // EvalLSA on the uploaded block (rpbacore.cpp:882-941).
 int32_t rpba_exteval(rpba_handle *H, double *resid, rpba_report *rep) {
-  if (!H) return RPBA_ERR_ARG;
+  if (!H || !H->opt.exteval) return RPBA_ERR_ARG;
   struct A {
     rpba_handle *H;
     double *resid;

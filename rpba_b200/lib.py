@@ -358,7 +358,14 @@ class Solver:
         return buf.value.decode()
 
     def state(self) -> Block:
-        out = self.block.copy()
+        """The adjusted block: new cameras, points and tracks (the
+        observation arrays xg, wx, wy, wxy and img_obs_off, which a solve
+        does not change, are shared with the input block).  The track
+        arrays keep the input's length; entries past pt_obs_off[-1] are 0."""
+        b = self.block
+        out = Block(np.empty_like(b.pmat), np.empty_like(b.K), np.empty_like(b.distpara), np.empty_like(b.XX),
+                    b.img_obs_off, b.xg, b.wx, b.wy, b.wxy, np.empty_like(b.pt_obs_off),
+                    np.zeros_like(b.pt_obs_image), np.zeros_like(b.pt_obs_slot))
         cb = out.as_c()
         st = load().rpba_get_state(self.h, C.byref(cb))
         if st != 0:
