@@ -319,6 +319,61 @@ int32_t rpba_triangulate_parts(const rpba_block *blk, const float *sig0w, const 
                                const int32_t *part, int32_t nparts, double *XX_out, uint8_t *keep, float *sig0v,
                                uint8_t *conv, double *sig0io, int64_t *redundancy, float *w3d);
 
+/* One GCP-mode step of the LSA: the per-partition call of the parallel
+ * RPBA, replacing LSA::InputLSAP + Adjust(false, os, true, 0, W3ijiv[it],
+ * true, gcpdatav[it]) + OutputLSAP (rpbacore.cpp:212-229; rbacore.cpp:
+ * 233-331, 333-616, 620-639).  blk holds the partition's images and its
+ * points; every camera is free (no scale camera); point p with
+ * gcpinfo[p] > -1 is held at gcpdata[gcpinfo[p]] (3 doubles) by a 3-D prior
+ * whose weight block (6 floats: XX YY ZZ XY XZ YZ) is the next row of W3 in
+ * the order of the points the LSA keeps (the reference's gcpnum); a point
+ * is kept with two or more observations, or with one and gcpinfo > 0.  The
+ * additional parameters count ncam_total times in the redundancy (the
+ * reference's nrcameras).  pmat_d: the cameras in double precision (null:
+ * blk->pmat).  One damped step (multfact 1e-4), stored unconditionally,
+ * without robust reweighting; the log gets the Sigma0 and Sigma0AO lines.
+ * Outputs: blk (cameras, points, tracks as rpba_get_state), pmat_d_out
+ * (12 doubles per image) and point_used (1 for the points the step took),
+ * each optional.  FP64 only (RPBA_PREC_FP64; RPBA_SOLVER_PCG with the
+ * reference's stop rule, or RPBA_SOLVER_DIRECT). */
+int32_t rpba_lsa_gcp_step(rpba_block *blk, const rpba_options *opt, const int32_t *gcpinfo, const float *W3,
+                          int32_t n_w3, const double *gcpdata, int32_t n_gcp, int32_t ncam_total,
+                          const double *pmat_d, double *pmat_d_out, uint8_t *point_used, rpba_report *rep,
+                          char *log, size_t cap);
+
+/* The parallel RPBA: the partitioned branch of CalcPLSA (rpbacore.cpp:
+ * 100-510), which the reference takes when min(Threads, iround(images /
+ * 70)) > 1.  part[image] in 0 .. nthreads - 1 (rpba_partition_images
+ * replaces the reference's METIS cut).  Each outer iteration after the
+ * first takes one rpba_lsa_gcp_step per partition and merges with
+ * CalcLSAXMulti on the GPU (robust thresholds when the robust stage starts,
+ * robust deletion, weight blocks of the shared points); the best iteration
+ * (lowest sigma0) is written back to blk (cameras, points, tracks), as the
+ * reference writes pointXXvold, PMatricesdold, XXdold and camerasold
+ * (rpbacore.cpp:498-507).  stats (optional): {sigma0 of the best
+ * iteration, outer iterations}.  FP64 only, like rpba_lsa_gcp_step. */
+int32_t rpba_calc_plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads, const int32_t *part,
+                                char *log, size_t cap, double *stats);
+
+/* The two steps of the parallel RPBA's loop: the partition step (the
+ * signature of rpba_lsa_gcp_step) and the merge pass (CalcLSAXMulti over
+ * every point of b with the cameras Pd, 12 doubles per image; part null:
+ * no weight blocks; s0_pt / red_pt: every point's contribution to the sum
+ * and to the redundancy, as the reference's per-thread sums take them). */
+typedef int32_t (*rpba_gcp_step_fn)(rpba_block *blk, const rpba_options *opt, const int32_t *gcpinfo,
+                                    const float *W3, int32_t n_w3, const double *gcpdata, int32_t n_gcp,
+                                    int32_t ncam_total, const double *pmat_d, double *pmat_d_out,
+                                    uint8_t *point_used, rpba_report *rep, char *log, size_t cap);
+typedef int32_t (*rpba_merge_fn)(const rpba_block *b, const double *Pd, const float *sig0w, int32_t robustmode,
+                                 int32_t weight_only, const int32_t *part, int32_t nparts, int32_t device,
+                                 double *XX_out, uint8_t *keep, float *sig0v, uint8_t *conv, float *w3d,
+                                 double *s0_pt, int32_t *red_pt);
+/* rpba_calc_plsa_parallel's loop with both steps supplied by the caller
+ * (the host-side check of the loop binds CPU implementations of them). */
+int32_t rpba_calc_plsa_parallel_hosted(rpba_block *blk, const rpba_options *opt, int32_t nthreads,
+                                       const int32_t *part, char *log, size_t cap, double *stats,
+                                       rpba_gcp_step_fn step, rpba_merge_fn merge);
+
 /* Camera partition of the reference's parallel RPBA: replaces
  * PartitionpointXXv (rpbacore.cpp:945-1037), which cuts the images'
  * covisibility graph (an edge where two images share a point observed at

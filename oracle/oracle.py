@@ -167,6 +167,32 @@ def lsa_gcp_step(block: Block, gcpinfo, W3, gcpdata, ncam_total: int, opts: Rpba
     return st, buf.value.decode()
 
 
+def lsa_gcp_step_full(block: Block, gcpinfo, W3, gcpdata, ncam_total: int, pmat_d=None,
+                      opts: RpbaOptionsC | None = None, log_cap: int = 1 << 16):
+    """oracle_lsa_gcp_step_full on a copy of ``block``: the GCP-mode step
+    with the cameras in double precision in and out.  Returns (status,
+    block, cameras (n_images, 12), point_used, log)."""
+    b = block.copy()
+    cb = b.as_c()
+    o = opts if opts is not None else make_options()
+    gi = np.ascontiguousarray(gcpinfo, np.int32)
+    w3 = np.ascontiguousarray(W3, np.float32).reshape(-1)
+    gd = np.ascontiguousarray(gcpdata, np.float64).reshape(-1)
+    pin = None if pmat_d is None else np.ascontiguousarray(pmat_d, np.float64).reshape(-1)
+    pout = np.zeros((b.n_images, 12))
+    used = np.zeros(max(b.n_points, 1), np.uint8)
+    buf = C.create_string_buffer(log_cap)
+    f = lib().oracle_lsa_gcp_step_full
+    f.restype = C.c_int32
+    f.argtypes = [C.POINTER(RpbaBlockC), C.POINTER(RpbaOptionsC), C.POINTER(C.c_int32), C.POINTER(C.c_float),
+                  C.c_int32, C.POINTER(C.c_double), C.c_int32, C.c_int32, C.POINTER(C.c_double),
+                  C.POINTER(C.c_double), C.POINTER(C.c_uint8), C.c_void_p, C.c_char_p, C.c_size_t]
+    st = f(C.byref(cb), C.byref(o), gi.ctypes.data_as(C.POINTER(C.c_int32)), w3.ctypes.data_as(C.POINTER(C.c_float)),
+           int(w3.size // 6), _dp(gd), int(gd.size // 3), int(ncam_total), None if pin is None else _dp(pin),
+           _dp(pout), used.ctypes.data_as(C.POINTER(C.c_uint8)), None, buf, log_cap)
+    return st, b, pout, used[:b.n_points].astype(bool), buf.value.decode()
+
+
 def parallel_threads(n_images: int, threads: int) -> int:
     """Partition count of CalcPLSA (rpbacore.cpp:79-85): min(Threads,
     iround(images / 70)), iround rounding halves away from zero; the

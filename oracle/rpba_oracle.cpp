@@ -1972,6 +1972,55 @@ extern "C" int32_t oracle_lsa_gcp_step(rpba_block *blk, const rpba_options *o, c
   return st;
 }
 
+/* The parallel RPBA's two steps with the signatures of the library's
+ * rpba_gcp_step_fn and rpba_merge_fn (checker side of the host-side test of
+ * the library's loop):
+ *   the partition step: oracle_lsa_gcp_step with the cameras in double
+ *   precision in and out and the points PointXXvIn took; the block gets
+ *   cameras, points and tracks whatever the step's status (OutputLSAP runs
+ *   after Adjust either way, rpbacore.cpp:229-231);
+ *   the merge pass: CalcLSAXMulti over every point (tri_impl), with every
+ *   point's contribution to the sum and to the redundancy. */
+extern "C" int32_t oracle_lsa_gcp_step_full(rpba_block *blk, const rpba_options *o, const int32_t *gcpinfo,
+                                            const float *W3, int32_t n_w3, const double *gcpdata, int32_t n_gcp,
+                                            int32_t ncam_total, const double *pmat_d, double *pmat_d_out,
+                                            uint8_t *point_used, rpba_report *rep, char *log, size_t cap) {
+  if (!blk || !o || !gcpinfo || (n_gcp > 0 && !gcpdata) || ncam_total < blk->n_images) return RPBA_ERR_ARG;
+  (void)n_w3;
+  (void)rep;
+  std::string os;
+  Opts op = make_opts(o);
+  op.robust = false;
+  GcpIn g{gcpinfo, W3, gcpdata, ncam_total};
+  g.Pd = pmat_d;
+  LSA lsa(blk, op, &os, g);
+  const int st = lsa.adjust_gcp_step();
+  lsa.output(blk);
+  if (pmat_d_out) std::memcpy(pmat_d_out, lsa.P.data(), sizeof(double) * lsa.P.size());
+  if (point_used) {
+    std::memset(point_used, 0, (size_t)blk->n_points);
+    for (int q : lsa.nrpv) point_used[q] = 1;
+  }
+  copy_log(os, log, cap);
+  return st;
+}
+
+extern "C" int32_t oracle_merge(const rpba_block *b, const double *Pd, const float *sig0w, int32_t robustmode,
+                                int32_t weight_only, const int32_t *part, int32_t nparts, int32_t device,
+                                double *XX_out, uint8_t *keep, float *sig0v, uint8_t *conv, float *w3d,
+                                double *s0_pt, int32_t *red_pt) {
+  (void)device;
+  for (int p = 0; p < b->n_points; ++p) {
+    double s0 = 0.;
+    int64_t red = 0;
+    tri_impl(b, Pd, p, p + 1, sig0w, robustmode, weight_only, part, nparts, XX_out, keep, sig0v, conv, &s0, &red,
+             w3d);
+    if (s0_pt) s0_pt[p] = s0;
+    if (red_pt) red_pt[p] = (int32_t)red;
+  }
+  return RPBA_OK;
+}
+
 /* ---------------------------------------------------------------------
  * Parallel RPBA: the partitioned branch of CalcPLSA, rpbacore.cpp:100-510.
  * The images are cut into nthreads partitions (part[image]; the reference

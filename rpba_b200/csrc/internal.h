@@ -8,6 +8,7 @@
 
 #include <vector>
 
+#include "../../include/rpba_b200.h"
 #include "common.cuh"
 
 namespace rpba {
@@ -68,6 +69,17 @@ struct DevLSA {
   const int2 *rowspan;      // [nimg] (diagonal entry, end entry) of each row
   float *tpart;             // [nboff * 9] FP32 form: transposed block products
   int *err;            // device error word
+  // GCP mode of the parallel RPBA's per-partition LSA (ao = 1): every
+  // camera free (no scale camera, camera 0 with a full block), and the
+  // points shared with other partitions held by 3-D priors.  Per point
+  // (local order): the GCP index into gcpdata, or -1, and the row of its
+  // weight block in W3 (6 floats: XX YY ZZ XY XZ YZ).  ao = 0 leaves every
+  // kernel as in the global LSA.
+  int ao = 0;
+  int n_w3 = 0;
+  const int *pt_gcp = nullptr, *pt_w3row = nullptr;
+  const float *W3 = nullptr;
+  const double *gcpdata = nullptr;
 };
 
 // Storage stride (elements) of one 9x9 block of the reduced camera system in
@@ -102,6 +114,9 @@ void launch_prepare_weights(const DevLSA &L, cudaStream_t s);
 void launch_reweight(const DevLSA &L, int iflag, float *vals_scratch, float *sig00v, int *nflag,
                      cudaStream_t s);
 void launch_final_cost(const DevLSA &L, double *partials, int nparts, cudaStream_t s);
+// GCP mode: the prior cost term of every point at the state XM (0 for a
+// point without a prior), out[0 .. npts)
+void launch_gcp_cost(const DevLSA &L, const double *XM, float *out, cudaStream_t s);
 void launch_exteval(int n_points, const int *pt_off, const int *pt_img, const int *pt_slot,
                     const int *img_off, const float *pmat, const float *K, const float *dist,
                     const float *XX, const float *xg, const float *wx, const float *wy,
@@ -272,6 +287,9 @@ struct TrackIn {
   const int *pt_off, *pt_img, *pt_slot, *img_off;
   const float *xg, *wx, *wy, *wxy, *XX;
   int np, n;
+  // GCP mode: per point its GCP index or -1; a point with a GCP index above
+  // 0 is kept with a single observation (rbacore.cpp:1954-1956)
+  const int *gcp = nullptr;
 };
 struct TrackScan {
   int *cnt, *pval, *ooff, *pidx, *err;  // [np + 1]
@@ -282,6 +300,7 @@ struct TrackOut {
   float2 *o_xg;
   float4 *o_w;
   double *X;
+  int *gcp = nullptr;  // GCP mode: the GCP index of every kept point
 };
 // returns the error bits (1: an index out of range, 2: an image twice in a track)
 int track_count(const TrackIn &T, TrackScan &W, int *nobs, int *npts, long long *max_pairs, cudaStream_t s);
@@ -293,6 +312,14 @@ int build_pairs(DevLSA &L, StructWork &S, long long max_pairs, long long *npairs
                 cudaStream_t s);
 void build_bsr(DevLSA &L, StructWork &S, cudaStream_t s);
 cudaError_t cub_exclusive_sum_int(void *tmp, size_t &bytes, const int *in, int *out, int n, cudaStream_t s);
+// CalcLSAXMulti for every point of b (triangulate.cu): the cameras Pd in
+// double precision (null: b->pmat), the other arguments as
+// rpba_triangulate_parts (part null: no weight blocks); s0_pt / red_pt
+// (optional): every point's contribution to sig0io and the redundancy
+int32_t triangulate_impl(const rpba_block *b, const double *Pd, const float *sig0w, const rpba_tri_options *opt,
+                         const int32_t *part, int32_t nparts, double *XX_out, uint8_t *keep, float *sig0v,
+                         uint8_t *conv, double *sig0io, int64_t *redundancy, float *w3d, double *s0_pt,
+                         int32_t *red_pt);
 
 }  // namespace rpba
 

@@ -57,8 +57,10 @@ struct Acc {
   __device__ __forceinline__ double value() const { return (double)s - (double)c; }
 };
 
+// In GCP mode camera 0 is free like the others and there is no scale
+// camera (normcamera = -1; rbacore.cpp:697-698, 1005-1008).
 __device__ __forceinline__ int role_of(const DevLSA &L, int k) {
-  return k == 0 ? ROLE_ZERO : (k == L.normcamera ? ROLE_NORM : ROLE_FREE);
+  return (k == 0 && !L.ao) ? ROLE_ZERO : (k == L.normcamera ? ROLE_NORM : ROLE_FREE);
 }
 
 // ----------------------------------------------------------- cost pass
@@ -88,6 +90,31 @@ __global__ void k_cost(DevLSA L, const double *__restrict__ XM, int srmv) {
       L.o_s0rmv[i] = val;
     }
   }
+}
+
+// GCP mode: the prior cost term of every point at the state XM, in the
+// reference's float accumulation (sig0ao, rbacore.cpp:1677-1729): the double
+// form d^T W d (d = gcp - X) in the reference's operation order, rounded to
+// float; 0 for a point without a prior.
+__global__ void k_gcp_cost(DevLSA L, const double *__restrict__ XM, float *out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= L.npts) return;
+  float t = 0.f;
+  const int gi = L.pt_gcp[p];
+  if (gi > -1) {
+    const float *w = L.W3 + 6 * (size_t)L.pt_w3row[p];
+    const double *gx = L.gcpdata + 3 * (size_t)gi;
+    const double *X = XM + L.nrioff + 3 * (size_t)p;
+    const double d1 = __dsub_rn(gx[0], X[0]), d2 = __dsub_rn(gx[1], X[1]), d3 = __dsub_rn(gx[2], X[2]);
+    const double a = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(d1, d1), (double)w[0]),
+                                         __dmul_rn(__dmul_rn(d2, d2), (double)w[1])),
+                               __dmul_rn(__dmul_rn(d3, d3), (double)w[2]));
+    const double b = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(d1, d2), (double)w[3]),
+                                         __dmul_rn(__dmul_rn(d1, d3), (double)w[4])),
+                               __dmul_rn(__dmul_rn(d2, d3), (double)w[5]));
+    t = __double2float_rn(__dadd_rn(a, __dmul_rn(2., b)));
+  }
+  out[p] = t;
 }
 
 // Sequential float sum in array order: the reference accumulates its cost
@@ -194,6 +221,18 @@ __global__ void k_point(DevLSA L, double multfact1) {
   for (int j = 0; j < 9; ++j) V[j] = grp_sum(V[j]);
 #pragma unroll
   for (int j = 0; j < 3; ++j) g[j] = grp_sum(g[j]);
+  if (L.ao && valid && L.pt_gcp[p] > -1) {
+    // CalcDerivatives3DGCP (rbacore.cpp:1677-1729): the 3-D prior of a
+    // point shared with other partitions, residual gcp - X, B = -I
+    const float *w = L.W3 + 6 * (size_t)L.pt_w3row[p];
+    const double *gx = L.gcpdata + 3 * (size_t)L.pt_gcp[p];
+    const double d1 = gx[0] - X0, d2 = gx[1] - X1, d3 = gx[2] - X2;
+    const double Wm[9] = {w[0], w[3], w[4], w[3], w[1], w[5], w[4], w[5], w[2]};
+#pragma unroll
+    for (int j = 0; j < 9; ++j) V[j] += Wm[j];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) g[r] += (-Wm[r * 3]) * d1 + (-Wm[r * 3 + 1]) * d2 + (-Wm[r * 3 + 2]) * d3;
+  }
   V[0] = (T)(V[0] * multfact1);
   V[4] = (T)(V[4] * multfact1);
   V[8] = (T)(V[8] * multfact1);
@@ -655,7 +694,7 @@ __global__ void k_decode(DevLSA L, const double *__restrict__ XM) {
   // previous trial cameras, which OutputLSAc reports
   if (*(volatile int *)L.err & 1) return;
   CamState &c = L.camn[k];
-  if (k == 0) {
+  if (k == 0 && !L.ao) {
     int a = -1;
     if (L.addmask & 1) c.d0 = XM[++a];
     if (L.addmask & 2) c.d1 = XM[++a];
@@ -698,7 +737,7 @@ __global__ void k_decode(DevLSA L, const double *__restrict__ XM) {
 __global__ void k_encode(DevLSA L) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= L.nimg) return;
-  if (k == 0) {
+  if (k == 0 && !L.ao) {
     int a = -1;
     if (L.addmask & 1) L.XPM[++a] = L.dc[0];
     if (L.addmask & 2) L.XPM[++a] = L.dc[1];
@@ -1090,6 +1129,10 @@ void launch_reweight(const DevLSA &L, int iflag, float *vals, float *sig00v, int
 
 void launch_final_cost(const DevLSA &L, double *partials, int nparts, cudaStream_t s) {
   k_final_cost<<<nparts, 256, 0, s>>>(L, partials);
+}
+
+void launch_gcp_cost(const DevLSA &L, const double *XM, float *out, cudaStream_t s) {
+  if (L.npts > 0) k_gcp_cost<<<nblk(L.npts, 256), 256, 0, s>>>(L, XM, out);
 }
 
 void launch_exteval(int n_points, const int *pt_off, const int *pt_img, const int *pt_slot, const int *img_off,

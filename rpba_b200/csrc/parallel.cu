@@ -1,0 +1,432 @@
+// parallel.cu -- the parallel RPBA (the partitioned branch of CalcPLSA,
+// rpbacore.cpp:100-510) on the GPU: host control, device work.
+//
+// The images are cut into nthreads partitions (part[image]; the reference
+// cuts the covisibility graph with METIS, rpba_partition_images replaces
+// it).  Outer iteration `iter`:
+//   iter > 1: every partition takes one GCP-mode LSA step on its images and
+//     the observations in them (rpba_lsa_gcp_step): the points it shares
+//     with other partitions are held by 3-D priors with the weight blocks of
+//     the last merge; the additional parameters stay fixed at iter 2; its
+//     cameras replace the scene's;
+//   the merge: every point is refined against the new cameras by
+//   CalcLSAXMulti on the GPU (one launch over all points): first a robust
+//   pass that gives the per-image thresholds when the robust stage starts,
+//   then the main pass (robust deletion, weight-only at iter 1, the
+//   per-partition weight blocks).  The reference sums its per-thread point
+//   chunks and then the chunks; the per-point contributions are summed here
+//   the same way, so sigma0 and every decision follow it;
+//   sigma0 = sum / (redundancy - unknowns); the best state is kept, and the
+//   points seen by more than one partition become the next GCPs at their
+//   refined positions;
+// until iflag runs out (the sig0frac rule) or 50 iterations.  The partition
+// steps run one after another: each is a whole-GPU solve.
+//
+// The loop is host code over two steps, the partition step and the merge
+// pass; rpba_calc_plsa_parallel binds them to the GPU (rpba_lsa_gcp_step and
+// the CalcLSAXMulti kernel), rpba_calc_plsa_parallel_hosted takes them from
+// the caller, so that the loop itself can be checked without a GPU.
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rpba_b200.h"
+#include "internal.h"
+
+namespace {
+
+struct PObs {
+  int image, slot;
+};
+struct PCam {
+  float K[9], d[2];
+};
+
+// a block over given cameras and point lists (views into its own vectors)
+struct TmpBlock {
+  rpba_block b{};
+  std::vector<int32_t> off, img, slot, ioff;
+  std::vector<float> XX, pmat, K, dist, xg, wx, wy, wxy;
+};
+
+// the merge pass on the GPU
+int32_t gpu_merge(const rpba_block *b, const double *Pd, const float *sig0w, int32_t robustmode, int32_t weight_only,
+                  const int32_t *part, int32_t nparts, int32_t device, double *XX_out, uint8_t *keep, float *sig0v,
+                  uint8_t *conv, float *w3d, double *s0_pt, int32_t *red_pt) {
+  rpba_tri_options to{};
+  to.robustmode = robustmode;
+  to.weight_only = weight_only;
+  to.device = device;
+  double a = 0.;
+  int64_t r = 0;
+  return rpba::triangulate_impl(b, Pd, sig0w, &to, part, nparts, XX_out, keep, sig0v, conv, &a, &r, w3d, s0_pt,
+                                red_pt);
+}
+
+int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads, const int32_t *part, char *log,
+                      size_t cap, double *stats, rpba_gcp_step_fn step_fn, rpba_merge_fn merge_fn) {
+  if (!blk || !opt || !part || nthreads < 2 || blk->n_images < 1 || blk->n_points < 0) return RPBA_ERR_ARG;
+  const int nrimages = blk->n_images, pxs = blk->n_points, T = nthreads;
+  for (int i = 0; i < nrimages; ++i)
+    if (part[i] < 0 || part[i] >= T) return RPBA_ERR_ARG;
+  std::string os;
+  const bool robustflag = opt->robust != 0;
+  const int nraddp = (opt->k2 ? 1 : 0) + (opt->k4 ? 1 : 0) + (opt->f ? 1 : 0);
+  // partitions: images in index order
+  std::vector<std::vector<int>> imgindv(T);
+  std::vector<int32_t> imgindbv(nrimages);
+  for (int i = 0; i < nrimages; ++i) {
+    imgindv[part[i]].push_back(i);
+    imgindbv[i] = part[i];
+  }
+  for (int it = 0; it < T; ++it)
+    if (imgindv[it].empty()) return RPBA_ERR_ARG;
+  for (int p = 0; p < pxs; ++p)
+    for (int t = blk->pt_obs_off[p]; t < blk->pt_obs_off[p + 1]; ++t) {
+      const int im = blk->pt_obs_image[t];
+      if (im < 0 || im >= nrimages || blk->pt_obs_slot[t] < 0 ||
+          blk->pt_obs_slot[t] >= blk->img_obs_off[im + 1] - blk->img_obs_off[im])
+        return RPBA_ERR_ARG;
+    }
+  // state: points and cameras in double precision, cameras' intrinsics
+  std::vector<double> XXd(3 * (size_t)pxs), XXdold, PMd(12 * (size_t)nrimages), PMdold;
+  for (size_t i = 0; i < XXd.size(); ++i) XXd[i] = (double)blk->XX[i];
+  for (size_t i = 0; i < PMd.size(); ++i) PMd[i] = (double)blk->pmat[i];
+  PMdold = PMd;
+  XXdold = XXd;
+  std::vector<PCam> cameras(nrimages), cameraps, camerasnew(nrimages), camerasold(nrimages);
+  for (int i = 0; i < nrimages; ++i) {
+    for (int c = 0; c < 9; ++c) cameras[i].K[c] = blk->K[9 * i + c];
+    cameras[i].d[0] = blk->distpara[2 * i];
+    cameras[i].d[1] = blk->distpara[2 * i + 1];
+  }
+  cameraps = cameras;
+  std::vector<std::vector<PObs>> pointXXv(pxs), pointXXvold;
+  for (int p = 0; p < pxs; ++p)
+    for (int t = blk->pt_obs_off[p]; t < blk->pt_obs_off[p + 1]; ++t)
+      pointXXv[p].push_back({blk->pt_obs_image[t], blk->pt_obs_slot[t]});
+  pointXXvold = pointXXv;
+  std::vector<std::vector<char>> pitflagsv(pxs);
+  std::vector<int> gcpinfo(pxs, -1);
+  std::vector<std::vector<PCam>> camerasoit(T, cameras);
+  std::vector<std::vector<double>> PMdd(T, PMd);
+  std::vector<std::vector<std::vector<PObs>>> pointXXvv(T);
+  std::vector<std::vector<int>> pindv(T);
+  std::vector<std::vector<int32_t>> gcpinfov(T);
+  std::vector<std::vector<float>> W3ijiv(T);
+  std::vector<double> gcpdatav;
+  std::vector<float> sig0wv(nrimages, 0.f);
+  const int nrparimages = (nrimages - 2) * 6 + 5 + nrimages * nraddp;
+  const int nrppt = pxs / T;
+  std::vector<int> beginv(T), endv(T);
+  for (int c = 0; c < T; ++c) {
+    beginv[c] = nrppt * c;
+    endv[c] = c == T - 1 ? pxs : nrppt * (c + 1);
+  }
+  double sig0opt = 1.e20, sig0g = 0.;
+  int iflag = robustflag ? 2 : 1, iter = 1;
+  float sig0frac = 1.01f;
+  // the weight blocks of the last main pass, per point and partition (only
+  // points that converged in it keep two or more observations, and only
+  // those become GCPs)
+  std::vector<float> w3d((size_t)pxs * T * 6, 0.f);
+
+  // one CalcLSAXMulti pass over all points with the current cameras; applies
+  // the refined points and the deletions; returns (sum, redundancy) with the
+  // per-point contributions summed chunk by chunk
+  int status = RPBA_OK;
+  auto sweep = [&](int robustmode, bool weightonly, bool wxy, std::vector<std::vector<float>> *sig0vv,
+                   double *sum, long long *redund) {
+    TmpBlock tb;
+    tb.b = *blk;
+    tb.off.assign(pxs + 1, 0);
+    for (int p = 0; p < pxs; ++p) {
+      for (const PObs &q : pointXXv[p]) {
+        tb.img.push_back(q.image);
+        tb.slot.push_back(q.slot);
+      }
+      tb.off[p + 1] = (int32_t)tb.img.size();
+    }
+    tb.XX.resize(3 * (size_t)pxs);
+    for (size_t i = 0; i < tb.XX.size(); ++i) tb.XX[i] = (float)XXd[i];
+    tb.K.resize(9 * (size_t)nrimages);
+    tb.dist.resize(2 * (size_t)nrimages);
+    for (int i = 0; i < nrimages; ++i) {
+      std::memcpy(&tb.K[9 * (size_t)i], cameraps[i].K, sizeof(float) * 9);
+      tb.dist[2 * i] = cameraps[i].d[0];
+      tb.dist[2 * i + 1] = cameraps[i].d[1];
+    }
+    tb.b.pt_obs_off = tb.off.data();
+    tb.b.pt_obs_image = tb.img.data();
+    tb.b.pt_obs_slot = tb.slot.data();
+    tb.b.XX = tb.XX.data();
+    tb.b.K = tb.K.data();
+    tb.b.distpara = tb.dist.data();
+    const size_t nt = tb.img.size();
+    std::vector<double> XXo(3 * (size_t)pxs), s0pt(pxs);
+    std::vector<uint8_t> keep(std::max<size_t>(nt, 1)), conv(std::max(pxs, 1));
+    std::vector<float> sv(std::max<size_t>(nt, 1));
+    std::vector<int32_t> redpt(pxs);
+    status = merge_fn(&tb.b, PMd.data(), sig0wv.data(), robustmode, weightonly ? 1 : 0, wxy ? imgindbv.data() : nullptr,
+                      wxy ? T : 1, opt->device, XXo.data(), keep.data(), sv.data(), conv.data(),
+                      wxy ? w3d.data() : nullptr, s0pt.data(), redpt.data());
+    if (status != RPBA_OK) return false;
+    if (sig0vv)
+      for (int p = 0; p < pxs; ++p)
+        for (int t = tb.off[p]; t < tb.off[p + 1]; ++t) (*sig0vv)[tb.img[t]].push_back(sv[t]);
+    for (int p = 0; p < pxs; ++p) {
+      if (pointXXv[p].empty()) continue;
+      for (int q = 0; q < 3; ++q) XXd[3 * (size_t)p + q] = XXo[3 * (size_t)p + q];
+      std::vector<PObs> kept;
+      for (int t = tb.off[p]; t < tb.off[p + 1]; ++t)
+        if (keep[t]) kept.push_back(pointXXv[p][t - tb.off[p]]);
+      pointXXv[p] = kept;
+    }
+    double a = 0.;
+    long long r = 0;
+    for (int c = 0; c < T; ++c) {
+      double ac = 0.;
+      long long rc = 0;
+      for (int p = beginv[c]; p < endv[c]; ++p) {
+        ac += s0pt[p];
+        rc += redpt[p];
+      }
+      a += ac;
+      r += rc;
+    }
+    *sum = a;
+    *redund = r;
+    return true;
+  };
+
+  while (iflag > 0 && iter < 51) {
+    bool robustflagit = false;
+    if (iter > 1) {
+      rpba_options ol = *opt;
+      ol.robust = 0;
+      if (iter < 3) ol.k2 = ol.k4 = ol.f = 0;
+      for (int it = 0; it < T; ++it) {
+        const std::vector<int> &imgs = imgindv[it];
+        const int m = (int)imgs.size();
+        TmpBlock tb;
+        std::vector<int> loc(nrimages, -1);
+        std::vector<double> Pd(12 * (size_t)m), Pout(12 * (size_t)m);
+        tb.pmat.resize(12 * (size_t)m);
+        tb.K.resize(9 * (size_t)m);
+        tb.dist.resize(2 * (size_t)m);
+        tb.ioff.assign(m + 1, 0);
+        for (int li = 0; li < m; ++li) {
+          const int g = imgs[li];
+          loc[g] = li;
+          for (int c = 0; c < 12; ++c) {
+            Pd[12 * li + c] = PMdd[it][12 * (size_t)g + c];
+            tb.pmat[12 * li + c] = (float)Pd[12 * li + c];
+          }
+          std::memcpy(&tb.K[9 * (size_t)li], camerasoit[it][g].K, sizeof(float) * 9);
+          tb.dist[2 * li] = camerasoit[it][g].d[0];
+          tb.dist[2 * li + 1] = camerasoit[it][g].d[1];
+          for (int sl = blk->img_obs_off[g]; sl < blk->img_obs_off[g + 1]; ++sl) {
+            tb.xg.push_back(blk->xg[2 * sl]);
+            tb.xg.push_back(blk->xg[2 * sl + 1]);
+            tb.wx.push_back(blk->wx[sl]);
+            tb.wy.push_back(blk->wy[sl]);
+            tb.wxy.push_back(blk->wxy[sl]);
+          }
+          tb.ioff[li + 1] = (int32_t)tb.wx.size();
+        }
+        const int np = (int)pindv[it].size();
+        tb.off.assign(np + 1, 0);
+        tb.XX.resize(3 * (size_t)np);
+        for (int j = 0; j < np; ++j) {
+          for (const PObs &q : pointXXvv[it][j]) {
+            tb.img.push_back(loc[q.image]);
+            tb.slot.push_back(q.slot);
+          }
+          tb.off[j + 1] = (int32_t)tb.img.size();
+          for (int c = 0; c < 3; ++c) tb.XX[3 * j + c] = (float)XXd[3 * (size_t)pindv[it][j] + c];
+        }
+        rpba_block &b = tb.b;
+        b.n_images = m;
+        b.n_points = np;
+        b.pmat = tb.pmat.data();
+        b.K = tb.K.data();
+        b.distpara = tb.dist.data();
+        b.XX = tb.XX.data();
+        b.img_obs_off = tb.ioff.data();
+        b.xg = tb.xg.data();
+        b.wx = tb.wx.data();
+        b.wy = tb.wy.data();
+        b.wxy = tb.wxy.data();
+        b.pt_obs_off = tb.off.data();
+        b.pt_obs_image = tb.img.data();
+        b.pt_obs_slot = tb.slot.data();
+        std::vector<uint8_t> used(std::max(np, 1), 0);
+        std::vector<char> lg(1 << 12);
+        const int st = step_fn(&b, &ol, gcpinfov[it].data(), W3ijiv[it].data(),
+                                         (int32_t)(W3ijiv[it].size() / 6), gcpdatav.data(),
+                                         (int32_t)(gcpdatav.size() / 3), nrimages, Pd.data(), Pout.data(),
+                                         used.data(), nullptr, lg.data(), lg.size());
+        if (st != RPBA_OK && st != RPBA_ERR_NO_OBS_IMAGE && st != RPBA_ERR_LOW_REDUNDANCY &&
+            st != RPBA_ERR_NAN_STEP)
+          return st;
+        os += lg.data();
+        // OutputLSAP: PointXXvOut clears the lists of the points that
+        // PointXXvIn did not take; the stored cameras and camerasnew
+        for (int j = 0; j < np; ++j)
+          if (!used[j]) pointXXvv[it][j].clear();
+        for (int li = 0; li < m; ++li) {
+          const int gi = imgs[li];
+          std::memcpy(&PMdd[it][12 * (size_t)gi], &Pout[12 * (size_t)li], sizeof(double) * 12);
+          std::memcpy(camerasoit[it][gi].K, &tb.K[9 * (size_t)li], sizeof(float) * 9);
+          camerasoit[it][gi].d[0] = tb.dist[2 * li];
+          camerasoit[it][gi].d[1] = tb.dist[2 * li + 1];
+        }
+      }
+      for (int it = 0; it < T; ++it)
+        for (int gi : imgindv[it]) {
+          std::memcpy(&PMd[12 * (size_t)gi], &PMdd[it][12 * (size_t)gi], sizeof(double) * 12);
+          cameraps[gi] = camerasoit[it][gi];
+          camerasnew[gi] = camerasoit[it][gi];
+        }
+    }
+    if (iflag == 1) {
+      robustflagit = robustflag;
+      if (robustflag) sig0frac = 1.02f;
+    }
+    if (iter > 1) {
+      for (int p = 0; p < pxs; ++p) pointXXv[p].clear();
+      for (int it = 0; it < T; ++it)
+        for (size_t j = 0; j < pindv[it].size(); ++j)
+          for (const PObs &q : pointXXvv[it][j]) pointXXv[pindv[it][j]].push_back(q);
+      for (int p = 0; p < pxs; ++p)
+        if (pointXXv[p].size() < 2) pointXXv[p].clear();
+    } else {
+      for (int i = 0; i < nrimages; ++i) cameraps[i] = camerasnew[i] = cameras[i];
+    }
+    for (int p = 0; p < pxs; ++p)
+      if (!pointXXv[p].empty()) {
+        pitflagsv[p].assign(T, 0);
+        for (const PObs &q : pointXXv[p]) pitflagsv[p][imgindbv[q.image]] = 1;
+      }
+    double sum = 0.;
+    long long redundancy = 0;
+    if (robustflagit) {
+      std::vector<std::vector<float>> sig0vvs(nrimages);
+      if (!sweep(1, false, false, &sig0vvs, &sum, &redundancy)) return status;
+      for (int i = 0; i < nrimages; ++i) {
+        if (sig0vvs[i].empty()) {
+          sig0wv[i] = 0.f;
+        } else {
+          std::sort(sig0vvs[i].begin(), sig0vvs[i].end());
+          sig0wv[i] = 1.f / (sig0vvs[i][(int)sig0vvs[i].size() / 2] * 2.1981f);
+        }
+      }
+    }
+    if (!sweep(robustflagit ? 2 : 0, iter == 1, true, nullptr, &sum, &redundancy)) return status;
+    sig0g = sum / (double)(redundancy - nrparimages);
+    if (sig0g <= sig0opt) {
+      XXdold = XXd;
+      PMdold = PMd;
+      pointXXvold = pointXXv;
+      camerasold = camerasnew;
+    }
+    for (int it = 0; it < T; ++it) {
+      camerasoit[it] = camerasnew;
+      for (int gi : imgindv[it])
+        std::memcpy(&PMdd[it][12 * (size_t)gi], &PMd[12 * (size_t)gi], sizeof(double) * 12);
+      pointXXvv[it].clear();
+      pindv[it].clear();
+      W3ijiv[it].clear();
+    }
+    // the next GCPs: points (tracks of 2 or more) seen by more than one partition
+    int nrgcpnew = 0;
+    gcpdatav.clear();
+    for (int c = 0; c < T; ++c)
+      for (int p = beginv[c]; p < endv[c]; ++p) {
+        if (pointXXv[p].size() < 2) continue;
+        int gnum = 0;
+        for (int it = 0; it < T && gnum < 2; ++it) gnum += pitflagsv[p][it];
+        if (gnum > 1) {
+          gcpinfo[p] = nrgcpnew;
+          for (int q = 0; q < 3; ++q) gcpdatav.push_back(XXd[3 * (size_t)p + q]);
+          for (int it = 0; it < T; ++it)
+            if (pitflagsv[p][it])
+              for (int q = 0; q < 6; ++q) W3ijiv[it].push_back(w3d[((size_t)p * T + it) * 6 + q]);
+          ++nrgcpnew;
+        } else {
+          gcpinfo[p] = -1;
+        }
+      }
+    for (int p = 0; p < pxs; ++p) {
+      std::vector<std::vector<PObs>> per(T);
+      for (const PObs &q : pointXXv[p]) per[imgindbv[q.image]].push_back(q);
+      for (int it = 0; it < T; ++it)
+        if (!per[it].empty()) {
+          pointXXvv[it].push_back(per[it]);
+          pindv[it].push_back(p);
+        }
+    }
+    for (int it = 0; it < T; ++it) {
+      gcpinfov[it].resize(pindv[it].size());
+      for (size_t j = 0; j < pindv[it].size(); ++j) gcpinfov[it][j] = gcpinfo[pindv[it][j]];
+    }
+    if (iter > 1) {
+      if (sig0g <= sig0opt) {
+        if (sig0opt < sig0g * sig0frac && iter > 3)
+          --iflag;
+        else
+          sig0opt = sig0g;
+      } else if (iter > 3) {
+        --iflag;
+      }
+    }
+    ++iter;
+  }
+  // pointXXvio = pointXXvold, PMatrices, XX, cameras (rpbacore.cpp:498-507)
+  int32_t t = 0;
+  for (int p = 0; p < pxs; ++p) {
+    blk->pt_obs_off[p] = t;
+    for (const PObs &q : pointXXvold[p]) {
+      blk->pt_obs_image[t] = q.image;
+      blk->pt_obs_slot[t] = q.slot;
+      ++t;
+    }
+  }
+  blk->pt_obs_off[pxs] = t;
+  for (size_t i = 0; i < PMdold.size(); ++i) blk->pmat[i] = (float)PMdold[i];
+  for (size_t i = 0; i < XXdold.size(); ++i) blk->XX[i] = (float)XXdold[i];
+  for (int i = 0; i < nrimages; ++i) {
+    std::memcpy(blk->K + 9 * (size_t)i, camerasold[i].K, sizeof(float) * 9);
+    blk->distpara[2 * i] = camerasold[i].d[0];
+    blk->distpara[2 * i + 1] = camerasold[i].d[1];
+  }
+  if (stats) {
+    stats[0] = sig0opt;
+    stats[1] = iter - 1;
+  }
+  if (log && cap) {
+    const size_t n = std::min(cap - 1, os.size());
+    std::memcpy(log, os.data(), n);
+    log[n] = 0;
+  }
+  return RPBA_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t rpba_calc_plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads,
+                                           const int32_t *part, char *log, size_t cap, double *stats) {
+  if (opt && (opt->exteval || opt->precision != RPBA_PREC_FP64 ||
+              (opt->solver != RPBA_SOLVER_PCG && opt->solver != RPBA_SOLVER_DIRECT)))
+    return RPBA_ERR_UNSUPPORTED;
+  return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, rpba_lsa_gcp_step, gpu_merge);
+}
+
+extern "C" int32_t rpba_calc_plsa_parallel_hosted(rpba_block *blk, const rpba_options *opt, int32_t nthreads,
+                                                  const int32_t *part, char *log, size_t cap, double *stats,
+                                                  rpba_gcp_step_fn step, rpba_merge_fn merge) {
+  if (!step || !merge) return RPBA_ERR_ARG;
+  return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, step, merge);
+}

@@ -200,6 +200,15 @@ struct rpba_handle {
   std::vector<float> h_pmat, h_K, h_dist, h_XX, h_xg, h_wx, h_wy, h_wxy;
   std::vector<int32_t> h_img_off, h_pt_off, h_pt_img, h_pt_slot;
 
+  // GCP mode (the parallel RPBA's per-partition LSA): the scene's camera
+  // count (unknowns of the additional parameters), the kept points with a
+  // prior, the float sum of their weight diagonals (PrepareWeights3D), and
+  // three segments of per-point prior cost terms
+  bool ao = false;
+  int ncam_total = 0, nrgcp = 0;
+  float w3diag_sum = 0.f;
+  float *aoterm = nullptr;
+
   // static parameterisation
   int nadd = 0, addmask = 0, nrpari = 0, nrparir = 0, nrioff = 0, normcamera = -1, begini = 1;
   int minimagenrdel = 2, xpmsize = 0, npts0 = 0, nobs0 = 0;
@@ -373,6 +382,7 @@ struct rpba_handle {
 
   void reset();
   int adjust();
+  int adjust_gcp_step();
   bool calc_bundle_sep(double multfact, int nrunknowns);
   void robust_delete();
   void structure();
@@ -380,7 +390,18 @@ struct rpba_handle {
 
 // ------------------------------------------------------------- create
 
-static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *o) {
+// The GCP-mode inputs of rpba_lsa_gcp_step.
+struct GcpSetup {
+  const int32_t *gcpinfo;  // [n_points] GCP index or -1
+  const float *W3;         // [n_w3 x 6]
+  int32_t n_w3;
+  const double *gcpdata;   // [n_gcp x 3]
+  int32_t n_gcp;
+  int32_t ncam_total;
+  const double *Pd;        // [n_images x 12] cameras in double precision, or null
+};
+
+static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *o, const GcpSetup *gs = nullptr) {
   H->opt = *o;
   H->dev = o->device;
   RPBA_CUDA_CHECK(cudaSetDevice(H->dev));
@@ -395,7 +416,9 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   H->XXnr = np;
   H->n_slots = b->img_obs_off[n];
   H->n_track_in = b->pt_obs_off[np];
-  H->robust = o->robust != 0;
+  H->robust = o->robust != 0 && !gs;  // the partition LSAs run without robust reweighting
+  H->ao = gs != nullptr;
+  H->ncam_total = gs ? gs->ncam_total : n;
   H->addmask = (o->k2 ? 1 : 0) | (o->k4 ? 2 : 0) | (o->f ? 4 : 0);
   H->nadd = (o->k2 ? 1 : 0) + (o->k4 ? 1 : 0) + (o->f ? 1 : 0);
   if (n > 65535) return RPBA_ERR_UNSUPPORTED;
@@ -480,6 +503,7 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   TI.wy = (const float *)upt(b->wy, sizeof(float) * H->n_slots);
   TI.wxy = (const float *)upt(b->wxy, sizeof(float) * H->n_slots);
   TI.XX = (const float *)upt(b->XX, sizeof(float) * 3 * np);
+  if (gs) TI.gcp = (const int *)upt(gs->gcpinfo, sizeof(int) * np);
   TrackScan TW;
   TW.cnt = (int *)tmalloc(sizeof(int) * (np + 1));
   TW.pval = (int *)tmalloc(sizeof(int) * (np + 1));
@@ -500,7 +524,7 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
 
   // PrepareCameras (rbacore.cpp:670-700)
   std::vector<double> P(12 * (size_t)n);
-  for (size_t i = 0; i < P.size(); ++i) P[i] = (double)b->pmat[i];
+  for (size_t i = 0; i < P.size(); ++i) P[i] = gs && gs->Pd ? gs->Pd[i] : (double)b->pmat[i];
   {
     std::vector<double> Tv(3 * (size_t)n);
     for (int i = 0; i < n; ++i)
@@ -518,7 +542,10 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
       }
     }
   }
-  if (n < 2 || H->normcamera < 1) return RPBA_ERR_ARG;
+  if (gs)
+    H->normcamera = -1;  // every camera free (rbacore.cpp:697-698)
+  else if (n < 2 || H->normcamera < 1)
+    return RPBA_ERR_ARG;
   // PrepareIteration (rbacore.cpp:127-229)
   rectify_host(&P[0], 4);
   CamState c0{};
@@ -533,13 +560,22 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
       H->lflflag = true;
       break;
     }
-  H->nrioff = H->nadd + H->nrparir + H->nrpari * (n - 2);
-  H->begini = H->nadd > 0 ? 0 : 1;
-  H->xpmsize = n * 6 + 3 * np + 7 * n;
-  // camparv as EncodeCameras lays it out (rbacore.cpp:999-1087)
+  // camparv as EncodeCameras lays it out (rbacore.cpp:999-1087); in GCP
+  // mode every camera has the full block and the state vector has room for
+  // the scene's cameras (xpmsize with nrcameras, rbacore.cpp:324)
   H->camparv.assign(n + 1, 0);
-  H->camparv[1] = H->nadd;
-  for (int k = 1; k < n; ++k) H->camparv[k + 1] = H->camparv[k] + (k == H->normcamera ? H->nrparir : H->nrpari);
+  if (gs) {
+    H->nrioff = H->nrpari * n;
+    H->begini = 0;
+    H->xpmsize = n * 6 + 3 * np + 7 * std::max(H->ncam_total, n);
+    for (int k = 0; k < n; ++k) H->camparv[k + 1] = H->camparv[k] + H->nrpari;
+  } else {
+    H->nrioff = H->nadd + H->nrparir + H->nrpari * (n - 2);
+    H->begini = H->nadd > 0 ? 0 : 1;
+    H->xpmsize = n * 6 + 3 * np + 7 * n;
+    H->camparv[1] = H->nadd;
+    for (int k = 1; k < n; ++k) H->camparv[k + 1] = H->camparv[k] + (k == H->normcamera ? H->nrparir : H->nrpari);
+  }
 
   std::vector<CamState> cams(n);
   std::vector<double> Kc(9 * (size_t)n), dc(2 * (size_t)n);
@@ -585,7 +621,40 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
     TO.pt_off = H->d0_pt_off;
     TO.pt_id = H->d0_pt_id;
     TO.X = H->d0_X;
+    if (gs) TO.gcp = dalloc<int>(npp, own);
     track_scatter(TI, TW, TO, nobs, npts, H->s);
+    if (gs) {
+      // the weight-block row of every kept point with a prior: they are
+      // numbered in point order (gcpnum, rbacore.cpp:1677-1729)
+      std::vector<int> kg(npts), rows(npp, -1);
+      if (npts) RPBA_CUDA_CHECK(cudaMemcpyAsync(kg.data(), TO.gcp, sizeof(int) * npts, cudaMemcpyDeviceToHost, H->s));
+      RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
+      int nr = 0;
+      for (int q = 0; q < npts; ++q) {
+        if (kg[q] < -1 || kg[q] >= gs->n_gcp) return RPBA_ERR_ARG;
+        if (kg[q] > -1) rows[q] = nr++;
+      }
+      if (nr > gs->n_w3) return RPBA_ERR_ARG;
+      H->nrgcp = nr;
+      // PrepareWeights3D: the float sum of the weight diagonals of the
+      // kept priors, row by row (rbacore.cpp:787-818)
+      float ws = 0.f;
+      for (int i = 0; i < nr; ++i) ws += gs->W3[6 * i] + gs->W3[6 * i + 1] + gs->W3[6 * i + 2];
+      H->w3diag_sum = ws;
+      int *drows = dalloc<int>(npp, own);
+      float *dW3 = dalloc<float>(6 * (size_t)std::max(gs->n_w3, 1), own);
+      double *dG = dalloc<double>(3 * (size_t)std::max(gs->n_gcp, 1), own);
+      up(drows, rows.data(), sizeof(int) * npp);
+      up(dW3, gs->W3, sizeof(float) * 6 * (size_t)gs->n_w3);
+      up(dG, gs->gcpdata, sizeof(double) * 3 * (size_t)gs->n_gcp);
+      H->L.ao = 1;
+      H->L.n_w3 = gs->n_w3;
+      H->L.pt_gcp = TO.gcp;
+      H->L.pt_w3row = drows;
+      H->L.W3 = dW3;
+      H->L.gcpdata = dG;
+      H->aoterm = dalloc<float>(3 * (size_t)npp, own);
+    }
   }
   up(H->d0_P, P.data(), sizeof(double) * P.size());
   up(H->d0_Kc, Kc.data(), sizeof(double) * Kc.size());
@@ -1044,6 +1113,110 @@ int rpba_handle::adjust() {
   }
   rep.linear_solves = solves;
   if (opt.solver == RPBA_SOLVER_LEARNED) rep.pcg_iterations = learned_iters;
+  return RPBA_OK;
+}
+
+// Adjust in GCP mode (rbacore.cpp:333-616 with robust = false, itbreakflag
+// = true, itmaxnum = 0, gcpflag = true): the per-partition call of the
+// parallel RPBA (rpbacore.cpp:225-229).  The cost with the priors, one damped
+// step (multfact 1e-4) stored unconditionally, and the Sigma0 / Sigma0AO
+// lines.  sig0ao is reset only by the first cost evaluation and by
+// CalcBundleSep, so the post-step value accumulates the prior terms of the
+// assembly pass and the back-substitution pass (both at the start state) and
+// of the trial cost pass, in that order: one sequential float sum over three
+// segments of per-point terms.
+int rpba_handle::adjust_gcp_step() {
+  const double multfact = 1.e-4;
+  const int imagepointnr = L.nobs, np = L.npts;
+  const int nrobsao = 3 * nrgcp;
+  const int nrobs = 2 * imagepointnr + nrobsao;
+  std::vector<int> cnt(nimg + 1);
+  PROF("structure_cam", 2, build_camera_order(L, S, s));
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(cnt.data(), S.ccnt, sizeof(int) * nimg, cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+  for (int i = 0; i < nimg; ++i)
+    if (cnt[i] == 0) {
+      if (nimg > 3) log += "BA-Error: No observations in image " + std::to_string(i) + " (image index)\n";
+      return RPBA_ERR_NO_OBS_IMAGE;
+    }
+  // a float sum of terms of either sign, in array order
+  auto seq_sum_any = [&](const float *v, int n) {
+    float out = 0.f;
+    if (n > 0) {
+      launch_seq_sum(v, n, sums + 1, s);
+      RPBA_CUDA_CHECK(cudaMemcpyAsync(&out, sums + 1, sizeof(float), cudaMemcpyDeviceToHost, s));
+      RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+    }
+    return out;
+  };
+  // PrepareWeights2D / PrepareWeights3D (rbacore.cpp:704-818)
+  PROF("weights", 1, launch_prepare_weights(L, s));
+  float wsum = seq_sum(L.o_wterm, L.nobs);
+  float wsumao = w3diag_sum;
+  const float wsumg = (float)(2 * imagepointnr + nrobsao) / (wsumao + wsum);
+  wsumao = (float)nrobsao / wsumao;
+  wsum = (float)(2 * imagepointnr) / wsum;
+  PROF("encode", 1, launch_encode(L, s));
+  // the additional parameters count once per camera of the scene
+  const int nrunknowns = nrioff + 3 * np + nadd * ncam_total;
+  const int redundancy = nrobs - nrunknowns;
+  if (redundancy < 0) {
+    if (nimg > 3) log += "BA-Error: Low redundancy\n";
+    return RPBA_ERR_LOW_REDUNDANCY;
+  }
+  RPBA_CUDA_CHECK(cudaMemsetAsync(L.x, 0, sizeof(double) * xpmsize, s));
+  structure();
+  // the cost at the start state
+  PROF("decode", 1, launch_decode(L, L.XPM, s));
+  PROF("cost", 1, launch_cost(L, L.XPM, true, s));
+  float sig0 = seq_sum(L.o_cost, L.nobs);
+  launch_gcp_cost(L, L.XPM, aoterm, s);
+  float sig0ao = seq_sum_any(aoterm, np);
+  const float sig0aoin = sig0 * wsumg / (float)redundancy;
+  sig0 = (sig0 + sig0ao) * wsumg / (float)(redundancy + nrobsao - 7);
+  const float sig0in = sig0;
+  // one damped step; its two passes see the priors at the start state
+  if (np > 0) {
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(aoterm + np, aoterm, sizeof(float) * np, cudaMemcpyDeviceToDevice, s));
+  }
+  calc_bundle_sep(multfact, nrunknowns);
+  rep.linear_solves = 1;
+  PROF("decode", 1, launch_decode(L, L.XPMn, s));
+  PROF("cost", 1, launch_cost(L, L.XPMn, true, s));
+  launch_gcp_cost(L, L.XPMn, aoterm + 2 * (size_t)np, s);
+  PROF("seq_sum", 1, launch_exact_sum(L.o_cost, L.nobs, sums, ES, s));
+  struct {
+    float sig0;
+    int err;
+    int iters;
+  } hv;
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(&hv.sig0, sums, sizeof(float), cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(&hv.err, L.err, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(&hv.iters, W.iters, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+  pcg_pending = false;
+  rep.pcg_iterations = opt.solver == RPBA_SOLVER_PCG ? hv.iters : 0;
+  if (hv.err & 2) return RPBA_ERR_DEVICE_TIMEOUT;
+  if (hv.err & 4) return RPBA_ERR_SOLVER;
+  if (hv.err & 1) return RPBA_ERR_NAN_STEP;
+  // the post-step sig0ao: one running float sum over the three passes'
+  // terms (the start state twice, the trial state once)
+  sig0ao = seq_sum_any(aoterm, 3 * np);
+  const float sig0aoiold = hv.sig0 * wsumg / (float)redundancy;
+  const float sig0old = (hv.sig0 + sig0ao) * wsumg / (float)(redundancy + nrobsao - 7);
+  PROF("store", 1, launch_store(L, xpmsize, s));
+  const float s_in = std::sqrt(sig0in * ihw2), s_out = std::sqrt(sig0old * ihw2);
+  log += "Sigma0: " + fmt_g(std::sqrt(sig0aoin * ihw2)) + ' ' + fmt_g(std::sqrt(sig0aoiold * ihw2)) + "  " +
+         std::to_string(redundancy) + ' ' + std::to_string(nrobs) + ' ' + std::to_string(nrunknowns) +
+         "  IT: 0  ITT: 0\n";
+  log += "Sigma0AO: " + fmt_g(std::sqrt(sig0ao * wsumao / (float)(nrobsao - 7))) + "  " + fmt_g(s_in) + ' ' +
+         fmt_g(s_out) + "  " + std::to_string(nrobsao) + " " + fmt_g(wsumao) + '\n';
+  rep.sigma0_in[0] = s_in;
+  rep.sigma0_out[0] = s_out;
+  rep.redundancy[0] = redundancy;
+  rep.nrobs[0] = nrobs;
+  rep.nrunknowns[0] = nrunknowns;
+  rep.passes_done = 1;
   return RPBA_OK;
 }
 
@@ -1680,6 +1853,81 @@ int32_t rpba_calc_plsa(rpba_block *blk, const rpba_options *opt, char *log, size
   }
   if (log && cap) rpba_get_log(H, log, cap);
   rpba_destroy(H);
+  return st;
+}
+
+int32_t rpba_lsa_gcp_step(rpba_block *blk, const rpba_options *opt, const int32_t *gcpinfo, const float *W3,
+                          int32_t n_w3, const double *gcpdata, int32_t n_gcp, int32_t ncam_total,
+                          const double *pmat_d, double *pmat_d_out, uint8_t *point_used, rpba_report *rep,
+                          char *log, size_t cap) {
+  if (!blk || !opt || !gcpinfo || n_w3 < 0 || n_gcp < 0 || (n_w3 > 0 && !W3) || (n_gcp > 0 && !gcpdata) ||
+      blk->n_images < 1 || blk->n_points < 0 || ncam_total < blk->n_images)
+    return RPBA_ERR_ARG;
+  if (opt->exteval || opt->precision != RPBA_PREC_FP64 ||
+      (opt->solver != RPBA_SOLVER_PCG && opt->solver != RPBA_SOLVER_DIRECT))
+    return RPBA_ERR_UNSUPPORTED;
+  if (rep) std::memset(rep, 0, sizeof *rep);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= opt->device) return RPBA_ERR_NO_DEVICE;
+  rpba_handle *H = new rpba_handle();
+  const GcpSetup gs{gcpinfo, W3, n_w3, gcpdata, n_gcp, ncam_total, pmat_d};
+  struct A {
+    rpba_handle *H;
+    const rpba_block *b;
+    const rpba_options *o;
+    const GcpSetup *g;
+  } a{H, blk, opt, &gs};
+  int st = guard([](void *p) {
+    A *a = (A *)p;
+    return create_impl(a->H, a->b, a->o, a->g);
+  }, &a);
+  if (st != RPBA_OK) {
+    delete H;
+    return st;
+  }
+  st = guard([](void *p) {
+    rpba_handle *H = (rpba_handle *)p;
+    RPBA_CUDA_CHECK(cudaSetDevice(H->dev));
+    AsyncScope scope(H->s, H->owned, H->owned_async);
+    H->log.clear();
+    std::memset(&H->rep, 0, sizeof H->rep);
+    H->rep.points_used = H->npts0;
+    H->reset();
+    return H->adjust_gcp_step();
+  }, H);
+  if (st == RPBA_OK || st == RPBA_ERR_NO_OBS_IMAGE || st == RPBA_ERR_LOW_REDUNDANCY || st == RPBA_ERR_NAN_STEP) {
+    int st2 = rpba_get_state(H, blk);
+    if (st2 == RPBA_OK && (pmat_d_out || point_used)) {
+      // OutputLSAP (rbacore.cpp:620-639): the cameras in double precision
+      // and the points PointXXvIn took (the others' lists are cleared)
+      struct B {
+        rpba_handle *H;
+        double *P;
+        uint8_t *used;
+      } bb{H, pmat_d_out, point_used};
+      st2 = guard([](void *p) {
+        B *b = (B *)p;
+        rpba_handle *H = b->H;
+        RPBA_CUDA_CHECK(cudaSetDevice(H->dev));
+        if (b->P)
+          RPBA_CUDA_CHECK(cudaMemcpyAsync(b->P, H->L.Pacc, sizeof(double) * 12 * H->nimg, cudaMemcpyDeviceToHost, H->s));
+        std::vector<int> ids(H->L.npts);
+        if (b->used && H->L.npts)
+          RPBA_CUDA_CHECK(
+              cudaMemcpyAsync(ids.data(), H->L.pt_id, sizeof(int) * H->L.npts, cudaMemcpyDeviceToHost, H->s));
+        RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
+        if (b->used) {
+          std::memset(b->used, 0, (size_t)H->XXnr);
+          for (int q : ids) b->used[q] = 1;
+        }
+        return (int)RPBA_OK;
+      }, &bb);
+    }
+    if (st == RPBA_OK) st = st2;
+  }
+  if (rep) *rep = H->rep;
+  if (log && cap) rpba_get_log(H, log, cap);
+  delete H;
   return st;
 }
 

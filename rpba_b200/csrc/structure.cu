@@ -254,7 +254,8 @@ void build_bsr(DevLSA &L, StructWork &S, cudaStream_t s) {
 
 // ---- PointXXvIn (rbacore.cpp:1918-1974) on the device: the track-ordered
 // observation arrays (point major, observations in track order) of the
-// points with at least two observations and |Z| > 1e-8.
+// points with at least two observations (in GCP mode also those with one
+// and a GCP index above 0) and |Z| > 1e-8.
 namespace {
 
 __global__ void k_track_count(TrackIn T, int *cnt, int *pval, long long *pairs, int *err) {
@@ -279,7 +280,7 @@ __global__ void k_track_count(TrackIn T, int *cnt, int *pval, long long *pairs, 
       if (T.pt_img[jj] == im) atomicOr(err, 2);  // an image twice in one track
     ++c;
   }
-  const bool valid = fabs((double)T.XX[3 * p + 2]) > 1.e-8 && c >= 2;
+  const bool valid = fabs((double)T.XX[3 * p + 2]) > 1.e-8 && (c >= 2 || (T.gcp && T.gcp[p] > 0 && c > 0));
   cnt[p] = valid ? c : 0;
   pval[p] = valid ? 1 : 0;
   pairs[p] = valid ? (long long)c * (c - 1) / 2 : 0;
@@ -292,6 +293,7 @@ __global__ void k_track_scatter(TrackIn T, const int *ooff, const int *pidx, con
   int o = ooff[p];
   O.pt_id[q] = p;
   O.pt_off[q] = o;
+  if (O.gcp) O.gcp[q] = T.gcp[p];
   for (int j = 0; j < 3; ++j) O.X[3 * (size_t)q + j] = (double)T.XX[3 * (size_t)p + j];
   for (int j = T.pt_off[p]; j < T.pt_off[p + 1]; ++j, ++o) {
     const int im = T.pt_img[j], slot = T.pt_slot[j];

@@ -27,7 +27,8 @@ namespace rpba {
 namespace {
 
 struct TriIn {
-  const float *pmat, *K, *dist, *XX, *xg, *wx, *wy, *wxy, *sig0w;
+  const double *pmat;  // cameras in double precision (the reference's PMatricesd)
+  const float *K, *dist, *XX, *xg, *wx, *wy, *wxy, *sig0w;
   const int *img_off, *pt_off, *pt_img, *pt_slot;
   const int *part;  // image -> partition (weight blocks), or null
   int np, robustmode, weight_only, nparts;
@@ -57,7 +58,7 @@ __device__ void tri_corr(const TriIn &I, const TriScratch &S, int s, int e, doub
   for (int t = s; t < e; ++t) {
     const int j = I.pt_img[t];
     const int sl = I.img_off[j] + I.pt_slot[t];
-    const float *P = I.pmat + 12 * j;
+    const double *P = I.pmat + 12 * j;
     double p1 = (double)P[0] * X0 + (double)P[1] * X1 + (double)P[2] * X2 + (double)P[3];
     double p2 = (double)P[4] * X0 + (double)P[5] * X1 + (double)P[6] * X2 + (double)P[7];
     double p3 = (double)P[8] * X0 + (double)P[9] * X1 + (double)P[10] * X2 + (double)P[11];
@@ -150,7 +151,7 @@ __global__ void k_triangulate(TriIn I, TriScratch S, TriOut O) {
     double N[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
     for (int t = s; t < e; ++t) {
       const int j = I.pt_img[t];
-      const float *P = I.pmat + 12 * j;
+      const double *P = I.pmat + 12 * j;
       const double x = S.p1[t], y = S.p2[t], P3 = S.p3[t], P1 = (double)S.p1[t] * S.p3[t],
                    P2 = (double)S.p2[t] * S.p3[t];
       double xp[3], yp[3];
@@ -291,9 +292,13 @@ __global__ void k_triangulate(TriIn I, TriScratch S, TriOut O) {
 
 using namespace rpba;
 
-static int32_t triangulate_impl(const rpba_block *b, const float *sig0w, const rpba_tri_options *opt,
-                                const int32_t *part, int32_t nparts, double *XX_out, uint8_t *keep, float *sig0v,
-                                uint8_t *conv, double *sig0io, int64_t *redundancy, float *w3d) {
+// CalcLSAXMulti over all points of b with the cameras Pd (12 doubles per
+// image; null: b->pmat widened to double); s0_pt / red_pt (optional): every
+// point's contribution to sig0io and to the redundancy.
+int32_t rpba::triangulate_impl(const rpba_block *b, const double *Pd, const float *sig0w,
+                               const rpba_tri_options *opt, const int32_t *part, int32_t nparts, double *XX_out,
+                               uint8_t *keep, float *sig0v, uint8_t *conv, double *sig0io, int64_t *redundancy,
+                               float *w3d, double *s0_pt, int32_t *red_pt) {
   if (!b || !opt || !XX_out || !keep || !sig0v || !conv || !sig0io || !redundancy) return RPBA_ERR_ARG;
   if (opt->robustmode < 0 || opt->robustmode > 2 || (opt->robustmode == 2 && !sig0w)) return RPBA_ERR_ARG;
   int ndev = 0;
@@ -332,7 +337,14 @@ static int32_t triangulate_impl(const rpba_block *b, const float *sig0w, const r
       return d;
     };
     TriIn I;
-    I.pmat = (const float *)up(b->pmat, sizeof(float) * 12 * nc);
+    if (Pd) {
+      I.pmat = (const double *)up(Pd, sizeof(double) * 12 * nc);
+    } else {
+      std::vector<double> P(12 * (size_t)nc);
+      for (size_t i = 0; i < P.size(); ++i) P[i] = (double)b->pmat[i];
+      I.pmat = (const double *)up(P.data(), sizeof(double) * P.size());
+      RPBA_CUDA_CHECK(cudaStreamSynchronize(s));  // P is a local
+    }
     I.K = (const float *)up(b->K, sizeof(float) * 9 * nc);
     I.dist = (const float *)up(b->distpara, sizeof(float) * 2 * nc);
     I.XX = (const float *)up(b->XX, sizeof(float) * 3 * np);
@@ -395,6 +407,8 @@ static int32_t triangulate_impl(const rpba_block *b, const float *sig0w, const r
     }
     *sig0io = a;
     *redundancy = r;
+    if (s0_pt) std::memcpy(s0_pt, s0.data(), sizeof(double) * np);
+    if (red_pt) std::memcpy(red_pt, red.data(), sizeof(int32_t) * np);
   } catch (const CudaError &) {
     return RPBA_ERR_CUDA;
   }
@@ -404,7 +418,8 @@ static int32_t triangulate_impl(const rpba_block *b, const float *sig0w, const r
 extern "C" int32_t rpba_triangulate(const rpba_block *b, const float *sig0w, const rpba_tri_options *opt,
                                     double *XX_out, uint8_t *keep, float *sig0v, uint8_t *conv, double *sig0io,
                                     int64_t *redundancy) {
-  return triangulate_impl(b, sig0w, opt, nullptr, 1, XX_out, keep, sig0v, conv, sig0io, redundancy, nullptr);
+  return triangulate_impl(b, nullptr, sig0w, opt, nullptr, 1, XX_out, keep, sig0v, conv, sig0io, redundancy, nullptr,
+                          nullptr, nullptr);
 }
 
 extern "C" int32_t rpba_triangulate_parts(const rpba_block *b, const float *sig0w, const rpba_tri_options *opt,
@@ -414,5 +429,6 @@ extern "C" int32_t rpba_triangulate_parts(const rpba_block *b, const float *sig0
   if (!b || !part || nparts < 1 || !w3d) return RPBA_ERR_ARG;
   for (int i = 0; i < b->n_images; ++i)
     if (part[i] < 0 || part[i] >= nparts) return RPBA_ERR_ARG;
-  return triangulate_impl(b, sig0w, opt, part, nparts, XX_out, keep, sig0v, conv, sig0io, redundancy, w3d);
+  return triangulate_impl(b, nullptr, sig0w, opt, part, nparts, XX_out, keep, sig0v, conv, sig0io, redundancy, w3d,
+                          nullptr, nullptr);
 }

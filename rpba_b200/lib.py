@@ -39,7 +39,8 @@ EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block
            "rpba_get_state", "rpba_get_log", "rpba_exteval", "rpba_kernel_stats", "rpba_float_sequential_sum",
            "rpba_float_sequential_sum_noalloc", "rpba_train_preconditioner",
            "rpba_set_preconditioner", "rpba_precond_loss_grad", "rpba_record_systems", "rpba_solve_batch",
-           "rpba_triangulate", "rpba_triangulate_parts", "rpba_partition_images", "rpba_destroy")
+           "rpba_triangulate", "rpba_triangulate_parts", "rpba_partition_images", "rpba_lsa_gcp_step",
+           "rpba_calc_plsa_parallel", "rpba_calc_plsa_parallel_hosted", "rpba_destroy")
 
 _lib = None
 
@@ -105,6 +106,16 @@ def load():
     L.rpba_triangulate_parts.restype = C.c_int32
     L.rpba_partition_images.argtypes = [bp, C.c_int32, C.POINTER(C.c_int32)]
     L.rpba_partition_images.restype = C.c_int32
+    L.rpba_lsa_gcp_step.argtypes = [bp, op, C.POINTER(C.c_int32), C.POINTER(C.c_float), C.c_int32,
+                                    C.POINTER(C.c_double), C.c_int32, C.c_int32, C.POINTER(C.c_double),
+                                    C.POINTER(C.c_double), C.POINTER(C.c_uint8), rp, C.c_char_p, C.c_size_t]
+    L.rpba_lsa_gcp_step.restype = C.c_int32
+    L.rpba_calc_plsa_parallel.argtypes = [bp, op, C.c_int32, C.POINTER(C.c_int32), C.c_char_p, C.c_size_t,
+                                          C.POINTER(C.c_double)]
+    L.rpba_calc_plsa_parallel.restype = C.c_int32
+    L.rpba_calc_plsa_parallel_hosted.argtypes = [bp, op, C.c_int32, C.POINTER(C.c_int32), C.c_char_p, C.c_size_t,
+                                                 C.POINTER(C.c_double), C.c_void_p, C.c_void_p]
+    L.rpba_calc_plsa_parallel_hosted.restype = C.c_int32
     L.rpba_triangulate.argtypes = [bp, C.POINTER(C.c_float), C.POINTER(RpbaTriOptionsC), C.POINTER(C.c_double),
                                    C.POINTER(C.c_uint8), C.POINTER(C.c_float), C.POINTER(C.c_uint8),
                                    C.POINTER(C.c_double), C.POINTER(C.c_int64)]
@@ -152,6 +163,55 @@ def CalcPLSA(block: Block, robust: bool = True, addflags=(True, True, True), thr
     if st in (2, 9):
         raise RpbaError(st, "CalcPLSA")
     return st, buf.value.decode(), rep.as_dict()
+
+
+def lsa_gcp_step(block: Block, gcpinfo, W3, gcpdata, ncam_total: int, pmat_d=None, solver: int = SOLVER_PCG,
+                 addflags=(True, True, True), device: int = 0, log_cap: int = 1 << 16):
+    """One GCP-mode LSA step on a copy of ``block`` (rpba_lsa_gcp_step, the
+    parallel RPBA's per-partition call).  gcpinfo: per point its GCP index
+    or -1; W3: (rows, 6) weight blocks in the order of the kept GCP points;
+    gcpdata: (n_gcp, 3).  Returns (status, block, cameras in double
+    precision (n_images, 12), point_used, report, log)."""
+    b = block.copy()
+    cb = b.as_c()
+    o = make_options(robust=False, k2=addflags[0], k4=addflags[1], f=addflags[2], solver=solver,
+                     precision=PREC_FP64, device=device)
+    gi = np.ascontiguousarray(gcpinfo, np.int32)
+    w3 = np.ascontiguousarray(W3, np.float32).reshape(-1)
+    gd = np.ascontiguousarray(gcpdata, np.float64).reshape(-1)
+    pin = None if pmat_d is None else np.ascontiguousarray(pmat_d, np.float64).reshape(-1)
+    pout = np.zeros((b.n_images, 12))
+    used = np.zeros(max(b.n_points, 1), np.uint8)
+    rep = RpbaReportC()
+    buf = C.create_string_buffer(log_cap)
+    dp = lambda a: None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+    st = load().rpba_lsa_gcp_step(C.byref(cb), C.byref(o), gi.ctypes.data_as(C.POINTER(C.c_int32)),
+                                  w3.ctypes.data_as(C.POINTER(C.c_float)), int(w3.size // 6), dp(gd),
+                                  int(gd.size // 3), int(ncam_total), dp(pin), dp(pout),
+                                  used.ctypes.data_as(C.POINTER(C.c_uint8)), C.byref(rep), buf, log_cap)
+    return st, b, pout, used[:b.n_points].astype(bool), rep.as_dict(), buf.value.decode()
+
+
+def calc_plsa_parallel(block: Block, part, nthreads: int, robust: bool = True, addflags=(True, True, True),
+                       solver: int = SOLVER_PCG, device: int = 0, log_cap: int = 1 << 20):
+    """The parallel RPBA (rpba_calc_plsa_parallel) on a copy of ``block``
+    with the camera partition ``part``.  Returns (status, adjusted block,
+    {"sig0opt", "iterations"}, log); the block's tracks are the best
+    iteration's, trimmed to their length."""
+    b = block.copy()
+    cb = b.as_c()
+    o = make_options(robust=robust, k2=addflags[0], k4=addflags[1], f=addflags[2], solver=solver,
+                     precision=PREC_FP64, device=device)
+    pt = np.ascontiguousarray(part, np.int32)
+    stats = np.zeros(2)
+    buf = C.create_string_buffer(log_cap)
+    st = load().rpba_calc_plsa_parallel(C.byref(cb), C.byref(o), int(nthreads),
+                                        pt.ctypes.data_as(C.POINTER(C.c_int32)), buf, log_cap,
+                                        stats.ctypes.data_as(C.POINTER(C.c_double)))
+    n = int(b.pt_obs_off[-1])
+    b.pt_obs_image = b.pt_obs_image[:n].copy()
+    b.pt_obs_slot = b.pt_obs_slot[:n].copy()
+    return st, b, {"sig0opt": float(stats[0]), "iterations": int(stats[1])}, buf.value.decode()
 
 
 def float_sequential_sum(v, device: int = 0) -> np.float32:
