@@ -13,12 +13,12 @@ import numpy as np
 import pytest
 
 
-def _hosted(oracle_mod, blk, part, k):
+def _hosted(oracle_mod, blk, part, k, **opts):
     import rpba_b200 as rb
     L, O = rb.load(), oracle_mod.lib()
     b = blk.copy()
     cb = b.as_c()
-    o = rb.make_options()
+    o = rb.make_options(**opts)
     stats = np.zeros(2)
     cap = 1 << 20
     buf = C.create_string_buffer(cap)
@@ -39,17 +39,22 @@ def loop_scenes():
     return {
         "arc": scenes.to_block(scenes.arc_scene(seed=5, n_cams=50, n_pts=8000)),
         "city": scenes.to_block(scenes.city_scene(seed=8, n_clusters=3, cams_per_cluster=20, n_pts=8000)),
+        "street": scenes.to_block(scenes.street_scene(seed=6, n_cams=80, n_pts=12000)),
     }
 
 
-@pytest.mark.parametrize("name,k", [("arc", 2), ("arc", 4), ("city", 3)])
-def test_library_loop_equals_oracle_loop(oracle_mod, loop_scenes, name, k):
+CASES = [("arc", 2, {}), ("arc", 4, {}), ("city", 3, {}), ("street", 2, {}),
+         ("arc", 3, {"robust": False}), ("city", 2, {"k2": False, "k4": False, "f": False})]
+
+
+@pytest.mark.parametrize("name,k,opts", CASES)
+def test_library_loop_equals_oracle_loop(oracle_mod, loop_scenes, name, k, opts):
     import rpba_b200 as rb
     blk = loop_scenes[name]
     part = rb.partition_images(blk, k)
-    st_o, b_o, s_o, log_o = oracle_mod.calc_plsa_parallel(blk, part, k)
-    st_h, b_h, s_h, log_h = _hosted(oracle_mod, blk, part, k)
-    print(f"{name} k={k}: {s_h['iterations']} iterations, sigma0 {s_h['sig0opt']:.6f}, "
+    st_o, b_o, s_o, log_o = oracle_mod.calc_plsa_parallel(blk, part, k, rb.make_options(**opts))
+    st_h, b_h, s_h, log_h = _hosted(oracle_mod, blk, part, k, **opts)
+    print(f"{name} k={k} {opts}: {s_h['iterations']} iterations, sigma0 {s_h['sig0opt']:.6f}, "
           f"{b_h.n_obs} of {blk.n_obs} observations")
     assert st_o == st_h == 0
     assert s_h == s_o
