@@ -76,3 +76,27 @@ def test_library_loop_rejects_bad_arguments(oracle_mod, loop_scenes):
     st = rb.load().rpba_calc_plsa_parallel(C.byref(cb), C.byref(o), 2, good.ctypes.data_as(C.POINTER(C.c_int32)),
                                            None, 0, None)
     assert st == 8  # RPBA_ERR_UNSUPPORTED: the partition steps are FP64 only
+
+
+def test_gcp_step_rejects_bad_arguments(loop_scenes):
+    """rpba_lsa_gcp_step checks its arguments before touching a device."""
+    import rpba_b200 as rb
+    blk = loop_scenes["arc"]
+    n = blk.n_points
+    gi = np.full(n, -1, np.int32)
+    W3 = np.zeros((0, 6), np.float32)
+    gd = np.zeros((0, 3))
+    st = rb.lsa_gcp_step(blk, gi, W3, gd, blk.n_images - 1)[0]
+    assert st == 1  # ncam_total below the block's image count
+    L = rb.load()
+    b = blk.copy()
+    cb = b.as_c()
+    for o, want in ((rb.make_options(precision=rb.PREC_MIXED), 8), (rb.make_options(solver=rb.SOLVER_LEARNED), 8),
+                    (rb.make_options(exteval=True), 8)):
+        st = L.rpba_lsa_gcp_step(C.byref(cb), C.byref(o), gi.ctypes.data_as(C.POINTER(C.c_int32)), None, 0, None,
+                                 0, blk.n_images, None, None, None, None, None, 0)
+        assert st == want
+    o = rb.make_options()
+    st = L.rpba_lsa_gcp_step(C.byref(cb), C.byref(o), None, None, 0, None, 0, blk.n_images, None, None, None, None,
+                             None, 0)
+    assert st == 1  # no gcpinfo
