@@ -28,7 +28,17 @@ def solved(oracle_mod):
 
 
 def _ints(log):
-    return [re.findall(r"\b\d+\b", l) for l in log.splitlines() if l.startswith(("Sigma0:", "Sigma0AO:"))]
+    """The integer fields of the Sigma0 lines (redundancy, observations,
+    unknowns, IT, ITT) and of the Sigma0AO line (prior observations)."""
+    out = []
+    for l in log.splitlines():
+        m = re.match(r"Sigma0: \S+ \S+\s+(\d+) (\d+) (\d+)\s+IT: (\d+)\s+ITT: (\d+)", l)
+        if m:
+            out.append(m.groups())
+        m = re.match(r"Sigma0AO: \S+\s+\S+ \S+\s+(\d+) ", l)
+        if m:
+            out.append(m.groups())
+    return out
 
 
 @pytest.mark.parametrize("every", [1, 3])
