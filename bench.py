@@ -73,12 +73,17 @@ def parse():
 
 
 def peaks():
+    """HBM copy bandwidth (GB/s) from MEASURED_PEAKS.json (key hbm_gbs, a
+    number or an object holding one), else the pool's earlier measurement."""
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
-    if os.path.exists(path):
+    try:
         with open(path) as fh:
-            d = json.load(fh)
-        return float(d["hbm_gbs"]), "measured"
-    return 6650.0, "fallback"
+            v = json.load(fh)["hbm_gbs"]
+        if isinstance(v, dict):
+            v = next(x for k, x in v.items() if isinstance(x, (int, float)) and k in ("value", "burst", "gbs"))
+        return float(v), "measured"
+    except (OSError, ValueError, KeyError, TypeError, StopIteration):
+        return 6650.0, "fallback"
 
 
 def traffic_ratio():
