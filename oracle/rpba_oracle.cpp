@@ -2486,6 +2486,42 @@ void *oracle_lsa_create(const rpba_block *blk, const rpba_options *o) {
   l->setup_pass_for_tests();
   return l;
 }
+/* The same in GCP mode (every camera free, 3-D priors). */
+void *oracle_lsa_create_gcp(const rpba_block *blk, const rpba_options *o, const int32_t *gcpinfo, const float *W3,
+                            const double *gcpdata, int32_t ncam_total) {
+  static std::string sink;
+  Opts op = make_opts(o);
+  op.robust = false;
+  LSA *l = new LSA(blk, op, &sink, GcpIn{gcpinfo, W3, gcpdata, ncam_total});
+  if (l->bad_setup) {
+    delete l;
+    return nullptr;
+  }
+  l->setup_pass_for_tests();
+  return l;
+}
+int32_t oracle_lsa_n_points(void *h) { return ((LSA *)h)->nrpts; }
+/* PointXXvIn's result: track offsets, images and slots (local order) and,
+ * in GCP mode, every kept point's GCP index. */
+void oracle_lsa_tracks(void *h, int32_t *toff, int32_t *timg, int32_t *tslot, int32_t *gcpi) {
+  LSA *l = (LSA *)h;
+  std::copy(l->toff.begin(), l->toff.end(), toff);
+  std::copy(l->timg.begin(), l->timg.end(), timg);
+  std::copy(l->tslot.begin(), l->tslot.end(), tslot);
+  if (gcpi && l->ao) std::copy(l->gcpi.begin(), l->gcpi.end(), gcpi);
+}
+/* One GCP-mode step on a fresh LSA: the state vector after it (the
+ * stored XPMatrices, nrioff3 entries). */
+int32_t oracle_lsa_gcp_step_xm(const rpba_block *blk, const rpba_options *o, const int32_t *gcpinfo,
+                               const float *W3, const double *gcpdata, int32_t ncam_total, double *xm_after) {
+  std::string os;
+  Opts op = make_opts(o);
+  op.robust = false;
+  LSA l(blk, op, &os, GcpIn{gcpinfo, W3, gcpdata, ncam_total});
+  const int st = l.adjust_gcp_step();
+  std::memcpy(xm_after, l.XPM.data(), sizeof(double) * l.nrioff3);
+  return st;
+}
 void oracle_lsa_destroy(void *h) { delete (LSA *)h; }
 int32_t oracle_lsa_xm_size(void *h) { return ((LSA *)h)->nrioff3; }
 int32_t oracle_lsa_n_track_obs(void *h) { return ((LSA *)h)->toff[((LSA *)h)->nrpts]; }

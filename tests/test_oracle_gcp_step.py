@@ -1,0 +1,145 @@
+"""The oracle's GCP-mode LSA step (the parallel RPBA's per-partition call,
+rbacore.cpp:333-616 with gcpflag) against an independent dense numpy
+restatement of the same damped Gauss-Newton step, built from the oracle's
+residuals and analytic Jacobians (themselves checked against finite
+differences in test_oracle_kat.py):
+
+  per point  V = sum Bp^T W Bp + W3,  g = sum Bp^T W d - W3 (gcp - X)
+             (the prior's residual is gcp - X, its Jacobian -I),
+             V's diagonal times (1 + mu);
+  cameras    S = sum Bc^T W Bc - sum C V^-1 C^T (C = sum Bc^T W Bp, every
+             camera free), b = sum Bc^T W d - sum C V^-1 g, S's diagonal
+             times (1 + mu) plus 1e-2;
+  step       xc = float(S^-1 b), xp = V^-1 (g - C^T xc), XPMnew = XPM - x;
+
+mu = 1e-4, the direct solver.  The step must agree to roundoff."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from rpba_b200 import scenes
+
+
+def _wrap(L):
+    vp = C.c_void_p
+    L.oracle_lsa_create_gcp.restype = vp
+    L.oracle_lsa_create_gcp.argtypes = [vp, vp, vp, vp, vp, C.c_int32]
+    for n in ("oracle_lsa_xm_size", "oracle_lsa_n_track_obs", "oracle_lsa_nrioff", "oracle_lsa_n_points"):
+        getattr(L, n).restype = C.c_int32
+        getattr(L, n).argtypes = [vp]
+    L.oracle_lsa_tracks.argtypes = [vp, vp, vp, vp, vp]
+    L.oracle_lsa_get_xm.argtypes = [vp, vp]
+    L.oracle_lsa_residuals.argtypes = [vp, vp, vp]
+    L.oracle_lsa_jacobian.argtypes = [vp, C.c_int, vp, vp, vp, vp]
+    L.oracle_lsa_destroy.argtypes = [vp]
+    L.oracle_lsa_gcp_step_xm.restype = C.c_int32
+    L.oracle_lsa_gcp_step_xm.argtypes = [vp, vp, vp, vp, vp, C.c_int32, vp]
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _numpy_step(L, h, blk, W3, gcpdata, mu=1e-4):
+    nx = L.oracle_lsa_xm_size(h)
+    nt = L.oracle_lsa_n_track_obs(h)
+    nrioff = L.oracle_lsa_nrioff(h)
+    npt = L.oracle_lsa_n_points(h)
+    toff = np.zeros(npt + 1, np.int32)
+    timg = np.zeros(max(nt, 1), np.int32)
+    tslot = np.zeros(max(nt, 1), np.int32)
+    gcpi = np.full(max(npt, 1), -1, np.int32)
+    L.oracle_lsa_tracks(h, _ptr(toff), _ptr(timg), _ptr(tslot), _ptr(gcpi))
+    xm = np.zeros(nx)
+    L.oracle_lsa_get_xm(h, _ptr(xm))
+    res = np.zeros(2 * nt)
+    L.oracle_lsa_residuals(h, _ptr(xm), _ptr(res))
+    slot = blk.img_obs_off[timg[:nt]] + tslot[:nt]
+    D = np.zeros((nrioff, nrioff))
+    bc = np.zeros(nrioff)
+    S = D.copy()
+    Vs, gs, Cs = [], [], []
+    row = 0
+    for i in range(npt):
+        V = np.zeros((3, 3))
+        g = np.zeros(3)
+        Ci = np.zeros((nrioff, 3))
+        for o in range(toff[i], toff[i + 1]):
+            Bc = np.zeros(18)
+            Bp = np.zeros(6)
+            nc = C.c_int()
+            co = C.c_int()
+            L.oracle_lsa_jacobian(h, o, _ptr(Bc), C.byref(nc), C.byref(co), _ptr(Bp))
+            Bc = Bc.reshape(2, 9)[:, :nc.value]
+            Bp = Bp.reshape(2, 3)
+            s = slot[o]
+            W = np.array([[blk.wx[s], blk.wxy[s]], [blk.wxy[s], blk.wy[s]]], np.float64)
+            d = res[2 * o:2 * o + 2]
+            cols = slice(co.value, co.value + nc.value)
+            D[cols, cols] += Bc.T @ W @ Bc
+            bc[cols] += Bc.T @ W @ d
+            Ci[cols] += Bc.T @ W @ Bp
+            V += Bp.T @ W @ Bp
+            g += Bp.T @ W @ d
+        if gcpi[i] > -1:
+            w = W3[row].astype(np.float64)
+            row += 1
+            Wm = np.array([[w[0], w[3], w[4]], [w[3], w[1], w[5]], [w[4], w[5], w[2]]])
+            dpr = gcpdata[gcpi[i]] - xm[nrioff + 3 * i:nrioff + 3 * i + 3]
+            V += Wm
+            g += -Wm @ dpr
+        V[np.diag_indices(3)] *= 1 + mu
+        Vi = np.linalg.inv(V)
+        D -= Ci @ Vi @ Ci.T
+        bc -= Ci @ Vi @ g
+        Vs.append(Vi)
+        gs.append(g)
+        Cs.append(Ci)
+    D[np.diag_indices(nrioff)] = D[np.diag_indices(nrioff)] * (1 + mu) + 1e-2
+    xc = np.linalg.solve(D, bc).astype(np.float32).astype(np.float64)
+    x = np.zeros(nx)
+    x[:nrioff] = xc
+    for i in range(npt):
+        x[nrioff + 3 * i:nrioff + 3 * i + 3] = Vs[i] @ (gs[i] - Cs[i].T @ xc)
+    return xm, x
+
+
+@pytest.mark.parametrize("every,offdiag", [(1, 0.0), (2, 0.3), (5, 0.3)])
+def test_gcp_step_matches_dense_restatement(oracle_mod, every, offdiag):
+    import rpba_b200 as rb
+    L = _wrap(oracle_mod.lib())
+    blk0 = scenes.to_block(scenes.arc_scene(seed=31, n_cams=6, n_pts=120, outlier_frac=0.0))
+    st, solved, _, _ = oracle_mod.calc_plsa(blk0, rb.make_options(robust=False))
+    assert st == 0
+    blk = solved.copy()
+    rng = np.random.default_rng(7)
+    P = blk.pmat.reshape(-1, 3, 4)
+    P[:, :, 3] += rng.normal(0, 0.02, (blk.n_images, 3)).astype(np.float32)
+    n = blk.n_points
+    gcpinfo = np.full(n, -1, np.int32)
+    sel = np.arange(0, n, every)
+    gcpinfo[sel] = np.arange(len(sel), dtype=np.int32)[::-1].copy()  # GCP indices in another order
+    W3 = np.zeros((len(sel), 6), np.float32)
+    W3[:, :3] = rng.uniform(50, 200, (len(sel), 3))
+    W3[:, 3:] = offdiag * rng.uniform(-1, 1, (len(sel), 3)) * 50
+    gcpdata = np.zeros((len(sel), 3))
+    gcpdata[gcpinfo[sel]] = solved.XX[sel] + rng.normal(0, 0.01, (len(sel), 3))
+    o = rb.make_options(robust=False, solver=rb.SOLVER_DIRECT)
+    cb = blk.as_c()
+    h = L.oracle_lsa_create_gcp(C.addressof(cb), C.addressof(o), _ptr(gcpinfo), _ptr(W3), _ptr(gcpdata),
+                                blk.n_images)
+    assert h
+    try:
+        xm, x = _numpy_step(L, h, blk, W3, gcpdata)
+    finally:
+        L.oracle_lsa_destroy(h)
+    after = np.zeros_like(xm)
+    st = L.oracle_lsa_gcp_step_xm(C.addressof(cb), C.addressof(o), _ptr(gcpinfo), _ptr(W3), _ptr(gcpdata),
+                                  blk.n_images, _ptr(after))
+    assert st == 0
+    x_or = xm - after
+    err = np.abs(x_or - x).max() / np.abs(x).max()
+    print(f"every {every}, off-diagonal {offdiag}: step size {np.abs(x).max():.3e}, relative difference {err:.2e}")
+    assert err < 1e-6
