@@ -2510,6 +2510,16 @@ void oracle_lsa_tracks(void *h, int32_t *toff, int32_t *timg, int32_t *tslot, in
   std::copy(l->tslot.begin(), l->tslot.end(), tslot);
   if (gcpi && l->ao) std::copy(l->gcpi.begin(), l->gcpi.end(), gcpi);
 }
+/* One damped solve (CalcBundleSep with multfact) on a test handle: the
+ * trial state vector XPMatricesnew = XPMatrices - x (nrioff3 entries). */
+int32_t oracle_lsa_step_xm(void *h, double multfact, double *xm_new) {
+  LSA *l = (LSA *)h;
+  l->iniflag = true;
+  l->x.assign(l->nrioff3 + l->nadd * l->nimg, 0.);
+  if (l->calc_bundle_sep(multfact)) return l->status != RPBA_OK ? l->status : RPBA_ERR_SOLVER;
+  for (int i = 0; i < l->nrioff3; ++i) xm_new[i] = l->XPM[i] - l->x[i];
+  return RPBA_OK;
+}
 /* One GCP-mode step on a fresh LSA: the state vector after it (the
  * stored XPMatrices, nrioff3 entries). */
 int32_t oracle_lsa_gcp_step_xm(const rpba_block *blk, const rpba_options *o, const int32_t *gcpinfo,

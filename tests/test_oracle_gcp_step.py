@@ -1,5 +1,6 @@
-"""The oracle's GCP-mode LSA step (the parallel RPBA's per-partition call,
-rbacore.cpp:333-616 with gcpflag) against an independent dense numpy
+"""The oracle's damped LSA step -- the GCP mode of the parallel RPBA's
+per-partition call (rbacore.cpp:333-616 with gcpflag) and the global LSA's
+CalcBundleSep (rbacore.cpp:1094-1195) -- against an independent dense numpy
 restatement of the same damped Gauss-Newton step, built from the oracle's
 residuals and analytic Jacobians (themselves checked against finite
 differences in test_oracle_kat.py):
@@ -12,7 +13,9 @@ differences in test_oracle_kat.py):
              times (1 + mu) plus 1e-2;
   step       xc = float(S^-1 b), xp = V^-1 (g - C^T xc), XPMnew = XPM - x;
 
-mu = 1e-4, the direct solver.  The step must agree to roundoff."""
+mu = 1e-4 in GCP mode (1e-3 for the global LSA's first pass, without
+priors and with its camera layout), the direct solver.  The step must agree
+to roundoff."""
 import ctypes as C
 
 import numpy as np
@@ -59,7 +62,6 @@ def _numpy_step(L, h, blk, W3, gcpdata, mu=1e-4):
     slot = blk.img_obs_off[timg[:nt]] + tslot[:nt]
     D = np.zeros((nrioff, nrioff))
     bc = np.zeros(nrioff)
-    S = D.copy()
     Vs, gs, Cs = [], [], []
     row = 0
     for i in range(npt):
@@ -142,4 +144,32 @@ def test_gcp_step_matches_dense_restatement(oracle_mod, every, offdiag):
     x_or = xm - after
     err = np.abs(x_or - x).max() / np.abs(x).max()
     print(f"every {every}, off-diagonal {offdiag}: step size {np.abs(x).max():.3e}, relative difference {err:.2e}")
+    assert err < 1e-6
+
+
+@pytest.mark.parametrize("addflags", [(True, True, True), (False, False, False)])
+def test_global_step_matches_dense_restatement(oracle_mod, addflags):
+    """The same restatement for the global LSA's damped solve (camera 0 with
+    the additional parameters only, the scale camera with one coordinate of
+    its projection centre fixed, no priors), mu = 1e-3 as in the first pass."""
+    import rpba_b200 as rb
+    L = _wrap(oracle_mod.lib())
+    L.oracle_lsa_create.restype = C.c_void_p
+    L.oracle_lsa_create.argtypes = [C.c_void_p, C.c_void_p]
+    L.oracle_lsa_step_xm.restype = C.c_int32
+    L.oracle_lsa_step_xm.argtypes = [C.c_void_p, C.c_double, C.c_void_p]
+    blk = scenes.to_block(scenes.arc_scene(seed=12, n_cams=7, n_pts=150, outlier_frac=0.0))
+    o = rb.make_options(robust=False, solver=rb.SOLVER_DIRECT, k2=addflags[0], k4=addflags[1], f=addflags[2])
+    cb = blk.as_c()
+    h = L.oracle_lsa_create(C.addressof(cb), C.addressof(o))
+    assert h
+    try:
+        xm, x = _numpy_step(L, h, blk, np.zeros((0, 6), np.float32), np.zeros((0, 3)), mu=1e-3)
+        new = np.zeros_like(xm)
+        assert L.oracle_lsa_step_xm(h, 1e-3, _ptr(new)) == 0
+    finally:
+        L.oracle_lsa_destroy(h)
+    x_or = xm - new
+    err = np.abs(x_or - x).max() / np.abs(x).max()
+    print(f"addflags {addflags}: step size {np.abs(x).max():.3e}, relative difference {err:.2e}")
     assert err < 1e-6
