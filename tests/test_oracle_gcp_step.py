@@ -14,8 +14,9 @@ differences in test_oracle_kat.py):
   step       xc = float(S^-1 b), xp = V^-1 (g - C^T xc), XPMnew = XPM - x;
 
 mu = 1e-4 in GCP mode (1e-3 for the global LSA's first pass, without
-priors and with its camera layout), the direct solver.  The step must agree
-to roundoff."""
+priors and with its camera layout), the direct solver; and the global step
+with the reference's PCG against SparsePCG restated on the dense system.
+The step must agree to roundoff."""
 import ctypes as C
 
 import numpy as np
@@ -45,7 +46,9 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p)
 
 
-def _numpy_step(L, h, blk, W3, gcpdata, mu=1e-4):
+def _system(L, h, blk, W3, gcpdata, mu):
+    """The damped, Schur-reduced system (S, b), the point blocks and every
+    camera's column range, at the handle's state vector xm."""
     nx = L.oracle_lsa_xm_size(h)
     nt = L.oracle_lsa_n_track_obs(h)
     nrioff = L.oracle_lsa_nrioff(h)
@@ -63,6 +66,7 @@ def _numpy_step(L, h, blk, W3, gcpdata, mu=1e-4):
     D = np.zeros((nrioff, nrioff))
     bc = np.zeros(nrioff)
     Vs, gs, Cs = [], [], []
+    cams = {}
     row = 0
     for i in range(npt):
         V = np.zeros((3, 3))
@@ -80,6 +84,8 @@ def _numpy_step(L, h, blk, W3, gcpdata, mu=1e-4):
             W = np.array([[blk.wx[s], blk.wxy[s]], [blk.wxy[s], blk.wy[s]]], np.float64)
             d = res[2 * o:2 * o + 2]
             cols = slice(co.value, co.value + nc.value)
+            if nc.value:
+                cams[timg[o]] = (co.value, nc.value)
             D[cols, cols] += Bc.T @ W @ Bc
             bc[cols] += Bc.T @ W @ d
             Ci[cols] += Bc.T @ W @ Bp
@@ -100,12 +106,66 @@ def _numpy_step(L, h, blk, W3, gcpdata, mu=1e-4):
         gs.append(g)
         Cs.append(Ci)
     D[np.diag_indices(nrioff)] = D[np.diag_indices(nrioff)] * (1 + mu) + 1e-2
-    xc = np.linalg.solve(D, bc).astype(np.float32).astype(np.float64)
-    x = np.zeros(nx)
+    return xm, D, bc, (Vs, gs, Cs), [cams[k] for k in sorted(cams)]
+
+
+def _backsub(xm, nrioff, xc, pts):
+    """Camera steps rounded to float as the reference stores them, then the
+    point steps."""
+    Vs, gs, Cs = pts
+    xc = xc.astype(np.float32).astype(np.float64)
+    x = np.zeros_like(xm)
     x[:nrioff] = xc
-    for i in range(npt):
+    for i in range(len(Vs)):
         x[nrioff + 3 * i:nrioff + 3 * i + 3] = Vs[i] @ (gs[i] - Cs[i].T @ xc)
-    return xm, x
+    return x
+
+
+def _numpy_step(L, h, blk, W3, gcpdata, mu=1e-4):
+    xm, S, b, pts, _ = _system(L, h, blk, W3, gcpdata, mu)
+    return xm, _backsub(xm, S.shape[0], np.linalg.solve(S, b), pts)
+
+
+def _sparse_pcg(S, b, blocks):
+    """SparsePCG (rbacore.cpp:1807-1914) on the dense S: block-Jacobi with
+    the inverse diagonal blocks, x0 = 0, alpha = 0 when |r.h| is below 1e-20
+    or above 1e20, the best iterate by sum (alpha A d)^2, stop once that sum
+    drops below 1e-5 of the first iteration's, beta = 0 when |r1.(h1 - h)|
+    is below 1e-10 and clamped at 0, at most max(unknowns, 1000) iterations."""
+    n = S.shape[0]
+    Cm = np.zeros_like(S)
+    for c0, nc in blocks:
+        sl = slice(c0, c0 + nc)
+        Cm[sl, sl] = np.linalg.inv(S[sl, sl])
+    x = np.zeros(n)
+    r = b.copy()
+    h = Cm @ r
+    d = h.copy()
+    xold = x.copy()
+    meandrold = meandr0 = 1e50
+    cap = max(sum(nc for _, nc in blocks), 1000)
+    for k in range(cap):
+        Ad = S @ d
+        rh = r @ h
+        alpha = 0.0 if (abs(rh) < 1e-20 or abs(rh) > 1e20) else rh / (d @ Ad)
+        x = x + alpha * d
+        dr = alpha * Ad
+        r1 = r - dr
+        meandr = dr @ dr
+        h1 = Cm @ r1
+        if k == 0:
+            meandr0 = meandr
+        if meandr < meandrold:
+            xold = x.copy()
+            meandrold = meandr
+        if meandr * 1e5 < meandr0:
+            break
+        r1h = r1 @ (h1 - h)
+        beta = 0.0 if abs(r1h) < 1e-10 else r1h / (r @ h)
+        beta = max(beta, 0.0)
+        d = h1 + beta * d
+        r, h = r1, h1
+    return xold, k + 1
 
 
 @pytest.mark.parametrize("every,offdiag", [(1, 0.0), (2, 0.3), (5, 0.3)])
@@ -172,4 +232,33 @@ def test_global_step_matches_dense_restatement(oracle_mod, addflags):
     x_or = xm - new
     err = np.abs(x_or - x).max() / np.abs(x).max()
     print(f"addflags {addflags}: step size {np.abs(x).max():.3e}, relative difference {err:.2e}")
+    assert err < 1e-6
+
+
+@pytest.mark.parametrize("seed", [12, 13])
+def test_pcg_step_matches_sparse_pcg_restatement(oracle_mod, seed):
+    """The global LSA's step with the reference's PCG (the drop-in's solver)
+    against SparsePCG restated on the dense reduced system."""
+    import rpba_b200 as rb
+    L = _wrap(oracle_mod.lib())
+    L.oracle_lsa_create.restype = C.c_void_p
+    L.oracle_lsa_create.argtypes = [C.c_void_p, C.c_void_p]
+    L.oracle_lsa_step_xm.restype = C.c_int32
+    L.oracle_lsa_step_xm.argtypes = [C.c_void_p, C.c_double, C.c_void_p]
+    blk = scenes.to_block(scenes.arc_scene(seed=seed, n_cams=9, n_pts=200, outlier_frac=0.0))
+    o = rb.make_options(robust=False, solver=rb.SOLVER_PCG)
+    cb = blk.as_c()
+    h = L.oracle_lsa_create(C.addressof(cb), C.addressof(o))
+    assert h
+    try:
+        xm, S, b, pts, blocks = _system(L, h, blk, np.zeros((0, 6), np.float32), np.zeros((0, 3)), 1e-3)
+        xc, iters = _sparse_pcg(S, b, blocks)
+        x = _backsub(xm, S.shape[0], xc, pts)
+        new = np.zeros_like(xm)
+        assert L.oracle_lsa_step_xm(h, 1e-3, _ptr(new)) == 0
+    finally:
+        L.oracle_lsa_destroy(h)
+    x_or = xm - new
+    err = np.abs(x_or - x).max() / np.abs(x).max()
+    print(f"seed {seed}: {iters} PCG iterations, step size {np.abs(x).max():.3e}, relative difference {err:.2e}")
     assert err < 1e-6
