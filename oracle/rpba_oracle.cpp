@@ -2510,6 +2510,22 @@ void oracle_lsa_tracks(void *h, int32_t *toff, int32_t *timg, int32_t *tslot, in
   std::copy(l->tslot.begin(), l->tslot.end(), tslot);
   if (gcpi && l->ao) std::copy(l->gcpi.begin(), l->gcpi.end(), gcpi);
 }
+/* Reweight2D on a test handle (robust options): the cost pass at the state
+ * vector gives sig0rmv (track order), then the reweighting with iflag.
+ * Outputs: sig0rmv, the per-image thresholds sig00v, the weights W (3 per
+ * observation), the flags and the float weight sum. */
+void oracle_lsa_reweight(void *h, int32_t iflag, float *sig0rmv, float *sig00v, float *W, uint8_t *flags,
+                         float *wsum) {
+  LSA *l = (LSA *)h;
+  l->calc_corrections(false, 1., l->XPM, true, false);
+  l->reweight(iflag);
+  const int n = l->toff[l->nrpts];
+  std::copy(l->sig0rmv.begin(), l->sig0rmv.begin() + n, sig0rmv);
+  std::copy(l->sig00v.begin(), l->sig00v.end(), sig00v);
+  std::copy(l->W.begin(), l->W.begin() + 3 * n, W);
+  for (int o = 0; o < n; ++o) flags[o] = l->isflag[o] ? 1 : 0;
+  *wsum = l->wsum;
+}
 /* One damped solve (CalcBundleSep with multfact) on a test handle: the
  * trial state vector XPMatricesnew = XPMatrices - x (nrioff3 entries). */
 int32_t oracle_lsa_step_xm(void *h, double multfact, double *xm_new) {

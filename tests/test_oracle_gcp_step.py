@@ -262,3 +262,67 @@ def test_pcg_step_matches_sparse_pcg_restatement(oracle_mod, seed):
     err = np.abs(x_or - x).max() / np.abs(x).max()
     print(f"seed {seed}: {iters} PCG iterations, step size {np.abs(x).max():.3e}, relative difference {err:.2e}")
     assert err < 1e-6
+
+
+@pytest.mark.parametrize("iflag", [2, 1])
+def test_reweight_matches_restatement(oracle_mod, iflag):
+    """Reweight2D (rbacore.cpp:820-887) restated in float32 from the cost
+    statistics sig0rmv: per image the median of sig0rmv (2t / (2t - 3))^2,
+    sig00 = 1 / (median 2.1981) (times 0.001 while iflag > 1); an
+    observation with sig0rmv sig00 > kf = 9 gets 1e-4 of its weight
+    (floor 1e-8); the float weight sum in track order.  Bit for bit."""
+    import rpba_b200 as rb
+    L = _wrap(oracle_mod.lib())
+    L.oracle_lsa_create.restype = C.c_void_p
+    L.oracle_lsa_create.argtypes = [C.c_void_p, C.c_void_p]
+    L.oracle_lsa_reweight.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 5
+    blk = scenes.to_block(scenes.arc_scene(seed=5, n_cams=20, n_pts=2000))
+    o = rb.make_options(robust=True)
+    cb = blk.as_c()
+    h = L.oracle_lsa_create(C.addressof(cb), C.addressof(o))
+    assert h
+    try:
+        nt, npt = L.oracle_lsa_n_track_obs(h), L.oracle_lsa_n_points(h)
+        toff = np.zeros(npt + 1, np.int32)
+        timg = np.zeros(nt, np.int32)
+        tslot = np.zeros(nt, np.int32)
+        L.oracle_lsa_tracks(h, _ptr(toff), _ptr(timg), _ptr(tslot), None)
+        s0 = np.zeros(nt, np.float32)
+        s00 = np.zeros(blk.n_images, np.float32)
+        W = np.zeros(3 * nt, np.float32)
+        fl = np.zeros(nt, np.uint8)
+        ws = np.zeros(1, np.float32)
+        L.oracle_lsa_reweight(h, iflag, _ptr(s0), _ptr(s00), _ptr(W), _ptr(fl), _ptr(ws))
+    finally:
+        L.oracle_lsa_destroy(h)
+    f32 = np.float32
+    lists = [[] for _ in range(blk.n_images)]
+    for p in range(npt):
+        pxs = max(2 * (toff[p + 1] - toff[p]), 4)
+        rf = f32(pxs) / f32(pxs - 3)
+        red = rf * rf
+        for t in range(toff[p], toff[p + 1]):
+            lists[timg[t]].append(s0[t] * red)
+    sig00 = np.zeros(blk.n_images, np.float32)
+    for i in range(blk.n_images):
+        v = sorted(lists[i])
+        sig00[i] = f32(1) / (v[len(v) // 2] * f32(2.1981))
+        if iflag > 1:
+            sig00[i] *= f32(0.001)
+    assert np.array_equal(sig00, s00)
+    slot = blk.img_obs_off[timg] + tslot
+    wold = np.stack([blk.wx[slot], blk.wy[slot], blk.wxy[slot]], 1).astype(np.float32)
+    ww = s0 * sig00[timg]
+    flags = ww > f32(9)
+    Wn = np.where(flags[:, None], f32(1e-4), f32(1)) * wold
+    low = Wn[:, 0] + Wn[:, 1] < f32(2e-8)
+    Wn[low] = np.array([1e-8, 1e-8, 0], np.float32)
+    wsum = f32(0)
+    for a, b in zip(Wn[:, 0], Wn[:, 1]):
+        wsum = f32(wsum + f32(a + b))
+    print(f"iflag {iflag}: {int(flags.sum())} of {nt} observations flagged")
+    assert np.array_equal(flags, fl.astype(bool))
+    assert np.array_equal(Wn.reshape(-1), W)
+    assert wsum == ws[0]
+    # the first robust iteration (0.001 sig00) flags nothing here; the next one does
+    assert (0 < flags.sum() < nt) if iflag == 1 else flags.sum() == 0
