@@ -2526,6 +2526,23 @@ void oracle_lsa_reweight(void *h, int32_t iflag, float *sig0rmv, float *sig00v, 
   for (int o = 0; o < n; ++o) flags[o] = l->isflag[o] ? 1 : 0;
   *wsum = l->wsum;
 }
+/* RobustDelete on a test handle, with the flags of a Reweight2D(iflag)
+ * taken as the stored state's (ISflagnew); the handle's tracks, points and
+ * weights are replaced (read them with oracle_lsa_tracks and
+ * oracle_lsa_points). */
+void oracle_lsa_robust_delete(void *h, int32_t iflag) {
+  LSA *l = (LSA *)h;
+  l->calc_corrections(false, 1., l->XPM, true, false);
+  l->reweight(iflag);
+  l->isflagnew = l->isflag;
+  l->robust_delete();
+}
+/* The kept points: their indices in the caller's block and coordinates. */
+void oracle_lsa_points(void *h, int32_t *nrpv, double *XX) {
+  LSA *l = (LSA *)h;
+  std::copy(l->nrpv.begin(), l->nrpv.end(), nrpv);
+  std::copy(l->XX.begin(), l->XX.end(), XX);
+}
 /* One damped solve (CalcBundleSep with multfact) on a test handle: the
  * trial state vector XPMatricesnew = XPMatrices - x (nrioff3 entries). */
 int32_t oracle_lsa_step_xm(void *h, double multfact, double *xm_new) {

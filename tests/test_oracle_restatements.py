@@ -1,4 +1,6 @@
-"""The oracle's damped LSA step -- the GCP mode of the parallel RPBA's
+"""Independent restatements that pin the oracle's pieces: its robust
+reweighting and deletion (Reweight2D, RobustDelete, bit for bit in float32)
+and its damped LSA step -- the GCP mode of the parallel RPBA's
 per-partition call (rbacore.cpp:333-616 with gcpflag) and the global LSA's
 CalcBundleSep (rbacore.cpp:1094-1195) -- against an independent dense numpy
 restatement of the same damped Gauss-Newton step, built from the oracle's
@@ -326,3 +328,73 @@ def test_reweight_matches_restatement(oracle_mod, iflag):
     assert wsum == ws[0]
     # the first robust iteration (0.001 sig00) flags nothing here; the next one does
     assert (0 < flags.sum() < nt) if iflag == 1 else flags.sum() == 0
+
+
+def test_robust_delete_matches_restatement(oracle_mod):
+    """RobustDelete (rbacore.cpp:920-995) restated: the flagged observations
+    of a point are erased, or the whole point when fewer than minimagenrdel
+    (3 with more than two images) would remain; the kept points keep their
+    order and coordinates."""
+    import rpba_b200 as rb
+    L = _wrap(oracle_mod.lib())
+    L.oracle_lsa_create.restype = C.c_void_p
+    L.oracle_lsa_create.argtypes = [C.c_void_p, C.c_void_p]
+    L.oracle_lsa_reweight.argtypes = [C.c_void_p, C.c_int32] + [C.c_void_p] * 5
+    L.oracle_lsa_robust_delete.argtypes = [C.c_void_p, C.c_int32]
+    L.oracle_lsa_points.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    blk = scenes.to_block(scenes.arc_scene(seed=5, n_cams=20, n_pts=2000, outlier_frac=0.08))
+    o = rb.make_options(robust=True)
+    cb = blk.as_c()
+
+    def tracks(h):
+        nt, npt = L.oracle_lsa_n_track_obs(h), L.oracle_lsa_n_points(h)
+        toff = np.zeros(npt + 1, np.int32)
+        timg = np.zeros(max(nt, 1), np.int32)
+        tslot = np.zeros(max(nt, 1), np.int32)
+        L.oracle_lsa_tracks(h, _ptr(toff), _ptr(timg), _ptr(tslot), None)
+        nrpv = np.zeros(max(npt, 1), np.int32)
+        X = np.zeros(3 * max(npt, 1))
+        L.oracle_lsa_points(h, _ptr(nrpv), _ptr(X))
+        return toff, timg[:nt], tslot[:nt], nrpv[:npt], X[:3 * npt].reshape(-1, 3)
+
+    h = L.oracle_lsa_create(C.addressof(cb), C.addressof(o))
+    assert h
+    try:
+        toff, timg, tslot, nrpv, X = tracks(h)
+        nt = len(timg)
+        s0 = np.zeros(nt, np.float32)
+        s00 = np.zeros(blk.n_images, np.float32)
+        W = np.zeros(3 * nt, np.float32)
+        fl = np.zeros(nt, np.uint8)
+        ws = np.zeros(1, np.float32)
+        L.oracle_lsa_reweight(h, 1, _ptr(s0), _ptr(s00), _ptr(W), _ptr(fl), _ptr(ws))
+    finally:
+        L.oracle_lsa_destroy(h)
+    h = L.oracle_lsa_create(C.addressof(cb), C.addressof(o))
+    try:
+        L.oracle_lsa_robust_delete(h, 1)
+        got = tracks(h)
+    finally:
+        L.oracle_lsa_destroy(h)
+    minimagenrdel = 3 if blk.n_images > 2 else 2
+    off, img, slot, ids, XX = [0], [], [], [], []
+    erased_pts = 0
+    for p in range(len(nrpv)):
+        tr = range(toff[p], toff[p + 1])
+        erase = [t for t in tr if fl[t]]
+        if erase and len(tr) - len(erase) < minimagenrdel:
+            erased_pts += 1
+            continue
+        keep = [t for t in tr if not fl[t]]
+        img += [timg[t] for t in keep]
+        slot += [tslot[t] for t in keep]
+        off.append(len(img))
+        ids.append(nrpv[p])
+        XX.append(X[p])
+    print(f"{int(fl.sum())} observations flagged, {erased_pts} points erased, {len(ids)} kept")
+    assert fl.sum() > 0 and erased_pts > 0
+    assert np.array_equal(got[0], np.array(off, np.int32))
+    assert np.array_equal(got[1], np.array(img, np.int32))
+    assert np.array_equal(got[2], np.array(slot, np.int32))
+    assert np.array_equal(got[3], np.array(ids, np.int32))
+    assert np.array_equal(got[4], np.array(XX).reshape(-1, 3))
