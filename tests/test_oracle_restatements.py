@@ -1,6 +1,6 @@
 """Independent restatements that pin the oracle's pieces: its robust
-reweighting and deletion (Reweight2D, RobustDelete, bit for bit in float32)
-and its damped LSA step -- the GCP mode of the parallel RPBA's
+reweighting and deletion (Reweight2D, RobustDelete, bit for bit in float32),
+Exteval (bit for bit) and its damped LSA step -- the GCP mode of the parallel RPBA's
 per-partition call (rbacore.cpp:333-616 with gcpflag) and the global LSA's
 CalcBundleSep (rbacore.cpp:1094-1195) -- against an independent dense numpy
 restatement of the same damped Gauss-Newton step, built from the oracle's
@@ -398,3 +398,64 @@ def test_robust_delete_matches_restatement(oracle_mod):
     assert np.array_equal(got[2], np.array(slot, np.int32))
     assert np.array_equal(got[3], np.array(ids, np.int32))
     assert np.array_equal(got[4], np.array(XX).reshape(-1, 3))
+
+
+def test_exteval_matches_restatement(oracle_mod):
+    """EvalLSA with CalcCorrPointMulti (rpbacore.cpp:778-837, 882-941) and
+    RadialReconstructionImage (rpba.h:850-857) restated operation by
+    operation: per observation dx, dy in double from the float cameras and
+    points; per point the float sums; the printed sqrtf(sig0g ihw2).  Bit
+    for bit."""
+    import rpba_b200 as rb
+    blk = scenes.to_block(scenes.arc_scene(seed=9, n_cams=15, n_pts=1500))
+    res_o, rep_o = oracle_mod.exteval(blk, rb.make_options())
+    f32 = np.float32
+    P = blk.pmat.astype(np.float64).reshape(-1, 3, 4)
+    res = np.zeros((blk.n_obs, 2))
+    sig0g = f32(0)
+    redundancy = nrobs = 0
+    for p in range(blk.n_points):
+        s, e = blk.pt_obs_off[p], blk.pt_obs_off[p + 1]
+        n = e - s
+        if n <= 1:
+            continue
+        X0, X1, X2 = (float(v) for v in blk.XX[p])
+        slots = blk.img_obs_off[blk.pt_obs_image[s:e]] + blk.pt_obs_slot[s:e]
+        wsum = f32(0)
+        for sl in slots:
+            wsum = f32(wsum + f32(blk.wx[sl] + blk.wy[sl]))
+        wsum = f32(wsum / f32(2 * n))
+        sig0 = f32(0)
+        for t in range(s, e):
+            j = blk.pt_obs_image[t]
+            sl = slots[t - s]
+            M = P[j]
+            p1 = ((M[0, 0] * X0 + M[0, 1] * X1) + M[0, 2] * X2) + M[0, 3]
+            p2 = ((M[1, 0] * X0 + M[1, 1] * X1) + M[1, 2] * X2) + M[1, 3]
+            p3 = ((M[2, 0] * X0 + M[2, 1] * X1) + M[2, 2] * X2) + M[2, 3]
+            p3 = (1e3 if p3 > 0 else -1e3) if abs(p3) < 1e-3 else 1.0 / p3
+            p1 *= p3
+            p2 *= p3
+            dist = p1 * p1 + p2 * p2
+            d0, d1 = float(blk.distpara[j, 0]), float(blk.distpara[j, 1])
+            z = 1.0 + (d0 * dist + d1 * dist * dist)
+            p1 *= z
+            p2 *= z
+            k = float(blk.K[j, 0])
+            p1 *= k
+            p2 *= k
+            dx = float(blk.xg[sl, 0]) - p1
+            dy = float(blk.xg[sl, 1]) - p2
+            res[t] = (dx, dy)
+            wx, wy, wxy = float(blk.wx[sl]), float(blk.wy[sl]), float(blk.wxy[sl])
+            sig0 = f32(sig0 + f32((dx * dx * wx + dy * dy * wy) + 2 * dx * dy * wxy))
+        sig0g = f32(sig0g + f32(sig0 / wsum))
+        redundancy += 2 * n - 3
+        nrobs += 2 * n
+    r = redundancy - (blk.n_images - 2) * 6 - 5 - blk.n_images * 3
+    sig0g = f32(sig0g * f32(f32(1) / f32(r)))
+    v = np.sqrt(f32(sig0g * f32(1)), dtype=np.float32)
+    print(f"Exteval sigma0 {v} ({rep_o['exteval_sigma0']}), {nrobs} observations, redundancy {r}")
+    assert np.array_equal(res, res_o)
+    assert rep_o["exteval_nrobs"] == nrobs and rep_o["exteval_redundancy"] == r
+    assert f32(rep_o["exteval_sigma0"]) == v
