@@ -459,3 +459,81 @@ def test_exteval_matches_restatement(oracle_mod):
     assert np.array_equal(res, res_o)
     assert rep_o["exteval_nrobs"] == nrobs and rep_o["exteval_redundancy"] == r
     assert f32(rep_o["exteval_sigma0"]) == v
+
+
+def _bal_text(rng, nc=7, npt=40, nobs=150):
+    obs = sorted({(int(rng.integers(nc)), int(rng.integers(npt))) for _ in range(nobs)})
+    rng.shuffle(obs)
+    lines = [f"{nc} {npt} {len(obs)}"]
+    for c, p in obs:
+        lines.append(f"{c} {p} {rng.normal(0, 300):.6f} {rng.normal(0, 300):.6f}")
+    for c in range(nc):
+        aa = rng.normal(0, 0.8, 3) if c else np.zeros(3)  # camera 0: the zero rotation
+        vals = list(aa) + list(rng.normal(0, 2, 3)) + [rng.uniform(400, 600), rng.normal(0, 1e-2),
+                                                       rng.normal(0, 1e-4)]
+        lines += [f"{v:.10g}" for v in vals]
+    for p in range(npt):
+        lines += [f"{v:.9g}" for v in rng.normal(0, 3, 3)]
+    return "\n".join(lines) + "\n", len(obs)
+
+
+@pytest.mark.parametrize("k24out", [True, False])
+def test_input_block_matches_restatement(oracle_mod, tmp_path, k24out):
+    """InputBlock (rpba.cpp:180-284) with ComputeRotationMatrixfromRodriguesAngle
+    (rpba.cpp:341-366) restated: floats parsed as floats, the rotation in
+    double rounded to float, K = diag(f, f, 1), distpara k1 f^2, k2 f^4 in
+    float unless k24out, negated image coordinates, unit weights, slots in
+    the order of appearance.  Bit for bit."""
+    import math
+    rng = np.random.default_rng(11 + k24out)
+    text, nobs = _bal_text(rng)
+    path = tmp_path / "bal.txt"
+    path.write_text(text)
+    b = oracle_mod.input_block(str(path), k24out=k24out)
+    tok = text.split()
+    nc, npt, no = int(tok[0]), int(tok[1]), int(tok[2])
+    f32 = np.float32
+    pos = 3
+    xin = [[] for _ in range(nc)]
+    tracks = [[] for _ in range(npt)]
+    for _ in range(no):
+        c, p, x, y = int(tok[pos]), int(tok[pos + 1]), f32(tok[pos + 2]), f32(tok[pos + 3])
+        pos += 4
+        xin[c].append((x, y))
+        tracks[p].append((c, len(xin[c]) - 1))
+    pmat = np.zeros((nc, 12), np.float32)
+    K = np.zeros((nc, 9), np.float32)
+    dist = np.zeros((nc, 2), np.float32)
+    for i in range(nc):
+        a, bb, c = float(tok[pos]), float(tok[pos + 1]), float(tok[pos + 2])
+        t = [f32(tok[pos + 3 + j]) for j in range(3)]
+        f, k2, k4 = f32(tok[pos + 6]), f32(tok[pos + 7]), f32(tok[pos + 8])
+        pos += 9
+        a2, b2, c2 = a * a, bb * bb, c * c
+        ab, ac, bc = a * bb, a * c, bb * c
+        aa = math.sqrt(a2 + b2 + c2)
+        ct = 0.5 if aa == 0.0 else (1.0 - math.cos(aa)) / (aa * aa)
+        st = 1.0 if aa == 0.0 else math.sin(aa) / aa
+        R = [1.0 - (b2 + c2) * ct, ab * ct - c * st, ac * ct + bb * st,
+             ab * ct + c * st, 1.0 - (c2 + a2) * ct, bc * ct - a * st,
+             ac * ct - bb * st, bc * ct + a * st, 1.0 - (a2 + b2) * ct]
+        for r in range(3):
+            pmat[i, 4 * r:4 * r + 3] = [f32(v) for v in R[3 * r:3 * r + 3]]
+            pmat[i, 4 * r + 3] = t[r]
+        K[i, 0] = K[i, 4] = f
+        K[i, 8] = f32(1)
+        dist[i] = (k2, k4) if k24out else (f32(f32(k2 * f) * f), f32(f32(f32(f32(k4 * f) * f) * f) * f))
+    XX = np.array([[f32(tok[pos + 3 * p + j]) for j in range(3)] for p in range(npt)], np.float32)
+    xg = np.array([(-x, -y) for c in range(nc) for x, y in xin[c]], np.float32)
+    img_off = np.cumsum([0] + [len(v) for v in xin]).astype(np.int32)
+    assert np.array_equal(b.pmat, pmat)
+    assert np.array_equal(b.K, K)
+    assert np.array_equal(b.distpara, dist)
+    assert np.array_equal(b.XX, XX)
+    assert np.array_equal(b.img_obs_off, img_off)
+    assert np.array_equal(b.xg, xg)
+    assert (b.wx == 1).all() and (b.wy == 1).all() and (b.wxy == 0).all()
+    off = np.cumsum([0] + [len(t) for t in tracks]).astype(np.int32)
+    assert np.array_equal(b.pt_obs_off, off)
+    assert np.array_equal(b.pt_obs_image, np.array([c for t in tracks for c, _ in t], np.int32))
+    assert np.array_equal(b.pt_obs_slot, np.array([s for t in tracks for _, s in t], np.int32))
