@@ -89,7 +89,9 @@ void angleaxis_to_R(double a, double b, double c, float *R) {
 
 // rpba.cpp:371-439
 void R_to_angleaxis(const float *R, double &a, double &b, double &c) {
-  auto m = [&](int r, int cc) { return (double)R[r * 3 + cc]; };
+  // the entries stay float as in the reference: a sum or difference of two
+  // entries is rounded to float, anything with a double constant is double
+  auto m = [&](int r, int cc) -> float { return R[r * 3 + cc]; };
   const double e0 = 0.01, e1 = 0.1, pi = 3.14159265358979323846;
   const double tr = (m(0, 0) + m(1, 1) + m(2, 2) - 1.) * 0.5;
   if (std::fabs(m(0, 1) - m(1, 0)) < e0 && std::fabs(m(1, 2) - m(2, 1)) < e0 && std::fabs(m(0, 2) - m(2, 0)) < e0) {

@@ -537,3 +537,80 @@ def test_input_block_matches_restatement(oracle_mod, tmp_path, k24out):
     assert np.array_equal(b.pt_obs_off, off)
     assert np.array_equal(b.pt_obs_image, np.array([c for t in tracks for c, _ in t], np.int32))
     assert np.array_equal(b.pt_obs_slot, np.array([s for t in tracks for _, s in t], np.int32))
+
+
+def _rodrigues_from_R(R):
+    """ComputeRodriguesAnglefromRotationMatrix (rpba.cpp:371-439) with the
+    reference's float and double arithmetic (sums of two matrix entries are
+    float, anything with a double constant double)."""
+    import math
+    f32 = np.float32
+    e0, e1, pi = 0.01, 0.1, 3.14159265358979323846
+    r = [[f32(R[i][j]) for j in range(3)] for i in range(3)]
+    trace1 = (float(f32(f32(r[0][0] + r[1][1]) + r[2][2])) - 1.0) * 0.5
+    d = lambda x, y: abs(float(f32(x - y)))
+    s = lambda x, y: abs(float(f32(x + y)))
+    if d(r[0][1], r[1][0]) < e0 and d(r[1][2], r[2][1]) < e0 and d(r[0][2], r[2][0]) < e0:
+        if s(r[0][1], r[1][0]) < e1 and s(r[1][2], r[2][1]) < e1 and s(r[0][2], r[2][0]) < e1 and trace1 > 0.9:
+            return 0.0, 0.0, 0.0
+        xx, yy, zz = (float(r[0][0]) + 1.0) * 0.5, (float(r[1][1]) + 1.0) * 0.5, (float(r[2][2]) + 1.0) * 0.5
+        xy, xz, yz = (float(f32(r[0][1] + r[1][0])) * 0.25, float(f32(r[0][2] + r[2][0])) * 0.25,
+                      float(f32(r[1][2] + r[2][1])) * 0.25)
+        if xx > yy and xx > zz:
+            if xx < e0:
+                return 0.0, math.sqrt(0.5) * pi, math.sqrt(0.5) * pi
+            t = math.sqrt(xx)
+            return t * pi, xy / t * pi, xz / t * pi
+        if yy > zz:
+            if yy < e0:
+                return math.sqrt(0.5) * pi, 0.0, math.sqrt(0.5) * pi
+            t = math.sqrt(yy)
+            return xy / t * pi, t * pi, yz / t * pi
+        if zz < e0:
+            return math.sqrt(0.5) * pi, math.sqrt(0.5) * pi, 0.0
+        t = math.sqrt(zz)
+        return xz / t * pi, yz / t * pi, t * pi
+    aa = math.acos(trace1)
+    bb = 0.5 * aa / math.sin(aa)
+    return (bb * float(f32(r[2][1] - r[1][2])), bb * float(f32(r[0][2] - r[2][0])),
+            bb * float(f32(r[1][0] - r[0][1])))
+
+
+@pytest.mark.parametrize("k24out", [True, False])
+def test_output_block_matches_restatement(oracle_mod, tmp_path, k24out):
+    """OutputBlock (rpba.cpp:286-338): counts, then per point its
+    observations sorted by image with the un-negated coordinates, per camera
+    the angle-axis of R, t, f and the distortion (divided by f^2 and f^4 in
+    double unless k24out), per point X; setprecision(8) is %.8g.  Text for
+    text, on the block read back and on an adjusted block."""
+    import rpba_b200 as rb
+    rng = np.random.default_rng(21 + k24out)
+    text, _ = _bal_text(rng)
+    src = tmp_path / "in.txt"
+    src.write_text(text)
+    blk = oracle_mod.input_block(str(src), k24out=k24out)
+    st, adj, _, _ = oracle_mod.calc_plsa(blk, rb.make_options(robust=False))
+    for b in (blk, adj):
+        out = tmp_path / "out.txt"
+        oracle_mod.output_block(str(out), b, k24out=k24out)
+        g = lambda v: "%.8g" % float(v)
+        lines = [f"{b.n_images} {b.n_points} {b.n_obs}"]
+        for p in range(b.n_points):
+            s, e = b.pt_obs_off[p], b.pt_obs_off[p + 1]
+            for c, sl in sorted(zip(b.pt_obs_image[s:e], b.pt_obs_slot[s:e])):
+                x, y = b.xg[b.img_obs_off[c] + sl]
+                lines.append(f"{c} {p} {g(-x)} {g(-y)}")
+        for i in range(b.n_images):
+            R = b.pmat[i].reshape(3, 4)[:, :3]
+            a, bb, c = _rodrigues_from_R(R)
+            f = b.K[i, 0]
+            if k24out:
+                d0, d1 = b.distpara[i]
+            else:
+                f2 = 1.0 / (float(f) * float(f))
+                d0, d1 = float(b.distpara[i, 0]) * f2, float(b.distpara[i, 1]) * f2 * f2
+            t = b.pmat[i].reshape(3, 4)[:, 3]
+            lines.append(" ".join(g(v) for v in (a, bb, c, t[0], t[1], t[2], f, d0)) + " " + g(d1))
+        for p in range(b.n_points):
+            lines.append(" ".join(g(v) for v in b.XX[p]))
+        assert out.read_text() == "\n".join(lines) + "\n"
