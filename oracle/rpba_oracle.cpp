@@ -2546,6 +2546,22 @@ void oracle_lsa_points(void *h, int32_t *nrpv, double *XX) {
   std::copy(l->nrpv.begin(), l->nrpv.end(), nrpv);
   std::copy(l->XX.begin(), l->XX.end(), XX);
 }
+/* The trial cameras the last decoding produced (eRMnew, ePCnew, camerasnew:
+ * 9, 3, 9 and 2 doubles per image) and defdiff. */
+double oracle_lsa_cameras(void *h, double *R, double *PC, double *K, double *d) {
+  LSA *l = (LSA *)h;
+  std::copy(l->Rn.begin(), l->Rn.end(), R);
+  std::copy(l->PCn.begin(), l->PCn.end(), PC);
+  std::copy(l->Kn.begin(), l->Kn.end(), K);
+  std::copy(l->dn.begin(), l->dn.end(), d);
+  return l->defdiff;
+}
+/* The float cost sum of the cost pass at the state vector. */
+float oracle_lsa_sig0(void *h) {
+  LSA *l = (LSA *)h;
+  l->calc_corrections(false, 1., l->XPM, true, false);
+  return l->sig0;
+}
 /* One damped solve (CalcBundleSep with multfact) on a test handle: the
  * trial state vector XPMatricesnew = XPMatrices - x (nrioff3 entries). */
 int32_t oracle_lsa_step_xm(void *h, double multfact, double *xm_new) {

@@ -614,3 +614,79 @@ def test_output_block_matches_restatement(oracle_mod, tmp_path, k24out):
         for p in range(b.n_points):
             lines.append(" ".join(g(v) for v in b.XX[p]))
         assert out.read_text() == "\n".join(lines) + "\n"
+
+
+def test_residuals_and_cost_match_restatement(oracle_mod):
+    """CalcCorrections' observation loop (rbacore.cpp:1215-1331) restated on
+    the oracle's decoded cameras: x = R (X + PC); 1/z with the |z| < 1e-3
+    guard; RadialReconstructionImage (rpba.h:850-857) in double; K in double;
+    d = xg - x, clamped to +-defdiff; the float cost terms
+    (d1^2 W0 + 2 d1 d2 W2) + d2^2 W1 summed in float in track order.  A few
+    observations are moved 2e4 px so that the clamp acts.  Bit for bit."""
+    import rpba_b200 as rb
+    L = _wrap(oracle_mod.lib())
+    L.oracle_lsa_create.restype = C.c_void_p
+    L.oracle_lsa_create.argtypes = [C.c_void_p, C.c_void_p]
+    L.oracle_lsa_cameras.restype = C.c_double
+    L.oracle_lsa_cameras.argtypes = [C.c_void_p] * 5
+    L.oracle_lsa_sig0.restype = C.c_float
+    L.oracle_lsa_sig0.argtypes = [C.c_void_p]
+    blk = scenes.to_block(scenes.arc_scene(seed=14, n_cams=12, n_pts=900))
+    blk.xg[::97] += np.float32(2e4)
+    o = rb.make_options(robust=False)
+    cb = blk.as_c()
+    h = L.oracle_lsa_create(C.addressof(cb), C.addressof(o))
+    assert h
+    try:
+        nt, npt, nx = L.oracle_lsa_n_track_obs(h), L.oracle_lsa_n_points(h), L.oracle_lsa_xm_size(h)
+        nrioff = L.oracle_lsa_nrioff(h)
+        toff = np.zeros(npt + 1, np.int32)
+        timg = np.zeros(nt, np.int32)
+        tslot = np.zeros(nt, np.int32)
+        L.oracle_lsa_tracks(h, _ptr(toff), _ptr(timg), _ptr(tslot), None)
+        xm = np.zeros(nx)
+        L.oracle_lsa_get_xm(h, _ptr(xm))
+        res_o = np.zeros(2 * nt)
+        L.oracle_lsa_residuals(h, _ptr(xm), _ptr(res_o))
+        n = blk.n_images
+        R, PC, K, dd = np.zeros(9 * n), np.zeros(3 * n), np.zeros(9 * n), np.zeros(2 * n)
+        defdiff = L.oracle_lsa_cameras(h, _ptr(R), _ptr(PC), _ptr(K), _ptr(dd))
+        sig0_o = L.oracle_lsa_sig0(h)
+    finally:
+        L.oracle_lsa_destroy(h)
+    f32 = np.float32
+    res = np.zeros(2 * nt)
+    sig0 = f32(0)
+    clamped = 0
+    for p in range(npt):
+        X = xm[nrioff + 3 * p:nrioff + 3 * p + 3]
+        for t in range(toff[p], toff[p + 1]):
+            k = timg[t]
+            v = (X[0] + PC[3 * k], X[1] + PC[3 * k + 1], X[2] + PC[3 * k + 2])
+            Rk = R[9 * k:9 * k + 9]
+            e = [((Rk[3 * r] * v[0] + Rk[3 * r + 1] * v[1]) + Rk[3 * r + 2] * v[2]) for r in range(3)]
+            z = e[2]
+            z = (-1e3 if z < 0 else 1e3) if abs(z) < 1e-3 else 1.0 / z
+            x, y = e[0] * z, e[1] * z
+            dist = x * x + y * y
+            zz = 1.0 + (dd[2 * k] * dist + dd[2 * k + 1] * dist * dist)
+            x, y = x * zz, y * zz
+            Kk = K[9 * k:9 * k + 9]
+            cx = (x * Kk[0] + y * Kk[1]) + Kk[2]
+            cy = y * Kk[4] + Kk[5]
+            sl = blk.img_obs_off[k] + tslot[t]
+            d1 = float(blk.xg[sl, 0]) - cx
+            d2 = float(blk.xg[sl, 1]) - cy
+            if abs(d1) > defdiff or abs(d2) > defdiff:
+                clamped += 1
+            d1 = min(max(d1, -defdiff), defdiff)
+            d2 = min(max(d2, -defdiff), defdiff)
+            res[2 * t], res[2 * t + 1] = d1, d2
+            a, b = f32(d1), f32(d2)
+            w0, w1, w2 = blk.wx[sl], blk.wy[sl], blk.wxy[sl]
+            val = f32(f32(f32(a * a) * w0) + f32(f32(f32(2) * a) * b) * w2) + f32(f32(b * b) * w1)
+            sig0 = f32(sig0 + val)
+    print(f"{nt} observations, {clamped} clamped, sig0 {sig0}")
+    assert clamped > 0
+    assert np.array_equal(res, res_o)
+    assert sig0 == f32(sig0_o)
