@@ -690,3 +690,49 @@ def test_residuals_and_cost_match_restatement(oracle_mod):
     assert clamped > 0
     assert np.array_equal(res, res_o)
     assert sig0 == f32(sig0_o)
+
+
+def _cayley(a, b, c):
+    """ComputeRotationMatrixfromRodrigues (rbacore.cpp:2014-2043)."""
+    a2, b2, c2 = a * a, b * b, c * c
+    ab, ac, bc = a * b, a * c, b * c
+    abc = 4 + a2 + b2 + c2
+    abc = (-1e20 if abc < 0 else 1e20) if abs(abc) < 1e-20 else 1.0 / abc
+    return np.array([[abc * (4 + a2 - b2 - c2), abc * (2 * ab - 4 * c), abc * (2 * ac + 4 * b)],
+                     [abc * (2 * ab + 4 * c), abc * (4 - a2 + b2 - c2), abc * (2 * bc - 4 * a)],
+                     [abc * (2 * ac - 4 * b), abc * (2 * bc + 4 * a), abc * (4 - a2 - b2 + c2)]])
+
+
+def _rectify(R):
+    """RectifyRotationMatrix3 (rpba.h:876-915): the quaternion of R's
+    antisymmetric part and trace, back to a rotation."""
+    import math
+    R = [[float(v) for v in row] for row in R]
+    a = [R[2][1] - R[1][2], R[0][2] - R[2][0], R[1][0] - R[0][1]]
+    a = [1e-20 if abs(v) < 1e-20 else v for v in a]
+    al = math.sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2])
+    a = [v / al for v in a]
+    phi = math.atan2(al, R[0][0] + R[1][1] + R[2][2] - 1.0)
+    q = [math.cos(phi * 0.5)] + [a[i] * math.sin(phi * 0.5) for i in range(3)]
+    return np.array([
+        [q[0] * q[0] + q[1] * q[1] - q[2] * q[2] - q[3] * q[3], 2 * (q[1] * q[2] - q[0] * q[3]),
+         2 * (q[1] * q[3] + q[0] * q[2])],
+        [2 * (q[2] * q[1] + q[0] * q[3]), q[0] * q[0] - q[1] * q[1] + q[2] * q[2] - q[3] * q[3],
+         2 * (q[2] * q[3] - q[0] * q[1])],
+        [2 * (q[3] * q[1] - q[0] * q[2]), 2 * (q[3] * q[2] + q[0] * q[1]),
+         q[0] * q[0] - q[1] * q[1] - q[2] * q[2] + q[3] * q[3]]])
+
+
+def test_rotation_parameterisation_matches_restatement(oracle_mod):
+    """The camera update's rotation: the Cayley form of the increment
+    (ComputeRotationMatrixfromRodrigues) and the quaternion rectification
+    (RectifyRotationMatrix3/4) restated from the reference's text, on small
+    and large increments and on perturbed, non-orthonormal matrices.  Bit
+    for bit."""
+    rng = np.random.default_rng(5)
+    for scale in (1e-8, 1e-3, 0.3, 3.0):
+        for _ in range(50):
+            a, b, c = rng.normal(0, scale, 3)
+            assert np.array_equal(oracle_mod.cayley(a, b, c), _cayley(a, b, c))
+            R = _cayley(a, b, c) + rng.normal(0, 1e-6, (3, 3))
+            assert np.array_equal(oracle_mod.rectify3(R.copy()), _rectify(R))
