@@ -2562,6 +2562,94 @@ float oracle_lsa_sig0(void *h) {
   l->calc_corrections(false, 1., l->XPM, true, false);
   return l->sig0;
 }
+/* The LSA's primitives one at a time, for a restatement of Adjust's
+ * control flow driven from outside (rbacore.cpp:333-616).  A raw handle
+ * (after the constructor only) and one operation per call:
+ *   0 PrepareWeights2D(pass = arg), flags cleared; out: wsum
+ *   1 points into XPMatrices, EncodeCameras; out: nrioff3, nraddpi *
+ *     nrcameras, observations, lflflag, 1 if an image has no observation
+ *   2 DecodeCameras(XPMatrices) and the cost pass; out: sig0
+ *   3 Reweight2D(iflag = arg); out: wsum, flagged observations
+ *   4 CalcBundleSep(multfact = arg), XPMatricesnew = XPMatrices - x; out:
+ *     1 if x holds a NaN or an infinity
+ *   5 DecodeCameras(XPMatricesnew) and the cost pass; out: sig0
+ *   6 StoreResultsIteration
+ *   7 RobustDelete (flags of the stored state); out: observations, points
+ *   8 iniflag = true (a new pass) */
+void *oracle_lsa_create_raw(const rpba_block *blk, const rpba_options *o) {
+  static std::string sink;
+  LSA *l = new LSA(blk, make_opts(o), &sink);
+  if (l->bad_setup) {
+    delete l;
+    return nullptr;
+  }
+  return l;
+}
+void oracle_lsa_op(void *h, int32_t op, double arg, double *out) {
+  LSA *l = (LSA *)h;
+  switch (op) {
+    case 0:
+      l->imagepointnr = l->toff[l->nrpts];
+      l->isflag.assign(l->imagepointnr, 0);
+      l->isflagnew.assign(l->imagepointnr, 0);
+      l->sig0rmv.assign(l->imagepointnr, 0.f);
+      l->prepare_weights((int)arg);
+      out[0] = l->wsum;
+      break;
+    case 1: {
+      for (int i = 0; i < l->nrpts; ++i)
+        for (int j = 0; j < 3; ++j) l->XPM[l->nrioff + i * 3 + j] = l->XX[3 * i + j];
+      l->encode_cameras();
+      std::vector<int> cnt(l->nimg, 0);
+      for (int o = 0; o < l->toff[l->nrpts]; ++o) ++cnt[l->timg[o]];
+      out[0] = l->nrioff3;
+      out[1] = l->nadd * l->nimg;
+      out[2] = l->toff[l->nrpts];
+      out[3] = l->lflflag ? 1 : 0;
+      out[4] = std::count(cnt.begin(), cnt.end(), 0) > 0 ? 1 : 0;
+      l->x.assign(l->nrioff3 + l->nadd * l->nimg, 0.);
+      break;
+    }
+    case 2:
+      l->decode_cameras(l->XPM);
+      l->calc_corrections(false, 1., l->XPM, true, false);
+      out[0] = l->sig0;
+      break;
+    case 3: {
+      l->reweight((int)arg);
+      int nf = 0;
+      for (char f : l->isflag) nf += f ? 1 : 0;
+      out[0] = l->wsum;
+      out[1] = nf;
+      break;
+    }
+    case 4: {
+      out[0] = l->calc_bundle_sep(arg) ? 2 : 0;
+      for (int i = 0; i < (int)l->x.size(); ++i) {
+        if (!std::isfinite(l->x[i])) out[0] = 1;
+        l->XPMn[i] = l->XPM[i] - l->x[i];
+      }
+      break;
+    }
+    case 5:
+      l->decode_cameras(l->XPMn);
+      l->calc_corrections(false, 1., l->XPMn, true, false);
+      out[0] = l->sig0;
+      break;
+    case 6:
+      l->store_results();
+      break;
+    case 7:
+      l->robust_delete();
+      out[0] = l->toff[l->nrpts];
+      out[1] = l->nrpts;
+      break;
+    case 8:
+      l->iniflag = true;
+      break;
+  }
+}
+void oracle_lsa_output(void *h, rpba_block *blk) { ((LSA *)h)->output(blk); }
 /* One damped solve (CalcBundleSep with multfact) on a test handle: the
  * trial state vector XPMatricesnew = XPMatrices - x (nrioff3 entries). */
 int32_t oracle_lsa_step_xm(void *h, double multfact, double *xm_new) {

@@ -736,3 +736,121 @@ def test_rotation_parameterisation_matches_restatement(oracle_mod):
             assert np.array_equal(oracle_mod.cayley(a, b, c), _cayley(a, b, c))
             R = _cayley(a, b, c) + rng.normal(0, 1e-6, (3, 3))
             assert np.array_equal(oracle_mod.rectify3(R.copy()), _rectify(R))
+
+
+def _adjust_restated(L, h, robust, report):
+    """Adjust (rbacore.cpp:333-616; itbreakflag false, no GCPs) restated from
+    the reference's text over the LSA's primitives: two passes (multfact
+    1e-3, then 1e-6), the pass-0 cost at the start, iflag = 2 (robust) or 1,
+    Reweight2D before every solve of the robust pass, sig0 = cost wsumg /
+    redundancy in float, iflag decremented when sig0old < sig0 sig0frac,
+    a step stored when it does not raise sig0 or is the pass's first,
+    RobustDelete after pass 0, at most 201 solves."""
+    f32 = np.float32
+    out = np.zeros(8)
+    op = lambda code, arg=0.0: (L.oracle_lsa_op(h, code, arg, _ptr(out)), out.copy())[1]
+    itt = 0
+    ittflag = True
+    multfact = 1e-3
+    sig0frac = None
+    sig0old = sig0in = f32(1e20)
+    nrobsnew = nrunknownsnew = redundancynew = 0
+    for it in (0, 1):
+        sig0old = f32(1e20)
+        if it > 0:
+            op(8)
+            multfact = 1e-6
+        if ittflag:
+            wsum = f32(op(0, it)[0])
+            ittflag = False
+        o1 = op(1)
+        nrioff3, naddc, nobs_t, lfl, empty = int(o1[0]), int(o1[1]), int(o1[2]), bool(o1[3]), bool(o1[4])
+        if empty:
+            return "no observations"
+        if sig0frac is None:
+            sig0frac = f32(1.01) if lfl else f32(1.05)
+        imagepointnr = nobs_t
+        nrobs = 2 * imagepointnr
+        wsum = f32(f32(2 * imagepointnr) / wsum)
+        wsumg = wsum
+        nrunknowns = nrioff3 + naddc
+        redundancy = nrobs - nrunknowns
+        if redundancy < 0:
+            return "low redundancy"
+        if it == 0:
+            sig0 = f32(op(2)[0])
+            sig0 = f32(f32(sig0 * wsumg) / f32(redundancy))
+            sig0in = sig0old = sig0
+        else:
+            sig0in = sig0old
+        iflag = 2 if robust else 1
+        it_ = 1
+        nunk_given, nobs_given = nrunknowns, nrobs
+        while iflag > 0:
+            if it == 0 and robust:
+                nrunknowns, nrobs = nunk_given, nobs_given
+                o3 = op(3, iflag)
+                nrobs -= 2 * int(o3[1])
+                redundancy = nrobs - nrunknowns
+                wsum = f32(f32(2 * imagepointnr) / f32(o3[0]))
+                wsumg = wsum
+            if op(4, multfact)[0] != 0:
+                return "solve failed"
+            sig0 = f32(op(5)[0])
+            sig0 = f32(f32(sig0 * wsumg) / f32(redundancy))
+            if sig0old < f32(sig0 * sig0frac):
+                iflag -= 1
+            if sig0 <= sig0old or it_ == 1:
+                op(6)
+                sig0old = sig0
+                nrobsnew, nrunknownsnew, redundancynew = nrobs, nrunknowns, redundancy
+            if itt > 200:
+                break
+            itt += 1
+            it_ += 1
+        s_in, s_out = np.sqrt(sig0in, dtype=np.float32), np.sqrt(sig0old, dtype=np.float32)
+        if it == 0 and robust:
+            red, nob, nun = redundancynew, nrobsnew, nrunknownsnew
+        else:
+            red, nob, nun = redundancy, nrobs, nrunknowns
+        report.append((float(s_in), float(s_out), red, nob, nun, itt))
+        if robust and it == 0:
+            op(7)
+        ittflag = True
+    return "ok"
+
+
+@pytest.mark.parametrize("seed,robust", [(5, True), (6, True), (7, False)])
+def test_adjust_control_matches_restatement(oracle_mod, seed, robust):
+    """The oracle's Adjust against the restated control flow driving the
+    same primitives: identical report (sigma0 in and out, redundancy,
+    observations, unknowns and solve count per pass) and final block."""
+    import rpba_b200 as rb
+    L = _wrap(oracle_mod.lib())
+    L.oracle_lsa_create_raw.restype = C.c_void_p
+    L.oracle_lsa_create_raw.argtypes = [C.c_void_p, C.c_void_p]
+    L.oracle_lsa_op.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_void_p]
+    L.oracle_lsa_output.argtypes = [C.c_void_p, C.c_void_p]
+    blk = scenes.to_block(scenes.arc_scene(seed=seed, n_cams=10, n_pts=800))
+    o = rb.make_options(robust=robust, solver=rb.SOLVER_PCG)
+    st, ref, rep, _ = oracle_mod.calc_plsa(blk, o)
+    assert st == 0
+    b = blk.copy()
+    cb = b.as_c()
+    h = L.oracle_lsa_create_raw(C.addressof(cb), C.addressof(o))
+    assert h
+    report = []
+    try:
+        assert _adjust_restated(L, h, robust, report) == "ok"
+        L.oracle_lsa_output(h, C.addressof(cb))
+    finally:
+        L.oracle_lsa_destroy(h)
+    print(report)
+    for it, (s_in, s_out, red, nob, nun, itt) in enumerate(report):
+        assert np.float32(rep["sigma0_in"][it]) == np.float32(s_in)
+        assert np.float32(rep["sigma0_out"][it]) == np.float32(s_out)
+        assert (rep["redundancy"][it], rep["nrobs"][it], rep["nrunknowns"][it], rep["itt"][it]) == (red, nob, nun, itt)
+    for n in ("pmat", "K", "distpara", "XX", "pt_obs_off"):
+        assert np.array_equal(getattr(b, n), getattr(ref, n)), n
+    m = int(ref.pt_obs_off[-1])
+    assert np.array_equal(b.pt_obs_image[:m], ref.pt_obs_image[:m])
