@@ -2650,6 +2650,14 @@ void oracle_lsa_op(void *h, int32_t op, double arg, double *out) {
   }
 }
 void oracle_lsa_output(void *h, rpba_block *blk) { ((LSA *)h)->output(blk); }
+/* DecodeCameras of a given state vector (nrioff3 entries); read the result
+ * with oracle_lsa_cameras. */
+void oracle_lsa_decode(void *h, const double *xm) {
+  LSA *l = (LSA *)h;
+  std::vector<double> XM(l->XPM);
+  std::memcpy(XM.data(), xm, sizeof(double) * l->nrioff3);
+  l->decode_cameras(XM);
+}
 /* One damped solve (CalcBundleSep with multfact) on a test handle: the
  * trial state vector XPMatricesnew = XPMatrices - x (nrioff3 entries). */
 int32_t oracle_lsa_step_xm(void *h, double multfact, double *xm_new) {

@@ -854,3 +854,133 @@ def test_adjust_control_matches_restatement(oracle_mod, seed, robust):
         assert np.array_equal(getattr(b, n), getattr(ref, n)), n
     m = int(ref.pt_obs_off[-1])
     assert np.array_equal(b.pt_obs_image[:m], ref.pt_obs_image[:m])
+
+
+@pytest.mark.parametrize("addflags", [(True, True, True), (False, True, False)])
+def test_camera_coding_matches_restatement(oracle_mod, addflags):
+    """PointXXvIn's selection and PrepareCameras' scale camera (rbacore.cpp:
+    670-700, 1918-1974), EncodeCameras (rbacore.cpp:999-1087) and
+    DecodeCameras (rbacore.cpp:1733-1800) restated: the scale camera is the
+    first one farthest (strictly) from camera 0 in R t of the caller's
+    cameras; encoding rectifies every camera but 0, PC = R^T t, the scale
+    camera's fixed coordinate the largest |PC| (compared in float);
+    decoding R = rectify(Cayley(w) R0), PC = PC0 + e, the additional
+    parameters, camera 0's intrinsics alone.  Bit for bit on a perturbed
+    state vector."""
+    import rpba_b200 as rb
+    L = _wrap(oracle_mod.lib())
+    L.oracle_lsa_create_raw.restype = C.c_void_p
+    L.oracle_lsa_create_raw.argtypes = [C.c_void_p, C.c_void_p]
+    L.oracle_lsa_op.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_void_p]
+    L.oracle_lsa_decode.argtypes = [C.c_void_p, C.c_void_p]
+    L.oracle_lsa_normcamera.restype = C.c_int32
+    L.oracle_lsa_normcamera.argtypes = [C.c_void_p]
+    L.oracle_lsa_cameras.restype = C.c_double
+    L.oracle_lsa_cameras.argtypes = [C.c_void_p] * 5
+    blk = scenes.to_block(scenes.arc_scene(seed=3, n_cams=8, n_pts=400))
+    off = blk.pt_obs_off.copy()
+    # a point with one observation and one with Z ~ 0: PointXXvIn drops both
+    one = int(np.nonzero(np.diff(off) >= 3)[0][0])
+    blk.pt_obs_off[one + 1:] -= np.int32(np.diff(off)[one] - 1)
+    keep_t = np.ones(len(blk.pt_obs_image), bool)
+    keep_t[off[one] + 1:off[one + 1]] = False
+    blk.pt_obs_image = blk.pt_obs_image[keep_t]
+    blk.pt_obs_slot = blk.pt_obs_slot[keep_t]
+    blk.XX[one + 1, 2] = np.float32(1e-9)
+    o = rb.make_options(robust=False, k2=addflags[0], k4=addflags[1], f=addflags[2])
+    nadd = sum(addflags)
+    cb = blk.as_c()
+    h = L.oracle_lsa_create_raw(C.addressof(cb), C.addressof(o))
+    assert h
+    n = blk.n_images
+    out = np.zeros(8)
+    try:
+        norm = L.oracle_lsa_normcamera(h)
+        L.oracle_lsa_op(h, 0, 0.0, _ptr(out))
+        L.oracle_lsa_op(h, 1, 0.0, _ptr(out))
+        nx, npt, nt = L.oracle_lsa_xm_size(h), L.oracle_lsa_n_points(h), L.oracle_lsa_n_track_obs(h)
+        nrioff = L.oracle_lsa_nrioff(h)
+        toff = np.zeros(npt + 1, np.int32)
+        timg = np.zeros(nt, np.int32)
+        tslot = np.zeros(nt, np.int32)
+        L.oracle_lsa_tracks(h, _ptr(toff), _ptr(timg), _ptr(tslot), None)
+        xm = np.zeros(nx)
+        L.oracle_lsa_get_xm(h, _ptr(xm))
+        rng = np.random.default_rng(2)
+        xm2 = xm.copy()
+        xm2[:nrioff] += rng.normal(0, 1e-3, nrioff)
+        L.oracle_lsa_decode(h, _ptr(xm2))
+        R, PC, K, dd = np.zeros(9 * n), np.zeros(3 * n), np.zeros(9 * n), np.zeros(2 * n)
+        L.oracle_lsa_cameras(h, _ptr(R), _ptr(PC), _ptr(K), _ptr(dd))
+    finally:
+        L.oracle_lsa_destroy(h)
+    # PointXXvIn
+    kept = [p for p in range(blk.n_points)
+            if blk.pt_obs_off[p + 1] - blk.pt_obs_off[p] >= 2 and abs(float(blk.XX[p, 2])) > 1e-8]
+    assert one not in kept and one + 1 not in kept
+    assert np.array_equal(toff, np.cumsum([0] + [blk.pt_obs_off[p + 1] - blk.pt_obs_off[p] for p in kept]))
+    assert np.array_equal(timg, np.concatenate([blk.pt_obs_image[blk.pt_obs_off[p]:blk.pt_obs_off[p + 1]]
+                                                for p in kept]))
+    # PrepareCameras
+    P = blk.pmat.astype(np.float64).reshape(n, 3, 4)
+    Tv = [[(P[i, r, 0] * P[i, 0, 3] + P[i, r, 1] * P[i, 1, 3]) + P[i, r, 2] * P[i, 2, 3] for r in range(3)]
+          for i in range(n)]
+    best, want = 0.0, -1
+    for i in range(1, n):
+        dist = 0.0
+        for j in range(3):
+            dist += (Tv[i][j] - Tv[0][j]) * (Tv[i][j] - Tv[0][j])
+        if dist > best:
+            best, want = dist, i
+    assert norm == want
+    # EncodeCameras, then DecodeCameras of the perturbed vector
+    nrparir, nrpari = 5 + nadd, 6 + nadd
+    camparv = [0, nadd]
+    for k in range(1, n):
+        camparv.append(camparv[-1] + (nrparir if k == norm else nrpari))
+    f32 = np.float32
+    for k in range(1, n):
+        Rb = _rectify(P[k, :, :3])
+        pcb = [Rb[0][i] * P[k, 0, 3] + Rb[1][i] * P[k, 1, 3] + Rb[2][i] * P[k, 2, 3] for i in range(3)]
+        cp = camparv[k]
+        Ra = _cayley(*xm2[cp:cp + 3])
+        Rn = np.array([[(Ra[i, 0] * Rb[0][j] + Ra[i, 1] * Rb[1][j]) + Ra[i, 2] * Rb[2][j] for j in range(3)]
+                       for i in range(3)])
+        Rn = _rectify(Rn)
+        if k == norm:
+            maxv, maxi = f32(0), 0
+            for i in range(3):
+                if abs(pcb[i]) > float(maxv):
+                    maxv, maxi = f32(abs(pcb[i])), i
+            es = [i for i in range(3) if i != maxi]
+            e = [0.0] * 3
+            e[es[0]], e[es[1]], e[maxi] = xm2[cp + 3], xm2[cp + 4], 0.0
+            a = 4
+        else:
+            e = list(xm2[cp + 3:cp + 6])
+            a = 5
+        assert np.array_equal(R[9 * k:9 * k + 9], Rn.reshape(-1)), k
+        assert np.array_equal(PC[3 * k:3 * k + 3], np.array([e[i] + pcb[i] for i in range(3)])), k
+        d0, d1, f = float(blk.distpara[k, 0]), float(blk.distpara[k, 1]), float(blk.K[k, 0])
+        if addflags[0]:
+            a += 1
+            d0 = xm2[cp + a]
+        if addflags[1]:
+            a += 1
+            d1 = xm2[cp + a]
+        if addflags[2]:
+            a += 1
+            f = xm2[cp + a]
+        assert (dd[2 * k], dd[2 * k + 1], K[9 * k], K[9 * k + 4], K[9 * k + 8]) == (d0, d1, f, f, 1.0), k
+    a = -1
+    d0, d1, f = float(blk.distpara[0, 0]), float(blk.distpara[0, 1]), float(blk.K[0, 0])
+    if addflags[0]:
+        a += 1
+        d0 = xm2[a]
+    if addflags[1]:
+        a += 1
+        d1 = xm2[a]
+    if addflags[2]:
+        a += 1
+        f = xm2[a]
+    assert (dd[0], dd[1], K[0], K[4], K[8]) == (d0, d1, f, f, 1.0)
