@@ -984,3 +984,169 @@ def test_camera_coding_matches_restatement(oracle_mod, addflags):
         a += 1
         f = xm2[a]
     assert (dd[0], dd[1], K[0], K[4], K[8]) == (d0, d1, f, f, 1.0)
+
+
+def _lsax_point(blk, p, sig0w, robustmode, weight_only):
+    """CalcLSAXMulti (rpbacore.cpp:536-773) with CalcCorrPointMulti
+    (778-837) and CalcCalibratedDerivatives (841-880) for one point,
+    restated; wxyflag off.  Returns (X, keep, conv, sig0io term, redundancy
+    term)."""
+    f32 = np.float32
+    s, e = blk.pt_obs_off[p], blk.pt_obs_off[p + 1]
+    imgs = list(blk.pt_obs_image[s:e])
+    slots = [blk.img_obs_off[j] + sl for j, sl in zip(imgs, blk.pt_obs_slot[s:e])]
+    P = blk.pmat.astype(np.float64).reshape(-1, 3, 4)
+    pxs = len(imgs)
+    wxi = [f32(blk.wx[sl]) for sl in slots]
+    wyi = [f32(blk.wy[sl]) for sl in slots]
+    wxyi = [f32(blk.wxy[sl]) for sl in slots]
+    wxo, wyo, wxyo = list(wxi), list(wyi), list(wxyi)
+    wsum = f32(0)
+    for a, b in zip(wxi, wyi):
+        wsum = f32(wsum + f32(a + b))
+
+    def corr(X):
+        c, s0, sv, p1v, p2v, p3v = [], f32(0), [], [], [], []
+        for js, j in enumerate(imgs):
+            M = P[j]
+            p1 = ((M[0, 0] * X[0] + M[0, 1] * X[1]) + M[0, 2] * X[2]) + M[0, 3]
+            p2 = ((M[1, 0] * X[0] + M[1, 1] * X[1]) + M[1, 2] * X[2]) + M[1, 3]
+            p3 = ((M[2, 0] * X[0] + M[2, 1] * X[1]) + M[2, 2] * X[2]) + M[2, 3]
+            p3 = (1e3 if p3 > 0 else -1e3) if abs(p3) < 1e-3 else 1.0 / p3
+            p1 *= p3
+            p2 *= p3
+            p1v.append(f32(p1))
+            p2v.append(f32(p2))
+            p3v.append(f32(p3))
+            dist = p1 * p1 + p2 * p2
+            z = 1.0 + (float(blk.distpara[j, 0]) * dist + float(blk.distpara[j, 1]) * dist * dist)
+            p1, p2 = p1 * z * float(blk.K[j, 0]), p2 * z * float(blk.K[j, 0])
+            dx = float(blk.xg[slots[js], 0]) - p1
+            dy = float(blk.xg[slots[js], 1]) - p2
+            c += [dx, dy]
+            w0, w1, w2 = float(wxi[js]), float(wyi[js]), float(wxyi[js])
+            s0 = f32(s0 + f32(dx * dx * w0 + dy * dy * w1 + 2 * dx * dy * w2))
+            sv.append(f32(dx * dx * float(wxo[js]) + dy * dy * float(wyo[js]) + 2 * dx * dy * float(wxyo[js])))
+        return c, s0, sv, p1v, p2v, p3v
+
+    X = Xold = Xin = [f32(v) for v in blk.XX[p]]
+    corrv, sig0opt, sig0v, p1v, p2v, p3v = corr([float(v) for v in X])
+    iflag = 2 if robustmode > 0 else 1
+    it = 1
+    conv = False
+    pxsd, pxs2 = pxs, 2 * pxs
+    delf = [False] * pxs
+    s0io, red = 0.0, 0
+    if weight_only:
+        wsum = f32(wsum / f32(pxs2))
+        s0io += float(f32(sig0opt / wsum))
+        red += pxs2 - 3
+    while iflag > -1 and it < 101:
+        N = np.zeros((3, 3))
+        BW = []
+        for js, j in enumerate(imgs):
+            x, y, P3 = float(p1v[js]), float(p2v[js]), float(p3v[js])
+            P1, P2 = float(f32(p1v[js] * p3v[js])), float(f32(p2v[js] * p3v[js]))
+            M = P[j]
+            xp = [M[0, c] * P3 - M[2, c] * P1 for c in range(3)]
+            yp = [M[1, c] * P3 - M[2, c] * P2 for c in range(3)]
+            k2, k4 = float(blk.distpara[j, 0]), float(blk.distpara[j, 1])
+            fx, fy, sk = float(blk.K[j, 0]), float(blk.K[j, 4]), float(blk.K[j, 1])
+            xy2 = x * x + y * y
+            xy4 = xy2 * xy2
+            xxpc = k4 * xy4 + x * (2 * k2 * x + 4 * k4 * x * xy2) + k2 * xy2 + 1.0
+            xypc = x * (4 * k4 * xy2 * y + 2 * k2 * y)
+            yxpc = y * (4 * k4 * x * xy2 + 2 * k2 * x)
+            yypc = y * (2 * k2 * y + 4 * k4 * xy2 * y) + k4 * xy4 + k2 * xy2 + 1.0
+            for c in range(3):
+                a0 = xxpc * xp[c] + xypc * yp[c]
+                b0 = yypc * yp[c] + yxpc * xp[c]
+                xp[c], yp[c] = a0 * fx + b0 * sk, b0 * fy
+            B = np.array([xp, yp])
+            w0, w1, w2 = float(wxi[js]), float(wyi[js]), float(wxyi[js])
+            Bw = np.array([[B[0, c] * w0 + B[1, c] * w2 for c in range(3)],
+                           [B[1, c] * w1 + B[0, c] * w2 for c in range(3)]])
+            BW.append(Bw)
+            N += B.T @ Bw
+        N[np.diag_indices(3)] *= 1.001
+        Ni = np.linalg.inv(N)
+        xip = np.zeros(3)
+        for i in range(pxs):
+            xip += Ni @ (BW[i].T @ np.array(corrv[2 * i:2 * i + 2]))
+        X = [f32(Xold[c] + f32(xip[c])) for c in range(3)]
+        corrv, sig0, sig0v, p1v, p2v, p3v = corr([float(v) for v in X])
+        if iflag == 1 and robustmode == 2:
+            for js, j in enumerate(imgs):
+                if f32(sig0v[js] * sig0w[j]) > f32(16):
+                    wxi[js] = f32(wxi[js] * f32(1e-4))
+                    wyi[js] = f32(wyi[js] * f32(1e-4))
+                    wxyi[js] = f32(wxyi[js] * f32(1e-4))
+                    if f32(wxi[js] + wyi[js]) < f32(2e-8):
+                        wxi[js] = wyi[js] = f32(1e-8)
+                        wxyi[js] = f32(0)
+                    pxsd -= 1
+                    delf[js] = True
+            if pxsd < 2:
+                break
+        if float(sig0) < float(sig0opt) * 1.001:
+            if sig0opt < f32(sig0 * f32(1.05)):
+                iflag -= 1
+            if not weight_only:
+                Xold = X
+            sig0opt = sig0
+            conv = True
+        else:
+            iflag -= 1
+        if weight_only:
+            break
+        it += 1
+    keep = [not (robustmode == 2 and d) for d in delf]
+    pxs2 -= 2 * sum(1 for d in delf if robustmode == 2 and d)
+    if sum(keep) < 2 or not conv:
+        return Xin, [False] * pxs, False, s0io, red
+    if not weight_only:
+        wsum = f32(wsum / f32(pxs2))
+        s0io += float(f32(sig0opt / wsum))
+        red += pxs2 - 3
+    return Xold, keep, True, s0io, red
+
+
+@pytest.mark.parametrize("robustmode,weight_only", [(0, False), (1, False), (2, False), (0, True)])
+def test_point_refinement_matches_restatement(oracle_mod, robustmode, weight_only):
+    """The oracle's CalcLSAXMulti (which the GPU kernel reproduces bit for
+    bit) against the restatement, point by point: the same convergence and
+    deletions and the same redundancy.  The restatement inverts the 3x3
+    normal matrix with numpy (the reference with Eigen, the oracle with its
+    cofactor form), so the refined float coordinates agree to roundoff that
+    can carry into the last accepted iterate: measured 97% of the points
+    identical, 99% within one float step, the worst 89 steps (1e-5
+    relative); the sigma0 sums within 1.5e-9; weight-only passes identical."""
+    from rpba_b200 import scenes as sc
+    bal = sc.arc_scene(seed=17, n_cams=12, n_pts=700)
+    blk = sc.to_block(bal)
+    rng = np.random.default_rng(4)
+    blk.XX += rng.normal(0, 0.02, blk.XX.shape).astype(np.float32)
+    sig0w = np.full(blk.n_images, 0.5, np.float32)
+    r = oracle_mod.triangulate(blk, sig0w if robustmode == 2 else None, robustmode, weight_only)
+    X_all, keep_all, conv_all = [], [], []
+    s0, red = 0.0, 0
+    for p in range(blk.n_points):
+        X, keep, conv, a, b = _lsax_point(blk, p, sig0w, robustmode, weight_only)
+        X_all.append(X)
+        keep_all += keep
+        conv_all.append(conv)
+        s0 += a
+        red += b
+    X_all = np.array(X_all, np.float32)
+    ulp = np.spacing(np.abs(r["XX"]).astype(np.float32))
+    print(f"robustmode {robustmode}, weight-only {weight_only}: {sum(conv_all)} of {blk.n_points} converged, "
+          f"{len(keep_all) - sum(keep_all)} observations not kept, max |dX| / ulp "
+          f"{(np.abs(X_all - r['XX']) / ulp).max():.1f}")
+    assert np.array_equal(np.array(conv_all), r["conv"].astype(bool))
+    assert np.array_equal(np.array(keep_all), r["keep"].astype(bool))
+    assert red == r["redundancy"]
+    steps = (np.abs(X_all - r["XX"]) / ulp).max(1)
+    assert (steps == 0).mean() >= 0.95 and np.percentile(steps, 99) <= 2 and steps.max() <= 128
+    if weight_only:
+        assert (steps == 0).all()
+    assert abs(s0 - r["sig0io"]) <= 5e-9 * abs(r["sig0io"])
