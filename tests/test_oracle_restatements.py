@@ -1150,3 +1150,220 @@ def test_point_refinement_matches_restatement(oracle_mod, robustmode, weight_onl
     if weight_only:
         assert (steps == 0).all()
     assert abs(s0 - r["sig0io"]) <= 5e-9 * abs(r["sig0io"])
+
+
+def _plsa_parallel_restated(oracle_mod, blk, part, T, opts):
+    """The parallel branch of CalcPLSA (rpbacore.cpp:100-510) restated in
+    Python from the reference's text; the partition steps and the merge
+    passes are the oracle's (oracle_lsa_gcp_step_full, oracle_merge)."""
+    import rpba_b200 as rb
+    from rpba_b200.block import Block
+    L = oracle_mod.lib()
+    L.oracle_merge.restype = C.c_int32
+    L.oracle_merge.argtypes = [C.c_void_p] * 7 + [C.c_int32] + [C.c_void_p] * 7
+    f32 = np.float32
+    n, npt = blk.n_images, blk.n_points
+    robust = bool(opts.robust)
+    nraddp = int(opts.k2) + int(opts.k4) + int(opts.f)
+    imgindv = [[i for i in range(n) if part[i] == it] for it in range(T)]
+    imgindbv = np.ascontiguousarray(part, np.int32)
+    pointXXv = [[(int(blk.pt_obs_image[t]), int(blk.pt_obs_slot[t])) for t in range(blk.pt_obs_off[p],
+                                                                                    blk.pt_obs_off[p + 1])]
+                for p in range(npt)]
+    XXd = blk.XX.astype(np.float64)
+    PMd = blk.pmat.astype(np.float64)
+    cameras = [(blk.K[i].copy(), blk.distpara[i].copy()) for i in range(n)]
+    cameraps = list(cameras)
+    camerasnew = list(cameras)
+    camerasoit = [list(cameras) for _ in range(T)]
+    PMdd = [PMd.copy() for _ in range(T)]
+    pointXXvv = [[] for _ in range(T)]
+    pindv = [[] for _ in range(T)]
+    gcpinfov = [[] for _ in range(T)]
+    W3ijiv = [[] for _ in range(T)]
+    gcpdatav = []
+    gcpinfo = [-1] * npt
+    pitflagsv = [None] * npt
+    sig0wv = np.zeros(n, np.float32)
+    w3d = np.zeros(npt * T * 6, np.float32)
+    nrparimages = (n - 2) * 6 + 5 + n * nraddp
+    nrppt = npt // T
+    beginv = [nrppt * c for c in range(T)]
+    endv = [nrppt * (c + 1) if c < T - 1 else npt for c in range(T)]
+    sig0opt = 1e20
+    iflag = 2 if robust else 1
+    it_ = 1
+    sig0frac = f32(1.01)
+    best = None
+    log = ""
+
+    def scene_block():
+        off = np.cumsum([0] + [len(v) for v in pointXXv]).astype(np.int32)
+        img = np.array([q[0] for v in pointXXv for q in v], np.int32)
+        slot = np.array([q[1] for v in pointXXv for q in v], np.int32)
+        K = np.array([c[0] for c in cameraps], np.float32)
+        d = np.array([c[1] for c in cameraps], np.float32)
+        return Block(blk.pmat.copy(), K, d, XXd.astype(np.float32), blk.img_obs_off, blk.xg, blk.wx, blk.wy,
+                     blk.wxy, off, img, slot)
+
+    def sweep(robustmode, weight_only, wxy, sig0vv):
+        nonlocal XXd
+        b = scene_block()
+        cb = b.as_c()
+        nt = len(b.pt_obs_image)
+        XXo = np.zeros(3 * npt)
+        keep = np.zeros(max(nt, 1), np.uint8)
+        sv = np.zeros(max(nt, 1), np.float32)
+        conv = np.zeros(max(npt, 1), np.uint8)
+        s0 = np.zeros(npt)
+        red = np.zeros(npt, np.int32)
+        Pd = np.ascontiguousarray(PMd)
+        L.oracle_merge(C.addressof(cb), _ptr(Pd), _ptr(sig0wv), robustmode, int(weight_only),
+                       _ptr(imgindbv) if wxy else None, T if wxy else 1, 0, _ptr(XXo), _ptr(keep), _ptr(sv),
+                       _ptr(conv), _ptr(w3d) if wxy else None, _ptr(s0), _ptr(red))
+        if sig0vv is not None:
+            for p in range(npt):
+                for t in range(b.pt_obs_off[p], b.pt_obs_off[p + 1]):
+                    sig0vv[b.pt_obs_image[t]].append(sv[t])
+        XXn = XXd.copy()
+        for p in range(npt):
+            if not pointXXv[p]:
+                continue
+            XXn[p] = XXo[3 * p:3 * p + 3]
+            pointXXv[p] = [pointXXv[p][t - b.pt_obs_off[p]] for t in range(b.pt_obs_off[p], b.pt_obs_off[p + 1])
+                           if keep[t]]
+        XXd = XXn
+        a, r = 0.0, 0
+        for c in range(T):
+            ac, rc = 0.0, 0
+            for p in range(beginv[c], endv[c]):
+                ac += s0[p]
+                rc += int(red[p])
+            a += ac
+            r += rc
+        return a, r
+
+    while iflag > 0 and it_ < 51:
+        robustflagit = False
+        if it_ > 1:
+            o = rb.make_options(robust=False, solver=opts.solver, k2=opts.k2 and it_ >= 3, k4=opts.k4 and it_ >= 3,
+                                f=opts.f and it_ >= 3)
+            for it in range(T):
+                imgs = imgindv[it]
+                loc = {g: li for li, g in enumerate(imgs)}
+                slots = [list(range(blk.img_obs_off[g], blk.img_obs_off[g + 1])) for g in imgs]
+                ioff = np.cumsum([0] + [len(s) for s in slots]).astype(np.int32)
+                flat = [s for ss in slots for s in ss]
+                pts = pointXXvv[it]
+                b = Block(PMdd[it][imgs].astype(np.float32), np.array([camerasoit[it][g][0] for g in imgs], np.float32),
+                          np.array([camerasoit[it][g][1] for g in imgs], np.float32),
+                          XXd[pindv[it]].astype(np.float32).reshape(-1, 3), ioff, blk.xg[flat], blk.wx[flat],
+                          blk.wy[flat], blk.wxy[flat],
+                          np.cumsum([0] + [len(v) for v in pts]).astype(np.int32),
+                          np.array([loc[q[0]] for v in pts for q in v], np.int32),
+                          np.array([q[1] for v in pts for q in v], np.int32))
+                W3 = np.array(W3ijiv[it], np.float32).reshape(-1, 6)
+                gd = np.array(gcpdatav, np.float64).reshape(-1, 3)
+                st, bo, Pout, used, lg = oracle_mod.lsa_gcp_step_full(b, np.array(gcpinfov[it], np.int32), W3, gd, n,
+                                                                       pmat_d=PMdd[it][imgs], opts=o)
+                log += lg
+                for j in range(len(pts)):
+                    if not used[j]:
+                        pts[j] = []
+                for li, g in enumerate(imgs):
+                    PMdd[it][g] = Pout[li]
+                    camerasoit[it][g] = (bo.K[li].copy(), bo.distpara[li].copy())
+            for it in range(T):
+                for g in imgindv[it]:
+                    PMd[g] = PMdd[it][g]
+                    cameraps[g] = camerasoit[it][g]
+                    camerasnew[g] = camerasoit[it][g]
+        if iflag == 1:
+            robustflagit = robust
+            if robust:
+                sig0frac = f32(1.02)
+        if it_ > 1:
+            pointXXv = [[] for _ in range(npt)]
+            for it in range(T):
+                for j, p in enumerate(pindv[it]):
+                    pointXXv[p] += pointXXvv[it][j]
+            pointXXv = [v if len(v) >= 2 else [] for v in pointXXv]
+        else:
+            cameraps = list(cameras)
+            camerasnew = list(cameras)
+        for p in range(npt):
+            if pointXXv[p]:
+                pitflagsv[p] = [False] * T
+                for q in pointXXv[p]:
+                    pitflagsv[p][part[q[0]]] = True
+        if robustflagit:
+            vv = [[] for _ in range(n)]
+            sweep(1, False, False, vv)
+            for i in range(n):
+                sig0wv[i] = 0 if not vv[i] else f32(1) / (sorted(vv[i])[len(vv[i]) // 2] * f32(2.1981))
+        a, r = sweep(2 if robustflagit else 0, it_ == 1, True, None)
+        sig0g = a / float(r - nrparimages)
+        if sig0g <= sig0opt:
+            best = (XXd.copy(), PMd.copy(), [list(v) for v in pointXXv], list(camerasnew))
+        camerasoit = [list(camerasnew) for _ in range(T)]
+        for it in range(T):
+            for g in imgindv[it]:
+                PMdd[it][g] = PMd[g]
+        pointXXvv = [[] for _ in range(T)]
+        pindv = [[] for _ in range(T)]
+        W3ijiv = [[] for _ in range(T)]
+        gcpdatav = []
+        nrgcp = 0
+        for c in range(T):
+            for p in range(beginv[c], endv[c]):
+                if len(pointXXv[p]) < 2:
+                    continue
+                if sum(pitflagsv[p]) > 1:
+                    gcpinfo[p] = nrgcp
+                    gcpdatav += list(XXd[p])
+                    for it in range(T):
+                        if pitflagsv[p][it]:
+                            W3ijiv[it] += list(w3d[(p * T + it) * 6:(p * T + it) * 6 + 6])
+                    nrgcp += 1
+                else:
+                    gcpinfo[p] = -1
+        for p in range(npt):
+            per = [[] for _ in range(T)]
+            for q in pointXXv[p]:
+                per[part[q[0]]].append(q)
+            for it in range(T):
+                if per[it]:
+                    pointXXvv[it].append(per[it])
+                    pindv[it].append(p)
+        gcpinfov = [[gcpinfo[p] for p in pindv[it]] for it in range(T)]
+        if it_ > 1:
+            if sig0g <= sig0opt:
+                if sig0opt < sig0g * float(sig0frac) and it_ > 3:
+                    iflag -= 1
+                else:
+                    sig0opt = sig0g
+            elif it_ > 3:
+                iflag -= 1
+        it_ += 1
+    return best, sig0opt, it_ - 1, log
+
+
+def test_parallel_loop_matches_python_restatement(oracle_mod):
+    """The oracle's parallel RPBA loop against the Python restatement of
+    rpbacore.cpp:100-510 driving the same partition step and merge pass:
+    the same best state, sigma0, iteration count and log."""
+    import rpba_b200 as rb
+    blk = scenes.to_block(scenes.arc_scene(seed=5, n_cams=30, n_pts=1500))
+    part = rb.partition_images(blk, 3)
+    o = rb.make_options()
+    st, b_o, s_o, log_o = oracle_mod.calc_plsa_parallel(blk, part, 3, o)
+    assert st == 0
+    (XXd, PMd, pxv, cams), sig0opt, iters, log = _plsa_parallel_restated(oracle_mod, blk, part, 3, o)
+    print(f"{iters} iterations, sigma0 {sig0opt:.6f}")
+    assert iters == s_o["iterations"] and sig0opt == s_o["sig0opt"]
+    assert log == log_o
+    assert np.array_equal(XXd.astype(np.float32), b_o.XX)
+    assert np.array_equal(PMd.astype(np.float32), b_o.pmat)
+    assert np.array_equal(np.array([c[0] for c in cams]), b_o.K)
+    assert np.array_equal(np.cumsum([0] + [len(v) for v in pxv]), b_o.pt_obs_off)
+    assert np.array_equal(np.array([q[0] for v in pxv for q in v], np.int32), b_o.pt_obs_image)
