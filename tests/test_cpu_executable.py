@@ -1,0 +1,78 @@
+"""The `rpba` executable (rpba.cpp:45-176 over the C ABI) without a GPU:
+the reference's `parameters` file is read (every key required, as
+rpba.cpp:56-64 reads them), the BAL file parsed, and the reference's header
+lines printed -- input file, flags, threads, cameras / points /
+observations, unknowns and redundancy (rpba.cpp:194-205) -- before the
+solve, which then reports the missing device and exits with status 2."""
+import os
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+EXE = os.path.join(ROOT, "rpba_b200", "rpba")
+
+pytestmark = pytest.mark.skipif(not os.path.exists(EXE), reason="executable not built")
+
+
+def _run(cwd, args=()):
+    import torch
+    env = dict(os.environ)
+    if not torch.cuda.is_available():
+        env["CUDA_VISIBLE_DEVICES"] = ""
+    return subprocess.run([EXE, *args], cwd=cwd, env=env, capture_output=True, text=True, timeout=120)
+
+
+@pytest.fixture
+def workdir(tmp_path, oracle_mod):
+    import rpba_b200 as rb
+    from rpba_b200 import scenes
+    blk = scenes.to_block(scenes.arc_scene(seed=2, n_cams=6, n_pts=80))
+    (tmp_path / "data").mkdir()
+    rb.OutputBlock(str(tmp_path / "data" / "scene.txt"), blk, k24out=True)
+    return tmp_path, blk
+
+
+def _params(path, **over):
+    kv = {"InputDir": "data", "File": "scene.txt", "Robust": "1", "Exteval": "0", "Threads": "1", "k2": "1",
+          "k4": "1", "f": "1", "k24out": "1"}
+    kv.update(over)
+    path.write_text("".join(f"{k}={v}\n" for k, v in kv.items() if v is not None))
+
+
+def test_header_and_missing_device(workdir):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present: the solve would run")
+    d, blk = workdir
+    _params(d / "parameters", Threads="3", k4="0")
+    r = _run(d)
+    out = r.stdout
+    nobs = blk.n_obs
+    nadd = 2
+    unk = 3 * blk.n_points + (blk.n_images - 2) * 6 + 5 + blk.n_images * nadd
+    assert "Inputfile: data/scene.txt" in out
+    assert "Robustflag: 1" in out and "Threads: 3" in out
+    assert "K2: 1\nK4: 0\nFocal length: 1" in out
+    assert f"Cameras: {blk.n_images}  Points: {blk.n_points} Observations {nobs}" in out
+    assert f"Unknowns {unk}  Redundancy {2 * nobs - unk}" in out
+    assert "no CUDA device" in r.stderr
+    assert r.returncode == 2
+
+
+@pytest.mark.parametrize("missing", ["InputDir", "Robust", "k24out", "Threads"])
+def test_missing_key(workdir, missing):
+    d, _ = workdir
+    _params(d / "parameters", **{missing: None})
+    r = _run(d)
+    assert r.returncode == 1
+    assert f"parameters: missing key {missing}" in r.stderr
+
+
+def test_no_parameters_file_and_extra_argument(workdir):
+    d, _ = workdir
+    r = _run(d)
+    assert r.returncode == 1 and 'cannot read file "parameters"' in r.stderr
+    _params(d / "parameters")
+    r = _run(d, ["x"])
+    assert r.returncode == 1 and "Parameter file not used" in r.stdout
