@@ -2321,6 +2321,17 @@ extern "C" int32_t oracle_calc_plsa_parallel(rpba_block *blk, const rpba_options
     }
     const auto sr = sweep(robustflagit ? 2 : 0, iter == 1, true, nullptr);
     sig0g = sr.first / (double)(sr.second - nrparimages);
+    {
+      // the progress line (rpbacore.cpp:377-389; ihw2 = 1 for unit image sizes)
+      long long nrobs = 0;
+      for (int p = 0; p < pxs; ++p) nrobs += (long long)pointXXv[p].size();
+      nrobs *= 2;
+      const float ihw2 = 1.f;
+      os += "IT: " + std::to_string(iter) + " " + std::to_string(iflag) + "  " + fmt_g(std::sqrt(sig0g * ihw2)) + ' ' +
+            fmt_g(sig0opt / sig0g) + "  " + fmt_g(sig0g) + " " + std::to_string(sr.second) + " " +
+            std::to_string(nrobs) + " " + std::to_string(nrparimages) + " " + std::to_string(nraddp) + "  " +
+            std::to_string(sr.second - nrparimages) + "\n";
+    }
     if (sig0g <= sig0opt) {
       XXdold = XXd;
       PMdold = PMd;

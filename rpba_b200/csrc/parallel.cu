@@ -27,7 +27,9 @@
 // the CalcLSAXMulti kernel), rpba_calc_plsa_parallel_hosted takes them from
 // the caller, so that the loop itself can be checked without a GPU.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -43,6 +45,12 @@ struct PObs {
 struct PCam {
   float K[9], d[2];
 };
+
+std::string fmt_g(double v) {
+  char b[64];
+  std::snprintf(b, sizeof b, "%g", v);
+  return b;
+}
 
 // a block over given cameras and point lists (views into its own vectors)
 struct TmpBlock {
@@ -326,6 +334,17 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
     }
     if (!sweep(robustflagit ? 2 : 0, iter == 1, true, nullptr, &sum, &redundancy)) return status;
     sig0g = sum / (double)(redundancy - nrparimages);
+    {
+      // the progress line (rpbacore.cpp:377-389; ihw2 = 1 for unit image sizes)
+      long long nrobs = 0;
+      for (int p = 0; p < pxs; ++p) nrobs += (long long)pointXXv[p].size();
+      nrobs *= 2;
+      const float ihw2 = 1.f;
+      os += "IT: " + std::to_string(iter) + " " + std::to_string(iflag) + "  " + fmt_g(std::sqrt(sig0g * ihw2)) + ' ' +
+            fmt_g(sig0opt / sig0g) + "  " + fmt_g(sig0g) + " " + std::to_string(redundancy) + " " +
+            std::to_string(nrobs) + " " + std::to_string(nrparimages) + " " + std::to_string(nraddp) + "  " +
+            std::to_string(redundancy - nrparimages) + "\n";
+    }
     if (sig0g <= sig0opt) {
       XXdold = XXd;
       PMdold = PMd;

@@ -1303,6 +1303,11 @@ def _plsa_parallel_restated(oracle_mod, blk, part, T, opts):
                 sig0wv[i] = 0 if not vv[i] else f32(1) / (sorted(vv[i])[len(vv[i]) // 2] * f32(2.1981))
         a, r = sweep(2 if robustflagit else 0, it_ == 1, True, None)
         sig0g = a / float(r - nrparimages)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            ratio = np.float64(sig0opt) / np.float64(sig0g)
+        nrobs = 2 * sum(len(v) for v in pointXXv)
+        log += (f"IT: {it_} {iflag}  {'%g' % np.sqrt(np.float64(sig0g))} {'%g' % ratio}  {'%g' % sig0g} {r} "
+                f"{nrobs} {nrparimages} {nraddp}  {r - nrparimages}\n")
         if sig0g <= sig0opt:
             best = (XXd.copy(), PMd.copy(), [list(v) for v in pointXXv], list(camerasnew))
         camerasoit = [list(camerasnew) for _ in range(T)]
