@@ -76,3 +76,27 @@ def test_no_parameters_file_and_extra_argument(workdir):
     _params(d / "parameters")
     r = _run(d, ["x"])
     assert r.returncode == 1 and "Parameter file not used" in r.stdout
+
+
+def test_partitioned_branch_header(tmp_path, oracle_mod):
+    """Partitioned=1 takes the reference's parallel branch where its rule
+    does (min(Threads, iround(images / 70)) > 1): the '#threads' line and one
+    'Thread:' line per partition, then the device is needed."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present: the solve would run")
+    import rpba_b200 as rb
+    from rpba_b200 import scenes
+    blk = scenes.to_block(scenes.arc_scene(seed=2, n_cams=150, n_pts=600))
+    (tmp_path / "data").mkdir()
+    rb.OutputBlock(str(tmp_path / "data" / "scene.txt"), blk, k24out=True)
+    _params(tmp_path / "parameters", Threads="4", Partitioned="1")
+    r = _run(tmp_path)
+    assert "#threads: 2 2" in r.stdout
+    lines = [l for l in r.stdout.splitlines() if l.startswith("Thread: ")]
+    assert len(lines) == 2 and sum(int(l.split()[3]) for l in lines) == blk.n_images
+    assert "no CUDA device" in r.stderr and r.returncode == 2
+    # the global branch below the rule's threshold: no partition lines
+    _params(tmp_path / "parameters", Threads="1", Partitioned="1")
+    r = _run(tmp_path)
+    assert "#threads" not in r.stdout and r.returncode == 2
