@@ -142,10 +142,11 @@ typedef struct rpba_report {
 
 typedef struct rpba_handle rpba_handle;
 
-/* Human-readable name of a status code. */
+/* Human-readable name of a status code (the reference reports its errors
+ * as "BA-Error: ..." lines instead, rbacore.cpp:415-424, 470-476, 541-548). */
 const char *rpba_status_string(int32_t status);
 
-/* Version string of the library build. */
+/* Version string of the library build (no counterpart in the reference). */
 const char *rpba_version(void);
 
 /* InputBlock (rpba.cpp:180-284): parse a BAL text file into a block whose
@@ -153,6 +154,8 @@ const char *rpba_version(void);
  * float quantisation, sign flip of the observations and k24out scaling. */
 int32_t rpba_input_block(const char *path, int32_t nraddpar, int32_t k24out,
                          rpba_block *out);
+/* Frees the arrays rpba_input_block allocated (no counterpart in the
+ * reference, whose block lives in std::vector and Eigen members). */
 void rpba_block_free(rpba_block *blk);
 
 /* OutputBlock (rpba.cpp:288-338): write a block as BAL text. The per-point
@@ -166,13 +169,19 @@ int32_t rpba_output_block(const char *path, rpba_block *blk, int32_t k24out);
 int32_t rpba_calc_plsa(rpba_block *blk, const rpba_options *opt, char *log,
                        size_t log_cap, rpba_report *rep);
 
-/* Handle API: upload once, solve many times from the uploaded state. */
+/* Handle API: upload once, solve many times from the uploaded state.  The
+ * global branch of CalcPLSA in steps (rpbacore.cpp:514-527): rpba_create is
+ * `new LSA(...)` (the constructor with PointXXvIn and PrepareCameras,
+ * rbacore.cpp:37-125, 670-700, 1918-1974), the problem copied to the GPU. */
 int32_t rpba_create(rpba_handle **h, const rpba_block *blk,
                     const rpba_options *opt);
+/* LSA::Adjust (rbacore.cpp:333-616) from the uploaded state. */
 int32_t rpba_solve(rpba_handle *h, rpba_report *rep);
-/* Copy the adjusted state into blk (pmat, K, distpara, XX, track lists). */
+/* Copy the adjusted state into blk (pmat, K, distpara, XX, track lists):
+ * OutputLSAc with PointXXvOut (rbacore.cpp:644-666, 1978-2010). */
 int32_t rpba_get_state(rpba_handle *h, rpba_block *blk);
-/* Copy the log of the last solve (NUL terminated, truncated to cap). */
+/* Copy the log of the last solve (NUL terminated, truncated to cap): what
+ * Adjust writes to CalcPLSA's ostream (rpbacore.cpp:28-39). */
 int32_t rpba_get_log(rpba_handle *h, char *log, size_t cap);
 /* Per-observation back-projection errors of the uploaded block, in track
  * order (dx, dy as double), as EvalLSA/CalcCorrPointMulti compute them
@@ -304,6 +313,7 @@ typedef struct rpba_tri_options {
   int32_t weight_only;  /* weightonlyflag                                   */
   int32_t device;
 } rpba_tri_options;
+/* CalcLSAXMulti (rpbacore.cpp:536-773) for every point, as described above. */
 int32_t rpba_triangulate(const rpba_block *blk, const float *sig0w, const rpba_tri_options *opt, double *XX_out,
                          uint8_t *keep, float *sig0v, uint8_t *conv, double *sig0io, int64_t *redundancy);
 
@@ -369,7 +379,8 @@ typedef int32_t (*rpba_merge_fn)(const rpba_block *b, const double *Pd, const fl
                                  double *XX_out, uint8_t *keep, float *sig0v, uint8_t *conv, float *w3d,
                                  double *s0_pt, int32_t *red_pt);
 /* rpba_calc_plsa_parallel's loop with both steps supplied by the caller
- * (the host-side check of the loop binds CPU implementations of them). */
+ * (the host-side check of the loop binds CPU implementations of them); no
+ * counterpart in the reference. */
 int32_t rpba_calc_plsa_parallel_hosted(rpba_block *blk, const rpba_options *opt, int32_t nthreads,
                                        const int32_t *part, char *log, size_t cap, double *stats,
                                        rpba_gcp_step_fn step, rpba_merge_fn merge);
@@ -400,6 +411,7 @@ typedef struct rpba_batch_report {
   int32_t workers;           /* scenes solved concurrently                    */
   int32_t failed;            /* scenes whose status is not RPBA_OK            */
 } rpba_batch_report;
+/* The batched form described above (no counterpart in the reference). */
 int32_t rpba_solve_batch(rpba_block *blocks, int32_t n, const rpba_options *opt, int32_t workers,
                          rpba_report *reports, int32_t *status, rpba_batch_report *br);
 
@@ -408,6 +420,8 @@ int32_t rpba_solve_batch(rpba_block *blocks, int32_t n, const rpba_options *opt,
  * created with rpba_options.verbose bit 1 (value 2) set.  No counterpart in
  * the reference (its only instrument is a wall-clock print, rpba.cpp:140). */
 int32_t rpba_kernel_stats(rpba_handle *h, char *json, size_t cap);
+/* Releases a handle and its device memory (`delete LSA1`,
+ * rpbacore.cpp:525). */
 void rpba_destroy(rpba_handle *h);
 
 #ifdef __cplusplus
