@@ -4,12 +4,16 @@ redundancy and an image without observations end with the same status and
 log line; a NaN camera ends with the NaN-step status; a PCG cap that the
 learned solver cannot meet falls back to the block-Jacobi PCG and the
 direct solve and still reaches the plain solver's RMS."""
+import os
+
 import numpy as np
 import pytest
 
 from rpba_b200 import scenes
 
-pytestmark = [pytest.mark.gpu, pytest.mark.skip(reason="first run on a GPU pending")]
+# run with RPBA_RUN_PENDING=1 until their first GPU run has passed
+pytestmark = [pytest.mark.gpu, pytest.mark.skipif(os.environ.get("RPBA_RUN_PENDING") != "1",
+                                                  reason="first run on a GPU pending")]
 
 
 def _pair(oracle_mod, blk, **kw):
