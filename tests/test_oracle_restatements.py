@@ -1372,3 +1372,119 @@ def test_parallel_loop_matches_python_restatement(oracle_mod):
     assert np.array_equal(np.array([c[0] for c in cams]), b_o.K)
     assert np.array_equal(np.cumsum([0] + [len(v) for v in pxv]), b_o.pt_obs_off)
     assert np.array_equal(np.array([q[0] for v in pxv for q in v], np.int32), b_o.pt_obs_image)
+
+
+@pytest.mark.parametrize("addflags", [(True, True, True), (True, False, True)])
+def test_jacobians_match_restatement(oracle_mod, addflags):
+    """CalcDerivatives (rbacore.cpp:1420-1616) with eCalcCalibratedDerivativesX
+    and eCalcCalibratedDerivatives3 (1620-1673) restated from the reference's
+    formulas for every observation: the rotation and projection-centre
+    columns in the camera frame, calibrated through the distortion and K, the
+    additional-parameter columns after it, camera 0's intrinsics alone and
+    the scale camera's two free centre coordinates; the point columns.  To
+    roundoff (1e-13 relative)."""
+    import rpba_b200 as rb
+    L = _wrap(oracle_mod.lib())
+    L.oracle_lsa_create_raw.restype = C.c_void_p
+    L.oracle_lsa_create_raw.argtypes = [C.c_void_p, C.c_void_p]
+    L.oracle_lsa_op.argtypes = [C.c_void_p, C.c_int32, C.c_double, C.c_void_p]
+    L.oracle_lsa_decode.argtypes = [C.c_void_p, C.c_void_p]
+    L.oracle_lsa_normcamera.restype = C.c_int32
+    L.oracle_lsa_normcamera.argtypes = [C.c_void_p]
+    L.oracle_lsa_cameras.restype = C.c_double
+    L.oracle_lsa_cameras.argtypes = [C.c_void_p] * 5
+    blk = scenes.to_block(scenes.arc_scene(seed=8, n_cams=7, n_pts=200))
+    o = rb.make_options(robust=False, k2=addflags[0], k4=addflags[1], f=addflags[2])
+    cb = blk.as_c()
+    h = L.oracle_lsa_create_raw(C.addressof(cb), C.addressof(o))
+    assert h
+    n = blk.n_images
+    out = np.zeros(8)
+    worst = 0.0
+    try:
+        norm = L.oracle_lsa_normcamera(h)
+        L.oracle_lsa_op(h, 0, 0.0, _ptr(out))
+        L.oracle_lsa_op(h, 1, 0.0, _ptr(out))
+        nx, npt, nt = L.oracle_lsa_xm_size(h), L.oracle_lsa_n_points(h), L.oracle_lsa_n_track_obs(h)
+        nrioff = L.oracle_lsa_nrioff(h)
+        toff = np.zeros(npt + 1, np.int32)
+        timg = np.zeros(nt, np.int32)
+        tslot = np.zeros(nt, np.int32)
+        L.oracle_lsa_tracks(h, _ptr(toff), _ptr(timg), _ptr(tslot), None)
+        xm = np.zeros(nx)
+        L.oracle_lsa_get_xm(h, _ptr(xm))
+        xm2 = xm.copy()
+        xm2[:nrioff] += np.random.default_rng(3).normal(0, 1e-3, nrioff)
+        L.oracle_lsa_decode(h, _ptr(xm2))
+        R, PC, K, dd = np.zeros(9 * n), np.zeros(3 * n), np.zeros(9 * n), np.zeros(2 * n)
+        L.oracle_lsa_cameras(h, _ptr(R), _ptr(PC), _ptr(K), _ptr(dd))
+        # the scale camera's free centre coordinates, as EncodeCameras picks them
+        P = blk.pmat.astype(np.float64).reshape(n, 3, 4)
+        Rb = _rectify(P[norm, :, :3])
+        pcb = [Rb[0][i] * P[norm, 0, 3] + Rb[1][i] * P[norm, 1, 3] + Rb[2][i] * P[norm, 2, 3] for i in range(3)]
+        maxv, maxi = np.float32(0), 0
+        for i in range(3):
+            if abs(pcb[i]) > float(maxv):
+                maxv, maxi = np.float32(abs(pcb[i])), i
+        esvm = [i for i in range(3) if i != maxi]
+        for p in range(npt):
+            X = xm[nrioff + 3 * p:nrioff + 3 * p + 3]
+            for t in range(toff[p], toff[p + 1]):
+                k = int(timg[t])
+                Bc = np.zeros(18)
+                Bp = np.zeros(6)
+                nc, co = C.c_int(), C.c_int()
+                L.oracle_lsa_jacobian(h, t, _ptr(Bc), C.byref(nc), C.byref(co), _ptr(Bp))
+                Rk = R[9 * k:9 * k + 9].reshape(3, 3)
+                v = X + PC[3 * k:3 * k + 3]
+                e = [(Rk[r, 0] * v[0] + Rk[r, 1] * v[1]) + Rk[r, 2] * v[2] for r in range(3)]
+                xs3 = e[2]
+                xs3 = (-1e3 if xs3 < 0 else 1e3) if abs(xs3) < 1e-3 else 1.0 / xs3
+                xh, yh = e[0] * xs3, e[1] * xs3
+                x1, x2 = xh * xs3, yh * xs3
+                xs31 = 1.0 / xs3
+                xs32 = xs31 * xs31
+                k2, k4 = dd[2 * k], dd[2 * k + 1]
+                K00, K01, K11 = K[9 * k], K[9 * k + 1], K[9 * k + 4]
+                xy2 = xh * xh + yh * yh
+                xy4 = xy2 * xy2
+                xxpc = k4 * xy4 + xh * (2 * k2 * xh + 4 * k4 * xh * xy2) + k2 * xy2 + 1.0
+                xypc = xh * (4 * k4 * xy2 * yh + 2 * k2 * yh)
+                yxpc = (4 * k4 * xh * xy2 + 2 * k2 * xh) * yh
+                yypc = yh * (2 * k2 * yh + 4 * k4 * xy2 * yh) + k4 * xy4 + k2 * xy2 + 1.0
+
+                def calib(col):
+                    xp = xxpc * col[0] + xypc * col[1]
+                    yp = yypc * col[1] + yxpc * col[0]
+                    return [xp * K00 + yp * K01, yp * K11]
+
+                pc = lambda j: [-Rk[0, j] * xs3 + Rk[2, j] * x1, -Rk[1, j] * xs3 + Rk[2, j] * x2]
+                rot = [[x2 * x1 * xs32, 1.0 + x2 * x2 * xs32], [-1.0 - x1 * x1 * xs32, -x2 * x1 * xs32],
+                       [x2 * xs31, -x1 * xs31]]
+                dist = xh * xh + yh * yh
+                zz = 1.0 + (k2 * dist + k4 * dist * dist)
+                add = []
+                if addflags[0]:
+                    add.append([-xh * xy2 * K00 - yh * xy2 * K01, -yh * xy2 * K11])
+                if addflags[1]:
+                    add.append([-xh * xy4 * K00 - yh * xy4 * K01, -yh * xy4 * K11])
+                if addflags[2]:
+                    add.append([-(xh * zz), -(yh * zz)])
+                point = [calib(pc(j)) for j in range(3)]
+                if k == 0:
+                    cols = add
+                elif k == norm:
+                    cols = [calib(c) for c in rot + [pc(esvm[0]), pc(esvm[1])]] + add
+                else:
+                    cols = [calib(c) for c in rot + [pc(0), pc(1), pc(2)]] + add
+                want_c = np.array(cols).T if cols else np.zeros((2, 0))
+                got_c = Bc.reshape(2, 9)[:, :nc.value]
+                assert got_c.shape == want_c.shape, (k, got_c.shape, want_c.shape)
+                want_p = np.array(point).T
+                for got, want in ((got_c, want_c), (Bp.reshape(2, 3), want_p)):
+                    if want.size:
+                        worst = max(worst, float(np.abs(got - want).max() / (np.abs(want).max() + 1e-300)))
+    finally:
+        L.oracle_lsa_destroy(h)
+    print(f"addflags {addflags}: worst relative difference {worst:.2e}")
+    assert worst < 1e-13
