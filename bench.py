@@ -68,6 +68,10 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-scale", type=float, default=0.01,
                     help="scale of the scene the CPU baseline solves (bounded sample)")
+    ap.add_argument("--ref-sample-scale", type=float, default=0.04,
+                    help="scale of the scene one step of --impl reference solves (bounded sample)")
+    ap.add_argument("--seed-offset", type=int, default=0, help="generator seed offset (another scene)")
+    ap.add_argument("--no-ablation", action="store_true", help="skip the preconditioner ablation solves")
     ap.add_argument("--e2e-steps", type=int, default=1)
     return ap.parse_args()
 
@@ -203,21 +207,63 @@ def cpu_sample_parallel(blk, out_global):
     """The reference's partitioned branch (Threads=0: min(host cores,
     iround(images / 70)) partitions, rpbacore.cpp:79-92, 100-510) as restated
     by the oracle, on the same sample, partition included in the time;
-    None when that sample takes the global branch."""
+    None when that sample takes the global branch.  The partition (the
+    stand-in for METIS) is the copy compiled into the oracle's library, so
+    this leg loads no GPU code."""
     import oracle
-    import rpba_b200 as rb
     threads = oracle.parallel_threads(blk.n_images, os.cpu_count() or 1)
     if threads < 2 or blk.n_images <= 5:
         return None
     t0 = time.perf_counter()
-    part = rb.partition_images(blk, threads)
+    part = oracle.partition_images(blk, threads)
     st, out, stats, _ = oracle.calc_plsa_parallel(blk, part, threads)
     dt = time.perf_counter() - t0
     ev = lambda b: oracle.exteval(b)[1]["exteval_sigma0"]
     return {"value": dt, "unit": UNIT, "cores": threads, "partitions": threads, "status": st,
             "outer_iterations": stats["iterations"], "exteval_sigma0": ev(out),
-            "global_exteval_sigma0": ev(out_global),
+            "global_exteval_sigma0": ev(out_global) if out_global is not None else None,
             "note": "Threads=0 branch of the reference: partition, per-partition GCP steps, CalcLSAXMulti merge"}
+
+
+def rooflines(kstats, hbm, peak_kind):
+    """Per-kernel device time share, achieved GB/s of its algorithmic bytes
+    (counted per launch by the library) and fraction of the HBM peak, for
+    every kernel at 3% of the solve or more; and the roofline object of the
+    dominant one.  For the PCG also the fraction on the minimal bytes: each
+    block of the reduced camera system read once with its entry, without the
+    transposed products' round trip (80 B per off-diagonal block)."""
+    rcs = kstats.pop("_rcs", None)
+    total_ms = sum(v["ms"] for v in kstats.values()) or 1.0
+    kernels = {}
+    for k, v in sorted(kstats.items(), key=lambda kv: -kv[1]["ms"]):
+        d = {"share": round(v["ms"] / total_ms, 4), "launches": v["launches"],
+             "avg_ms": v["ms"] / max(v["launches"], 1)}
+        if v.get("bytes", 0) > 0 and v["ms"] > 0 and d["share"] >= 0.03:
+            ach = v["bytes"] / (v["ms"] * 1e-3) / 1e9
+            d.update({"achieved_gbs": ach, "frac": ach / hbm, "algorithmic_bytes": v["bytes"] / v["launches"]})
+        kernels[k] = d
+    timed_k = {k: v for k, v in kstats.items() if v.get("bytes", 0) > 0}
+    dom = max(timed_k, key=lambda k: timed_k[k]["ms"]) if timed_k else None
+    if not dom:
+        return None, kernels
+    d = timed_k[dom]
+    avg_s = d["ms"] * 1e-3 / d["launches"]
+    alg = d["bytes"] / d["launches"]
+    ach = alg / avg_s / 1e9
+    ratio, src = traffic_ratio() if dom == "pcg" else (None, None)
+    roofline = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                "traffic": alg * ratio if ratio else None,
+                "traffic_note": (f"ncu DRAM bytes / algorithmic bytes = {ratio:.3f} from {src}, scaled to "
+                                 "this launch's algorithmic bytes") if ratio else None,
+                "algorithmic_bytes_per_launch": alg, "avg_launch_ms": d["ms"] / d["launches"]}
+    if dom == "pcg" and rcs and rcs.get("fp32"):
+        nb = rcs["offdiag_blocks"]
+        full_it = 332.0 * (rcs["rows"] + nb) + 80.0 * nb + rcs["rows"] * (648.0 + 22 * 72.0 + 2 * 720.0 + 2 * 72.0)
+        minimal = alg * (full_it - 80.0 * nb) / full_it
+        roofline["frac_minimal_bytes"] = minimal / avg_s / 1e9 / hbm
+        roofline["minimal_bytes_note"] = "each block read once with its entry, no transposed-product round trip"
+    return roofline, kernels
 
 
 def config_dict(args, blk=None):
@@ -232,31 +278,77 @@ def config_dict(args, blk=None):
 
 
 def run_reference(args):
+    """The reference's CPU path on the host cores: its default branch for
+    this workload (Threads=0, the partitioned RPBA with min(cores,
+    iround(images / 70)) partitions on OpenMP threads, restated by the
+    oracle) on a bounded sample of the workload per step -- a scene of the
+    same family at --ref-sample-scale of its size -- with the value scaled
+    to the full workload by observation count.  The cost of the reference's
+    solve grows faster than its observation count (more PCG iterations,
+    larger partitions), so the scaled value is a lower bound of its
+    full-workload time.  Beside it, once, the single-threaded global LSA
+    (Threads=1, the algorithm the plain GPU form reproduces) on the
+    --cpu-sample-scale sample, scaled the same way."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    times, rep, st, blk = [], None, 0, None
+    import oracle
+    import rpba_b200 as rb  # the options container only: no GPU library is loaded
+    full = make_block(args.config, args.scale, args.seed_offset)  # the workload itself: its size and config
+    cfg, n_full = config_dict(args, full), full.n_obs
+    del full
+    sblk = make_block(args.config, args.ref_sample_scale, args.seed_offset)
+    threads = oracle.parallel_threads(sblk.n_images, os.cpu_count() or 1)
+    times, par = [], None
     for i in range(args.warmup + args.steps):
-        dt, rep, st, blk, out = cpu_sample(args.config, args.cpu_sample_scale)
+        par = cpu_sample_parallel(sblk, None)
+        if par is None:  # too small for the partitioned branch: the global LSA is the reference's path
+            t0 = time.perf_counter()
+            oracle.calc_plsa(sblk, rb.make_options(solver=rb.SOLVER_PCG))
+            dt = time.perf_counter() - t0
+        else:
+            dt = par["value"]
         if i >= args.warmup:
             times.append(dt)
-    v = statistics.median(times)
-    par = cpu_sample_parallel(blk, out)
-    sample = (f"one complete solve (reference stop rule) of the same scene family at "
-              f"{args.cpu_sample_scale:g} of the workload: {blk.n_images} cameras, {blk.n_points} points, "
-              f"{blk.n_obs} observations; one thread (the reference's global LSA is single-threaded)")
+    t_sample = statistics.median(times)
+    factor = n_full / sblk.n_obs
+    v = t_sample * factor
+    g_dt, g_rep, g_st, gblk, _ = cpu_sample(args.config, args.cpu_sample_scale)
+    sample = (f"per step one complete solve of a scene of the same family at {args.ref_sample_scale:g} of the "
+              f"workload ({sblk.n_images} cameras, {sblk.n_points} points, {sblk.n_obs} observations) by the "
+              f"reference's Threads=0 branch on {threads if par else 1} host threads; value = median step time "
+              f"x {factor:.1f} (full-workload observations / sample observations), a lower bound of the "
+              f"full-workload time")
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": dict(config_dict(args), sample=sample),
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample,
-                         "linear_solves": rep["linear_solves"], "final_rms": rep["rms"], "status": st,
-                         "parallel": par},
+        "config": cfg,
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads if par else 1, "kind": "port",
+                         "sample": sample, "sample_seconds": t_sample, "scale_factor": factor,
+                         "step_times": times, "partitioned": par,
+                         "global_lsa": {"value": g_dt * n_full / gblk.n_obs, "sample_seconds": g_dt, "cores": 1,
+                                        "sample": (f"one complete solve at {args.cpu_sample_scale:g} of the "
+                                                   f"workload ({gblk.n_images} cameras, {gblk.n_obs} "
+                                                   "observations), one thread, scaled by observation count"),
+                                        "linear_solves": g_rep["linear_solves"], "final_rms": g_rep["rms"],
+                                        "status": g_st}},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "loaded_repo_libraries": repo_libraries(),
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def repo_libraries():
+    """Shared libraries of this repository mapped into the process (the
+    reference arm must run the oracle's alone)."""
+    try:
+        with open("/proc/self/maps") as fh:
+            paths = {ln.split()[-1] for ln in fh if ln.rstrip().endswith(".so")}
+    except OSError:
+        return None
+    return sorted(os.path.relpath(p, ROOT) for p in paths if p.startswith(ROOT + os.sep))
 
 
 def main():
@@ -275,7 +367,7 @@ def main():
     g = Group(rank, world, "nccl", 600.0, device=torch.device("cuda", local))
     barrier, max_over_ranks = g.barrier, g.max
 
-    blk = make_block(args.config, args.scale)
+    blk = make_block(args.config, args.scale, args.seed_offset)
     w = learned_weights()
     prec = rb.PREC_MIXED if args.precision == "mixed" else rb.PREC_FP64
     ours_kw = dict(solver=rb.SOLVER_LEARNED, precision=prec, pcg_tolerance=args.tol, device=local)
@@ -345,37 +437,56 @@ def main():
     kstats = P.kernel_stats()
     P.close()
     hbm, peak_kind = peaks()
-    timed_k = {k: v for k, v in kstats.items() if v.get("bytes", 0) > 0}
-    dom = max(timed_k, key=lambda k: timed_k[k]["ms"]) if timed_k else None
-    roofline = None
-    if dom:
-        d = timed_k[dom]
-        avg_s = d["ms"] * 1e-3 / d["launches"]
-        alg = d["bytes"] / d["launches"]
-        ach = alg / avg_s / 1e9
-        ratio, src = traffic_ratio() if dom == "pcg" else (None, None)
-        roofline = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s",
-                    "frac": ach / hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-                    "traffic": alg * ratio if ratio else None,
-                    "traffic_note": (f"ncu DRAM bytes / algorithmic bytes = {ratio:.3f} from {src}, scaled to "
-                                     "this launch's algorithmic bytes") if ratio else None,
-                    "algorithmic_bytes_per_launch": alg, "avg_launch_ms": d["ms"] / d["launches"]}
-    total_ms = sum(v["ms"] for v in kstats.values())
-    kernel_share = {k: round(v["ms"] / total_ms, 4) for k, v in sorted(kstats.items(), key=lambda kv: -kv[1]["ms"])}
+    roofline, kernels = rooflines(kstats, hbm, peak_kind)
+    kernel_share = {k: v["share"] for k, v in kernels.items()}
+
+    # what each part of the preconditioner buys: the same learned solver
+    # without the network (block-Jacobi part plus the coarse space), and
+    # without the coarse space (network only), one solve each, same tolerance
+    ablation = None
+    if not args.no_ablation:
+        ablation = {}
+        for name, kw, wt in (("no_network", ours_kw, None),
+                             ("no_coarse_space", dict(ours_kw, coarse_aggregates=-1), w)):
+            S = rb.Solver(blk, **kw)
+            S.set_preconditioner(wt)
+            flush.zero_()
+            torch.cuda.synchronize()
+            _, ra = S.solve()
+            S.close()
+            ablation[name] = {"value": ra["solve_seconds"], "unit": UNIT, "pcg_iterations": ra["pcg_iterations"],
+                              "linear_solves": ra["linear_solves"], "pcg_fallbacks": ra["pcg_fallbacks"],
+                              "final_rms": ra["rms"]}
+        ablation["with_both"] = {"value": value, "pcg_iterations": reps[-1]["pcg_iterations"],
+                                 "final_rms": reps[-1]["rms"]}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         dt, rep_c, st_c, sblk, sout = cpu_sample(args.config, args.cpu_sample_scale)
+        same = {}
+        for name, kw, wt in (("ours", ours_kw, w), ("plain_fp64", plain_kw, None)):
+            S = rb.Solver(sblk, **kw)
+            S.set_preconditioner(wt)
+            S.solve()
+            _, rep_g = S.solve()
+            S.close()
+            same[name] = rep_g["solve_seconds"]
+        # end to end through the C ABI from host buffers, as the e2e value
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
         S = rb.Solver(sblk, **ours_kw)
         S.set_preconditioner(w)
         S.solve()
-        _, rep_g = S.solve()
+        S.state()
         S.close()
+        torch.cuda.synchronize()
+        same["ours_e2e"] = time.perf_counter() - t0
         cpu = {"value": dt, "unit": UNIT, "cores": 1, "kind": "port",
                "sample": (f"one complete solve of the same scene family at {args.cpu_sample_scale:g} of the "
                           f"workload ({sblk.n_images} cameras, {sblk.n_obs} observations) on one host core"),
                "linear_solves": rep_c["linear_solves"], "final_rms": rep_c["rms"],
-               "gpu_same_sample_s": rep_g["solve_seconds"], "parallel": cpu_sample_parallel(sblk, sout)}
+               "gpu_same_sample_s": same["ours"], "gpu_plain_fp64_same_sample_s": same["plain_fp64"],
+               "gpu_e2e_same_sample_s": same["ours_e2e"], "parallel": cpu_sample_parallel(sblk, sout)}
 
     if rank == 0:
         r0 = reps[-1]
@@ -395,6 +506,8 @@ def main():
                       "pcg_fallbacks": r0["pcg_fallbacks"], "final_rms": r0["rms"], "final_cost": r0["cost"],
                       "obs_deleted": r0["obs_deleted"], "step_times": times},
             "kernel_share": kernel_share,
+            "kernels": kernels,
+            "ablation": ablation,
         }
         print(json.dumps(line), flush=True)
     g.close()

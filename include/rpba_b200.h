@@ -287,13 +287,18 @@ int32_t rpba_precond_loss_grad(const rpba_precond_set *set, const float *weights
  * the work is enqueued on `stream` (a cudaStream_t; NULL = legacy default
  * stream) and the call returns without waiting for it.  Scratch lives in one
  * static device array of the library (about 20 KB, held by every GPU that
- * loads the library until the process exits), which caps n at 4,194,304
- * (512 CTAs x 8192 elements): larger n returns RPBA_ERR_TOO_LARGE.  The first
- * call on a device looks up that array's device address (a blocking runtime
- * query), so make the first call on each device before any stream capture.
- * All calls share the one array: calls that overlap on the GPU (different
- * streams, or different host threads, on the same device) race and must be
- * serialised by the caller.  No counterpart in the reference. */
+ * loads the library until the process exits), which caps n at 4,194,304 on
+ * every device: larger n returns RPBA_ERR_TOO_LARGE.  The first call on a
+ * device (and the first after cudaDeviceReset or with another context
+ * current) looks up that array's device address (a blocking runtime query),
+ * so make the first call on each device before any stream capture.
+ * The call first sets *d_out to NaN; the kernel overwrites it with the sum.
+ * A NaN left in *d_out after the stream has run means the call failed on the
+ * device (a bounded grid-barrier wait ran out); a valid sum of finite inputs
+ * >= 0 is never NaN.  All calls share the one array: calls that overlap on
+ * the GPU (different streams, or different host threads, on the same
+ * device) race and must be serialised by the caller.  No counterpart in the
+ * reference. */
 int32_t rpba_float_sequential_sum_noalloc(const float *d_v, int64_t n, float *d_out, void *stream);
 
 /* Per-point refinement against fixed cameras: CalcLSAXMulti
@@ -420,6 +425,15 @@ int32_t rpba_solve_batch(rpba_block *blocks, int32_t n, const rpba_options *opt,
  * created with rpba_options.verbose bit 1 (value 2) set.  No counterpart in
  * the reference (its only instrument is a wall-clock print, rpba.cpp:140). */
 int32_t rpba_kernel_stats(rpba_handle *h, char *json, size_t cap);
+/* Test hook of the bounded device waits.  With extra_ctas = 1 every grid
+ * barrier of the handle's persistent PCG waits for one CTA more than the
+ * launch has -- an arrival that never comes -- for at most timeout_ns
+ * (1 ms .. 2 s), so the wait runs out, the kernel sets the error word and
+ * returns, and the solve ends with RPBA_ERR_DEVICE_TIMEOUT; the handle stays
+ * usable.  (0, 0) restores normal operation (the default 2 s limit).  The
+ * reference has no device waits and no counterpart; its error exits are
+ * the BA-Error lines of rbacore.cpp:415-424, 470-476 and 541-546. */
+int32_t rpba_debug_barrier_timeout(rpba_handle *h, int32_t extra_ctas, int64_t timeout_ns);
 /* Releases a handle and its device memory (`delete LSA1`,
  * rpbacore.cpp:525). */
 void rpba_destroy(rpba_handle *h);

@@ -201,6 +201,22 @@ def parallel_threads(n_images: int, threads: int) -> int:
     return int(min(threads, int(q + 0.5)))
 
 
+def partition_images(block: Block, nparts: int) -> np.ndarray:
+    """The camera partition that stands in for METIS (PartitionpointXXv,
+    rpbacore.cpp:945-1037): the library's own bisection, compiled into this
+    library (oracle_partition_images) so that the CPU baseline loads no GPU
+    code.  Part (0 .. nparts - 1) of every image."""
+    part = np.zeros(block.n_images, np.int32)
+    cb = block.as_c()
+    f = lib().oracle_partition_images
+    f.restype = C.c_int32
+    f.argtypes = [C.POINTER(RpbaBlockC), C.c_int32, C.POINTER(C.c_int32)]
+    st = f(C.byref(cb), int(nparts), part.ctypes.data_as(C.POINTER(C.c_int32)))
+    if st != 0:
+        raise RuntimeError(f"oracle_partition_images: status {st}")
+    return part
+
+
 def calc_plsa_parallel(block: Block, part, nthreads: int, opts: RpbaOptionsC | None = None,
                        log_cap: int = 1 << 20):
     """The parallel RPBA (the partitioned branch of CalcPLSA,

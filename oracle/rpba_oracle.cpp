@@ -1220,57 +1220,75 @@ void LSA::sparse_pcg() {
 }
 
 /* Dense Cholesky of the reduced camera system (the --direct oracle mode
- * the GPU's direct form is compared with). */
+ * the GPU's direct form is compared with): the textbook row-by-row
+ * Cholesky-Crout factorisation L L^T of the symmetrised matrix, then the
+ * forward and back substitutions, every sum taken in increasing index order.
+ * The matrix is held in its envelope (row r from the first column any of its
+ * camera's blocks reaches): L has the same envelope, every entry left of it
+ * is an exact zero, and the terms the dense loops would add for those
+ * columns are exact zeros, so skipping them changes no value -- the result
+ * is that of the dense loops at a fraction of the work on chain- and
+ * grid-like scenes. */
 void LSA::direct_solve() {
   const int nb = nimg;
   std::vector<int> off(nb + 1, 0);
   for (int i = 0; i < nb; ++i) off[i + 1] = off[i] + (i >= begini ? cam_np(i) : 0);
   const int n = off[nb];
-  std::vector<double> A((size_t)n * n, 0.), y(n);
+  /* first column of every scalar row, and the row starts of the envelope */
+  std::vector<int> fc(n);
+  for (int i = begini; i < nb; ++i) {
+    int f = off[i];
+    for (auto &kv : Off[i]) f = std::min(f, off[kv.first]);
+    for (int a = 0; a < cam_np(i); ++a) fc[off[i] + a] = f;
+  }
+  std::vector<size_t> rs(n + 1, 0);
+  for (int r = 0; r < n; ++r) rs[r + 1] = rs[r] + (size_t)(r - fc[r] + 1);
+  std::vector<double> L(rs[n], 0.), y(n);
+  auto at = [&](int r, int c) -> double & { return L[rs[r] + (size_t)(c - fc[r])]; };
   for (int i = begini; i < nb; ++i) {
     const int ni = cam_np(i);
+    /* symmetrised diagonal block (the assembled blocks are symmetric to
+     * roundoff); the off-diagonal blocks enter both triangles with the same
+     * value, whose symmetrised mean is itself */
     for (int a = 0; a < ni; ++a)
-      for (int c = 0; c < ni; ++c) A[(size_t)(off[i] + a) * n + off[i] + c] = Dg[i][a * ni + c];
+      for (int c = 0; c <= a; ++c)
+        at(off[i] + a, off[i] + c) = c == a ? Dg[i][a * ni + a] : 0.5 * (Dg[i][a * ni + c] + Dg[i][c * ni + a]);
     for (auto &kv : Off[i]) {
       const int row = kv.first, nr = cam_np(row);
       for (int a = 0; a < nr; ++a)
         for (int c = 0; c < ni; ++c) {
-          A[(size_t)(off[row] + a) * n + off[i] + c] = kv.second[a * ni + c];
-          A[(size_t)(off[i] + c) * n + off[row] + a] = kv.second[a * ni + c];
+          const double v = kv.second[a * ni + c];
+          at(off[i] + c, off[row] + a) = 0.5 * (v + v);
         }
     }
     for (int a = 0; a < ni; ++a) y[off[i] + a] = rhs[i][a];
   }
-  /* symmetrise (the assembled diagonal blocks are symmetric to roundoff) */
-  for (int i = 0; i < n; ++i)
-    for (int j = 0; j < i; ++j) {
-      const double s = 0.5 * (A[(size_t)i * n + j] + A[(size_t)j * n + i]);
-      A[(size_t)i * n + j] = A[(size_t)j * n + i] = s;
-    }
   for (int j = 0; j < n; ++j) {
-    double s = A[(size_t)j * n + j];
-    for (int k = 0; k < j; ++k) s -= A[(size_t)j * n + k] * A[(size_t)j * n + k];
+    double s = at(j, j);
+    for (int k = fc[j]; k < j; ++k) s -= at(j, k) * at(j, k);
     if (!(s > 0.)) {
       status = RPBA_ERR_SOLVER;
       return;
     }
     const double l = std::sqrt(s);
-    A[(size_t)j * n + j] = l;
+    at(j, j) = l;
     for (int i = j + 1; i < n; ++i) {
-      double t = A[(size_t)i * n + j];
-      for (int k = 0; k < j; ++k) t -= A[(size_t)i * n + k] * A[(size_t)j * n + k];
-      A[(size_t)i * n + j] = t / l;
+      if (fc[i] > j) continue;  /* L(i, j) stays an exact zero */
+      double t = at(i, j);
+      for (int k = std::max(fc[i], fc[j]); k < j; ++k) t -= at(i, k) * at(j, k);
+      at(i, j) = t / l;
     }
   }
   for (int i = 0; i < n; ++i) {
     double s = y[i];
-    for (int k = 0; k < i; ++k) s -= A[(size_t)i * n + k] * y[k];
-    y[i] = s / A[(size_t)i * n + i];
+    for (int k = fc[i]; k < i; ++k) s -= at(i, k) * y[k];
+    y[i] = s / at(i, i);
   }
   for (int i = n - 1; i >= 0; --i) {
     double s = y[i];
-    for (int k = i + 1; k < n; ++k) s -= A[(size_t)k * n + i] * y[k];
-    y[i] = s / A[(size_t)i * n + i];
+    for (int k = i + 1; k < n; ++k)
+      if (fc[k] <= i) s -= at(k, i) * y[k];
+    y[i] = s / at(i, i);
   }
   for (int i = begini; i < nb; ++i)
     for (int a = 0; a < cam_np(i); ++a) rhs[i][a] = y[off[i] + a];

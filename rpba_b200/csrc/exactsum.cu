@@ -20,6 +20,8 @@
 //
 // The first HEAD elements and any stretch where s is zero or subnormal are
 // added by one warp in plain sequence.  Inputs must be finite and >= 0.
+#include <cuda.h>
+
 #include <mutex>
 
 #include "../../include/rpba_b200.h"
@@ -336,14 +338,15 @@ void launch_exact_sum(const float *v, int n, float *out, const ExactSumWork &W, 
 // keeps its scratch -- the per-CTA run sums, the run control word and the
 // grid-barrier counters of k_exact_sum -- in one statically sized device
 // array that every GPU loading the library holds until the process exits
-// (about 20 KB).  Its size caps the input at NA_MAX_CTAS CTAs of NA_CHUNK
-// elements each.
+// (about 20 KB).  Its size caps the grid at NA_MAX_CTAS CTAs; inputs up to
+// NA_MAX_N elements are accepted on any device (with fewer resident CTAs,
+// each CTA takes a longer chunk).
 using namespace rpba;
 
 namespace {
 
-constexpr int NA_MAX_CTAS = 512;  // resident on 148 SMs at 4 CTAs per SM
-constexpr int NA_CHUNK = 8192;
+constexpr int NA_MAX_CTAS = 512;
+constexpr int NA_CHUNK = 8192;  // elements per CTA when the grid allows it
 constexpr long long NA_MAX_N = (long long)NA_MAX_CTAS * NA_CHUNK;  // 4,194,304
 constexpr size_t NA_OFF_RC = 0;
 // two entries per CTA (one per incoming parity)
@@ -356,9 +359,43 @@ constexpr size_t NA_BYTES = NA_OFF_ERR + 16;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
 
+// The array's device address belongs to the context the module was loaded
+// in: after cudaDeviceReset (or when the caller makes another context
+// current) it is looked up again.  Contexts are told apart by their
+// process-unique id (cuCtxGetId); the two driver calls are fetched through
+// the runtime, so the library does not link the driver library.
+typedef CUresult (*PfnCtxGetCurrent)(CUcontext *);
+typedef CUresult (*PfnCtxGetId)(CUcontext, unsigned long long *);
+
 constexpr int NA_MAX_DEVICES = 64;
+struct NaSlot {
+  unsigned long long ctx_id;  // 0: not looked up yet
+  unsigned char *addr;        // device address of the scratch in that context
+};
 std::mutex g_na_mutex;
-unsigned char *g_na_addr[NA_MAX_DEVICES];  // device address of the scratch, per device
+NaSlot g_na[NA_MAX_DEVICES];
+PfnCtxGetCurrent g_ctx_current = nullptr;
+PfnCtxGetId g_ctx_id = nullptr;
+
+// Id of the calling thread's current context; 0 when none is current.
+// Call with g_na_mutex held.
+bool current_ctx_id(unsigned long long *id) {
+  if (!g_ctx_current || !g_ctx_id) {
+    void *a = nullptr, *b = nullptr;
+    cudaDriverEntryPointQueryResult qa, qb;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+        qa != cudaDriverEntryPointSuccess || !a ||
+        cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+        qb != cudaDriverEntryPointSuccess || !b)
+      return false;
+    g_ctx_current = (PfnCtxGetCurrent)a;
+    g_ctx_id = (PfnCtxGetId)b;
+  }
+  CUcontext ctx = nullptr;
+  if (g_ctx_current(&ctx) != CUDA_SUCCESS) return false;
+  *id = 0;
+  return !ctx || g_ctx_id(ctx, id) == CUDA_SUCCESS;
+}
 
 }  // namespace
 
@@ -371,27 +408,40 @@ extern "C" int32_t rpba_float_sequential_sum_noalloc(const float *d_v, int64_t n
   cudaStream_t s = (cudaStream_t)stream;
   unsigned char *base;
   {
-    // set-up, once per device, with that device current: the array's name
-    // is only a host-side stand-in, so its device address is looked up
+    // set-up, once per device and context, with that device current: the
+    // array's name is only a host-side stand-in, so its device address is
+    // looked up (the lookup also makes the runtime's context current when
+    // this thread has none yet)
     std::lock_guard<std::mutex> lock(g_na_mutex);
-    if (!g_na_addr[dev]) {
+    unsigned long long id = 0;
+    if (!current_ctx_id(&id)) return RPBA_ERR_CUDA;
+    if (id == 0 || g_na[dev].ctx_id != id) {
       void *p = nullptr;
       if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return RPBA_ERR_CUDA;
-      g_na_addr[dev] = (unsigned char *)p;
+      if (id == 0 && (!current_ctx_id(&id) || id == 0)) return RPBA_ERR_CUDA;
+      g_na[dev].ctx_id = id;
+      g_na[dev].addr = (unsigned char *)p;
     }
-    base = g_na_addr[dev];
+    base = g_na[dev].addr;
   }
   const int ni = (int)n;
+  // until the sum is written, *d_out holds a NaN (all bits set): a grid
+  // barrier that runs out leaves it there
+  if (cudaMemsetAsync(d_out, 0xff, sizeof(float), s) != cudaSuccess) return RPBA_ERR_CUDA;
   if (ni <= 4 * HEAD) {
-    k_warp_sum<<<1, 32, 0, s>>>(d_v, ni, d_out);
-    return cudaGetLastError() == cudaSuccess ? RPBA_OK : RPBA_ERR_CUDA;
+    void *wargs[] = {(void *)&d_v, (void *)&ni, (void *)&d_out};
+    return cudaLaunchKernel((const void *)k_warp_sum, dim3(1), dim3(32), wargs, 0, s) == cudaSuccess ? RPBA_OK
+                                                                                                      : RPBA_ERR_CUDA;
   }
-  const int G = (ni + NA_CHUNK - 1) / NA_CHUNK;
   int nsm = 0, per = 0;
   if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_exact_sum, ES_T, 0) != cudaSuccess)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_exact_sum, ES_T, 0) != cudaSuccess || nsm * per < 1)
     return RPBA_ERR_CUDA;
-  if (G > nsm * per) return RPBA_ERR_TOO_LARGE;  // the CTAs would not all be resident
+  // every CTA must be resident (cooperative launch) and own a slot of the
+  // array: past either limit the CTAs take longer chunks
+  int G = (ni + NA_CHUNK - 1) / NA_CHUNK;
+  if (G > NA_MAX_CTAS) G = NA_MAX_CTAS;
+  if (G > nsm * per) G = nsm * per;
   EsArgs A;
   A.v = d_v;
   A.n = ni;

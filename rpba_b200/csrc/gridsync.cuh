@@ -15,9 +15,10 @@ __device__ __forceinline__ unsigned long long gtimer() {
 
 // Barrier over all CTAs of a cooperative launch (co-residency guaranteed).
 // bar[0] counts arrivals, bar[1] is the generation.  The wait is bounded:
-// after BAR_TIMEOUT_NS it sets err bit 2 and returns false; every caller
-// then leaves the kernel.
-__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned nblocks, int *err) {
+// after timeout_ns (BAR_TIMEOUT_NS unless a caller shortens it) it sets err
+// bit 2 and returns false; every caller then leaves the kernel.
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned nblocks, int *err,
+                                             unsigned long long timeout_ns = BAR_TIMEOUT_NS) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned *vgen = bar + 1;
@@ -32,7 +33,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned nblocks, in
       const unsigned long long t0 = gtimer();
       while (*vgen == gen) {
         if (*(volatile int *)err) break;
-        if (gtimer() - t0 > BAR_TIMEOUT_NS) {
+        if (gtimer() - t0 > timeout_ns) {
           atomicOr(err, 2);
           break;
         }

@@ -69,6 +69,11 @@ struct DevLSA {
   const int2 *rowspan;      // [nimg] (diagonal entry, end entry) of each row
   float *tpart;             // [nboff * 9] FP32 form: transposed block products
   int *err;            // device error word
+  // Test hook of the bounded waits (rpba_debug_barrier_timeout): the PCG's
+  // grid barriers wait for bar_extra CTAs more than the launch has, for at
+  // most bar_timeout_ns (0: the default limit).  Both 0 in normal use.
+  unsigned bar_extra = 0;
+  unsigned long long bar_timeout_ns = 0;
   // GCP mode of the parallel RPBA's per-partition LSA (ao = 1): every
   // camera free (no scale camera, camera 0 with a full block), and the
   // points shared with other partitions held by 3-D priors.  Per point

@@ -52,6 +52,10 @@ struct PcgArgs {
   unsigned *bar;
   int *err;
   int *iters;
+  // grid barriers wait for G + bar_extra arrivals, at most bar_ns each
+  // (bar_extra 0 and the default limit outside the timeout test hook)
+  unsigned bar_extra;
+  unsigned long long bar_ns;
   int row0, row1, nitems, msize;
   int mode;     // 0: reference stop rule; 1: relative preconditioned residual
   double tol2;  // mode 1: stop when r^T M^-1 r <= tol2 * (r0^T M^-1 r0)
@@ -285,7 +289,7 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
     cta_sum<1, PCG_W>(v, sh);
     if (threadIdx.x == 0) A.red2[4 * blockIdx.x] = v[0];
   }
-  if (!grid_barrier(A.bar, G, A.err)) return;
+  if (!grid_barrier(A.bar, G + A.bar_extra, A.err, A.bar_ns)) return;
   double erthk;
   {
     double v[1];
@@ -462,7 +466,7 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
     }
     cta_sum<1, PCG_W>(pdq, sh);
     if (threadIdx.x == 0) A.red1[4 * blockIdx.x] = pdq[0];
-    if (!grid_barrier(A.bar, G, A.err)) return;
+    if (!grid_barrier(A.bar, G + A.bar_extra, A.err, A.bar_ns)) return;
     double edtAdk;
     {
       double v[1];
@@ -547,7 +551,7 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
         }
         __syncthreads();
       }
-      if (!grid_barrier(A.bar, G, A.err)) return;
+      if (!grid_barrier(A.bar, G + A.bar_extra, A.err, A.bar_ns)) return;
       for (int a = blockIdx.x; a < A.nagg; a += G) {
         double z[CO_M];
 #pragma unroll
@@ -594,7 +598,7 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
       A.red2[4 * blockIdx.x + 1] = p2[1];
       A.red2[4 * blockIdx.x + 2] = p2[2];
     }
-    if (!grid_barrier(A.bar, G, A.err)) return;
+    if (!grid_barrier(A.bar, G + A.bar_extra, A.err, A.bar_ns)) return;
     double g3[3];
     grid_sum<3, PCG_W>(A.red2, G, g3, sh);
     const double meandr = g3[0], er1th1 = g3[1];
@@ -730,6 +734,8 @@ int pcg_iterate(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStre
   A.bar = W.bar;
   A.err = L.err;
   A.iters = W.iters;
+  A.bar_extra = L.bar_extra;
+  A.bar_ns = L.bar_timeout_ns ? L.bar_timeout_ns : BAR_TIMEOUT_NS;
   A.row0 = L.begini;
   A.row1 = L.nimg;
   A.nitems = L.nitems;

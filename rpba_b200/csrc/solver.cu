@@ -1827,10 +1827,24 @@ int32_t rpba_kernel_stats(rpba_handle *H, char *json, size_t cap) {
     o += b;
     first = false;
   }
+  // the reduced camera system's size, for per-iteration byte counts
+  char b[160];
+  std::snprintf(b, sizeof b, "%s\"_rcs\": {\"rows\": %d, \"offdiag_blocks\": %d, \"fp32\": %d}", first ? "" : ", ",
+                H->nimg - H->begini, H->L.nboff, H->L.blocks32 ? 1 : 0);
+  o += b;
   o += "}";
   const size_t n = std::min(cap - 1, o.size());
   std::memcpy(json, o.data(), n);
   json[n] = 0;
+  return RPBA_OK;
+}
+
+int32_t rpba_debug_barrier_timeout(rpba_handle *H, int32_t extra_ctas, int64_t timeout_ns) {
+  if (!H || extra_ctas < 0 || extra_ctas > 1 || timeout_ns < 0 || timeout_ns > 2000000000ll ||
+      (extra_ctas > 0 && timeout_ns < 1000000))
+    return RPBA_ERR_ARG;
+  H->L.bar_extra = (unsigned)extra_ctas;
+  H->L.bar_timeout_ns = (unsigned long long)timeout_ns;
   return RPBA_OK;
 }
 

@@ -40,7 +40,8 @@ EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block
            "rpba_float_sequential_sum_noalloc", "rpba_train_preconditioner",
            "rpba_set_preconditioner", "rpba_precond_loss_grad", "rpba_record_systems", "rpba_solve_batch",
            "rpba_triangulate", "rpba_triangulate_parts", "rpba_partition_images", "rpba_lsa_gcp_step",
-           "rpba_calc_plsa_parallel", "rpba_calc_plsa_parallel_hosted", "rpba_destroy")
+           "rpba_calc_plsa_parallel", "rpba_calc_plsa_parallel_hosted", "rpba_debug_barrier_timeout",
+           "rpba_destroy")
 
 _lib = None
 
@@ -122,6 +123,8 @@ def load():
     L.rpba_triangulate.restype = C.c_int32
     L.rpba_kernel_stats.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     L.rpba_kernel_stats.restype = C.c_int32
+    L.rpba_debug_barrier_timeout.argtypes = [C.c_void_p, C.c_int32, C.c_int64]
+    L.rpba_debug_barrier_timeout.restype = C.c_int32
     L.rpba_destroy.argtypes = [C.c_void_p]
     _lib = L
     return L
@@ -458,6 +461,13 @@ class Solver:
         buf = C.create_string_buffer(1 << 16)
         load().rpba_kernel_stats(self.h, buf, 1 << 16)
         return json.loads(buf.value.decode())
+
+    def debug_barrier_timeout(self, extra_ctas: int, timeout_ns: int):
+        """Test hook: the PCG's grid barriers wait for `extra_ctas` CTAs that
+        do not exist, for at most `timeout_ns`; (0, 0) restores them."""
+        st = load().rpba_debug_barrier_timeout(self.h, int(extra_ctas), int(timeout_ns))
+        if st != 0:
+            raise RpbaError(st, "rpba_debug_barrier_timeout")
 
     def close(self):
         if self.h:

@@ -90,3 +90,12 @@ def test_rpba_executable_rejects_arguments():
     exe = os.path.join(ROOT, "rpba_b200", "rpba")
     r = subprocess.run([exe, "x"], capture_output=True, text=True)
     assert r.returncode == 1 and "Parameter file not used" in r.stdout
+
+
+def test_barrier_timeout_hook_checks_its_arguments():
+    """The bounded-wait test hook refuses a missing handle and limits outside
+    1 ms .. 2 s (no device needed for the checks)."""
+    import rpba_b200 as rb
+    L = rb.load()
+    assert L.rpba_debug_barrier_timeout(None, 1, 20_000_000) == 1
+    assert L.rpba_debug_barrier_timeout(None, 0, 0) == 1

@@ -4,16 +4,13 @@ redundancy and an image without observations end with the same status and
 log line; a NaN camera ends with the NaN-step status; a PCG cap that the
 learned solver cannot meet falls back to the block-Jacobi PCG and the
 direct solve and still reaches the plain solver's RMS."""
-import os
 
 import numpy as np
 import pytest
 
 from rpba_b200 import scenes
 
-# run with RPBA_RUN_PENDING=1 until their first GPU run has passed
-pytestmark = [pytest.mark.gpu, pytest.mark.skipif(os.environ.get("RPBA_RUN_PENDING") != "1",
-                                                  reason="first run on a GPU pending")]
+pytestmark = pytest.mark.gpu
 
 
 def _pair(oracle_mod, blk, **kw):
@@ -62,3 +59,31 @@ def test_pcg_cap_falls_back(oracle_mod):
     P.close()
     assert st == 0 and rep["pcg_fallbacks"] > 0
     assert abs(rep["rms"] - rep_d["rms"]) <= 1e-4 * rep_d["rms"]
+
+
+def test_pcg_barrier_wait_runs_out_and_handle_recovers():
+    """A bounded wait that runs out: the persistent PCG's grid barriers are
+    made to wait for a CTA that does not exist (test hook), with a 20 ms
+    limit.  The kernel sets the error word and returns, the solve ends with
+    the device-timeout status instead of hanging, and the same handle then
+    solves normally, equal to a fresh handle."""
+    import time
+    import rpba_b200 as rb
+    blk = scenes.to_block(scenes.arc_scene(seed=5, n_cams=20, n_pts=2000))
+    S = rb.Solver(blk)
+    S.debug_barrier_timeout(1, 20_000_000)
+    t0 = time.perf_counter()
+    with pytest.raises(rb.RpbaError) as e:
+        S.solve()
+    dt = time.perf_counter() - t0
+    assert e.value.status == 6, e.value
+    assert dt < 30.0, dt
+    S.debug_barrier_timeout(0, 0)
+    st, rep = S.solve()
+    S.close()
+    F = rb.Solver(blk)
+    st_f, rep_f = F.solve()
+    F.close()
+    assert st == st_f == 0
+    assert rep["cost"] == rep_f["cost"] and rep["linear_solves"] == rep_f["linear_solves"]
+    print(f"timed-out solve returned after {dt * 1e3:.0f} ms")

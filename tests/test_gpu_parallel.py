@@ -9,15 +9,12 @@ sides solve the partition systems with the dense direct solver, so the
 bars are roundoff-level: cameras within 1e-9 (scaled), the same points
 taken, the same log integers; the loop's iteration count equal and its
 final Exteval sigma0 within 1e-6 relative."""
-import os
 import re
 
 import numpy as np
 import pytest
 
-# run with RPBA_RUN_PENDING=1 until their first GPU run has passed
-pytestmark = [pytest.mark.gpu, pytest.mark.skipif(os.environ.get("RPBA_RUN_PENDING") != "1",
-                                                  reason="first run on a GPU pending")]
+pytestmark = pytest.mark.gpu
 
 
 @pytest.fixture(scope="module")

@@ -45,6 +45,7 @@ def test_noalloc_sum_matches_allocating_entry_point_twice():
         dout = torch.full((1,), -1.0, dtype=torch.float32, device="cuda")
         assert _call(L, dv, v.size, dout) == 0
         got = np.float32(dout.cpu().numpy()[0])
+        assert np.isfinite(got), got  # NaN would mean a failed call
         assert got.tobytes() == expect.tobytes(), (got, expect)
 
 
