@@ -94,8 +94,9 @@ enum {
 typedef struct rpba_options {
   int32_t robust;        /* parameters: Robust                              */
   int32_t exteval;       /* parameters: Exteval (evaluate only, EvalLSA)    */
-  int32_t threads;       /* parameters: Threads (accepted; the GPU runs the
-                            global LSA, the reference's Threads=1 branch)   */
+  int32_t threads;       /* parameters: Threads: selects the partitioned or the
+                            global branch as the reference does (see
+                            rpba_calc_plsa); < 1: the host's threads        */
   int32_t k2, k4, f;     /* parameters: k2, k4, f  -> addflags[0..2]        */
   int32_t solver;        /* RPBA_SOLVER_*                                   */
   int32_t precision;     /* RPBA_PREC_*                                     */
@@ -149,6 +150,12 @@ const char *rpba_status_string(int32_t status);
 /* Version string of the library build (no counterpart in the reference). */
 const char *rpba_version(void);
 
+/* The reference's branch rule of CalcPLSA (rpbacore.cpp:79-92): the
+ * partition count min(threads, iround(n_images / 70)) when it is above 1,
+ * there are more than five images and exteval is 0; otherwise 1 (the global
+ * LSA).  threads < 1: the host's hardware threads.  Host code, no device. */
+int32_t rpba_partition_count(int32_t n_images, int32_t threads, int32_t exteval);
+
 /* InputBlock (rpba.cpp:180-284): parse a BAL text file into a block whose
  * arrays are allocated by the library (free with rpba_block_free).  Same
  * float quantisation, sign flip of the observations and k24out scaling. */
@@ -165,7 +172,16 @@ int32_t rpba_output_block(const char *path, rpba_block *blk, int32_t k24out);
 /* CalcPLSA (rpbacore.cpp:28-531): adjust (or, with opt->exteval, evaluate)
  * the block in place on the GPU.  The log receives the lines the reference
  * writes to its ostream ("Sigma0: ...", "BA-Error: ...", "ITTTT: ...");
- * pass log=NULL to skip it.  rep may be NULL. */
+ * pass log=NULL to skip it.  rep may be NULL.  The branch follows the
+ * reference's rule (rpbacore.cpp:79-92, rpba_partition_count below): with
+ * min(threads, iround(n_images / 70)) > 1 and more than five images the
+ * partitioned RPBA runs (rpba_calc_plsa_parallel over rpba_partition_images,
+ * the reference's "#threads", "Partitioning runtime" and "Thread:" lines at
+ * the head of the log; rep then carries only the status), else the global
+ * LSA.  threads < 1 means the host's hardware threads, as Threads = 0 does
+ * in the reference's parameters file (rpba.cpp:88-89).  The partitioned
+ * branch runs the drop-in form (FP64, PCG or direct); the mixed and learned
+ * forms always solve the whole block. */
 int32_t rpba_calc_plsa(rpba_block *blk, const rpba_options *opt, char *log,
                        size_t log_cap, rpba_report *rep);
 

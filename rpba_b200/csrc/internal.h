@@ -68,6 +68,8 @@ struct DevLSA {
   const int4 *item_meta;    // (row, first entry, end entry, 0)
   const int2 *rowspan;      // [nimg] (diagonal entry, end entry) of each row
   float *tpart;             // [nboff * 9] FP32 form: transposed block products
+  const int2 *bidx;         // FP32 form: (row, column) of every block, storage order
+  const int *firstN;        // [nimg + 1] first off-diagonal block of every row
   int *err;            // device error word
   // Test hook of the bounded waits (rpba_debug_barrier_timeout): the PCG's
   // grid barriers wait for bar_extra CTAs more than the launch has, for at
@@ -245,6 +247,11 @@ void learned_adam(float *W, float *m, float *v, const float *grad, float lr, int
 // ---- PCG (pcg.cu)
 struct PcgWork {
   double *r, *d, *q, *h, *x, *xbest, *Cinv, *partials, *part;
+  // FP32 form: d^k in FP32 ([nimg * 12]), and the SpMV's row sums of the
+  // diagonal blocks, of the rows' first runs, and of the warp runs that
+  // start inside a row ([nimg * 9], [nimg * 9], [warps * 9])
+  float *d32;
+  double *pdiag, *prow, *pw;
   double *drs;  // [nimg * 9] 1 / sqrt of the camera blocks' diagonal entries (learned features)
   unsigned *bar;
   int *iters;
@@ -261,6 +268,7 @@ int pcg_prepare(const DevLSA &L, const PcgWork &W, int mode, const float *weight
 int pcg_iterate(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s, int mode, double tol,
                 const CoarseWork *coarse);
 int pcg_max_grid(int device);
+int pcg_warps32();  // warps per CTA of the FP32 form's persistent PCG
 
 // ---- structure (structure.cu)
 struct StructWork {
@@ -274,6 +282,7 @@ struct StructWork {
   int *bcnt, *boff;
   int *nrun;
   int *cntN, *cntT, *firstN, *firstT, *rowtmp;
+  int2 *bidx;  // FP32 form: (row, column) of every block in storage order
   unsigned *tkey, *tkey2;
   int *tidx, *tidx2;
   int2 *contrib;

@@ -20,14 +20,11 @@ namespace rpba {
 
 namespace {
 
-// Threads per CTA of the persistent kernel, per block storage type: 1024 in
-// the FP64 form (32 warps, two work items in flight each through shared
-// memory), 640 in the FP32 form (20 warps whose three-slot register pipeline
-// and transposed products use 96 registers a thread; measured faster than
-// 768 and 1024).
+// Threads per CTA of the FP64 form's persistent kernel: 32 warps, two work
+// items in flight each through shared memory.  (The FP32 form is k_pcg32.)
 template <class BT>
 constexpr int pcg_threads() {
-  return sizeof(BT) == 8 ? 1024 : 640;
+  return 1024;
 }
 template <class BT>
 constexpr int pcg_warps() {
@@ -43,6 +40,14 @@ struct PcgArgs {
   const int4 *item_meta;  // (row, first entry, end entry, 0)
   const int2 *rowspan;    // (diagonal entry, end entry) of each row
   float *tpart;           // FP32 form: transposed products of the off-diagonal blocks
+  // FP32 form (k_pcg32): (row, column) of every block in storage order, the
+  // first off-diagonal block of every row, d^k in FP32 (12 floats a camera),
+  // and the phase-1 row sums (diagonal, row head, warp-run head)
+  const int2 *bidx;
+  const int *firstN;
+  int nboff;
+  float *d32;
+  double *pdiag, *prow, *pw;
   const double *Cinv;
   double *r, *h, *x, *xbest, *D0, *D1;
   double *part;        // [nitems * 9] SpMV partial rows
@@ -135,11 +140,10 @@ __device__ __forceinline__ void cp_async_wait() {
 // and its d^k values (column and row) are loaded into registers, while the
 // current item is multiplied.
 constexpr int P1_ELEMS = 3 * 81;
-// Dynamic shared memory: the FP64 form's stages; the FP32 form keeps its
-// pipeline in registers
+// Dynamic shared memory: the FP64 form's stages
 template <class BT>
 constexpr size_t pcg_smem_bytes() {
-  return sizeof(BT) == 8 ? sizeof(BT) * (size_t)pcg_warps<BT>() * 2 * P1_ELEMS : 0;
+  return sizeof(BT) * (size_t)pcg_warps<BT>() * 2 * P1_ELEMS;
 }
 struct P1Item {
   int it, row, ne;  // item, its row, entries (0 past the end)
@@ -189,69 +193,27 @@ __device__ __forceinline__ void p1_issue(const PcgArgs &A, int it, BT *stage, co
   cp_async_commit();
 }
 
-// First item of warp w's chunk in the FP32 form's phase 1 (the items are
-// split into nwarps contiguous chunks of near-equal size).
-__device__ __forceinline__ int chunk_start(long long w, int nitems, int nwarps) {
-  return (int)(w * nitems / nwarps);
-}
-
-// q of one row (valid in lanes < 9) from the phase-1 partials.  FP32 form:
-// the transposed products of the row's transposed entries (in entry order,
-// three interleaved groups), then one partial per (row, chunk) segment,
-// stored at the segment's first item: the row's first item and every chunk
-// start inside the row, summed in item order.  FP64 form: one partial per item, the three 9-lane groups taking
-// every third item (four loads in flight), in a fixed order.
-template <class BT>
-__device__ __forceinline__ double row_q(const PcgArgs &A, int row, int nwarps, int lane, int grp, int rr) {
+// q of one row (valid in lanes < 9) from the phase-1 partials of the FP64
+// form: one partial per item, the three 9-lane groups taking every third
+// item (four loads in flight), in a fixed order.
+__device__ __forceinline__ double row_q(const PcgArgs &A, int row, int lane, int grp, int rr) {
   const int t0 = A.row_item_off[row], t1 = A.row_item_off[row + 1];
-  if constexpr (sizeof(BT) == 4) {
-    // transposed products of the row's transposed entries (blocks stored by
-    // the rows before it): the three 9-lane groups take every third entry
-    double qt = 0.;
-    if (lane < 27) {
-      const int e1 = __ldg(&A.rowspan[row].x);
-#pragma unroll 4
-      for (int e = A.rowoff[row] + grp; e < e1; e += 3) {
-        const int blk = (__ldg(&A.ent[e].y) & 0x7fffffff) - A.row1;
-        qt += (double)__ldcg(A.tpart + (size_t)blk * 9 + rr);
-      }
+  double qg = 0.;
+  if (lane < 27) {
+    double q0 = 0., q1 = 0., q2 = 0., q3 = 0.;
+    int t = t0 + grp;
+    for (; t + 9 < t1; t += 12) {
+      q0 += __ldcg(A.part + (size_t)t * 9 + rr);
+      q1 += __ldcg(A.part + (size_t)(t + 3) * 9 + rr);
+      q2 += __ldcg(A.part + (size_t)(t + 6) * 9 + rr);
+      q3 += __ldcg(A.part + (size_t)(t + 9) * 9 + rr);
     }
-    const double qa = __shfl_down_sync(0xffffffffu, qt, 9);
-    const double qb = __shfl_down_sync(0xffffffffu, qt, 18);
-    double q = qt + qa + qb;
-    if (lane < 9 && t0 < t1) {
-      q += __ldcg(A.part + (size_t)t0 * 9 + lane);
-      // smallest w whose chunk starts after t0
-      long long w = ((long long)(t0 + 1) * nwarps + A.nitems - 1) / A.nitems;
-      int prev = t0;
-      for (; w < nwarps; ++w) {
-        const int st = chunk_start(w, A.nitems, nwarps);
-        if (st >= t1) break;
-        if (st != prev) {
-          q += __ldcg(A.part + (size_t)st * 9 + lane);
-          prev = st;
-        }
-      }
-    }
-    return q;
-  } else {
-    double qg = 0.;
-    if (lane < 27) {
-      double q0 = 0., q1 = 0., q2 = 0., q3 = 0.;
-      int t = t0 + grp;
-      for (; t + 9 < t1; t += 12) {
-        q0 += __ldcg(A.part + (size_t)t * 9 + rr);
-        q1 += __ldcg(A.part + (size_t)(t + 3) * 9 + rr);
-        q2 += __ldcg(A.part + (size_t)(t + 6) * 9 + rr);
-        q3 += __ldcg(A.part + (size_t)(t + 9) * 9 + rr);
-      }
-      for (; t < t1; t += 3) q0 += __ldcg(A.part + (size_t)t * 9 + rr);
-      qg = (q0 + q1) + (q2 + q3);
-    }
-    const double qa = __shfl_down_sync(0xffffffffu, qg, 9);
-    const double qb = __shfl_down_sync(0xffffffffu, qg, 18);
-    return qg + qa + qb;
+    for (; t < t1; t += 3) q0 += __ldcg(A.part + (size_t)t * 9 + rr);
+    qg = (q0 + q1) + (q2 + q3);
   }
+  const double qa = __shfl_down_sync(0xffffffffu, qg, 9);
+  const double qb = __shfl_down_sync(0xffffffffu, qg, 18);
+  return qg + qa + qb;
 }
 
 // Iteration k (two grid barriers):
@@ -265,10 +227,11 @@ __device__ __forceinline__ double row_q(const PcgArgs &A, int row, int nwarps, i
 //           (kept in hj), and the aggregate's restriction P^T r1 is formed
 //  phase 2b per aggregate: z = A_c^-1[aggregate rows] (P^T r1), then
 //           h1 = hj + P z and the two dot products
-// BT: the storage type of the reduced camera system's blocks (double, or
-// float in the mixed-precision form); vectors and sums are FP64 either way.
+// BT: the storage type of the reduced camera system's blocks, double (the
+// FP32 form has its own kernel, k_pcg32 below).
 template <bool CO, class BT>
 __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
+  static_assert(sizeof(BT) == 8, "k_pcg is the FP64 form");
   constexpr int PCG_T = pcg_threads<BT>(), PCG_W = pcg_warps<BT>();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gwarp = blockIdx.x * PCG_W + warp, nwarps = gridDim.x * PCG_W;
@@ -305,7 +268,6 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
     double *dcur = (k & 1) ? A.D1 : A.D0;
     // ---- phase 1
     double pdq[1] = {0.};
-    if constexpr (sizeof(BT) == 8) {
       {
         P1Item cur, nxt;
         p1_issue<BT>(A, gwarp, stage0, dprev, beta_prev, lane, grp, rr, cur);
@@ -337,133 +299,6 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
         cp_async_wait<0>();
         __syncwarp();
       }
-    } else {
-      // FP32 blocks, symmetric SpMV: the items cover each row's diagonal and
-      // normal entries, so every off-diagonal block is read once and gives
-      // both products: its row's (block row rr times the column camera's
-      // d^k) and its column's (block column rr, re-read from L1, times the
-      // row camera's d^k, stored in the block's slot of tpart; phase 2 adds
-      // it to the column's row, and its share of d^T A d is summed here).
-      // Each warp walks one contiguous chunk of the items (row order) with a
-      // three-slot register pipeline: the blocks of item t + 2 (and the d^k
-      // entries they multiply) are loaded while item t is multiplied, the
-      // entries of item t + 3 one step earlier; entry positions follow from
-      // the walk (row spans), so no load waits on another.  Products are
-      // formed in FP32 (FP32 blocks times d^k rounded to FP32); the row sums
-      // are carried in FP64, per (row, chunk) segment in registers, written
-      // once at the segment's first item.
-      const int c0 = chunk_start(gwarp, A.nitems, nwarps);
-      const int c1 = chunk_start(gwarp + 1, A.nitems, nwarps);
-      if (c0 < c1) {
-        const BT *blocks = (const BT *)A.blocks;
-        const int4 m0 = A.item_meta[c0];
-        int wrow = m0.x, we = m0.y, wend = __ldg(&A.rowspan[m0.x].y);
-        int rowN = 0;
-        int2 enN = make_int2(-1, 0);
-        // entries of the walk's next item (lanes < 27, col -1 past the row);
-        // a row's items run from its diagonal entry to its end
-        auto ent_next = [&]() {
-          rowN = wrow;
-          enN = make_int2(-1, 0);
-          if (lane < 27 && we + grp < wend) enN = __ldg(A.ent + we + grp);
-          we += 3;
-          if (we >= wend && ++wrow < A.row1) {
-            const int2 sp = __ldg(A.rowspan + wrow);
-            we = sp.x;
-            wend = sp.y;
-          }
-        };
-        // loads of the item whose entries are in enN into a slot, then the
-        // next entries (items past the chunk load nothing); ob: the lane's
-        // off-diagonal block (-1: none or the diagonal)
-        auto slot_load = [&](int t, float (&b)[9], float &dc, int &row, int &ob) {
-          row = rowN;
-          dc = 0.f;
-          ob = -1;
-          const int2 en = enN;
-          if (t < c1 && en.x >= 0) {
-            if (en.y >= A.row1) ob = en.y - A.row1;
-            // row rr of the block, or column rr of a transposed one
-            const bool tr = en.y < 0;
-            const BT *B = blocks + (size_t)(en.y & 0x7fffffff) * BS32 + (tr ? rr : rr * 9);
-            const int sc = tr ? 9 : 1;
-#pragma unroll
-            for (int c = 0; c < 9; ++c) b[c] = __ldg(B + c * sc);
-            const size_t j = (size_t)en.x * 9 + rr;
-            dc = (float)(__ldcg(A.h + j) + beta_prev * __ldcg(dprev + j));
-          } else {
-#pragma unroll
-            for (int c = 0; c < 9; ++c) b[c] = 0.f;
-          }
-          if (t + 1 < c1) ent_next();
-        };
-        auto dk_of = [&](int row) {
-          return lane < 9 ? __ldcg(A.h + (size_t)row * 9 + lane) + beta_prev * __ldcg(dprev + (size_t)row * 9 + lane)
-                          : 0.;
-        };
-        float bA[9], bB[9], bC[9];
-        float dA, dB, dC;
-        int rA, rB, rC, oA, oB, oC;
-        ent_next();
-        slot_load(c0, bA, dA, rA, oA);
-        slot_load(c0 + 1, bB, dB, rB, oB);
-        int seg = c0, segrow = rA;
-        double racc = 0., dseg = dk_of(segrow);
-        // d^k of the segment's row in every lane (FP32), for the transposed
-        // products
-        float xr[9];
-        auto row_x = [&]() {
-          const float v = (float)dseg;
-#pragma unroll
-          for (int c = 0; c < 9; ++c) xr[c] = __shfl_sync(0xffffffffu, v, c);
-        };
-        row_x();
-        // item t from slot (b, d, r, o); the slot `nb` receives item t + 2.
-        // An off-diagonal block's transposed product (column rr of the block,
-        // re-read from L1, times the row's d^k) goes to its slot of tpart.
-        auto step = [&](int t, const float (&b)[9], float d, int r, int o, float (&nb)[9], float &nd, int &nr,
-                        int &no) {
-          slot_load(t + 2, nb, nd, nr, no);
-          float acc = 0.f;
-#pragma unroll
-          for (int c = 0; c < 9; ++c) acc = fmaf(b[c], __shfl_sync(0xffffffffu, d, (lane < 27 ? gbase : 0) + c), acc);
-          const float a1 = __shfl_down_sync(0xffffffffu, acc, 9);
-          const float a2 = __shfl_down_sync(0xffffffffu, acc, 18);
-          if (r != segrow) {
-            if (lane < 9) {
-              A.part[(size_t)seg * 9 + lane] = racc;
-              pdq[0] += dseg * racc;
-            }
-            seg = t;
-            segrow = r;
-            racc = 0.;
-            dseg = dk_of(r);
-            row_x();
-          }
-          if (lane < 9) racc += (double)acc + (double)a1 + (double)a2;
-          if (o >= 0) {
-            const BT *Bc = blocks + (size_t)(o + A.row1) * BS32 + rr;
-            float yt = 0.f;
-#pragma unroll
-            for (int c = 0; c < 9; ++c) yt = fmaf(__ldg(Bc + c * 9), xr[c], yt);
-            A.tpart[(size_t)o * 9 + rr] = yt;
-            // the transposed product's share of d^T A d: d_c^T (B^T d_r)
-            pdq[0] += (double)d * (double)yt;
-          }
-        };
-        for (int t = c0; t < c1; t += 3) {
-          step(t, bA, dA, rA, oA, bC, dC, rC, oC);
-          if (t + 1 >= c1) break;
-          step(t + 1, bB, dB, rB, oB, bA, dA, rA, oA);
-          if (t + 2 >= c1) break;
-          step(t + 2, bC, dC, rC, oC, bB, dB, rB, oB);
-        }
-        if (lane < 9) {
-          A.part[(size_t)seg * 9 + lane] = racc;
-          pdq[0] += dseg * racc;
-        }
-      }
-    }
     cta_sum<1, PCG_W>(pdq, sh);
     if (threadIdx.x == 0) A.red1[4 * blockIdx.x] = pdq[0];
     if (!grid_barrier(A.bar, G + A.bar_extra, A.err, A.bar_ns)) return;
@@ -484,7 +319,7 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
       for (int row = A.row0 + gwarp; row < A.row1; row += nwarps) {
         const size_t i = (size_t)row * 9 + (lane < 9 ? lane : 0);
         double r1v = 0., hv = 0.;
-        const double q = row_q<BT>(A, row, nwarps, lane, grp, rr);
+        const double q = row_q(A, row, lane, grp, rr);
         if (lane < 9) {
           hv = __ldcg(A.h + i);
           const double dk = hv + beta_prev * __ldcg(dprev + i);
@@ -518,7 +353,7 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
           const int row = A.agg_rows[t];
           const size_t i = (size_t)row * 9 + (lane < 9 ? lane : 0);
           double r1v = 0.;
-          const double q = row_q<BT>(A, row, nwarps, lane, grp, rr);
+          const double q = row_q(A, row, lane, grp, rr);
           if (lane < 9) {
             const double hv = __ldcg(A.h + i);
             const double dk = hv + beta_prev * __ldcg(dprev + i);
@@ -630,6 +465,537 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// The FP32 form's persistent PCG (mixed precision and the learned solver).
+//
+// Phase 1 streams the reduced camera system through shared memory with 1-D
+// TMA bulk copies.  The blocks are read in storage order: the diagonal
+// blocks of rows begini.. first, then every off-diagonal block once (upper
+// triangle, row major).  The stream is cut into groups of 32 blocks, and
+// every warp owns a contiguous run of groups (equal counts, so every warp
+// moves the same bytes).  One elected lane copies a group's blocks (32 x
+// 324 B) and their (row, column) pairs into the warp's stage, completing on
+// the stage's mbarrier; each lane then owns one block: it forms the block's
+// row product B d_col (summed into its row) and, for an off-diagonal block,
+// the transposed product B^T d_row, which goes to the block's slot of tpart
+// through a bulk store of the whole group.  Lane i reads its block at byte
+// 324 i of the stage: 81 i is a distinct bank for every lane, so the reads
+// are conflict-free.  The gathered vector is d^k rounded to FP32 (d32, 12
+// floats per camera so that a camera is three aligned 16-byte loads),
+// formed for all rows in phase D before phase 1.
+//
+// Row sums: a diagonal block's product is written to pdiag[row]; the
+// off-diagonal products of a row are summed per group by a segmented warp
+// scan in FP32, then carried across groups in FP64 and written once per
+// (row, warp run): to prow[row] by the warp that holds the row's first block,
+// to pw[warp] by a warp whose run starts inside the row.  Phase 2 adds, per
+// row and in a fixed order, pdiag, prow, the pw of the runs that start inside
+// the row, and the transposed products of the row's blocks stored by earlier
+// rows (its transposed entries).
+//
+// Iteration k: phase D (d^k = h + beta d^(k-1), FP64 and FP32 copies),
+// barrier, phase 1 (A d^k and d^T A d), barrier, phase 2 (as in the FP64
+// form; with the coarse space split in 2a and 2b by one more barrier),
+// barrier.
+constexpr int P32_W = 16;  // warps per CTA
+constexpr int P32_T = P32_W * 32;
+constexpr int GB = 32;     // blocks per group: one per lane
+constexpr int STG_BLK = GB * 324 + 16;
+constexpr int STG_IDX = GB * 8 + 16;
+constexpr int STG_OUT = GB * 36;
+constexpr int STG_BYTES = STG_BLK + STG_IDX + STG_OUT + 16;  // + the mbarrier
+constexpr size_t P32_SMEM = (size_t)P32_W * STG_BYTES;
+static_assert(STG_BLK % 16 == 0 && STG_IDX % 16 == 0 && STG_OUT % 16 == 0, "16-byte aligned stage parts");
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// global -> shared bulk copy completing on `bar` (this CTA's own shared
+// memory; the source is this GPU's memory; no multicast)
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_store(void *dst, const void *src, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src)),
+               "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+
+// Group g of the stream: its first block (storage index), its block count
+// and, for an off-diagonal group, the first block's off-diagonal index.
+struct Grp32 {
+  long long start;
+  int n;
+  bool diag;
+  long long boff;
+};
+__device__ __forceinline__ Grp32 group_of(long long g, int gd, int row0, int row1, int nboff) {
+  Grp32 q;
+  if (g < gd) {
+    q.start = row0 + GB * g;
+    q.n = (int)min((long long)GB, row1 - q.start);
+    q.diag = true;
+    q.boff = -1;
+  } else {
+    const long long j = g - gd;
+    q.boff = GB * j;
+    q.start = row1 + q.boff;
+    q.n = (int)min((long long)GB, nboff - q.boff);
+    q.diag = false;
+  }
+  return q;
+}
+// first group of warp w's run (NG groups over NW warps)
+__device__ __forceinline__ long long run_start(long long w, long long ng, long long nw) { return w * ng / nw; }
+
+// Byte offsets of a group's data inside its 16-byte aligned copies.
+__device__ __forceinline__ unsigned blk_misalign(const float *blocks, long long start) {
+  return (unsigned)(((unsigned long long)(blocks + start * 81)) & 15ull);
+}
+__device__ __forceinline__ unsigned idx_misalign(const int2 *bidx, long long start) {
+  return (unsigned)(((unsigned long long)(bidx + start)) & 15ull);
+}
+
+// Issue the copies of group q into the warp's stage (one lane).
+__device__ __forceinline__ void group_issue(const PcgArgs &A, const Grp32 &q, unsigned char *stg,
+                                            unsigned long long *bar) {
+  const float *blocks = (const float *)A.blocks;
+  const unsigned mb = blk_misalign(blocks, q.start), mi = idx_misalign(A.bidx, q.start);
+  const unsigned nb_bytes = (mb + (unsigned)q.n * 324u + 15u) & ~15u;
+  const unsigned ni_bytes = (mi + (unsigned)q.n * 8u + 15u) & ~15u;
+  mbar_expect_tx(bar, nb_bytes + ni_bytes);
+  bulk_load(stg, (const unsigned char *)(blocks + q.start * 81) - mb, nb_bytes, bar);
+  bulk_load(stg + STG_BLK, (const unsigned char *)(A.bidx + q.start) - mi, ni_bytes, bar);
+}
+
+// Bounded wait on the stage's mbarrier (the copies of this CTA's own
+// memory end in microseconds; the limit only keeps a fault from hanging).
+__device__ __forceinline__ bool stage_wait(const PcgArgs &A, unsigned long long *bar, unsigned parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = gtimer();
+  while (!mbar_try_wait(bar, parity)) {
+    if (gtimer() - t0 > A.bar_ns) return false;
+  }
+  return true;
+}
+
+// FP32 d^k of camera c (12-float stride) into v[0..8]
+__device__ __forceinline__ void load_d32(const float *d32, int c, float (&v)[9]) {
+  const float4 *p = (const float4 *)(d32 + (size_t)c * 12);
+  const float4 a = __ldcg(p), b = __ldcg(p + 1), e = __ldcg(p + 2);
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+  v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  v[8] = e.x;
+}
+
+// q of one row in lanes < 9 (FP32 form).
+__device__ __forceinline__ double row_q32(const PcgArgs &A, int row, long long ng, long long nw, long long gd,
+                                          int lane) {
+  // transposed products of the blocks stored by earlier rows: one entry per
+  // lane, nine FP64 partial sums, then a fixed butterfly
+  double acc[9];
+#pragma unroll
+  for (int j = 0; j < 9; ++j) acc[j] = 0.;
+  const int e0 = __ldg(A.rowoff + row), e1 = __ldg(&A.rowspan[row].x);
+#pragma unroll 2
+  for (int e = e0 + lane; e < e1; e += 32) {
+    const long long b = (long long)(__ldg(&A.ent[e].y) & 0x7fffffff) - A.row1;
+    const float *t = A.tpart + b * 9;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) acc[j] += (double)__ldcg(t + j);
+  }
+#pragma unroll
+  for (int j = 0; j < 9; ++j)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], o);
+  double q = 0.;
+#pragma unroll
+  for (int j = 0; j < 9; ++j)
+    if (lane == j) q = acc[j];
+  if (lane < 9) {
+    const size_t i = (size_t)row * 9 + lane;
+    q += __ldcg(A.pdiag + i);
+    const int f0 = __ldg(A.firstN + row), f1 = __ldg(A.firstN + row + 1);
+    if (f1 > f0) {
+      q += __ldcg(A.prow + i);
+      // runs that start strictly inside the row's off-diagonal blocks
+      const long long glo = gd + f0 / GB + 1, ghi = gd + (f1 - 1) / GB;
+      if (glo <= ghi) {
+        for (long long w = (glo * nw + ng - 1) / ng; w < nw; ++w) {
+          const long long g = run_start(w, ng, nw);
+          if (g > ghi) break;
+          if (g >= glo && run_start(w + 1, ng, nw) > g) q += __ldcg(A.pw + (size_t)w * 9 + lane);
+        }
+      }
+    }
+  }
+  return q;
+}
+
+template <bool CO>
+__global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gwarp = blockIdx.x * P32_W + warp, nwarps = gridDim.x * P32_W;
+  const int G = gridDim.x;
+  __shared__ double sh[P32_W + 1][4];
+  extern __shared__ __align__(16) unsigned char pcg_dyn[];
+  unsigned char *stg = pcg_dyn + (size_t)warp * STG_BYTES;
+  float *outb = (float *)(stg + STG_BLK + STG_IDX);
+  unsigned long long *mbar = (unsigned long long *)(stg + STG_BLK + STG_IDX + STG_OUT);
+  unsigned parity = 0;
+  if (lane == 0) mbar_init(mbar, 1);
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  __syncwarp();
+  const float *blocks = (const float *)A.blocks;
+  const long long gd = (A.row1 - A.row0 + GB - 1) / GB, go = ((long long)A.nboff + GB - 1) / GB;
+  const long long ng = gd + go, nw = nwarps;
+  // r^T h of the start vectors
+  {
+    double v[1] = {0.};
+    for (int row = A.row0 + gwarp; row < A.row1; row += nwarps)
+      if (lane < 9) {
+        const size_t i = (size_t)row * 9 + lane;
+        v[0] += A.r[i] * A.h[i];
+      }
+    cta_sum<1, P32_W>(v, sh);
+    if (threadIdx.x == 0) A.red2[4 * blockIdx.x] = v[0];
+  }
+  if (!grid_barrier(A.bar, G + A.bar_extra, A.err, A.bar_ns)) return;
+  double erthk;
+  {
+    double v[1];
+    grid_sum<1, P32_W>(A.red2, G, v, sh);
+    erthk = v[0];
+  }
+  double meandrold = 1.e50, meandr0 = 1.e50, beta_prev = 0.;
+  const double erthk0 = erthk;
+  bool converged = false;
+  int k;
+  for (k = 0; k < A.msize; ++k) {
+    const double *dprev = (k & 1) ? A.D0 : A.D1;
+    double *dcur = (k & 1) ? A.D1 : A.D0;
+    // ---- phase D: d^k for every row, FP64 and FP32
+    for (int row = A.row0 + gwarp; row < A.row1; row += nwarps)
+      if (lane < 9) {
+        const size_t i = (size_t)row * 9 + lane;
+        const double dk = __ldcg(A.h + i) + beta_prev * __ldcg(dprev + i);
+        dcur[i] = dk;
+        A.d32[(size_t)row * 12 + lane] = (float)dk;
+      }
+    if (!grid_barrier(A.bar, G + A.bar_extra, A.err, A.bar_ns)) return;
+    // ---- phase 1
+    double pdq = 0.;
+    {
+      const long long g0 = run_start(gwarp, ng, nw), g1 = run_start(gwarp + 1, ng, nw);
+      int cur_row = -1;   // row of the running sum (-1: none yet in this run)
+      bool cur_head = false;
+      double racc = 0.;   // running sum of cur_row, component `lane` (lanes < 9)
+      auto flush = [&]() {
+        if (cur_row >= 0 && lane < 9) {
+          double *dst = cur_head ? A.prow + (size_t)cur_row * 9 : A.pw + (size_t)gwarp * 9;
+          dst[lane] = racc;
+        }
+      };
+      if (g0 < g1 && lane == 0) group_issue(A, group_of(g0, (int)gd, A.row0, A.row1, A.nboff), stg, mbar);
+      bool ok = true;
+      for (long long g = g0; g < g1; ++g) {
+        const Grp32 q = group_of(g, (int)gd, A.row0, A.row1, A.nboff);
+        if (!stage_wait(A, mbar, parity)) {
+          ok = false;
+          break;
+        }
+        parity ^= 1u;
+        const unsigned mb = blk_misalign(blocks, q.start), mi = idx_misalign(A.bidx, q.start);
+        const bool act = lane < q.n;
+        int2 rc = make_int2(-1 - lane, -1);
+        float dc[9], dr[9], y[9], t[9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+          y[j] = 0.f;
+          t[j] = 0.f;
+        }
+        if (act) {
+          rc = *(const int2 *)(stg + STG_BLK + mi + 8 * lane);
+          load_d32(A.d32, rc.y, dc);
+          load_d32(A.d32, rc.x, dr);
+          const float *B = (const float *)(stg + mb + 324 * lane);
+#pragma unroll
+          for (int i = 0; i < 9; ++i) {
+            float yi = 0.f;
+#pragma unroll
+            for (int j = 0; j < 9; ++j) {
+              const float b = B[i * 9 + j];
+              yi = fmaf(b, dc[j], yi);
+              t[j] = fmaf(b, dr[i], t[j]);
+            }
+            y[i] = yi;
+          }
+          double s = 0.;
+#pragma unroll
+          for (int i = 0; i < 9; ++i) s += (double)dr[i] * (double)y[i];
+          if (!q.diag)
+#pragma unroll
+            for (int j = 0; j < 9; ++j) s += (double)dc[j] * (double)t[j];
+          pdq += s;
+        }
+        // the stage's blocks are read: the next group's copies may land
+        __syncwarp();
+        if (lane == 0 && g + 1 < g1) {
+          fence_proxy_async();
+          group_issue(A, group_of(g + 1, (int)gd, A.row0, A.row1, A.nboff), stg, mbar);
+        }
+        if (q.diag) {
+          if (act) {
+            double *dst = A.pdiag + (size_t)rc.x * 9;
+#pragma unroll
+            for (int i = 0; i < 9; ++i) dst[i] = (double)y[i];
+          }
+          continue;
+        }
+        // transposed products: staged, then one bulk store of the group
+        if (lane == 0) bulk_wait_read();
+        __syncwarp();
+        if (act)
+#pragma unroll
+          for (int j = 0; j < 9; ++j) outb[9 * lane + j] = t[j];
+        fence_proxy_async();
+        __syncwarp();
+        if (lane == 0) bulk_store(A.tpart + q.boff * 9, outb, ((unsigned)q.n * 36u + 15u) & ~15u);
+        // segmented scan of the row products (rows non-decreasing in lane
+        // order; inactive lanes carry distinct negative rows)
+        const int row = rc.x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const int ru = __shfl_up_sync(0xffffffffu, row, o);
+#pragma unroll
+          for (int j = 0; j < 9; ++j) {
+            const float vu = __shfl_up_sync(0xffffffffu, y[j], o);
+            if (lane >= o && ru == row) y[j] += vu;
+          }
+        }
+        const int rnext = __shfl_down_sync(0xffffffffu, row, 1);
+        const bool end = act && (lane == q.n - 1 || rnext != row);
+        unsigned ends = __ballot_sync(0xffffffffu, end);
+        int seg_first = 0;  // first lane of the segment ending at e
+        while (ends) {
+          const int e = __ffs(ends) - 1;
+          ends &= ends - 1;
+          const int re = __shfl_sync(0xffffffffu, row, e);
+          double sv = 0.;
+#pragma unroll
+          for (int j = 0; j < 9; ++j) {
+            const float tv = __shfl_sync(0xffffffffu, y[j], e);
+            if (lane == j) sv = (double)tv;
+          }
+          if (re == cur_row) {
+            racc += sv;
+          } else {
+            flush();
+            // a segment starts the row unless it is the run's first and the
+            // row began before the run
+            cur_head = cur_row >= 0 || seg_first > 0 || q.boff + seg_first == (long long)__ldg(A.firstN + re);
+            cur_row = re;
+            racc = sv;
+          }
+          seg_first = e + 1;
+        }
+      }
+      if (ok) flush();
+      if (lane == 0) bulk_wait_all();
+      __syncwarp();
+      if (!ok) {
+        // a copy that never completed: record it, give it one more bounded
+        // wait, and leave after the grid barrier below has failed as well
+        if (lane == 0) atomicOr(A.err, 2);
+        stage_wait(A, mbar, parity);
+      }
+    }
+    // the transposed products (async-proxy writes) before the barrier's release
+    asm volatile("fence.proxy.async.global;\n" ::: "memory");
+    {
+      double v[1] = {pdq};
+      cta_sum<1, P32_W>(v, sh);
+      if (threadIdx.x == 0) A.red1[4 * blockIdx.x] = v[0];
+    }
+    if (!grid_barrier(A.bar, G + A.bar_extra, A.err, A.bar_ns)) return;
+    double edtAdk;
+    {
+      double v[1];
+      grid_sum<1, P32_W>(A.red1, G, v, sh);
+      edtAdk = v[0];
+    }
+    double alpha;
+    if (fabs(erthk) < 1.e-20 || fabs(erthk) > 1.e20)
+      alpha = 0.;
+    else
+      alpha = erthk / edtAdk;
+    // ---- phase 2
+    double p2[3] = {0., 0., 0.};
+    if constexpr (!CO) {
+      for (int row = A.row0 + gwarp; row < A.row1; row += nwarps) {
+        const size_t i = (size_t)row * 9 + (lane < 9 ? lane : 0);
+        double r1v = 0., hv = 0.;
+        const double q = row_q32(A, row, ng, nw, gd, lane);
+        if (lane < 9) {
+          hv = __ldcg(A.h + i);
+          const double dk = __ldcg(dcur + i);
+          A.x[i] = A.x[i] + alpha * dk;
+          const double dr = alpha * q;
+          r1v = A.r[i] - dr;
+          p2[0] += dr * dr;
+        }
+        const double *C = A.Cinv + (size_t)row * 81;
+        double h1v = 0.;
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+          const double rc = __shfl_sync(0xffffffffu, r1v, c);
+          if (lane < 9) h1v += __ldg(C + lane * 9 + c) * rc;
+        }
+        if (lane < 9) {
+          A.r[i] = r1v;
+          A.h[i] = h1v;
+          p2[1] += r1v * (h1v - hv);
+          p2[2] += r1v * h1v;
+        }
+      }
+    } else {
+      __shared__ double shr[P32_W][CO_M];
+      __shared__ double shz[CO_M];
+      for (int a = blockIdx.x; a < A.nagg; a += G) {
+        const int t0 = A.agg_off[a], t1 = A.agg_off[a + 1];
+        double rcw = 0.;
+        for (int t = t0 + warp; t < t1; t += P32_W) {
+          const int row = A.agg_rows[t];
+          const size_t i = (size_t)row * 9 + (lane < 9 ? lane : 0);
+          double r1v = 0.;
+          const double q = row_q32(A, row, ng, nw, gd, lane);
+          if (lane < 9) {
+            const double dk = __ldcg(dcur + i);
+            A.x[i] = __ldcg(A.x + i) + alpha * dk;
+            const double dr = alpha * q;
+            r1v = __ldcg(A.r + i) - dr;
+            p2[0] += dr * dr;
+          }
+          const double *C = A.Cinv + (size_t)row * 81;
+          const double *Pk = A.P + (size_t)row * (9 * CO_M);
+          double h1v = 0.;
+#pragma unroll
+          for (int c = 0; c < 9; ++c) {
+            const double rc = __shfl_sync(0xffffffffu, r1v, c);
+            if (lane < 9) h1v += __ldg(C + lane * 9 + c) * rc;
+            if (lane < CO_M) rcw += __ldg(Pk + c * CO_M + lane) * rc;
+          }
+          if (lane < 9) {
+            A.r[i] = r1v;
+            A.hj[i] = h1v;
+          }
+        }
+        if (lane < CO_M) shr[warp][lane] = rcw;
+        __syncthreads();
+        if (threadIdx.x < CO_M) {
+          double sum = 0.;
+          for (int w = 0; w < P32_W; ++w) sum += shr[w][threadIdx.x];
+          A.rc[a * CO_M + threadIdx.x] = sum;
+        }
+        __syncthreads();
+      }
+      if (!grid_barrier(A.bar, G + A.bar_extra, A.err, A.bar_ns)) return;
+      for (int a = blockIdx.x; a < A.nagg; a += G) {
+        double z[CO_M];
+#pragma unroll
+        for (int j = 0; j < CO_M; ++j) z[j] = 0.;
+        for (int i = threadIdx.x; i < A.nc; i += P32_T) {
+          const double rv = __ldcg(A.rc + i);
+#pragma unroll
+          for (int j = 0; j < CO_M; ++j) z[j] += __ldg(A.Ainv + (size_t)(a * CO_M + j) * A.nc + i) * rv;
+        }
+#pragma unroll
+        for (int j = 0; j < CO_M; ++j) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) z[j] += __shfl_xor_sync(0xffffffffu, z[j], o);
+          if (lane == 0) shr[warp][j] = z[j];
+        }
+        __syncthreads();
+        if (threadIdx.x < CO_M) {
+          double sum = 0.;
+          for (int w = 0; w < P32_W; ++w) sum += shr[w][threadIdx.x];
+          shz[threadIdx.x] = sum;
+        }
+        __syncthreads();
+        const int t0 = A.agg_off[a], t1 = A.agg_off[a + 1];
+        for (int t = t0 + warp; t < t1; t += P32_W) {
+          const int row = A.agg_rows[t];
+          if (lane < 9) {
+            const size_t i = (size_t)row * 9 + lane;
+            const double *Pk = A.P + (size_t)row * (9 * CO_M) + lane * CO_M;
+            double h1v = __ldcg(A.hj + i);
+#pragma unroll
+            for (int j = 0; j < CO_M; ++j) h1v += __ldg(Pk + j) * shz[j];
+            const double hv = __ldcg(A.h + i), r1v = __ldcg(A.r + i);
+            p2[1] += r1v * (h1v - hv);
+            p2[2] += r1v * h1v;
+            A.h[i] = h1v;
+          }
+        }
+        __syncthreads();
+      }
+    }
+    cta_sum<3, P32_W>(p2, sh);
+    if (threadIdx.x == 0) {
+      A.red2[4 * blockIdx.x] = p2[0];
+      A.red2[4 * blockIdx.x + 1] = p2[1];
+      A.red2[4 * blockIdx.x + 2] = p2[2];
+    }
+    if (!grid_barrier(A.bar, G + A.bar_extra, A.err, A.bar_ns)) return;
+    double g3[3];
+    grid_sum<3, P32_W>(A.red2, G, g3, sh);
+    const double meandr = g3[0], er1th1 = g3[1];
+    if (k == 0) meandr0 = meandr;
+    const bool finite = isfinite(g3[0]) && isfinite(g3[2]);
+    const bool improved = (A.mode == 1 && finite) || meandr < meandrold;
+    if (improved) {
+      meandrold = meandr;
+      for (int row = A.row0 + gwarp; row < A.row1; row += nwarps)
+        if (lane < 9) A.xbest[(size_t)row * 9 + lane] = __ldcg(A.x + (size_t)row * 9 + lane);
+    }
+    if (A.mode == 0 && meandr * 1.e5 < meandr0) break;
+    if (A.mode == 1 && !finite) break;
+    if (A.mode == 1 && g3[2] <= A.tol2 * erthk0) {
+      converged = true;
+      break;
+    }
+    double beta = fabs(er1th1) < 1.e-10 ? 0. : er1th1 / erthk;
+    if (beta < 0.) beta = 0.;
+    beta_prev = beta;
+    erthk = g3[2];
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    A.iters[0] = k < A.msize ? k + 1 : A.msize;
+    A.iters[1] = converged ? 1 : 0;
+  }
+}
+
 // Preconditioner C_k = S_kk^-1 (rbacore.cpp:1839-1846) and the start
 // vectors: r = b, h = C r, d^(-1) = 0, x = 0, best = b.
 __global__ void k_pcg_setup(DevLSA L, PcgWork W) {
@@ -665,11 +1031,11 @@ void pcg_set_smem() {
                        (int)pcg_smem_bytes<double>());
   cudaFuncSetAttribute(k_pcg<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                        (int)pcg_smem_bytes<double>());
-  cudaFuncSetAttribute(k_pcg<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)pcg_smem_bytes<float>());
-  cudaFuncSetAttribute(k_pcg<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)pcg_smem_bytes<float>());
+  cudaFuncSetAttribute(k_pcg32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P32_SMEM);
+  cudaFuncSetAttribute(k_pcg32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P32_SMEM);
 }
+
+int pcg_warps32() { return P32_W; }
 
 int pcg_max_grid(int device) {
   int nsm = 0, per = 0, per2 = 0;
@@ -680,11 +1046,9 @@ int pcg_max_grid(int device) {
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true, double>, pcg_threads<double>(),
                                                 pcg_smem_bytes<double>());
   per = std::min(per, per2);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<false, float>, pcg_threads<float>(),
-                                                pcg_smem_bytes<float>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg32<false>, P32_T, P32_SMEM);
   per = std::min(per, per2);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg<true, float>, pcg_threads<float>(),
-                                                pcg_smem_bytes<float>());
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_pcg32<true>, P32_T, P32_SMEM);
   per = std::min(per, per2);
   if (per < 1) per = 1;
   return nsm * per;
@@ -709,8 +1073,16 @@ int pcg_iterate(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStre
   const bool co = coarse && coarse->nagg > 0;
   const int nrows = L.nimg - L.begini;
   if (nrows <= 0) return 0;
-  const int wpc = L.blocks32 ? pcg_warps<float>() : pcg_warps<double>();
-  int g = (L.nitems + wpc - 1) / wpc;
+  int g;
+  if (L.blocks32) {
+    // FP32 form: groups of 32 blocks (the diagonal blocks of the system's
+    // rows, then the off-diagonal blocks), at least one group per warp
+    const long long ng = (nrows + GB - 1) / GB + ((long long)L.nboff + GB - 1) / GB;
+    g = (int)std::min<long long>((ng + P32_W - 1) / P32_W, grid);
+  } else {
+    const int wpc = pcg_warps<double>();
+    g = (L.nitems + wpc - 1) / wpc;
+  }
   if (g > grid) g = grid;
   if (g < 1) g = 1;
   PcgArgs A;
@@ -721,6 +1093,13 @@ int pcg_iterate(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStre
   A.item_meta = L.item_meta;
   A.rowspan = L.rowspan;
   A.tpart = L.tpart;
+  A.bidx = L.bidx;
+  A.firstN = L.firstN;
+  A.nboff = L.nboff;
+  A.d32 = W.d32;
+  A.pdiag = W.pdiag;
+  A.prow = W.prow;
+  A.pw = W.pw;
   A.Cinv = W.Cinv;
   A.r = W.r;
   A.h = W.h;
@@ -753,13 +1132,18 @@ int pcg_iterate(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStre
   RPBA_CUDA_CHECK(cudaMemsetAsync(W.bar, 0, 2 * sizeof(unsigned), s));
   void *args[] = {&A};
   const void *fn;
-  if (L.blocks32)
-    fn = co ? (const void *)k_pcg<true, float> : (const void *)k_pcg<false, float>;
-  else
+  size_t smem;
+  int nthreads;
+  if (L.blocks32) {
+    fn = co ? (const void *)k_pcg32<true> : (const void *)k_pcg32<false>;
+    smem = P32_SMEM;
+    nthreads = P32_T;
+  } else {
     fn = co ? (const void *)k_pcg<true, double> : (const void *)k_pcg<false, double>;
-  const size_t smem = L.blocks32 ? pcg_smem_bytes<float>() : pcg_smem_bytes<double>();
+    smem = pcg_smem_bytes<double>();
+    nthreads = pcg_threads<double>();
+  }
   pcg_set_smem();
-  const int nthreads = L.blocks32 ? pcg_threads<float>() : pcg_threads<double>();
   RPBA_CUDA_CHECK(cudaLaunchCooperativeKernel(fn, dim3(g), dim3(nthreads), args, smem, s));
   return 0;
 }

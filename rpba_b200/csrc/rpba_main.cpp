@@ -3,12 +3,12 @@
 // (keys Robust, Exteval, Threads, k2, k4, f, k24out, InputDir, File; all
 // required, as rpba.cpp:56-64 reads them), loads InputDir/File as BAL text,
 // runs CalcPLSA on the GPU and prints the reference's console lines.
-// Extra optional keys: Solver (pcg | direct | learned), Precision (fp64 |
-// mixed), MaxIterations, Output (write the adjusted block as BAL text; the
-// reference has this call commented out, rpba.cpp:144-150), Partitioned
-// (1: take the reference's partitioned branch where its rule does,
-// min(Threads, iround(images / 70)) > 1 and more than five images,
-// rpbacore.cpp:79-92; default 0: the global LSA on the GPU).
+// Threads selects the branch as in the reference (rpbacore.cpp:79-92): the
+// partitioned RPBA when min(Threads, iround(images / 70)) > 1 and there are
+// more than five images, else the global LSA; Threads = 0 means the host's
+// hardware threads.  Extra optional keys: Solver (pcg | direct | learned),
+// Precision (fp64 | mixed), MaxIterations, Output (write the adjusted block
+// as BAL text; the reference has this call commented out, rpba.cpp:144-150).
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -116,28 +116,11 @@ int main(int argc, char **argv) {
   std::vector<char> log(1 << 20);
   rpba_report rep{};
   const auto t0 = std::chrono::steady_clock::now();
-  const int nrthreads = std::min(mt, (int)std::lround((float)blk.n_images / 70.f));
-  const bool partitioned = kv.count("Partitioned") && parse<int>(kv["Partitioned"]) && !extevalflag &&
-                           nrthreads > 1 && blk.n_images > 5;
-  if (partitioned) {
-    // the parallel branch: its header lines (rpbacore.cpp:110-178)
-    std::printf("#threads: %d %d\n", nrthreads, (int)std::lround((float)blk.n_images / 70.f));
-    std::vector<int32_t> part(blk.n_images);
-    const auto tp = std::chrono::steady_clock::now();
-    st = rpba_partition_images(&blk, nrthreads, part.data());
-    std::printf("\n\nPartitioning runtime: %gs\n\n",
-                (float)std::chrono::duration<double>(std::chrono::steady_clock::now() - tp).count());
-    if (st == RPBA_OK) {
-      std::vector<int> cnt(nrthreads, 0);
-      for (int32_t q : part) ++cnt[q];
-      for (int it = 0, a = 0; it < nrthreads; a += cnt[it], ++it)
-        std::printf("Thread: %d #images %d indices %d %d\n", it, cnt[it], a, a + cnt[it]);
-      double stats[2];
-      st = rpba_calc_plsa_parallel(&blk, &opt, nrthreads, part.data(), log.data(), log.size(), stats);
-    }
-  } else {
-    st = rpba_calc_plsa(&blk, &opt, log.data(), log.size(), &rep);
-  }
+  // the branch (global or partitioned) follows the reference's rule inside
+  // rpba_calc_plsa; the partitioned branch's lines are console output
+  const bool partitioned = rpba_partition_count(blk.n_images, mt, extevalflag) > 1 &&
+                           opt.precision == RPBA_PREC_FP64 && opt.solver != RPBA_SOLVER_LEARNED;
+  st = rpba_calc_plsa(&blk, &opt, log.data(), log.size(), &rep);
   const double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   // the partitioned branch's progress lines are console output in the reference
   if (partitioned || blk.n_images < 50 || mt == 1 || extevalflag) std::printf("%s", log.data());

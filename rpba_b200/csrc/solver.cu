@@ -292,7 +292,7 @@ struct rpba_handle {
     if (nb <= blocks_cap && cur) return;
     const int cap = std::max(nb, 1);
     if (cur) {
-      for (void *p : {cur, (void *)S.ent, (void *)S.item_meta, (void *)W.part, (void *)L.tpart}) {
+      for (void *p : {cur, (void *)S.ent, (void *)S.item_meta, (void *)W.part, (void *)L.tpart, (void *)S.bidx}) {
         if (!p) continue;
         auto it = std::find(owned_async.begin(), owned_async.end(), p);
         if (it != owned_async.end()) {
@@ -305,8 +305,11 @@ struct rpba_handle {
       }
     }
     if (mixed) {
-      L.blocks32 = dalloc<float>((size_t)(nimg + cap) * BS32, owned);
-      L.tpart = dalloc<float>((size_t)cap * 9, owned);
+      // slack past the last block, row pair and transposed product: the
+      // FP32 PCG's bulk copies round their sizes up to 16 bytes
+      L.blocks32 = dalloc<float>((size_t)(nimg + cap) * BS32 + 16, owned);
+      L.tpart = dalloc<float>((size_t)cap * 9 + 16, owned);
+      S.bidx = dalloc<int2>((size_t)nimg + cap + 4, owned);
     } else
       L.blocks = dalloc<double>((size_t)(nimg + cap) * BS64, owned);
     S.ent = dalloc<int2>((size_t)nimg + 2 * (size_t)cap, owned);
@@ -776,6 +779,12 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   W.partials = dalloc<double>(8 * (size_t)H->pcg_grid, own);
   W.bar = dalloc<unsigned>(2, own);
   W.iters = dalloc<int>(2, own);
+  if (o->precision == RPBA_PREC_MIXED) {
+    W.d32 = dalloc<float>(12 * (size_t)n + 4, own);
+    W.pdiag = dalloc<double>(nv, own);
+    W.prow = dalloc<double>(nv, own);
+    W.pw = dalloc<double>(9 * (size_t)H->pcg_grid * pcg_warps32(), own);
+  }
   RPBA_CUDA_CHECK(cudaMemsetAsync(W.q, 0, sizeof(double) * nv, H->s));
   RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
   return RPBA_OK;
@@ -1850,9 +1859,63 @@ int32_t rpba_debug_barrier_timeout(rpba_handle *H, int32_t extra_ctas, int64_t t
 
 void rpba_destroy(rpba_handle *H) { delete H; }
 
+int32_t rpba_partition_count(int32_t n_images, int32_t threads, int32_t exteval) {
+  int mt = threads;
+  if (mt < 1) mt = std::max(1, (int)std::thread::hardware_concurrency());
+  // boost::math::iround: nearest, halves away from zero
+  const int minnrthreads = (int)std::lround((float)n_images / 70.f);
+  const int nr = std::min(mt, minnrthreads);
+  return (!exteval && nr > 1 && n_images > 5) ? nr : 1;
+}
+
+namespace {
+// CalcPLSA's partitioned branch (rpbacore.cpp:100-510): the reference's
+// console lines (rpbacore.cpp:110, 140, 157) at the head of the log, the
+// partition, and the loop.
+int32_t calc_plsa_partitioned(rpba_block *blk, const rpba_options *opt, int nrthreads, char *log, size_t cap,
+                              rpba_report *rep) {
+  std::string head = "#threads: " + std::to_string(nrthreads) + " " +
+                     std::to_string((int)std::lround((float)blk->n_images / 70.f)) + "\n";
+  std::vector<int32_t> part(blk->n_images);
+  const auto tp = std::chrono::steady_clock::now();
+  int32_t st = rpba_partition_images(blk, nrthreads, part.data());
+  char line[160];
+  std::snprintf(line, sizeof line, "\n\nPartitioning runtime: %gs\n\n",
+                (float)std::chrono::duration<double>(std::chrono::steady_clock::now() - tp).count());
+  head += line;
+  if (st == RPBA_OK) {
+    std::vector<int> cnt(nrthreads, 0);
+    for (int32_t q : part) ++cnt[q];
+    for (int it = 0, a = 0; it < nrthreads; a += cnt[it], ++it) {
+      std::snprintf(line, sizeof line, "Thread: %d #images %d indices %d %d\n", it, cnt[it], a, a + cnt[it]);
+      head += line;
+    }
+  }
+  size_t used = 0;
+  if (log && cap) {
+    used = std::min(cap - 1, head.size());
+    std::memcpy(log, head.data(), used);
+    log[used] = 0;
+  }
+  if (st == RPBA_OK) {
+    double stats[2] = {0., 0.};
+    st = rpba_calc_plsa_parallel(blk, opt, nrthreads, part.data(), log ? log + used : nullptr,
+                                 log ? cap - used : 0, stats);
+  }
+  if (rep) rep->status = st;
+  return st;
+}
+}  // namespace
+
 int32_t rpba_calc_plsa(rpba_block *blk, const rpba_options *opt, char *log, size_t cap, rpba_report *rep) {
   if (!blk || !opt) return RPBA_ERR_ARG;
   if (rep) std::memset(rep, 0, sizeof *rep);
+  // the reference's branch rule (rpbacore.cpp:79-92); the partitioned branch
+  // runs the drop-in FP64 form, the other forms always solve the whole block
+  const int nrthreads = rpba_partition_count(blk->n_images, opt->threads, opt->exteval);
+  if (nrthreads > 1 && opt->precision == RPBA_PREC_FP64 &&
+      (opt->solver == RPBA_SOLVER_PCG || opt->solver == RPBA_SOLVER_DIRECT))
+    return calc_plsa_partitioned(blk, opt, nrthreads, log, cap, rep);
   rpba_handle *H = nullptr;
   int st = rpba_create(&H, blk, opt);
   if (st != RPBA_OK) return st;

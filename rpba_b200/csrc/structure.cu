@@ -142,6 +142,19 @@ __global__ void k_fill_items(const int *rowoff, const int *cntT, const int *row_
   }
 }
 
+// (row, column) of every block of the reduced camera system in storage
+// order: the diagonal blocks, then the off-diagonal blocks (key row * n + col)
+__global__ void k_fill_bidx(const unsigned *bkey, int nb, int nimg, int2 *bidx) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)nimg + nb) return;
+  if (i < nimg) {
+    bidx[i] = make_int2((int)i, (int)i);
+  } else {
+    const unsigned key = bkey[i - nimg];
+    bidx[i] = make_int2((int)(key / (unsigned)nimg), (int)(key % (unsigned)nimg));
+  }
+}
+
 __global__ void k_fill_diag(int nimg, const int *rowoff, const int *cntT, int2 *ent) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nimg) return;
@@ -244,6 +257,11 @@ void build_bsr(DevLSA &L, StructWork &S, cudaStream_t s) {
   RPBA_CUDA_CHECK(cudaMemcpyAsync(&nitems, S.row_item_off + n, sizeof(int), cudaMemcpyDeviceToHost, s));
   RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
   k_fill_items<<<nblk(n, 256), 256, 0, s>>>(S.rowoff, S.cntT, S.row_item_off, n, L.begini, sym, S.item_meta);
+  if (L.blocks32) {
+    k_fill_bidx<<<nblk((long long)n + nb, 256), 256, 0, s>>>(S.bkey, nb, n, S.bidx);
+    L.bidx = S.bidx;
+    L.firstN = S.firstN;
+  }
   L.rowoff = S.rowoff;
   L.ent = S.ent;
   L.nitems = nitems;

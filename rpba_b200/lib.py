@@ -41,6 +41,7 @@ EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block
            "rpba_set_preconditioner", "rpba_precond_loss_grad", "rpba_record_systems", "rpba_solve_batch",
            "rpba_triangulate", "rpba_triangulate_parts", "rpba_partition_images", "rpba_lsa_gcp_step",
            "rpba_calc_plsa_parallel", "rpba_calc_plsa_parallel_hosted", "rpba_debug_barrier_timeout",
+           "rpba_partition_count",
            "rpba_destroy")
 
 _lib = None
@@ -123,6 +124,8 @@ def load():
     L.rpba_triangulate.restype = C.c_int32
     L.rpba_kernel_stats.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     L.rpba_kernel_stats.restype = C.c_int32
+    L.rpba_partition_count.argtypes = [C.c_int32, C.c_int32, C.c_int32]
+    L.rpba_partition_count.restype = C.c_int32
     L.rpba_debug_barrier_timeout.argtypes = [C.c_void_p, C.c_int32, C.c_int64]
     L.rpba_debug_barrier_timeout.restype = C.c_int32
     L.rpba_destroy.argtypes = [C.c_void_p]

@@ -1,13 +1,19 @@
-"""Independent replicas over ranks: one process per GPU, each solving its own
-scene, with no collective on the data path.
+"""Work over ranks: one process per GPU, no collective on the data path.
 
 The reference's global LSA does not shard (one linear system per LM step);
 its own parallel form partitions the scene into independent LSAs
-(rpbacore.cpp:100-510).  Across GPUs this library therefore runs replicas:
-every rank times its own solves, and the job's time is the slowest rank's
-(max over ranks), its throughput the units of all ranks over that time.
-Only these host-side reductions cross ranks, through torch.distributed
-(NCCL on GPUs, gloo on CPU).
+(rpbacore.cpp:100-510).  Across GPUs this library therefore splits work that
+is independent by nature:
+
+* replicas (one scene): every rank solves its own copy; the job's time is
+  the slowest rank's (max over ranks);
+* scene-parallel (many independent scenes, the batched workload): the scenes
+  are dealt to ranks by size (``shard``), every rank solves its share, the
+  per-scene results are gathered in scene order and the job's time is the
+  slowest rank's (``scene_parallel``).
+
+Only these host-side reductions and gathers cross ranks, through
+torch.distributed (NCCL on GPUs, gloo on CPU).
 """
 from __future__ import annotations
 
@@ -76,3 +82,34 @@ def time_steps(g: Group, step: Callable[[], float], steps: int, warmup: int,
     g.barrier()
     med = statistics.median(times)
     return {"times": times, "median": med, "max_over_ranks": g.max(med)}
+
+
+def shard(costs, world: int) -> list:
+    """Owner rank of every item: largest first to the least-loaded rank
+    (ties: lower index, lower rank), deterministic on every rank."""
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = [0.0] * world
+    owner = [0] * len(costs)
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[i] = r
+        load[r] += costs[i]
+    return owner
+
+
+def scene_parallel(g: Group, costs, solve: Callable[[list], tuple]) -> dict:
+    """Solve independent scenes split over the ranks.  ``solve(indices)``
+    runs this rank's scenes and returns (per-scene result dicts in the order
+    of ``indices``, its seconds).  Returns, on every rank, the results of all
+    scenes in scene order, the owner of each, and the job's seconds (max over
+    ranks of the ranks' seconds)."""
+    owner = shard(costs, g.world)
+    mine = [i for i, r in enumerate(owner) if r == g.rank]
+    g.barrier()
+    results, secs = solve(mine)
+    job = g.max(secs)
+    merged = [None] * len(costs)
+    for part in g.gather(list(zip(mine, results))):
+        for i, res in part:
+            merged[i] = res
+    return {"scenes": merged, "owner": owner, "job_seconds": job, "rank_seconds": secs}

@@ -79,9 +79,10 @@ def test_no_parameters_file_and_extra_argument(workdir):
 
 
 def test_partitioned_branch_header(tmp_path, oracle_mod):
-    """Partitioned=1 takes the reference's parallel branch where its rule
-    does (min(Threads, iround(images / 70)) > 1): the '#threads' line and one
-    'Thread:' line per partition, then the device is needed."""
+    """Threads selects the reference's parallel branch where its rule does
+    (min(Threads, iround(images / 70)) > 1, rpbacore.cpp:79-92): the
+    '#threads' line and one 'Thread:' line per partition, then the device is
+    needed; Threads=1 keeps the global branch."""
     import torch
     if torch.cuda.is_available():
         pytest.skip("a GPU is present: the solve would run")
@@ -90,13 +91,30 @@ def test_partitioned_branch_header(tmp_path, oracle_mod):
     blk = scenes.to_block(scenes.arc_scene(seed=2, n_cams=150, n_pts=600))
     (tmp_path / "data").mkdir()
     rb.OutputBlock(str(tmp_path / "data" / "scene.txt"), blk, k24out=True)
-    _params(tmp_path / "parameters", Threads="4", Partitioned="1")
+    _params(tmp_path / "parameters", Threads="4")
     r = _run(tmp_path)
     assert "#threads: 2 2" in r.stdout
     lines = [l for l in r.stdout.splitlines() if l.startswith("Thread: ")]
     assert len(lines) == 2 and sum(int(l.split()[3]) for l in lines) == blk.n_images
     assert "no CUDA device" in r.stderr and r.returncode == 2
     # the global branch below the rule's threshold: no partition lines
-    _params(tmp_path / "parameters", Threads="1", Partitioned="1")
+    _params(tmp_path / "parameters", Threads="1")
     r = _run(tmp_path)
     assert "#threads" not in r.stdout and r.returncode == 2
+
+
+def test_partition_count_follows_the_reference_rule(oracle_mod):
+    """rpba_partition_count against the rule restated by the oracle
+    (min(Threads, iround(images / 70)), partitioned above 1 with more than
+    five images, never with Exteval), including the rounding at the halves."""
+    import os
+    import rpba_b200 as rb
+    L = rb.load()
+    for n in (5, 6, 50, 104, 105, 106, 139, 140, 175, 13700):
+        for t in (1, 2, 3, 8, 64, 500):
+            want = oracle_mod.parallel_threads(n, t)
+            want = want if want > 1 and n > 5 else 1
+            assert L.rpba_partition_count(n, t, 0) == want, (n, t)
+            assert L.rpba_partition_count(n, t, 1) == 1
+    hw = os.cpu_count() or 1
+    assert L.rpba_partition_count(13700, 0, 0) == max(1, min(hw, 196)) if min(hw, 196) > 1 else 1

@@ -83,3 +83,62 @@ def test_replicas_failure_surfaces_as_error_not_hang():
     by = {o[1]: o for o in out}
     assert by[1][0] == "err" and "planted failure" in by[1][2]
     assert 0 in by and by[0][0] == "err", out  # the survivor's collective failed
+
+
+def test_shard_balances_and_is_deterministic():
+    from rpba_b200.replicas import shard
+    from rpba_b200 import scenes
+    costs = [kw["n_cams"] for kw in scenes.batch_scene_specs()]
+    for world in (1, 2, 3, 8):
+        own = shard(costs, world)
+        assert own == shard(costs, world) and sorted(set(own)) == list(range(world))
+        load = [sum(c for c, o in zip(costs, own) if o == r) for r in range(world)]
+        assert max(load) - min(load) <= max(costs)
+
+
+def _scene_worker(rank, world, port, q):
+    try:
+        from rpba_b200.replicas import Group, scene_parallel
+        import oracle
+        import rpba_b200 as rb
+        from rpba_b200 import scenes
+        g = Group(rank, world, backend="gloo", timeout_s=30.0, init_method=f"tcp://127.0.0.1:{port}")
+        specs = scenes.batch_scene_specs(n_scenes=6, cmin=8, cmax=16, pts_per_cam=40)
+
+        def solve(idx):
+            t0 = time.perf_counter()
+            out = []
+            for i in idx:
+                st, _, rep, _ = oracle.calc_plsa(scenes._arc_block(specs[i]), rb.make_options())
+                out.append({"status": st, "rms": rep["rms"], "rank": rank})
+            return out, time.perf_counter() - t0
+
+        res = scene_parallel(g, [kw["n_cams"] for kw in specs], solve)
+        q.put(("ok", rank, res))
+        g.close()
+    except Exception as e:
+        q.put(("err", rank, repr(e)))
+
+
+def test_scene_parallel_gloo():
+    """Batched scenes split over two gloo ranks: every scene solved exactly
+    once, by its owner, results gathered in scene order on both ranks, job
+    time = max over the ranks' times."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _port()
+    ps = [ctx.Process(target=_scene_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = [q.get(timeout=240) for _ in range(2)]
+    for p in ps:
+        p.join(timeout=10)
+    assert all(o[0] == "ok" for o in out), out
+    by = {o[1]: o[2] for o in out}
+    for r in (0, 1):
+        res = by[r]
+        assert len(res["scenes"]) == 6 and all(s is not None and s["status"] == 0 for s in res["scenes"])
+        assert [s["rank"] for s in res["scenes"]] == res["owner"]
+        assert res["job_seconds"] == pytest.approx(max(by[0]["rank_seconds"], by[1]["rank_seconds"]))
+    assert by[0]["scenes"] == by[1]["scenes"]
+    assert set(by[0]["owner"]) == {0, 1}

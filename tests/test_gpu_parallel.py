@@ -83,3 +83,28 @@ def test_parallel_loop_matches_oracle(oracle_mod, k):
     e_o, e_g = ev(b_o), ev(b_g)
     print(f"k={k}: Exteval sigma0 GPU {e_g:.7f} oracle {e_o:.7f}, {s_g['iterations']} iterations")
     assert abs(e_g - e_o) <= 1e-6 * e_o
+
+
+def test_calc_plsa_threads_selects_the_partitioned_branch(oracle_mod):
+    """rpba_calc_plsa with threads = 4 on a 150-image scene takes the
+    reference's partitioned branch (rpbacore.cpp:79-92: min(4, iround(150 /
+    70)) = 2 partitions): the log opens with the reference's '#threads: 2 2'
+    and 'Thread:' lines, and the block equals the partitioned loop's on the
+    same partition; threads = 1 keeps the global branch."""
+    import rpba_b200 as rb
+    from rpba_b200 import scenes
+    blk = scenes.to_block(scenes.arc_scene(seed=9, n_cams=150, n_pts=9000))
+    b = blk.copy()
+    st, log, rep = rb.CalcPLSA(b, threads=4, solver=rb.SOLVER_DIRECT)
+    assert st == 0, log[-2000:]
+    assert log.startswith("#threads: 2 2\n"), log[:200]
+    assert sum(1 for l in log.splitlines() if l.startswith("Thread: ")) == 2
+    part = oracle_mod.partition_images(blk, 2)
+    st_o, b_o, s_o, _ = oracle_mod.calc_plsa_parallel(blk, part, 2, rb.make_options(solver=rb.SOLVER_DIRECT))
+    assert st_o == 0
+    ev = lambda x: oracle_mod.exteval(x)[1]["exteval_sigma0"]
+    e_o, e_g = ev(b_o), ev(b)
+    print(f"Threads=4 branch: Exteval sigma0 GPU {e_g:.7f} oracle {e_o:.7f}")
+    assert abs(e_g - e_o) <= 1e-6 * e_o
+    st1, log1, _ = rb.CalcPLSA(blk.copy(), threads=1, solver=rb.SOLVER_DIRECT)
+    assert st1 == 0 and not log1.startswith("#threads")
