@@ -441,6 +441,14 @@ int32_t rpba_solve_batch(rpba_block *blocks, int32_t n, const rpba_options *opt,
  * created with rpba_options.verbose bit 1 (value 2) set.  No counterpart in
  * the reference (its only instrument is a wall-clock print, rpba.cpp:140). */
 int32_t rpba_kernel_stats(rpba_handle *h, char *json, size_t cap);
+/* The inverse of a dense symmetric positive definite n x n matrix (row
+ * major, host buffers; the lower triangle of A is read), computed by the
+ * library's tiled Cholesky factorisation and inverse on the FP64 tensor
+ * cores -- the kernel that inverts the learned solver's coarse operator --
+ * for checking it against an independent implementation.
+ * RPBA_ERR_SOLVER when A is not positive definite.  No counterpart in the
+ * reference. */
+int32_t rpba_spd_inverse(const double *A, int32_t n, double *Ainv, int32_t device);
 /* Test hook of the bounded device waits.  With extra_ctas = 1 every grid
  * barrier of the handle's persistent PCG waits for one CTA more than the
  * launch has -- an arrival that never comes -- for at most timeout_ns

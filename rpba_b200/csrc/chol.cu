@@ -1,0 +1,407 @@
+// chol.cu -- tiled FP64 Cholesky factorisation of symmetric positive definite
+// matrices held as 64 x 64 tiles, in one cooperative launch, with the tile
+// products on the FP64 tensor cores (mma.sync m8n8k4 f64; sm_100a has no
+// FP64 kind of tcgen05.mma).
+//
+// Storage: the lower triangle in tiles, row by row; tile row I holds the
+// tiles of columns fcol[I] .. I, with fcol nondecreasing (an envelope: a
+// dense matrix has fcol = 0).  A Cholesky factor keeps the envelope of its
+// matrix, so L overwrites A in place.  hrow[J] is the last tile row whose
+// envelope reaches column J.
+//
+// Right-looking, per tile column J:
+//   P  the diagonal tile is factored (one warp, shared memory) and inverted:
+//      L_JJ and L_JJ^-1 (Linv[J]);
+//   T  every tile below it: L_IJ = A_IJ L_JJ^-T, a tile product;
+//   U  the trailing tiles: A_IK -= L_IJ L_KJ^T for J < K <= I <= hrow[J].
+// Phases are separated by bounded grid barriers; the tiles of a phase are
+// dealt to the CTAs round robin.  The factorisation of tile J + 1 is done by
+// the CTA that applies its last update (in phase U of column J), so P costs
+// no barrier of its own.  A non-positive pivot sets bit 4 of the error word.
+//
+// For a dense matrix the same launch can go on to the inverse:
+//   X  = L^-1, right-looking by tile rows: X_Ij = Linv_I R_Ij (j <= I), then
+//        R_Kj -= L_KI X_Ij for K > I;
+//   A^-1 = X^T X, one output tile per work item, both triangles written.
+#include "gridsync.cuh"
+#include "internal.h"
+
+namespace rpba {
+
+namespace {
+
+constexpr int CT = 64;                  // tile edge
+constexpr int CLD = 68;                 // shared leading dimension: conflict-free fragment loads
+constexpr int CTH = 256;                // threads per CTA (8 warps)
+constexpr int TS = CT * CT;             // doubles per stored tile
+constexpr size_t CSMEM = 2 * CT * CLD * sizeof(double);
+
+struct Tiles {
+  double *L;               // tile storage (row major inside a tile, ld 64)
+  const long long *toff;   // [nt] first tile of row I
+  const int *fcol;         // [nt] first tile column of row I
+  const int *hrow;         // [nt] last tile row reaching column J
+  double *Linv;            // [nt][TS] inverses of the diagonal tiles
+  double *X;               // dense inverse only: [nt(nt+1)/2][TS] L^-1, lower tiles
+  double *Ainv;            // dense inverse only: [nt(nt+1)/2][TS] A^-1, lower tiles
+  int nt;
+  int want_inverse;
+  unsigned *bar;
+  int *err;
+  unsigned long long bar_ns;
+};
+
+__device__ __forceinline__ double *tile_at(const Tiles &T, int I, int J) {
+  return T.L + (size_t)(T.toff[I] + (J - T.fcol[I])) * TS;
+}
+__device__ __forceinline__ size_t tri(int I, int J) { return (size_t)I * (I + 1) / 2 + J; }
+
+// D (8x8, two per thread) += A (8x4, one per thread) * B (4x8, one per thread)
+__device__ __forceinline__ void dmma(double &d0, double &d1, double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d0), "+d"(d1)
+               : "d"(a), "d"(b));
+}
+
+// acc (warp w: rows 8w .. 8w + 7, all 64 columns, 8 fragments of 2) +=
+// sA sB^T over k = 0 .. 63; sA, sB in shared memory with ld CLD.
+__device__ __forceinline__ void gemm_nt(const double *sA, const double *sB, double (&acc)[8][2]) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const double *pa = sA + (8 * w + g) * CLD + t;
+  const double *pb = sB + g * CLD + t;
+#pragma unroll 4
+  for (int kk = 0; kk < CT / 4; ++kk) {
+    const double a = pa[4 * kk];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) dmma(acc[j][0], acc[j][1], a, pb[8 * j * CLD + 4 * kk]);
+  }
+}
+
+// Global tile (ld 64) -> shared (ld CLD), optionally transposed.
+__device__ __forceinline__ void load_tile(double *s, const double *g, bool trans) {
+  for (int idx = threadIdx.x; idx < TS; idx += CTH) {
+    const int i = idx >> 6, j = idx & 63;
+    if (trans)
+      s[j * CLD + i] = __ldcg(g + idx);
+    else
+      s[i * CLD + j] = __ldcg(g + idx);
+  }
+}
+
+// Fragment positions of acc[j][e]: row 8w + g, column 8j + 2t + e.
+template <class F>
+__device__ __forceinline__ void for_frag(F f) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int r = 8 * w + (lane >> 2), c0 = 2 * (lane & 3);
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    f(j, 0, r, 8 * j + c0);
+    f(j, 1, r, 8 * j + c0 + 1);
+  }
+}
+
+// Factor the diagonal tile in place (one warp factors, then one warp
+// inverts; the other warps wait at the block barriers) and write L_JJ and
+// L_JJ^-1.  s and si: two shared tiles (ld CT + 1).
+__device__ void potrf_tile(double *gtile, double *ginv, int *err, double *s, double *si) {
+  constexpr int LD = CT + 1;
+  const int lane = threadIdx.x & 31;
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < TS; idx += CTH) s[(idx >> 6) * LD + (idx & 63)] = __ldcg(gtile + idx);
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    for (int k = 0; k < CT; ++k) {
+      const double d = s[k * LD + k];
+      if (!(d > 0.) && lane == 0) atomicOr(err, 4);
+      const double dk = sqrt(d > 0. ? d : 1.);
+      __syncwarp();
+      if (lane == 0) s[k * LD + k] = dk;
+      for (int i = k + 1 + lane; i < CT; i += 32) s[i * LD + k] /= dk;
+      __syncwarp();
+      for (int i = k + 1 + lane; i < CT; i += 32) {
+        const double lik = s[i * LD + k];
+        for (int j = k + 1; j <= i; ++j) s[i * LD + j] -= lik * s[j * LD + k];
+      }
+      __syncwarp();
+    }
+    // L^-1 row by row: columns c = lane, lane + 32; four partial sums
+    for (int i = 0; i < CT; ++i) {
+      const double dii = s[i * LD + i];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int c = lane + 32 * h;
+        double v = 0.;
+        if (c < i) {
+          double p0 = 0., p1 = 0., p2 = 0., p3 = 0.;
+          int m = c;
+          for (; m + 3 < i; m += 4) {
+            p0 += s[i * LD + m] * si[m * LD + c];
+            p1 += s[i * LD + m + 1] * si[(m + 1) * LD + c];
+            p2 += s[i * LD + m + 2] * si[(m + 2) * LD + c];
+            p3 += s[i * LD + m + 3] * si[(m + 3) * LD + c];
+          }
+          for (; m < i; ++m) p0 += s[i * LD + m] * si[m * LD + c];
+          v = -((p0 + p1) + (p2 + p3)) / dii;
+        } else if (c == i) {
+          v = 1. / dii;
+        }
+        si[i * LD + c] = v;
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < TS; idx += CTH) {
+    const int i = idx >> 6, j = idx & 63;
+    gtile[idx] = j <= i ? s[i * LD + j] : 0.;
+    ginv[idx] = si[i * LD + j];
+  }
+  __syncthreads();
+}
+
+// k-th item of the lower triangle (bi >= bk) of an m x m tile triangle
+__device__ __forceinline__ void tri_item(long long t, int &bi, int &bk) {
+  int i = (int)((sqrt(8. * (double)t + 1.) - 1.) / 2.);
+  while ((long long)(i + 1) * (i + 2) / 2 <= t) ++i;
+  while ((long long)i * (i + 1) / 2 > t) --i;
+  bi = i;
+  bk = (int)(t - (long long)i * (i + 1) / 2);
+}
+
+__global__ void __launch_bounds__(CTH, 1) k_chol_tiles(Tiles T) {
+  extern __shared__ __align__(16) double csm[];
+  double *sA = csm, *sB = csm + CT * CLD;
+  const int G = gridDim.x;
+  const unsigned nb = (unsigned)G;
+  // tile 0's diagonal block
+  if (blockIdx.x == 0) potrf_tile(tile_at(T, 0, 0), T.Linv, T.err, sA, sB);
+  if (!grid_barrier(T.bar, nb, T.err, T.bar_ns)) return;
+  for (int J = 0; J < T.nt; ++J) {
+    const int h = T.hrow[J], m = h - J;
+    // T: L_IJ = A_IJ L_JJ^-T
+    if (m > 0) {
+      bool have = false;
+      for (int t = blockIdx.x; t < m; t += G) {
+        const int I = J + 1 + t;
+        double *gt = tile_at(T, I, J);
+        if (!have) {
+          __syncthreads();
+          load_tile(sB, T.Linv + (size_t)J * TS, false);
+          have = true;
+        }
+        load_tile(sA, gt, false);
+        __syncthreads();
+        double acc[8][2] = {};
+        gemm_nt(sA, sB, acc);
+        __syncthreads();
+        for_frag([&](int j, int e, int r, int c) { gt[r * CT + c] = acc[j][e]; });
+      }
+    }
+    if (!grid_barrier(T.bar, nb, T.err, T.bar_ns)) return;
+    // U: A_IK -= L_IJ L_KJ^T; the tile (J+1, J+1) is then factored by its CTA
+    const long long nu = (long long)m * (m + 1) / 2;
+    for (long long t = blockIdx.x; t < nu; t += G) {
+      int bi, bk;
+      tri_item(t, bi, bk);
+      const int I = J + 1 + bi, K = J + 1 + bk;
+      __syncthreads();
+      load_tile(sA, tile_at(T, I, J), false);
+      load_tile(sB, tile_at(T, K, J), false);
+      __syncthreads();
+      double acc[8][2] = {};
+      gemm_nt(sA, sB, acc);
+      double *gt = tile_at(T, I, K);
+      for_frag([&](int j, int e, int r, int c) { gt[r * CT + c] -= acc[j][e]; });
+      if (bi == 0 && bk == 0) {
+        __syncthreads();
+        potrf_tile(gt, T.Linv + (size_t)(J + 1) * TS, T.err, sA, sB);
+      }
+    }
+    if (m == 0 && J + 1 < T.nt && blockIdx.x == (J + 1) % G)
+      potrf_tile(tile_at(T, J + 1, J + 1), T.Linv + (size_t)(J + 1) * TS, T.err, sA, sB);
+    if (!grid_barrier(T.bar, nb, T.err, T.bar_ns)) return;
+  }
+  if (!T.want_inverse) return;
+  // X = L^-1 (dense): X holds R (initially the identity) and becomes X
+  const int nt = T.nt;
+  for (int I = 0; I < nt; ++I) {
+    // X_Ij = Linv_I R_Ij, j <= I
+    bool have = false;
+    for (int j = blockIdx.x; j <= I; j += G) {
+      double *gx = T.X + tri(I, j) * TS;
+      if (!have) {
+        __syncthreads();
+        load_tile(sA, T.Linv + (size_t)I * TS, false);
+        have = true;
+      }
+      load_tile(sB, gx, true);  // R^T: the product Linv R as Linv (R^T)^T
+      __syncthreads();
+      double acc[8][2] = {};
+      gemm_nt(sA, sB, acc);
+      __syncthreads();
+      for_frag([&](int jj, int e, int r, int c) { gx[r * CT + c] = acc[jj][e]; });
+    }
+    if (!grid_barrier(T.bar, nb, T.err, T.bar_ns)) return;
+    // R_Kj -= L_KI X_Ij, K > I, j <= I
+    const long long nu = (long long)(nt - 1 - I) * (I + 1);
+    for (long long t = blockIdx.x; t < nu; t += G) {
+      const int K = I + 1 + (int)(t / (I + 1)), j = (int)(t % (I + 1));
+      __syncthreads();
+      load_tile(sA, tile_at(T, K, I), false);
+      load_tile(sB, T.X + tri(I, j) * TS, true);
+      __syncthreads();
+      double acc[8][2] = {};
+      gemm_nt(sA, sB, acc);
+      double *gr = T.X + tri(K, j) * TS;
+      for_frag([&](int jj, int e, int r, int c) { gr[r * CT + c] -= acc[jj][e]; });
+    }
+    if (!grid_barrier(T.bar, nb, T.err, T.bar_ns)) return;
+  }
+  // A^-1 tile (i, k), k <= i: sum over m >= i of X_mi^T X_mk
+  const long long no = (long long)nt * (nt + 1) / 2;
+  for (long long t = blockIdx.x; t < no; t += G) {
+    int bi, bk;
+    tri_item(t, bi, bk);
+    double acc[8][2] = {};
+    for (int mt = bi; mt < nt; ++mt) {
+      __syncthreads();
+      load_tile(sA, T.X + tri(mt, bi) * TS, true);
+      load_tile(sB, T.X + tri(mt, bk) * TS, true);
+      __syncthreads();
+      gemm_nt(sA, sB, acc);
+    }
+    double *ga = T.Ainv + tri(bi, bk) * TS;
+    for_frag([&](int j, int e, int r, int c) { ga[r * CT + c] = acc[j][e]; });
+  }
+}
+
+// Dense n x n row-major (lower triangle used), scaled by d_i d_j (+ eps on
+// the diagonal), into lower tiles; the padding of the last diagonal tile is
+// the identity.  X starts as the identity (diagonal tiles), zero elsewhere.
+__global__ void k_pack_dense(const double *A, const double *dsc, double eps, int n, int nt, double *Lt, double *X) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long ntile = (long long)nt * (nt + 1) / 2;
+  if (idx >= ntile * TS) return;
+  const long long t = idx / TS;
+  const int e = (int)(idx % TS), a = e >> 6, b = e & 63;
+  int I, J;
+  tri_item(t, I, J);
+  const int i = I * CT + a, j = J * CT + b;
+  double v = 0.;
+  if (i < n && j < n) {
+    if (j <= i) {
+      v = A[(size_t)i * n + j] * dsc[i] * dsc[j];
+      if (i == j) v += eps;
+    }
+  } else if (i == j) {
+    v = 1.;
+  }
+  Lt[idx] = v;
+  X[idx] = (i == j) ? 1. : 0.;
+}
+
+// Lower inverse tiles back to the dense matrix (both triangles), scaled.
+__global__ void k_unpack_dense(const double *At, const double *dsc, int n, int nt, double *Ainv) {
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long ntile = (long long)nt * (nt + 1) / 2;
+  if (idx >= ntile * TS) return;
+  const long long t = idx / TS;
+  const int e = (int)(idx % TS), a = e >> 6, b = e & 63;
+  int I, J;
+  tri_item(t, I, J);
+  const int i = I * CT + a, j = J * CT + b;
+  if (i >= n || j >= n || (I == J && b > a)) return;
+  const double v = At[idx] * dsc[i] * dsc[j];
+  Ainv[(size_t)i * n + j] = v;
+  Ainv[(size_t)j * n + i] = v;
+}
+
+__global__ void k_dense_meta(int nt, long long *toff, int *fcol, int *hrow) {
+  const int I = blockIdx.x * blockDim.x + threadIdx.x;
+  if (I >= nt) return;
+  toff[I] = (long long)I * (I + 1) / 2;
+  fcol[I] = 0;
+  hrow[I] = nt - 1;
+}
+
+// one CTA per SM (fewer arrivals per grid barrier); 0 if none fits
+int chol_grid() {
+  int dev = 0, nsm = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaFuncSetAttribute(k_chol_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CSMEM);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_chol_tiles, CTH, CSMEM);
+  return per >= 1 ? nsm : 0;
+}
+
+}  // namespace
+
+// Factor the envelope tiles in place (L over A) and write the inverses of
+// the diagonal tiles; one cooperative launch.
+void tile_cholesky(double *tiles, const long long *toff, const int *fcol, const int *hrow, double *Linv, int nt,
+                   unsigned *bar, int *err, cudaStream_t s) {
+  if (nt <= 0) return;
+  Tiles T;
+  T.L = tiles;
+  T.toff = toff;
+  T.fcol = fcol;
+  T.hrow = hrow;
+  T.Linv = Linv;
+  T.X = nullptr;
+  T.Ainv = nullptr;
+  T.nt = nt;
+  T.want_inverse = 0;
+  T.bar = bar;
+  T.err = err;
+  T.bar_ns = BAR_TIMEOUT_NS;
+  const int g = std::max(1, chol_grid());
+  RPBA_CUDA_CHECK(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s));
+  void *args[] = {&T};
+  RPBA_CUDA_CHECK(cudaLaunchCooperativeKernel((const void *)k_chol_tiles, dim3(g), dim3(CTH), args, CSMEM, s));
+}
+
+size_t spd_inverse_bytes(int n) {
+  const long long nt = (n + CT - 1) / CT;
+  return (size_t)(3 * (nt * (nt + 1) / 2) + nt) * TS * sizeof(double) + nt * 16 + 64;
+}
+
+// A^-1 of the dense SPD matrix (D A D + eps I) scaled back by D, with D =
+// diag(dsc): A (row major n x n, lower triangle used) -> Ainv (both
+// triangles).  One cooperative launch for the factorisation and the inverse.
+void spd_inverse_scaled(const double *A, const double *dsc, double eps, int n, double *Ainv, void *work,
+                        unsigned *bar, int *err, cudaStream_t s) {
+  if (n <= 0) return;
+  const int nt = (n + CT - 1) / CT;
+  const long long ntile = (long long)nt * (nt + 1) / 2;
+  double *Lt = (double *)work;
+  double *X = Lt + ntile * TS;
+  double *At = X + ntile * TS;
+  double *Linv = At + ntile * TS;
+  long long *toff = (long long *)(Linv + (size_t)nt * TS);
+  int *fcol = (int *)(toff + nt);
+  int *hrow = fcol + nt;
+  k_dense_meta<<<(nt + 127) / 128, 128, 0, s>>>(nt, toff, fcol, hrow);
+  k_pack_dense<<<(int)((ntile * TS + 255) / 256), 256, 0, s>>>(A, dsc, eps, n, nt, Lt, X);
+  Tiles T;
+  T.L = Lt;
+  T.toff = toff;
+  T.fcol = fcol;
+  T.hrow = hrow;
+  T.Linv = Linv;
+  T.X = X;
+  T.Ainv = At;
+  T.nt = nt;
+  T.want_inverse = 1;
+  T.bar = bar;
+  T.err = err;
+  T.bar_ns = BAR_TIMEOUT_NS;
+  const int g = (int)std::max<long long>(1, std::min<long long>(chol_grid(), ntile));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s));
+  void *args[] = {&T};
+  RPBA_CUDA_CHECK(cudaLaunchCooperativeKernel((const void *)k_chol_tiles, dim3(g), dim3(CTH), args, CSMEM, s));
+  k_unpack_dense<<<(int)((ntile * TS + 255) / 256), 256, 0, s>>>(At, dsc, n, nt, Ainv);
+  RPBA_CUDA_CHECK(cudaGetLastError());
+}
+
+}  // namespace rpba

@@ -202,14 +202,6 @@ __global__ void k_coarse_diag(CoarseWork C) {
   const double d = C.Ac[(size_t)i * C.nc + i];
   C.dsc[i] = d > 0. ? 1. / sqrt(d) : 1.;
 }
-__global__ void k_coarse_scale(double *A, const double *dsc, int n, int add_diag) {
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= (long long)n * n) return;
-  const int i = (int)(g / n), j = (int)(g % n);
-  double v = A[g] * dsc[i] * dsc[j];
-  if (add_diag && i == j) v += 1e-6;
-  A[g] = v;
-}
 
 // rc_a = sum_{k in a} P_k^T r_k (rows in order)
 __global__ void k_coarse_restrict(CoarseWork C, const double *r) {
@@ -337,18 +329,17 @@ void coarse_build(const DevLSA &L, int max_aggs, CoarseWork &C, std::vector<void
   C.row_agg = calloc_dev<int>(nimg, owned);
   C.P = calloc_dev<double>((size_t)nimg * CP, owned);
   C.Ac = calloc_dev<double>(nc * nc, owned);
-  C.X = calloc_dev<double>(nc * nc, owned);
   C.Ainv = calloc_dev<double>(nc * nc, owned);
-  C.Linv = calloc_dev<double>((nc + 63) / 64 * 64 * 64, owned);
   C.rc = calloc_dev<double>(nc, owned);
   C.dsc = calloc_dev<double>(nc, owned);
   C.hj = calloc_dev<double>((size_t)nimg * 9, owned);
   C.err = calloc_dev<int>(1, owned);
+  C.work = calloc_dev<char>(spd_inverse_bytes((int)nc), owned);
+  C.bar = calloc_dev<unsigned>(2, owned);
   RPBA_CUDA_CHECK(cudaMemcpyAsync(C.agg_off, off.data(), sizeof(int) * (nagg + 1), cudaMemcpyHostToDevice, s));
   RPBA_CUDA_CHECK(cudaMemcpyAsync(C.agg_rows, rows.data(), sizeof(int) * rows.size(), cudaMemcpyHostToDevice, s));
   RPBA_CUDA_CHECK(cudaMemcpyAsync(C.row_agg, row_agg.data(), sizeof(int) * nimg, cudaMemcpyHostToDevice, s));
   RPBA_CUDA_CHECK(cudaMemsetAsync(C.P, 0, sizeof(double) * (size_t)nimg * CP, s));
-  RPBA_CUDA_CHECK(cudaMemsetAsync(C.X, 0, sizeof(double) * nc * nc, s));
   RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
 }
 
@@ -450,12 +441,10 @@ void coarse_assemble(const DevLSA &L, CoarseWork &C, int structure_version, cuda
 
 void coarse_factor(CoarseWork &C, cudaStream_t s) {
   if (C.nagg <= 0) return;
-  const size_t nn = (size_t)C.nc * C.nc;
+  // Jacobi scaling, then the scaled matrix plus 1e-6 on its diagonal is
+  // factored and inverted in one launch, and the inverse scaled back
   k_coarse_diag<<<(C.nc + 255) / 256, 256, 0, s>>>(C);
-  k_coarse_scale<<<(int)((nn + 255) / 256), 256, 0, s>>>(C.Ac, C.dsc, C.nc, 1);
-  dense_cholesky(C.Ac, C.nc, C.Linv, C.err, s);
-  dense_spd_inverse(C.Ac, C.nc, C.Linv, C.X, C.Ainv, s);
-  k_coarse_scale<<<(int)((nn + 255) / 256), 256, 0, s>>>(C.Ainv, C.dsc, C.nc, 0);
+  spd_inverse_scaled(C.Ac, C.dsc, 1e-6, C.nc, C.Ainv, C.work, C.bar, C.err, s);
   RPBA_CUDA_CHECK(cudaGetLastError());
 }
 

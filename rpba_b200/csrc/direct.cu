@@ -1,15 +1,26 @@
-// direct.cu -- dense FP64 Cholesky solve of the reduced camera system (the
+// direct.cu -- sparse direct Cholesky solve of the reduced camera system (the
 // plain direct form; the reference itself only runs PCG, rbacore.cpp:1176).
 //
-// The system (camera blocks k >= begini, sizes np_k, compact offsets) is
-// expanded into a dense row-major n x n lower triangle, factored L L^T by a
-// right-looking blocked algorithm with T x T tiles:
-//   potrf   one CTA factors the diagonal tile in shared memory and writes
-//           L_jj^-1 (also a lower triangle)
-//   trsm    every tile below it: A_ij <- A_ij L_jj^-T (a T x T x T product)
-//   syrk    trailing lower triangle: A_ik -= A_ij A_kj^T
-// then solved by blocked forward and back substitution.  A non-positive
-// pivot sets an error bit; the host reports RPBA_ERR_SOLVER.
+// Symbolic part (host, once per structure): the cameras of the system are
+// ordered by reverse Cuthill-McKee on their covisibility graph, which keeps
+// the nonzeros near the diagonal on chain-like (street) and grid-like
+// (aerial) scenes.  In that order the unknowns' envelope -- for every row
+// the first column any covisible camera reaches -- holds the Cholesky factor
+// exactly (a factor has no fill outside the envelope of its matrix).  The
+// envelope is kept at 64 x 64 tile granularity, its left edge made
+// nondecreasing (rows with a longer reach widen the rows above them).
+//
+// Numeric part (device, per linear system): the blocks are scattered into
+// the envelope tiles, the tiles factored in one cooperative launch
+// (chol.cu: right-looking, tile products on the FP64 tensor cores), and the
+// system solved by forward and back substitution over the tiles in one more
+// cooperative launch (one grid barrier per tile row and direction).  A
+// non-positive pivot sets bit 4 of the error word (RPBA_ERR_SOLVER).
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "gridsync.cuh"
 #include "internal.h"
 
 namespace rpba {
@@ -17,413 +28,371 @@ namespace rpba {
 namespace {
 
 constexpr int T = 64;
-constexpr int DT = 256;
+constexpr int TS = T * T;
+constexpr int ST = 256;  // threads per CTA of the solve
 
-// diagonal blocks into the dense lower triangle
-__global__ void k_dense_fill(DevLSA L, const int *coff, int n, double *A) {
+__global__ void k_env_diag_pad(double *tiles, const long long *toff, const int *fcol, int nt, int n) {
+  const int r = n + blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nt * T) return;
+  const int I = r / T, a = r % T;
+  tiles[(size_t)(toff[I] + (I - fcol[I])) * TS + a * T + a] = 1.;
+}
+
+__device__ __forceinline__ void env_put(double *tiles, const long long *toff, const int *fcol, int R, int C,
+                                        double v) {
+  if (C > R) {
+    const int t = R;
+    R = C;
+    C = t;
+  }
+  const int I = R / T, J = C / T;
+  tiles[(size_t)(toff[I] + (J - fcol[I])) * TS + (R % T) * T + (C % T)] = v;
+}
+
+// diagonal blocks: entries on and below the diagonal (as assembled)
+__global__ void k_env_fill_diag(DevLSA L, const int *pos, double *tiles, const long long *toff, const int *fcol) {
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int r = (int)(gid / 81) + L.begini;
   if (r >= L.nimg) return;
-  const int e = (int)(gid % 81);
+  const int e = (int)(gid % 81), i = e / 9, j = e % 9;
   const int nr = L.camparv[r + 1] - L.camparv[r];
-  const int i = e / 9, j = e % 9;
   if (i >= nr || j > i) return;
-  A[(size_t)(coff[r] + i) * n + coff[r] + j] = blk_at(L, (size_t)r, e);
+  env_put(tiles, toff, fcol, pos[r] + i, pos[r] + j, blk_at(L, (size_t)r, e));
 }
 
-// off-diagonal blocks through the row entries: row r, column c > r,
-// block (r, c) stored row major (r params x c params); the dense lower
-// triangle gets its transpose at (c, r)
-__global__ void k_dense_fill_off(DevLSA L, const int *coff, int n, double *A) {
+// off-diagonal blocks (row r, column c > r, stored r params x c params)
+__global__ void k_env_fill_off(DevLSA L, const unsigned *bkey, const int *pos, double *tiles, const long long *toff,
+                               const int *fcol) {
   const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int row = (int)(gid / 81) + L.begini;
-  if (row >= L.nimg) return;
-  const int e = (int)(gid % 81);
-  const int i = e / 9, j = e % 9;
-  const int nr = L.camparv[row + 1] - L.camparv[row];
-  if (i >= nr) return;
-  for (int t = L.rowoff[row]; t < L.rowoff[row + 1]; ++t) {
-    const int2 en = L.ent[t];
-    if (en.y < 0 || en.x <= row) continue;  // normal entries right of the diagonal
-    const int col = en.x;
-    const int nc = L.camparv[col + 1] - L.camparv[col];
-    if (j >= nc) continue;
-    A[(size_t)(coff[col] + j) * n + coff[row] + i] = blk_at(L, (size_t)en.y, i * 9 + j);
-  }
+  const long long b = gid / 81;
+  if (b >= L.nboff) return;
+  const int e = (int)(gid % 81), i = e / 9, j = e % 9;
+  const unsigned key = bkey[b];
+  const int r = (int)(key / (unsigned)L.nimg), c = (int)(key % (unsigned)L.nimg);
+  const int nr = L.camparv[r + 1] - L.camparv[r], nc = L.camparv[c + 1] - L.camparv[c];
+  if (i >= nr || j >= nc) return;
+  env_put(tiles, toff, fcol, pos[r] + i, pos[c] + j, blk_at(L, (size_t)L.nimg + b, e));
 }
 
-__global__ void k_gather_rhs(DevLSA L, const int *coff, double *y) {
+__global__ void k_env_gather(DevLSA L, const int *pos, const double *b, double *y) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x + L.begini;
   if (k >= L.nimg) return;
   const int np = L.camparv[k + 1] - L.camparv[k];
-  for (int a = 0; a < np; ++a) y[coff[k] + a] = L.rhs[(size_t)k * 9 + a];
+  const double *src = b ? b + (size_t)k * 9 : L.rhs + (size_t)k * 9;
+  for (int a = 0; a < np; ++a) y[pos[k] + a] = src[a];
 }
 
-__global__ void k_gather_vec(DevLSA L, const int *coff, const double *b, double *y) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x + L.begini;
-  if (k >= L.nimg) return;
-  const int np = L.camparv[k + 1] - L.camparv[k];
-  for (int a = 0; a < np; ++a) y[coff[k] + a] = b[(size_t)k * 9 + a];
-}
-
-__global__ void k_scatter_solution(DevLSA L, const int *coff, const double *y, double *xsol) {
+__global__ void k_env_scatter(DevLSA L, const int *pos, const double *y, double *xsol) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= L.nimg) return;
-  for (int a = 0; a < 9; ++a) {
-    const int np = L.camparv[k + 1] - L.camparv[k];
-    xsol[(size_t)k * 9 + a] = (k >= L.begini && a < np) ? y[coff[k] + a] : 0.;
-  }
+  const int np = L.camparv[k + 1] - L.camparv[k];
+  for (int a = 0; a < 9; ++a) xsol[(size_t)k * 9 + a] = (k >= L.begini && a < np) ? y[pos[k] + a] : 0.;
 }
 
-// Factor the diagonal tile at j0 (size tb <= T) in shared memory; writes
-// L back into A and L^-1 into Linv (T x T, row major).
-constexpr int SMEM2 = 2 * T * (T + 1) * sizeof(double);  // two padded tiles (66.5 KB)
+struct SolveArgs {
+  const double *tiles, *Linv;
+  const long long *toff;
+  const int *fcol, *hrow;
+  double *y;
+  int nt;
+  unsigned *bar;
+  int *err;
+  unsigned long long bar_ns;
+};
 
-__global__ void __launch_bounds__(DT) k_potrf(double *A, int n, int j0, int tb, double *Linv, int *err) {
-  extern __shared__ double dyn[];
-  double(*s)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn);
-  double(*inv)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn + T * (T + 1));
-  const int tid = threadIdx.x;
-  for (int idx = tid; idx < T * T; idx += DT) {
-    const int i = idx / T, j = idx % T;
-    s[i][j] = (i < tb && j <= i) ? A[(size_t)(j0 + i) * n + j0 + j] : (i == j ? 1. : 0.);
-  }
-  __syncthreads();
-  for (int k = 0; k < tb; ++k) {
-    if (tid == 0) {
-      const double d = s[k][k];
-      if (!(d > 0.)) atomicOr(err, 4);
-      s[k][k] = sqrt(d > 0. ? d : 1.);
-    }
-    __syncthreads();
-    const double dk = s[k][k];
-    for (int i = k + 1 + tid; i < tb; i += DT) s[i][k] /= dk;
-    __syncthreads();
-    for (int idx = tid; idx < (tb - k - 1) * (tb - k - 1); idx += DT) {
-      const int i = k + 1 + idx / (tb - k - 1), j = k + 1 + idx % (tb - k - 1);
-      if (j <= i) s[i][j] -= s[i][k] * s[j][k];
-    }
-    __syncthreads();
-  }
-  // L^-1 by forward substitution, one column per thread
-  for (int c = tid; c < T; c += DT) {
-    for (int i = 0; i < T; ++i) {
-      double v = (i == c) ? 1. : 0.;
-      for (int m = c; m < i; ++m) v -= s[i][m] * inv[m][c];
-      inv[i][c] = (i >= c) ? v / s[i][i] : 0.;
-    }
-  }
-  __syncthreads();
-  for (int idx = tid; idx < T * T; idx += DT) {
-    const int i = idx / T, j = idx % T;
-    if (i < tb && j <= i) A[(size_t)(j0 + i) * n + j0 + j] = s[i][j];
-    Linv[idx] = inv[i][j];
-  }
+__device__ __forceinline__ const double *etile(const SolveArgs &A, int I, int J) {
+  return A.tiles + (size_t)(A.toff[I] + (J - A.fcol[I])) * TS;
 }
 
-// Tiles below the diagonal tile: A_ij <- A_ij L^-T.  One CTA per tile row
-// (rows r0 .. r0 + T of the panel).
-__global__ void __launch_bounds__(DT) k_trsm(double *A, int n, int j0, int tb, const double *Linv) {
-  extern __shared__ double dyn[];
-  double(*a)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn);
-  double(*li)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn + T * (T + 1));
-  const int r0 = j0 + tb + blockIdx.x * T;
-  const int rb = min(T, n - r0);
-  const int tid = threadIdx.x;
-  for (int idx = tid; idx < T * T; idx += DT) {
-    const int i = idx / T, j = idx % T;
-    a[i][j] = (i < rb && j < tb) ? A[(size_t)(r0 + i) * n + j0 + j] : 0.;
-    li[i][j] = Linv[idx];
-  }
+// y_I -= M y_J (trans = 0) or y_I -= M^T y_J (trans = 1) for a 64 x 64 tile M
+__device__ void tile_gemv_sub(const double *M, const double *yj, double *yi, bool trans, double *sv, double *sp) {
+  const int t = threadIdx.x;
   __syncthreads();
-  // out[i][j] = sum_m a[i][m] * li[j][m]  (L^-T), 4 x 4 outputs per thread
-  const int ti = (tid / 16) * 4, tj = (tid % 16) * 4;
-  double o[4][4] = {};
-  for (int m = 0; m < tb; ++m) {
-    double av[4], bv[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      av[u] = a[ti + u][m];
-      bv[u] = li[tj + u][m];
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int v = 0; v < 4; ++v) o[u][v] += av[u] * bv[v];
-  }
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v)
-      if (ti + u < rb && tj + v < tb) A[(size_t)(r0 + ti + u) * n + j0 + tj + v] = o[u][v];
-}
-
-// Trailing update of the lower triangle: tile (bi, bk), bk <= bi, of the
-// rows/columns after the panel: A_ik -= P_i P_k^T.
-__global__ void __launch_bounds__(DT) k_syrk(double *A, int n, int j0, int tb, int m) {
-  // blockIdx.x enumerates the m (m + 1) / 2 lower tiles
-  const int t = blockIdx.x;
-  int bi = (int)((sqrt(8. * t + 1.) - 1.) / 2.);
-  while ((bi + 1) * (bi + 2) / 2 <= t) ++bi;
-  while (bi * (bi + 1) / 2 > t) --bi;
-  const int bk = t - bi * (bi + 1) / 2;
-  const int base = j0 + tb;
-  const int ri = base + bi * T, rk = base + bk * T;
-  const int nbi = min(T, n - ri), nbk = min(T, n - rk);
-  extern __shared__ double dyn[];
-  double(*pi)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn);
-  double(*pk)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn + T * (T + 1));
-  const int tid = threadIdx.x;
-  for (int idx = tid; idx < T * T; idx += DT) {
-    const int i = idx / T, j = idx % T;
-    pi[i][j] = (i < nbi && j < tb) ? A[(size_t)(ri + i) * n + j0 + j] : 0.;
-    pk[i][j] = (i < nbk && j < tb) ? A[(size_t)(rk + i) * n + j0 + j] : 0.;
-  }
+  if (t < T) sv[t] = __ldcg(yj + t);
   __syncthreads();
-  const int ti = (tid / 16) * 4, tj = (tid % 16) * 4;
-  double o[4][4] = {};
-  for (int mm = 0; mm < tb; ++mm) {
-    double av[4], bv[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      av[u] = pi[ti + u][mm];
-      bv[u] = pk[tj + u][mm];
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int v = 0; v < 4; ++v) o[u][v] += av[u] * bv[v];
-  }
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const int gi = ri + ti + u, gk = rk + tj + v;
-      if (ti + u < nbi && tj + v < nbk && gk <= gi) A[(size_t)gi * n + gk] -= o[u][v];
-    }
-}
-
-// Forward substitution on a tile: y_j <- L_jj^-1 y_j (single CTA).
-__global__ void k_tile_solve(const double *Linv, int tb, double *y, int j0, int transpose) {
-  __shared__ double v[T];
-  const int tid = threadIdx.x;
-  if (tid < T) v[tid] = tid < tb ? y[j0 + tid] : 0.;
-  __syncthreads();
-  if (tid < tb) {
+  if (!trans) {
+    // row r = t / 4, columns 16 (t % 4) .. + 16
+    const int r = t >> 2, c0 = (t & 3) * 16;
     double s = 0.;
-    if (!transpose)
-      for (int m = 0; m <= tid; ++m) s += Linv[tid * T + m] * v[m];
-    else
-      for (int m = tid; m < tb; ++m) s += Linv[m * T + tid] * v[m];
-    y[j0 + tid] = s;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) s += __ldcg(M + r * T + c0 + c) * sv[c0 + c];
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    if ((t & 3) == 0) yi[r] = __ldcg(yi + r) - s;
+  } else {
+    // column c = t % 64, rows 16 (t / 64) .. + 16
+    const int c = t & 63, r0 = (t >> 6) * 16;
+    double s = 0.;
+#pragma unroll
+    for (int r = 0; r < 16; ++r) s += __ldcg(M + (r0 + r) * T + c) * sv[r0 + r];
+    sp[t] = s;
+    __syncthreads();
+    if (t < T) yi[t] = __ldcg(yi + t) - ((sp[t] + sp[t + 64]) + (sp[t + 128] + sp[t + 192]));
   }
+  __syncthreads();
 }
 
-// y[i] -= sum_{m in panel} L[i][j0 + m] y[j0 + m] for rows i >= j0 + tb
-// (forward) ; y[i] -= sum_{m in panel} L[j0 + m][i] y[j0 + m] for i < j0
-// (backward).  One warp per row.
-__global__ void k_panel_update(const double *A, int n, int j0, int tb, double *y, int backward) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-  const int i = backward ? warp : j0 + tb + warp;
-  if ((backward && i >= j0) || (!backward && i >= n)) return;
+// y_J = Linv_J y_J (trans = 0) or Linv_J^T y_J (trans = 1)
+__device__ void tile_gemv_set(const double *Li, double *yj, bool trans, double *sv, double *sp) {
+  const int t = threadIdx.x;
+  __syncthreads();
+  if (t < T) sv[t] = __ldcg(yj + t);
+  __syncthreads();
+  const int c = t & 63, q = t >> 6;
   double s = 0.;
-  for (int m = lane; m < tb; m += 32)
-    s += (backward ? A[(size_t)(j0 + m) * n + i] : A[(size_t)i * n + j0 + m]) * y[j0 + m];
+  if (!trans) {
+    // output row c, columns 16 q .. + 16
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if (lane == 0) y[i] -= s;
+    for (int m = 0; m < 16; ++m) s += __ldcg(Li + c * T + 16 * q + m) * sv[16 * q + m];
+  } else {
+    // output column c: sum over rows 16 q .. + 16
+#pragma unroll
+    for (int m = 0; m < 16; ++m) s += __ldcg(Li + (16 * q + m) * T + c) * sv[16 * q + m];
+  }
+  sp[t] = s;
+  __syncthreads();
+  if (t < T) yj[t] = (sp[t] + sp[t + 64]) + (sp[t + 128] + sp[t + 192]);
+  __syncthreads();
 }
 
-
-// Tile row it of X = L^-1: CTA j < it forms X_ij = -Linv_i sum_{j<=m<i}
-// L_im X_mj (tile rows < it are complete); CTA j == it copies Linv_i.
-__global__ void __launch_bounds__(DT) k_inv_row(const double *A, int n, const double *Linv, double *X, int it) {
-  extern __shared__ double dyn[];
-  double(*a)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn);
-  double(*b)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn + T * (T + 1));
-  const int jt = blockIdx.x, tid = threadIdx.x;
-  const int i0 = it * T, ib = min(T, n - i0), j0 = jt * T, jb = min(T, n - j0);
-  const double *Li = Linv + (size_t)it * T * T;
-  if (jt == it) {
-    for (int idx = tid; idx < T * T; idx += DT) {
-      const int i = idx / T, j = idx % T;
-      if (i < ib && j < jb) X[(size_t)(i0 + i) * n + j0 + j] = Li[idx];
+// Forward then back substitution over the envelope tiles.  A tile row's
+// diagonal solve is done by the CTA that applies the row's last update, so
+// every step costs one grid barrier.
+__global__ void __launch_bounds__(ST) k_env_solve(SolveArgs A) {
+  __shared__ double sv[T], sp[ST];
+  const int G = gridDim.x, nt = A.nt;
+  // forward: L y = b
+  if (blockIdx.x == 0) tile_gemv_set(A.Linv, A.y, false, sv, sp);
+  if (!grid_barrier(A.bar, G, A.err, A.bar_ns)) return;
+  for (int J = 0; J < nt - 1; ++J) {
+    const int m = A.hrow[J] - J;
+    for (int t = blockIdx.x; t < m; t += G) {
+      const int I = J + 1 + t;
+      tile_gemv_sub(etile(A, I, J), A.y + (size_t)J * T, A.y + (size_t)I * T, false, sv, sp);
+      if (t == 0) tile_gemv_set(A.Linv + (size_t)I * TS, A.y + (size_t)I * T, false, sv, sp);
     }
-    return;
+    if (m == 0 && blockIdx.x == (J + 1) % G)
+      tile_gemv_set(A.Linv + (size_t)(J + 1) * TS, A.y + (size_t)(J + 1) * T, false, sv, sp);
+    if (!grid_barrier(A.bar, G, A.err, A.bar_ns)) return;
   }
-  const int ti = (tid / 16) * 4, tj = (tid % 16) * 4;
-  double o[4][4] = {};
-  for (int mt = jt; mt < it; ++mt) {
-    const int m0 = mt * T, mb = min(T, n - m0);
-    __syncthreads();
-    for (int idx = tid; idx < T * T; idx += DT) {
-      const int i = idx / T, j = idx % T;
-      a[i][j] = (i < ib && j < mb) ? A[(size_t)(i0 + i) * n + m0 + j] : 0.;    // L_im
-      b[i][j] = (i < mb && j < jb) ? X[(size_t)(m0 + i) * n + j0 + j] : 0.;    // X_mj
+  // backward: L^T x = y
+  if (blockIdx.x == 0) tile_gemv_set(A.Linv + (size_t)(nt - 1) * TS, A.y + (size_t)(nt - 1) * T, true, sv, sp);
+  if (!grid_barrier(A.bar, G, A.err, A.bar_ns)) return;
+  for (int J = nt - 1; J > 0; --J) {
+    const int m = J - A.fcol[J];
+    for (int t = blockIdx.x; t < m; t += G) {
+      const int K = J - 1 - t;
+      tile_gemv_sub(etile(A, J, K), A.y + (size_t)J * T, A.y + (size_t)K * T, true, sv, sp);
+      if (t == 0) tile_gemv_set(A.Linv + (size_t)K * TS, A.y + (size_t)K * T, true, sv, sp);
     }
-    __syncthreads();
-    for (int m = 0; m < mb; ++m) {
-      double av[4], bv[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        av[u] = a[ti + u][m];
-        bv[u] = b[m][tj + u];
-      }
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) o[u][v] += av[u] * bv[v];
-    }
+    if (m == 0 && blockIdx.x == (J - 1) % G)
+      tile_gemv_set(A.Linv + (size_t)(J - 1) * TS, A.y + (size_t)(J - 1) * T, true, sv, sp);
+    if (!grid_barrier(A.bar, G, A.err, A.bar_ns)) return;
   }
-  __syncthreads();
-  // Y -> shared b, then X_ij = -Linv_i Y
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) b[ti + u][tj + v] = o[u][v];
-  for (int idx = tid; idx < T * T; idx += DT) a[idx / T][idx % T] = Li[idx];
-  __syncthreads();
-  double y[4][4] = {};
-  for (int m = 0; m < ib; ++m) {
-    double av[4], bv[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      av[u] = a[ti + u][m];
-      bv[u] = b[m][tj + u];
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u)
-#pragma unroll
-      for (int v = 0; v < 4; ++v) y[u][v] += av[u] * bv[v];
-  }
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v)
-      if (ti + u < ib && tj + v < jb) X[(size_t)(i0 + ti + u) * n + j0 + tj + v] = -y[u][v];
 }
 
-// A^-1 = X^T X for tile (bi, bk), bk <= bi: sum over tile rows m >= bi of
-// X_m,bi^T X_m,bk; written to both triangles.
-__global__ void __launch_bounds__(DT) k_xtx(const double *X, int n, double *Ainv) {
-  const int t = blockIdx.x;
-  int bi = (int)((sqrt(8. * t + 1.) - 1.) / 2.);
-  while ((bi + 1) * (bi + 2) / 2 <= t) ++bi;
-  while (bi * (bi + 1) / 2 > t) --bi;
-  const int bk = t - bi * (bi + 1) / 2;
-  const int ri = bi * T, rk = bk * T, nbi = min(T, n - ri), nbk = min(T, n - rk);
-  extern __shared__ double dyn[];
-  double(*pi)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn);
-  double(*pk)[T + 1] = reinterpret_cast<double(*)[T + 1]>(dyn + T * (T + 1));
-  const int tid = threadIdx.x, ti = (tid / 16) * 4, tj = (tid % 16) * 4;
-  const int ntiles = (n + T - 1) / T;
-  double o[4][4] = {};
-  for (int mt = bi; mt < ntiles; ++mt) {
-    const int m0 = mt * T, mb = min(T, n - m0);
-    __syncthreads();
-    for (int idx = tid; idx < T * T; idx += DT) {
-      const int m = idx / T, j = idx % T;
-      pi[m][j] = (m < mb && j < nbi) ? X[(size_t)(m0 + m) * n + ri + j] : 0.;
-      pk[m][j] = (m < mb && j < nbk) ? X[(size_t)(m0 + m) * n + rk + j] : 0.;
+// Reverse Cuthill-McKee order of the vertices of a graph (CSR, neighbours
+// of every vertex), every component from a pseudo-peripheral vertex.
+std::vector<int> rcm_order(int n, const std::vector<int> &off, const std::vector<int> &adj) {
+  std::vector<int> deg(n), order;
+  order.reserve(n);
+  for (int v = 0; v < n; ++v) deg[v] = off[v + 1] - off[v];
+  std::vector<char> seen(n, 0);
+  std::vector<int> lvl(n, -1), q;
+  auto bfs_last = [&](int s, int &ecc) {
+    // level structure from s: a vertex of least degree in the last level
+    q.assign(1, s);
+    lvl[s] = 0;
+    for (size_t h = 0; h < q.size(); ++h) {
+      const int v = q[h];
+      for (int e = off[v]; e < off[v + 1]; ++e)
+        if (lvl[adj[e]] < 0) {
+          lvl[adj[e]] = lvl[v] + 1;
+          q.push_back(adj[e]);
+        }
     }
-    __syncthreads();
-    for (int m = 0; m < mb; ++m) {
-      double av[4], bv[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        av[u] = pi[m][ti + u];
-        bv[u] = pk[m][tj + u];
+    ecc = lvl[q.back()];
+    int best = q.back();
+    for (int v : q)
+      if (lvl[v] == ecc && (deg[v] < deg[best] || (deg[v] == deg[best] && v < best))) best = v;
+    for (int v : q) lvl[v] = -1;
+    return best;
+  };
+  std::vector<int> byd(n);
+  std::iota(byd.begin(), byd.end(), 0);
+  std::stable_sort(byd.begin(), byd.end(), [&](int a, int b) { return deg[a] < deg[b]; });
+  std::vector<int> nb;
+  for (int s0 : byd) {
+    if (seen[s0]) continue;
+    int s = s0, ecc = -1;
+    for (int it = 0; it < 6; ++it) {
+      int e2 = 0;
+      const int c = bfs_last(s, e2);
+      if (e2 <= ecc) break;
+      ecc = e2;
+      s = c;
+    }
+    const size_t base = order.size();
+    order.push_back(s);
+    seen[s] = 1;
+    for (size_t h = base; h < order.size(); ++h) {
+      const int v = order[h];
+      nb.clear();
+      for (int e = off[v]; e < off[v + 1]; ++e)
+        if (!seen[adj[e]]) nb.push_back(adj[e]);
+      std::sort(nb.begin(), nb.end(), [&](int a, int b) { return deg[a] < deg[b] || (deg[a] == deg[b] && a < b); });
+      for (int w : nb) {
+        seen[w] = 1;
+        order.push_back(w);
       }
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-#pragma unroll
-        for (int v = 0; v < 4; ++v) o[u][v] += av[u] * bv[v];
     }
   }
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v)
-      if (ti + u < nbi && tj + v < nbk) {
-        Ainv[(size_t)(ri + ti + u) * n + rk + tj + v] = o[u][v];
-        Ainv[(size_t)(rk + tj + v) * n + ri + ti + u] = o[u][v];
-      }
+  std::reverse(order.begin(), order.end());
+  return order;
+}
+
+int solve_grid() {
+  int dev = 0, nsm = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_env_solve, ST, 0);
+  return per >= 1 ? nsm : 0;
 }
 
 }  // namespace
 
-size_t direct_bytes(int n) { return (size_t)n * n * sizeof(double); }
-
-// Factor a dense SPD matrix in place: the lower triangle of A (row major,
-// n x n) becomes L with A = L L^T; Linv receives the inverses of L's
-// diagonal T x T tiles.  A non-positive pivot sets bit 4 of *err.
-void dense_cholesky(double *A, int n, double *Linv, int *err, cudaStream_t s) {
-  if (n <= 0) return;
-  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
-  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
-  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_syrk, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
-  const int ntiles = (n + T - 1) / T;
-  for (int jt = 0; jt < ntiles; ++jt) {
-    const int j0 = jt * T, tb = min(T, n - j0);
-    k_potrf<<<1, DT, SMEM2, s>>>(A, n, j0, tb, Linv + (size_t)jt * T * T, err);
-    const int rows_below = n - j0 - tb;
-    if (rows_below > 0) {
-      const int m = (rows_below + T - 1) / T;
-      k_trsm<<<m, DT, SMEM2, s>>>(A, n, j0, tb, Linv + (size_t)jt * T * T);
-      k_syrk<<<m * (m + 1) / 2, DT, SMEM2, s>>>(A, n, j0, tb, m);
+// Ordering and envelope of the current structure (host); device buffers
+// sized for it.  Returns false when the envelope's tiles exceed max_bytes.
+bool direct_analyse(const DevLSA &L, const unsigned *d_bkey, const std::vector<int> &camparv, size_t max_bytes,
+                    DirectWork &W, std::vector<void *> &owned, cudaStream_t s) {
+  const int nimg = L.nimg, b0 = L.begini, nc = nimg - b0, nb = L.nboff;
+  std::vector<unsigned> key(std::max(nb, 1));
+  if (nb) RPBA_CUDA_CHECK(cudaMemcpyAsync(key.data(), d_bkey, sizeof(unsigned) * nb, cudaMemcpyDeviceToHost, s));
+  RPBA_CUDA_CHECK(cudaStreamSynchronize(s));
+  // covisibility graph of the system's cameras (local index k - begini)
+  std::vector<int> off(nc + 1, 0), adj(2 * (size_t)nb);
+  for (int b = 0; b < nb; ++b) {
+    ++off[key[b] / nimg - b0 + 1];
+    ++off[key[b] % nimg - b0 + 1];
+  }
+  for (int v = 0; v < nc; ++v) off[v + 1] += off[v];
+  {
+    std::vector<int> fill(off.begin(), off.end() - 1);
+    for (int b = 0; b < nb; ++b) {
+      const int r = (int)(key[b] / nimg) - b0, c = (int)(key[b] % nimg) - b0;
+      adj[fill[r]++] = c;
+      adj[fill[c]++] = r;
     }
   }
-}
-
-// Explicit inverse from the factor: X = L^-1 tile row by tile row
-// (X_ij = -L_ii^-1 sum_{j <= m < i} L_im X_mj), then A^-1 = X^T X, both
-// triangles written.  X and Ainv are n x n row major.
-void dense_spd_inverse(const double *A, int n, const double *Linv, double *X, double *Ainv, cudaStream_t s) {
-  if (n <= 0) return;
-  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_inv_row, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
-  RPBA_CUDA_CHECK(cudaFuncSetAttribute(k_xtx, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM2));
-  const int ntiles = (n + T - 1) / T;
-  for (int it = 0; it < ntiles; ++it) k_inv_row<<<it + 1, DT, SMEM2, s>>>(A, n, Linv, X, it);
-  k_xtx<<<ntiles * (ntiles + 1) / 2, DT, SMEM2, s>>>(X, n, Ainv);
-}
-
-// Factor S = L L^T (kept in W.A / W.Linv) and solve S x = b for the
-// reduced camera system; x in xsol (padded 9 per camera).  A non-positive
-// pivot sets L.err bit 4.
-void direct_factor(const DevLSA &L, const DirectWork &W, cudaStream_t s) {
-  const int n = W.n;
-  if (n <= 0) return;
-  RPBA_CUDA_CHECK(cudaMemsetAsync(W.A, 0, (size_t)n * n * sizeof(double), s));
-  const long long nd = (long long)(L.nimg - L.begini) * 81;
-  if (nd > 0) {
-    k_dense_fill<<<(int)((nd + 255) / 256), 256, 0, s>>>(L, W.coff, n, W.A);
-    k_dense_fill_off<<<(int)((nd + 255) / 256), 256, 0, s>>>(L, W.coff, n, W.A);
+  const std::vector<int> order = rcm_order(nc, off, adj);
+  // first unknown of every camera in the order
+  std::vector<int> pos(nimg, 0);
+  int n = 0;
+  for (int v : order) {
+    pos[v + b0] = n;
+    n += camparv[v + b0 + 1] - camparv[v + b0];
   }
-  dense_cholesky(W.A, n, W.Linv, L.err, s);
+  const int nt = (n + T - 1) / T;
+  // envelope: first column of every camera's rows, then per tile row
+  std::vector<int> fc(std::max(nt, 1), 0);
+  for (int I = 0; I < nt; ++I) fc[I] = I;
+  for (int v = 0; v < nc; ++v) {
+    int first = pos[v + b0];
+    for (int e = off[v]; e < off[v + 1]; ++e) first = std::min(first, pos[adj[e] + b0]);
+    const int np = camparv[v + b0 + 1] - camparv[v + b0];
+    for (int a = 0; a < np; ++a) {
+      const int I = (pos[v + b0] + a) / T;
+      fc[I] = std::min(fc[I], first / T);
+    }
+  }
+  for (int I = nt - 2; I >= 0; --I) fc[I] = std::min(fc[I], fc[I + 1]);
+  std::vector<long long> toff(std::max(nt, 1), 0);
+  long long ntiles = 0;
+  for (int I = 0; I < nt; ++I) {
+    toff[I] = ntiles;
+    ntiles += I - fc[I] + 1;
+  }
+  std::vector<int> hrow(std::max(nt, 1), 0);
+  for (int J = 0, I = 0; J < nt; ++J) {
+    while (I + 1 < nt && fc[I + 1] <= J) ++I;
+    hrow[J] = std::max(I, J);
+  }
+  const size_t bytes = (size_t)(ntiles + nt) * TS * sizeof(double);
+  W.n = n;
+  W.nt = nt;
+  W.ntiles = ntiles;
+  W.env_bytes = bytes;
+  if (bytes > max_bytes) return false;
+  auto dal = [&](size_t b) {
+    void *p = nullptr;
+    RPBA_CUDA_CHECK(cudaMalloc(&p, std::max<size_t>(b, 16)));
+    owned.push_back(p);
+    return p;
+  };
+  if ((size_t)ntiles > W.cap_tiles) {
+    W.tiles = (double *)dal((size_t)ntiles * TS * sizeof(double));
+    W.cap_tiles = (size_t)ntiles;
+  }
+  if (nt > W.cap_nt) {
+    W.Linv = (double *)dal((size_t)nt * TS * sizeof(double));
+    W.y = (double *)dal((size_t)nt * T * sizeof(double));
+    W.toff = (long long *)dal(sizeof(long long) * nt);
+    W.fcol = (int *)dal(sizeof(int) * nt);
+    W.hrow = (int *)dal(sizeof(int) * nt);
+    W.cap_nt = nt;
+  }
+  if (!W.pos) {
+    W.pos = (int *)dal(sizeof(int) * nimg);
+    W.bar = (unsigned *)dal(2 * sizeof(unsigned));
+  }
+  W.bkey = d_bkey;
+  RPBA_CUDA_CHECK(cudaMemcpyAsync(W.pos, pos.data(), sizeof(int) * nimg, cudaMemcpyHostToDevice, s));
+  if (nt) {
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(W.toff, toff.data(), sizeof(long long) * nt, cudaMemcpyHostToDevice, s));
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(W.fcol, fc.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, s));
+    RPBA_CUDA_CHECK(cudaMemcpyAsync(W.hrow, hrow.data(), sizeof(int) * nt, cudaMemcpyHostToDevice, s));
+  }
+  RPBA_CUDA_CHECK(cudaStreamSynchronize(s));  // the host vectors go out of scope
+  return true;
+}
+
+// Factor the reduced camera system into the envelope tiles.
+void direct_factor(const DevLSA &L, const DirectWork &W, cudaStream_t s) {
+  if (W.n <= 0) return;
+  RPBA_CUDA_CHECK(cudaMemsetAsync(W.tiles, 0, (size_t)W.ntiles * TS * sizeof(double), s));
+  const int pad = W.nt * T - W.n;
+  if (pad > 0) k_env_diag_pad<<<(pad + 127) / 128, 128, 0, s>>>(W.tiles, W.toff, W.fcol, W.nt, W.n);
+  const long long nd = (long long)(L.nimg - L.begini) * 81;
+  if (nd > 0) k_env_fill_diag<<<(int)((nd + 255) / 256), 256, 0, s>>>(L, W.pos, W.tiles, W.toff, W.fcol);
+  const long long no = (long long)L.nboff * 81;
+  if (no > 0) k_env_fill_off<<<(int)((no + 255) / 256), 256, 0, s>>>(L, W.bkey, W.pos, W.tiles, W.toff, W.fcol);
+  tile_cholesky(W.tiles, W.toff, W.fcol, W.hrow, W.Linv, W.nt, W.bar, L.err, s);
 }
 
 // x = S^-1 b with the factor from direct_factor; b and x padded 9 per camera
 // (b == nullptr: the assembled right-hand side L.rhs).
 void direct_resolve(const DevLSA &L, const DirectWork &W, const double *b, double *xsol, cudaStream_t s) {
-  const int n = W.n;
-  if (n <= 0) return;
-  if (b)
-    k_gather_vec<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W.coff, b, W.y);
-  else
-    k_gather_rhs<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W.coff, W.y);
-  const int ntiles = (n + T - 1) / T;
-  for (int jt = 0; jt < ntiles; ++jt) {
-    const int j0 = jt * T, tb = min(T, n - j0);
-    k_tile_solve<<<1, T, 0, s>>>(W.Linv + (size_t)jt * T * T, tb, W.y, j0, 0);
-    const int rows = n - j0 - tb;
-    if (rows > 0) k_panel_update<<<(rows * 32 + 255) / 256, 256, 0, s>>>(W.A, n, j0, tb, W.y, 0);
-  }
-  for (int jt = ntiles - 1; jt >= 0; --jt) {
-    const int j0 = jt * T, tb = min(T, n - j0);
-    k_tile_solve<<<1, T, 0, s>>>(W.Linv + (size_t)jt * T * T, tb, W.y, j0, 1);
-    if (j0 > 0) k_panel_update<<<(j0 * 32 + 255) / 256, 256, 0, s>>>(W.A, n, j0, tb, W.y, 1);
-  }
-  k_scatter_solution<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W.coff, W.y, xsol);
+  if (W.n <= 0) return;
+  const int pad = W.nt * T - W.n;
+  if (pad > 0) RPBA_CUDA_CHECK(cudaMemsetAsync(W.y + W.n, 0, sizeof(double) * pad, s));
+  k_env_gather<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W.pos, b, W.y);
+  SolveArgs A;
+  A.tiles = W.tiles;
+  A.Linv = W.Linv;
+  A.toff = W.toff;
+  A.fcol = W.fcol;
+  A.hrow = W.hrow;
+  A.y = W.y;
+  A.nt = W.nt;
+  A.bar = W.bar;
+  A.err = L.err;
+  A.bar_ns = BAR_TIMEOUT_NS;
+  const int g = std::max(1, std::min(solve_grid(), W.nt));
+  RPBA_CUDA_CHECK(cudaMemsetAsync(W.bar, 0, 2 * sizeof(unsigned), s));
+  void *args[] = {&A};
+  RPBA_CUDA_CHECK(cudaLaunchCooperativeKernel((const void *)k_env_solve, dim3(g), dim3(ST), args, 0, s));
+  k_env_scatter<<<(L.nimg + 127) / 128, 128, 0, s>>>(L, W.pos, W.y, xsol);
+  RPBA_CUDA_CHECK(cudaGetLastError());
 }
 
 void direct_solve(const DevLSA &L, const DirectWork &W, double *xsol, cudaStream_t s) {

@@ -150,19 +150,40 @@ void launch_exact_sum(const float *v, int n, float *out, const ExactSumWork &W, 
 
 // ---- dense direct solve (direct.cu)
 struct DirectWork {
-  int n;          // unknowns of the reduced camera system
-  double *A;      // n x n
-  double *Linv;   // ceil(n / 64) tiles of 64 x 64
-  double *y;      // n
-  int *coff;      // [nimg + 1] compact parameter offsets
+  int n = 0;              // unknowns of the reduced camera system
+  int nt = 0;             // 64-wide tile rows
+  long long ntiles = 0;   // tiles of the envelope
+  size_t env_bytes = 0;   // device bytes the envelope and its inverses take
+  double *tiles = nullptr;         // [ntiles][64 * 64] lower envelope, then L
+  double *Linv = nullptr;          // [nt][64 * 64] inverses of the diagonal tiles
+  double *y = nullptr;             // [nt * 64] right-hand side / solution, factor order
+  long long *toff = nullptr;       // [nt] first tile of each tile row
+  int *fcol = nullptr, *hrow = nullptr;  // [nt] first tile column of a row, last tile row of a column
+  int *pos = nullptr;              // [nimg] first unknown of each camera in factor order
+  unsigned *bar = nullptr;         // grid-barrier words
+  const unsigned *bkey = nullptr;  // (row * nimg + column) of each off-diagonal block
+  size_t cap_tiles = 0;
+  int cap_nt = 0;
 };
-size_t direct_bytes(int n);
+// Camera order (reverse Cuthill-McKee) and envelope of the current structure
+// (host), device buffers sized for it; false when the envelope would take
+// more than max_bytes.
+bool direct_analyse(const DevLSA &L, const unsigned *d_bkey, const std::vector<int> &camparv, size_t max_bytes,
+                    DirectWork &W, std::vector<void *> &owned, cudaStream_t s);
 void direct_solve(const DevLSA &L, const DirectWork &W, double *xsol, cudaStream_t s);
 void direct_factor(const DevLSA &L, const DirectWork &W, cudaStream_t s);
 void direct_resolve(const DevLSA &L, const DirectWork &W, const double *b, double *xsol, cudaStream_t s);
-// dense SPD helpers (row major n x n, 64 x 64 tiles)
-void dense_cholesky(double *A, int n, double *Linv, int *err, cudaStream_t s);
-void dense_spd_inverse(const double *A, int n, const double *Linv, double *X, double *Ainv, cudaStream_t s);
+// Tiled Cholesky of a lower envelope of 64 x 64 tiles in place, with the
+// inverses of the diagonal tiles (chol.cu; one cooperative launch).
+void tile_cholesky(double *tiles, const long long *toff, const int *fcol, const int *hrow, double *Linv, int nt,
+                   unsigned *bar, int *err, cudaStream_t s);
+// A^-1 of (D A D + eps I), scaled back by D = diag(dsc), for a dense SPD
+// matrix (row major n x n, lower triangle used): tiled Cholesky and inverse
+// in one cooperative launch on the FP64 tensor cores (chol.cu).  work:
+// spd_inverse_bytes(n); bar: two barrier words; err bit 4: not SPD.
+size_t spd_inverse_bytes(int n);
+void spd_inverse_scaled(const double *A, const double *dsc, double eps, int n, double *Ainv, void *work,
+                        unsigned *bar, int *err, cudaStream_t s);
 
 // ---- coarse space of the two-level preconditioner (coarse.cu)
 // Cameras are grouped into spatially compact aggregates; each aggregate
@@ -176,11 +197,13 @@ struct CoarseWork {
   int *agg_rows = nullptr;       // rows of the system grouped by aggregate
   int *row_agg = nullptr;        // [nimg] aggregate of a row, -1 outside
   double *P = nullptr;           // [nimg * 9 * CO_M]
-  double *Ac = nullptr, *X = nullptr, *Ainv = nullptr, *Linv = nullptr;
+  double *Ac = nullptr, *Ainv = nullptr;
   double *rc = nullptr;          // [nc] restricted residual
   double *dsc = nullptr;         // [nc] Jacobi scaling of A_c
   double *hj = nullptr;          // [nimg * 9] fine part of the preconditioned residual
   int *err = nullptr;            // bit 4: coarse matrix not positive definite
+  void *work = nullptr;          // spd_inverse_bytes(nc)
+  unsigned *bar = nullptr;       // grid-barrier words of the factorisation
   // Galerkin assembly (grown on demand, released by coarse_release)
   int built_version = -1, nruns = 0, nsegs = 0;
   unsigned *ekey = nullptr, *ekey2 = nullptr, *run_key = nullptr, *rkey = nullptr, *rkey2 = nullptr,

@@ -337,19 +337,21 @@ struct rpba_handle {
     return CW.nagg > 0 ? &CW : nullptr;
   }
 
-  void ensure_direct() {
-    if (DW.A) return;
-    std::vector<int> coff(nimg + 1, 0);
-    for (int k = 0; k < nimg; ++k) coff[k + 1] = coff[k] + (k >= begini ? camparv[k + 1] - camparv[k] : 0);
-    for (int k = 0; k < begini; ++k) coff[k] = 0;
-    const int n = coff[nimg];
-    DW.n = n;
-    DW.A = dalloc<double>((size_t)n * n, owned);
-    DW.Linv = dalloc<double>((size_t)((n + 63) / 64) * 64 * 64, owned);
-    DW.y = dalloc<double>(n, owned);
-    DW.coff = dalloc<int>(nimg + 1, owned);
-    RPBA_CUDA_CHECK(cudaMemcpyAsync(DW.coff, coff.data(), sizeof(int) * (nimg + 1), cudaMemcpyHostToDevice, s));
+  // Direct-solve structure (camera order and envelope), rebuilt when the
+  // pair structure changes; false when the envelope does not fit in device
+  // memory (the reduced camera system is too dense for the direct form).
+  int direct_version = -1;
+  bool direct_ok = false;
+  bool ensure_direct() {
+    if (direct_version == structure_version) return direct_ok;
+    size_t fr = 0, tot = 0;
+    RPBA_CUDA_CHECK(cudaMemGetInfo(&fr, &tot));
+    const size_t reuse = DW.cap_tiles * 64 * 64 * sizeof(double);
+    direct_ok = direct_analyse(L, S.bkey, camparv, (fr + reuse) / 10 * 7, DW, owned, s);
+    direct_version = structure_version;
+    return direct_ok;
   }
+  bool direct_too_large = false;
 
   // Batched solves (rpba_solve_batch) run many handles on one GPU at once.
   // Cooperative kernels (the persistent PCG, the exact sums) need all their
@@ -792,6 +794,7 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
 
 // Restore the uploaded input state (the LSA after its constructor).
 void rpba_handle::reset() {
+  direct_too_large = false;
   L.nobs = nobs0;
   L.npts = npts0;
   auto cp = [&](void *d, const void *src, size_t bytes) {
@@ -855,12 +858,15 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
   PROF("pair", 1, launch_pair_pass(L, s));
   int msize = 0;
   for (int k = begini; k < nimg; ++k) msize += camparv[k + 1] - camparv[k];
-  const int nunk = msize;
   if (msize < 1000) msize = 1000;
   if (opt.pcg_max_iterations > 0) msize = opt.pcg_max_iterations;
   if (opt.solver == RPBA_SOLVER_DIRECT) {
-    ensure_direct();
-    PROF("direct", 1, direct_solve(L, DW, W.xbest, s));
+    if (!ensure_direct()) {
+      direct_too_large = true;
+      return true;
+    }
+    CoopLock lk(this);
+    PROF("direct", 3, direct_solve(L, DW, W.xbest, s));
   } else if (opt.solver == RPBA_SOLVER_LEARNED) {
     // PCG with the two-level preconditioner: the learned block-Jacobi part
     // plus the aggregate coarse space.  Stop rule: the reference's
@@ -884,7 +890,10 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
         prof.next_bytes = (Nc + 2. * Nb) * (L.blocks32 ? 324. : 648.) + nc * nc * 8;
         PROF("coarse_assemble", 4, coarse_assemble(L, CW, structure_version, s));
         prof.next_bytes = 4. * nc * nc * 8;
-        PROF("coarse_factor", 4, coarse_factor(CW, s));
+        {
+          CoopLock lk(this);
+          PROF("coarse_factor", 2, coarse_factor(CW, s));
+        }
         coarse_stale = false;
         fresh = true;
       }
@@ -937,9 +946,9 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
         std::snprintf(line, sizeof line, "PCG fallback (block-Jacobi): iterations %d converged %d\n", it2[0], it2[1]);
         log += line;
       }
-      if (it2[1] == 0 && nunk <= 40000) {
-        ensure_direct();
-        PROF("direct", 1, direct_solve(L, DW, W.xbest, s));
+      if (it2[1] == 0 && ensure_direct()) {
+        CoopLock lk(this);
+        PROF("direct", 3, direct_solve(L, DW, W.xbest, s));
       }
     }
   } else {
@@ -1060,11 +1069,15 @@ int rpba_handle::adjust() {
         wsumg = wsum;
       }
       calc_bundle_sep(multfact, nrunknowns);
+      if (direct_too_large) return RPBA_ERR_TOO_LARGE;
       ++solves;
       rep.linear_solves = solves;
       PROF("decode", 1, launch_decode(L, L.XPMn, s));
       PROF("cost", 1, launch_cost(L, L.XPMn, true, s));
-      PROF("seq_sum", 1, launch_exact_sum(L.o_cost, L.nobs, sums, ES, s));
+      {
+        CoopLock lk(this);
+        PROF("seq_sum", 1, launch_exact_sum(L.o_cost, L.nobs, sums, ES, s));
+      }
       struct {
         float sig0;
         int err;
@@ -1189,6 +1202,7 @@ int rpba_handle::adjust_gcp_step() {
     RPBA_CUDA_CHECK(cudaMemcpyAsync(aoterm + np, aoterm, sizeof(float) * np, cudaMemcpyDeviceToDevice, s));
   }
   calc_bundle_sep(multfact, nrunknowns);
+  if (direct_too_large) return RPBA_ERR_TOO_LARGE;
   rep.linear_solves = 1;
   PROF("decode", 1, launch_decode(L, L.XPMn, s));
   PROF("cost", 1, launch_cost(L, L.XPMn, true, s));
@@ -1846,6 +1860,51 @@ int32_t rpba_kernel_stats(rpba_handle *H, char *json, size_t cap) {
   std::memcpy(json, o.data(), n);
   json[n] = 0;
   return RPBA_OK;
+}
+
+int32_t rpba_spd_inverse(const double *A, int32_t n, double *Ainv, int32_t device) {
+  if (!A || !Ainv || n <= 0) return RPBA_ERR_ARG;
+  if (n > 16384) return RPBA_ERR_TOO_LARGE;
+  struct Args {
+    const double *A;
+    int n;
+    double *Ainv;
+    int device;
+  } args{A, n, Ainv, device};
+  return guard(
+      [](void *p) -> int {
+        const Args &a = *(const Args *)p;
+        RPBA_CUDA_CHECK(cudaSetDevice(a.device));
+        const size_t bytes = sizeof(double) * (size_t)a.n * a.n;
+        std::vector<void *> owned;  // freed on every return
+        struct Free {
+          std::vector<void *> &v;
+          ~Free() {
+            for (void *q : v) cudaFree(q);
+          }
+        } fr{owned};
+        auto dal = [&](size_t b) {
+          void *q = nullptr;
+          RPBA_CUDA_CHECK(cudaMalloc(&q, std::max<size_t>(b, 16)));
+          owned.push_back(q);
+          return q;
+        };
+        double *dA = (double *)dal(bytes), *dI = (double *)dal(bytes), *dd = (double *)dal(sizeof(double) * a.n);
+        void *work = dal(spd_inverse_bytes(a.n));
+        unsigned *bar = (unsigned *)dal(2 * sizeof(unsigned));
+        int *err = (int *)dal(sizeof(int));
+        const std::vector<double> ones(a.n, 1.);
+        RPBA_CUDA_CHECK(cudaMemcpy(dA, a.A, bytes, cudaMemcpyHostToDevice));
+        RPBA_CUDA_CHECK(cudaMemcpy(dd, ones.data(), sizeof(double) * a.n, cudaMemcpyHostToDevice));
+        RPBA_CUDA_CHECK(cudaMemset(err, 0, sizeof(int)));
+        spd_inverse_scaled(dA, dd, 0., a.n, dI, work, bar, err, 0);
+        int e = 0;
+        RPBA_CUDA_CHECK(cudaMemcpy(a.Ainv, dI, bytes, cudaMemcpyDeviceToHost));
+        RPBA_CUDA_CHECK(cudaMemcpy(&e, err, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e & 2) return RPBA_ERR_DEVICE_TIMEOUT;
+        return (e & 4) ? RPBA_ERR_SOLVER : RPBA_OK;
+      },
+      &args);
 }
 
 int32_t rpba_debug_barrier_timeout(rpba_handle *H, int32_t extra_ctas, int64_t timeout_ns) {

@@ -41,7 +41,7 @@ EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block
            "rpba_set_preconditioner", "rpba_precond_loss_grad", "rpba_record_systems", "rpba_solve_batch",
            "rpba_triangulate", "rpba_triangulate_parts", "rpba_partition_images", "rpba_lsa_gcp_step",
            "rpba_calc_plsa_parallel", "rpba_calc_plsa_parallel_hosted", "rpba_debug_barrier_timeout",
-           "rpba_partition_count",
+           "rpba_partition_count", "rpba_spd_inverse",
            "rpba_destroy")
 
 _lib = None
@@ -124,6 +124,8 @@ def load():
     L.rpba_triangulate.restype = C.c_int32
     L.rpba_kernel_stats.argtypes = [C.c_void_p, C.c_char_p, C.c_size_t]
     L.rpba_kernel_stats.restype = C.c_int32
+    L.rpba_spd_inverse.argtypes = [C.POINTER(C.c_double), C.c_int32, C.POINTER(C.c_double), C.c_int32]
+    L.rpba_spd_inverse.restype = C.c_int32
     L.rpba_partition_count.argtypes = [C.c_int32, C.c_int32, C.c_int32]
     L.rpba_partition_count.restype = C.c_int32
     L.rpba_debug_barrier_timeout.argtypes = [C.c_void_p, C.c_int32, C.c_int64]
@@ -246,6 +248,19 @@ def train_preconditioner(blocks, steps=300, batch=0, lr=3e-3, probes=2, seed=1, 
     if st != 0:
         raise RpbaError(st, "rpba_train_preconditioner")
     return w, {k: getattr(rep, k) for k, _ in rep._fields_}
+
+
+def spd_inverse(A, device: int = 0) -> np.ndarray:
+    """A^-1 of a dense SPD matrix by the library's tiled FP64 tensor-core
+    Cholesky and inverse (rpba_spd_inverse)."""
+    A = np.ascontiguousarray(A, np.float64)
+    n = A.shape[0]
+    out = np.zeros_like(A)
+    st = load().rpba_spd_inverse(A.ctypes.data_as(C.POINTER(C.c_double)), n,
+                                 out.ctypes.data_as(C.POINTER(C.c_double)), device)
+    if st != 0:
+        raise RpbaError(st, "rpba_spd_inverse")
+    return out
 
 
 def partition_images(block: Block, nparts: int) -> np.ndarray:
