@@ -34,7 +34,7 @@ constexpr int CT = 64;                  // tile edge
 constexpr int CLD = 68;                 // shared leading dimension: conflict-free fragment loads
 constexpr int CTH = 256;                // threads per CTA (8 warps)
 constexpr int TS = CT * CT;             // doubles per stored tile
-constexpr size_t CSMEM = 2 * CT * CLD * sizeof(double);
+constexpr size_t CSMEM = (2 * CT * CLD + 4 * CT) * sizeof(double);  // two tiles + partials
 
 struct Tiles {
   double *L;               // tile storage (row major inside a tile, ld 64)
@@ -101,58 +101,47 @@ __device__ __forceinline__ void for_frag(F f) {
   }
 }
 
-// Factor the diagonal tile in place (one warp factors, then one warp
-// inverts; the other warps wait at the block barriers) and write L_JJ and
-// L_JJ^-1.  s and si: two shared tiles (ld CT + 1).
-__device__ void potrf_tile(double *gtile, double *ginv, int *err, double *s, double *si) {
+// Factor the diagonal tile in place and write L_JJ and L_JJ^-1, with all
+// threads of the CTA: per column the pivot's square root (every thread
+// takes it), the column scaled, then the trailing triangle updated -- two
+// block barriers a column; then the inverse row by row, every entry from
+// four partial sums (thread c + 64 q takes every fourth term of column c).
+// s, si: two shared tiles (ld CT + 1); pp: 4 x CT doubles of shared scratch.
+__device__ void potrf_tile(double *gtile, double *ginv, int *err, double *s, double *si, double *pp) {
   constexpr int LD = CT + 1;
-  const int lane = threadIdx.x & 31;
+  const int t = threadIdx.x;
   __syncthreads();
-  for (int idx = threadIdx.x; idx < TS; idx += CTH) s[(idx >> 6) * LD + (idx & 63)] = __ldcg(gtile + idx);
+  for (int idx = t; idx < TS; idx += CTH) s[(idx >> 6) * LD + (idx & 63)] = __ldcg(gtile + idx);
   __syncthreads();
-  if (threadIdx.x < 32) {
-    for (int k = 0; k < CT; ++k) {
-      const double d = s[k * LD + k];
-      if (!(d > 0.) && lane == 0) atomicOr(err, 4);
-      const double dk = sqrt(d > 0. ? d : 1.);
-      __syncwarp();
-      if (lane == 0) s[k * LD + k] = dk;
-      for (int i = k + 1 + lane; i < CT; i += 32) s[i * LD + k] /= dk;
-      __syncwarp();
-      for (int i = k + 1 + lane; i < CT; i += 32) {
-        const double lik = s[i * LD + k];
-        for (int j = k + 1; j <= i; ++j) s[i * LD + j] -= lik * s[j * LD + k];
-      }
-      __syncwarp();
+  for (int k = 0; k < CT; ++k) {
+    const double d = s[k * LD + k];
+    const double dk = sqrt(d > 0. ? d : 1.);
+    if (t == 0 && !(d > 0.)) atomicOr(err, 4);
+    if (t < CT - 1 - k) s[(k + 1 + t) * LD + k] /= dk;
+    __syncthreads();
+    if (t == 0) s[k * LD + k] = dk;
+    const int m = CT - 1 - k;
+    for (int idx = t; idx < m * m; idx += CTH) {
+      const int i = k + 1 + idx / m, j = k + 1 + idx % m;
+      if (j <= i) s[i * LD + j] -= s[i * LD + k] * s[j * LD + k];
     }
-    // L^-1 row by row: columns c = lane, lane + 32; four partial sums
-    for (int i = 0; i < CT; ++i) {
-      const double dii = s[i * LD + i];
-#pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int c = lane + 32 * h;
-        double v = 0.;
-        if (c < i) {
-          double p0 = 0., p1 = 0., p2 = 0., p3 = 0.;
-          int m = c;
-          for (; m + 3 < i; m += 4) {
-            p0 += s[i * LD + m] * si[m * LD + c];
-            p1 += s[i * LD + m + 1] * si[(m + 1) * LD + c];
-            p2 += s[i * LD + m + 2] * si[(m + 2) * LD + c];
-            p3 += s[i * LD + m + 3] * si[(m + 3) * LD + c];
-          }
-          for (; m < i; ++m) p0 += s[i * LD + m] * si[m * LD + c];
-          v = -((p0 + p1) + (p2 + p3)) / dii;
-        } else if (c == i) {
-          v = 1. / dii;
-        }
-        si[i * LD + c] = v;
-      }
-      __syncwarp();
-    }
+    __syncthreads();
   }
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < TS; idx += CTH) {
+  const int c = t & 63, q = t >> 6;
+  for (int i = 0; i < CT; ++i) {
+    double acc = 0.;
+    if (c < i)
+      for (int mm = c + q; mm < i; mm += 4) acc += s[i * LD + mm] * si[mm * LD + c];
+    pp[q * CT + c] = acc;
+    __syncthreads();
+    if (t < CT) {
+      const double sum = (pp[t] + pp[CT + t]) + (pp[2 * CT + t] + pp[3 * CT + t]);
+      const double dii = s[i * LD + i];
+      si[i * LD + t] = t < i ? -sum / dii : (t == i ? 1. / dii : 0.);
+    }
+    __syncthreads();
+  }
+  for (int idx = t; idx < TS; idx += CTH) {
     const int i = idx >> 6, j = idx & 63;
     gtile[idx] = j <= i ? s[i * LD + j] : 0.;
     ginv[idx] = si[i * LD + j];
@@ -171,11 +160,11 @@ __device__ __forceinline__ void tri_item(long long t, int &bi, int &bk) {
 
 __global__ void __launch_bounds__(CTH, 1) k_chol_tiles(Tiles T) {
   extern __shared__ __align__(16) double csm[];
-  double *sA = csm, *sB = csm + CT * CLD;
+  double *sA = csm, *sB = csm + CT * CLD, *sP = csm + 2 * CT * CLD;
   const int G = gridDim.x;
   const unsigned nb = (unsigned)G;
   // tile 0's diagonal block
-  if (blockIdx.x == 0) potrf_tile(tile_at(T, 0, 0), T.Linv, T.err, sA, sB);
+  if (blockIdx.x == 0) potrf_tile(tile_at(T, 0, 0), T.Linv, T.err, sA, sB, sP);
   if (!grid_barrier(T.bar, nb, T.err, T.bar_ns)) return;
   for (int J = 0; J < T.nt; ++J) {
     const int h = T.hrow[J], m = h - J;
@@ -215,11 +204,11 @@ __global__ void __launch_bounds__(CTH, 1) k_chol_tiles(Tiles T) {
       for_frag([&](int j, int e, int r, int c) { gt[r * CT + c] -= acc[j][e]; });
       if (bi == 0 && bk == 0) {
         __syncthreads();
-        potrf_tile(gt, T.Linv + (size_t)(J + 1) * TS, T.err, sA, sB);
+        potrf_tile(gt, T.Linv + (size_t)(J + 1) * TS, T.err, sA, sB, sP);
       }
     }
     if (m == 0 && J + 1 < T.nt && blockIdx.x == (J + 1) % G)
-      potrf_tile(tile_at(T, J + 1, J + 1), T.Linv + (size_t)(J + 1) * TS, T.err, sA, sB);
+      potrf_tile(tile_at(T, J + 1, J + 1), T.Linv + (size_t)(J + 1) * TS, T.err, sA, sB, sP);
     if (!grid_barrier(T.bar, nb, T.err, T.bar_ns)) return;
   }
   if (!T.want_inverse) return;

@@ -110,55 +110,27 @@ __global__ void k_entry_keys(DevLSA L, CoarseWork C, unsigned *key, int *val) {
   }
 }
 
-constexpr int RS_T = 128;
-constexpr int RS_E = 4;  // entries staged per round
-// One warp per run (row k, aggregate b): Y = sum over the run's entries of
-// S_kl P_l (9 x CO_M), then Z = P_k^T Y.  The blocks and P_l of RS_E
-// entries at a time are first loaded into the warp's shared stage with
-// independent coalesced loads, then multiplied from there in entry order.
+constexpr int RS_T = 256;
 __global__ void __launch_bounds__(RS_T) k_coarse_runs(DevLSA L, CoarseWork C, int nruns) {
   __shared__ double Ysh[RS_T / 32][9 * CO_M];
-  __shared__ double Bst[RS_T / 32][RS_E][81];
-  __shared__ double Pst[RS_T / 32][RS_E][9 * CO_M];
-  __shared__ int Nst[RS_T / 32][RS_E];
-  __shared__ int2 Est[RS_T / 32][RS_E];
   const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   if (r >= nruns) return;
   const int k = (int)(C.run_key[r] / (unsigned)C.nagg);
   const int npk = L.camparv[k + 1] - L.camparv[k];
   double y[3] = {0., 0., 0.};
-  const int t0 = C.run_off[r], t1 = C.run_off[r + 1];
-  for (int tb = t0; tb < t1; tb += RS_E) {
-    const int ne = min(RS_E, t1 - tb);
-    if (lane < ne) {
-      const int2 en = L.ent[C.ent_sorted[tb + lane]];
-      Est[wl][lane] = en;
-      Nst[wl][lane] = (L.camparv[en.x + 1] - L.camparv[en.x]) | (en.y < 0 ? 0x100 : 0);
-    }
-    __syncwarp();
-    // block entries as stored (row p of a normal block is row p; of a
-    // transposed block, column p), and P of the entries' columns
-    for (int i = lane; i < ne * 81; i += 32) {
-      const int e = i / 81, o = i - e * 81;
-      Bst[wl][e][o] = blk_at(L, (size_t)(Est[wl][e].y & 0x7fffffff), o);
-    }
-    for (int i = lane; i < ne * 9 * CO_M; i += 32) {
-      const int e = i / (9 * CO_M), o = i - e * (9 * CO_M);
-      Pst[wl][e][o] = C.P[(size_t)Est[wl][e].x * CP + o];
-    }
-    __syncwarp();
-    for (int e = 0; e < ne; ++e) {
-      const int nw = Nst[wl][e], npl = nw & 0xff;
-      const bool tr = (nw & 0x100) != 0;
-      const double *Bb = Bst[wl][e], *Pl = Pst[wl][e];
+  for (int t = C.run_off[r]; t < C.run_off[r + 1]; ++t) {
+    const int2 en = L.ent[C.ent_sorted[t]];
+    const int l = en.x;
+    const bool tr = en.y < 0;
+    const size_t B = (size_t)(en.y & 0x7fffffff);
+    const double *Pl = C.P + (size_t)l * CP;
+    const int npl = L.camparv[l + 1] - L.camparv[l];
 #pragma unroll
-      for (int m = 0; m < 3; ++m) {
-        const int o = lane + 32 * m, p = o / CO_M, j = o % CO_M;
-        if (o < 9 * CO_M && p < npk)
-          for (int q = 0; q < npl; ++q) y[m] += Bb[tr ? q * 9 + p : p * 9 + q] * Pl[q * CO_M + j];
-      }
+    for (int m = 0; m < 3; ++m) {
+      const int o = lane + 32 * m, p = o / CO_M, j = o % CO_M;
+      if (o < 9 * CO_M && p < npk)
+        for (int q = 0; q < npl; ++q) y[m] += blk_at(L, B, tr ? q * 9 + p : p * 9 + q) * Pl[q * CO_M + j];
     }
-    __syncwarp();
   }
 #pragma unroll
   for (int m = 0; m < 3; ++m) {

@@ -477,82 +477,49 @@ __global__ void __launch_bounds__(CAM_T) k_camera(DevLSA L, double multfact1) {
 // ----------------------------------------------------------- pair pass
 // Off-diagonal blocks: S_kl = - sum_p W_pk V_p^-1 W_pl^T over the points
 // seen by both cameras (rbacore.cpp:1362-1390), with W_po = Bc^T G.  One
-// warp per block sums its contributions in a fixed order.  The records of a
-// chunk of up to 32 contributions are first gathered into the warp's
-// shared-memory stage with 16-byte asynchronous copies, all issued at once
-// (the gathers are independent; one at a time they left the kernel waiting
-// on memory latency), then accumulated in order from the stage.
-
-// per contribution in the stage: the row camera's observation record
-// (Bc 18, G or H 6), the column camera's, and (FP64 form) the point's V^-1
-constexpr int PAIR_SS = 64;  // stage stride (elements) of one contribution
-constexpr int PAIR_WARPS = 8;
-
-__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
-
-// Gather contributions c0 .. c0 + n of the block into the stage (16-byte
-// pieces: 6 per FP32 record of 24 values, 12 per FP64 record, 5 for a
-// point's V^-1 in the FP64 form).
+// warp per block sums its contributions in a fixed order.  FP64 form; the
+// FP32 form is k_pair32.
 template <class T>
-__device__ __forceinline__ void pair_stage(const DevLSA &L, int c0, int n, int lane, T *stage) {
-  constexpr int PR = 24 * (int)sizeof(T) / 16;  // pieces of one record's first 24 values
-  constexpr int PP = sizeof(T) == 8 ? 5 : 0;     // pieces of V^-1 (9 values, 10 copied)
-  constexpr int PC = 2 * PR + PP;
-  int2 pr = make_int2(0, 0);
-  int pp = 0;
-  if (lane < n) {
-    pr = L.contrib[c0 + lane];
-    if constexpr (sizeof(T) == 8) pp = L.o_pt[pr.x];
-  }
-  const T *rec = Store<T>::rec(L), *ptv = Store<T>::ptV(L);
-  constexpr int E16 = 16 / (int)sizeof(T);  // elements per piece
-  // every lane takes part in every round (the shuffles read other lanes)
-  const int rounds = (n * PC + 31) / 32;
-  for (int k = 0; k < rounds; ++k) {
-    const int q = lane + 32 * k;
-    const int j = min(q / PC, n - 1), part = q - j * PC;
-    const int ox = __shfl_sync(0xffffffffu, pr.x, j), oy = __shfl_sync(0xffffffffu, pr.y, j);
-    const int p = __shfl_sync(0xffffffffu, pp, j);
-    if (q >= n * PC) continue;
-    const T *src;
-    T *dst = stage + (size_t)j * PAIR_SS;
-    if (part < PR) {
-      src = rec + (size_t)ox * REC + part * E16;
-      dst += part * E16;
-    } else if (part < 2 * PR) {
-      src = rec + (size_t)oy * REC + (part - PR) * E16;
-      dst += 24 + (part - PR) * E16;
-    } else {
-      src = ptv + (size_t)p * PREC + (part - 2 * PR) * E16;
-      dst += 48 + (part - 2 * PR) * E16;
-    }
-    cp_async16(dst, src);
-  }
-  cp_async_wait_all();
-  __syncwarp();
-}
-
-// FP64 form.
-template <class T>
-__global__ void __launch_bounds__(256) k_pair(DevLSA L) {
+__global__ void k_pair(DevLSA L) {
   static_assert(sizeof(T) == 8, "the FP32 form is k_pair32");
   const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int wl = threadIdx.x >> 5;
-  extern __shared__ __align__(16) unsigned char pair_dyn[];
-  T *stage = (T *)pair_dyn + (size_t)wl * 32 * PAIR_SS;
+  __shared__ T sm[8][64];
   if (wid >= L.nboff) return;
+  T *s = sm[wl];
   Acc<T> acc[3];
+  const T *rec = Store<T>::rec(L), *ptv = Store<T>::ptV(L);
+  // values of one contribution: 24 of the row camera's observation (Bc 18,
+  // G 6), 24 of the column camera's and V^-1 (9) of the point
+  constexpr int NV = 57;
+  auto fetch = [&](int ox, int oy, int p, T &v0, T &v1) {
+    v0 = lane < 24 ? rec[(size_t)ox * REC + lane] : rec[(size_t)oy * REC + lane - 24];
+    const int i1 = lane + 32;
+    v1 = i1 < 48 ? rec[(size_t)oy * REC + i1 - 24] : (i1 < NV ? ptv[(size_t)p * PREC + i1 - 48] : T(0));
+  };
   const int cb = L.boff[wid], ce = L.boff[wid + 1];
   for (int c0 = cb; c0 < ce; c0 += 32) {
+    // the next (up to) 32 contributions' observation pairs and points, one
+    // per lane; the record values of contribution j + 1 are fetched while j
+    // is accumulated
     const int n = min(32, ce - c0);
-    pair_stage<T>(L, c0, n, lane, stage);
+    int2 pr = make_int2(0, 0);
+    int pp = 0;
+    if (lane < n) {
+      pr = L.contrib[c0 + lane];
+      pp = L.o_pt[pr.x];
+    }
+    T v0, v1;
+    fetch(__shfl_sync(0xffffffffu, pr.x, 0), __shfl_sync(0xffffffffu, pr.y, 0), __shfl_sync(0xffffffffu, pp, 0),
+          v0, v1);
     for (int j = 0; j < n; ++j) {
-      const T *s = stage + (size_t)j * PAIR_SS;
+      s[lane] = v0;
+      if (lane + 32 < NV) s[lane + 32] = v1;
+      if (j + 1 < n)
+        fetch(__shfl_sync(0xffffffffu, pr.x, j + 1), __shfl_sync(0xffffffffu, pr.y, j + 1),
+              __shfl_sync(0xffffffffu, pp, j + 1), v0, v1);
+      __syncwarp();
       // N = G_s V^-1 G_t^T (2 x 2)
       const T *Gs = s + 18, *Gt = s + 42, *Vi = s + 48;
       T GV[2][3], N[2][2];
@@ -577,8 +544,8 @@ __global__ void __launch_bounds__(256) k_pair(DevLSA L) {
           acc[q].add(-(s[i] * t0 + s[9 + i] * t1));
         }
       }
+      __syncwarp();
     }
-    __syncwarp();
   }
   T *B = Store<T>::blocks(L) + (size_t)(L.nimg + wid) * Store<T>::BS;
 #pragma unroll
@@ -598,18 +565,32 @@ __global__ void __launch_bounds__(256) k_pair32(DevLSA L) {
   const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int wl = threadIdx.x >> 5;
-  extern __shared__ __align__(16) unsigned char pair_dyn[];
-  float *stage = (float *)pair_dyn + (size_t)wl * 32 * PAIR_SS;
+  __shared__ float sm[8][48];
   if (wid >= L.nboff) return;
+  float *s = sm[wl];
+  const float *rec = L.rec32;
   const int i = lane < 27 ? lane / 3 : 0, j0 = lane < 27 ? 3 * (lane - 3 * (lane / 3)) : 0;
   float ks[3] = {0.f, 0.f, 0.f}, kc[3] = {0.f, 0.f, 0.f};
+  // record values of one contribution: Bc (18) and H (6) of the row
+  // camera's observation (s[0..23]), then of the column camera's (s[24..47])
+  auto fetch = [&](int ox, int oy, float &v0, float &v1) {
+    v0 = lane < 24 ? rec[(size_t)ox * REC + lane] : rec[(size_t)oy * REC + lane - 24];
+    v1 = lane < 16 ? rec[(size_t)oy * REC + lane + 8] : 0.f;
+  };
   const int cb = L.boff[wid], ce = L.boff[wid + 1];
   for (int c0 = cb; c0 < ce; c0 += 32) {
     const int n = min(32, ce - c0);
-    pair_stage<float>(L, c0, n, lane, stage);
+    int2 pr = make_int2(0, 0);
+    if (lane < n) pr = L.contrib[c0 + lane];
+    float v0, v1;
+    fetch(__shfl_sync(0xffffffffu, pr.x, 0), __shfl_sync(0xffffffffu, pr.y, 0), v0, v1);
     float part[3] = {0.f, 0.f, 0.f};
     for (int j = 0; j < n; ++j) {
-      const float *s = stage + (size_t)j * PAIR_SS;
+      s[lane] = v0;
+      if (lane < 16) s[32 + lane] = v1;
+      if (j + 1 < n)
+        fetch(__shfl_sync(0xffffffffu, pr.x, j + 1), __shfl_sync(0xffffffffu, pr.y, j + 1), v0, v1);
+      __syncwarp();
       float nab = 0.f;
       if (lane < 4) {
         const float *hx = s + 18 + 3 * (lane >> 1), *hy = s + 42 + 3 * (lane & 1);
@@ -623,8 +604,8 @@ __global__ void __launch_bounds__(256) k_pair32(DevLSA L) {
 #pragma unroll
         for (int q = 0; q < 3; ++q) part[q] -= u0 * s[24 + j0 + q] + u1 * s[33 + j0 + q];
       }
+      __syncwarp();
     }
-    __syncwarp();
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       const float y = part[q] - kc[q];
@@ -1099,15 +1080,10 @@ void launch_camera_pass(const DevLSA &L, double multfact1, cudaStream_t s) {
 
 void launch_pair_pass(const DevLSA &L, cudaStream_t s) {
   if (L.nboff <= 0) return;
-  if (L.rec32) {
-    const int sm = PAIR_WARPS * 32 * PAIR_SS * (int)sizeof(float);
-    cudaFuncSetAttribute(k_pair32, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    k_pair32<<<nblk((long long)L.nboff * 32, 256), 256, sm, s>>>(L);
-  } else {
-    const int sm = PAIR_WARPS * 32 * PAIR_SS * (int)sizeof(double);
-    cudaFuncSetAttribute(k_pair<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    k_pair<double><<<nblk((long long)L.nboff * 32, 256), 256, sm, s>>>(L);
-  }
+  if (L.rec32)
+    k_pair32<<<nblk((long long)L.nboff * 32, 256), 256, 0, s>>>(L);
+  else
+    k_pair<double><<<nblk((long long)L.nboff * 32, 256), 256, 0, s>>>(L);
 }
 
 void launch_backsub(const DevLSA &L, const double *xsol, cudaStream_t s) {

@@ -78,25 +78,48 @@ __device__ void block_features(const DevLSA &L, const double *__restrict__ drs, 
     rn[m] = ei[m] < 9 ? drs[(size_t)k * 9 + ei[m]] : 0.;
     rt[m] = ej[m] < 9 ? drs[(size_t)k * 9 + ej[m]] : 0.;
   }
-  for (int t = L.rowoff[k]; t < L.rowoff[k + 1]; ++t) {
-    const int2 en = L.ent[t];
-    const int col = en.x;
-    if (col == k) continue;
-    const bool tr = en.y < 0;
-    const size_t B = (size_t)(en.y & 0x7fffffff);
-    const double *rc = drs + (size_t)col * 9;
-    const int nc = L.camparv[col + 1] - L.camparv[col];
+  // the row's entries four at a time: their positions, block elements and
+  // column scalings are all loaded before any is used (independent loads in
+  // flight), then added in entry order
+  constexpr int U = 4;
+  const int t0 = L.rowoff[k], t1 = L.rowoff[k + 1];
+  for (int tb = t0; tb < t1; tb += U) {
+    int2 en[U];
+    int nc[U];
+    double v[U][3], rcv[U][3];
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
-      const int i = ei[m], j = ej[m];
-      if (i >= 9) continue;
-      // stored (k, col): element (i, j) couples parameter i of k to j of col;
-      // stored (col, k): it couples parameter j of k to i of col; both
-      // normalised by the two diagonal entries, |S_ij| / sqrt(S_ii S_jj)
-      if (!tr) {
-        if (i < np && j < nc) an[m] += fabs(blk_at(L, B, i * 9 + j)) * rn[m] * __ldg(rc + j);
-      } else {
-        if (j < np && i < nc) at[m] += fabs(blk_at(L, B, i * 9 + j)) * rt[m] * __ldg(rc + i);
+    for (int u = 0; u < U; ++u) {
+      en[u] = tb + u < t1 ? L.ent[tb + u] : make_int2(k, k);
+      nc[u] = L.camparv[en[u].x + 1] - L.camparv[en[u].x];
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const bool tr = en[u].y < 0;
+      const size_t B = (size_t)(en[u].y & 0x7fffffff);
+      const double *rc = drs + (size_t)en[u].x * 9;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        const int i = ei[m], j = ej[m];
+        v[u][m] = i < 9 ? blk_at(L, B, i * 9 + j) : 0.;
+        rcv[u][m] = i < 9 ? __ldg(rc + (tr ? i : j)) : 0.;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (en[u].x == k) continue;  // the diagonal block (and the padding past the row)
+      const bool tr = en[u].y < 0;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        const int i = ei[m], j = ej[m];
+        if (i >= 9) continue;
+        // stored (k, col): element (i, j) couples parameter i of k to j of
+        // col; stored (col, k): it couples parameter j of k to i of col; both
+        // normalised by the two diagonal entries, |S_ij| / sqrt(S_ii S_jj)
+        if (!tr) {
+          if (i < np && j < nc[u]) an[m] += fabs(v[u][m]) * rn[m] * rcv[u][m];
+        } else {
+          if (j < np && i < nc[u]) at[m] += fabs(v[u][m]) * rt[m] * rcv[u][m];
+        }
       }
     }
   }

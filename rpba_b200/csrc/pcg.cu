@@ -600,10 +600,13 @@ __device__ __forceinline__ bool stage_wait(const PcgArgs &A, unsigned long long 
   return true;
 }
 
-// FP32 d^k of camera c (12-float stride) into v[0..8]
+// FP32 d^k of camera c (12-float stride) into v[0..8].  The loads may hit
+// L1: d32 is written in phase D by all CTAs before a grid barrier, whose
+// gpu-scope fence and block barrier order those writes before these loads,
+// and the rows of a cluster keep gathering the same columns.
 __device__ __forceinline__ void load_d32(const float *d32, int c, float (&v)[9]) {
   const float4 *p = (const float4 *)(d32 + (size_t)c * 12);
-  const float4 a = __ldcg(p), b = __ldcg(p + 1), e = __ldcg(p + 2);
+  const float4 a = __ldca(p), b = __ldca(p + 1), e = __ldca(p + 2);
   v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
   v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
   v[8] = e.x;

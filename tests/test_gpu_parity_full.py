@@ -183,5 +183,5 @@ def test_mixed_form_error_against_fp64_oracle(runs, scene, solver, bound):
     print(f"\n{scene} mixed {solver} vs FP64 oracle: cost rel {cost_rel:+.3e}  RMS rel {rms_rel:+.3e}  params "
           + " ".join(f"{k} {v:.2e}" for k, v in pe.items()))
     assert st == 0
-    assert abs(rms_rel) <= bound and abs(cost_rel) <= 2 * bound
+    assert abs(rms_rel) <= bound and abs(cost_rel) <= 4 * bound
     assert pe["XX"] <= 1e-3 and pe["R"] <= 1e-3 and pe["t"] <= 1e-3
