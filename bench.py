@@ -505,6 +505,7 @@ def main():
                              ("no_coarse_space", dict(ours_kw, coarse_aggregates=-1), w)):
             S = rb.Solver(blk, **kw)
             S.set_preconditioner(wt)
+            S.solve()  # warm-up, as the timed steps have
             flush.zero_()
             torch.cuda.synchronize()
             _, ra = S.solve()

@@ -58,9 +58,11 @@ def test_two_level_reaches_direct_rms_in_fewer_iterations(city_blocks):
 def test_learned_correction_gain(city_blocks):
     """Training on the direct solver's systems of two scenes lowers the
     training objective, and on a held-out scene the learned two-level PCG
-    still reaches the direct RMS without fallback; the iteration counts with
-    and without the network are reported (its gain over the coarse space
-    alone is small: at most a 10% regression is allowed)."""
+    reaches the direct RMS without fallback.  What the network gains over
+    the same two-level preconditioner without it is printed: with the
+    coarse space in place it is about one percent of the PCG iterations or
+    less (the coarse space carries the gain over block-Jacobi); the test
+    holds it to no more than a 2% regression."""
     import rpba_b200 as rb
     train, held = city_blocks
     w, rep = rb.train_preconditioner(train, steps=300, lr=1e-3, probes=4)
@@ -71,10 +73,12 @@ def test_learned_correction_gain(city_blocks):
     ref = _solve(held, solver=rb.SOLVER_DIRECT)
     plain = _solve(held, solver=rb.SOLVER_LEARNED, pcg_tolerance=1e-6)
     learned = _solve(held, w, solver=rb.SOLVER_LEARNED, pcg_tolerance=1e-6)
-    print(f"iterations: two-level {plain['pcg_iterations']}  learned two-level {learned['pcg_iterations']}")
+    gain = 1.0 - learned["pcg_iterations"] / plain["pcg_iterations"]
+    print(f"iterations: two-level {plain['pcg_iterations']}  learned two-level {learned['pcg_iterations']}  "
+          f"gain {100 * gain:+.1f}%")
     assert learned["pcg_fallbacks"] == 0
     assert abs(learned["rms"] - ref["rms"]) <= 1e-6 * ref["rms"]
-    assert learned["pcg_iterations"] <= 1.1 * plain["pcg_iterations"]
+    assert gain >= -0.02
 
 
 def _spmv(ts, x):
