@@ -720,6 +720,23 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
           dst[lane] = racc;
         }
       };
+      // per-lane running sums of the open row over the groups inside it,
+      // folded into racc (lanes 0..8) at the row's end in a fixed butterfly
+      double lacc[9];
+#pragma unroll
+      for (int j = 0; j < 9; ++j) lacc[j] = 0.;
+      auto fold_lanes = [&]() {
+        double v = 0.;
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+          double a = lacc[j];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+          if (lane == j) v = a;
+          lacc[j] = 0.;
+        }
+        racc += v;
+      };
       if (g0 < g1 && lane == 0) group_issue(A, group_of(g0, (int)gd, A.row0, A.row1, A.nboff), stg, mbar);
       bool ok = true;
       for (long long g = g0; g < g1; ++g) {
@@ -785,9 +802,19 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
         fence_proxy_async();
         __syncwarp();
         if (lane == 0) bulk_store(A.tpart + q.boff * 9, outb, ((unsigned)q.n * 36u + 15u) & ~15u);
-        // segmented scan of the row products (rows non-decreasing in lane
-        // order; inactive lanes carry distinct negative rows)
         const int row = rc.x;
+        // a group inside the open row (most groups: a row has hundreds of
+        // blocks): every lane adds its product to its own FP64 running sum
+        if (cur_row >= 0 && __all_sync(0xffffffffu, !act || row == cur_row)) {
+          if (act)
+#pragma unroll
+            for (int j = 0; j < 9; ++j) lacc[j] += (double)y[j];
+          continue;
+        }
+        // a row boundary: the lanes' running sums join the open row's sum,
+        // then a segmented scan of the group's products (rows non-decreasing
+        // in lane order; inactive lanes carry distinct negative rows)
+        fold_lanes();
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
           const int ru = __shfl_up_sync(0xffffffffu, row, o);
@@ -824,7 +851,10 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
           seg_first = e + 1;
         }
       }
-      if (ok) flush();
+      if (ok) {
+        fold_lanes();
+        flush();
+      }
       if (lane == 0) bulk_wait_all();
       __syncwarp();
       if (!ok) {
