@@ -260,11 +260,17 @@ def rooflines(kstats, hbm, peak_kind):
                                  "this launch's algorithmic bytes") if ratio else None,
                 "algorithmic_bytes_per_launch": alg, "avg_launch_ms": d["ms"] / d["launches"]}
     if dom == "pcg" and rcs and rcs.get("fp32"):
-        nb = rcs["offdiag_blocks"]
-        full_it = 332.0 * (rcs["rows"] + nb) + 80.0 * nb + rcs["rows"] * (648.0 + 22 * 72.0 + 2 * 720.0 + 2 * 72.0)
-        minimal = alg * (full_it - 80.0 * nb) / full_it
+        # the library's count per iteration (solver.cu): blocks with their
+        # 16 B index, the transposed products' 64 B slots written and read,
+        # the per-row vectors; minimal: each block once with an 8 B index
+        nb, rows = rcs["offdiag_blocks"], rcs["rows"]
+        per_row = rows * (648.0 + 22 * 72.0 + 2 * 720.0 + 2 * 72.0)
+        full_it = 340.0 * (rows + nb) + 128.0 * nb + per_row
+        min_it = 332.0 * (rows + nb) + per_row
+        minimal = alg * min_it / full_it
         roofline["frac_minimal_bytes"] = minimal / avg_s / 1e9 / hbm
-        roofline["minimal_bytes_note"] = "each block read once with its entry, no transposed-product round trip"
+        roofline["minimal_bytes_note"] = ("each block read once with an 8 B index, no transposed-product round trip "
+                                          "and no slot padding")
     return roofline, kernels
 
 

@@ -67,9 +67,10 @@ struct DevLSA {
   const int *row_item_off;  // [nimg + 1]
   const int4 *item_meta;    // (row, first entry, end entry, 0)
   const int2 *rowspan;      // [nimg] (diagonal entry, end entry) of each row
-  float *tpart;             // [nboff * 9] FP32 form: transposed block products
-  const int2 *bidx;         // FP32 form: (row, column) of every block, storage order
+  float *tpart;             // [nboff * 16] FP32 form: transposed block products, column order
+  const int4 *bidx;         // FP32 form: (row, column, transposed slot, 0) of every block, storage order
   const int *firstN;        // [nimg + 1] first off-diagonal block of every row
+  const int *firstT;        // [nimg + 1] first transposed slot of every row (blocks in its column)
   int *err;            // device error word
   // Test hook of the bounded waits (rpba_debug_barrier_timeout): the PCG's
   // grid barriers wait for bar_extra CTAs more than the launch has, for at
@@ -305,7 +306,7 @@ struct StructWork {
   int *bcnt, *boff;
   int *nrun;
   int *cntN, *cntT, *firstN, *firstT, *rowtmp;
-  int2 *bidx;  // FP32 form: (row, column) of every block in storage order
+  int4 *bidx;  // FP32 form: (row, column, transposed slot, 0) of every block in storage order
   unsigned *tkey, *tkey2;
   int *tidx, *tidx2;
   int2 *contrib;

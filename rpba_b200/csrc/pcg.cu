@@ -43,8 +43,8 @@ struct PcgArgs {
   // FP32 form (k_pcg32): (row, column) of every block in storage order, the
   // first off-diagonal block of every row, d^k in FP32 (12 floats a camera),
   // and the phase-1 row sums (diagonal, row head, warp-run head)
-  const int2 *bidx;
-  const int *firstN;
+  const int4 *bidx;
+  const int *firstN, *firstT;
   int nboff;
   float *d32;
   double *pdiag, *prow, *pw;
@@ -474,11 +474,16 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
 // triangle, row major).  The stream is cut into groups of 32 blocks, and
 // every warp owns a contiguous run of groups (equal counts, so every warp
 // moves the same bytes).  One elected lane copies a group's blocks (32 x
-// 324 B) and their (row, column) pairs into the warp's stage, completing on
-// the stage's mbarrier; each lane then owns one block: it forms the block's
-// row product B d_col (summed into its row) and, for an off-diagonal block,
-// the transposed product B^T d_row, which goes to the block's slot of tpart
-// through a bulk store of the whole group.  Lane i reads its block at byte
+// 324 B) and their (row, column, slot) triples into the warp's stage,
+// completing on the stage's mbarrier; each lane then owns one block: it forms
+// the block's row product B d_col (summed into its row) and, for an
+// off-diagonal block, the transposed product B^T d_row, which goes to the
+// block's slot of tpart.  The slots are in column order (the blocks of
+// column c, i.e. the transposed entries of row c, are consecutive), and a
+// slot is 64 bytes (9 values, zero padding: two whole sectors, so the
+// scattered writes need no read of the rest of a sector), so that phase 2
+// reads each row's transposed products as one contiguous run.  Lane i reads
+// its block at byte
 // 324 i of the stage: 81 i is a distinct bank for every lane, so the reads
 // are conflict-free.  The gathered vector is d^k rounded to FP32 (d32, 12
 // floats per camera so that a camera is three aligned 16-byte loads),
@@ -490,8 +495,8 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
 // (row, warp run): to prow[row] by the warp that holds the row's first block,
 // to pw[warp] by a warp whose run starts inside the row.  Phase 2 adds, per
 // row and in a fixed order, pdiag, prow, the pw of the runs that start inside
-// the row, and the transposed products of the row's blocks stored by earlier
-// rows (its transposed entries).
+// the row, and the row's run of transposed products (the blocks stored by
+// earlier rows in its column).
 //
 // Iteration k: phase D (d^k = h + beta d^(k-1), FP64 and FP32 copies),
 // barrier, phase 1 (A d^k and d^T A d), barrier, phase 2 (as in the FP64
@@ -501,11 +506,10 @@ constexpr int P32_W = 16;  // warps per CTA
 constexpr int P32_T = P32_W * 32;
 constexpr int GB = 32;     // blocks per group: one per lane
 constexpr int STG_BLK = GB * 324 + 16;
-constexpr int STG_IDX = GB * 8 + 16;
-constexpr int STG_OUT = GB * 36;
-constexpr int STG_BYTES = STG_BLK + STG_IDX + STG_OUT + 16;  // + the mbarrier
+constexpr int STG_IDX = GB * 16;
+constexpr int STG_BYTES = STG_BLK + STG_IDX + 16;  // + the mbarrier
 constexpr size_t P32_SMEM = (size_t)P32_W * STG_BYTES;
-static_assert(STG_BLK % 16 == 0 && STG_IDX % 16 == 0 && STG_OUT % 16 == 0, "16-byte aligned stage parts");
+static_assert(STG_BLK % 16 == 0 && STG_IDX % 16 == 0, "16-byte aligned stage parts");
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
@@ -532,14 +536,6 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned b
                "l"(src), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
-__device__ __forceinline__ void bulk_store(void *dst, const void *src, unsigned bytes) {
-  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;\n" ::"l"(dst), "r"(smem_u32(src)),
-               "r"(bytes)
-               : "memory");
-  asm volatile("cp.async.bulk.commit_group;\n" ::: "memory");
-}
-__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;\n" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;\n" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
 
 // Group g of the stream: its first block (storage index), its block count
@@ -573,20 +569,18 @@ __device__ __forceinline__ long long run_start(long long w, long long ng, long l
 __device__ __forceinline__ unsigned blk_misalign(const float *blocks, long long start) {
   return (unsigned)(((unsigned long long)(blocks + start * 81)) & 15ull);
 }
-__device__ __forceinline__ unsigned idx_misalign(const int2 *bidx, long long start) {
-  return (unsigned)(((unsigned long long)(bidx + start)) & 15ull);
-}
+constexpr int TP_STRIDE = 16;  // floats per transposed-product slot (64 B)
 
 // Issue the copies of group q into the warp's stage (one lane).
 __device__ __forceinline__ void group_issue(const PcgArgs &A, const Grp32 &q, unsigned char *stg,
                                             unsigned long long *bar) {
   const float *blocks = (const float *)A.blocks;
-  const unsigned mb = blk_misalign(blocks, q.start), mi = idx_misalign(A.bidx, q.start);
+  const unsigned mb = blk_misalign(blocks, q.start);
   const unsigned nb_bytes = (mb + (unsigned)q.n * 324u + 15u) & ~15u;
-  const unsigned ni_bytes = (mi + (unsigned)q.n * 8u + 15u) & ~15u;
+  const unsigned ni_bytes = (unsigned)q.n * 16u;
   mbar_expect_tx(bar, nb_bytes + ni_bytes);
   bulk_load(stg, (const unsigned char *)(blocks + q.start * 81) - mb, nb_bytes, bar);
-  bulk_load(stg + STG_BLK, (const unsigned char *)(A.bidx + q.start) - mi, ni_bytes, bar);
+  bulk_load(stg + STG_BLK, A.bidx + q.start, ni_bytes, bar);
 }
 
 // Bounded wait on the stage's mbarrier (the copies of this CTA's own
@@ -615,18 +609,26 @@ __device__ __forceinline__ void load_d32(const float *d32, int c, float (&v)[9])
 // q of one row in lanes < 9 (FP32 form).
 __device__ __forceinline__ double row_q32(const PcgArgs &A, int row, long long ng, long long nw, long long gd,
                                           int lane) {
-  // transposed products of the blocks stored by earlier rows: one entry per
-  // lane, nine FP64 partial sums, then a fixed butterfly
+  // the row's run of transposed products (slots firstT[row] ..
+  // firstT[row + 1]): one slot per lane (three 16-byte loads), nine FP64
+  // partial sums, then a fixed butterfly
   double acc[9];
 #pragma unroll
   for (int j = 0; j < 9; ++j) acc[j] = 0.;
-  const int e0 = __ldg(A.rowoff + row), e1 = __ldg(&A.rowspan[row].x);
-#pragma unroll 2
+  const int e0 = __ldg(A.firstT + row), e1 = __ldg(A.firstT + row + 1);
+#pragma unroll 4
   for (int e = e0 + lane; e < e1; e += 32) {
-    const long long b = (long long)(__ldg(&A.ent[e].y) & 0x7fffffff) - A.row1;
-    const float *t = A.tpart + b * 9;
-#pragma unroll
-    for (int j = 0; j < 9; ++j) acc[j] += (double)__ldcg(t + j);
+    const float4 *t = (const float4 *)(A.tpart + (size_t)e * TP_STRIDE);
+    const float4 a = __ldcg(t), b = __ldcg(t + 1), c = __ldcg(t + 2);
+    acc[0] += (double)a.x;
+    acc[1] += (double)a.y;
+    acc[2] += (double)a.z;
+    acc[3] += (double)a.w;
+    acc[4] += (double)b.x;
+    acc[5] += (double)b.y;
+    acc[6] += (double)b.z;
+    acc[7] += (double)b.w;
+    acc[8] += (double)c.x;
   }
 #pragma unroll
   for (int j = 0; j < 9; ++j)
@@ -664,8 +666,7 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
   __shared__ double sh[P32_W + 1][4];
   extern __shared__ __align__(16) unsigned char pcg_dyn[];
   unsigned char *stg = pcg_dyn + (size_t)warp * STG_BYTES;
-  float *outb = (float *)(stg + STG_BLK + STG_IDX);
-  unsigned long long *mbar = (unsigned long long *)(stg + STG_BLK + STG_IDX + STG_OUT);
+  unsigned long long *mbar = (unsigned long long *)(stg + STG_BLK + STG_IDX);
   unsigned parity = 0;
   if (lane == 0) mbar_init(mbar, 1);
   asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -746,9 +747,9 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
           break;
         }
         parity ^= 1u;
-        const unsigned mb = blk_misalign(blocks, q.start), mi = idx_misalign(A.bidx, q.start);
+        const unsigned mb = blk_misalign(blocks, q.start);
         const bool act = lane < q.n;
-        int2 rc = make_int2(-1 - lane, -1);
+        int4 rc = make_int4(-1 - lane, -1, 0, 0);
         float dc[9], dr[9], y[9], t[9];
 #pragma unroll
         for (int j = 0; j < 9; ++j) {
@@ -756,7 +757,7 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
           t[j] = 0.f;
         }
         if (act) {
-          rc = *(const int2 *)(stg + STG_BLK + mi + 8 * lane);
+          rc = *(const int4 *)(stg + STG_BLK + 16 * lane);
           load_d32(A.d32, rc.y, dc);
           load_d32(A.d32, rc.x, dr);
           const float *B = (const float *)(stg + mb + 324 * lane);
@@ -793,15 +794,14 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
           }
           continue;
         }
-        // transposed products: staged, then one bulk store of the group
-        if (lane == 0) bulk_wait_read();
-        __syncwarp();
-        if (act)
-#pragma unroll
-          for (int j = 0; j < 9; ++j) outb[9 * lane + j] = t[j];
-        fence_proxy_async();
-        __syncwarp();
-        if (lane == 0) bulk_store(A.tpart + q.boff * 9, outb, ((unsigned)q.n * 36u + 15u) & ~15u);
+        // the transposed product to the block's slot (column order)
+        if (act) {
+          float4 *dst = (float4 *)(A.tpart + (size_t)rc.z * TP_STRIDE);
+          __stcg(dst, make_float4(t[0], t[1], t[2], t[3]));
+          __stcg(dst + 1, make_float4(t[4], t[5], t[6], t[7]));
+          __stcg(dst + 2, make_float4(t[8], 0.f, 0.f, 0.f));
+          __stcg(dst + 3, make_float4(0.f, 0.f, 0.f, 0.f));
+        }
         const int row = rc.x;
         // a group inside the open row (most groups: a row has hundreds of
         // blocks): every lane adds its product to its own FP64 running sum
@@ -855,7 +855,6 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
         fold_lanes();
         flush();
       }
-      if (lane == 0) bulk_wait_all();
       __syncwarp();
       if (!ok) {
         // a copy that never completed: record it, give it one more bounded
@@ -864,8 +863,6 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
         stage_wait(A, mbar, parity);
       }
     }
-    // the transposed products (async-proxy writes) before the barrier's release
-    asm volatile("fence.proxy.async.global;\n" ::: "memory");
     {
       double v[1] = {pdq};
       cta_sum<1, P32_W>(v, sh);
@@ -1128,6 +1125,7 @@ int pcg_iterate(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStre
   A.tpart = L.tpart;
   A.bidx = L.bidx;
   A.firstN = L.firstN;
+  A.firstT = L.firstT;
   A.nboff = L.nboff;
   A.d32 = W.d32;
   A.pdiag = W.pdiag;

@@ -272,16 +272,15 @@ struct rpba_handle {
 
   // Algorithmic bytes of one PCG iteration.  FP64 form: every block read from
   // both sides with its entry (648 + 8 B per side).  FP32 form (symmetric):
-  // every block read once with its entry (324 + 8 B), and per off-diagonal
-  // block the transposed product written and read (36 B each) with the
-  // transposed entry (8 B).  Per camera row: the preconditioner (648 B) and
+  // every block read once with its index (324 + 16 B), and per off-diagonal
+  // block the transposed product written and read (a 64 B slot each way).  Per camera row: the preconditioner (648 B) and
   // 22 reads/writes of 9-vectors (72 B each); with the coarse space P_k twice
   // (720 B each) and the block part of h twice; A_c^-1 stays in L2 and is
   // not counted.
   double pcg_bytes_per_iteration(bool coarse) const {
     const double Nc = nimg - begini, Nb = L.nboff;
     const double row = 648. + 22. * 72. + (coarse ? 2. * 720. + 2. * 72. : 0.);
-    const double blocks = L.blocks32 ? 332. * (Nc + Nb) + 80. * Nb : 656. * (Nc + 2. * Nb);
+    const double blocks = L.blocks32 ? 340. * (Nc + Nb) + 128. * Nb : 656. * (Nc + 2. * Nb);
     return blocks + Nc * row;
   }
 
@@ -308,8 +307,8 @@ struct rpba_handle {
       // slack past the last block, row pair and transposed product: the
       // FP32 PCG's bulk copies round their sizes up to 16 bytes
       L.blocks32 = dalloc<float>((size_t)(nimg + cap) * BS32 + 16, owned);
-      L.tpart = dalloc<float>((size_t)cap * 9 + 16, owned);
-      S.bidx = dalloc<int2>((size_t)nimg + cap + 4, owned);
+      L.tpart = dalloc<float>((size_t)cap * 16 + 16, owned);
+      S.bidx = dalloc<int4>((size_t)nimg + cap + 4, owned);
     } else
       L.blocks = dalloc<double>((size_t)(nimg + cap) * BS64, owned);
     S.ent = dalloc<int2>((size_t)nimg + 2 * (size_t)cap, owned);

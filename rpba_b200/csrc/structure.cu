@@ -142,17 +142,24 @@ __global__ void k_fill_items(const int *rowoff, const int *cntT, const int *row_
   }
 }
 
-// (row, column) of every block of the reduced camera system in storage
-// order: the diagonal blocks, then the off-diagonal blocks (key row * n + col)
-__global__ void k_fill_bidx(const unsigned *bkey, int nb, int nimg, int2 *bidx) {
+// (row, column, transposed slot) of every block of the reduced camera
+// system in storage order: the diagonal blocks, then the off-diagonal blocks
+// (key row * n + col); the slot of an off-diagonal block is its position in
+// column order (the sorted transposed keys), -1 for a diagonal block
+__global__ void k_fill_bidx(const unsigned *bkey, int nb, int nimg, int4 *bidx) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)nimg + nb) return;
   if (i < nimg) {
-    bidx[i] = make_int2((int)i, (int)i);
+    bidx[i] = make_int4((int)i, (int)i, -1, 0);
   } else {
     const unsigned key = bkey[i - nimg];
-    bidx[i] = make_int2((int)(key / (unsigned)nimg), (int)(key % (unsigned)nimg));
+    bidx[i] = make_int4((int)(key / (unsigned)nimg), (int)(key % (unsigned)nimg), 0, 0);
   }
+}
+__global__ void k_fill_slots(const int *tidx_sorted, int nb, int nimg, int4 *bidx) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nb) return;
+  bidx[nimg + tidx_sorted[q]].z = q;
 }
 
 __global__ void k_fill_diag(int nimg, const int *rowoff, const int *cntT, int2 *ent) {
@@ -259,8 +266,10 @@ void build_bsr(DevLSA &L, StructWork &S, cudaStream_t s) {
   k_fill_items<<<nblk(n, 256), 256, 0, s>>>(S.rowoff, S.cntT, S.row_item_off, n, L.begini, sym, S.item_meta);
   if (L.blocks32) {
     k_fill_bidx<<<nblk((long long)n + nb, 256), 256, 0, s>>>(S.bkey, nb, n, S.bidx);
+    if (nb > 0) k_fill_slots<<<nblk(nb, 256), 256, 0, s>>>(S.tidx2, nb, n, S.bidx);
     L.bidx = S.bidx;
     L.firstN = S.firstN;
+    L.firstT = S.firstT;
   }
   L.rowoff = S.rowoff;
   L.ent = S.ent;
