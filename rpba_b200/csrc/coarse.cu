@@ -111,62 +111,25 @@ __global__ void k_entry_keys(DevLSA L, CoarseWork C, unsigned *key, int *val) {
 }
 
 constexpr int RS_T = 256;
-constexpr int RS_PF = 4;  // entries whose values are in flight per warp
-// One warp per run (row k, aggregate b): Y = sum over the run's entries of
-// S_kl P_l (9 x CO_M), then Z = P_k^T Y.  The block and P_l of an entry are
-// loaded coalesced (each lane three values of each) into a register ring
-// RS_PF entries ahead, staged in shared memory and multiplied there, in
-// entry order.
 __global__ void __launch_bounds__(RS_T) k_coarse_runs(DevLSA L, CoarseWork C, int nruns) {
   __shared__ double Ysh[RS_T / 32][9 * CO_M];
-  __shared__ double Bs[RS_T / 32][81];
-  __shared__ double Ps[RS_T / 32][9 * CO_M];
   const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   if (r >= nruns) return;
   const int k = (int)(C.run_key[r] / (unsigned)C.nagg);
   const int npk = L.camparv[k + 1] - L.camparv[k];
-  const int t0 = C.run_off[r], t1 = C.run_off[r + 1];
-  auto fetch = [&](int t, double (&bv)[3], double (&pv)[3], int2 &en) {
-    en = L.ent[C.ent_sorted[t]];
-    const size_t B = (size_t)(en.y & 0x7fffffff);
-    const double *Pl = C.P + (size_t)en.x * CP;
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      const int e = lane + 32 * q;
-      bv[q] = e < 81 ? blk_at(L, B, e) : 0.;
-      pv[q] = e < 9 * CO_M ? Pl[e] : 0.;
-    }
-  };
-  double bv[RS_PF][3], pv[RS_PF][3];
-  int2 env[RS_PF];
-#pragma unroll
-  for (int u = 0; u < RS_PF; ++u)
-    if (t0 + u < t1) fetch(t0 + u, bv[u], pv[u], env[u]);
   double y[3] = {0., 0., 0.};
-  for (int tb = t0; tb < t1; tb += RS_PF) {
+  for (int t = C.run_off[r]; t < C.run_off[r + 1]; ++t) {
+    const int2 en = L.ent[C.ent_sorted[t]];
+    const int l = en.x;
+    const bool tr = en.y < 0;
+    const size_t B = (size_t)(en.y & 0x7fffffff);
+    const double *Pl = C.P + (size_t)l * CP;
+    const int npl = L.camparv[l + 1] - L.camparv[l];
 #pragma unroll
-    for (int u = 0; u < RS_PF; ++u) {
-      const int t = tb + u;
-      if (t >= t1) break;
-#pragma unroll
-      for (int q = 0; q < 3; ++q) {
-        const int e = lane + 32 * q;
-        if (e < 81) Bs[wl][e] = bv[u][q];
-        if (e < 9 * CO_M) Ps[wl][e] = pv[u][q];
-      }
-      const int2 en = env[u];
-      if (t + RS_PF < t1) fetch(t + RS_PF, bv[u], pv[u], env[u]);
-      __syncwarp();
-      const int l = en.x;
-      const bool tr = en.y < 0;
-      const int npl = L.camparv[l + 1] - L.camparv[l];
-#pragma unroll
-      for (int m = 0; m < 3; ++m) {
-        const int o = lane + 32 * m, p = o / CO_M, j = o % CO_M;
-        if (o < 9 * CO_M && p < npk)
-          for (int q = 0; q < npl; ++q) y[m] += Bs[wl][tr ? q * 9 + p : p * 9 + q] * Ps[wl][q * CO_M + j];
-      }
-      __syncwarp();
+    for (int m = 0; m < 3; ++m) {
+      const int o = lane + 32 * m, p = o / CO_M, j = o % CO_M;
+      if (o < 9 * CO_M && p < npk)
+        for (int q = 0; q < npl; ++q) y[m] += blk_at(L, B, tr ? q * 9 + p : p * 9 + q) * Pl[q * CO_M + j];
     }
   }
 #pragma unroll

@@ -475,8 +475,6 @@ __global__ void __launch_bounds__(CAM_T) k_camera(DevLSA L, double multfact1) {
 }
 
 // ----------------------------------------------------------- pair pass
-// Contributions whose record values are in flight at a time per warp.
-constexpr int PAIR_PF = 4;
 // Off-diagonal blocks: S_kl = - sum_p W_pk V_p^-1 W_pl^T over the points
 // seen by both cameras (rbacore.cpp:1362-1390), with W_po = Bc^T G.  One
 // warp per block sums its contributions in a fixed order.  FP64 form; the
@@ -503,8 +501,8 @@ __global__ void k_pair(DevLSA L) {
   const int cb = L.boff[wid], ce = L.boff[wid + 1];
   for (int c0 = cb; c0 < ce; c0 += 32) {
     // the next (up to) 32 contributions' observation pairs and points, one
-    // per lane; the record values of contribution j + PAIR_PF are fetched
-    // while j is accumulated
+    // per lane; the record values of contribution j + 1 are fetched while j
+    // is accumulated
     const int n = min(32, ce - c0);
     int2 pr = make_int2(0, 0);
     int pp = 0;
@@ -512,50 +510,41 @@ __global__ void k_pair(DevLSA L) {
       pr = L.contrib[c0 + lane];
       pp = L.o_pt[pr.x];
     }
-    // PAIR_PF contributions' values in flight at a time (a register ring)
-    T v0[PAIR_PF], v1[PAIR_PF];
+    T v0, v1;
+    fetch(__shfl_sync(0xffffffffu, pr.x, 0), __shfl_sync(0xffffffffu, pr.y, 0), __shfl_sync(0xffffffffu, pp, 0),
+          v0, v1);
+    for (int j = 0; j < n; ++j) {
+      s[lane] = v0;
+      if (lane + 32 < NV) s[lane + 32] = v1;
+      if (j + 1 < n)
+        fetch(__shfl_sync(0xffffffffu, pr.x, j + 1), __shfl_sync(0xffffffffu, pr.y, j + 1),
+              __shfl_sync(0xffffffffu, pp, j + 1), v0, v1);
+      __syncwarp();
+      // N = G_s V^-1 G_t^T (2 x 2)
+      const T *Gs = s + 18, *Gt = s + 42, *Vi = s + 48;
+      T GV[2][3], N[2][2];
 #pragma unroll
-    for (int u = 0; u < PAIR_PF; ++u)
-      if (u < n)
-        fetch(__shfl_sync(0xffffffffu, pr.x, u), __shfl_sync(0xffffffffu, pr.y, u), __shfl_sync(0xffffffffu, pp, u),
-              v0[u], v1[u]);
-    for (int jb = 0; jb < n; jb += PAIR_PF) {
+      for (int a = 0; a < 2; ++a)
 #pragma unroll
-      for (int u = 0; u < PAIR_PF; ++u) {
-        const int j = jb + u;
-        if (j >= n) break;
-        s[lane] = v0[u];
-        if (lane + 32 < NV) s[lane + 32] = v1[u];
-        if (j + PAIR_PF < n)
-          fetch(__shfl_sync(0xffffffffu, pr.x, j + PAIR_PF), __shfl_sync(0xffffffffu, pr.y, j + PAIR_PF),
-                __shfl_sync(0xffffffffu, pp, j + PAIR_PF), v0[u], v1[u]);
-        __syncwarp();
-        // N = G_s V^-1 G_t^T (2 x 2)
-        const T *Gs = s + 18, *Gt = s + 42, *Vi = s + 48;
-        T GV[2][3], N[2][2];
+        for (int b = 0; b < 3; ++b)
+          GV[a][b] = Gs[a * 3] * Vi[b] + Gs[a * 3 + 1] * Vi[3 + b] + Gs[a * 3 + 2] * Vi[6 + b];
 #pragma unroll
-        for (int a = 0; a < 2; ++a)
+      for (int a = 0; a < 2; ++a)
 #pragma unroll
-          for (int b = 0; b < 3; ++b)
-            GV[a][b] = Gs[a * 3] * Vi[b] + Gs[a * 3 + 1] * Vi[3 + b] + Gs[a * 3 + 2] * Vi[6 + b];
+        for (int b = 0; b < 2; ++b)
+          N[a][b] = GV[a][0] * Gt[b * 3] + GV[a][1] * Gt[b * 3 + 1] + GV[a][2] * Gt[b * 3 + 2];
 #pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-          for (int b = 0; b < 2; ++b)
-            N[a][b] = GV[a][0] * Gt[b * 3] + GV[a][1] * Gt[b * 3 + 1] + GV[a][2] * Gt[b * 3 + 2];
-#pragma unroll
-        for (int q = 0; q < 3; ++q) {
-          const int e = lane + 32 * q;
-          if (e < 81) {
-            const int i = e / 9, jj = e % 9;
-            const T bt0 = s[24 + jj], bt1 = s[24 + 9 + jj];
-            const T t0 = N[0][0] * bt0 + N[0][1] * bt1;
-            const T t1 = N[1][0] * bt0 + N[1][1] * bt1;
-            acc[q].add(-(s[i] * t0 + s[9 + i] * t1));
-          }
+      for (int q = 0; q < 3; ++q) {
+        const int e = lane + 32 * q;
+        if (e < 81) {
+          const int i = e / 9, jj = e % 9;
+          const T bt0 = s[24 + jj], bt1 = s[24 + 9 + jj];
+          const T t0 = N[0][0] * bt0 + N[0][1] * bt1;
+          const T t1 = N[1][0] * bt0 + N[1][1] * bt1;
+          acc[q].add(-(s[i] * t0 + s[9 + i] * t1));
         }
-        __syncwarp();
       }
+      __syncwarp();
     }
   }
   T *B = Store<T>::blocks(L) + (size_t)(L.nimg + wid) * Store<T>::BS;
@@ -593,39 +582,29 @@ __global__ void __launch_bounds__(256) k_pair32(DevLSA L) {
     const int n = min(32, ce - c0);
     int2 pr = make_int2(0, 0);
     if (lane < n) pr = L.contrib[c0 + lane];
-    // the records of PAIR_PF contributions are in flight at a time (a ring
-    // in registers); contribution j is accumulated from the shared stage
-    float v0[PAIR_PF], v1[PAIR_PF];
-#pragma unroll
-    for (int u = 0; u < PAIR_PF; ++u)
-      if (u < n) fetch(__shfl_sync(0xffffffffu, pr.x, u), __shfl_sync(0xffffffffu, pr.y, u), v0[u], v1[u]);
+    float v0, v1;
+    fetch(__shfl_sync(0xffffffffu, pr.x, 0), __shfl_sync(0xffffffffu, pr.y, 0), v0, v1);
     float part[3] = {0.f, 0.f, 0.f};
-    for (int jb = 0; jb < n; jb += PAIR_PF) {
-#pragma unroll
-      for (int u = 0; u < PAIR_PF; ++u) {
-        const int j = jb + u;
-        if (j >= n) break;
-        s[lane] = v0[u];
-        if (lane < 16) s[32 + lane] = v1[u];
-        if (j + PAIR_PF < n)
-          fetch(__shfl_sync(0xffffffffu, pr.x, j + PAIR_PF), __shfl_sync(0xffffffffu, pr.y, j + PAIR_PF), v0[u],
-                v1[u]);
-        __syncwarp();
-        float nab = 0.f;
-        if (lane < 4) {
-          const float *hx = s + 18 + 3 * (lane >> 1), *hy = s + 42 + 3 * (lane & 1);
-          nab = hx[0] * hy[0] + hx[1] * hy[1] + hx[2] * hy[2];
-        }
-        const float n00 = __shfl_sync(0xffffffffu, nab, 0), n01 = __shfl_sync(0xffffffffu, nab, 1);
-        const float n10 = __shfl_sync(0xffffffffu, nab, 2), n11 = __shfl_sync(0xffffffffu, nab, 3);
-        if (lane < 27) {
-          const float bx0 = s[i], bx1 = s[9 + i];
-          const float u0 = bx0 * n00 + bx1 * n10, u1 = bx0 * n01 + bx1 * n11;
-#pragma unroll
-          for (int q = 0; q < 3; ++q) part[q] -= u0 * s[24 + j0 + q] + u1 * s[33 + j0 + q];
-        }
-        __syncwarp();
+    for (int j = 0; j < n; ++j) {
+      s[lane] = v0;
+      if (lane < 16) s[32 + lane] = v1;
+      if (j + 1 < n)
+        fetch(__shfl_sync(0xffffffffu, pr.x, j + 1), __shfl_sync(0xffffffffu, pr.y, j + 1), v0, v1);
+      __syncwarp();
+      float nab = 0.f;
+      if (lane < 4) {
+        const float *hx = s + 18 + 3 * (lane >> 1), *hy = s + 42 + 3 * (lane & 1);
+        nab = hx[0] * hy[0] + hx[1] * hy[1] + hx[2] * hy[2];
       }
+      const float n00 = __shfl_sync(0xffffffffu, nab, 0), n01 = __shfl_sync(0xffffffffu, nab, 1);
+      const float n10 = __shfl_sync(0xffffffffu, nab, 2), n11 = __shfl_sync(0xffffffffu, nab, 3);
+      if (lane < 27) {
+        const float bx0 = s[i], bx1 = s[9 + i];
+        const float u0 = bx0 * n00 + bx1 * n10, u1 = bx0 * n01 + bx1 * n11;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) part[q] -= u0 * s[24 + j0 + q] + u1 * s[33 + j0 + q];
+      }
+      __syncwarp();
     }
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
