@@ -551,7 +551,7 @@ __global__ void k_pair(DevLSA L) {
 #pragma unroll
   for (int q = 0; q < 3; ++q) {
     const int e = lane + 32 * q;
-    if (e < 81) B[e] = (T)acc[q].value();
+    if (e < 81) __stcs(B + e, (T)acc[q].value());  // streaming: keep L2 for the records
   }
 }
 
@@ -617,7 +617,7 @@ __global__ void __launch_bounds__(256) k_pair32(DevLSA L) {
   if (lane < 27) {
     float *B = L.blocks32 + (size_t)(L.nimg + wid) * BS32 + i * 9 + j0;
 #pragma unroll
-    for (int q = 0; q < 3; ++q) B[q] = (float)((double)ks[q] - (double)kc[q]);
+    for (int q = 0; q < 3; ++q) __stcs(B + q, (float)((double)ks[q] - (double)kc[q]));  // keep L2 for the records
   }
 }
 
