@@ -491,9 +491,11 @@ def main():
         e2e_times.append(time.perf_counter() - t0)
     e2e = max_over_ranks(statistics.median(e2e_times))
 
-    # per-kernel device times of one more solve (CUDA events around launches)
+    # per-kernel device times of one more solve (CUDA events around
+    # launches), after a warm-up solve on the same handle like the timed ones
     P = rb.Solver(blk, verbose=2, **ours_kw)
     P.set_preconditioner(w)
+    P.solve()
     P.solve()
     kstats = P.kernel_stats()
     P.close()

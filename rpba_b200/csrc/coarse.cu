@@ -100,12 +100,17 @@ __global__ void k_coarse_P(DevLSA L, CoarseWork C) {
 //     Z = P_k^T Y (10 x 10).
 //  3. The runs sorted by (aggregate of k, b) (stable: row order); one warp
 //     per coarse block (a, b) sums its runs' Z in that order.
+// A_c is symmetric (S is): only the blocks (a, b) with b >= a are summed,
+// and each block with b > a is written to (b, a) transposed as well, so
+// the entries (k, l) whose column's aggregate precedes the row's are left
+// out of the runs.
 __global__ void k_entry_keys(DevLSA L, CoarseWork C, unsigned *key, int *val) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= L.nimg) return;
+  const int a = C.row_agg[k];
   for (int e = L.rowoff[k]; e < L.rowoff[k + 1]; ++e) {
     const int b = C.row_agg[L.ent[e].x];
-    key[e] = b < 0 ? 0xffffffffu : (unsigned)k * (unsigned)C.nagg + (unsigned)b;
+    key[e] = (b < 0 || b < a) ? 0xffffffffu : (unsigned)k * (unsigned)C.nagg + (unsigned)b;
     val[e] = e;
   }
 }
@@ -176,7 +181,10 @@ __global__ void k_coarse_blocks(CoarseWork C, int nsegs) {
 #pragma unroll
   for (int m = 0; m < 4; ++m) {
     const int o = lane + 32 * m, i = o / CO_M, j = o % CO_M;
-    if (o < CO_M * CO_M) C.Ac[(size_t)(a * CO_M + i) * C.nc + b * CO_M + j] = acc[m];
+    if (o < CO_M * CO_M) {
+      C.Ac[(size_t)(a * CO_M + i) * C.nc + b * CO_M + j] = acc[m];
+      if (b != a) C.Ac[(size_t)(b * CO_M + j) * C.nc + a * CO_M + i] = acc[m];
+    }
   }
 }
 

@@ -12,6 +12,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <type_traits>
+#include <utility>
+
 #define RPBA_P 9  // padded camera block size (6 + 3 intrinsics)
 
 namespace rpba {
@@ -117,56 +120,49 @@ __device__ __forceinline__ int jacobians(const CamState &c, const ObsEval &e, in
 #pragma unroll
   for (int j = 0; j < RPBA_P; ++j) Bc[0][j] = Bc[1][j] = (T)0;
   const double xyp4 = xy2 * xy2;
-  double ic0[3], ic1[3];
-  int ni = 0;
-  if (addmask & 1) {
-    ic0[ni] = -u * xy2 * c.K00 - v * xy2 * c.K01;
-    ic1[ni] = -v * xy2 * c.K11;
-    ++ni;
-  }
-  if (addmask & 2) {
-    ic0[ni] = -u * xyp4 * c.K00 - v * xyp4 * c.K01;
-    ic1[ni] = -v * xyp4 * c.K11;
-    ++ni;
-  }
-  if (addmask & 4) {
-    ic0[ni] = -e.uu;
-    ic1[ni] = -e.vv;
-    ++ni;
-  }
-  if (role == ROLE_ZERO) {
-    for (int j = 0; j < ni; ++j) {
-      Bc[0][j] = (T)ic0[j];
-      Bc[1][j] = (T)ic1[j];
-    }
-    return ni;
-  }
+  // the intrinsic columns (k2, k4, f) that addmask selects, in that order.
+  // Every array index below is a compile-time constant (a runtime choice is
+  // a select), so the camera, Bc and the columns stay in registers.
+  const bool hk2 = (addmask & 1) != 0, hk4 = (addmask & 2) != 0, hf = (addmask & 4) != 0;
+  const int ni = (int)hk2 + (int)hk4 + (int)hf;
+  const double a0 = -u * xy2 * c.K00 - v * xy2 * c.K01, a1 = -v * xy2 * c.K11;
+  const double b0 = -u * xyp4 * c.K00 - v * xyp4 * c.K01, b1 = -v * xyp4 * c.K11;
+  const double f0 = -e.uu, f1 = -e.vv;
+  const double ic0[3] = {hk2 ? a0 : (hk4 ? b0 : f0), (hk2 && hk4) ? b0 : f0, f0};
+  const double ic1[3] = {hk2 ? a1 : (hk4 ? b1 : f1), (hk2 && hk4) ? b1 : f1, f1};
+  auto put_intrinsics = [&](auto first) {
+    constexpr int n0 = decltype(first)::value;
+#pragma unroll
+    for (int t = 0; t < 3; ++t)
+      if (t < ni) {
+        Bc[0][n0 + t] = (T)ic0[t];
+        Bc[1][n0 + t] = (T)ic1[t];
+      }
+    return n0 + ni;
+  };
+  if (role == ROLE_ZERO) return put_intrinsics(std::integral_constant<int, 0>{});
   const double xs31 = 1. / xs3;
   const double xs32 = xs31 * xs31;
   calib(x2 * x1 * xs32, 1. + x2 * x2 * xs32, Bc[0][0], Bc[1][0]);
   calib(-1. - x1 * x1 * xs32, -x2 * x1 * xs32, Bc[0][1], Bc[1][1]);
   calib(x2 * xs31, -x1 * xs31, Bc[0][2], Bc[1][2]);
-  int n = 3;
   if (role == ROLE_NORM) {
+#pragma unroll
     for (int j = 0; j < 2; ++j) {
-      const int s = esvm[j];
-      calib(-c.R[s] * xs3 + c.R[6 + s] * x1, -c.R[3 + s] * xs3 + c.R[6 + s] * x2, Bc[0][n],
-            Bc[1][n]);
-      ++n;
+      const int s = esvm[j];  // a column of R: 0, 1 or 2
+      const double r0 = s == 0 ? c.R[0] : (s == 1 ? c.R[1] : c.R[2]);
+      const double r3 = s == 0 ? c.R[3] : (s == 1 ? c.R[4] : c.R[5]);
+      const double r6 = s == 0 ? c.R[6] : (s == 1 ? c.R[7] : c.R[8]);
+      calib(-r0 * xs3 + r6 * x1, -r3 * xs3 + r6 * x2, Bc[0][3 + j], Bc[1][3 + j]);
     }
-  } else {
-    for (int j = 0; j < 3; ++j) {
-      Bc[0][n] = Bp[0][j];
-      Bc[1][n] = Bp[1][j];
-      ++n;
-    }
+    return put_intrinsics(std::integral_constant<int, 5>{});
   }
-  for (int j = 0; j < ni; ++j) {
-    Bc[0][n] = (T)ic0[j];
-    Bc[1][n] = (T)ic1[j];
-    ++n;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    Bc[0][3 + j] = Bp[0][j];
+    Bc[1][3 + j] = Bp[1][j];
   }
-  return n;
+  return put_intrinsics(std::integral_constant<int, 6>{});
 }
 
 // 3x3 inverse by cofactors; m, out row major.
@@ -288,6 +284,96 @@ __device__ __forceinline__ void lu_inverse9(int n, const double *A, double *Ai) 
     for (int i = 0; i < n; ++i) Ai[i * 9 + col] = y[i];
   }
   for (int i = n; i < 9; ++i) Ai[i * 9 + i] = 1.;
+}
+
+// lu_inverse9 by one warp: the same operations in the same order (the
+// compiler may contract them into FMAs differently, so the last bits can
+// differ), with row r of the factor in lane r's registers (r < 9) and
+// column col of the inverse solved by lane col.  `row` holds row `lane` of
+// the input (lanes < 9; anything in the other lanes); every lane of the warp
+// calls it; lanes < n write their column of the inverse to Ai (Ai may be the
+// input's storage: nothing is read from memory).
+// Step k of lu_inverse9_warp's factorisation (k a compile-time constant, so
+// that the rows stay in registers).
+template <int k>
+__device__ __forceinline__ void lu9_warp_step(int n, double (&row)[9], int &perm, int lane) {
+  constexpr unsigned FULL = 0xffffffffu;
+  if (k >= n) return;
+  // pivot: the first row p >= k of the largest |LU[p][k]| (a strictly
+  // larger value replaces, as the serial scan does)
+  double best = __shfl_sync(FULL, fabs(row[k]), k);
+  int p = k;
+#pragma unroll
+  for (int r = k + 1; r < 9; ++r) {
+    const double v = __shfl_sync(FULL, fabs(row[k]), r);
+    if (r < n && v > best) {
+      best = v;
+      p = r;
+    }
+  }
+  if (p != k) {
+    const int src = lane == k ? p : (lane == p ? k : lane);
+#pragma unroll
+    for (int c = 0; c < 9; ++c) row[c] = __shfl_sync(FULL, row[c], src);
+    perm = __shfl_sync(FULL, perm, src);
+  }
+  const double piv = __shfl_sync(FULL, row[k], k);
+  const bool below = lane > k && lane < n;
+  const double l = below ? row[k] / piv : 0.;
+  if (below) row[k] = l;
+#pragma unroll
+  for (int c = k + 1; c < 9; ++c) {
+    const double pk = __shfl_sync(FULL, row[c], k);
+    if (below && c < n) row[c] -= l * pk;
+  }
+}
+
+template <int... K>
+__device__ __forceinline__ void lu9_warp_factor(int n, double (&row)[9], int &perm, int lane,
+                                                std::integer_sequence<int, K...>) {
+  (lu9_warp_step<K>(n, row, perm, lane), ...);
+}
+
+// lu_inverse9 by one warp: the same operations in the same order (the
+// compiler may contract them into FMAs differently, so the last bits can
+// differ), with row r of the factor in lane r's registers (r < 9) and
+// column col of the inverse solved by lane col.  `row` holds row `lane` of
+// the input (lanes < 9; anything in the other lanes); every lane of the warp
+// calls it; lanes < 9 write their column of the inverse to Ai (Ai may be the
+// input's storage: nothing is read from memory).
+__device__ __forceinline__ void lu_inverse9_warp(int n, double (&row)[9], double *Ai, int lane) {
+  constexpr unsigned FULL = 0xffffffffu;
+  int perm = lane;
+  lu9_warp_factor(n, row, perm, lane, std::make_integer_sequence<int, 9>{});
+  // column `lane` of the inverse: forward then back substitution
+  double y[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    y[i] = 0.;
+    if (i < n) {
+      double s = __shfl_sync(FULL, perm, i) == lane ? 1. : 0.;
+#pragma unroll
+      for (int j = 0; j < i; ++j) s -= __shfl_sync(FULL, row[j], i) * y[j];
+      y[i] = s;
+    }
+  }
+#pragma unroll
+  for (int i = 8; i >= 0; --i) {
+    if (i < n) {
+      double s = y[i];
+#pragma unroll
+      for (int j = i + 1; j < 9; ++j) {
+        const double u = __shfl_sync(FULL, row[j], i);
+        if (j < n) s -= u * y[j];
+      }
+      y[i] = s / __shfl_sync(FULL, row[i], i);
+    }
+  }
+  __syncwarp();
+  if (lane < 9) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) Ai[i * 9 + lane] = (lane < n && i < n) ? y[i] : (i == lane && i >= n ? 1. : 0.);
+  }
 }
 
 }  // namespace rpba

@@ -272,11 +272,15 @@ void learned_adam(float *W, float *m, float *v, const float *grad, float lr, int
 struct PcgWork {
   double *r, *d, *q, *h, *x, *xbest, *Cinv, *partials, *part;
   // FP32 form: d^k in FP32 ([nimg * 12]), and the SpMV's row sums of the
-  // diagonal blocks, of the rows' first runs, and of the warp runs that
-  // start inside a row ([nimg * 9], [nimg * 9], [warps * 9])
+  // diagonal blocks, of the rows' first runs, and of the chunk runs that
+  // start inside a row ([nimg * 9], [nimg * 9], [groups * 9]); per chunk its
+  // share of d^T A d ([groups]); the chunk counter
   float *d32;
-  double *pdiag, *prow, *pw;
+  double *pdiag, *prow, *pw, *pdqc;
+  unsigned *ctr;  // [2] next phase-1 chunk, next phase-2 row
+  double *rowc;   // [nimg * 12] with the coarse space: per row P_k^T r and its share of |dr|^2
   double *drs;  // [nimg * 9] 1 / sqrt of the camera blocks' diagonal entries (learned features)
+  float *feat;  // [nimg * 20] the learned preconditioner's features per camera row
   unsigned *bar;
   int *iters;
 };

@@ -322,21 +322,26 @@ __global__ void k_point32(DevLSA L, double multfact1) {
     V[5] += G[0][2] * Bp[0][2] + G[1][2] * Bp[1][2];
 #pragma unroll
     for (int a = 0; a < 3; ++a) g[a] += G[0][a] * e.d1 + G[1][a] * e.d2;
-    float *r = L.rec32 + (size_t)o * REC;
+    // the record's floats 0..25 in 16-byte stores: Bc, then Jp until the
+    // factor is known (replaced by H below), then W d
     const bool cam_active = k >= L.begini;
+    float v[28];
 #pragma unroll
     for (int j = 0; j < RPBA_P; ++j) {
-      r[j] = cam_active ? Bc[0][j] : 0.f;
-      r[9 + j] = cam_active ? Bc[1][j] : 0.f;
+      v[j] = cam_active ? Bc[0][j] : 0.f;
+      v[9 + j] = cam_active ? Bc[1][j] : 0.f;
     }
-    // Jp until the factor is known; replaced by H below
 #pragma unroll
     for (int j = 0; j < 3; ++j) {
-      r[18 + j] = Bp[0][j];
-      r[21 + j] = Bp[1][j];
+      v[18 + j] = Bp[0][j];
+      v[21 + j] = Bp[1][j];
     }
-    r[24] = (float)(e.d1 * W0 + e.d2 * W2);
-    r[25] = (float)(e.d1 * W2 + e.d2 * W1);
+    v[24] = (float)(e.d1 * W0 + e.d2 * W2);
+    v[25] = (float)(e.d1 * W2 + e.d2 * W1);
+    float4 *r4 = (float4 *)(L.rec32 + (size_t)o * REC);
+#pragma unroll
+    for (int j = 0; j < 6; ++j) r4[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+    *(float2 *)(r4 + 6) = make_float2(v[24], v[25]);
   }
 #pragma unroll
   for (int j = 0; j < 6; ++j) V[j] = grp_sum(V[j]);
@@ -382,9 +387,11 @@ __global__ void k_point32(DevLSA L, double multfact1) {
     float *r = L.rec32 + (size_t)o * REC;
     const float4 w = L.o_w[o];
     const double W0 = w.x, W1 = w.y, W2 = w.z;
+    // floats 16..27 of the record (Jp at 18..23, W d at 24, 25)
+    const float4 ra = *(const float4 *)(r + 16), rb = *(const float4 *)(r + 20), rcv = *(const float4 *)(r + 24);
     double H[2][3];
     {
-      const double p00 = r[18], p01 = r[19], p02 = r[20], p10 = r[21], p11 = r[22], p12 = r[23];
+      const double p00 = ra.z, p01 = ra.w, p02 = rb.x, p10 = rb.y, p11 = rb.z, p12 = rb.w;
       const double G0[3] = {p00 * W0 + p10 * W2, p01 * W0 + p11 * W2, p02 * W0 + p12 * W2};
       const double G1[3] = {p00 * W2 + p10 * W1, p01 * W2 + p11 * W1, p02 * W2 + p12 * W1};
       H[0][0] = m[0] * G0[0];
@@ -394,19 +401,17 @@ __global__ void k_point32(DevLSA L, double multfact1) {
       H[1][1] = m[1] * G1[0] + m[2] * G1[1];
       H[1][2] = m[3] * G1[0] + m[4] * G1[1] + m[5] * G1[2];
     }
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      r[18 + j] = (float)H[0][j];
-      r[21 + j] = (float)H[1][j];
-    }
     const double h00 = H[0][0] * H[0][0] + H[0][1] * H[0][1] + H[0][2] * H[0][2];
     const double h01 = H[0][0] * H[1][0] + H[0][1] * H[1][1] + H[0][2] * H[1][2];
     const double h11 = H[1][0] * H[1][0] + H[1][1] * H[1][1] + H[1][2] * H[1][2];
-    r[26] = (float)(W0 - h00);
-    r[27] = (float)(W2 - h01);
-    r[28] = (float)(W1 - h11);
-    r[29] = (float)((double)r[24] - (H[0][0] * q0 + H[0][1] * q1 + H[0][2] * q2));
-    r[30] = (float)((double)r[25] - (H[1][0] * q0 + H[1][1] * q1 + H[1][2] * q2));
+    // floats 16..31 in 16-byte stores: H at 18..23, W - H H^T at 26..28,
+    // W d - H q at 29, 30 (16, 17, 24, 25 rewritten unchanged, 31 zero)
+    float4 *r4 = (float4 *)(r + 16);
+    r4[0] = make_float4(ra.x, ra.y, (float)H[0][0], (float)H[0][1]);
+    r4[1] = make_float4((float)H[0][2], (float)H[1][0], (float)H[1][1], (float)H[1][2]);
+    r4[2] = make_float4(rcv.x, rcv.y, (float)(W0 - h00), (float)(W2 - h01));
+    r4[3] = make_float4((float)(W1 - h11), (float)((double)rcv.x - (H[0][0] * q0 + H[0][1] * q1 + H[0][2] * q2)),
+                        (float)((double)rcv.y - (H[1][0] * q0 + H[1][1] * q1 + H[1][2] * q2)), 0.f);
   }
 }
 
@@ -556,23 +561,49 @@ __global__ void k_pair(DevLSA L) {
 }
 
 // FP32 form of the pair pass (whitened records): S_kl -= sum Bc_k^T (H_k
-// H_l^T) Bc_l over the block's contributions.  One warp per block: four
-// lanes form N = H_k H_l^T (2 x 2) and broadcast it; lanes 0..26 own the
-// three entries (i, 3 (lane % 3) .. + 2) of block row i = lane / 3.  Each
-// lane sums a chunk of up to 32 contributions in FP32, in order, and adds the
-// chunk into a compensated (Kahan) sum, so the entry is deterministic.
+// H_l^T) Bc_l over the block's contributions.  One warp per block; per
+// contribution the warp stages the row camera's and the column camera's
+// record (Bc 18 and H 6 floats each, coalesced 4-byte loads, the next
+// contribution's loads in flight) in shared memory in the order the lanes
+// read them: lanes 0..26 own the three entries (i, 3 (lane % 3) .. + 2) of
+// block row i = lane / 3, and each forms N = H_k H_l^T itself (two 16-byte
+// and two 8-byte broadcast loads, 12 FMAs), U_i = (Bc_k[0][i], Bc_k[1][i]) N
+// (one 8-byte load) and its three entries from the three (Bc_l[0][j],
+// Bc_l[1][j]) pairs (one 16-byte and one 8-byte load): twelve shared-memory
+// or global instructions per contribution.  Each lane sums a chunk of up to
+// 32 contributions in FP32, in order, and adds the chunk into a compensated
+// (Kahan) sum, so the entry is deterministic.
+// Staging layout (floats): row record: pairs (Bc[0][j], Bc[1][j]) at 2 j,
+// H at 20..25; column record: the pairs of j = 3 g .. 3 g + 2 at 28 + 8 g
+// (16-byte aligned groups), H at 52..57.
+constexpr int PS = 60;  // floats per warp
+__device__ __forceinline__ int pair_slot_x(int e) {
+  return e < 9 ? 2 * e : (e < 18 ? 2 * (e - 9) + 1 : e + 2);
+}
+__device__ __forceinline__ int pair_slot_y(int e) {
+  if (e < 18) {
+    const int r = e < 9 ? 0 : 1, j = e - 9 * r;
+    return 28 + 8 * (j / 3) + 2 * (j % 3) + r;
+  }
+  return 52 + (e - 18);
+}
 __global__ void __launch_bounds__(256) k_pair32(DevLSA L) {
   const int wid = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int wl = threadIdx.x >> 5;
-  __shared__ float sm[8][48];
+  __shared__ __align__(16) float sm[8][PS];
+  __shared__ int2 spr[8][32];
   if (wid >= L.nboff) return;
   float *s = sm[wl];
+  int2 *sp = spr[wl];
   const float *rec = L.rec32;
-  const int i = lane < 27 ? lane / 3 : 0, j0 = lane < 27 ? 3 * (lane - 3 * (lane / 3)) : 0;
+  const int i = lane < 27 ? lane / 3 : 0, g = lane < 27 ? lane - 3 * (lane / 3) : 0;
+  // destinations of this lane's two record values: v0 = float `lane` of the
+  // row record (lane < 24) or float lane - 24 of the column record; v1 =
+  // float lane + 8 of the column record (lane < 16)
+  const int d0 = lane < 24 ? pair_slot_x(lane) : pair_slot_y(lane - 24);
+  const int d1 = pair_slot_y(lane < 16 ? lane + 8 : 8);
   float ks[3] = {0.f, 0.f, 0.f}, kc[3] = {0.f, 0.f, 0.f};
-  // record values of one contribution: Bc (18) and H (6) of the row
-  // camera's observation (s[0..23]), then of the column camera's (s[24..47])
   auto fetch = [&](int ox, int oy, float &v0, float &v1) {
     v0 = lane < 24 ? rec[(size_t)ox * REC + lane] : rec[(size_t)oy * REC + lane - 24];
     v1 = lane < 16 ? rec[(size_t)oy * REC + lane + 8] : 0.f;
@@ -580,30 +611,35 @@ __global__ void __launch_bounds__(256) k_pair32(DevLSA L) {
   const int cb = L.boff[wid], ce = L.boff[wid + 1];
   for (int c0 = cb; c0 < ce; c0 += 32) {
     const int n = min(32, ce - c0);
-    int2 pr = make_int2(0, 0);
-    if (lane < n) pr = L.contrib[c0 + lane];
+    if (lane < n) sp[lane] = L.contrib[c0 + lane];
+    __syncwarp();
     float v0, v1;
-    fetch(__shfl_sync(0xffffffffu, pr.x, 0), __shfl_sync(0xffffffffu, pr.y, 0), v0, v1);
+    {
+      const int2 q = sp[0];
+      fetch(q.x, q.y, v0, v1);
+    }
     float part[3] = {0.f, 0.f, 0.f};
     for (int j = 0; j < n; ++j) {
-      s[lane] = v0;
-      if (lane < 16) s[32 + lane] = v1;
-      if (j + 1 < n)
-        fetch(__shfl_sync(0xffffffffu, pr.x, j + 1), __shfl_sync(0xffffffffu, pr.y, j + 1), v0, v1);
+      s[d0] = v0;
+      if (lane < 16) s[d1] = v1;
+      if (j + 1 < n) {
+        const int2 q = sp[j + 1];
+        fetch(q.x, q.y, v0, v1);
+      }
       __syncwarp();
-      float nab = 0.f;
-      if (lane < 4) {
-        const float *hx = s + 18 + 3 * (lane >> 1), *hy = s + 42 + 3 * (lane & 1);
-        nab = hx[0] * hy[0] + hx[1] * hy[1] + hx[2] * hy[2];
-      }
-      const float n00 = __shfl_sync(0xffffffffu, nab, 0), n01 = __shfl_sync(0xffffffffu, nab, 1);
-      const float n10 = __shfl_sync(0xffffffffu, nab, 2), n11 = __shfl_sync(0xffffffffu, nab, 3);
-      if (lane < 27) {
-        const float bx0 = s[i], bx1 = s[9 + i];
-        const float u0 = bx0 * n00 + bx1 * n10, u1 = bx0 * n01 + bx1 * n11;
-#pragma unroll
-        for (int q = 0; q < 3; ++q) part[q] -= u0 * s[24 + j0 + q] + u1 * s[33 + j0 + q];
-      }
+      const float4 hx = *(const float4 *)(s + 20), hy = *(const float4 *)(s + 52);
+      const float2 hx2 = *(const float2 *)(s + 24), hy2 = *(const float2 *)(s + 56);
+      const float n00 = hx.x * hy.x + hx.y * hy.y + hx.z * hy.z;
+      const float n01 = hx.x * hy.w + hx.y * hy2.x + hx.z * hy2.y;
+      const float n10 = hx.w * hy.x + hx2.x * hy.y + hx2.y * hy.z;
+      const float n11 = hx.w * hy.w + hx2.x * hy2.x + hx2.y * hy2.y;
+      const float2 bx = *(const float2 *)(s + 2 * i);
+      const float4 ya = *(const float4 *)(s + 28 + 8 * g);
+      const float2 yb = *(const float2 *)(s + 32 + 8 * g);
+      const float u0 = bx.x * n00 + bx.y * n10, u1 = bx.x * n01 + bx.y * n11;
+      part[0] -= u0 * ya.x + u1 * ya.y;
+      part[1] -= u0 * ya.z + u1 * ya.w;
+      part[2] -= u0 * yb.x + u1 * yb.y;
       __syncwarp();
     }
 #pragma unroll
@@ -613,9 +649,10 @@ __global__ void __launch_bounds__(256) k_pair32(DevLSA L) {
       kc[q] = (t - ks[q]) - y;
       ks[q] = t;
     }
+    __syncwarp();  // sp is rewritten by the next chunk
   }
   if (lane < 27) {
-    float *B = L.blocks32 + (size_t)(L.nimg + wid) * BS32 + i * 9 + j0;
+    float *B = L.blocks32 + (size_t)(L.nimg + wid) * BS32 + i * 9 + 3 * g;
 #pragma unroll
     for (int q = 0; q < 3; ++q) __stcs(B + q, (float)((double)ks[q] - (double)kc[q]));  // keep L2 for the records
   }

@@ -173,18 +173,40 @@ __device__ __forceinline__ void mlp_forward_warp(const float *W, const float f[N
     h2[u] = tanhf(a);
   }
   float o[NN_O];
-  for (int i = 0; i < NN_O; ++i) o[i] = b2[i];
-  for (int j = 0; j < NN_H; ++j) {
-    const float hj = __shfl_sync(0xffffffffu, h2[j >> 5], j & 31);
 #pragma unroll
-    for (int i = 0; i < NN_O; ++i) o[i] += W2[i * NN_H + j] * hj;
-  }
+  for (int i = 0; i < NN_O; ++i) o[i] = b2[i];
+#pragma unroll
+  for (int u = 0; u < 2; ++u)
+    for (int jj = 0; jj < 32; ++jj) {
+      const int j = 32 * u + jj;
+      const float hj = __shfl_sync(0xffffffffu, h2[u], jj);
+#pragma unroll
+      for (int i = 0; i < NN_O; ++i) o[i] += W2[i * NN_H + j] * hj;
+    }
+#pragma unroll
   for (int i = 0; i < NN_O; ++i) s[i] = expf(ALPHA * tanhf(o[i]));
 }
 
+// Features of every camera row >= begini, one warp per row (block_features),
+// to feat[k * NN_FS ..]: a kernel of its own, so that its loads run at the
+// occupancy of a small register count.
+constexpr int NN_FS = 20;  // floats per row of feat
+__global__ void __launch_bounds__(128) k_learned_features(DevLSA L, const double *drs, float *feat) {
+  const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+  if (k >= L.nimg || k < L.begini) return;
+  float f[NN_F];
+  block_features(L, drs, k, lane, f);
+  float v = 0.f;
+#pragma unroll
+  for (int j = 0; j < NN_F; ++j)
+    if (lane == j) v = f[j];
+  if (lane < NN_F) feat[(size_t)k * NN_FS + lane] = v;
+}
+
 // PCG start with the learned preconditioner (replaces k_pcg_setup), one
-// warp per camera row: C_k = diag(s) S_kk^-1 diag(s); W == nullptr gives
-// plain block-Jacobi.
+// warp per camera row: C_k = diag(s) S_kk^-1 diag(s) with S_kk^-1 from
+// lu_inverse9_warp and s from the network on the row's features
+// (k_learned_features); W == nullptr gives plain block-Jacobi.
 __global__ void k_learned_setup(DevLSA L, PcgWork Wk, const float *weights) {
   __shared__ float Ws[NN_WEIGHTS];
   for (int i = threadIdx.x; i < NN_WEIGHTS; i += blockDim.x) Ws[i] = weights ? bf16r(weights[i]) : 0.f;
@@ -199,27 +221,35 @@ __global__ void k_learned_setup(DevLSA L, PcgWork Wk, const float *weights) {
     return;
   }
   const int np = L.camparv[k + 1] - L.camparv[k];
-  if (lane == 0) {
-    // the block goes to C first, then is inverted in place (lu_inverse9
-    // copies its input before writing the inverse)
-    load_block(L, (size_t)k, C);
-    lu_inverse9(np, C, C);
+  {
+    double row[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) row[c] = lane < 9 ? blk_at(L, (size_t)k, lane * 9 + c) : 0.;
+    lu_inverse9_warp(np, row, C, lane);
   }
   float sc[NN_O];
+#pragma unroll
   for (int a = 0; a < NN_O; ++a) sc[a] = 1.f;
   if (weights) {
+    const float fl = lane < NN_F ? Wk.feat[(size_t)k * NN_FS + lane] : 0.f;
     float f[NN_F];
-    block_features(L, Wk.drs, k, lane, f);
+#pragma unroll
+    for (int j = 0; j < NN_F; ++j) f[j] = __shfl_sync(0xffffffffu, fl, j);
     mlp_forward_warp(Ws, f, lane, sc);
   }
   __syncwarp();
   if (lane < 9) {
     const int a = lane;
+    float sa = 1.f;
+#pragma unroll
+    for (int j = 0; j < NN_O; ++j)
+      if (j == a) sa = sc[j];
     double sum = 0.;
+#pragma unroll
     for (int c = 0; c < 9; ++c) {
       double cv = C[a * 9 + c];
       if (weights && a < np && c < np) {
-        cv *= (double)sc[a] * (double)sc[c];
+        cv *= (double)sa * (double)sc[c];
         C[a * 9 + c] = cv;
       }
       sum += cv * L.rhs[o + c];
@@ -510,7 +540,10 @@ __global__ void k_rec_uc(DevLSA L, TrainSet T, int row0, int pr, const double *v
 }  // namespace
 
 void learned_pcg_setup(const DevLSA &L, const PcgWork &W, const float *weights, cudaStream_t s) {
-  if (weights) k_diag_rsqrt<<<(L.nimg * 9 + 255) / 256, 256, 0, s>>>(L, W.drs);
+  if (weights) {
+    k_diag_rsqrt<<<(L.nimg * 9 + 255) / 256, 256, 0, s>>>(L, W.drs);
+    k_learned_features<<<(L.nimg + 3) / 4, 128, 0, s>>>(L, W.drs, W.feat);
+  }
   k_learned_setup<<<(L.nimg + 7) / 8, 256, 0, s>>>(L, W, weights);
 }
 

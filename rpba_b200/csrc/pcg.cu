@@ -12,6 +12,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstdlib>
 
 #include "gridsync.cuh"
 #include "internal.h"
@@ -47,7 +48,10 @@ struct PcgArgs {
   const int *firstN, *firstT;
   int nboff;
   float *d32;
-  double *pdiag, *prow, *pw;
+  double *pdiag, *prow, *pw;  // pw: per chunk
+  double *pdqc;               // per chunk: its share of d^T A d
+  unsigned *ctr;              // next chunk of phase 1
+  int chunk;                  // groups per phase-1 chunk
   const double *Cinv;
   double *r, *h, *x, *xbest, *D0, *D1;
   double *part;        // [nitems * 9] SpMV partial rows
@@ -69,6 +73,7 @@ struct PcgArgs {
   const int *agg_off, *agg_rows;
   const double *P, *Ainv;
   double *rc, *hj;
+  double *rowc;  // FP32 form: per row its restriction P_k^T r1 (CO_M) and its share of dr^2, stride RC_S
 };
 
 // Deterministic CTA sum of up to three values; valid in every thread.
@@ -562,14 +567,17 @@ __device__ __forceinline__ Grp32 group_of(long long g, int gd, int row0, int row
   }
   return q;
 }
-// first group of warp w's run (NG groups over NW warps)
-__device__ __forceinline__ long long run_start(long long w, long long ng, long long nw) { return w * ng / nw; }
+// Phase 1 is cut into chunks of A.chunk groups (fixed boundaries); the warps take
+// chunks from a counter, so a fast warp takes more of them, and everything a
+// chunk writes (its row sums, its share of d^T A d) depends only on the
+// chunk: the result does not depend on which warp took it.
 
 // Byte offsets of a group's data inside its 16-byte aligned copies.
 __device__ __forceinline__ unsigned blk_misalign(const float *blocks, long long start) {
   return (unsigned)(((unsigned long long)(blocks + start * 81)) & 15ull);
 }
 constexpr int TP_STRIDE = 16;  // floats per transposed-product slot (64 B)
+constexpr int RC_S = 12;       // doubles per row of rowc
 
 // Issue the copies of group q into the warp's stage (one lane).
 __device__ __forceinline__ void group_issue(const PcgArgs &A, const Grp32 &q, unsigned char *stg,
@@ -607,15 +615,16 @@ __device__ __forceinline__ void load_d32(const float *d32, int c, float (&v)[9])
 }
 
 // q of one row in lanes < 9 (FP32 form).
-__device__ __forceinline__ double row_q32(const PcgArgs &A, int row, long long ng, long long nw, long long gd,
-                                          int lane) {
+__device__ __forceinline__ double row_q32(const PcgArgs &A, int row, long long gd, int lane) {
   // the row's run of transposed products (slots firstT[row] ..
-  // firstT[row + 1]): one slot per lane (three 16-byte loads), nine FP64
-  // partial sums, then a fixed butterfly
+  // firstT[row + 1]): one slot per lane (three 16-byte loads), and the sums
+  // of the phase-1 chunks that start strictly inside the row's off-diagonal
+  // blocks, one chunk per lane; nine FP64 partial sums, then a fixed butterfly
   double acc[9];
 #pragma unroll
   for (int j = 0; j < 9; ++j) acc[j] = 0.;
   const int e0 = __ldg(A.firstT + row), e1 = __ldg(A.firstT + row + 1);
+  const int f0 = __ldg(A.firstN + row), f1 = __ldg(A.firstN + row + 1);
 #pragma unroll 4
   for (int e = e0 + lane; e < e1; e += 32) {
     const float4 *t = (const float4 *)(A.tpart + (size_t)e * TP_STRIDE);
@@ -630,6 +639,14 @@ __device__ __forceinline__ double row_q32(const PcgArgs &A, int row, long long n
     acc[7] += (double)b.w;
     acc[8] += (double)c.x;
   }
+  if (f1 > f0) {
+    const long long ch = A.chunk, glo = gd + f0 / GB + 1, ghi = gd + (f1 - 1) / GB;
+    for (long long c = (glo + ch - 1) / ch + lane; c * ch <= ghi; c += 32) {
+      const double *w = A.pw + (size_t)c * 9;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) acc[j] += __ldcg(w + j);
+    }
+  }
 #pragma unroll
   for (int j = 0; j < 9; ++j)
 #pragma unroll
@@ -641,19 +658,7 @@ __device__ __forceinline__ double row_q32(const PcgArgs &A, int row, long long n
   if (lane < 9) {
     const size_t i = (size_t)row * 9 + lane;
     q += __ldcg(A.pdiag + i);
-    const int f0 = __ldg(A.firstN + row), f1 = __ldg(A.firstN + row + 1);
-    if (f1 > f0) {
-      q += __ldcg(A.prow + i);
-      // runs that start strictly inside the row's off-diagonal blocks
-      const long long glo = gd + f0 / GB + 1, ghi = gd + (f1 - 1) / GB;
-      if (glo <= ghi) {
-        for (long long w = (glo * nw + ng - 1) / ng; w < nw; ++w) {
-          const long long g = run_start(w, ng, nw);
-          if (g > ghi) break;
-          if (g >= glo && run_start(w + 1, ng, nw) > g) q += __ldcg(A.pw + (size_t)w * 9 + lane);
-        }
-      }
-    }
+    if (f1 > f0) q += __ldcg(A.prow + i);
   }
   return q;
 }
@@ -673,7 +678,7 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
   __syncwarp();
   const float *blocks = (const float *)A.blocks;
   const long long gd = (A.row1 - A.row0 + GB - 1) / GB, go = ((long long)A.nboff + GB - 1) / GB;
-  const long long ng = gd + go, nw = nwarps;
+  const long long ng = gd + go, ch = A.chunk, nch = (ng + ch - 1) / ch;
   // r^T h of the start vectors
   {
     double v[1] = {0.};
@@ -707,17 +712,24 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
         dcur[i] = dk;
         A.d32[(size_t)row * 12 + lane] = (float)dk;
       }
+    if (blockIdx.x == 0 && threadIdx.x < 2) A.ctr[threadIdx.x] = 0u;
     if (!grid_barrier(A.bar, G + A.bar_extra, A.err, A.bar_ns)) return;
     // ---- phase 1
-    double pdq = 0.;
     {
-      const long long g0 = run_start(gwarp, ng, nw), g1 = run_start(gwarp + 1, ng, nw);
-      int cur_row = -1;   // row of the running sum (-1: none yet in this run)
+      auto grab = [&]() -> long long {
+        unsigned c = 0;
+        if (lane == 0) c = atomicAdd(A.ctr, 1u);
+        return (long long)__shfl_sync(0xffffffffu, c, 0);
+      };
+      long long c = grab();
+      long long cn = c < nch ? grab() : nch;  // the next chunk, taken one ahead
+      int cur_row = -1;   // row of the running sum (-1: none yet in this chunk)
       bool cur_head = false;
       double racc = 0.;   // running sum of cur_row, component `lane` (lanes < 9)
+      double pdq = 0.;    // this chunk's share of d^T A d (per lane)
       auto flush = [&]() {
         if (cur_row >= 0 && lane < 9) {
-          double *dst = cur_head ? A.prow + (size_t)cur_row * 9 : A.pw + (size_t)gwarp * 9;
+          double *dst = cur_head ? A.prow + (size_t)cur_row * 9 : A.pw + (size_t)c * 9;
           dst[lane] = racc;
         }
       };
@@ -738,8 +750,13 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
         }
         racc += v;
       };
-      if (g0 < g1 && lane == 0) group_issue(A, group_of(g0, (int)gd, A.row0, A.row1, A.nboff), stg, mbar);
+      if (c < nch && lane == 0) group_issue(A, group_of(c * ch, (int)gd, A.row0, A.row1, A.nboff), stg, mbar);
       bool ok = true;
+      while (c < nch) {
+      const long long g0 = c * ch, g1 = min(ng, g0 + ch);
+      cur_row = -1;
+      racc = 0.;
+      pdq = 0.;
       for (long long g = g0; g < g1; ++g) {
         const Grp32 q = group_of(g, (int)gd, A.row0, A.row1, A.nboff);
         if (!stage_wait(A, mbar, parity)) {
@@ -781,10 +798,12 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
           pdq += s;
         }
         // the stage's blocks are read: the next group's copies may land
+        // (the next group of this chunk, or the first of the next chunk)
         __syncwarp();
-        if (lane == 0 && g + 1 < g1) {
+        const long long gn = g + 1 < g1 ? g + 1 : (cn < nch ? cn * ch : -1);
+        if (lane == 0 && gn >= 0) {
           fence_proxy_async();
-          group_issue(A, group_of(g + 1, (int)gd, A.row0, A.row1, A.nboff), stg, mbar);
+          group_issue(A, group_of(gn, (int)gd, A.row0, A.row1, A.nboff), stg, mbar);
         }
         if (q.diag) {
           if (act) {
@@ -842,8 +861,8 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
             racc += sv;
           } else {
             flush();
-            // a segment starts the row unless it is the run's first and the
-            // row began before the run
+            // a segment starts the row unless it is the chunk's first and
+            // the row began before the chunk
             cur_head = cur_row >= 0 || seg_first > 0 || q.boff + seg_first == (long long)__ldg(A.firstN + re);
             cur_row = re;
             racc = sv;
@@ -851,9 +870,15 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
           seg_first = e + 1;
         }
       }
-      if (ok) {
-        fold_lanes();
-        flush();
+      if (!ok) break;
+      fold_lanes();
+      flush();
+      // the chunk's share of d^T A d, summed over its lanes in a fixed order
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) pdq += __shfl_xor_sync(0xffffffffu, pdq, o);
+      if (lane == 0) A.pdqc[c] = pdq;
+      c = cn;
+      cn = c < nch ? grab() : nch;
       }
       __syncwarp();
       if (!ok) {
@@ -863,17 +888,27 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
         stage_wait(A, mbar, parity);
       }
     }
-    {
-      double v[1] = {pdq};
-      cta_sum<1, P32_W>(v, sh);
-      if (threadIdx.x == 0) A.red1[4 * blockIdx.x] = v[0];
-    }
+
     if (!grid_barrier(A.bar, G + A.bar_extra, A.err, A.bar_ns)) return;
     double edtAdk;
     {
-      double v[1];
-      grid_sum<1, P32_W>(A.red1, G, v, sh);
-      edtAdk = v[0];
+      // d^T A d: every CTA sums the chunks' shares in the same fixed order
+      // (thread t takes chunks t, t + P32_T, ...; then a butterfly per warp
+      // and the warps in order)
+      double v = 0.;
+      for (long long i = threadIdx.x; i < nch; i += P32_T) v += __ldcg(A.pdqc + i);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) sh[warp][0] = v;
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double t = 0.;
+        for (int w = 0; w < P32_W; ++w) t += sh[w][0];
+        sh[P32_W][0] = t;
+      }
+      __syncthreads();
+      edtAdk = sh[P32_W][0];
+      __syncthreads();
     }
     double alpha;
     if (fabs(erthk) < 1.e-20 || fabs(erthk) > 1.e20)
@@ -886,7 +921,7 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
       for (int row = A.row0 + gwarp; row < A.row1; row += nwarps) {
         const size_t i = (size_t)row * 9 + (lane < 9 ? lane : 0);
         double r1v = 0., hv = 0.;
-        const double q = row_q32(A, row, ng, nw, gd, lane);
+        const double q = row_q32(A, row, gd, lane);
         if (lane < 9) {
           hv = __ldcg(A.h + i);
           const double dk = __ldcg(dcur + i);
@@ -910,43 +945,79 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
         }
       }
     } else {
-      __shared__ double shr[P32_W][CO_M];
+      __shared__ double shr[P32_W][CO_M + 1];
       __shared__ double shz[CO_M];
+      // 2a: rows in any order, taken from a counter (the rows of high index,
+      // with the longest runs of transposed products, first); each row's
+      // results go to its own slots, so nothing depends on which warp took it
+      // Every load of a row that does not depend on q is issued before the
+      // row's walk: lanes 0..8 hold row `lane` of C_k, lanes 16..25 column
+      // `lane - 16` of P_k (9 doubles a lane either way).
+      const int nrows = A.row1 - A.row0;
+      auto grab_row = [&]() -> int {
+        unsigned t = 0;
+        if (lane == 0) t = atomicAdd(A.ctr + 1, 1u);
+        return (int)__shfl_sync(0xffffffffu, t, 0);
+      };
+      const bool cl = lane < 9, pl = lane >= 16 && lane < 16 + CO_M;
+      for (int t = grab_row(); t < nrows;) {
+        const int row = A.row1 - 1 - t;
+        const int tn = grab_row();  // the next row, taken one ahead
+        const size_t i = (size_t)row * 9 + (cl ? lane : 0);
+        double cp[9];
+        {
+          const double *C = A.Cinv + (size_t)row * 81 + (cl ? lane * 9 : 0);
+          const double *Pk = A.P + (size_t)row * (9 * CO_M) + (pl ? lane - 16 : 0);
+#pragma unroll
+          for (int c = 0; c < 9; ++c) cp[c] = cl ? __ldg(C + c) : (pl ? __ldg(Pk + c * CO_M) : 0.);
+        }
+        double dk = 0., xv = 0., rv = 0.;
+        if (cl) {
+          dk = __ldcg(dcur + i);
+          xv = __ldcg(A.x + i);
+          rv = __ldcg(A.r + i);
+        }
+        const double q = row_q32(A, row, gd, lane);
+        double r1v = 0., d2 = 0.;
+        if (cl) {
+          A.x[i] = xv + alpha * dk;
+          const double dr = alpha * q;
+          r1v = rv - dr;
+          d2 = dr * dr;
+        }
+        double acc = 0.;  // lanes 0..8: h_j; lanes 16..25: the restriction
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+          const double rc = __shfl_sync(0xffffffffu, r1v, c);
+          acc += cp[c] * rc;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) d2 += __shfl_xor_sync(0xffffffffu, d2, o);
+        if (cl) {
+          A.r[i] = r1v;
+          A.hj[i] = acc;
+        }
+        if (pl) A.rowc[(size_t)row * RC_S + lane - 16] = acc;
+        if (lane == 31) A.rowc[(size_t)row * RC_S + CO_M] = d2;
+        t = tn;
+      }
+      if (!grid_barrier(A.bar, G + A.bar_extra, A.err, A.bar_ns)) return;
+      // 2a': per aggregate, its rows' restrictions and shares of dr^2 in a
+      // fixed order (warp w: rows w, w + P32_W, ...; then the warps in order)
       for (int a = blockIdx.x; a < A.nagg; a += G) {
         const int t0 = A.agg_off[a], t1 = A.agg_off[a + 1];
-        double rcw = 0.;
-        for (int t = t0 + warp; t < t1; t += P32_W) {
-          const int row = A.agg_rows[t];
-          const size_t i = (size_t)row * 9 + (lane < 9 ? lane : 0);
-          double r1v = 0.;
-          const double q = row_q32(A, row, ng, nw, gd, lane);
-          if (lane < 9) {
-            const double dk = __ldcg(dcur + i);
-            A.x[i] = __ldcg(A.x + i) + alpha * dk;
-            const double dr = alpha * q;
-            r1v = __ldcg(A.r + i) - dr;
-            p2[0] += dr * dr;
-          }
-          const double *C = A.Cinv + (size_t)row * 81;
-          const double *Pk = A.P + (size_t)row * (9 * CO_M);
-          double h1v = 0.;
-#pragma unroll
-          for (int c = 0; c < 9; ++c) {
-            const double rc = __shfl_sync(0xffffffffu, r1v, c);
-            if (lane < 9) h1v += __ldg(C + lane * 9 + c) * rc;
-            if (lane < CO_M) rcw += __ldg(Pk + c * CO_M + lane) * rc;
-          }
-          if (lane < 9) {
-            A.r[i] = r1v;
-            A.hj[i] = h1v;
-          }
-        }
-        if (lane < CO_M) shr[warp][lane] = rcw;
+        double v = 0.;
+        if (lane <= CO_M)
+          for (int t = t0 + warp; t < t1; t += P32_W) v += __ldcg(A.rowc + (size_t)A.agg_rows[t] * RC_S + lane);
+        if (lane <= CO_M) shr[warp][lane] = v;
         __syncthreads();
-        if (threadIdx.x < CO_M) {
+        if (threadIdx.x <= CO_M) {
           double sum = 0.;
           for (int w = 0; w < P32_W; ++w) sum += shr[w][threadIdx.x];
-          A.rc[a * CO_M + threadIdx.x] = sum;
+          if (threadIdx.x < CO_M)
+            A.rc[a * CO_M + threadIdx.x] = sum;
+          else
+            p2[0] += sum;
         }
         __syncthreads();
       }
@@ -1027,7 +1098,8 @@ __global__ void __launch_bounds__(P32_T, 1) k_pcg32(PcgArgs A) {
 }
 
 // Preconditioner C_k = S_kk^-1 (rbacore.cpp:1839-1846) and the start
-// vectors: r = b, h = C r, d^(-1) = 0, x = 0, best = b.
+// vectors: r = b, h = C r, d^(-1) = 0, x = 0, best = b.  One thread per
+// camera with the serial lu_inverse9 (the drop-in form's numerics).
 __global__ void k_pcg_setup(DevLSA L, PcgWork W) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= L.nimg) return;
@@ -1066,6 +1138,19 @@ void pcg_set_smem() {
 }
 
 int pcg_warps32() { return P32_W; }
+
+// Groups of 32 blocks per phase-1 chunk of the FP32 PCG: small enough that
+// the warps finish together, large enough that the chunk's fixed work (its
+// first segmented scan, its sums) stays small.  RPBA_PCG32_CHUNK (1..64)
+// overrides it for tuning.
+static int pcg32_chunk() {
+  static const int c = [] {
+    const char *e = getenv("RPBA_PCG32_CHUNK");
+    const int v = e ? atoi(e) : 4;
+    return v < 1 ? 1 : (v > 64 ? 64 : v);
+  }();
+  return c;
+}
 
 int pcg_max_grid(int device) {
   int nsm = 0, per = 0, per2 = 0;
@@ -1131,6 +1216,10 @@ int pcg_iterate(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStre
   A.pdiag = W.pdiag;
   A.prow = W.prow;
   A.pw = W.pw;
+  A.pdqc = W.pdqc;
+  A.ctr = W.ctr;
+  A.rowc = W.rowc;
+  A.chunk = pcg32_chunk();
   A.Cinv = W.Cinv;
   A.r = W.r;
   A.h = W.h;

@@ -291,7 +291,8 @@ struct rpba_handle {
     if (nb <= blocks_cap && cur) return;
     const int cap = std::max(nb, 1);
     if (cur) {
-      for (void *p : {cur, (void *)S.ent, (void *)S.item_meta, (void *)W.part, (void *)L.tpart, (void *)S.bidx}) {
+      for (void *p : {cur, (void *)S.ent, (void *)S.item_meta, (void *)W.part, (void *)L.tpart, (void *)S.bidx,
+                      (void *)W.pw, (void *)W.pdqc}) {
         if (!p) continue;
         auto it = std::find(owned_async.begin(), owned_async.end(), p);
         if (it != owned_async.end()) {
@@ -309,6 +310,10 @@ struct rpba_handle {
       L.blocks32 = dalloc<float>((size_t)(nimg + cap) * BS32 + 16, owned);
       L.tpart = dalloc<float>((size_t)cap * 16 + 16, owned);
       S.bidx = dalloc<int4>((size_t)nimg + cap + 4, owned);
+      // phase-1 chunks of the FP32 PCG: at most one per group of 32 blocks
+      const size_t groups = ((size_t)nimg + cap) / 32 + 4;
+      W.pw = dalloc<double>(9 * groups, owned);
+      W.pdqc = dalloc<double>(groups, owned);
     } else
       L.blocks = dalloc<double>((size_t)(nimg + cap) * BS64, owned);
     S.ent = dalloc<int2>((size_t)nimg + 2 * (size_t)cap, owned);
@@ -774,6 +779,7 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   W.q = dalloc<double>(nv, own);
   W.h = dalloc<double>(nv, own);
   W.drs = dalloc<double>(nv, own);
+  W.feat = dalloc<float>(20 * (size_t)n, own);
   W.x = dalloc<double>(nv, own);
   W.xbest = dalloc<double>(nv, own);
   W.Cinv = dalloc<double>(81 * (size_t)n, own);
@@ -784,7 +790,8 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
     W.d32 = dalloc<float>(12 * (size_t)n + 4, own);
     W.pdiag = dalloc<double>(nv, own);
     W.prow = dalloc<double>(nv, own);
-    W.pw = dalloc<double>(9 * (size_t)H->pcg_grid * pcg_warps32(), own);
+    W.ctr = dalloc<unsigned>(4, own);
+    W.rowc = dalloc<double>(12 * (size_t)n, own);
   }
   RPBA_CUDA_CHECK(cudaMemsetAsync(W.q, 0, sizeof(double) * nv, H->s));
   RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
