@@ -103,13 +103,17 @@ __device__ __forceinline__ void for_frag(F f) {
 
 // Factor the diagonal tile in place and write L_JJ and L_JJ^-1, with all
 // threads of the CTA: per column the pivot's square root (every thread
-// takes it), the column scaled, then the trailing triangle updated -- two
-// block barriers a column; then the inverse row by row, every entry from
-// four partial sums (thread c + 64 q takes every fourth term of column c).
-// s, si: two shared tiles (ld CT + 1); pp: 4 x CT doubles of shared scratch.
+// takes it), the column scaled, then the trailing triangle updated (warp w
+// rows k + 1 + w, + 8, ...; lane l columns k + 1 + l, + 32, ...) -- two
+// block barriers a column; then the inverse by columns: four lanes of one
+// warp per column c (lane q takes every fourth term mm = c + q, c + q + 4,
+// ... of entry (i, c), the four partial sums added as (p0 + p1) + (p2 + p3)),
+// rows i in order with warp barriers only.
+// s, si: two shared tiles (ld CT + 1); pp: unused scratch.
 __device__ void potrf_tile(double *gtile, double *ginv, int *err, double *s, double *si, double *pp) {
+  (void)pp;
   constexpr int LD = CT + 1;
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   __syncthreads();
   for (int idx = t; idx < TS; idx += CTH) s[(idx >> 6) * LD + (idx & 63)] = __ldcg(gtile + idx);
   __syncthreads();
@@ -120,27 +124,30 @@ __device__ void potrf_tile(double *gtile, double *ginv, int *err, double *s, dou
     if (t < CT - 1 - k) s[(k + 1 + t) * LD + k] /= dk;
     __syncthreads();
     if (t == 0) s[k * LD + k] = dk;
-    const int m = CT - 1 - k;
-    for (int idx = t; idx < m * m; idx += CTH) {
-      const int i = k + 1 + idx / m, j = k + 1 + idx % m;
-      if (j <= i) s[i * LD + j] -= s[i * LD + k] * s[j * LD + k];
+    for (int i = k + 1 + w; i < CT; i += CTH / 32) {
+      const double lik = s[i * LD + k];
+      for (int j = k + 1 + lane; j <= i; j += 32) s[i * LD + j] -= lik * s[j * LD + k];
     }
     __syncthreads();
   }
-  const int c = t & 63, q = t >> 6;
-  for (int i = 0; i < CT; ++i) {
-    double acc = 0.;
-    if (c < i)
-      for (int mm = c + q; mm < i; mm += 4) acc += s[i * LD + mm] * si[mm * LD + c];
-    pp[q * CT + c] = acc;
-    __syncthreads();
-    if (t < CT) {
-      const double sum = (pp[t] + pp[CT + t]) + (pp[2 * CT + t] + pp[3 * CT + t]);
-      const double dii = s[i * LD + i];
-      si[i * LD + t] = t < i ? -sum / dii : (t == i ? 1. / dii : 0.);
+  {
+    const int c = t >> 2, q = t & 3;  // column c (0..63), partial q
+    for (int i = 0; i < CT; ++i) {
+      double acc = 0.;
+      if (c < i)
+        for (int mm = c + q; mm < i; mm += 4) acc += s[i * LD + mm] * si[mm * LD + c];
+      const double a1 = __shfl_down_sync(0xffffffffu, acc, 1);
+      const double p01 = acc + a1;  // lanes q = 0 and 2: (p0 + p1), (p2 + p3)
+      const double p23 = __shfl_down_sync(0xffffffffu, p01, 2);
+      if (q == 0) {
+        const double sum = p01 + p23;
+        const double dii = s[i * LD + i];
+        si[i * LD + c] = c < i ? -sum / dii : (c == i ? 1. / dii : 0.);
+      }
+      __syncwarp();
     }
-    __syncthreads();
   }
+  __syncthreads();
   for (int idx = t; idx < TS; idx += CTH) {
     const int i = idx >> 6, j = idx & 63;
     gtile[idx] = j <= i ? s[i * LD + j] : 0.;
@@ -166,87 +173,75 @@ __global__ void __launch_bounds__(CTH, 1) k_chol_tiles(Tiles T) {
   // tile 0's diagonal block
   if (blockIdx.x == 0) potrf_tile(tile_at(T, 0, 0), T.Linv, T.err, sA, sB, sP);
   if (!grid_barrier(T.bar, nb, T.err, T.bar_ns)) return;
+  // With the inverse, X = L^-1 is formed in the same loop: tile row J of X
+  // in phase T of column J (X_Jj = Linv_J R_Jj, its R final after the
+  // updates of the earlier columns), and its updates R_Kj -= L_KJ X_Jj in
+  // phase U -- the same products in the same order as a separate pass over
+  // the tile rows, without its barriers.
+  const int nxj = T.want_inverse ? 1 : 0;
   for (int J = 0; J < T.nt; ++J) {
     const int h = T.hrow[J], m = h - J;
-    // T: L_IJ = A_IJ L_JJ^-T
-    if (m > 0) {
-      bool have = false;
-      for (int t = blockIdx.x; t < m; t += G) {
-        const int I = J + 1 + t;
-        double *gt = tile_at(T, I, J);
-        if (!have) {
-          __syncthreads();
-          load_tile(sB, T.Linv + (size_t)J * TS, false);
-          have = true;
-        }
-        load_tile(sA, gt, false);
-        __syncthreads();
-        double acc[8][2] = {};
-        gemm_nt(sA, sB, acc);
-        __syncthreads();
-        for_frag([&](int j, int e, int r, int c) { gt[r * CT + c] = acc[j][e]; });
-      }
-    }
-    if (!grid_barrier(T.bar, nb, T.err, T.bar_ns)) return;
-    // U: A_IK -= L_IJ L_KJ^T; the tile (J+1, J+1) is then factored by its CTA
-    const long long nu = (long long)m * (m + 1) / 2;
-    for (long long t = blockIdx.x; t < nu; t += G) {
-      int bi, bk;
-      tri_item(t, bi, bk);
-      const int I = J + 1 + bi, K = J + 1 + bk;
+    // T: L_IJ = A_IJ L_JJ^-T (items 0 .. m - 1); X_Jj = Linv_J R_Jj (items
+    // m .. m + J with the inverse)
+    const int ntt = m + nxj * (J + 1);
+    for (int t = blockIdx.x; t < ntt; t += G) {
       __syncthreads();
-      load_tile(sA, tile_at(T, I, J), false);
-      load_tile(sB, tile_at(T, K, J), false);
+      double *gt;
+      if (t < m) {
+        gt = tile_at(T, J + 1 + t, J);
+        load_tile(sA, gt, false);
+        load_tile(sB, T.Linv + (size_t)J * TS, false);
+      } else {
+        gt = T.X + tri(J, t - m) * TS;
+        load_tile(sA, T.Linv + (size_t)J * TS, false);
+        load_tile(sB, gt, true);  // R^T: the product Linv R as Linv (R^T)^T
+      }
       __syncthreads();
       double acc[8][2] = {};
       gemm_nt(sA, sB, acc);
-      double *gt = tile_at(T, I, K);
+      __syncthreads();
+      for_frag([&](int j, int e, int r, int c) { gt[r * CT + c] = acc[j][e]; });
+    }
+    if (!grid_barrier(T.bar, nb, T.err, T.bar_ns)) return;
+    // U: A_IK -= L_IJ L_KJ^T (items 0 .. nu - 1); the tile (J+1, J+1) is
+    // then factored by the CTA of item 0, which takes no other item when
+    // there are other CTAs.  With the inverse also R_Kj -= L_KJ X_Jj, K > J,
+    // j <= J (items nu .. nu + m (J + 1) - 1).
+    const long long nu = (long long)m * (m + 1) / 2;
+    const long long ntu = nu + (long long)nxj * m * (J + 1);
+    const long long t0 = (G > 1 && blockIdx.x > 0) ? blockIdx.x : 0, dt = (G > 1 && blockIdx.x > 0) ? G - 1 : G;
+    for (long long t = (G > 1 && blockIdx.x == 0) ? 0 : t0; t < ntu; t += dt) {
+      __syncthreads();
+      double *gt;
+      if (t < nu) {
+        int bi, bk;
+        tri_item(t, bi, bk);
+        load_tile(sA, tile_at(T, J + 1 + bi, J), false);
+        load_tile(sB, tile_at(T, J + 1 + bk, J), false);
+        gt = tile_at(T, J + 1 + bi, J + 1 + bk);
+      } else {
+        const long long u = t - nu;
+        const int K = J + 1 + (int)(u / (J + 1)), j = (int)(u % (J + 1));
+        load_tile(sA, tile_at(T, K, J), false);
+        load_tile(sB, T.X + tri(J, j) * TS, true);
+        gt = T.X + tri(K, j) * TS;
+      }
+      __syncthreads();
+      double acc[8][2] = {};
+      gemm_nt(sA, sB, acc);
       for_frag([&](int j, int e, int r, int c) { gt[r * CT + c] -= acc[j][e]; });
-      if (bi == 0 && bk == 0) {
+      if (t == 0) {
         __syncthreads();
         potrf_tile(gt, T.Linv + (size_t)(J + 1) * TS, T.err, sA, sB, sP);
       }
+      if (G > 1 && blockIdx.x == 0) break;  // CTA 0: item 0 and the factor only
     }
     if (m == 0 && J + 1 < T.nt && blockIdx.x == (J + 1) % G)
       potrf_tile(tile_at(T, J + 1, J + 1), T.Linv + (size_t)(J + 1) * TS, T.err, sA, sB, sP);
     if (!grid_barrier(T.bar, nb, T.err, T.bar_ns)) return;
   }
   if (!T.want_inverse) return;
-  // X = L^-1 (dense): X holds R (initially the identity) and becomes X
   const int nt = T.nt;
-  for (int I = 0; I < nt; ++I) {
-    // X_Ij = Linv_I R_Ij, j <= I
-    bool have = false;
-    for (int j = blockIdx.x; j <= I; j += G) {
-      double *gx = T.X + tri(I, j) * TS;
-      if (!have) {
-        __syncthreads();
-        load_tile(sA, T.Linv + (size_t)I * TS, false);
-        have = true;
-      }
-      load_tile(sB, gx, true);  // R^T: the product Linv R as Linv (R^T)^T
-      __syncthreads();
-      double acc[8][2] = {};
-      gemm_nt(sA, sB, acc);
-      __syncthreads();
-      for_frag([&](int jj, int e, int r, int c) { gx[r * CT + c] = acc[jj][e]; });
-    }
-    if (!grid_barrier(T.bar, nb, T.err, T.bar_ns)) return;
-    // R_Kj -= L_KI X_Ij, K > I, j <= I
-    const long long nu = (long long)(nt - 1 - I) * (I + 1);
-    for (long long t = blockIdx.x; t < nu; t += G) {
-      const int K = I + 1 + (int)(t / (I + 1)), j = (int)(t % (I + 1));
-      __syncthreads();
-      load_tile(sA, tile_at(T, K, I), false);
-      load_tile(sB, T.X + tri(I, j) * TS, true);
-      __syncthreads();
-      double acc[8][2] = {};
-      gemm_nt(sA, sB, acc);
-      double *gr = T.X + tri(K, j) * TS;
-      for_frag([&](int jj, int e, int r, int c) { gr[r * CT + c] -= acc[jj][e]; });
-    }
-    if (!grid_barrier(T.bar, nb, T.err, T.bar_ns)) return;
-  }
   // A^-1 tile (i, k), k <= i: sum over m >= i of X_mi^T X_mk
   const long long no = (long long)nt * (nt + 1) / 2;
   for (long long t = blockIdx.x; t < no; t += G) {

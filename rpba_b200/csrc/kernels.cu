@@ -442,13 +442,26 @@ __global__ void __launch_bounds__(CAM_T) k_camera(DevLSA L, double multfact1) {
   } else if (tid < 54) {
     ei = tid - 45;
   }
+  // staging of a chunk: every warp reads the chunk's observation indices
+  // once (lane j: observation j) and passes them by shuffle, so that the
+  // CAM_SV record values a thread stages are independent loads in flight
+  constexpr int CAM_SV = (CAM_B * 23 + CAM_T - 1) / CAM_T;
+  const int lane = tid & 31;
   for (int base = beg; base < end; base += CAM_B) {
     const int nb = min(CAM_B, end - base);
-    for (int idx = tid; idx < nb * 23; idx += CAM_T) {
-      const int ob = idx / 23, c = idx % 23;
-      const int o = L.camlist[base + ob];
+    const int ol = lane < nb ? L.camlist[base + lane] : 0;
+    T vals[CAM_SV];
+#pragma unroll
+    for (int m = 0; m < CAM_SV; ++m) {
+      const int idx = tid + CAM_T * m, ob = idx / 23, c = idx - 23 * (idx / 23);
+      const int o = __shfl_sync(0xffffffffu, ol, ob & 31);
       const T *r = Store<T>::rec(L) + (size_t)o * REC;
-      s[ob][c] = c < 18 ? r[c] : r[26 + (c - 18)];
+      vals[m] = idx < nb * 23 ? (c < 18 ? r[c] : r[26 + (c - 18)]) : T(0);
+    }
+#pragma unroll
+    for (int m = 0; m < CAM_SV; ++m) {
+      const int idx = tid + CAM_T * m, ob = idx / 23, c = idx - 23 * (idx / 23);
+      if (idx < nb * 23) s[ob][c] = vals[m];
     }
     __syncthreads();
     if (tid < 45) {
@@ -671,8 +684,23 @@ __global__ void k_backsub(DevLSA L, const double *__restrict__ xsol) {
   for (int o = t0 + ln; o < t1; o += GRP) {
     const int k = L.o_cam[o];
     if (k < L.begini) continue;
-    const T *r = Store<T>::rec(L) + (size_t)o * REC;
+    const T *rp = Store<T>::rec(L) + (size_t)o * REC;
     const double *dc = xsol + (size_t)k * 9;
+    T r[24];
+    if constexpr (sizeof(T) == 4) {
+      // the FP32 record's first 24 floats in six 16-byte loads
+#pragma unroll
+      for (int v = 0; v < 6; ++v) {
+        const float4 q = __ldg((const float4 *)rp + v);
+        r[4 * v] = q.x;
+        r[4 * v + 1] = q.y;
+        r[4 * v + 2] = q.z;
+        r[4 * v + 3] = q.w;
+      }
+    } else {
+#pragma unroll
+      for (int a = 0; a < 24; ++a) r[a] = rp[a];
+    }
     T s0 = 0., s1 = 0.;
 #pragma unroll
     for (int a = 0; a < 9; ++a) {

@@ -58,14 +58,18 @@ __global__ void k_diag_rsqrt(DevLSA L, double *drs) {
 // drs: 1 / sqrt of every camera block's diagonal entries (k_diag_rsqrt).
 __device__ void block_features(const DevLSA &L, const double *__restrict__ drs, int k, int lane, float f[NN_F]) {
   const int np = L.camparv[k + 1] - L.camparv[k];
-  double Dd[9];
-  for (int a = 0; a < 9; ++a) Dd[a] = blk_at(L, (size_t)k, a * 10);
-  double ld[9], mean = 0.;
-  for (int a = 0; a < 9; ++a) {
-    ld[a] = a < np ? log(fmax(Dd[a], 1e-300)) : 0.;
-    if (a < np) mean += ld[a];
+  {
+    // f[0..8] first, so that only nine floats stay live through the walk
+    double ld[9], mean = 0.;
+#pragma unroll
+    for (int a = 0; a < 9; ++a) {
+      ld[a] = a < np ? log(fmax(blk_at(L, (size_t)k, a * 10), 1e-300)) : 0.;
+      if (a < np) mean += ld[a];
+    }
+    mean /= (np > 0 ? np : 1);
+#pragma unroll
+    for (int a = 0; a < 9; ++a) f[a] = a < np ? (float)(ld[a] - mean) : 0.f;
   }
-  mean /= (np > 0 ? np : 1);
   // per owned slot: row i, column j of the stored block, and this row's
   // diagonal entry for either orientation
   int ei[3], ej[3];
@@ -78,15 +82,16 @@ __device__ void block_features(const DevLSA &L, const double *__restrict__ drs, 
     rn[m] = ei[m] < 9 ? drs[(size_t)k * 9 + ei[m]] : 0.;
     rt[m] = ej[m] < 9 ? drs[(size_t)k * 9 + ej[m]] : 0.;
   }
-  // the row's entries four at a time: their positions, block elements and
-  // column scalings are all loaded before any is used (independent loads in
-  // flight), then added in entry order
-  constexpr int U = 4;
+  // the row's entries eight at a time: their positions, block elements and
+  // column scalings (as floats: features need no more) are all loaded
+  // before any is used (independent loads in flight), then added in entry
+  // order in FP64
+  constexpr int U = 8;
   const int t0 = L.rowoff[k], t1 = L.rowoff[k + 1];
   for (int tb = t0; tb < t1; tb += U) {
     int2 en[U];
     int nc[U];
-    double v[U][3], rcv[U][3];
+    float v[U][3], rcv[U][3];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       en[u] = tb + u < t1 ? L.ent[tb + u] : make_int2(k, k);
@@ -100,8 +105,8 @@ __device__ void block_features(const DevLSA &L, const double *__restrict__ drs, 
 #pragma unroll
       for (int m = 0; m < 3; ++m) {
         const int i = ei[m], j = ej[m];
-        v[u][m] = i < 9 ? blk_at(L, B, i * 9 + j) : 0.;
-        rcv[u][m] = i < 9 ? __ldg(rc + (tr ? i : j)) : 0.;
+        v[u][m] = i < 9 ? (float)blk_at(L, B, i * 9 + j) : 0.f;
+        rcv[u][m] = i < 9 ? (float)__ldg(rc + (tr ? i : j)) : 0.f;
       }
     }
 #pragma unroll
@@ -116,9 +121,9 @@ __device__ void block_features(const DevLSA &L, const double *__restrict__ drs, 
         // col; stored (col, k): it couples parameter j of k to i of col; both
         // normalised by the two diagonal entries, |S_ij| / sqrt(S_ii S_jj)
         if (!tr) {
-          if (i < np && j < nc[u]) an[m] += fabs(v[u][m]) * rn[m] * rcv[u][m];
+          if (i < np && j < nc[u]) an[m] += fabs((double)v[u][m]) * rn[m] * (double)rcv[u][m];
         } else {
-          if (j < np && i < nc[u]) at[m] += fabs(v[u][m]) * rt[m] * rcv[u][m];
+          if (j < np && i < nc[u]) at[m] += fabs((double)v[u][m]) * rt[m] * (double)rcv[u][m];
         }
       }
     }
@@ -134,10 +139,8 @@ __device__ void block_features(const DevLSA &L, const double *__restrict__ drs, 
     cpl[a] = v;
   }
   const int deg = L.rowoff[k + 1] - L.rowoff[k] - 1;  // entries besides the diagonal block
-  for (int a = 0; a < 9; ++a) {
-    f[a] = a < np ? (float)(ld[a] - mean) : 0.f;
-    f[9 + a] = a < np ? (float)log1p(cpl[a]) : 0.f;
-  }
+#pragma unroll
+  for (int a = 0; a < 9; ++a) f[9 + a] = a < np ? (float)log1p(cpl[a]) : 0.f;
   f[18] = (float)(log1p((double)deg) / 4.);
 }
 

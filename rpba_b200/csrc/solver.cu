@@ -284,6 +284,15 @@ struct rpba_handle {
     return blocks + Nc * row;
   }
 
+  // Algorithmic bytes of the PCG set-up: per camera row its diagonal block,
+  // C_k out (648 B) and five 9-vectors (r, h, x, best, rhs); with the
+  // learned preconditioner also the features, every block of every row read
+  // from both sides with its entry and the column's parameter count.
+  double setup_bytes(bool features) const {
+    const double Nc = nimg - begini, Nb = L.nboff, Eb = L.blocks32 ? 4. : 8.;
+    return Nc * (81. * Eb + 648. + 5. * 72.) + (features ? (Nc + 2. * Nb) * (81. * Eb + 8. + 8.) : 0.);
+  }
+
   // reduced camera system storage: FP64, or FP32 in the mixed form
   void ensure_blocks(int nb) {
     const bool mixed = opt.precision == RPBA_PREC_MIXED;
@@ -381,6 +390,7 @@ struct rpba_handle {
   float seq_sum(const float *v, int n) {
     {
       CoopLock lk(this);
+      prof.next_bytes = 4. * n;  // each element read once
       PROF("seq_sum", 1, launch_exact_sum(v, n, sums, ES, s));
     }
     float out = 0.f;
@@ -906,6 +916,7 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
       const int cap_try = (cw && !fresh) ? std::min(cap, 3 * coarse_ref_iters + 20) : cap;
       {
         CoopLock lk(this);
+        prof.next_bytes = setup_bytes(d_weights != nullptr);
         PROF("pcg_setup", cw ? 3 : 1, pcg_prepare(L, W, mode, d_weights, cw, s));
         PROF("pcg", 1, pcg_iterate(L, W, cap_try, pcg_grid, s, mode, opt.pcg_tolerance, cw));
       }
@@ -940,6 +951,7 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
       int it2[2] = {0, 0};
       {
         CoopLock lk(this);
+        prof.next_bytes = setup_bytes(false);
         PROF("pcg_setup", 1, pcg_prepare(L, W, 1, nullptr, nullptr, s));
         PROF("pcg", 1, pcg_iterate(L, W, msize, pcg_grid, s, 1, opt.pcg_tolerance > 0. ? opt.pcg_tolerance : 1e-6,
                                     nullptr));
@@ -960,6 +972,7 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
   } else {
     {
       CoopLock lk(this);
+      prof.next_bytes = setup_bytes(false);
       PROF("pcg_setup", 1, pcg_prepare(L, W, 0, nullptr, nullptr, s));
       PROF("pcg", 1, pcg_iterate(L, W, msize, pcg_grid, s, 0, 0., nullptr));
     }
@@ -971,6 +984,9 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
     learned_record(L, cw, W.xbest, W.Cinv, W.drs, rec_seed + 104729ull * (unsigned long long)rep.linear_solves, *rec_T,
                    *rec_H, s);
   }
+  // back-substitution: obs (camera 4, record 24 E, the camera's step 72
+  // gathered) + point (point record 12 E, offsets 8, step 24 out)
+  prof.next_bytes = No * (4 + 24 * E + 72) + Np * (12 * E + 8 + 24);
   PROF("backsub", 1, launch_backsub(L, W.xbest, s));
   PROF("xcam", 1, launch_xcam(L, W.xbest, s));
   PROF("update", 1, launch_update(L, nrunknowns, s));
@@ -1082,6 +1098,7 @@ int rpba_handle::adjust() {
       PROF("cost", 1, launch_cost(L, L.XPMn, true, s));
       {
         CoopLock lk(this);
+        prof.next_bytes = 4. * L.nobs;
         PROF("seq_sum", 1, launch_exact_sum(L.o_cost, L.nobs, sums, ES, s));
       }
       struct {
@@ -1213,6 +1230,7 @@ int rpba_handle::adjust_gcp_step() {
   PROF("decode", 1, launch_decode(L, L.XPMn, s));
   PROF("cost", 1, launch_cost(L, L.XPMn, true, s));
   launch_gcp_cost(L, L.XPMn, aoterm + 2 * (size_t)np, s);
+  prof.next_bytes = 4. * L.nobs;
   PROF("seq_sum", 1, launch_exact_sum(L.o_cost, L.nobs, sums, ES, s));
   struct {
     float sig0;
