@@ -102,34 +102,53 @@ __device__ __forceinline__ void for_frag(F f) {
 }
 
 // Factor the diagonal tile in place and write L_JJ and L_JJ^-1, with all
-// threads of the CTA: per column the pivot's square root (every thread
-// takes it), the column scaled, then the trailing triangle updated (warp w
-// rows k + 1 + w, + 8, ...; lane l columns k + 1 + l, + 32, ...) -- two
-// block barriers a column; then the inverse by columns: four lanes of one
-// warp per column c (lane q takes every fourth term mm = c + q, c + q + 4,
-// ... of entry (i, c), the four partial sums added as (p0 + p1) + (p2 + p3)),
-// rows i in order with warp barriers only.
-// s, si: two shared tiles (ld CT + 1); pp: unused scratch.
+// threads of the CTA.  Factor: panels of eight columns; warp 0 factors a
+// panel (per column the pivot's square root, the column scaled, the
+// panel's later columns updated; warp barriers only), then all threads
+// apply the panel to the trailing triangle, each entry's eight updates in
+// column order -- so every entry sees the same operations in the same
+// order as the unblocked column loop; two block barriers a panel.  Inverse:
+// four lanes of one warp per column c, rows i in order (lane q takes the
+// terms mm = c + q, c + q + 4, ... of entry (i, c), the partial sums added as
+// (p0 + p1) + (p2 + p3), times the row's reciprocal pivot), warp barriers
+// only.  s, si: two shared tiles (ld CT + 1); pp: CT doubles of scratch
+// (the reciprocal pivots).
 __device__ void potrf_tile(double *gtile, double *ginv, int *err, double *s, double *si, double *pp) {
-  (void)pp;
-  constexpr int LD = CT + 1;
+  constexpr int LD = CT + 1, PW = 8;
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   __syncthreads();
   for (int idx = t; idx < TS; idx += CTH) s[(idx >> 6) * LD + (idx & 63)] = __ldcg(gtile + idx);
   __syncthreads();
-  for (int k = 0; k < CT; ++k) {
-    const double d = s[k * LD + k];
-    const double dk = sqrt(d > 0. ? d : 1.);
-    if (t == 0 && !(d > 0.)) atomicOr(err, 4);
-    if (t < CT - 1 - k) s[(k + 1 + t) * LD + k] /= dk;
-    __syncthreads();
-    if (t == 0) s[k * LD + k] = dk;
-    for (int i = k + 1 + w; i < CT; i += CTH / 32) {
-      const double lik = s[i * LD + k];
-      for (int j = k + 1 + lane; j <= i; j += 32) s[i * LD + j] -= lik * s[j * LD + k];
+  for (int k0 = 0; k0 < CT; k0 += PW) {
+    if (w == 0) {
+      for (int k = k0; k < k0 + PW; ++k) {
+        const double d = s[k * LD + k];
+        const double dk = sqrt(d > 0. ? d : 1.);
+        if (lane == 0 && !(d > 0.)) atomicOr(err, 4);
+        for (int i = k + 1 + lane; i < CT; i += 32) s[i * LD + k] /= dk;
+        __syncwarp();
+        if (lane == 0) s[k * LD + k] = dk;
+        // the panel's later columns j (k < j < k0 + PW), rows i >= j
+        for (int j = k + 1; j < k0 + PW; ++j) {
+          const double ljk = s[j * LD + k];
+          for (int i = j + lane; i < CT; i += 32) s[i * LD + j] -= s[i * LD + k] * ljk;
+        }
+        __syncwarp();
+      }
     }
     __syncthreads();
+    // trailing triangle (rows and columns >= k0 + PW): the panel's updates
+    for (int i = k0 + PW + w; i < CT; i += CTH / 32)
+      for (int j = k0 + PW + lane; j <= i; j += 32) {
+        double v = s[i * LD + j];
+#pragma unroll
+        for (int k = k0; k < k0 + PW; ++k) v -= s[i * LD + k] * s[j * LD + k];
+        s[i * LD + j] = v;
+      }
+    __syncthreads();
   }
+  if (t < CT) pp[t] = 1. / s[t * LD + t];
+  __syncthreads();
   {
     const int c = t >> 2, q = t & 3;  // column c (0..63), partial q
     for (int i = 0; i < CT; ++i) {
@@ -140,9 +159,8 @@ __device__ void potrf_tile(double *gtile, double *ginv, int *err, double *s, dou
       const double p01 = acc + a1;  // lanes q = 0 and 2: (p0 + p1), (p2 + p3)
       const double p23 = __shfl_down_sync(0xffffffffu, p01, 2);
       if (q == 0) {
-        const double sum = p01 + p23;
-        const double dii = s[i * LD + i];
-        si[i * LD + c] = c < i ? -sum / dii : (c == i ? 1. / dii : 0.);
+        const double rdi = pp[i];
+        si[i * LD + c] = c < i ? -(p01 + p23) * rdi : (c == i ? rdi : 0.);
       }
       __syncwarp();
     }

@@ -984,9 +984,9 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
     learned_record(L, cw, W.xbest, W.Cinv, W.drs, rec_seed + 104729ull * (unsigned long long)rep.linear_solves, *rec_T,
                    *rec_H, s);
   }
-  // back-substitution: obs (camera 4, record 24 E, the camera's step 72
-  // gathered) + point (point record 12 E, offsets 8, step 24 out)
-  prof.next_bytes = No * (4 + 24 * E + 72) + Np * (12 * E + 8 + 24);
+  // back-substitution: obs (camera 4, record 24 E) + the cameras' steps
+  // (72, read once) + point (point record 12 E, offsets 8, step 24 out)
+  prof.next_bytes = No * (4 + 24 * E) + Nc * 72 + Np * (12 * E + 8 + 24);
   PROF("backsub", 1, launch_backsub(L, W.xbest, s));
   PROF("xcam", 1, launch_xcam(L, W.xbest, s));
   PROF("update", 1, launch_update(L, nrunknowns, s));
