@@ -78,15 +78,33 @@ __device__ __forceinline__ void gemm_nt(const double *sA, const double *sB, doub
   }
 }
 
-// Global tile (ld 64) -> shared (ld CLD), optionally transposed.
+// Global tile (ld 64) -> shared (ld CLD), optionally transposed: every
+// thread's sixteen loads are issued before its first store.
 __device__ __forceinline__ void load_tile(double *s, const double *g, bool trans) {
-  for (int idx = threadIdx.x; idx < TS; idx += CTH) {
-    const int i = idx >> 6, j = idx & 63;
+  double v[TS / CTH];
+#pragma unroll
+  for (int q = 0; q < TS / CTH; ++q) v[q] = __ldcg(g + threadIdx.x + q * CTH);
+#pragma unroll
+  for (int q = 0; q < TS / CTH; ++q) {
+    const int idx = threadIdx.x + q * CTH, i = idx >> 6, j = idx & 63;
     if (trans)
-      s[j * CLD + i] = __ldcg(g + idx);
+      s[j * CLD + i] = v[q];
     else
-      s[i * CLD + j] = __ldcg(g + idx);
+      s[i * CLD + j] = v[q];
   }
+}
+
+// Tile update gt -= acc (fragment positions): the sixteen old values are
+// loaded before any is written back.
+__device__ __forceinline__ void sub_frag(double *gt, const double (&acc)[8][2]) {
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int r = 8 * w + (lane >> 2), c0 = 2 * (lane & 3);
+  double2 old[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) old[j] = __ldcg((const double2 *)(gt + r * CT + 8 * j + c0));
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+    *(double2 *)(gt + r * CT + 8 * j + c0) = make_double2(old[j].x - acc[j][0], old[j].y - acc[j][1]);
 }
 
 // Fragment positions of acc[j][e]: row 8w + g, column 8j + 2t + e.
@@ -117,7 +135,13 @@ __device__ void potrf_tile(double *gtile, double *ginv, int *err, double *s, dou
   constexpr int LD = CT + 1, PW = 8;
   const int t = threadIdx.x, lane = t & 31, w = t >> 5;
   __syncthreads();
-  for (int idx = t; idx < TS; idx += CTH) s[(idx >> 6) * LD + (idx & 63)] = __ldcg(gtile + idx);
+  {
+    double v[TS / CTH];
+#pragma unroll
+    for (int q = 0; q < TS / CTH; ++q) v[q] = __ldcg(gtile + t + q * CTH);
+#pragma unroll
+    for (int q = 0; q < TS / CTH; ++q) s[((t + q * CTH) >> 6) * LD + ((t + q * CTH) & 63)] = v[q];
+  }
   __syncthreads();
   for (int k0 = 0; k0 < CT; k0 += PW) {
     if (w == 0) {
@@ -247,7 +271,7 @@ __global__ void __launch_bounds__(CTH, 1) k_chol_tiles(Tiles T) {
       __syncthreads();
       double acc[8][2] = {};
       gemm_nt(sA, sB, acc);
-      for_frag([&](int j, int e, int r, int c) { gt[r * CT + c] -= acc[j][e]; });
+      sub_frag(gt, acc);
       if (t == 0) {
         __syncthreads();
         potrf_tile(gt, T.Linv + (size_t)(J + 1) * TS, T.err, sA, sB, sP);

@@ -115,33 +115,86 @@ __global__ void k_entry_keys(DevLSA L, CoarseWork C, unsigned *key, int *val) {
   }
 }
 
-constexpr int RS_T = 256;
+// Step 2, one warp per run.  Per entry (l, S_kl) the warp stages S_kl in the
+// run's orientation (row p of k, column q of l) and P_l^T in shared memory,
+// the global loads of the next entry already in flight; lane (j, s) < 30
+// then owns Y[3 s .. 3 s + 2][j] and reads row p of S and column j of P_l as
+// 16-byte pairs.  Each Y entry sums q = 0 .. npl - 1 per entry, the entries
+// in run order (the same operations in the same order as a lane per Y entry
+// reading both operands from global memory).
+constexpr int RS_T = 256, RS_W = RS_T / 32;
 __global__ void __launch_bounds__(RS_T) k_coarse_runs(DevLSA L, CoarseWork C, int nruns) {
-  __shared__ double Ysh[RS_T / 32][9 * CO_M];
+  __shared__ __align__(16) double Ssh[RS_W][90];   // S_kl[p][q] at 10 p + q
+  __shared__ __align__(16) double Psh[RS_W][100];  // P_l[q][j] at 10 j + q
+  __shared__ double Ysh[RS_W][9 * CO_M];
   const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   if (r >= nruns) return;
+  double *Ss = Ssh[wl], *Ps = Psh[wl];
   const int k = (int)(C.run_key[r] / (unsigned)C.nagg);
   const int npk = L.camparv[k + 1] - L.camparv[k];
+  const int jc = lane % 10, s3 = lane < 30 ? lane / 10 : 0;
   double y[3] = {0., 0., 0.};
-  for (int t = C.run_off[r]; t < C.run_off[r + 1]; ++t) {
-    const int2 en = L.ent[C.ent_sorted[t]];
-    const int l = en.x;
-    const bool tr = en.y < 0;
+  const int t0 = C.run_off[r], t1 = C.run_off[r + 1];
+  int2 en = make_int2(0, 0);
+  double sv[3], pv[3];
+  auto fetch = [&](int t) {
+    en = L.ent[C.ent_sorted[t]];
     const size_t B = (size_t)(en.y & 0x7fffffff);
-    const double *Pl = C.P + (size_t)l * CP;
-    const int npl = L.camparv[l + 1] - L.camparv[l];
+    const double *Pl = C.P + (size_t)en.x * CP;
 #pragma unroll
     for (int m = 0; m < 3; ++m) {
-      const int o = lane + 32 * m, p = o / CO_M, j = o % CO_M;
-      if (o < 9 * CO_M && p < npk)
-        for (int q = 0; q < npl; ++q) y[m] += blk_at(L, B, tr ? q * 9 + p : p * 9 + q) * Pl[q * CO_M + j];
+      const int e = lane + 32 * m;
+      sv[m] = e < 81 ? blk_at(L, B, e) : 0.;
+      pv[m] = e < CP ? __ldg(Pl + e) : 0.;
     }
-  }
+  };
+  if (t0 < t1) fetch(t0);
+  for (int t = t0; t < t1; ++t) {
+    const bool tr = en.y < 0;
+    const int l = en.x;
 #pragma unroll
-  for (int m = 0; m < 3; ++m) {
-    const int o = lane + 32 * m;
-    if (o < 9 * CO_M) Ysh[wl][o] = y[m];
+    for (int m = 0; m < 3; ++m) {
+      const int e = lane + 32 * m;
+      if (e < 81) {
+        const int i = e / 9, c = e - 9 * (e / 9);
+        Ss[tr ? c * 10 + i : i * 10 + c] = sv[m];
+      }
+      if (e < CP) {
+        const int q = e / CO_M, j = e - CO_M * (e / CO_M);
+        Ps[j * 10 + q] = pv[m];
+      }
+    }
+    const int npl = L.camparv[l + 1] - L.camparv[l];
+    __syncwarp();
+    if (t + 1 < t1) fetch(t + 1);
+    double pc[10];
+#pragma unroll
+    for (int h = 0; h < 5; ++h) {
+      const double2 v = *(const double2 *)(Ps + jc * 10 + 2 * h);
+      pc[2 * h] = v.x;
+      pc[2 * h + 1] = v.y;
+    }
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+      const int p = 3 * s3 + u;
+      double sr[10];
+#pragma unroll
+      for (int h = 0; h < 5; ++h) {
+        const double2 v = *(const double2 *)(Ss + p * 10 + 2 * h);
+        sr[2 * h] = v.x;
+        sr[2 * h + 1] = v.y;
+      }
+      if (lane < 30 && p < npk) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q)
+          if (q < npl) y[u] += sr[q] * pc[q];
+      }
+    }
+    __syncwarp();
   }
+  if (lane < 30)
+#pragma unroll
+    for (int u = 0; u < 3; ++u) Ysh[wl][(3 * s3 + u) * CO_M + jc] = y[u];
   __syncwarp();
   const double *Pk = C.P + (size_t)k * CP;
 #pragma unroll

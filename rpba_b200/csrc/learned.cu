@@ -86,16 +86,18 @@ __device__ void block_features(const DevLSA &L, const double *__restrict__ drs, 
   // column scalings (as floats: features need no more) are all loaded
   // before any is used (independent loads in flight), then added in entry
   // order in FP64
+  // (the next batch's entries are loaded one batch ahead, lane u entry u)
   constexpr int U = 8;
   const int t0 = L.rowoff[k], t1 = L.rowoff[k + 1];
+  int2 enl = (lane < U && t0 + lane < t1) ? L.ent[t0 + lane] : make_int2(k, k);
   for (int tb = t0; tb < t1; tb += U) {
     int2 en[U];
     int nc[U];
     float v[U][3], rcv[U][3];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-      en[u] = tb + u < t1 ? L.ent[tb + u] : make_int2(k, k);
-      nc[u] = L.camparv[en[u].x + 1] - L.camparv[en[u].x];
+      en[u].x = __shfl_sync(0xffffffffu, enl.x, u);
+      en[u].y = __shfl_sync(0xffffffffu, enl.y, u);
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
@@ -108,6 +110,12 @@ __device__ void block_features(const DevLSA &L, const double *__restrict__ drs, 
         v[u][m] = i < 9 ? (float)blk_at(L, B, i * 9 + j) : 0.f;
         rcv[u][m] = i < 9 ? (float)__ldg(rc + (tr ? i : j)) : 0.f;
       }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) nc[u] = L.camparv[en[u].x + 1] - L.camparv[en[u].x];
+    {
+      const int tn = tb + U + lane;
+      enl = (lane < U && tn < t1) ? L.ent[tn] : make_int2(k, k);
     }
 #pragma unroll
     for (int u = 0; u < U; ++u) {
