@@ -16,7 +16,11 @@
 // element k with S + R_(k-1) + floor(v_k/u) >= 2^24 (the sum leaves the
 // binade); that element is added with a real float addition and a new run
 // starts in the new binade.  Runs are few: the sum leaves a binade only when
-// it doubles.
+// it doubles.  Each step of the scan covers a window, the elements from the
+// run's start on, as many again as the sum has taken so far: the sum doubles
+// inside it unless the terms shrink (then the next step takes the next
+// window in the same binade), so the steps together read the input about
+// twice instead of once per binade.
 //
 // The first HEAD elements and any stretch where s is zero or subnormal are
 // added by one warp in plain sequence.  Inputs must be finite and >= 0.
@@ -36,6 +40,7 @@ constexpr int ES_T = 256;
 constexpr int HEAD = 2048;
 constexpr long long RCLAMP = 1ll << 30;  // n * RCLAMP < 2^61 for n < 2^31
 constexpr int MAX_SEGMENTS = 512;
+constexpr int ES_WMIN = 65536;  // smallest window of a run step
 
 struct EsCtl {
   float s;    // running sum before element i
@@ -124,9 +129,6 @@ __device__ float warp_seq(const float *v, int i, int i_end, float s) {
 __global__ void __launch_bounds__(ES_T) k_exact_sum(EsArgs A) {
   const int G = gridDim.x, c = blockIdx.x, tid = threadIdx.x;
   const int n = A.n;
-  const int chunk = (n + G - 1) / G;
-  const int lo = min(n, c * chunk), hi = min(n, lo + chunk);
-  const int per = (chunk + ES_T - 1) / ES_T;
   __shared__ Xf s_x[ES_T];  // per-thread composites of the current run
   __shared__ long long s_rtot, s_R;
   __shared__ int s_cx, s_qx, s_tcross, s_q;
@@ -151,8 +153,8 @@ __global__ void __launch_bounds__(ES_T) k_exact_sum(EsArgs A) {
     const int i0 = __ldcg(&A.ctl->i);
     if (i0 >= n) break;
     if (seg >= MAX_SEGMENTS) {
-      // more binade changes than any finite float sum can make: finish in
-      // plain sequence, still exact
+      // far more steps (binade changes and windows) than sums of real data
+      // take: finish in plain sequence, still exact
       if (c == 0 && tid < 32) {
         const float sr = warp_seq(A.v, i0, n, s);
         if (tid == 0) A.ctl->s = sr;
@@ -168,8 +170,18 @@ __global__ void __launch_bounds__(ES_T) k_exact_sum(EsArgs A) {
     const int p0 = (int)(S & 1);
     const long long TOP = 1ll << 24;
 
+    // The step's window: the elements from i0 on, as many again as the sum
+    // has taken so far (at least ES_WMIN).  The sum leaves its binade when it
+    // doubles, so the crossing is inside the window unless the terms shrink;
+    // a window without a crossing ends the step at its last element, the sum
+    // still in the same binade, and the next step takes the next window.
+    // The window is cut into G chunks (CTA c: chunk c).
+    const int wend = (int)min((long long)n, (long long)i0 + max((long long)i0, (long long)ES_WMIN));
+    const int chunk = (wend - i0 + G - 1) / G;
+    const int lo = min(wend, i0 + c * chunk), hi = min(wend, lo + chunk);
+    const int per = (chunk + ES_T - 1) / ES_T;
     // phase A: composite of each thread's contiguous sub-range of this
-    // chunk (from max(lo, i0)), then of the chunk
+    // chunk, then of the chunk
     const int a0 = max(lo, i0);
     const int t_lo = lo + tid * per, t_hi = min(hi, t_lo + per);
     Xf tx = xf_identity();
@@ -222,7 +234,7 @@ __global__ void __launch_bounds__(ES_T) k_exact_sum(EsArgs A) {
     if (cxi == INT_MAX) {
       if (c == 0 && tid == 0) {
         A.ctl->s = (float)((double)(S + s_rtot) * u);
-        A.ctl->i = n;
+        A.ctl->i = wend;
       }
     } else if (c == cxi) {
       // the crossing chunk: thread 0 finds the first crossing thread range,

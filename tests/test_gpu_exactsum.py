@@ -25,6 +25,9 @@ def _cases():
     t[100_000:] = (rng.random(100_000)).astype(np.float32)
     yield "subnormal start", t
     yield "huge first", np.concatenate([[np.float32(3e38)], rng.random(100_000).astype(np.float32)])
+    # shrinking terms: the sum stays in one binade across many windows
+    yield "shrinking terms", (1.0 / np.sqrt(1.0 + np.arange(2_000_000))).astype(np.float32)
+    yield "growing terms", (np.arange(1_500_000) * 1e-3).astype(np.float32)
 
 
 @pytest.mark.parametrize("name,v", list(_cases()), ids=[c[0] for c in _cases()])
@@ -33,3 +36,14 @@ def test_exact_sum_bitwise(name, v):
     ref = np.cumsum(v, dtype=np.float32)[-1] if v.size else np.float32(0)
     got = rb.float_sequential_sum(v)
     assert got.tobytes() == np.float32(ref).tobytes(), (name, got, ref)
+
+
+def test_exact_sum_bitwise_bench_size():
+    """The bench's size: 29M cost-like terms (generated inside the test, not
+    at collection)."""
+    import rpba_b200 as rb
+    rng = np.random.default_rng(6)
+    v = (rng.normal(0, 0.5, 29_000_000) ** 2 * rng.uniform(0.1, 2.0, 29_000_000)).astype(np.float32)
+    ref = np.cumsum(v, dtype=np.float32)[-1]
+    got = rb.float_sequential_sum(v)
+    assert got.tobytes() == np.float32(ref).tobytes(), (got, ref)
