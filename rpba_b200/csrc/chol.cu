@@ -121,11 +121,11 @@ __device__ __forceinline__ void for_frag(F f) {
 
 // Factor the diagonal tile in place and write L_JJ and L_JJ^-1, with all
 // threads of the CTA.  Factor: panels of eight columns; warp 0 factors a
-// panel (per column the pivot's square root, the column scaled, the
-// panel's later columns updated; warp barriers only), then all threads
-// apply the panel to the trailing triangle, each entry's eight updates in
-// column order -- so every entry sees the same operations in the same
-// order as the unblocked column loop; two block barriers a panel.  Inverse:
+// panel (per column the pivot's square root, the column scaled by its
+// reciprocal, the panel's later columns updated; warp barriers only), then
+// all threads apply the panel to the trailing triangle, each entry's eight
+// updates in column order, as in the unblocked column loop; two block
+// barriers a panel.  Inverse:
 // four lanes of one warp per column c, rows i in order (lane q takes the
 // terms mm = c + q, c + q + 4, ... of entry (i, c), the partial sums added as
 // (p0 + p1) + (p2 + p3), times the row's reciprocal pivot), warp barriers
@@ -147,9 +147,9 @@ __device__ void potrf_tile(double *gtile, double *ginv, int *err, double *s, dou
     if (w == 0) {
       for (int k = k0; k < k0 + PW; ++k) {
         const double d = s[k * LD + k];
-        const double dk = sqrt(d > 0. ? d : 1.);
+        const double dk = sqrt(d > 0. ? d : 1.), rdk = 1. / dk;
         if (lane == 0 && !(d > 0.)) atomicOr(err, 4);
-        for (int i = k + 1 + lane; i < CT; i += 32) s[i * LD + k] /= dk;
+        for (int i = k + 1 + lane; i < CT; i += 32) s[i * LD + k] *= rdk;
         __syncwarp();
         if (lane == 0) s[k * LD + k] = dk;
         // the panel's later columns j (k < j < k0 + PW), rows i >= j

@@ -41,6 +41,7 @@ constexpr int HEAD = 2048;
 constexpr long long RCLAMP = 1ll << 30;  // n * RCLAMP < 2^61 for n < 2^31
 constexpr int MAX_SEGMENTS = 512;
 constexpr int ES_WMIN = 65536;  // smallest window of a run step
+constexpr int ES_MAXG = 512;    // CTAs at most (their composites are staged in shared memory)
 
 struct EsCtl {
   float s;    // running sum before element i
@@ -130,6 +131,8 @@ __global__ void __launch_bounds__(ES_T) k_exact_sum(EsArgs A) {
   const int G = gridDim.x, c = blockIdx.x, tid = threadIdx.x;
   const int n = A.n;
   __shared__ Xf s_x[ES_T];  // per-thread composites of the current run
+  __shared__ long long s_cR[2 * ES_MAXG], s_cM[2 * ES_MAXG];  // the chunks' composites
+  __shared__ unsigned char s_cT[2 * ES_MAXG];
   __shared__ long long s_rtot, s_R;
   __shared__ int s_cx, s_qx, s_tcross, s_q;
 
@@ -207,23 +210,29 @@ __global__ void __launch_bounds__(ES_T) k_exact_sum(EsArgs A) {
     // phase B (every CTA, one thread): walk the chunk composites in order
     // from the run's start state; find the first chunk that crosses, the
     // state at its start, and the state at the end
+    // (the composites are first copied to shared memory by all threads,
+    // independent loads, so the walk's dependent steps are shared loads)
+    for (int j = tid; j < 2 * G; j += ES_T) {
+      s_cR[j] = __ldcg(A.Rc + j);
+      s_cM[j] = __ldcg(A.Mc + j);
+      s_cT[j] = (unsigned char)__ldcg(A.Tc + j);
+    }
+    __syncthreads();
     if (tid == 0) {
       long long R = 0;
       int q = p0, cxq = INT_MAX;
       long long Rx = 0;
       int qx = 0;
       for (int cc = 0; cc < G; ++cc) {
-        const long long Mq = __ldcg(A.Mc + 2 * cc + q);
+        const long long Mq = s_cM[2 * cc + q];
         if (Mq != LLONG_MIN && S + R + Mq >= TOP) {
           cxq = cc;
           Rx = R;
           qx = q;
           break;
         }
-        const long long Rq = __ldcg(A.Rc + 2 * cc + q);
-        const int qn = __ldcg(A.Tc + 2 * cc + q);
-        R += Rq;
-        q = qn;
+        R += s_cR[2 * cc + q];
+        q = s_cT[2 * cc + q];
       }
       s_cx = cxq;
       s_rtot = cxq == INT_MAX ? R : Rx;
@@ -311,7 +320,8 @@ int exact_sum_max_grid(int device) {
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_exact_sum, ES_T, 0);
   if (per < 1) per = 1;
-  return nsm * (per < 2 ? per : 2);
+  const int g = nsm * (per < 2 ? per : 2);
+  return g < ES_MAXG ? g : ES_MAXG;
 }
 
 void launch_exact_sum(const float *v, int n, float *out, const ExactSumWork &W, cudaStream_t s) {
@@ -358,6 +368,7 @@ using namespace rpba;
 namespace {
 
 constexpr int NA_MAX_CTAS = 512;
+static_assert(NA_MAX_CTAS <= ES_MAXG, "k_exact_sum stages at most ES_MAXG chunk composites");
 constexpr int NA_CHUNK = 8192;  // elements per CTA when the grid allows it
 constexpr long long NA_MAX_N = (long long)NA_MAX_CTAS * NA_CHUNK;  // 4,194,304
 constexpr size_t NA_OFF_RC = 0;

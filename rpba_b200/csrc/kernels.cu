@@ -444,13 +444,15 @@ __global__ void __launch_bounds__(CAM_T) k_camera(DevLSA L, double multfact1) {
   }
   // staging of a chunk: every warp reads the chunk's observation indices
   // once (lane j: observation j) and passes them by shuffle, so that the
-  // CAM_SV record values a thread stages are independent loads in flight
+  // CAM_SV record values a thread stages are independent loads in flight;
+  // the next chunk's record values are loaded while this chunk is summed,
+  // and the indices two chunks ahead
   constexpr int CAM_SV = (CAM_B * 23 + CAM_T - 1) / CAM_T;
   const int lane = tid & 31;
-  for (int base = beg; base < end; base += CAM_B) {
+  auto idx_of = [&](int base) { return base + lane < end ? L.camlist[base + lane] : 0; };
+  T vals[CAM_SV];
+  auto fetch = [&](int base, int ol) {
     const int nb = min(CAM_B, end - base);
-    const int ol = lane < nb ? L.camlist[base + lane] : 0;
-    T vals[CAM_SV];
 #pragma unroll
     for (int m = 0; m < CAM_SV; ++m) {
       const int idx = tid + CAM_T * m, ob = idx / 23, c = idx - 23 * (idx / 23);
@@ -458,12 +460,22 @@ __global__ void __launch_bounds__(CAM_T) k_camera(DevLSA L, double multfact1) {
       const T *r = Store<T>::rec(L) + (size_t)o * REC;
       vals[m] = idx < nb * 23 ? (c < 18 ? r[c] : r[26 + (c - 18)]) : T(0);
     }
+  };
+  int ol_next = idx_of(beg + CAM_B);
+  if (beg < end) fetch(beg, idx_of(beg));
+  for (int base = beg; base < end; base += CAM_B) {
+    const int nb = min(CAM_B, end - base);
 #pragma unroll
     for (int m = 0; m < CAM_SV; ++m) {
       const int idx = tid + CAM_T * m, ob = idx / 23, c = idx - 23 * (idx / 23);
       if (idx < nb * 23) s[ob][c] = vals[m];
     }
     __syncthreads();
+    if (base + CAM_B < end) {
+      const int ol = ol_next;
+      ol_next = idx_of(base + 2 * CAM_B);
+      fetch(base + CAM_B, ol);
+    }
     if (tid < 45) {
       for (int ob = 0; ob < nb; ++ob) {
         const T b0i = s[ob][ei], b1i = s[ob][9 + ei], b0j = s[ob][ej], b1j = s[ob][9 + ej];
