@@ -67,11 +67,13 @@ __device__ __forceinline__ Xf xf_identity() {
 // a then b
 __device__ __forceinline__ Xf xf_then(const Xf &a, const Xf &b) {
   Xf x;
+#pragma unroll
   for (int p = 0; p < 2; ++p) {
-    const int m = a.q[p];
-    x.R[p] = a.R[p] + b.R[m];
-    x.q[p] = b.q[m];
-    x.M[p] = b.M[m] == LLONG_MIN ? a.M[p] : max(a.M[p], a.R[p] + b.M[m]);
+    const bool m = a.q[p] != 0;  // b's state entered with parity a.q[p] (selects: no indexing)
+    const long long bR = m ? b.R[1] : b.R[0], bM = m ? b.M[1] : b.M[0];
+    x.R[p] = a.R[p] + bR;
+    x.q[p] = m ? b.q[1] : b.q[0];
+    x.M[p] = bM == LLONG_MIN ? a.M[p] : max(a.M[p], a.R[p] + bM);
   }
   return x;
 }
@@ -131,6 +133,7 @@ __global__ void __launch_bounds__(ES_T) k_exact_sum(EsArgs A) {
   const int G = gridDim.x, c = blockIdx.x, tid = threadIdx.x;
   const int n = A.n;
   __shared__ Xf s_x[ES_T];  // per-thread composites of the current run
+  __shared__ Xf s_w[ES_T / 32];  // per-warp composites
   __shared__ long long s_cR[2 * ES_MAXG], s_cM[2 * ES_MAXG];  // the chunks' composites
   __shared__ unsigned char s_cT[2 * ES_MAXG];
   __shared__ long long s_rtot, s_R;
@@ -194,11 +197,30 @@ __global__ void __launch_bounds__(ES_T) k_exact_sum(EsArgs A) {
       classify(A.v[k], scale, fl, r, tie);
       xf_push(tx, fl, r, tie);
     }
-    s_x[tid] = tx;
+    s_x[tid] = tx;  // kept for the crossing chunk's walk
+    // the chunk's composite: each warp's thread composites combined in a
+    // tree that keeps lane order ((x0 x1)(x2 x3))..., then the warps' in
+    // order (the composition is exact integer arithmetic and associative)
+    {
+      const int lane = tid & 31;
+      Xf wx = tx;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        Xf ot;
+#pragma unroll
+        for (int p = 0; p < 2; ++p) {
+          ot.R[p] = __shfl_down_sync(0xffffffffu, wx.R[p], o);
+          ot.M[p] = __shfl_down_sync(0xffffffffu, wx.M[p], o);
+          ot.q[p] = __shfl_down_sync(0xffffffffu, wx.q[p], o);
+        }
+        if ((lane & (2 * o - 1)) == 0) wx = xf_then(wx, ot);
+      }
+      if (lane == 0) s_w[tid >> 5] = wx;
+    }
     __syncthreads();
     if (tid == 0) {
-      Xf cx = xf_identity();
-      for (int t = 0; t < ES_T; ++t) cx = xf_then(cx, s_x[t]);
+      Xf cx = s_w[0];
+      for (int w = 1; w < ES_T / 32; ++w) cx = xf_then(cx, s_w[w]);
       for (int p = 0; p < 2; ++p) {
         A.Rc[2 * c + p] = cx.R[p];
         A.Mc[2 * c + p] = cx.M[p];
