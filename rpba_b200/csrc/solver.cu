@@ -226,6 +226,7 @@ struct rpba_handle {
   float4 *d0_o_wold;
   double *d0_P, *d0_Kc, *d0_dc, *d0_X;
   CamState *d0_camn;
+  float *d_XXin = nullptr;  // the caller's points as given (rpba_get_state keeps the unused ones)
 
   // working state
   DevLSA L{};
@@ -449,6 +450,8 @@ static int create_impl(rpba_handle *H, const rpba_block *b, const rpba_options *
   H->h_K.assign(b->K, b->K + 9 * n);
   H->h_dist.assign(b->distpara, b->distpara + 2 * n);
   H->h_XX.assign(b->XX, b->XX + 3 * np);
+  H->d_XXin = dalloc<float>(3 * (size_t)std::max(np, 1), own);
+  if (np) RPBA_CUDA_CHECK(cudaMemcpyAsync(H->d_XXin, b->XX, sizeof(float) * 3 * np, cudaMemcpyHostToDevice, H->s));
   if (o->exteval) {
     H->h_img_off.assign(b->img_obs_off, b->img_obs_off + n + 1);
     H->h_xg.assign(b->xg, b->xg + 2 * H->n_slots);
@@ -1380,6 +1383,38 @@ int32_t rpba_get_log(rpba_handle *H, char *log, size_t cap) {
   return RPBA_OK;
 }
 
+namespace {
+// rpba_get_state on the device, for tracks kept as one CSR over strictly
+// increasing point ids (the layout the solver keeps).  Violations of that
+// layout set *bad.
+__global__ void k_state_check(const int *pt_off, const int *pt_id, int np, int nall, int *bad) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= np) return;
+  if (pt_off[q] > pt_off[q + 1] || pt_id[q] < 0 || pt_id[q] >= nall || (q > 0 && pt_id[q - 1] >= pt_id[q]))
+    atomicOr(bad, 1);
+}
+// The solved points into the caller's point array (the others keep their
+// input values, already in XXf).
+__global__ void k_state_xx(const double *X, const int *pt_id, int np, float *XXf) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= np) return;
+  const size_t i = (size_t)pt_id[q];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) XXf[3 * i + j] = (float)X[3 * (size_t)q + j];
+}
+// Track offsets over all nall input points: point ids from that of kept
+// point q - 1 up to (not including) that of kept point q end where kept
+// point q - 1 ends (pt_off[q]); off[0] = 0.  Thread q in 0 .. np.
+__global__ void k_state_off(const int *pt_off, const int *pt_id, int np, int nall, int *off) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q > np) return;
+  if (q == 0) off[0] = 0;
+  const int lo = q == 0 ? 0 : pt_id[q - 1], hi = q == np ? nall : pt_id[q];
+  const int v = pt_off[q];
+  for (int i = lo; i < hi; ++i) off[i + 1] = v;
+}
+}  // namespace
+
 // OutputLSAc + PointXXvOut (rbacore.cpp:644-666, 1978-2010).
 int32_t rpba_get_state(rpba_handle *H, rpba_block *blk) {
   if (!H || !blk || H->opt.exteval) return RPBA_ERR_ARG;
@@ -1393,25 +1428,85 @@ int32_t rpba_get_state(rpba_handle *H, rpba_block *blk) {
     rpba_handle *H = a->H;
     rpba_block *b = a->b;
     RPBA_CUDA_CHECK(cudaSetDevice(H->dev));
-    const int n = H->nimg, no = H->L.nobs, np = H->L.npts;
+    const int n = H->nimg, no = H->L.nobs, np = H->L.npts, nall = H->XXnr;
     std::vector<double> P(12 * (size_t)n);
     std::vector<CamState> cams(n);
-    std::vector<int> pt_off(np + 1), pt_id(np);
-    std::vector<double> X(3 * (size_t)np);
     auto dn = [&](void *h, const void *d, size_t bytes) {
       if (bytes) RPBA_CUDA_CHECK(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, H->s));
     };
+    auto cameras_out = [&]() {
+      for (size_t i = 0; i < P.size(); ++i) b->pmat[i] = (float)P[i];
+      for (int i = 0; i < n; ++i) {
+        const CamState &c = cams[i];
+        float *K = b->K + 9 * i;
+        const float *Ki = H->h_K.data() + 9 * i;
+        K[0] = (float)c.K00;
+        K[1] = (float)c.K01;
+        K[2] = (float)c.K02;
+        K[3] = Ki[3];
+        K[4] = (float)c.K11;
+        K[5] = (float)c.K12;
+        K[6] = Ki[6];
+        K[7] = Ki[7];
+        K[8] = 1.f;
+        b->distpara[2 * i] = (float)c.d0;
+        b->distpara[2 * i + 1] = (float)c.d1;
+      }
+    };
     dn(P.data(), H->L.Pacc, sizeof(double) * P.size());
     dn(cams.data(), H->L.camn, sizeof(CamState) * n);
+    // The output tracks are the device's, point by point in increasing
+    // point order.  When the device lists are one CSR from 0 to nobs over
+    // strictly increasing point ids (the layout the solver keeps), that
+    // concatenation is the device arrays as they are, and the points and
+    // offsets are formed on the device: everything goes straight into the
+    // caller's arrays.  Otherwise the tracks are gathered point by point on
+    // the host.
+    {
+      int *dbad = nullptr, *doff = nullptr;
+      float *dxx = nullptr;
+      RPBA_CUDA_CHECK(cudaMallocAsync(&dbad, sizeof(int) * 4, H->s));
+      RPBA_CUDA_CHECK(cudaMemsetAsync(dbad, 0, sizeof(int) * 4, H->s));
+      if (np > 0) k_state_check<<<(np + 255) / 256, 256, 0, H->s>>>(H->L.pt_off, H->L.pt_id, np, nall, dbad);
+      int ends[2] = {0, 0}, bad = 0;
+      dn(&ends[0], H->L.pt_off, sizeof(int));
+      dn(&ends[1], H->L.pt_off + np, sizeof(int));
+      dn(&bad, dbad, sizeof(int));
+      RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
+      const bool fast = bad == 0 && ends[0] == 0 && ends[1] == no && no <= H->n_track_in;
+      if (fast) {
+        RPBA_CUDA_CHECK(cudaMallocAsync(&dxx, sizeof(float) * 3 * std::max(nall, 1), H->s));
+        RPBA_CUDA_CHECK(cudaMallocAsync(&doff, sizeof(int) * (nall + 1), H->s));
+        if (nall)
+          RPBA_CUDA_CHECK(cudaMemcpyAsync(dxx, H->d_XXin, sizeof(float) * 3 * nall, cudaMemcpyDeviceToDevice, H->s));
+        if (np > 0) k_state_xx<<<(np + 255) / 256, 256, 0, H->s>>>(H->L.XPM + H->nrioff, H->L.pt_id, np, dxx);
+        k_state_off<<<(np + 1 + 255) / 256, 256, 0, H->s>>>(H->L.pt_off, H->L.pt_id, np, nall, doff);
+        RPBA_CUDA_CHECK(cudaGetLastError());
+        dn(b->XX, dxx, sizeof(float) * 3 * nall);
+        dn(b->pt_obs_off, doff, sizeof(int) * (nall + 1));
+        dn(b->pt_obs_image, H->L.o_cam, sizeof(int) * no);
+        dn(b->pt_obs_slot, H->L.o_slot, sizeof(int) * no);
+        RPBA_CUDA_CHECK(cudaFreeAsync(dxx, H->s));
+        RPBA_CUDA_CHECK(cudaFreeAsync(doff, H->s));
+      }
+      RPBA_CUDA_CHECK(cudaFreeAsync(dbad, H->s));
+      if (fast) {
+        RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
+        cameras_out();
+        // entries past the kept observations are 0
+        if (H->n_track_in > no) {
+          std::memset(b->pt_obs_image + no, 0, sizeof(int) * (size_t)(H->n_track_in - no));
+          std::memset(b->pt_obs_slot + no, 0, sizeof(int) * (size_t)(H->n_track_in - no));
+        }
+        return (int)RPBA_OK;
+      }
+    }
+    std::vector<int> pt_off(np + 1), pt_id(np);
+    std::vector<double> X(3 * (size_t)np);
     dn(pt_off.data(), H->L.pt_off, sizeof(int) * (np + 1));
     dn(pt_id.data(), H->L.pt_id, sizeof(int) * np);
     dn(X.data(), H->L.XPM + H->nrioff, sizeof(double) * 3 * np);
     RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
-    // The output tracks are the device's, point by point in increasing
-    // point order.  When the device lists are one CSR from 0 to nobs over
-    // strictly increasing point ids (the layout the solver keeps), that
-    // concatenation is the device arrays as they are: copy them straight
-    // into the caller's; otherwise gather them point by point.
     bool direct = pt_off[0] == 0 && pt_off[np] == no && no <= H->n_track_in;
     for (int q = 0; q < np && direct; ++q)
       direct = pt_off[q] <= pt_off[q + 1] && pt_id[q] >= 0 && pt_id[q] < H->XXnr && (q == 0 || pt_id[q - 1] < pt_id[q]);
@@ -1426,23 +1521,7 @@ int32_t rpba_get_state(rpba_handle *H, rpba_block *blk) {
       dn(o_slot.data(), H->L.o_slot, sizeof(int) * no);
     }
     RPBA_CUDA_CHECK(cudaStreamSynchronize(H->s));
-    for (size_t i = 0; i < P.size(); ++i) b->pmat[i] = (float)P[i];
-    for (int i = 0; i < n; ++i) {
-      const CamState &c = cams[i];
-      float *K = b->K + 9 * i;
-      const float *Ki = H->h_K.data() + 9 * i;
-      K[0] = (float)c.K00;
-      K[1] = (float)c.K01;
-      K[2] = (float)c.K02;
-      K[3] = Ki[3];
-      K[4] = (float)c.K11;
-      K[5] = (float)c.K12;
-      K[6] = Ki[6];
-      K[7] = Ki[7];
-      K[8] = 1.f;
-      b->distpara[2 * i] = (float)c.d0;
-      b->distpara[2 * i + 1] = (float)c.d1;
-    }
+    cameras_out();
     std::memcpy(b->XX, H->h_XX.data(), sizeof(float) * H->h_XX.size());
     int w = 0, q = 0;
     b->pt_obs_off[0] = 0;
@@ -1460,6 +1539,10 @@ int32_t rpba_get_state(rpba_handle *H, rpba_block *blk) {
         ++q;
       }
       b->pt_obs_off[i + 1] = w;
+    }
+    if (H->n_track_in > w) {
+      std::memset(b->pt_obs_image + w, 0, sizeof(int) * (size_t)(H->n_track_in - w));
+      std::memset(b->pt_obs_slot + w, 0, sizeof(int) * (size_t)(H->n_track_in - w));
     }
     return (int)RPBA_OK;
   }, &a);

@@ -438,15 +438,24 @@ class Solver:
         load().rpba_get_log(self.h, buf, cap)
         return buf.value.decode()
 
-    def state(self) -> Block:
+    def state(self, out: Block | None = None) -> Block:
         """The adjusted block: new cameras, points and tracks (the
         observation arrays xg, wx, wy, wxy and img_obs_off, which a solve
         does not change, are shared with the input block).  The track
-        arrays keep the input's length; entries past pt_obs_off[-1] are 0."""
+        arrays keep the input's length; entries past pt_obs_off[-1] are 0.
+        ``out``: a block of the input's shape whose pmat, K, distpara, XX and
+        track arrays receive the result (for example arrays in page-locked
+        memory, reused from call to call); it is returned."""
         b = self.block
-        out = Block(np.empty_like(b.pmat), np.empty_like(b.K), np.empty_like(b.distpara), np.empty_like(b.XX),
-                    b.img_obs_off, b.xg, b.wx, b.wy, b.wxy, np.empty_like(b.pt_obs_off),
-                    np.zeros_like(b.pt_obs_image), np.zeros_like(b.pt_obs_slot))
+        if out is None:
+            out = Block(np.empty_like(b.pmat), np.empty_like(b.K), np.empty_like(b.distpara), np.empty_like(b.XX),
+                        b.img_obs_off, b.xg, b.wx, b.wy, b.wxy, np.empty_like(b.pt_obs_off),
+                        np.zeros_like(b.pt_obs_image), np.zeros_like(b.pt_obs_slot))
+        else:
+            for name in ("pmat", "K", "distpara", "XX", "pt_obs_off", "pt_obs_image", "pt_obs_slot"):
+                a, ref = getattr(out, name), getattr(b, name)
+                if a.shape != ref.shape or a.dtype != ref.dtype or not a.flags.c_contiguous or not a.flags.writeable:
+                    raise ValueError(f"state(out=...): {name} must be a writable C-contiguous {ref.dtype} array of shape {ref.shape}")
         cb = out.as_c()
         st = load().rpba_get_state(self.h, C.byref(cb))
         if st != 0:

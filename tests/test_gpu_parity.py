@@ -187,3 +187,25 @@ def test_error_no_observations_in_image(oracle_mod):
     assert o[0] == 3 and g[0] == 3
     assert "BA-Error: No observations in image 5" in g[3]
     assert g[3] == o[3]
+
+
+def test_state_into_caller_arrays(arc_block):
+    """Solver.state(out=...) writes the same result into the caller's arrays
+    (stale values in them overwritten, the track tails zeroed) as state()."""
+    import rpba_b200 as rb
+    with rb.Solver(arc_block) as s:
+        st, rep = s.solve()
+        assert st == 0
+        a = s.state()
+        out = arc_block.copy()
+        for name in ("pmat", "K", "distpara", "XX"):
+            getattr(out, name)[...] = 7.0
+        out.pt_obs_off[...] = -1
+        out.pt_obs_image[...] = -1
+        out.pt_obs_slot[...] = -1
+        b = s.state(out=out)
+        assert b is out
+    for name in ("pmat", "K", "distpara", "XX", "pt_obs_off", "pt_obs_image", "pt_obs_slot"):
+        assert np.array_equal(getattr(a, name), getattr(b, name)), name
+    end = int(b.pt_obs_off[-1])
+    assert not b.pt_obs_image[end:].any() and not b.pt_obs_slot[end:].any()
