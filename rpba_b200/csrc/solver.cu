@@ -911,7 +911,9 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
         prof.next_bytes = 4. * nc * nc * 8;
         {
           CoopLock lk(this);
-          PROF("coarse_factor", 2, coarse_factor(CW, s));
+          // diagonal scaling, tile metadata, packing, the factorisation and
+          // inverse, unpacking
+          PROF("coarse_factor", 5, coarse_factor(CW, s));
         }
         coarse_stale = false;
         fresh = true;
@@ -920,7 +922,9 @@ bool rpba_handle::calc_bundle_sep(double multfact, int nrunknowns) {
       {
         CoopLock lk(this);
         prof.next_bytes = setup_bytes(d_weights != nullptr);
-        PROF("pcg_setup", cw ? 3 : 1, pcg_prepare(L, W, mode, d_weights, cw, s));
+        // set-up kernels: rsqrt, features and set-up with weights (else the
+        // set-up alone), the coarse restriction and prolongation
+        PROF("pcg_setup", (d_weights ? 3 : 1) + (cw ? 2 : 0), pcg_prepare(L, W, mode, d_weights, cw, s));
         PROF("pcg", 1, pcg_iterate(L, W, cap_try, pcg_grid, s, mode, opt.pcg_tolerance, cw));
       }
       RPBA_CUDA_CHECK(cudaMemcpyAsync(it, W.iters, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
