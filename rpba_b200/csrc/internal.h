@@ -296,7 +296,6 @@ int pcg_prepare(const DevLSA &L, const PcgWork &W, int mode, const float *weight
 int pcg_iterate(const DevLSA &L, const PcgWork &W, int msize, int grid, cudaStream_t s, int mode, double tol,
                 const CoarseWork *coarse);
 int pcg_max_grid(int device);
-int pcg_warps32();  // warps per CTA of the FP32 form's persistent PCG
 
 // ---- structure (structure.cu)
 struct StructWork {

@@ -4,8 +4,9 @@
 // the squared step increment drops by 1e5 or after msize iterations,
 // beta = r1^T (h1 - h) / r^T h clamped at 0.
 //
-// One cooperative launch runs the whole solve.  Rows (cameras) are owned by
-// warps; a 9x9 block product uses 27 lanes (3 blocks at a time).  Dot
+// One cooperative launch runs the whole solve.  FP64 form (k_pcg): rows
+// (cameras) are owned by warps; a 9x9 block product uses 27 lanes (3 blocks
+// at a time).  The FP32 form (k_pcg32) is described before it.  Dot
 // products are reduced per CTA and then, after a grid barrier, by every CTA
 // in the same fixed order, so all CTAs take identical decisions.  The grid
 // barrier's wait is bounded: after 2 s it sets an error bit and returns.
@@ -476,19 +477,19 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
 // Phase 1 streams the reduced camera system through shared memory with 1-D
 // TMA bulk copies.  The blocks are read in storage order: the diagonal
 // blocks of rows begini.. first, then every off-diagonal block once (upper
-// triangle, row major).  The stream is cut into groups of 32 blocks, and
-// every warp owns a contiguous run of groups (equal counts, so every warp
-// moves the same bytes).  One elected lane copies a group's blocks (32 x
-// 324 B) and their (row, column, slot) triples into the warp's stage,
-// completing on the stage's mbarrier; each lane then owns one block: it forms
-// the block's row product B d_col (summed into its row) and, for an
-// off-diagonal block, the transposed product B^T d_row, which goes to the
-// block's slot of tpart.  The slots are in column order (the blocks of
-// column c, i.e. the transposed entries of row c, are consecutive), and a
-// slot is 64 bytes (9 values, zero padding: two whole sectors, so the
-// scattered writes need no read of the rest of a sector), so that phase 2
-// reads each row's transposed products as one contiguous run.  Lane i reads
-// its block at byte
+// triangle, row major).  The stream is cut into groups of 32 blocks and the
+// groups into chunks of A.chunk groups (fixed boundaries); warps take chunks
+// from a counter, the next one taken a chunk ahead, so a fast warp takes
+// more of them.  One elected lane copies a group's blocks (32 x 324 B) and
+// their (row, column, slot) triples into the warp's stage, completing on the
+// stage's mbarrier; each lane then owns one block: it forms the block's row
+// product B d_col (summed into its row) and, for an off-diagonal block, the
+// transposed product B^T d_row, which goes to the block's slot of tpart.
+// The slots are in column order (the blocks of column c, i.e. the
+// transposed entries of row c, are consecutive), and a slot is 64 bytes (9
+// values, zero padding: two whole sectors, so the scattered writes need no
+// read of the rest of a sector), so that phase 2 reads each row's
+// transposed products as one contiguous run.  Lane i reads its block at byte
 // 324 i of the stage: 81 i is a distinct bank for every lane, so the reads
 // are conflict-free.  The gathered vector is d^k rounded to FP32 (d32, 12
 // floats per camera so that a camera is three aligned 16-byte loads),
@@ -496,16 +497,19 @@ __global__ void __launch_bounds__(pcg_threads<BT>(), 1) k_pcg(PcgArgs A) {
 //
 // Row sums: a diagonal block's product is written to pdiag[row]; the
 // off-diagonal products of a row are summed per group by a segmented warp
-// scan in FP32, then carried across groups in FP64 and written once per
-// (row, warp run): to prow[row] by the warp that holds the row's first block,
-// to pw[warp] by a warp whose run starts inside the row.  Phase 2 adds, per
-// row and in a fixed order, pdiag, prow, the pw of the runs that start inside
-// the row, and the row's run of transposed products (the blocks stored by
-// earlier rows in its column).
+// scan in FP32 (a group inside the open row: per-lane FP64 running sums),
+// carried across groups in FP64 and written once per (row, chunk): to
+// prow[row] by the chunk that holds the row's first block, to pw[chunk] by a
+// chunk that starts inside the row; each chunk's share of d^T A d goes to
+// pdqc[chunk].  Everything a chunk writes depends on the chunk only, not on
+// the warp that took it.  Phase 2 adds, per row and in a fixed order, pdiag,
+// prow, the pw of the chunks that start inside the row, and the row's run of
+// transposed products (the blocks stored by earlier rows in its column).
 //
 // Iteration k: phase D (d^k = h + beta d^(k-1), FP64 and FP32 copies),
 // barrier, phase 1 (A d^k and d^T A d), barrier, phase 2 (as in the FP64
-// form; with the coarse space split in 2a and 2b by one more barrier),
+// form; with the coarse space: 2a, rows taken from a counter, barrier, 2a',
+// the aggregates' restrictions, barrier, 2b, the coarse correction),
 // barrier.
 constexpr int P32_W = 16;  // warps per CTA
 constexpr int P32_T = P32_W * 32;
@@ -1137,7 +1141,6 @@ void pcg_set_smem() {
   cudaFuncSetAttribute(k_pcg32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)P32_SMEM);
 }
 
-int pcg_warps32() { return P32_W; }
 
 // Groups of 32 blocks per phase-1 chunk of the FP32 PCG: small enough that
 // the warps finish together, large enough that the chunk's fixed work (its
