@@ -564,12 +564,28 @@ def main():
         S.close()
         torch.cuda.synchronize()
         same["ours_e2e"] = time.perf_counter() - t0
+        par = cpu_sample_parallel(sblk, sout)
+        if par is not None:
+            # the same branch on the GPU (rpba_calc_plsa_parallel: the partition
+            # steps on host threads, their solves and the merge on the device),
+            # same partition count, partition included; the first run warms up
+            import oracle
+            k = par["partitions"]
+            for _ in range(2):
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                part_g = rb.partition_images(sblk, k)
+                st_p, b_p, s_p, _ = rb.calc_plsa_parallel(sblk, part_g, k)
+                torch.cuda.synchronize()
+                dt_p = time.perf_counter() - t0
+            par.update({"gpu_same_sample_s": dt_p, "gpu_status": st_p, "gpu_outer_iterations": s_p["iterations"],
+                        "gpu_exteval_sigma0": oracle.exteval(b_p)[1]["exteval_sigma0"]})
         cpu = {"value": dt, "unit": UNIT, "cores": 1, "kind": "port",
                "sample": (f"one complete solve of the same scene family at {args.cpu_sample_scale:g} of the "
                           f"workload ({sblk.n_images} cameras, {sblk.n_obs} observations) on one host core"),
                "linear_solves": rep_c["linear_solves"], "final_rms": rep_c["rms"],
                "gpu_same_sample_s": same["ours"], "gpu_plain_fp64_same_sample_s": same["plain_fp64"],
-               "gpu_e2e_same_sample_s": same["ours_e2e"], "parallel": cpu_sample_parallel(sblk, sout)}
+               "gpu_e2e_same_sample_s": same["ours_e2e"], "parallel": par}
 
     if rank == 0:
         r0 = reps[-1]

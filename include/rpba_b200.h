@@ -366,7 +366,9 @@ int32_t rpba_triangulate_parts(const rpba_block *blk, const float *sig0w, const 
  * Outputs: blk (cameras, points, tracks as rpba_get_state), pmat_d_out
  * (12 doubles per image) and point_used (1 for the points the step took),
  * each optional.  FP64 only (RPBA_PREC_FP64; RPBA_SOLVER_PCG with the
- * reference's stop rule, or RPBA_SOLVER_DIRECT). */
+ * reference's stop rule, or RPBA_SOLVER_DIRECT).  Calls from several host
+ * threads may overlap: each has its own device memory and stream, and their
+ * cooperative kernels take turns (one process-wide lock). */
 int32_t rpba_lsa_gcp_step(rpba_block *blk, const rpba_options *opt, const int32_t *gcpinfo, const float *W3,
                           int32_t n_w3, const double *gcpdata, int32_t n_gcp, int32_t ncam_total,
                           const double *pmat_d, double *pmat_d_out, uint8_t *point_used, rpba_report *rep,
@@ -376,7 +378,9 @@ int32_t rpba_lsa_gcp_step(rpba_block *blk, const rpba_options *opt, const int32_
  * 100-510), which the reference takes when min(Threads, iround(images /
  * 70)) > 1.  part[image] in 0 .. nthreads - 1 (rpba_partition_images
  * replaces the reference's METIS cut).  Each outer iteration after the
- * first takes one rpba_lsa_gcp_step per partition and merges with
+ * first takes one rpba_lsa_gcp_step per partition -- concurrently, on host
+ * threads (at most one per core), as the reference's OpenMP loop does; the
+ * result does not depend on their order -- and merges with
  * CalcLSAXMulti on the GPU (robust thresholds when the robust stage starts,
  * robust deletion, weight blocks of the shared points); the best iteration
  * (lowest sigma0) is written back to blk (cameras, points, tracks), as the

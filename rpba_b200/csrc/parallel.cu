@@ -20,18 +20,23 @@
 //   points seen by more than one partition become the next GCPs at their
 //   refined positions;
 // until iflag runs out (the sig0frac rule) or 50 iterations.  The partition
-// steps run one after another: each is a whole-GPU solve.
+// steps of an outer iteration run concurrently on host threads, each on its
+// own handle and stream (their cooperative kernels one at a time: the
+// persistent PCG and the exact sums need every SM); each step's result does
+// not depend on the others, so neither does the loop's.
 //
 // The loop is host code over two steps, the partition step and the merge
 // pass; rpba_calc_plsa_parallel binds them to the GPU (rpba_lsa_gcp_step and
 // the CalcLSAXMulti kernel), rpba_calc_plsa_parallel_hosted takes them from
 // the caller, so that the loop itself can be checked without a GPU.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/rpba_b200.h"
@@ -59,6 +64,10 @@ struct TmpBlock {
   std::vector<float> XX, pmat, K, dist, xg, wx, wy, wxy;
 };
 
+// host threads for the partition steps (the reference runs one OpenMP
+// thread per partition, rpbacore.cpp:219-235; here at most one per core)
+int host_workers() { return (int)std::max(1u, std::thread::hardware_concurrency()); }
+
 // the merge pass on the GPU
 int32_t gpu_merge(const rpba_block *b, const double *Pd, const float *sig0w, int32_t robustmode, int32_t weight_only,
                   const int32_t *part, int32_t nparts, int32_t device, double *XX_out, uint8_t *keep, float *sig0v,
@@ -74,7 +83,7 @@ int32_t gpu_merge(const rpba_block *b, const double *Pd, const float *sig0w, int
 }
 
 int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads, const int32_t *part, char *log,
-                      size_t cap, double *stats, rpba_gcp_step_fn step_fn, rpba_merge_fn merge_fn) {
+                      size_t cap, double *stats, rpba_gcp_step_fn step_fn, rpba_merge_fn merge_fn, int workers) {
   if (!blk || !opt || !part || nthreads < 2 || blk->n_images < 1 || blk->n_points < 0) return RPBA_ERR_ARG;
   const int nrimages = blk->n_images, pxs = blk->n_points, T = nthreads;
   for (int i = 0; i < nrimages; ++i)
@@ -215,7 +224,9 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
       rpba_options ol = *opt;
       ol.robust = 0;
       if (iter < 3) ol.k2 = ol.k4 = ol.f = 0;
-      for (int it = 0; it < T; ++it) {
+      // the step of partition `it`: its log goes to plog, its results to
+      // the partition's own state (PMdd[it], camerasoit[it], pointXXvv[it])
+      auto part_step = [&](int it, std::string &plog) -> int {
         const std::vector<int> &imgs = imgindv[it];
         const int m = (int)imgs.size();
         TmpBlock tb;
@@ -279,7 +290,7 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
         if (st != RPBA_OK && st != RPBA_ERR_NO_OBS_IMAGE && st != RPBA_ERR_LOW_REDUNDANCY &&
             st != RPBA_ERR_NAN_STEP)
           return st;
-        os += lg.data();
+        plog = lg.data();
         // OutputLSAP: PointXXvOut clears the lists of the points that
         // PointXXvIn did not take; the stored cameras and camerasnew
         for (int j = 0; j < np; ++j)
@@ -291,6 +302,32 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
           camerasoit[it][gi].d[0] = tb.dist[2 * li];
           camerasoit[it][gi].d[1] = tb.dist[2 * li + 1];
         }
+        return (int)RPBA_OK;
+      };
+      // the partitions' steps are independent: run them on `workers` host
+      // threads (partitions taken from a counter), then take their logs and
+      // the first failure in partition order, as a sequential loop would
+      std::vector<int> pst(T, RPBA_OK);
+      std::vector<std::string> plogs(T);
+      std::atomic<int> next{0};
+      auto body = [&]() {
+        for (;;) {
+          const int it = next.fetch_add(1);
+          if (it >= T) break;
+          try {
+            pst[it] = part_step(it, plogs[it]);
+          } catch (const std::bad_alloc &) {
+            pst[it] = RPBA_ERR_CUDA;
+          }
+        }
+      };
+      std::vector<std::thread> th;
+      for (int k = 1; k < std::min(workers, T); ++k) th.emplace_back(body);
+      body();
+      for (auto &t : th) t.join();
+      for (int it = 0; it < T; ++it) {
+        if (pst[it] != RPBA_OK) return pst[it];
+        os += plogs[it];
       }
       for (int it = 0; it < T; ++it)
         for (int gi : imgindv[it]) {
@@ -440,12 +477,12 @@ extern "C" int32_t rpba_calc_plsa_parallel(rpba_block *blk, const rpba_options *
   if (opt && (opt->exteval || opt->precision != RPBA_PREC_FP64 ||
               (opt->solver != RPBA_SOLVER_PCG && opt->solver != RPBA_SOLVER_DIRECT)))
     return RPBA_ERR_UNSUPPORTED;
-  return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, rpba_lsa_gcp_step, gpu_merge);
+  return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, rpba_lsa_gcp_step, gpu_merge, host_workers());
 }
 
 extern "C" int32_t rpba_calc_plsa_parallel_hosted(rpba_block *blk, const rpba_options *opt, int32_t nthreads,
                                                   const int32_t *part, char *log, size_t cap, double *stats,
                                                   rpba_gcp_step_fn step, rpba_merge_fn merge) {
   if (!step || !merge) return RPBA_ERR_ARG;
-  return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, step, merge);
+  return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, step, merge, host_workers());
 }

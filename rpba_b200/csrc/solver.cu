@@ -1237,8 +1237,11 @@ int rpba_handle::adjust_gcp_step() {
   PROF("decode", 1, launch_decode(L, L.XPMn, s));
   PROF("cost", 1, launch_cost(L, L.XPMn, true, s));
   launch_gcp_cost(L, L.XPMn, aoterm + 2 * (size_t)np, s);
-  prof.next_bytes = 4. * L.nobs;
-  PROF("seq_sum", 1, launch_exact_sum(L.o_cost, L.nobs, sums, ES, s));
+  {
+    CoopLock lk(this);
+    prof.next_bytes = 4. * L.nobs;
+    PROF("seq_sum", 1, launch_exact_sum(L.o_cost, L.nobs, sums, ES, s));
+  }
   struct {
     float sig0;
     int err;
@@ -1288,6 +1291,9 @@ int guard(int (*fn)(void *), void *arg) {
     return RPBA_ERR_CUDA;
   }
 }
+
+// taken by the cooperative launches of every rpba_lsa_gcp_step in the process
+std::mutex g_gcp_coop;
 
 }  // namespace
 
@@ -2117,6 +2123,10 @@ int32_t rpba_lsa_gcp_step(rpba_block *blk, const rpba_options *opt, const int32_
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= opt->device) return RPBA_ERR_NO_DEVICE;
   rpba_handle *H = new rpba_handle();
+  // the partition steps of one outer iteration run concurrently (the
+  // reference's OpenMP loop, rpbacore.cpp:219-235); their cooperative
+  // kernels take one process-wide lock, as a batch's do
+  H->coop = &g_gcp_coop;
   const GcpSetup gs{gcpinfo, W3, n_w3, gcpdata, n_gcp, ncam_total, pmat_d};
   struct A {
     rpba_handle *H;

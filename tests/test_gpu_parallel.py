@@ -108,3 +108,21 @@ def test_calc_plsa_threads_selects_the_partitioned_branch(oracle_mod):
     assert abs(e_g - e_o) <= 1e-6 * e_o
     st1, log1, _ = rb.CalcPLSA(blk.copy(), threads=1, solver=rb.SOLVER_DIRECT)
     assert st1 == 0 and not log1.startswith("#threads")
+
+
+def test_parallel_loop_is_reproducible():
+    """The partition steps of an outer iteration run concurrently on host
+    threads, each on its own handle and stream, with the reference's PCG as
+    the partition solver (cooperative kernels one at a time); two runs give
+    the same block, statistics and log bit for bit, whichever order the
+    steps ran in."""
+    import rpba_b200 as rb
+    from rpba_b200 import scenes
+    blk = scenes.to_block(scenes.arc_scene(seed=5, n_cams=50, n_pts=8000))
+    part = rb.partition_images(blk, 4)
+    st1, b1, s1, log1 = rb.calc_plsa_parallel(blk, part, 4)
+    st2, b2, s2, log2 = rb.calc_plsa_parallel(blk, part, 4)
+    assert st1 == st2 == 0, log1[-2000:]
+    assert s1 == s2 and log1 == log2
+    for name in ("pmat", "K", "distpara", "XX", "pt_obs_off", "pt_obs_image", "pt_obs_slot"):
+        assert np.array_equal(getattr(b1, name), getattr(b2, name)), name
