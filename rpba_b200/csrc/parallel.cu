@@ -44,8 +44,31 @@
 
 namespace {
 
-struct PObs {
-  int image, slot;
+// observation lists of points (the reference's pointXXv: a list of (image,
+// slot) per point) in CSR form: point p's observations are entries
+// off[p] .. off[p + 1] - 1 of img and slot
+struct Tracks {
+  std::vector<int32_t> off, img, slot;
+  int len(int p) const { return off[p + 1] - off[p]; }
+  void start(int npts) {
+    off.assign(1, 0);
+    off.reserve(npts + 1);
+    img.clear();
+    slot.clear();
+  }
+  void add(int32_t i, int32_t s) {
+    img.push_back(i);
+    slot.push_back(s);
+  }
+  void close_point() { off.push_back((int32_t)img.size()); }
+};
+// a partition's points (the reference's pointXXvv[it] and pindv[it]):
+// global point index, the observations in the partition's images (global
+// image indices), and whether the partition's last step took the point
+struct PartTracks {
+  std::vector<int> pind;
+  Tracks tr;
+  std::vector<uint8_t> used;
 };
 struct PCam {
   float K[9], d[2];
@@ -120,17 +143,22 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
     cameras[i].d[1] = blk->distpara[2 * i + 1];
   }
   cameraps = cameras;
-  std::vector<std::vector<PObs>> pointXXv(pxs), pointXXvold;
-  for (int p = 0; p < pxs; ++p)
+  Tracks pointXXv, pointXXvold;
+  pointXXv.start(pxs);
+  for (int p = 0; p < pxs; ++p) {
     for (int t = blk->pt_obs_off[p]; t < blk->pt_obs_off[p + 1]; ++t)
-      pointXXv[p].push_back({blk->pt_obs_image[t], blk->pt_obs_slot[t]});
+      pointXXv.add(blk->pt_obs_image[t], blk->pt_obs_slot[t]);
+    pointXXv.close_point();
+  }
   pointXXvold = pointXXv;
-  std::vector<std::vector<char>> pitflagsv(pxs);
+  // the lists at the start of the outer iteration (the reference's
+  // pitflagsv, the partitions a point's observations fall in, is taken
+  // from them)
+  Tracks pitlists;
   std::vector<int> gcpinfo(pxs, -1);
   std::vector<std::vector<PCam>> camerasoit(T, cameras);
   std::vector<std::vector<double>> PMdd(T, PMd);
-  std::vector<std::vector<std::vector<PObs>>> pointXXvv(T);
-  std::vector<std::vector<int>> pindv(T);
+  std::vector<PartTracks> pointXXvv(T);
   std::vector<std::vector<int32_t>> gcpinfov(T);
   std::vector<std::vector<float>> W3ijiv(T);
   std::vector<double> gcpdatav;
@@ -158,14 +186,6 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
                    double *sum, long long *redund) {
     TmpBlock tb;
     tb.b = *blk;
-    tb.off.assign(pxs + 1, 0);
-    for (int p = 0; p < pxs; ++p) {
-      for (const PObs &q : pointXXv[p]) {
-        tb.img.push_back(q.image);
-        tb.slot.push_back(q.slot);
-      }
-      tb.off[p + 1] = (int32_t)tb.img.size();
-    }
     tb.XX.resize(3 * (size_t)pxs);
     for (size_t i = 0; i < tb.XX.size(); ++i) tb.XX[i] = (float)XXd[i];
     tb.K.resize(9 * (size_t)nrimages);
@@ -175,13 +195,13 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
       tb.dist[2 * i] = cameraps[i].d[0];
       tb.dist[2 * i + 1] = cameraps[i].d[1];
     }
-    tb.b.pt_obs_off = tb.off.data();
-    tb.b.pt_obs_image = tb.img.data();
-    tb.b.pt_obs_slot = tb.slot.data();
+    tb.b.pt_obs_off = pointXXv.off.data();
+    tb.b.pt_obs_image = pointXXv.img.data();
+    tb.b.pt_obs_slot = pointXXv.slot.data();
     tb.b.XX = tb.XX.data();
     tb.b.K = tb.K.data();
     tb.b.distpara = tb.dist.data();
-    const size_t nt = tb.img.size();
+    const size_t nt = pointXXv.img.size();
     std::vector<double> XXo(3 * (size_t)pxs), s0pt(pxs);
     std::vector<uint8_t> keep(std::max<size_t>(nt, 1)), conv(std::max(pxs, 1));
     std::vector<float> sv(std::max<size_t>(nt, 1));
@@ -191,16 +211,21 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
                       wxy ? w3d.data() : nullptr, s0pt.data(), redpt.data());
     if (status != RPBA_OK) return false;
     if (sig0vv)
-      for (int p = 0; p < pxs; ++p)
-        for (int t = tb.off[p]; t < tb.off[p + 1]; ++t) (*sig0vv)[tb.img[t]].push_back(sv[t]);
+      for (size_t t = 0; t < nt; ++t) (*sig0vv)[pointXXv.img[t]].push_back(sv[t]);
+    // the refined points, and every list without the deleted observations
+    Tracks kept;
+    kept.start(pxs);
+    kept.img.reserve(nt);
+    kept.slot.reserve(nt);
     for (int p = 0; p < pxs; ++p) {
-      if (pointXXv[p].empty()) continue;
-      for (int q = 0; q < 3; ++q) XXd[3 * (size_t)p + q] = XXo[3 * (size_t)p + q];
-      std::vector<PObs> kept;
-      for (int t = tb.off[p]; t < tb.off[p + 1]; ++t)
-        if (keep[t]) kept.push_back(pointXXv[p][t - tb.off[p]]);
-      pointXXv[p] = kept;
+      if (pointXXv.len(p) > 0) {
+        for (int q = 0; q < 3; ++q) XXd[3 * (size_t)p + q] = XXo[3 * (size_t)p + q];
+        for (int t = pointXXv.off[p]; t < pointXXv.off[p + 1]; ++t)
+          if (keep[t]) kept.add(pointXXv.img[t], pointXXv.slot[t]);
+      }
+      kept.close_point();
     }
+    pointXXv = std::move(kept);
     double a = 0.;
     long long r = 0;
     for (int c = 0; c < T; ++c) {
@@ -225,7 +250,8 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
       ol.robust = 0;
       if (iter < 3) ol.k2 = ol.k4 = ol.f = 0;
       // the step of partition `it`: its log goes to plog, its results to
-      // the partition's own state (PMdd[it], camerasoit[it], pointXXvv[it])
+      // the partition's own state (PMdd[it], camerasoit[it],
+      // pointXXvv[it].used)
       auto part_step = [&](int it, std::string &plog) -> int {
         const std::vector<int> &imgs = imgindv[it];
         const int m = (int)imgs.size();
@@ -246,26 +272,23 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
           std::memcpy(&tb.K[9 * (size_t)li], camerasoit[it][g].K, sizeof(float) * 9);
           tb.dist[2 * li] = camerasoit[it][g].d[0];
           tb.dist[2 * li + 1] = camerasoit[it][g].d[1];
-          for (int sl = blk->img_obs_off[g]; sl < blk->img_obs_off[g + 1]; ++sl) {
-            tb.xg.push_back(blk->xg[2 * sl]);
-            tb.xg.push_back(blk->xg[2 * sl + 1]);
-            tb.wx.push_back(blk->wx[sl]);
-            tb.wy.push_back(blk->wy[sl]);
-            tb.wxy.push_back(blk->wxy[sl]);
-          }
+          // the image's observation slots are contiguous in the block
+          const int s0 = blk->img_obs_off[g], s1 = blk->img_obs_off[g + 1];
+          tb.xg.insert(tb.xg.end(), blk->xg + 2 * (size_t)s0, blk->xg + 2 * (size_t)s1);
+          tb.wx.insert(tb.wx.end(), blk->wx + s0, blk->wx + s1);
+          tb.wy.insert(tb.wy.end(), blk->wy + s0, blk->wy + s1);
+          tb.wxy.insert(tb.wxy.end(), blk->wxy + s0, blk->wxy + s1);
           tb.ioff[li + 1] = (int32_t)tb.wx.size();
         }
-        const int np = (int)pindv[it].size();
-        tb.off.assign(np + 1, 0);
+        PartTracks &pt = pointXXvv[it];
+        const int np = (int)pt.pind.size();
+        tb.off = pt.tr.off;  // copies: the step writes its tracks back into the block
+        tb.slot = pt.tr.slot;
+        tb.img.resize(pt.tr.img.size());
+        for (size_t t = 0; t < pt.tr.img.size(); ++t) tb.img[t] = loc[pt.tr.img[t]];
         tb.XX.resize(3 * (size_t)np);
-        for (int j = 0; j < np; ++j) {
-          for (const PObs &q : pointXXvv[it][j]) {
-            tb.img.push_back(loc[q.image]);
-            tb.slot.push_back(q.slot);
-          }
-          tb.off[j + 1] = (int32_t)tb.img.size();
-          for (int c = 0; c < 3; ++c) tb.XX[3 * j + c] = (float)XXd[3 * (size_t)pindv[it][j] + c];
-        }
+        for (int j = 0; j < np; ++j)
+          for (int c = 0; c < 3; ++c) tb.XX[3 * j + c] = (float)XXd[3 * (size_t)pt.pind[j] + c];
         rpba_block &b = tb.b;
         b.n_images = m;
         b.n_points = np;
@@ -293,8 +316,7 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
         plog = lg.data();
         // OutputLSAP: PointXXvOut clears the lists of the points that
         // PointXXvIn did not take; the stored cameras and camerasnew
-        for (int j = 0; j < np; ++j)
-          if (!used[j]) pointXXvv[it][j].clear();
+        pt.used.assign(used.begin(), used.begin() + np);
         for (int li = 0; li < m; ++li) {
           const int gi = imgs[li];
           std::memcpy(&PMdd[it][12 * (size_t)gi], &Pout[12 * (size_t)li], sizeof(double) * 12);
@@ -341,20 +363,36 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
       if (robustflag) sig0frac = 1.02f;
     }
     if (iter > 1) {
-      for (int p = 0; p < pxs; ++p) pointXXv[p].clear();
-      for (int it = 0; it < T; ++it)
-        for (size_t j = 0; j < pindv[it].size(); ++j)
-          for (const PObs &q : pointXXvv[it][j]) pointXXv[pindv[it][j]].push_back(q);
-      for (int p = 0; p < pxs; ++p)
-        if (pointXXv[p].size() < 2) pointXXv[p].clear();
+      // every point's list: its lists in the partitions that took it, in
+      // partition order; lists of fewer than two observations are cleared
+      std::vector<int32_t> cnt(pxs + 1, 0);
+      for (int it = 0; it < T; ++it) {
+        const PartTracks &pt = pointXXvv[it];
+        for (size_t j = 0; j < pt.pind.size(); ++j)
+          if (pt.used[j]) cnt[pt.pind[j]] += pt.tr.len((int)j);
+      }
+      Tracks nl;
+      nl.off.assign(pxs + 1, 0);
+      for (int p = 0; p < pxs; ++p) nl.off[p + 1] = nl.off[p] + (cnt[p] < 2 ? 0 : cnt[p]);
+      nl.img.resize(nl.off[pxs]);
+      nl.slot.resize(nl.off[pxs]);
+      std::vector<int32_t> cur(nl.off.begin(), nl.off.end() - 1);
+      for (int it = 0; it < T; ++it) {
+        const PartTracks &pt = pointXXvv[it];
+        for (size_t j = 0; j < pt.pind.size(); ++j) {
+          const int p = pt.pind[j];
+          if (!pt.used[j] || cnt[p] < 2) continue;
+          for (int t = pt.tr.off[j]; t < pt.tr.off[j + 1]; ++t) {
+            nl.img[cur[p]] = pt.tr.img[t];
+            nl.slot[cur[p]++] = pt.tr.slot[t];
+          }
+        }
+      }
+      pointXXv = std::move(nl);
     } else {
       for (int i = 0; i < nrimages; ++i) cameraps[i] = camerasnew[i] = cameras[i];
     }
-    for (int p = 0; p < pxs; ++p)
-      if (!pointXXv[p].empty()) {
-        pitflagsv[p].assign(T, 0);
-        for (const PObs &q : pointXXv[p]) pitflagsv[p][imgindbv[q.image]] = 1;
-      }
+    pitlists = pointXXv;
     double sum = 0.;
     long long redundancy = 0;
     if (robustflagit) {
@@ -373,9 +411,7 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
     sig0g = sum / (double)(redundancy - nrparimages);
     {
       // the progress line (rpbacore.cpp:377-389; ihw2 = 1 for unit image sizes)
-      long long nrobs = 0;
-      for (int p = 0; p < pxs; ++p) nrobs += (long long)pointXXv[p].size();
-      nrobs *= 2;
+      const long long nrobs = 2 * (long long)pointXXv.img.size();
       const float ihw2 = 1.f;
       os += "IT: " + std::to_string(iter) + " " + std::to_string(iflag) + "  " + fmt_g(std::sqrt(sig0g * ihw2)) + ' ' +
             fmt_g(sig0opt / sig0g) + "  " + fmt_g(sig0g) + " " + std::to_string(redundancy) + " " +
@@ -392,41 +428,61 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
       camerasoit[it] = camerasnew;
       for (int gi : imgindv[it])
         std::memcpy(&PMdd[it][12 * (size_t)gi], &PMd[12 * (size_t)gi], sizeof(double) * 12);
-      pointXXvv[it].clear();
-      pindv[it].clear();
       W3ijiv[it].clear();
     }
     // the next GCPs: points (tracks of 2 or more) seen by more than one partition
+    // (the point chunks beginv[c] .. endv[c] of the reference's threads
+    // cover the points in order)
     int nrgcpnew = 0;
     gcpdatav.clear();
-    for (int c = 0; c < T; ++c)
-      for (int p = beginv[c]; p < endv[c]; ++p) {
-        if (pointXXv[p].size() < 2) continue;
-        int gnum = 0;
-        for (int it = 0; it < T && gnum < 2; ++it) gnum += pitflagsv[p][it];
-        if (gnum > 1) {
-          gcpinfo[p] = nrgcpnew;
-          for (int q = 0; q < 3; ++q) gcpdatav.push_back(XXd[3 * (size_t)p + q]);
-          for (int it = 0; it < T; ++it)
-            if (pitflagsv[p][it])
-              for (int q = 0; q < 6; ++q) W3ijiv[it].push_back(w3d[((size_t)p * T + it) * 6 + q]);
-          ++nrgcpnew;
-        } else {
-          gcpinfo[p] = -1;
+    std::vector<int> seen(T, -1), parts;
+    for (int p = 0; p < pxs; ++p) {
+      if (pointXXv.len(p) < 2) continue;
+      // the partitions the point's observations fell in at the start of
+      // the iteration, in increasing order
+      parts.clear();
+      for (int t = pitlists.off[p]; t < pitlists.off[p + 1]; ++t) {
+        const int it = imgindbv[pitlists.img[t]];
+        if (seen[it] != p) {
+          seen[it] = p;
+          parts.push_back(it);
         }
       }
-    for (int p = 0; p < pxs; ++p) {
-      std::vector<std::vector<PObs>> per(T);
-      for (const PObs &q : pointXXv[p]) per[imgindbv[q.image]].push_back(q);
-      for (int it = 0; it < T; ++it)
-        if (!per[it].empty()) {
-          pointXXvv[it].push_back(per[it]);
-          pindv[it].push_back(p);
-        }
+      if (parts.size() > 1) {
+        std::sort(parts.begin(), parts.end());
+        gcpinfo[p] = nrgcpnew;
+        for (int q = 0; q < 3; ++q) gcpdatav.push_back(XXd[3 * (size_t)p + q]);
+        for (int it : parts)
+          for (int q = 0; q < 6; ++q) W3ijiv[it].push_back(w3d[((size_t)p * T + it) * 6 + q]);
+        ++nrgcpnew;
+      } else {
+        gcpinfo[p] = -1;
+      }
     }
+    // every partition's points, in point order, with their observations in
+    // the partition's images
+    std::vector<int> lastp(T, -1);
     for (int it = 0; it < T; ++it) {
-      gcpinfov[it].resize(pindv[it].size());
-      for (size_t j = 0; j < pindv[it].size(); ++j) gcpinfov[it][j] = gcpinfo[pindv[it][j]];
+      pointXXvv[it].pind.clear();
+      pointXXvv[it].tr.start(0);
+    }
+    for (int p = 0; p < pxs; ++p)
+      for (int t = pointXXv.off[p]; t < pointXXv.off[p + 1]; ++t) {
+        PartTracks &pt = pointXXvv[imgindbv[pointXXv.img[t]]];
+        const int it = imgindbv[pointXXv.img[t]];
+        if (lastp[it] != p) {
+          if (lastp[it] >= 0) pt.tr.close_point();
+          lastp[it] = p;
+          pt.pind.push_back(p);
+        }
+        pt.tr.add(pointXXv.img[t], pointXXv.slot[t]);
+      }
+    for (int it = 0; it < T; ++it) {
+      PartTracks &pt = pointXXvv[it];
+      if (lastp[it] >= 0) pt.tr.close_point();
+      pt.used.assign(pt.pind.size(), 1);
+      gcpinfov[it].resize(pt.pind.size());
+      for (size_t j = 0; j < pt.pind.size(); ++j) gcpinfov[it][j] = gcpinfo[pt.pind[j]];
     }
     if (iter > 1) {
       if (sig0g <= sig0opt) {
@@ -441,16 +497,9 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
     ++iter;
   }
   // pointXXvio = pointXXvold, PMatrices, XX, cameras (rpbacore.cpp:498-507)
-  int32_t t = 0;
-  for (int p = 0; p < pxs; ++p) {
-    blk->pt_obs_off[p] = t;
-    for (const PObs &q : pointXXvold[p]) {
-      blk->pt_obs_image[t] = q.image;
-      blk->pt_obs_slot[t] = q.slot;
-      ++t;
-    }
-  }
-  blk->pt_obs_off[pxs] = t;
+  for (int p = 0; p <= pxs; ++p) blk->pt_obs_off[p] = pointXXvold.off[p];
+  std::copy(pointXXvold.img.begin(), pointXXvold.img.end(), blk->pt_obs_image);
+  std::copy(pointXXvold.slot.begin(), pointXXvold.slot.end(), blk->pt_obs_slot);
   for (size_t i = 0; i < PMdold.size(); ++i) blk->pmat[i] = (float)PMdold[i];
   for (size_t i = 0; i < XXdold.size(); ++i) blk->XX[i] = (float)XXdold[i];
   for (int i = 0; i < nrimages; ++i) {
