@@ -91,6 +91,21 @@ struct TmpBlock {
 // thread per partition, rpbacore.cpp:219-235; here at most one per core)
 int host_workers() { return (int)std::max(1u, std::thread::hardware_concurrency()); }
 
+// f(i) for i in 0 .. n - 1 on up to `workers` host threads, contiguous
+// ranges of i per thread
+template <class F>
+void parallel_for(int n, int workers, F &&f) {
+  const int T = std::max(1, std::min(workers, n / 64));
+  auto body = [&](int k) {
+    const int i1 = (int)((long long)n * (k + 1) / T);
+    for (int i = (int)((long long)n * k / T); i < i1; ++i) f(i);
+  };
+  std::vector<std::thread> th;
+  for (int k = 1; k < T; ++k) th.emplace_back(body, k);
+  body(0);
+  for (auto &t : th) t.join();
+}
+
 // the merge pass on the GPU
 int32_t gpu_merge(const rpba_block *b, const double *Pd, const float *sig0w, int32_t robustmode, int32_t weight_only,
                   const int32_t *part, int32_t nparts, int32_t device, double *XX_out, uint8_t *keep, float *sig0v,
@@ -398,14 +413,15 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
     if (robustflagit) {
       std::vector<std::vector<float>> sig0vvs(nrimages);
       if (!sweep(1, false, false, &sig0vvs, &sum, &redundancy)) return status;
-      for (int i = 0; i < nrimages; ++i) {
+      // every image's median statistic (images dealt to host threads)
+      parallel_for(nrimages, workers, [&](int i) {
         if (sig0vvs[i].empty()) {
           sig0wv[i] = 0.f;
         } else {
           std::sort(sig0vvs[i].begin(), sig0vvs[i].end());
           sig0wv[i] = 1.f / (sig0vvs[i][(int)sig0vvs[i].size() / 2] * 2.1981f);
         }
-      }
+      });
     }
     if (!sweep(robustflagit ? 2 : 0, iter == 1, true, nullptr, &sum, &redundancy)) return status;
     sig0g = sum / (double)(redundancy - nrparimages);
