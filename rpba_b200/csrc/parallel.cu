@@ -91,17 +91,20 @@ struct TmpBlock {
 // thread per partition, rpbacore.cpp:219-235; here at most one per core)
 int host_workers() { return (int)std::max(1u, std::thread::hardware_concurrency()); }
 
-// f(i) for i in 0 .. n - 1 on up to `workers` host threads, contiguous
-// ranges of i per thread
+// Host-side passes over points, observations or partitions run on host
+// threads in W contiguous ranges; where the output is a list in item order,
+// a first pass counts per range and a second writes at the prefix sums, so
+// the result does not depend on W.
+//   nranges: at most `workers` ranges of at least `grain` items
+//   parallel_ranges: f(k, lo, hi) for range k = [n k / W, n (k + 1) / W)
+int nranges(long long n, int workers, int grain) {
+  return (int)std::max(1ll, std::min((long long)workers, n / grain));
+}
 template <class F>
-void parallel_for(int n, int workers, F &&f) {
-  const int T = std::max(1, std::min(workers, n / 64));
-  auto body = [&](int k) {
-    const int i1 = (int)((long long)n * (k + 1) / T);
-    for (int i = (int)((long long)n * k / T); i < i1; ++i) f(i);
-  };
+void parallel_ranges(int n, int W, F &&f) {
+  auto body = [&](int k) { f(k, (int)((long long)n * k / W), (int)((long long)n * (k + 1) / W)); };
   std::vector<std::thread> th;
-  for (int k = 1; k < T; ++k) th.emplace_back(body, k);
+  for (int k = 1; k < W; ++k) th.emplace_back(body, k);
   body(0);
   for (auto &t : th) t.join();
 }
@@ -228,18 +231,36 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
     if (sig0vv)
       for (size_t t = 0; t < nt; ++t) (*sig0vv)[pointXXv.img[t]].push_back(sv[t]);
     // the refined points, and every list without the deleted observations
+    // (point ranges on host threads: the kept observations counted, then
+    // written at the ranges' prefix sums)
+    const int W = nranges(pxs, workers, 4096);
+    std::vector<int32_t> kc(W + 1, 0);
+    parallel_ranges(pxs, W, [&](int k, int p0, int p1) {
+      int32_t c = 0;
+      for (int p = p0; p < p1; ++p)
+        if (pointXXv.len(p) > 0)
+          for (int t = pointXXv.off[p]; t < pointXXv.off[p + 1]; ++t) c += keep[t] ? 1 : 0;
+      kc[k + 1] = c;
+    });
+    for (int k = 0; k < W; ++k) kc[k + 1] += kc[k];
     Tracks kept;
-    kept.start(pxs);
-    kept.img.reserve(nt);
-    kept.slot.reserve(nt);
-    for (int p = 0; p < pxs; ++p) {
-      if (pointXXv.len(p) > 0) {
+    kept.off.resize(pxs + 1);
+    kept.img.resize(kc[W]);
+    kept.slot.resize(kc[W]);
+    parallel_ranges(pxs, W, [&](int k, int p0, int p1) {
+      int32_t o = kc[k];
+      for (int p = p0; p < p1; ++p) {
+        kept.off[p] = o;
+        if (pointXXv.len(p) == 0) continue;
         for (int q = 0; q < 3; ++q) XXd[3 * (size_t)p + q] = XXo[3 * (size_t)p + q];
         for (int t = pointXXv.off[p]; t < pointXXv.off[p + 1]; ++t)
-          if (keep[t]) kept.add(pointXXv.img[t], pointXXv.slot[t]);
+          if (keep[t]) {
+            kept.img[o] = pointXXv.img[t];
+            kept.slot[o++] = pointXXv.slot[t];
+          }
       }
-      kept.close_point();
-    }
+    });
+    kept.off[pxs] = kc[W];
     pointXXv = std::move(kept);
     double a = 0.;
     long long r = 0;
@@ -380,29 +401,38 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
     if (iter > 1) {
       // every point's list: its lists in the partitions that took it, in
       // partition order; lists of fewer than two observations are cleared
+      // (each partition list's place in its point's list is counted in
+      // partition order; the lists are then copied by partitions on host
+      // threads)
       std::vector<int32_t> cnt(pxs + 1, 0);
+      std::vector<std::vector<int32_t>> dst(T);
       for (int it = 0; it < T; ++it) {
         const PartTracks &pt = pointXXvv[it];
-        for (size_t j = 0; j < pt.pind.size(); ++j)
+        dst[it].resize(pt.pind.size());
+        for (size_t j = 0; j < pt.pind.size(); ++j) {
+          dst[it][j] = cnt[pt.pind[j]];
           if (pt.used[j]) cnt[pt.pind[j]] += pt.tr.len((int)j);
+        }
       }
       Tracks nl;
       nl.off.assign(pxs + 1, 0);
       for (int p = 0; p < pxs; ++p) nl.off[p + 1] = nl.off[p] + (cnt[p] < 2 ? 0 : cnt[p]);
       nl.img.resize(nl.off[pxs]);
       nl.slot.resize(nl.off[pxs]);
-      std::vector<int32_t> cur(nl.off.begin(), nl.off.end() - 1);
-      for (int it = 0; it < T; ++it) {
-        const PartTracks &pt = pointXXvv[it];
-        for (size_t j = 0; j < pt.pind.size(); ++j) {
-          const int p = pt.pind[j];
-          if (!pt.used[j] || cnt[p] < 2) continue;
-          for (int t = pt.tr.off[j]; t < pt.tr.off[j + 1]; ++t) {
-            nl.img[cur[p]] = pt.tr.img[t];
-            nl.slot[cur[p]++] = pt.tr.slot[t];
+      parallel_ranges(T, nranges(T, workers, 1), [&](int, int i0, int i1) {
+        for (int it = i0; it < i1; ++it) {
+          const PartTracks &pt = pointXXvv[it];
+          for (size_t j = 0; j < pt.pind.size(); ++j) {
+            const int p = pt.pind[j];
+            if (!pt.used[j] || cnt[p] < 2) continue;
+            int32_t o = nl.off[p] + dst[it][j];
+            for (int t = pt.tr.off[j]; t < pt.tr.off[j + 1]; ++t, ++o) {
+              nl.img[o] = pt.tr.img[t];
+              nl.slot[o] = pt.tr.slot[t];
+            }
           }
         }
-      }
+      });
       pointXXv = std::move(nl);
     } else {
       for (int i = 0; i < nrimages; ++i) cameraps[i] = camerasnew[i] = cameras[i];
@@ -413,13 +443,15 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
     if (robustflagit) {
       std::vector<std::vector<float>> sig0vvs(nrimages);
       if (!sweep(1, false, false, &sig0vvs, &sum, &redundancy)) return status;
-      // every image's median statistic (images dealt to host threads)
-      parallel_for(nrimages, workers, [&](int i) {
-        if (sig0vvs[i].empty()) {
-          sig0wv[i] = 0.f;
-        } else {
-          std::sort(sig0vvs[i].begin(), sig0vvs[i].end());
-          sig0wv[i] = 1.f / (sig0vvs[i][(int)sig0vvs[i].size() / 2] * 2.1981f);
+      // every image's median statistic (images on host threads)
+      parallel_ranges(nrimages, nranges(nrimages, workers, 16), [&](int, int i0, int i1) {
+        for (int i = i0; i < i1; ++i) {
+          if (sig0vvs[i].empty()) {
+            sig0wv[i] = 0.f;
+          } else {
+            std::sort(sig0vvs[i].begin(), sig0vvs[i].end());
+            sig0wv[i] = 1.f / (sig0vvs[i][(int)sig0vvs[i].size() / 2] * 2.1981f);
+          }
         }
       });
     }
@@ -448,54 +480,124 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
     }
     // the next GCPs: points (tracks of 2 or more) seen by more than one partition
     // (the point chunks beginv[c] .. endv[c] of the reference's threads
-    // cover the points in order)
-    int nrgcpnew = 0;
-    gcpdatav.clear();
-    std::vector<int> seen(T, -1), parts;
-    for (int p = 0; p < pxs; ++p) {
-      if (pointXXv.len(p) < 2) continue;
-      // the partitions the point's observations fell in at the start of
-      // the iteration, in increasing order
-      parts.clear();
-      for (int t = pitlists.off[p]; t < pitlists.off[p + 1]; ++t) {
-        const int it = imgindbv[pitlists.img[t]];
-        if (seen[it] != p) {
-          seen[it] = p;
-          parts.push_back(it);
+    // cover the points in order).  Point ranges on host threads: a point
+    // with a list of two or more observations whose observations fell in
+    // two or more partitions at the start of the iteration becomes GCP
+    // number g (in point order) and adds its weight block for each of
+    // those partitions to the partition's W3 rows (in point order); the
+    // other points with such lists get -1.  First pass: the counts per
+    // range; second: the entries at the ranges' prefix sums.
+    {
+      const int W = nranges(pxs, workers, 4096);
+      std::vector<int8_t> isg(pxs, -1);
+      std::vector<int32_t> ng(W + 1, 0), nw((size_t)(W + 1) * T, 0);
+      // the distinct partitions of the point's start-of-iteration list
+      auto parts_of = [&](int p, std::vector<int> &seen, std::vector<int> &parts) {
+        parts.clear();
+        for (int t = pitlists.off[p]; t < pitlists.off[p + 1]; ++t) {
+          const int it = imgindbv[pitlists.img[t]];
+          if (seen[it] != p) {
+            seen[it] = p;
+            parts.push_back(it);
+          }
         }
+      };
+      parallel_ranges(pxs, W, [&](int k, int p0, int p1) {
+        std::vector<int> seen(T, -1), parts;
+        std::vector<int32_t> w(T, 0);  // counted locally: the ranges' counts share cache lines
+        int32_t g = 0;
+        for (int p = p0; p < p1; ++p) {
+          if (pointXXv.len(p) < 2) continue;
+          parts_of(p, seen, parts);
+          isg[p] = parts.size() > 1 ? 1 : 0;
+          if (!isg[p]) continue;
+          ++g;
+          for (int it : parts) ++w[it];
+        }
+        ng[k + 1] = g;
+        std::copy(w.begin(), w.end(), nw.begin() + (size_t)(k + 1) * T);
+      });
+      for (int k = 0; k < W; ++k) {
+        ng[k + 1] += ng[k];
+        for (int it = 0; it < T; ++it) nw[(size_t)(k + 1) * T + it] += nw[(size_t)k * T + it];
       }
-      if (parts.size() > 1) {
-        std::sort(parts.begin(), parts.end());
-        gcpinfo[p] = nrgcpnew;
-        for (int q = 0; q < 3; ++q) gcpdatav.push_back(XXd[3 * (size_t)p + q]);
-        for (int it : parts)
-          for (int q = 0; q < 6; ++q) W3ijiv[it].push_back(w3d[((size_t)p * T + it) * 6 + q]);
-        ++nrgcpnew;
-      } else {
-        gcpinfo[p] = -1;
-      }
+      gcpdatav.assign(3 * (size_t)ng[W], 0.);
+      for (int it = 0; it < T; ++it) W3ijiv[it].assign(6 * (size_t)nw[(size_t)W * T + it], 0.f);
+      parallel_ranges(pxs, W, [&](int k, int p0, int p1) {
+        std::vector<int> seen(T, -1), parts;
+        std::vector<int32_t> wp(nw.begin() + (size_t)k * T, nw.begin() + (size_t)(k + 1) * T);
+        int32_t g = ng[k];
+        for (int p = p0; p < p1; ++p) {
+          if (isg[p] < 0) continue;
+          if (!isg[p]) {
+            gcpinfo[p] = -1;
+            continue;
+          }
+          gcpinfo[p] = g;
+          for (int q = 0; q < 3; ++q) gcpdatav[3 * (size_t)g + q] = XXd[3 * (size_t)p + q];
+          parts_of(p, seen, parts);
+          for (int it : parts)
+            std::memcpy(&W3ijiv[it][6 * (size_t)wp[it]++], &w3d[((size_t)p * T + it) * 6], sizeof(float) * 6);
+          ++g;
+        }
+      });
     }
     // every partition's points, in point order, with their observations in
-    // the partition's images
-    std::vector<int> lastp(T, -1);
-    for (int it = 0; it < T; ++it) {
-      pointXXvv[it].pind.clear();
-      pointXXvv[it].tr.start(0);
-    }
-    for (int p = 0; p < pxs; ++p)
-      for (int t = pointXXv.off[p]; t < pointXXv.off[p + 1]; ++t) {
-        PartTracks &pt = pointXXvv[imgindbv[pointXXv.img[t]]];
-        const int it = imgindbv[pointXXv.img[t]];
-        if (lastp[it] != p) {
-          if (lastp[it] >= 0) pt.tr.close_point();
-          lastp[it] = p;
-          pt.pind.push_back(p);
+    // the partition's images (point ranges on host threads: points and
+    // observations counted per range and partition, then written at the
+    // prefix sums)
+    {
+      const int W = nranges(pxs, workers, 4096);
+      std::vector<int32_t> cp((size_t)(W + 1) * T, 0), co((size_t)(W + 1) * T, 0);
+      parallel_ranges(pxs, W, [&](int k, int p0, int p1) {
+        std::vector<int> lastp(T, -1);
+        std::vector<int32_t> np_(T, 0), no_(T, 0);  // counted locally, as above
+        for (int p = p0; p < p1; ++p)
+          for (int t = pointXXv.off[p]; t < pointXXv.off[p + 1]; ++t) {
+            const int it = imgindbv[pointXXv.img[t]];
+            if (lastp[it] != p) {
+              lastp[it] = p;
+              ++np_[it];
+            }
+            ++no_[it];
+          }
+        std::copy(np_.begin(), np_.end(), cp.begin() + (size_t)(k + 1) * T);
+        std::copy(no_.begin(), no_.end(), co.begin() + (size_t)(k + 1) * T);
+      });
+      for (int k = 0; k < W; ++k)
+        for (int it = 0; it < T; ++it) {
+          cp[(size_t)(k + 1) * T + it] += cp[(size_t)k * T + it];
+          co[(size_t)(k + 1) * T + it] += co[(size_t)k * T + it];
         }
-        pt.tr.add(pointXXv.img[t], pointXXv.slot[t]);
+      for (int it = 0; it < T; ++it) {
+        PartTracks &pt = pointXXvv[it];
+        const int32_t npt = cp[(size_t)W * T + it], nob = co[(size_t)W * T + it];
+        pt.pind.resize(npt);
+        pt.tr.off.resize(npt + 1);
+        pt.tr.off[npt] = nob;
+        pt.tr.img.resize(nob);
+        pt.tr.slot.resize(nob);
       }
+      parallel_ranges(pxs, W, [&](int k, int p0, int p1) {
+        std::vector<int> lastp(T, -1);
+        std::vector<int32_t> pp(cp.begin() + (size_t)k * T, cp.begin() + (size_t)(k + 1) * T);
+        std::vector<int32_t> oo(co.begin() + (size_t)k * T, co.begin() + (size_t)(k + 1) * T);
+        for (int p = p0; p < p1; ++p)
+          for (int t = pointXXv.off[p]; t < pointXXv.off[p + 1]; ++t) {
+            const int it = imgindbv[pointXXv.img[t]];
+            PartTracks &pt = pointXXvv[it];
+            if (lastp[it] != p) {
+              lastp[it] = p;
+              pt.pind[pp[it]] = p;
+              pt.tr.off[pp[it]++] = oo[it];
+            }
+            pt.tr.img[oo[it]] = pointXXv.img[t];
+            pt.tr.slot[oo[it]++] = pointXXv.slot[t];
+          }
+      });
+    }
     for (int it = 0; it < T; ++it) {
       PartTracks &pt = pointXXvv[it];
-      if (lastp[it] >= 0) pt.tr.close_point();
       pt.used.assign(pt.pind.size(), 1);
       gcpinfov[it].resize(pt.pind.size());
       for (size_t j = 0; j < pt.pind.size(); ++j) gcpinfov[it][j] = gcpinfo[pt.pind[j]];
