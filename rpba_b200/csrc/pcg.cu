@@ -536,8 +536,8 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned 
       : "memory");
   return ok != 0;
 }
-// global -> shared bulk copy completing on `bar` (this CTA's own shared
-// memory; the source is this GPU's memory; no multicast)
+// global -> shared bulk copy completing on `bar` (one destination: this
+// CTA's own shared memory; the source is this GPU's own memory)
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
   asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
                    smem_u32(dst)),
