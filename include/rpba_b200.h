@@ -57,7 +57,8 @@ typedef enum rpba_status {
   RPBA_ERR_UNSUPPORTED = 8,     /* input the GPU path does not accept       */
   RPBA_ERR_NO_DEVICE = 9,       /* no CUDA device / library not usable      */
   RPBA_ERR_SOLVER = 10,         /* direct factorisation failed (not SPD)    */
-  RPBA_ERR_TOO_LARGE = 11       /* input exceeds a fixed-size scratch area  */
+  RPBA_ERR_TOO_LARGE = 11,      /* input exceeds a fixed-size scratch area  */
+  RPBA_ERR_COMM = 12            /* a collective between ranks failed        */
 } rpba_status;
 
 typedef struct rpba_block {
@@ -409,6 +410,36 @@ typedef int32_t (*rpba_merge_fn)(const rpba_block *b, const double *Pd, const fl
 int32_t rpba_calc_plsa_parallel_hosted(rpba_block *blk, const rpba_options *opt, int32_t nthreads,
                                        const int32_t *part, char *log, size_t cap, double *stats,
                                        rpba_gcp_step_fn step, rpba_merge_fn merge);
+
+/* All-gather between the ranks of a multi-rank call: every rank passes
+ * `bytes` bytes (the same count on every rank) and receives every rank's,
+ * in rank order, at recv (world x bytes); returns 0 on success.  Every rank
+ * calls it the same number of times.  The caller supplies it (over
+ * torch.distributed, MPI, ...): the library has no transport of its own. */
+typedef int32_t (*rpba_allgather_fn)(void *ctx, const void *send, uint64_t bytes, void *recv);
+
+/* rpba_calc_plsa_parallel over several ranks (one process per GPU; this
+ * rank's GPU is opt->device): one scene, its partitions dealt to the ranks
+ * (largest first to the least-loaded rank).  Every rank holds the whole
+ * block and runs the whole loop: the partition steps of its own partitions
+ * on its GPU, then, after each round of steps, two all-gathers (the sizes,
+ * then the steps' results: status, log, the partitions' cameras, which
+ * points each step took), after which every rank merges all points on its
+ * GPU and takes the same decisions.  Every rank ends with the same block,
+ * log and stats, equal to the one-rank call's.  A failed all-gather returns
+ * RPBA_ERR_COMM (on every rank whose collective failed); a partition step's
+ * failure is returned by every rank, after the exchange that reports it.
+ * Like the reference's partitioned branch (rpbacore.cpp:100-510), with its
+ * OpenMP threads replaced by ranks and threads; no single counterpart. */
+int32_t rpba_calc_plsa_parallel_ranks(rpba_block *blk, const rpba_options *opt, int32_t nthreads,
+                                      const int32_t *part, char *log, size_t cap, double *stats, int32_t rank,
+                                      int32_t world, rpba_allgather_fn allgather, void *ctx);
+/* The same with both steps supplied by the caller (the host-side check of
+ * the multi-rank loop); no counterpart in the reference. */
+int32_t rpba_calc_plsa_parallel_ranks_hosted(rpba_block *blk, const rpba_options *opt, int32_t nthreads,
+                                             const int32_t *part, char *log, size_t cap, double *stats,
+                                             rpba_gcp_step_fn step, rpba_merge_fn merge, int32_t rank,
+                                             int32_t world, rpba_allgather_fn allgather, void *ctx);
 
 /* Camera partition of the reference's parallel RPBA: replaces
  * PartitionpointXXv (rpbacore.cpp:945-1037), which cuts the images'

@@ -123,9 +123,51 @@ int32_t gpu_merge(const rpba_block *b, const double *Pd, const float *sig0w, int
                                 red_pt);
 }
 
+// Ranks of a multi-rank loop (one process per GPU): every rank holds the
+// whole scene and keeps the whole loop state; it runs the partition steps
+// of the partitions it owns, and after each round of steps the ranks
+// exchange the steps' results through `ag` (an all-gather supplied by the
+// caller), so that every rank continues from the same state.  ag null: one
+// rank, no exchange.
+struct Ranks {
+  int rank = 0, world = 1;
+  rpba_allgather_fn ag = nullptr;
+  void *ctx = nullptr;
+};
+
+// byte records of the exchange
+void put(std::vector<uint8_t> &b, const void *p, size_t n) {
+  const uint8_t *c = (const uint8_t *)p;
+  b.insert(b.end(), c, c + n);
+}
+template <class V>
+void put_v(std::vector<uint8_t> &b, const V &v) {
+  put(b, &v, sizeof v);
+}
+struct Reader {
+  const uint8_t *p, *end;
+  bool ok = true;
+  void get(void *d, size_t n) {
+    if ((size_t)(end - p) < n) {
+      ok = false;
+      return;
+    }
+    std::memcpy(d, p, n);
+    p += n;
+  }
+  template <class V>
+  V get_v() {
+    V v{};
+    get(&v, sizeof v);
+    return v;
+  }
+};
+
 int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads, const int32_t *part, char *log,
-                      size_t cap, double *stats, rpba_gcp_step_fn step_fn, rpba_merge_fn merge_fn, int workers) {
+                      size_t cap, double *stats, rpba_gcp_step_fn step_fn, rpba_merge_fn merge_fn, int workers,
+                      const Ranks &rk = Ranks()) {
   if (!blk || !opt || !part || nthreads < 2 || blk->n_images < 1 || blk->n_points < 0) return RPBA_ERR_ARG;
+  if (rk.world < 1 || rk.rank < 0 || rk.rank >= rk.world || (rk.world > 1 && !rk.ag)) return RPBA_ERR_ARG;
   const int nrimages = blk->n_images, pxs = blk->n_points, T = nthreads;
   for (int i = 0; i < nrimages; ++i)
     if (part[i] < 0 || part[i] >= T) return RPBA_ERR_ARG;
@@ -141,6 +183,22 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
   }
   for (int it = 0; it < T; ++it)
     if (imgindv[it].empty()) return RPBA_ERR_ARG;
+  // the owner rank of every partition: largest (observation slots) first to
+  // the least-loaded rank, ties to the lower index and rank -- the same on
+  // every rank
+  std::vector<int> owner(T, 0);
+  {
+    std::vector<long long> cost(T, 0), load(rk.world, 0);
+    for (int i = 0; i < nrimages; ++i) cost[part[i]] += blk->img_obs_off[i + 1] - blk->img_obs_off[i];
+    std::vector<int> order(T);
+    for (int it = 0; it < T; ++it) order[it] = it;
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    for (int it : order) {
+      const int r = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+      owner[it] = r;
+      load[r] += cost[it];
+    }
+  }
   for (int p = 0; p < pxs; ++p)
     for (int t = blk->pt_obs_off[p]; t < blk->pt_obs_off[p + 1]; ++t) {
       const int im = blk->pt_obs_image[t];
@@ -362,16 +420,20 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
         }
         return (int)RPBA_OK;
       };
-      // the partitions' steps are independent: run them on `workers` host
-      // threads (partitions taken from a counter), then take their logs and
-      // the first failure in partition order, as a sequential loop would
-      std::vector<int> pst(T, RPBA_OK);
+      // the partitions' steps are independent: run this rank's on `workers`
+      // host threads (partitions taken from a counter), exchange the results
+      // between ranks, then take the logs and the first failure in
+      // partition order, as a sequential loop would
+      std::vector<int> pst(T, RPBA_OK), mine;
+      for (int it = 0; it < T; ++it)
+        if (owner[it] == rk.rank) mine.push_back(it);
       std::vector<std::string> plogs(T);
       std::atomic<int> next{0};
       auto body = [&]() {
         for (;;) {
-          const int it = next.fetch_add(1);
-          if (it >= T) break;
+          const int q = next.fetch_add(1);
+          if (q >= (int)mine.size()) break;
+          const int it = mine[q];
           try {
             pst[it] = part_step(it, plogs[it]);
           } catch (const std::bad_alloc &) {
@@ -380,9 +442,55 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
         }
       };
       std::vector<std::thread> th;
-      for (int k = 1; k < std::min(workers, T); ++k) th.emplace_back(body);
+      for (int k = 1; k < std::min(workers, (int)mine.size()); ++k) th.emplace_back(body);
       body();
       for (auto &t : th) t.join();
+      if (rk.ag) {
+        // this rank's partitions: status, log, cameras (double matrices,
+        // intrinsics) of their images, and which of their points the step
+        // took
+        std::vector<uint8_t> pay;
+        for (int it : mine) {
+          put_v(pay, (int32_t)it);
+          put_v(pay, (int32_t)pst[it]);
+          put_v(pay, (uint64_t)plogs[it].size());
+          put(pay, plogs[it].data(), plogs[it].size());
+          for (int gi : imgindv[it]) {
+            put(pay, &PMdd[it][12 * (size_t)gi], sizeof(double) * 12);
+            put_v(pay, camerasoit[it][gi]);
+          }
+          const std::vector<uint8_t> &u = pointXXvv[it].used;
+          put_v(pay, (uint64_t)u.size());
+          put(pay, u.data(), u.size());
+        }
+        // sizes first, then the records padded to the largest
+        const uint64_t sz = pay.size();
+        std::vector<uint64_t> szs(rk.world);
+        if (rk.ag(rk.ctx, &sz, sizeof sz, szs.data()) != 0) return RPBA_ERR_COMM;
+        const uint64_t mx = std::max<uint64_t>(1, *std::max_element(szs.begin(), szs.end()));
+        pay.resize(mx);
+        std::vector<uint8_t> all(mx * rk.world);
+        if (rk.ag(rk.ctx, pay.data(), mx, all.data()) != 0) return RPBA_ERR_COMM;
+        for (int r = 0; r < rk.world; ++r) {
+          if (r == rk.rank) continue;
+          Reader rd{all.data() + mx * r, all.data() + mx * r + szs[r]};
+          while (rd.ok && rd.p < rd.end) {
+            const int it = rd.get_v<int32_t>();
+            if (!rd.ok || it < 0 || it >= T || owner[it] != r) return RPBA_ERR_COMM;
+            pst[it] = rd.get_v<int32_t>();
+            plogs[it].resize(rd.get_v<uint64_t>());
+            rd.get(&plogs[it][0], plogs[it].size());
+            for (int gi : imgindv[it]) {
+              rd.get(&PMdd[it][12 * (size_t)gi], sizeof(double) * 12);
+              camerasoit[it][gi] = rd.get_v<PCam>();
+            }
+            std::vector<uint8_t> &u = pointXXvv[it].used;
+            if (rd.get_v<uint64_t>() != u.size()) return RPBA_ERR_COMM;
+            rd.get(u.data(), u.size());
+          }
+          if (!rd.ok) return RPBA_ERR_COMM;
+        }
+      }
       for (int it = 0; it < T; ++it) {
         if (pst[it] != RPBA_OK) return pst[it];
         os += plogs[it];
@@ -652,4 +760,34 @@ extern "C" int32_t rpba_calc_plsa_parallel_hosted(rpba_block *blk, const rpba_op
                                                   rpba_gcp_step_fn step, rpba_merge_fn merge) {
   if (!step || !merge) return RPBA_ERR_ARG;
   return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, step, merge, host_workers());
+}
+
+extern "C" int32_t rpba_calc_plsa_parallel_ranks(rpba_block *blk, const rpba_options *opt, int32_t nthreads,
+                                                 const int32_t *part, char *log, size_t cap, double *stats,
+                                                 int32_t rank, int32_t world, rpba_allgather_fn allgather,
+                                                 void *ctx) {
+  if (opt && (opt->exteval || opt->precision != RPBA_PREC_FP64 ||
+              (opt->solver != RPBA_SOLVER_PCG && opt->solver != RPBA_SOLVER_DIRECT)))
+    return RPBA_ERR_UNSUPPORTED;
+  if (!allgather) return RPBA_ERR_ARG;
+  Ranks rk;
+  rk.rank = rank;
+  rk.world = world;
+  rk.ag = allgather;
+  rk.ctx = ctx;
+  return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, rpba_lsa_gcp_step, gpu_merge, host_workers(), rk);
+}
+
+extern "C" int32_t rpba_calc_plsa_parallel_ranks_hosted(rpba_block *blk, const rpba_options *opt,
+                                                        int32_t nthreads, const int32_t *part, char *log,
+                                                        size_t cap, double *stats, rpba_gcp_step_fn step,
+                                                        rpba_merge_fn merge, int32_t rank, int32_t world,
+                                                        rpba_allgather_fn allgather, void *ctx) {
+  if (!step || !merge || !allgather) return RPBA_ERR_ARG;
+  Ranks rk;
+  rk.rank = rank;
+  rk.world = world;
+  rk.ag = allgather;
+  rk.ctx = ctx;
+  return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, step, merge, host_workers(), rk);
 }

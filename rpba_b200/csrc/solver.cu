@@ -1313,6 +1313,7 @@ const char *rpba_status_string(int32_t st) {
     case RPBA_ERR_NO_DEVICE: return "no CUDA device";
     case RPBA_ERR_SOLVER: return "direct solve failed";
     case RPBA_ERR_TOO_LARGE: return "input exceeds the fixed scratch of an allocation-free call";
+    case RPBA_ERR_COMM: return "a collective between ranks failed";
     default: return "unknown status";
   }
 }

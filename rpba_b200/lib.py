@@ -31,7 +31,7 @@ LIB_PATH = os.path.join(_HERE, "librpba_b200.so")
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "no observations in image",
           4: "low redundancy", 5: "NaN step", 6: "device timeout", 7: "I/O error",
           8: "unsupported input", 9: "no CUDA device", 10: "direct solve failed",
-          11: "input too large for an allocation-free call"}
+          11: "input too large for an allocation-free call", 12: "a collective between ranks failed"}
 
 # Every entry point include/rpba_b200.h declares.
 EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block_free",
@@ -40,11 +40,36 @@ EXPORTS = ("rpba_status_string", "rpba_version", "rpba_input_block", "rpba_block
            "rpba_float_sequential_sum_noalloc", "rpba_train_preconditioner",
            "rpba_set_preconditioner", "rpba_precond_loss_grad", "rpba_record_systems", "rpba_solve_batch",
            "rpba_triangulate", "rpba_triangulate_parts", "rpba_partition_images", "rpba_lsa_gcp_step",
-           "rpba_calc_plsa_parallel", "rpba_calc_plsa_parallel_hosted", "rpba_debug_barrier_timeout",
+           "rpba_calc_plsa_parallel", "rpba_calc_plsa_parallel_hosted", "rpba_calc_plsa_parallel_ranks",
+           "rpba_calc_plsa_parallel_ranks_hosted", "rpba_debug_barrier_timeout",
            "rpba_partition_count", "rpba_spd_inverse",
            "rpba_destroy")
 
 _lib = None
+
+# rpba_allgather_fn: (ctx, send, bytes, recv) -> 0 on success
+AllgatherFn = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p)
+
+
+def allgather_callback(gather, world: int) -> AllgatherFn:
+    """An rpba_allgather_fn over a Python all-gather ``gather(data: bytes)
+    -> bytes`` that returns every rank's bytes concatenated in rank order.
+    A failure (an exception, or a result of the wrong length) returns 1 to
+    the library, which ends the call with status 12 (keep the returned
+    object alive for the call)."""
+
+    def cb(ctx, send, n, recv):
+        try:
+            out = gather(C.string_at(send, n) if n else b"")
+            if len(out) != world * n:
+                return 1
+            if out:
+                C.memmove(recv, out, len(out))
+            return 0
+        except Exception:
+            return 1
+
+    return AllgatherFn(cb)
 
 
 class RpbaError(RuntimeError):
@@ -118,6 +143,14 @@ def load():
     L.rpba_calc_plsa_parallel_hosted.argtypes = [bp, op, C.c_int32, C.POINTER(C.c_int32), C.c_char_p, C.c_size_t,
                                                  C.POINTER(C.c_double), C.c_void_p, C.c_void_p]
     L.rpba_calc_plsa_parallel_hosted.restype = C.c_int32
+    L.rpba_calc_plsa_parallel_ranks.argtypes = [bp, op, C.c_int32, C.POINTER(C.c_int32), C.c_char_p, C.c_size_t,
+                                                C.POINTER(C.c_double), C.c_int32, C.c_int32, AllgatherFn,
+                                                C.c_void_p]
+    L.rpba_calc_plsa_parallel_ranks.restype = C.c_int32
+    L.rpba_calc_plsa_parallel_ranks_hosted.argtypes = [bp, op, C.c_int32, C.POINTER(C.c_int32), C.c_char_p,
+                                                       C.c_size_t, C.POINTER(C.c_double), C.c_void_p, C.c_void_p,
+                                                       C.c_int32, C.c_int32, AllgatherFn, C.c_void_p]
+    L.rpba_calc_plsa_parallel_ranks_hosted.restype = C.c_int32
     L.rpba_triangulate.argtypes = [bp, C.POINTER(C.c_float), C.POINTER(RpbaTriOptionsC), C.POINTER(C.c_double),
                                    C.POINTER(C.c_uint8), C.POINTER(C.c_float), C.POINTER(C.c_uint8),
                                    C.POINTER(C.c_double), C.POINTER(C.c_int64)]
@@ -216,6 +249,36 @@ def calc_plsa_parallel(block: Block, part, nthreads: int, robust: bool = True, a
     st = load().rpba_calc_plsa_parallel(C.byref(cb), C.byref(o), int(nthreads),
                                         pt.ctypes.data_as(C.POINTER(C.c_int32)), buf, log_cap,
                                         stats.ctypes.data_as(C.POINTER(C.c_double)))
+    n = int(b.pt_obs_off[-1])
+    b.pt_obs_image = b.pt_obs_image[:n].copy()
+    b.pt_obs_slot = b.pt_obs_slot[:n].copy()
+    return st, b, {"sig0opt": float(stats[0]), "iterations": int(stats[1])}, buf.value.decode()
+
+
+def calc_plsa_parallel_ranks(block: Block, part, nthreads: int, rank: int, world: int, gather,
+                             robust: bool = True, addflags=(True, True, True), solver: int = SOLVER_PCG,
+                             device: int = 0, log_cap: int = 1 << 20, steps=None):
+    """The parallel RPBA over ranks (rpba_calc_plsa_parallel_ranks) on a copy
+    of ``block``: this rank runs its partitions' steps on ``device``;
+    ``gather(data: bytes) -> bytes`` is the all-gather between the ranks
+    (``replicas.bytes_allgather`` over torch.distributed).  ``steps``:
+    (step, merge) C function pointers to run the hosted form instead (the
+    host-side check binds the oracle's).  Returns what calc_plsa_parallel
+    returns; every rank gets the same."""
+    b = block.copy()
+    cb = b.as_c()
+    o = make_options(robust=robust, k2=addflags[0], k4=addflags[1], f=addflags[2], solver=solver,
+                     precision=PREC_FP64, device=device)
+    pt = np.ascontiguousarray(part, np.int32)
+    stats = np.zeros(2)
+    buf = C.create_string_buffer(log_cap)
+    ag = allgather_callback(gather, world)
+    args = (C.byref(cb), C.byref(o), int(nthreads), pt.ctypes.data_as(C.POINTER(C.c_int32)), buf, log_cap,
+            stats.ctypes.data_as(C.POINTER(C.c_double)))
+    if steps is None:
+        st = load().rpba_calc_plsa_parallel_ranks(*args, int(rank), int(world), ag, None)
+    else:
+        st = load().rpba_calc_plsa_parallel_ranks_hosted(*args, steps[0], steps[1], int(rank), int(world), ag, None)
     n = int(b.pt_obs_off[-1])
     b.pt_obs_image = b.pt_obs_image[:n].copy()
     b.pt_obs_slot = b.pt_obs_slot[:n].copy()

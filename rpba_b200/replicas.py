@@ -66,6 +66,28 @@ class Group:
             self.dist.destroy_process_group()
 
 
+def bytes_allgather(device=None):
+    """An all-gather of byte strings over the default torch.distributed
+    group, as rpba_calc_plsa_parallel_ranks wants it: every rank passes the
+    same number of bytes and gets every rank's, concatenated in rank order
+    (one rank, no group: its own).  ``device``: where the buffers go for
+    the collective (a CUDA device with NCCL; None with gloo)."""
+    import torch
+    import torch.distributed as dist
+
+    def gather(data: bytes) -> bytes:
+        if not dist.is_initialized() or dist.get_world_size() == 1:
+            return data
+        t = torch.frombuffer(bytearray(data), dtype=torch.uint8) if data else torch.empty(0, dtype=torch.uint8)
+        if device is not None:
+            t = t.to(device)
+        outs = [torch.empty_like(t) for _ in range(dist.get_world_size())]
+        dist.all_gather(outs, t)
+        return b"".join(o.cpu().numpy().tobytes() for o in outs)
+
+    return gather
+
+
 def time_steps(g: Group, step: Callable[[], float], steps: int, warmup: int,
                before_step: Callable[[], None] | None = None) -> dict:
     """Warm-up, then `steps` timed calls of `step` (which returns its own

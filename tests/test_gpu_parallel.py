@@ -126,3 +126,29 @@ def test_parallel_loop_is_reproducible():
     assert s1 == s2 and log1 == log2
     for name in ("pmat", "K", "distpara", "XX", "pt_obs_off", "pt_obs_image", "pt_obs_slot"):
         assert np.array_equal(getattr(b1, name), getattr(b2, name)), name
+
+
+def test_ranks_form_on_one_rank_equals_the_loop():
+    """rpba_calc_plsa_parallel_ranks on one rank, its all-gather returning
+    the rank's own bytes: the exchange of the partition steps' results runs
+    (written and read back after every round of steps) and the block,
+    statistics and log equal rpba_calc_plsa_parallel's bit for bit.  (Over
+    several ranks the loop is checked on CPU with gloo ranks,
+    test_cpu_parallel_ranks.py.)"""
+    import rpba_b200 as rb
+    from rpba_b200 import lib, scenes
+    blk = scenes.to_block(scenes.arc_scene(seed=5, n_cams=50, n_pts=8000))
+    part = rb.partition_images(blk, 4)
+    st1, b1, s1, log1 = rb.calc_plsa_parallel(blk, part, 4)
+    calls = []
+
+    def gather(data):
+        calls.append(len(data))
+        return data
+
+    st2, b2, s2, log2 = lib.calc_plsa_parallel_ranks(blk, part, 4, 0, 1, gather)
+    assert st1 == st2 == 0, log2[-2000:]
+    assert s1 == s2 and log1 == log2
+    assert len(calls) == 2 * (s2["iterations"] - 1)
+    for name in ("pmat", "K", "distpara", "XX", "pt_obs_off", "pt_obs_image", "pt_obs_slot"):
+        assert np.array_equal(getattr(b1, name), getattr(b2, name)), name
