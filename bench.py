@@ -75,6 +75,9 @@ def parse():
     ap.add_argument("--no-ablation", action="store_true", help="skip the preconditioner ablation solves")
     ap.add_argument("--batch-scenes", type=int, default=256, help="--config 4: scenes of the batched workload")
     ap.add_argument("--e2e-steps", type=int, default=1)
+    ap.add_argument("--ranks-scale", type=float, default=0.1,
+                    help="scale of the city-family scene the partitioned branch solves over the ranks")
+    ap.add_argument("--no-ranks", action="store_true", help="skip the partitioned branch over the ranks")
     return ap.parse_args()
 
 
@@ -364,6 +367,57 @@ def run_reference(args):
     return 0
 
 
+def partitioned_over_ranks(args, g, local):
+    """One scene over the ranks in the reference's own partitioned algorithm:
+    the city family at --ranks-scale, every rank holding the whole scene,
+    the partitions (the reference's count for the host's cores) dealt to the
+    ranks and the partition steps' results all-gathered after every round
+    (rpba_calc_plsa_parallel_ranks; one rank: rpba_calc_plsa_parallel).
+    Wall time of the second of two runs, max over ranks; the same scene at
+    every rank count (strong scaling).  Every rank takes the same
+    collective steps whatever fails; a failure is reported, not raised."""
+    import hashlib
+    import math
+    import torch
+    import rpba_b200 as rb
+    from rpba_b200.replicas import bytes_allgather
+    sblk = make_block(3, args.ranks_scale, args.seed_offset)
+    k = max(2, min(os.cpu_count() or 1, int(math.floor(sblk.n_images / 70 + 0.5))))
+    err, dt, st, iters, h, part = None, float("nan"), None, None, None, None
+    try:
+        part = rb.partition_images(sblk, k)
+    except Exception as e:
+        err = f"{type(e).__name__}: {e}"
+    gather = bytes_allgather(torch.device("cuda", local))
+    for _ in range(2):
+        g.barrier()
+        if err is not None:
+            continue
+        try:
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if g.world == 1:
+                st, b, stats, _ = rb.calc_plsa_parallel(sblk, part, k, device=local)
+            else:
+                st, b, stats, _ = rb.calc_plsa_parallel_ranks(sblk, part, k, g.rank, g.world, gather, device=local)
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            iters = stats["iterations"]
+            h = hashlib.sha1(b"".join(np.ascontiguousarray(getattr(b, n)).tobytes()
+                                      for n in ("pmat", "K", "distpara", "XX", "pt_obs_off", "pt_obs_image",
+                                                "pt_obs_slot"))).hexdigest()
+        except Exception as e:
+            err = f"{type(e).__name__}: {e}"
+    infos = g.gather({"seconds": dt, "status": st, "hash": h, "error": err})
+    return {"value": max(i["seconds"] for i in infos), "unit": UNIT, "scaling": "strong", "ranks": g.world,
+            "partitions": k,
+            "workload": (f"city family at {args.ranks_scale:g} scale ({sblk.n_images} cameras, {sblk.n_obs} "
+                         "observations), the reference's partitioned branch, reference PCG in the steps"),
+            "status": [i["status"] for i in infos], "outer_iterations": iters,
+            "identical_on_all_ranks": len({i["hash"] for i in infos}) == 1,
+            "errors": [i["error"] for i in infos if i["error"]]}
+
+
 def repo_libraries():
     """Shared libraries of this repository mapped into the process (the
     reference arm must run the oracle's alone)."""
@@ -591,6 +645,8 @@ def main():
                "gpu_same_sample_s": same["ours"], "gpu_plain_fp64_same_sample_s": same["plain_fp64"],
                "gpu_e2e_same_sample_s": same["ours_e2e"], "parallel": par}
 
+    ranks = None if args.no_ranks else partitioned_over_ranks(args, g, local)
+
     if rank == 0:
         r0 = reps[-1]
         line = {
@@ -612,6 +668,7 @@ def main():
             "kernel_share": kernel_share,
             "kernels": kernels,
             "ablation": ablation,
+            "one_scene_over_ranks": ranks,
         }
         print(json.dumps(line), flush=True)
     g.close()

@@ -164,3 +164,52 @@ def test_bad_rank_arguments(oracle_mod):
         st = lib.calc_plsa_parallel_ranks(blk, part, k, rank, world, lambda d: d * max(world, 1),
                                           steps=_steps(oracle_mod))[0]
         assert st == 1, (rank, world)
+
+
+def _bench_worker(rank, world, port, q):
+    try:
+        import argparse
+        import os
+        import sys
+        sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+        import bench
+        from rpba_b200.replicas import Group
+        g = Group(rank, world, backend="gloo", timeout_s=60.0, init_method=f"tcp://127.0.0.1:{port}")
+        args = argparse.Namespace(ranks_scale=0.01, seed_offset=0)
+        q.put(("ok", rank, bench.partitioned_over_ranks(args, g, 0)))
+        g.close()
+    except Exception as e:  # reported to the parent
+        q.put(("err", rank, repr(e)))
+
+
+def _has_cuda():
+    import torch
+    return torch.cuda.is_available()
+
+
+@pytest.mark.skipif(_has_cuda(), reason="the failure it plants is the absence of a GPU")
+def test_bench_leg_reports_a_failure_on_every_rank_without_hanging():
+    """bench.py's one-scene-over-ranks leg takes the same collective steps on
+    every rank whatever fails: here every rank fails to reach a GPU (none on
+    this host) and both ranks return the leg's record with the errors."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _port()
+    ps = [ctx.Process(target=_bench_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    out = []
+    deadline = time.time() + 240
+    while len(out) < 2 and time.time() < deadline:
+        try:
+            out.append(q.get(timeout=max(0.1, deadline - time.time())))
+        except Exception:
+            break
+    for p in ps:
+        p.join(timeout=10)
+        if p.is_alive():
+            p.kill()
+    assert len(out) == 2, out
+    for r in out:
+        assert r[0] == "ok", r
+        assert r[2]["ranks"] == 2 and len(r[2]["errors"]) == 2, r[2]
