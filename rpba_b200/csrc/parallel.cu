@@ -478,8 +478,10 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
             const int it = rd.get_v<int32_t>();
             if (!rd.ok || it < 0 || it >= T || owner[it] != r) return RPBA_ERR_COMM;
             pst[it] = rd.get_v<int32_t>();
-            plogs[it].resize(rd.get_v<uint64_t>());
-            rd.get(&plogs[it][0], plogs[it].size());
+            const uint64_t nlog = rd.get_v<uint64_t>();
+            if (!rd.ok || nlog > (uint64_t)(rd.end - rd.p)) return RPBA_ERR_COMM;
+            plogs[it].assign((const char *)rd.p, (size_t)nlog);
+            rd.p += nlog;
             for (int gi : imgindv[it]) {
               rd.get(&PMdd[it][12 * (size_t)gi], sizeof(double) * 12);
               camerasoit[it][gi] = rd.get_v<PCam>();
@@ -747,19 +749,34 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
 
 }  // namespace
 
+// The loop's host containers may throw (allocation, thread creation); no
+// exception crosses the C ABI.
+template <class F>
+int32_t no_throw(F &&f) {
+  try {
+    return f();
+  } catch (const std::exception &) {
+    return RPBA_ERR_CUDA;
+  }
+}
+
 extern "C" int32_t rpba_calc_plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads,
                                            const int32_t *part, char *log, size_t cap, double *stats) {
   if (opt && (opt->exteval || opt->precision != RPBA_PREC_FP64 ||
               (opt->solver != RPBA_SOLVER_PCG && opt->solver != RPBA_SOLVER_DIRECT)))
     return RPBA_ERR_UNSUPPORTED;
-  return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, rpba_lsa_gcp_step, gpu_merge, host_workers());
+  return no_throw([&] {
+    return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, rpba_lsa_gcp_step, gpu_merge, host_workers());
+  });
 }
 
 extern "C" int32_t rpba_calc_plsa_parallel_hosted(rpba_block *blk, const rpba_options *opt, int32_t nthreads,
                                                   const int32_t *part, char *log, size_t cap, double *stats,
                                                   rpba_gcp_step_fn step, rpba_merge_fn merge) {
   if (!step || !merge) return RPBA_ERR_ARG;
-  return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, step, merge, host_workers());
+  return no_throw([&] {
+    return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, step, merge, host_workers());
+  });
 }
 
 extern "C" int32_t rpba_calc_plsa_parallel_ranks(rpba_block *blk, const rpba_options *opt, int32_t nthreads,
@@ -775,7 +792,9 @@ extern "C" int32_t rpba_calc_plsa_parallel_ranks(rpba_block *blk, const rpba_opt
   rk.world = world;
   rk.ag = allgather;
   rk.ctx = ctx;
-  return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, rpba_lsa_gcp_step, gpu_merge, host_workers(), rk);
+  return no_throw([&] {
+    return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, rpba_lsa_gcp_step, gpu_merge, host_workers(), rk);
+  });
 }
 
 extern "C" int32_t rpba_calc_plsa_parallel_ranks_hosted(rpba_block *blk, const rpba_options *opt,
@@ -789,5 +808,7 @@ extern "C" int32_t rpba_calc_plsa_parallel_ranks_hosted(rpba_block *blk, const r
   rk.world = world;
   rk.ag = allgather;
   rk.ctx = ctx;
-  return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, step, merge, host_workers(), rk);
+  return no_throw([&] {
+    return plsa_parallel(blk, opt, nthreads, part, log, cap, stats, step, merge, host_workers(), rk);
+  });
 }
