@@ -518,7 +518,8 @@ class Solver:
             for name in ("pmat", "K", "distpara", "XX", "pt_obs_off", "pt_obs_image", "pt_obs_slot"):
                 a, ref = getattr(out, name), getattr(b, name)
                 if a.shape != ref.shape or a.dtype != ref.dtype or not a.flags.c_contiguous or not a.flags.writeable:
-                    raise ValueError(f"state(out=...): {name} must be a writable C-contiguous {ref.dtype} array of shape {ref.shape}")
+                    raise ValueError(f"state(out=...): {name} must be a writable C-contiguous {ref.dtype} "
+                                     f"array of shape {ref.shape}")
         cb = out.as_c()
         st = load().rpba_get_state(self.h, C.byref(cb))
         if st != 0:
