@@ -56,6 +56,14 @@ class BAL:
 
 # ----------------------------------------------------------------- rotations
 
+
+def host_share() -> int:
+    """Host cores for this process's generator pool: the node's cores split
+    between the processes torchrun starts on it (LOCAL_WORLD_SIZE), so that
+    ranks generating their scenes at once do not oversubscribe the host."""
+    local = max(1, int(os.environ.get("LOCAL_WORLD_SIZE", "1")))
+    return max(1, (os.cpu_count() or 1) // local)
+
 def aa_to_R(aa: np.ndarray) -> np.ndarray:
     """Angle-axis -> rotation (rpba.cpp:343-366 formula), float64."""
     a, b, c = aa[:, 0], aa[:, 1], aa[:, 2]
@@ -187,8 +195,7 @@ def _assemble(rng, R_true, C_true, f_true, k_true, X_true, props, vis_fn, t_want
     base = int(rng.integers(0, 2**62))
     jobs = [(s, min(s + chunk, n_p), base + s, props, vis_fn, t_want, n_c) for s in range(0, n_p, chunk)]
     if workers is None:
-        import os
-        workers = min(len(jobs), os.cpu_count() or 1, 32) if n_p > 1_000_000 else 1
+        workers = min(len(jobs), host_share(), 32) if n_p > 1_000_000 else 1
     if workers > 1:
         # spawn (not fork): callers may already hold a CUDA context
         import multiprocessing as mp
@@ -411,7 +418,7 @@ def batch_scenes(seed=20264, n_scenes=256, cmin=20, cmax=400, pts_per_cam=150):
 def batch_blocks(seed=20264, n_scenes=256, cmin=20, cmax=400, pts_per_cam=150, workers=None):
     """The batched workload as blocks, generated in parallel processes."""
     specs = batch_scene_specs(seed, n_scenes, cmin, cmax, pts_per_cam)
-    workers = workers or min(len(specs), os.cpu_count() or 1, 32)
+    workers = workers or min(len(specs), host_share(), 32)
     if workers <= 1:
         return [_arc_block(kw) for kw in specs]
     import multiprocessing as mp
