@@ -34,14 +34,68 @@ Graph build_graph(const rpba_block *b) {
   g.w.assign(n, 0);
   // BM[i]: sum of the track lengths of the image's points (tracks of >= 2)
   std::vector<long long> bm(n, 0);
+  for (int p = 0; p < b->n_points; ++p) {
+    const int t0 = b->pt_obs_off[p], t1 = b->pt_obs_off[p + 1];
+    if (t1 - t0 < 2) continue;
+    for (int t = t0; t < t1; ++t) bm[b->pt_obs_image[t]] += t1 - t0;
+  }
+  for (int i = 0; i < n; ++i) g.w[i] = (long long)std::pow((double)bm[i], 0.3333);
+  g.off.assign(n + 1, 0);
+  const int T = n >= 256 ? (int)std::min(32u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+  auto run = [&](auto &&work) {
+    std::vector<std::thread> th;
+    for (int k = 1; k < T; ++k) th.emplace_back(work, k);
+    work(0);
+    for (auto &t : th) t.join();
+  };
+  if (n <= 32768) {
+    // neighbours of every image as a bit row (n bits; at most 128 MB in
+    // all), images split over host threads in contiguous ranges: each
+    // thread streams every track in order and sets, for each of its images
+    // in the track, the bits of the track's other images; the rows are then
+    // read out in index order, so the lists come out sorted
+    const size_t words = ((size_t)n + 63) / 64;
+    std::vector<uint64_t> bits((size_t)n * words, 0);
+    run([&](int k) {
+      const int lo = (int)((long long)n * k / T), hi = (int)((long long)n * (k + 1) / T);
+      for (int p = 0; p < b->n_points; ++p) {
+        const int t0 = b->pt_obs_off[p], t1 = b->pt_obs_off[p + 1];
+        if (t1 - t0 < 2) continue;
+        for (int t = t0; t < t1; ++t) {
+          const int i = b->pt_obs_image[t];
+          if (i < lo || i >= hi) continue;
+          uint64_t *row = &bits[(size_t)i * words];
+          for (int u = t0; u < t1; ++u) {
+            const int j = b->pt_obs_image[u];
+            if (j != i) row[j >> 6] |= 1ull << (j & 63);
+          }
+        }
+      }
+    });
+    for (int i = 0; i < n; ++i) {
+      int c = 0;
+      for (size_t w = 0; w < words; ++w) c += __builtin_popcountll(bits[(size_t)i * words + w]);
+      g.off[i + 1] = g.off[i] + c;
+    }
+    g.adj.resize(g.off[n]);
+    run([&](int k) {
+      for (int i = (int)((long long)n * k / T); i < (int)((long long)n * (k + 1) / T); ++i) {
+        int o = g.off[i];
+        for (size_t w = 0; w < words; ++w)
+          for (uint64_t v = bits[(size_t)i * words + w]; v; v &= v - 1) g.adj[o++] = (int)(w * 64) + __builtin_ctzll(v);
+      }
+    });
+    return g;
+  }
+  // larger scenes: neighbours of every image through its points (a stamp
+  // array per thread marks the ones already listed), images split over host
+  // threads in contiguous ranges; each list is sorted, so the result does not
+  // depend on the thread count
   std::vector<int> ipo(n + 1, 0);  // image -> points (CSR)
   for (int p = 0; p < b->n_points; ++p) {
     const int t0 = b->pt_obs_off[p], t1 = b->pt_obs_off[p + 1];
     if (t1 - t0 < 2) continue;
-    for (int t = t0; t < t1; ++t) {
-      bm[b->pt_obs_image[t]] += t1 - t0;
-      ++ipo[b->pt_obs_image[t] + 1];
-    }
+    for (int t = t0; t < t1; ++t) ++ipo[b->pt_obs_image[t] + 1];
   }
   for (int i = 0; i < n; ++i) ipo[i + 1] += ipo[i];
   std::vector<int> ipts(ipo[n]), fill(ipo.begin(), ipo.end() - 1);
@@ -50,14 +104,8 @@ Graph build_graph(const rpba_block *b) {
     if (t1 - t0 < 2) continue;
     for (int t = t0; t < t1; ++t) ipts[fill[b->pt_obs_image[t]]++] = p;
   }
-  for (int i = 0; i < n; ++i) g.w[i] = (long long)std::pow((double)bm[i], 0.3333);
-  // neighbours of every image through its points (a stamp array per thread
-  // marks the ones already listed), images split over host threads in
-  // contiguous ranges; each list is sorted, so the result does not depend on
-  // the thread count
   std::vector<std::vector<int>> nbr(n);
-  const int T = n >= 256 ? (int)std::min(32u, std::max(1u, std::thread::hardware_concurrency())) : 1;
-  auto work = [&](int k) {
+  run([&](int k) {
     std::vector<int> stamp(n, -1);
     for (int i = (int)((long long)n * k / T); i < (int)((long long)n * (k + 1) / T); ++i) {
       std::vector<int> &out = nbr[i];
@@ -73,12 +121,7 @@ Graph build_graph(const rpba_block *b) {
       }
       std::sort(out.begin(), out.end());
     }
-  };
-  std::vector<std::thread> th;
-  for (int k = 1; k < T; ++k) th.emplace_back(work, k);
-  work(0);
-  for (auto &t : th) t.join();
-  g.off.assign(n + 1, 0);
+  });
   for (int i = 0; i < n; ++i) g.off[i + 1] = g.off[i] + (int)nbr[i].size();
   g.adj.resize(g.off[n]);
   for (int i = 0; i < n; ++i) std::copy(nbr[i].begin(), nbr[i].end(), g.adj.begin() + g.off[i]);
