@@ -25,10 +25,17 @@
 // persistent PCG and the exact sums need every SM); each step's result does
 // not depend on the others, so neither does the loop's.
 //
+// Over several ranks (one process per GPU, rpba_calc_plsa_parallel_ranks)
+// every rank keeps the whole loop, runs the steps of the partitions it owns
+// and all-gathers the steps' results with the others after every round of
+// steps, through the caller's transport; the merge and the bookkeeping are
+// repeated on every rank, so every rank takes the same decisions.
+//
 // The loop is host code over two steps, the partition step and the merge
-// pass; rpba_calc_plsa_parallel binds them to the GPU (rpba_lsa_gcp_step and
-// the CalcLSAXMulti kernel), rpba_calc_plsa_parallel_hosted takes them from
-// the caller, so that the loop itself can be checked without a GPU.
+// pass; rpba_calc_plsa_parallel(_ranks) binds them to the GPU
+// (rpba_lsa_gcp_step and the CalcLSAXMulti kernel), the _hosted forms take
+// them from the caller, so that the loop itself can be checked without a
+// GPU.
 #include <algorithm>
 #include <atomic>
 #include <cmath>
