@@ -1,10 +1,13 @@
-"""Work over ranks: one process per GPU, no collective on the data path.
+"""Work over ranks: one process per GPU.
 
 The reference's global LSA does not shard (one linear system per LM step);
 its own parallel form partitions the scene into independent LSAs
 (rpbacore.cpp:100-510).  Across GPUs this library therefore splits work that
 is independent by nature:
 
+* one scene in the partitioned form: the partitions' steps dealt to the
+  ranks, their results all-gathered after every round of steps
+  (rpba_calc_plsa_parallel_ranks, whose transport is ``bytes_allgather``);
 * replicas (one scene): every rank solves its own copy; the job's time is
   the slowest rank's (max over ranks);
 * scene-parallel (many independent scenes, the batched workload): the scenes
@@ -12,8 +15,8 @@ is independent by nature:
   per-scene results are gathered in scene order and the job's time is the
   slowest rank's (``scene_parallel``).
 
-Only these host-side reductions and gathers cross ranks, through
-torch.distributed (NCCL on GPUs, gloo on CPU).
+Only these host-side exchanges cross ranks, through torch.distributed
+(NCCL on GPUs, gloo on CPU).
 """
 from __future__ import annotations
 
