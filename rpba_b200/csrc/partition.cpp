@@ -130,10 +130,15 @@ Graph build_graph(const rpba_block *b) {
 
 class Bisector {
  public:
-  Bisector(const Graph &g, int32_t *part) : g_(g), part_(part), in_(g.w.size(), 0), mark_(g.w.size(), 0) {}
+  // spawn_depth: levels of the recursion whose first half is cut on a
+  // thread of its own (with its own Bisector: its own scratch arrays, so
+  // the halves share nothing but the graph; a cut depends only on its set,
+  // so the parts do not depend on the threads)
+  Bisector(const Graph &g, int32_t *part, int spawn_depth = 0)
+      : g_(g), part_(part), spawn_depth_(spawn_depth), in_(g.w.size(), 0), mark_(g.w.size(), 0) {}
 
   // Cuts `verts` (sorted) into k parts numbered base .. base + k - 1.
-  void cut(std::vector<int> verts, int k, int base) {
+  void cut(std::vector<int> verts, int k, int base, int depth = 0) {
     if (k <= 1 || verts.size() <= 1) {
       for (int v : verts) part_[v] = base;
       return;
@@ -218,8 +223,14 @@ class Bisector {
     const int keep = ++tag_;
     for (int v : best) mark_[v] = keep;
     for (int v : verts) (mark_[v] == keep ? h2 : h1).push_back(v);
-    cut(h1, k1, base);
-    cut(h2, k - k1, base + k1);
+    if (depth < spawn_depth_ && h1.size() >= 256 && h2.size() >= 256) {
+      std::thread t([&] { Bisector(g_, part_, spawn_depth_).cut(std::move(h1), k1, base, depth + 1); });
+      cut(std::move(h2), k - k1, base + k1, depth + 1);
+      t.join();
+    } else {
+      cut(std::move(h1), k1, base, depth + 1);
+      cut(std::move(h2), k - k1, base + k1, depth + 1);
+    }
   }
 
  private:
@@ -247,6 +258,7 @@ class Bisector {
 
   const Graph &g_;
   int32_t *part_;
+  int spawn_depth_;
   std::vector<int> in_, mark_;
   int tag_ = 0;
 };
@@ -258,6 +270,8 @@ extern "C" int32_t rpba_partition_images(const rpba_block *blk, int32_t nparts, 
   const Graph g = build_graph(blk);
   std::vector<int> all(blk->n_images);
   for (int i = 0; i < blk->n_images; ++i) all[i] = i;
-  Bisector(g, part).cut(all, nparts, 0);
+  int depth = 0;  // about one thread per host core at the deepest spawning level
+  for (unsigned c = std::max(1u, std::thread::hardware_concurrency()); c > 1 && depth < 6; c >>= 1) ++depth;
+  Bisector(g, part, depth).cut(all, nparts, 0);
   return RPBA_OK;
 }
