@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <atomic>
 #include <charconv>
+#include <memory>
 #include <string>
 #include <thread>
 #include <vector>
@@ -23,7 +24,7 @@ namespace {
 
 // Whitespace-separated number reader over a whole file in memory.
 struct Reader {
-  std::vector<char> buf;
+  std::unique_ptr<char[]> buf;  // the whole file (not zero-filled first)
   const char *p = nullptr, *e = nullptr;
   bool ok = true;
   bool open(const char *path) {
@@ -32,11 +33,11 @@ struct Reader {
     std::fseek(f, 0, SEEK_END);
     const long n = std::ftell(f);
     std::fseek(f, 0, SEEK_SET);
-    buf.resize((size_t)n + 1);
-    const size_t got = std::fread(buf.data(), 1, (size_t)n, f);
+    buf.reset(new char[(size_t)n + 1]);
+    const size_t got = std::fread(buf.get(), 1, (size_t)n, f);
     std::fclose(f);
     buf[got] = 0;
-    p = buf.data();
+    p = buf.get();
     e = p + got;
     return true;
   }
@@ -278,10 +279,15 @@ int32_t rpba_input_block(const char *path, int32_t nraddpar, int32_t k24out, rpb
   if (par) {
     BodyOut O{nc, np, no, ocam.data(), opt.data(), ox.data(), oy.data(), cam_d.data(), cam_f.data(), xx.data()};
     if (!parse_body_parallel(r.p, r.e, O, T)) return RPBA_ERR_IO;
-    for (long long i = 0; i < no; ++i) {
-      ++cnt[ocam[i] + 1];
-      ++pcnt[opt[i] + 1];
-    }
+    // the counts per image and per point (threads own ranges of images,
+    // then of points, each scanning every observation)
+    parallel_for(T, [&](int k) {
+      const long long c0 = nc * k / T, c1 = nc * (k + 1) / T, p0 = np * k / T, p1 = np * (k + 1) / T;
+      for (long long i = 0; i < no; ++i) {
+        if (ocam[i] >= c0 && ocam[i] < c1) ++cnt[ocam[i] + 1];
+        if (opt[i] >= p0 && opt[i] < p1) ++pcnt[opt[i] + 1];
+      }
+    });
   } else {
     for (long long i = 0; i < no; ++i) {
       const long long c = r.integer(), p = r.integer();
@@ -313,20 +319,38 @@ int32_t rpba_input_block(const char *path, int32_t nraddpar, int32_t k24out, rpb
   b.pt_obs_slot = cal<int32_t>(no);
   for (long long i = 0; i < nc; ++i) b.img_obs_off[i + 1] = b.img_obs_off[i] + cnt[i + 1];
   for (long long i = 0; i < np; ++i) b.pt_obs_off[i + 1] = b.pt_obs_off[i] + pcnt[i + 1];
-  std::vector<int32_t> ifill(nc, 0), pfill(np, 0);
-  for (long long i = 0; i < no; ++i) {
-    const int c = ocam[i], p = opt[i];
-    const int slot = ifill[c]++;
-    const int sl = b.img_obs_off[c] + slot;
-    b.xg[2 * sl] = -ox[i];
-    b.xg[2 * sl + 1] = -oy[i];
-    b.wx[sl] = 1.f;
-    b.wy[sl] = 1.f;
-    b.wxy[sl] = 0.f;
-    const int w = b.pt_obs_off[p] + pfill[p]++;
-    b.pt_obs_image[w] = c;
-    b.pt_obs_slot[w] = slot;
-  }
+  // every observation's slot in its image and entry in its point's track,
+  // in file order (with threads: each owns a range of images, then of
+  // points, and scans every observation; the same slots and entries)
+  std::vector<int32_t> ifill(nc, 0), pfill(np, 0), oslot(no);
+  const int TS = par ? T : 1;
+  auto fill_images = [&](int k) {
+    const long long c0 = nc * k / TS, c1 = nc * (k + 1) / TS;
+    for (long long i = 0; i < no; ++i) {
+      const int c = ocam[i];
+      if (c < c0 || c >= c1) continue;
+      const int slot = ifill[c]++;
+      const int sl = b.img_obs_off[c] + slot;
+      oslot[i] = slot;
+      b.xg[2 * (size_t)sl] = -ox[i];
+      b.xg[2 * (size_t)sl + 1] = -oy[i];
+      b.wx[sl] = 1.f;
+      b.wy[sl] = 1.f;
+      b.wxy[sl] = 0.f;
+    }
+  };
+  auto fill_points = [&](int k) {
+    const long long p0 = np * k / TS, p1 = np * (k + 1) / TS;
+    for (long long i = 0; i < no; ++i) {
+      const int p = opt[i];
+      if (p < p0 || p >= p1) continue;
+      const int w = b.pt_obs_off[p] + pfill[p]++;
+      b.pt_obs_image[w] = ocam[i];
+      b.pt_obs_slot[w] = oslot[i];
+    }
+  };
+  parallel_for(TS, fill_images);
+  parallel_for(TS, fill_points);
   for (long long i = 0; i < nc; ++i) {
     const double a = par ? cam_d[3 * i] : r.dbl(), bb = par ? cam_d[3 * i + 1] : r.dbl(),
                  c = par ? cam_d[3 * i + 2] : r.dbl();
