@@ -404,6 +404,14 @@ void rpba_block_free(rpba_block *b) {
   std::memset(b, 0, sizeof *b);
 }
 
+// printf's "%.8g" and "%d" (std::to_chars in the general format with a
+// precision gives printf's characters for that conversion in the "C" locale;
+// the value is taken as a double, as printf's varargs promote it)
+namespace {
+inline char *put_g8(char *p, double v) { return std::to_chars(p, p + 40, v, std::chars_format::general, 8).ptr; }
+inline char *put_d(char *p, int v) { return std::to_chars(p, p + 16, v).ptr; }
+}  // namespace
+
 int32_t rpba_output_block(const char *path, rpba_block *b, int32_t k24out) {
   if (!path || !b) return RPBA_ERR_ARG;
   FILE *f = std::fopen(path, "w");
@@ -426,18 +434,28 @@ int32_t rpba_output_block(const char *path, rpba_block *b, int32_t k24out) {
         b->pt_obs_image[j] = v[j - s].first;
         b->pt_obs_slot[j] = v[j - s].second;
         const int sl = b->img_obs_off[v[j - s].first] + v[j - s].second;
-        const int n = std::snprintf(line, sizeof line, "%d %d %.8g %.8g\n", v[j - s].first, i, -b->xg[2 * sl],
-                                    -b->xg[2 * sl + 1]);
-        out.append(line, (size_t)n);
+        char *q = put_d(line, v[j - s].first);
+        *q++ = ' ';
+        q = put_d(q, i);
+        *q++ = ' ';
+        q = put_g8(q, -b->xg[2 * sl]);
+        *q++ = ' ';
+        q = put_g8(q, -b->xg[2 * sl + 1]);
+        *q++ = '\n';
+        out.append(line, (size_t)(q - line));
       }
     }
   };
   auto pt_lines = [&](int p0, int p1, std::string &out) {
     char line[96];
     for (int i = p0; i < p1; ++i) {
-      const int n = std::snprintf(line, sizeof line, "%.8g %.8g %.8g\n", b->XX[3 * i], b->XX[3 * i + 1],
-                                  b->XX[3 * i + 2]);
-      out.append(line, (size_t)n);
+      char *q = put_g8(line, b->XX[3 * i]);
+      *q++ = ' ';
+      q = put_g8(q, b->XX[3 * i + 1]);
+      *q++ = ' ';
+      q = put_g8(q, b->XX[3 * i + 2]);
+      *q++ = '\n';
+      out.append(line, (size_t)(q - line));
     }
   };
   // large blocks: per-thread buffers over point ranges, written in order
