@@ -97,3 +97,45 @@ def test_partition_rejects_bad_arguments(blocks):
     with pytest.raises(rb.RpbaError) as ei:
         rb.partition_images(blocks["arc"], 0)
     assert ei.value.status == 1
+
+
+def _chain_block(n):
+    """A block of n images in a chain, for the partition only (no geometry):
+    two points seen by images i, i + 1 for every i, and every fifth i a
+    point seen by i, i + 1, i + 2."""
+    from rpba_b200.block import Block
+    tracks = []
+    for i in range(n - 1):
+        tracks += [[i, i + 1], [i, i + 1]]
+        if i % 5 == 0 and i + 2 < n:
+            tracks.append([i, i + 1, i + 2])
+    cnt = np.zeros(n, np.int64)
+    img, slot = [], []
+    for t in tracks:
+        for i in t:
+            img.append(i)
+            slot.append(cnt[i])
+            cnt[i] += 1
+    off = np.concatenate([[0], np.cumsum([len(t) for t in tracks])]).astype(np.int32)
+    ioff = np.concatenate([[0], np.cumsum(cnt)]).astype(np.int32)
+    ns, npt = int(ioff[-1]), len(tracks)
+    f32 = lambda *s: np.zeros(s, np.float32)
+    return Block(f32(n, 12), f32(n, 9), f32(n, 2), f32(npt, 3), ioff, f32(ns, 2), np.ones(ns, np.float32),
+                 np.ones(ns, np.float32), f32(ns), off, np.array(img, np.int32), np.array(slot, np.int32))
+
+
+def test_partition_of_a_scene_past_the_bit_row_graph():
+    """Past 32,768 images the covisibility graph is built image by image
+    through its points instead of as bit rows (whose n^2 bits would pass 128
+    MB); the parts keep the same properties: contiguous, balanced,
+    deterministic."""
+    import rpba_b200 as rb
+    blk = _chain_block(33000)
+    edges, w = _graph(blk)
+    for k in (2, 5):
+        part = rb.partition_images(blk, k)
+        assert np.array_equal(part, rb.partition_images(blk, k))
+        for q in range(k):
+            assert _connected(np.nonzero(part == q)[0], edges), (k, q)
+        pw = np.bincount(part, weights=w, minlength=k)
+        assert pw.max() <= 1.35 * pw.mean() + w.max(), (k, pw)
