@@ -42,7 +42,10 @@ def _port():
         return s.getsockname()[1]
 
 
-def _rank_worker(rank, world, port, case, fail_rank, q):
+OPTS = {"": {}, "plain": {"robust": False}, "noadd": {"addflags": (False, False, False)}}
+
+
+def _rank_worker(rank, world, port, case, fail_rank, q, opts=""):
     try:
         import torch.distributed as dist
         dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
@@ -59,18 +62,18 @@ def _rank_worker(rank, world, port, case, fail_rank, q):
             failing = C.CFUNCTYPE(C.c_int32, *STEP_ARGS)(lambda *a: 10)
             step = C.cast(failing, C.c_void_p)
         st, b, s, log = lib.calc_plsa_parallel_ranks(blk, part, k, rank, world, bytes_allgather(),
-                                                     steps=(step, merge))
+                                                     steps=(step, merge), **OPTS[opts])
         q.put(("ok", rank, st, {n: getattr(b, n) for n in NAMES}, s, log))
         dist.destroy_process_group()
     except Exception as e:  # reported to the parent
         q.put(("err", rank, repr(e)))
 
 
-def _run(world, case, fail_rank=-1, timeout=300):
+def _run(world, case, fail_rank=-1, timeout=300, opts=""):
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _port()
-    ps = [ctx.Process(target=_rank_worker, args=(r, world, port, case, fail_rank, q)) for r in range(world)]
+    ps = [ctx.Process(target=_rank_worker, args=(r, world, port, case, fail_rank, q, opts)) for r in range(world)]
     for p in ps:
         p.start()
     out = []
@@ -95,6 +98,12 @@ def oracle_loops(oracle_mod):
         blk, k = _scene(case)
         part = rb.partition_images(blk, k)
         res[case] = oracle_mod.calc_plsa_parallel(blk, part, k, rb.make_options())
+    blk, k = _scene("arc")
+    part = rb.partition_images(blk, k)
+    res["arc/plain"] = oracle_mod.calc_plsa_parallel(blk, part, k, rb.make_options(robust=False))
+    blk, k = _scene("city")
+    part = rb.partition_images(blk, k)
+    res["city/noadd"] = oracle_mod.calc_plsa_parallel(blk, part, k, rb.make_options(k2=False, k4=False, f=False))
     return res
 
 
@@ -125,14 +134,16 @@ def test_one_rank_through_the_exchange_equals_oracle_loop(oracle_mod, oracle_loo
     assert len(calls) == 2 * (s["iterations"] - 1)  # sizes and records after every round of steps
 
 
-@pytest.mark.parametrize("world,case", [(2, "arc"), (3, "city"), (4, "city")])
-def test_ranks_equal_oracle_loop(oracle_loops, world, case):
-    """world 4 with 3 partitions: one rank owns none and only exchanges."""
-    out = _run(world, case)
+@pytest.mark.parametrize("world,case,opts", [(2, "arc", ""), (3, "city", ""), (4, "city", ""), (2, "arc", "plain"),
+                                             (2, "city", "noadd")])
+def test_ranks_equal_oracle_loop(oracle_loops, world, case, opts):
+    """world 4 with 3 partitions: one rank owns none and only exchanges;
+    also without robust reweighting and without additional parameters."""
+    out = _run(world, case, opts=opts)
     assert len(out) == world, out
     for r in out:
         assert r[0] == "ok", r
-        _same(r[2], r[3], r[4], r[5], oracle_loops[case])
+        _same(r[2], r[3], r[4], r[5], oracle_loops[case + ("/" + opts if opts else "")])
 
 
 def test_failed_allgather_is_reported(oracle_mod):
