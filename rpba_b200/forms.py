@@ -9,12 +9,18 @@ Forms (the solver and precision options of rpba_create):
   mixed_direct   FP32 assembly, the same direct solve
   learned        FP32 assembly, the learned two-level PCG at relative
                  tolerance --tol (weights from rpba_b200/precond_weights.npy)
+  partitioned    the reference's partitioned branch (Threads=0): the
+                 reference's partition count for this host's cores,
+                 min(cores, iround(images / 70)), the partition included,
+                 FP64 with the reference's PCG in the partition steps
 
-Each form: one warm-up solve on its handle, then --repeats solves from the
-same start state; prints one JSON line per form with the median device time
-of the whole robust LM run (CUDA events inside the library), the linear
-solve and PCG iteration counts, the final RMS reprojection error and cost,
-and the status.  A form the workload does not admit (the direct forms past
+Each solver form: one warm-up solve on its handle, then --repeats solves
+from the same start state; prints one JSON line per form with the median
+device time of the whole robust LM run (CUDA events inside the library),
+the linear solve and PCG iteration counts, the final RMS reprojection error
+and cost, and the status.  The partitioned form (host control around device
+steps) reports the wall time of the last of 1 + --repeats runs, its outer
+iterations and best sigma0.  A form the workload does not admit (the direct forms past
 the envelope's size) reports its status instead of a time.
 """
 from __future__ import annotations
@@ -24,7 +30,7 @@ import json
 import statistics
 import time
 
-FORMS = ("plain", "direct", "mixed_direct", "learned")
+FORMS = ("plain", "direct", "mixed_direct", "learned", "partitioned")
 
 
 def main():
@@ -56,6 +62,9 @@ def main():
     if "learned" in forms and weights is None:
         raise SystemExit("rpba_b200/precond_weights.npy is missing: python -m rpba_b200.train_precond")
     for f in forms:
+        if f == "partitioned":
+            print(json.dumps(partitioned(lib, blk, a, gen)), flush=True)
+            continue
         S = lib.Solver(blk, device=a.device, **kws[f])
         if f == "learned":
             S.set_preconditioner(weights)
@@ -77,6 +86,27 @@ def main():
                          "pcg_fallbacks": rep["pcg_fallbacks"], "final_rms": rep["rms"], "final_cost": rep["cost"],
                          "obs_deleted": rep["obs_deleted"]})
         print(json.dumps(line), flush=True)
+
+
+def partitioned(lib, blk, a, gen) -> dict:
+    """The reference's Threads=0 branch on the GPU, wall time."""
+    import math
+    import os
+    k = min(os.cpu_count() or 1, int(math.floor(blk.n_images / 70 + 0.5)))
+    line = {"config": a.config, "scale": a.scale, "n_images": blk.n_images, "n_obs": blk.n_obs,
+            "scene_generation_s": round(gen, 1), "form": "partitioned", "partitions": k}
+    if k < 2:
+        line.update({"status": None, "note": "one partition: the reference takes the global LSA"})
+        return line
+    times = []
+    for _ in range(1 + max(1, a.repeats)):
+        t0 = time.perf_counter()
+        part = lib.partition_images(blk, k)
+        st, _, stats, _ = lib.calc_plsa_parallel(blk, part, k, device=a.device)
+        times.append(time.perf_counter() - t0)
+    line.update({"status": st, "status_text": lib.load().rpba_status_string(st).decode(), "seconds": times[-1],
+                 "step_times": times[1:], "outer_iterations": stats["iterations"], "sig0opt": stats["sig0opt"]})
+    return line
 
 
 if __name__ == "__main__":
