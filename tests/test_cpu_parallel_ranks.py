@@ -28,6 +28,8 @@ def _scene(case):
     from rpba_b200 import scenes
     if case == "arc":
         return scenes.to_block(scenes.arc_scene(seed=5, n_cams=50, n_pts=8000)), 4
+    if case == "street":  # the street workload at full size: 1,000 cameras, 943k observations
+        return scenes.to_block(scenes.make_scene(1, scale=1.0)), 8
     return scenes.to_block(scenes.city_scene(seed=8, n_clusters=3, cams_per_cluster=20, n_pts=8000)), 3
 
 
@@ -94,7 +96,7 @@ def _run(world, case, fail_rank=-1, timeout=300, opts=""):
 def oracle_loops(oracle_mod):
     import rpba_b200 as rb
     res = {}
-    for case in ("arc", "city"):
+    for case in ("arc", "city", "street"):
         blk, k = _scene(case)
         part = rb.partition_images(blk, k)
         res[case] = oracle_mod.calc_plsa_parallel(blk, part, k, rb.make_options())
@@ -135,7 +137,7 @@ def test_one_rank_through_the_exchange_equals_oracle_loop(oracle_mod, oracle_loo
 
 
 @pytest.mark.parametrize("world,case,opts", [(2, "arc", ""), (3, "city", ""), (4, "city", ""), (2, "arc", "plain"),
-                                             (2, "city", "noadd")])
+                                             (2, "city", "noadd"), (4, "street", "")])
 def test_ranks_equal_oracle_loop(oracle_loops, world, case, opts):
     """world 4 with 3 partitions: one rank owns none and only exchanges;
     also without robust reweighting and without additional parameters."""
