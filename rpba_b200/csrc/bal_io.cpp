@@ -15,6 +15,7 @@
 #include <charconv>
 #include <memory>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -171,10 +172,17 @@ size_t io_parallel_min_bytes() {
 
 inline bool is_ws(char c) { return c == ' ' || c == '\n' || c == '\r' || c == '\t'; }
 
+// f(k) for k < T, one thread each (a k whose thread cannot be created runs
+// on the calling thread: the ranges are independent)
 template <class F>
 void parallel_for(int T, F &&f) {
   std::vector<std::thread> th;
-  for (int k = 1; k < T; ++k) th.emplace_back(f, k);
+  int k = 1;
+  try {
+    for (; k < T; ++k) th.emplace_back(f, k);
+  } catch (const std::system_error &) {
+  }
+  for (int j = k; j < T; ++j) f(j);
   f(0);
   for (auto &t : th) t.join();
 }

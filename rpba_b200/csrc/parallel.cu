@@ -42,7 +42,10 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <exception>
+#include <mutex>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -107,13 +110,30 @@ int host_workers() { return (int)std::max(1u, std::thread::hardware_concurrency(
 int nranges(long long n, int workers, int grain) {
   return (int)std::max(1ll, std::min((long long)workers, n / grain));
 }
+//   (a range whose thread cannot be created runs on the calling thread; an
+//   exception in a range is rethrown on the calling thread after the join)
 template <class F>
 void parallel_ranges(int n, int W, F &&f) {
-  auto body = [&](int k) { f(k, (int)((long long)n * k / W), (int)((long long)n * (k + 1) / W)); };
+  std::exception_ptr err;
+  std::mutex em;
+  auto body = [&](int k) {
+    try {
+      f(k, (int)((long long)n * k / W), (int)((long long)n * (k + 1) / W));
+    } catch (...) {
+      std::lock_guard<std::mutex> lock(em);
+      if (!err) err = std::current_exception();
+    }
+  };
   std::vector<std::thread> th;
-  for (int k = 1; k < W; ++k) th.emplace_back(body, k);
+  int k = 1;
+  try {
+    for (; k < W; ++k) th.emplace_back(body, k);
+  } catch (const std::system_error &) {
+  }
+  for (int j = k; j < W; ++j) body(j);
   body(0);
   for (auto &t : th) t.join();
+  if (err) std::rethrow_exception(err);
 }
 
 // the merge pass on the GPU
@@ -443,13 +463,16 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
           const int it = mine[q];
           try {
             pst[it] = part_step(it, plogs[it]);
-          } catch (const std::bad_alloc &) {
+          } catch (const std::exception &) {  // allocation: reported as the step's failure
             pst[it] = RPBA_ERR_CUDA;
           }
         }
       };
       std::vector<std::thread> th;
-      for (int k = 1; k < std::min(workers, (int)mine.size()); ++k) th.emplace_back(body);
+      try {  // fewer workers if the host refuses a thread: the counter hands out the rest
+        for (int k = 1; k < std::min(workers, (int)mine.size()); ++k) th.emplace_back(body);
+      } catch (const std::system_error &) {
+      }
       body();
       for (auto &t : th) t.join();
       if (rk.ag) {

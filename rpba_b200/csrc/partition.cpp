@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -42,9 +43,16 @@ Graph build_graph(const rpba_block *b) {
   for (int i = 0; i < n; ++i) g.w[i] = (long long)std::pow((double)bm[i], 0.3333);
   g.off.assign(n + 1, 0);
   const int T = n >= 256 ? (int)std::min(32u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+  // work(k) for k < T, one thread each (a k whose thread cannot be created
+  // runs on the calling thread: the ranges are independent)
   auto run = [&](auto &&work) {
     std::vector<std::thread> th;
-    for (int k = 1; k < T; ++k) th.emplace_back(work, k);
+    int k = 1;
+    try {
+      for (; k < T; ++k) th.emplace_back(work, k);
+    } catch (const std::system_error &) {
+    }
+    for (int j = k; j < T; ++j) work(j);
     work(0);
     for (auto &t : th) t.join();
   };
@@ -223,8 +231,14 @@ class Bisector {
     const int keep = ++tag_;
     for (int v : best) mark_[v] = keep;
     for (int v : verts) (mark_[v] == keep ? h2 : h1).push_back(v);
+    std::thread t;
     if (depth < spawn_depth_ && h1.size() >= 256 && h2.size() >= 256) {
-      std::thread t([&] { Bisector(g_, part_, spawn_depth_).cut(std::move(h1), k1, base, depth + 1); });
+      try {
+        t = std::thread([&] { Bisector(g_, part_, spawn_depth_).cut(std::move(h1), k1, base, depth + 1); });
+      } catch (const std::system_error &) {  // no thread: both halves here
+      }
+    }
+    if (t.joinable()) {
       cut(std::move(h2), k - k1, base + k1, depth + 1);
       t.join();
     } else {
