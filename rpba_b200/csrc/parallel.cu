@@ -254,10 +254,11 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
     pointXXv.close_point();
   }
   pointXXvold = pointXXv;
-  // the lists at the start of the outer iteration (the reference's
-  // pitflagsv, the partitions a point's observations fall in, is taken
-  // from them)
-  Tracks pitlists;
+  // the reference's pitflagsv: the partitions each point's observations
+  // fall in at the start of the outer iteration, distinct, in order of
+  // first appearance (CSR: point p's are pitp[pitp_off[p] ..
+  // pitp_off[p + 1]))
+  std::vector<int32_t> pitp_off(pxs + 1, 0), pitp;
   std::vector<int> gcpinfo(pxs, -1);
   std::vector<std::vector<PCam>> camerasoit(T, cameras);
   std::vector<std::vector<double>> PMdd(T, PMd);
@@ -577,7 +578,44 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
     } else {
       for (int i = 0; i < nrimages; ++i) cameraps[i] = camerasnew[i] = cameras[i];
     }
-    pitlists = pointXXv;
+    {
+      // (point ranges on host threads: counts, then entries at the prefix
+      // sums)
+      const int W = nranges(pxs, workers, 4096);
+      std::vector<int32_t> cr(W + 1, 0);
+      auto distinct = [&](int p, std::vector<int> &seen, auto &&emit) {
+        for (int t = pointXXv.off[p]; t < pointXXv.off[p + 1]; ++t) {
+          const int it = imgindbv[pointXXv.img[t]];
+          if (seen[it] != p) {
+            seen[it] = p;
+            emit(it);
+          }
+        }
+      };
+      parallel_ranges(pxs, W, [&](int k, int p0, int p1) {
+        std::vector<int> seen(T, -1);
+        int32_t c = 0;
+        for (int p = p0; p < p1; ++p) {
+          int32_t n = 0;
+          distinct(p, seen, [&](int) { ++n; });
+          pitp_off[p + 1] = n;
+          c += n;
+        }
+        cr[k + 1] = c;
+      });
+      for (int k = 0; k < W; ++k) cr[k + 1] += cr[k];
+      pitp.resize(cr[W]);
+      parallel_ranges(pxs, W, [&](int k, int p0, int p1) {
+        std::vector<int> seen(T, -1);
+        int32_t o = cr[k];
+        for (int p = p0; p < p1; ++p) {
+          const int32_t n = pitp_off[p + 1];
+          pitp_off[p + 1] = o + n;  // the end of p's entries (its start is the previous point's end)
+          distinct(p, seen, [&](int it) { pitp[o++] = it; });
+        }
+      });
+      pitp_off[0] = 0;
+    }
     double sum = 0.;
     long long redundancy = 0;
     if (robustflagit) {
@@ -632,15 +670,8 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
       std::vector<int8_t> isg(pxs, -1);
       std::vector<int32_t> ng(W + 1, 0), nw((size_t)(W + 1) * T, 0);
       // the distinct partitions of the point's start-of-iteration list
-      auto parts_of = [&](int p, std::vector<int> &seen, std::vector<int> &parts) {
-        parts.clear();
-        for (int t = pitlists.off[p]; t < pitlists.off[p + 1]; ++t) {
-          const int it = imgindbv[pitlists.img[t]];
-          if (seen[it] != p) {
-            seen[it] = p;
-            parts.push_back(it);
-          }
-        }
+      auto parts_of = [&](int p, std::vector<int> &, std::vector<int> &parts) {
+        parts.assign(pitp.begin() + pitp_off[p], pitp.begin() + pitp_off[p + 1]);
       };
       parallel_ranges(pxs, W, [&](int k, int p0, int p1) {
         std::vector<int> seen(T, -1), parts;
