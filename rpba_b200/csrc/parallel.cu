@@ -286,6 +286,10 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
   // the refined points and the deletions; returns (sum, redundancy) with the
   // per-point contributions summed chunk by chunk
   int status = RPBA_OK;
+  std::vector<double> XXo(3 * (size_t)pxs), s0pt(pxs);
+  std::vector<uint8_t> keep, conv(std::max(pxs, 1));
+  std::vector<float> sv;
+  std::vector<int32_t> redpt(pxs);
   auto sweep = [&](int robustmode, bool weightonly, bool wxy, std::vector<std::vector<float>> *sig0vv,
                    double *sum, long long *redund) {
     TmpBlock tb;
@@ -306,16 +310,23 @@ int32_t plsa_parallel(rpba_block *blk, const rpba_options *opt, int32_t nthreads
     tb.b.K = tb.K.data();
     tb.b.distpara = tb.dist.data();
     const size_t nt = pointXXv.img.size();
-    std::vector<double> XXo(3 * (size_t)pxs), s0pt(pxs);
-    std::vector<uint8_t> keep(std::max<size_t>(nt, 1)), conv(std::max(pxs, 1));
-    std::vector<float> sv(std::max<size_t>(nt, 1));
-    std::vector<int32_t> redpt(pxs);
+    // the merge's outputs (it writes every point's and every track entry's;
+    // the buffers are kept from sweep to sweep: the track only shrinks)
+    if (keep.size() < std::max<size_t>(nt, 1)) {
+      keep.resize(std::max<size_t>(nt, 1));
+      sv.resize(std::max<size_t>(nt, 1));
+    }
     status = merge_fn(&tb.b, PMd.data(), sig0wv.data(), robustmode, weightonly ? 1 : 0, wxy ? imgindbv.data() : nullptr,
                       wxy ? T : 1, opt->device, XXo.data(), keep.data(), sv.data(), conv.data(),
                       wxy ? w3d.data() : nullptr, s0pt.data(), redpt.data());
     if (status != RPBA_OK) return false;
-    if (sig0vv)
-      for (size_t t = 0; t < nt; ++t) (*sig0vv)[pointXXv.img[t]].push_back(sv[t]);
+    if (sig0vv)  // every image's statistics in track order (image ranges on host threads)
+      parallel_ranges(nrimages, nranges(nrimages, workers, 64), [&](int, int i0, int i1) {
+        for (size_t t = 0; t < nt; ++t) {
+          const int i = pointXXv.img[t];
+          if (i >= i0 && i < i1) (*sig0vv)[i].push_back(sv[t]);
+        }
+      });
     // the refined points, and every list without the deleted observations
     // (point ranges on host threads: the kept observations counted, then
     // written at the ranges' prefix sums)
